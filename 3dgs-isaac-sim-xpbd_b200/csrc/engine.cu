@@ -1,0 +1,1229 @@
+// Host engine and C ABI of the B200 XPBD Gaussian-graph solver.
+//
+// One Engine holds one scene resident in HBM.  A step (runXPBDSimulation,
+// forward.cu:12038-12751) is enqueued as a fixed kernel sequence on the engine's stream;
+// all step settings live in a device-side StepParams block that is refreshed before each
+// step, so the sequence is captured once into a CUDA graph and replayed until its
+// topology (iteration count, enabled constraints, colour counts) changes.  The C ABI
+// at the bottom exposes the reference's 29 singleton entry points (xpbd_capi.cu) on top
+// of a process-global engine, plus this library's extensions (xpbd_b200_*).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/xpbd_capi.h"
+#include "kernels.cuh"
+#include "xpbd_internal.h"
+
+namespace xpbd {
+
+static std::string g_err;
+
+static int fail(const char* fmt, ...)
+{
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	g_err = buf;
+	return -1;
+}
+
+#define CK(expr)                                                                           \
+	do {                                                                                   \
+		const cudaError_t e_ = (expr);                                                     \
+		if (e_ != cudaSuccess) return fail("%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
+			__FILE__, __LINE__);                                                           \
+	} while (0)
+
+template <typename T>
+struct DBuf {
+	T* p = nullptr;
+	size_t n = 0;
+	cudaError_t alloc(size_t count)
+	{
+		release();
+		n = count;
+		if (count == 0) return cudaSuccess;
+		return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count);
+	}
+	void release()
+	{
+		if (p) cudaFree(p);
+		p = nullptr;
+		n = 0;
+	}
+	size_t bytes() const { return sizeof(T) * n; }
+};
+
+// Solver settings.  Like the reference's file-static settings (forward.cu:53-92,
+// 224-265, 300-361) they outlive create/destroy; defaults are the reference's.
+struct Settings {
+	int iters = 20;
+	float dt = 1.0f / 60.0f, under_relax = 0.6f, vel_damping = 0.59f, stiffness_scale = 1.0f,
+		inv_mass_scale = 1.0f, dist_compliance = 1e-3f, shape_compliance = 0.0f, shape_blend = 0.1f,
+		angle_compliance = 0.0f, angle_blend = 0.2f;
+	bool use_distance = true, use_shape = false, use_angle = false, use_volume = false, shape_robust = true;
+	float vol_compliance = 1e-6f, vol_aniso = 0.05f;
+	int ring_k = 1, max_members = 64, leader_min_hop = 1;
+	bool topo_dirty = false;
+	bool dist_gs = false, vol_gs = false;
+	int warp_mode = 0;               // 0 auto (warp when mean members >= 40), 1 thread, 2 warp
+	bool sc_enabled = false, sc_within = false;
+	float sc_radius_scale = 1.5f, sc_exclude_scale = 2.0f, sc_search_scale = 1.5f, sc_fast_rel = 0.0f;
+	bool ground_on = false;
+	float ground_n[3] = { 0.0f, 0.0f, 1.0f };
+	float ground_h = 0.0f, ground_friction = 0.5f, ground_restitution = 0.3f, ground_radius = 0.0f,
+		ground_slop = 0.0f, ground_gravity = 0.0f;
+	float object_shape = 0.0f;
+	bool jstats = true;
+	KinCollider kin[kMaxColliders];
+	int kin_count = 0;
+	float kin_margin = 0.0f, kin_friction = 0.0f;
+	bool use_graph = true;
+};
+static Settings S;
+
+enum Stage {
+	ST_PREDICT, ST_DISTANCE, ST_VOL_SOLVE, ST_VOL_GATHER, ST_VOL_GS, ST_SHAPE, ST_SC_BUILD, ST_SC_SOLVE,
+	ST_PROJECT, ST_VELOCITY, ST_JSTATS, ST_OTHER, ST_COUNT
+};
+static const char* kStageNames[ST_COUNT] = { "predict", "distance", "volume_solve", "volume_gather", "volume_gs",
+	"shape", "selfcol_build", "selfcol_solve", "project", "velocity", "jstats", "other" };
+
+class Engine {
+public:
+	// ---- created inputs (caller order) ----
+	int n = 0, n_edges = 0;
+	std::vector<float> in_pos, in_scales, in_rots, in_opacity, in_rest, in_stiff;
+	std::vector<int> in_edges;
+	bool built = false, stepped = false;
+	int generation = 0;
+
+	// ---- host topology ----
+	HostGraph graph;
+	HostClusters clusters;
+	HostEdgeColoring coloring;
+	bool coloring_built = false;
+	std::vector<int> obj_id;
+	int num_objects = 0;
+	float spacing = 0.0f;
+	int sc_table = 0;
+
+	// ---- device state ----
+	DBuf<float4> pos_curr, pos_next, pos_tmp, vel, pos_rest;
+	DBuf<float> pos_out3;
+	DBuf<int> off, nbr;
+	DBuf<float> ndist, nstiff, lam;
+	DBuf<int> vol_off, vol_idx, rev_off, rev_idx, mat_type, vol_gs_order;
+	DBuf<float> det_rest, v_rest, rest_len, sigma_rest, lam_vol;
+	DBuf<float4> rec;
+	DBuf<int2> gs_edge;
+	DBuf<float> gs_rest, gs_stiff, gs_lam;
+	DBuf<unsigned int> sc_keys;
+	DBuf<int> sc_bucket, sc_start, sc_cursor, sc_idx_sorted, sc_contacts, sc_counts, sc_block_sums, d_obj_id;
+	DBuf<float4> sc_dp;
+	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
+	DBuf<int> att_idx;
+	DBuf<float> att_pos;
+	bool att_active = false;
+	StepParams* d_params = nullptr;
+	StepParams* h_params = nullptr;
+	DevCounters* d_ctr = nullptr;
+	DevCounters* h_ctr = nullptr;
+	int* h_att_idx = nullptr;
+	float* h_att_pos = nullptr;
+	int h_att_cap = 0;
+
+	// ---- execution ----
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	cudaGraphExec_t graph_exec = nullptr;
+	std::vector<long long> graph_key;
+	long long graph_kernels = 0;
+	long long launches = 0;
+	bool profiling = false;
+	struct Rec { int stage; cudaEvent_t a, b; };
+	std::vector<Rec> prof_records;
+	std::vector<cudaEvent_t> event_pool;
+	size_t event_next = 0;
+	double prof_ms[ST_COUNT] = {};
+	long long prof_count[ST_COUNT] = {};
+
+	~Engine() { release(); }
+
+	void release()
+	{
+		if (graph_exec) cudaGraphExecDestroy(graph_exec);
+		graph_exec = nullptr;
+		graph_key.clear();
+		free_device();
+		if (d_params) cudaFree(d_params);
+		if (h_params) cudaFreeHost(h_params);
+		if (d_ctr) cudaFree(d_ctr);
+		if (h_ctr) cudaFreeHost(h_ctr);
+		if (h_att_idx) cudaFreeHost(h_att_idx);
+		if (h_att_pos) cudaFreeHost(h_att_pos);
+		d_params = nullptr; h_params = nullptr; d_ctr = nullptr; h_ctr = nullptr;
+		h_att_idx = nullptr; h_att_pos = nullptr; h_att_cap = 0;
+		for (auto& e : event_pool) cudaEventDestroy(e);
+		event_pool.clear();
+		prof_records.clear();
+		if (own_stream && stream) cudaStreamDestroy(stream);
+		stream = nullptr;
+		own_stream = false;
+	}
+
+	void free_device()
+	{
+		pos_curr.release(); pos_next.release(); pos_tmp.release(); vel.release(); pos_rest.release();
+		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
+		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
+		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
+		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
+		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
+		sc_contacts.release(); sc_counts.release(); sc_block_sums.release(); d_obj_id.release(); sc_dp.release();
+		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
+		att_idx.release(); att_pos.release();
+		att_active = false;
+		coloring_built = false;
+		sc_table = 0;
+		built = false;
+	}
+
+	int ensure_stream()
+	{
+		if (!stream) {
+			CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+			own_stream = true;
+		}
+		if (!d_params) {
+			CK(cudaMalloc(&d_params, sizeof(StepParams)));
+			CK(cudaMallocHost(&h_params, sizeof(StepParams)));
+			CK(cudaMalloc(&d_ctr, sizeof(DevCounters)));
+			CK(cudaMallocHost(&h_ctr, sizeof(DevCounters)));
+			CK(cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), stream));
+			memset(h_ctr, 0, sizeof(DevCounters));
+		}
+		return 0;
+	}
+
+	// ------------------------------------------------------------------ build
+	// ensureChainmailGPU (forward.cu:10519-10845): graph upload, colourings, clusters
+	int build()
+	{
+		free_device();
+		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		graph_key.clear();
+		if (ensure_stream()) return -1;
+		build_graph(n, n_edges, in_edges.data(), in_rest.data(), in_stiff.data(), graph);
+		const int m = graph.off[n];
+		std::vector<float4> p4(n);
+		for (int i = 0; i < n; ++i) p4[i] = make_float4(in_pos[3 * i], in_pos[3 * i + 1], in_pos[3 * i + 2], 1.0f);
+		CK(pos_curr.alloc(n)); CK(pos_next.alloc(n)); CK(pos_tmp.alloc(n)); CK(vel.alloc(n)); CK(pos_rest.alloc(n));
+		CK(pos_out3.alloc(3 * (size_t)n));
+		CK(cudaMemcpyAsync(pos_curr.p, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+		for (auto& v : p4) v.w = 0.0f;
+		CK(cudaMemcpyAsync(pos_rest.p, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemsetAsync(vel.p, 0, vel.bytes(), stream));
+		CK(cudaMemcpyAsync(pos_out3.p, in_pos.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+		CK(off.alloc(n + 1)); CK(nbr.alloc(std::max(m, 1))); CK(ndist.alloc(std::max(m, 1)));
+		CK(nstiff.alloc(std::max(m, 1))); CK(lam.alloc(std::max(m, 1)));
+		CK(cudaMemcpyAsync(off.p, graph.off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		if (m > 0) {
+			CK(cudaMemcpyAsync(nbr.p, graph.nbr.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(ndist.p, graph.ndist.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(nstiff.p, graph.nstiff.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
+		}
+		CK(d_scales.alloc(3 * (size_t)n)); CK(d_rots.alloc(4 * (size_t)n));
+		CK(d_out_scales.alloc(3 * (size_t)n)); CK(d_out_quats.alloc(4 * (size_t)n));
+		CK(cudaMemcpyAsync(d_scales.p, in_scales.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(d_rots.p, in_rots.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, stream));
+		CK(det_rest.alloc(n)); CK(v_rest.alloc(n)); CK(rest_len.alloc(n)); CK(sigma_rest.alloc(6 * (size_t)n));
+		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * (size_t)n));
+		CK(cudaMemsetAsync(rec.p, 0, rec.bytes(), stream));
+		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
+		build_components(graph, 50, obj_id, num_objects);
+		CK(d_obj_id.alloc(n));
+		CK(cudaMemcpyAsync(d_obj_id.p, obj_id.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+		spacing = graph_spacing(graph);
+		S.topo_dirty = false;
+		if (rebuild_clusters()) return -1;
+		CK(cudaStreamSynchronize(stream));
+		++generation;
+		built = true;
+		return 0;
+	}
+
+	// rebuildVolumeClusters (forward.cu:9814-10403): host BFS/FPS, then rest covariance on the GPU
+	int rebuild_clusters()
+	{
+		build_clusters(graph, in_pos.data(), S.ring_k, S.max_members, S.leader_min_hop, clusters);
+		const size_t nv = std::max<size_t>(clusters.vol_idx.size(), 1), nr = std::max<size_t>(clusters.rev_idx.size(), 1);
+		CK(vol_off.alloc(n + 1)); CK(vol_idx.alloc(nv)); CK(rev_off.alloc(n + 1)); CK(rev_idx.alloc(nr));
+		CK(cudaMemcpyAsync(vol_off.p, clusters.vol_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(vol_idx.p, clusters.vol_idx.data(), sizeof(int) * clusters.vol_idx.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(rev_off.p, clusters.rev_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(rev_idx.p, clusters.rev_idx.data(), sizeof(int) * clusters.rev_idx.size(), cudaMemcpyHostToDevice, stream));
+		vol_gs_order.release();
+		if (!clusters.gs_order.empty()) {
+			CK(vol_gs_order.alloc(clusters.gs_order.size()));
+			CK(cudaMemcpyAsync(vol_gs_order.p, clusters.gs_order.data(), sizeof(int) * clusters.gs_order.size(),
+				cudaMemcpyHostToDevice, stream));
+		}
+		const int blocks = (n + kBlock - 1) / kBlock;
+		dev::k_volume_rest<<<blocks, kBlock, 0, stream>>>(n, pos_rest.p, vol_off.p, vol_idx.p, off.p, nbr.p,
+			S.vol_aniso, sigma_rest.p, det_rest.p, v_rest.p, rest_len.p, mat_type.p);
+		CK(cudaGetLastError());
+		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
+		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		graph_key.clear();
+		++generation;
+		return 0;
+	}
+
+	int ensure_coloring()
+	{
+		if (coloring_built) return 0;
+		build_edge_coloring(graph, coloring);
+		const size_t ne = coloring.edge.size();
+		CK(gs_edge.alloc(std::max<size_t>(ne, 1))); CK(gs_rest.alloc(std::max<size_t>(ne, 1)));
+		CK(gs_stiff.alloc(std::max<size_t>(ne, 1))); CK(gs_lam.alloc(std::max<size_t>(ne, 1)));
+		if (ne) {
+			CK(cudaMemcpyAsync(gs_edge.p, coloring.edge.data(), sizeof(int2) * ne, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(gs_rest.p, coloring.rest.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(gs_stiff.p, coloring.stiff.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, stream));
+		}
+		CK(cudaStreamSynchronize(stream));
+		coloring_built = true;
+		return 0;
+	}
+
+	// selfColEnsureBuffers (forward.cu:11728-11758): table = pow2 >= max(1024, 2N)
+	int ensure_selfcol()
+	{
+		if (sc_table) return 0;
+		int table = 1024;
+		while (table < 2 * n) table <<= 1;
+		sc_table = table;
+		const int buckets = table + 1;   // + sentinel bucket
+		CK(sc_keys.alloc(n)); CK(sc_bucket.alloc(buckets + 1)); CK(sc_start.alloc(buckets + 1));
+		CK(sc_cursor.alloc(buckets)); CK(sc_idx_sorted.alloc(n)); CK(sc_contacts.alloc((size_t)n * kSelfColMax));
+		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
+		CK(cudaMemsetAsync(sc_counts.p, 0, sc_counts.bytes(), stream));
+		return 0;
+	}
+
+	// ------------------------------------------------------------------ params
+	void fill_params()
+	{
+		StepParams& P = *h_params;
+		memset(&P, 0, sizeof(P));
+		P.dt = S.dt;
+		P.inv_mass_scale = S.inv_mass_scale;
+		P.stiffness_scale = S.stiffness_scale;
+		P.under_relax = S.under_relax;
+		P.dist_compliance = S.dist_compliance;
+		P.vol_compliance = S.vol_compliance;
+		P.shape_compliance = S.shape_compliance;
+		P.shape_blend = S.shape_blend;
+		P.vel_damping = S.vel_damping;
+		// stepPhysicsOnly gravity: -g * n when g > 0 (forward.cu:13257-13259)
+		if (S.ground_gravity > 0.0f) {
+			P.gx = -S.ground_gravity * S.ground_n[0];
+			P.gy = -S.ground_gravity * S.ground_n[1];
+			P.gz = -S.ground_gravity * S.ground_n[2];
+		}
+		P.ground_on = S.ground_on ? 1 : 0;
+		for (int k = 0; k < 3; ++k) P.gn[k] = S.ground_n[k];
+		P.ground_plane = S.ground_h + S.ground_radius;
+		P.ground_slop = S.ground_slop;
+		P.ground_friction = S.ground_friction;
+		P.ground_restitution = S.ground_restitution;
+		P.resting_speed = 2.0f * S.ground_gravity * S.dt;
+		P.kin_count = S.kin_count;
+		P.kin_margin = S.kin_margin;
+		P.kin_friction = S.kin_friction;
+		memcpy(P.kin, S.kin, sizeof(KinCollider) * S.kin_count);
+		// selfColBuild constants (forward.cu:11798-11831), host float arithmetic
+		const float dc = S.sc_radius_scale * spacing;
+		const float search = S.sc_search_scale * dc;
+		const float excl = S.sc_exclude_scale * dc;
+		P.sc_dc = dc;
+		P.sc_search = search;
+		P.sc_excl2 = excl * excl;
+		P.sc_cross_excl2 = dc * dc;
+		P.sc_fast_rel = S.sc_fast_rel * dc;
+		P.sc_search_plus16dc = search + 16.0f * dc;
+		P.sc_within = S.sc_within ? 1 : 0;
+	}
+
+	bool use_warp() const
+	{
+		if (S.warp_mode == 2) return true;
+		if (S.warp_mode == 1) return false;
+		return clusters.avg_members >= 40.0f;
+	}
+	bool selfcol_on() const { return S.sc_enabled && spacing > 0.0f && S.sc_radius_scale * spacing > 0.0f; }
+	bool dist_gs_on() const { return S.use_distance && S.dist_gs && coloring_built && !coloring.edge.empty(); }
+	bool vol_gs_on() const { return S.use_volume && S.vol_gs && clusters.gs_color_off.size() > 1; }
+
+	std::vector<long long> topology_key() const
+	{
+		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), use_warp(),
+			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
+			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table };
+	}
+
+	// ------------------------------------------------------------------ launching
+	template <typename K, typename... A>
+	void launch(int stage, dim3 grid, dim3 block, K kernel, A... args)
+	{
+		cudaEvent_t a = nullptr, b = nullptr;
+		if (profiling) {
+			a = next_event();
+			b = next_event();
+			cudaEventRecord(a, stream);
+		}
+		kernel<<<grid, block, 0, stream>>>(args...);
+		++launches;
+		if (profiling) {
+			cudaEventRecord(b, stream);
+			prof_records.push_back({ stage, a, b });
+		}
+	}
+	cudaEvent_t next_event()
+	{
+		if (event_next == event_pool.size()) {
+			cudaEvent_t e;
+			cudaEventCreate(&e);
+			event_pool.push_back(e);
+		}
+		return event_pool[event_next++];
+	}
+	static dim3 blocks_for(long long items, int per_block = kBlock)
+	{
+		return dim3((unsigned)((items + per_block - 1) / per_block));
+	}
+
+	// one step's kernel sequence (the body of runXPBDSimulation)
+	int enqueue_step()
+	{
+		const int N = n;
+		const dim3 B(kBlock), G = blocks_for(N);
+		const dim3 GW = blocks_for((long long)N * 32);   // one warp per Gaussian / cluster
+		const bool sc = selfcol_on();
+		CK(cudaMemsetAsync(d_ctr, 0, offsetof(DevCounters, jstats), stream));
+		launch(ST_PREDICT, G, B, dev::k_predict, N, (const StepParams*)d_params, (const float4*)pos_curr.p, pos_next.p,
+			vel.p, S.use_volume ? lam_vol.p : (float*)nullptr);
+		if (sc) {
+			const int buckets = sc_table + 1;
+			CK(cudaMemsetAsync(sc_bucket.p, 0, sc_bucket.bytes(), stream));
+			CK(cudaMemsetAsync(sc_cursor.p, 0, sc_cursor.bytes(), stream));
+			launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr);
+			launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_keys, N, (const float4*)pos_curr.p, (const DevCounters*)d_ctr,
+				(unsigned)(sc_table - 1), (unsigned)sc_table, sc_keys.p, sc_bucket.p);
+			const int scan_n = buckets + 1;
+			const int nb = (scan_n + 1023) / 1024;
+			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_blocks, (const int*)sc_bucket.p, sc_start.p, scan_n,
+				sc_block_sums.p);
+			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, nb);
+			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_add, sc_start.p, scan_n, (const int*)sc_block_sums.p);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_scatter, N, (const unsigned*)sc_keys.p, (const int*)sc_start.p,
+				sc_cursor.p, sc_idx_sorted.p);
+			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
+				sc_idx_sorted.p);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_build, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
+				(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p,
+				(const int*)sc_start.p, (unsigned)(sc_table - 1), (const int*)d_obj_id.p, d_ctr, sc_contacts.p,
+				sc_counts.p);
+		}
+		float4* pin = pos_next.p;
+		float4* pout = pos_tmp.p;
+		const bool dgs = dist_gs_on(), vgs = vol_gs_on(), warp = use_warp();
+		const bool project = S.kin_count > 0 || S.ground_on || sc;
+		for (int it = 0; it < S.iters; ++it) {
+			const int first = (it == 0), last = (it == S.iters - 1);
+			if (dgs) {
+				for (size_t c = 0; c + 1 < coloring.color_off.size(); ++c) {
+					const int begin = coloring.color_off[c], count = coloring.color_off[c + 1] - begin;
+					if (count <= 0) continue;
+					launch(ST_DISTANCE, blocks_for(count), B, dev::k_distance_gs, begin, count, N,
+						(const StepParams*)d_params, pin, (const int2*)gs_edge.p, (const float*)gs_rest.p,
+						(const float*)gs_stiff.p, gs_lam.p, first ? 0 : 1);
+				}
+			}
+			else if (S.use_distance) {
+				launch(ST_DISTANCE, G, B, dev::k_distance_jacobi, N, (const StepParams*)d_params, (const float4*)pin,
+					pout, (const int*)off.p, (const int*)nbr.p, (const float*)ndist.p, (const float*)nstiff.p, lam.p,
+					first ? 0 : 1, last ? 0 : 1);
+				std::swap(pin, pout);
+			}
+			if (S.use_volume) {
+				if (vgs) {
+					for (size_t c = 0; c + 1 < clusters.gs_color_off.size(); ++c) {
+						const int begin = clusters.gs_color_off[c], count = clusters.gs_color_off[c + 1] - begin;
+						if (count <= 0) continue;
+						launch(ST_VOL_GS, blocks_for(count, 64), dim3(64), dev::k_volume_gs, begin, count,
+							(const int*)vol_gs_order.p, N, (const StepParams*)d_params, pin, (const int*)vol_off.p,
+							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p,
+							(const float*)rest_len.p, 1);
+					}
+				}
+				else {
+					if (warp)
+						launch(ST_VOL_SOLVE, GW, B, dev::k_volume_solve_warp<8>, N, (const StepParams*)d_params,
+							(const float4*)pin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, first ? 0 : 1);
+					else
+						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, (const StepParams*)d_params,
+							(const float4*)pin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, first ? 0 : 1);
+					if (warp)
+						launch(ST_VOL_GATHER, GW, B, dev::k_volume_gather_warp, N, (const StepParams*)d_params,
+							(const float4*)pin, pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p,
+							(const float*)rest_len.p);
+					else
+						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, (const StepParams*)d_params,
+							(const float4*)pin, pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p,
+							(const float*)rest_len.p);
+					std::swap(pin, pout);
+				}
+			}
+			if (S.use_shape) {
+				launch(ST_SHAPE, G, B, dev::k_shape_match, N, (const StepParams*)d_params, (const float4*)pin, pout,
+					(const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p, S.shape_robust ? 1 : 0);
+				std::swap(pin, pout);
+			}
+			if (sc)
+				launch(ST_SC_SOLVE, G, B, dev::k_sc_solve, N, (const StepParams*)d_params, (const float4*)pin,
+					(const float4*)pos_curr.p, (const float4*)pos_rest.p, (const int*)sc_contacts.p,
+					(const int*)sc_counts.p, (const DevCounters*)d_ctr, sc_dp.p);
+			if (project)
+				launch(ST_PROJECT, G, B, dev::k_project, N, (const StepParams*)d_params, pin, (const float4*)pos_curr.p,
+					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0);
+		}
+		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
+			vel.p, pos_out3.p);
+		if (S.jstats) {
+			CK(cudaMemsetAsync(d_ctr->jstats, 0, sizeof(double) * 3, stream));
+			launch(ST_JSTATS, G, B, dev::k_jstats, N, (const float4*)pos_curr.p, (const int*)vol_off.p,
+				(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, (const float*)v_rest.p,
+				d_ctr);
+		}
+		CK(cudaGetLastError());
+		return 0;
+	}
+
+	// ------------------------------------------------------------------ step
+	int step_async()
+	{
+		if (!built) {
+			if (build()) return -1;
+		}
+		else if (S.topo_dirty) {
+			S.topo_dirty = false;
+			if (rebuild_clusters()) return -1;
+		}
+		if (S.use_distance && S.dist_gs && ensure_coloring()) return -1;
+		if (S.sc_enabled && ensure_selfcol()) return -1;
+		fill_params();
+		CK(cudaMemcpyAsync(d_params, h_params, sizeof(StepParams), cudaMemcpyHostToDevice, stream));
+		if (profiling || !S.use_graph) {
+			if (enqueue_step()) return -1;
+		}
+		else {
+			const auto key = topology_key();
+			if (!graph_exec || key != graph_key) {
+				if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+				cudaGraph_t g = nullptr;
+				CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+				const long long before = launches;
+				const int rc = enqueue_step();
+				const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+				if (rc) { if (g) cudaGraphDestroy(g); return -1; }
+				CK(ec);
+				graph_kernels = launches - before;
+				launches = before;
+				const cudaError_t ei = cudaGraphInstantiate(&graph_exec, g, 0);
+				cudaGraphDestroy(g);
+				CK(ei);
+				graph_key = key;
+			}
+			CK(cudaGraphLaunch(graph_exec, stream));
+			launches += graph_kernels;
+		}
+		stepped = true;
+		return 0;
+	}
+
+	int sync()
+	{
+		CK(cudaStreamSynchronize(stream));
+		CK(cudaGetLastError());
+		return 0;
+	}
+
+	int read_counters()
+	{
+		CK(cudaMemcpyAsync(h_ctr, d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream));
+		CK(cudaStreamSynchronize(stream));
+		return 0;
+	}
+
+	void profile_collect()
+	{
+		if (!prof_records.empty()) cudaStreamSynchronize(stream);
+		for (const auto& r : prof_records) {
+			float ms = 0.0f;
+			if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+				prof_ms[r.stage] += ms;
+				prof_count[r.stage] += 1;
+			}
+		}
+		prof_records.clear();
+		event_next = 0;
+	}
+
+	// ------------------------------------------------------------------ attach
+	// setAttachedParticles (forward.cu:6759-6788): restore the saved inverse masses, save
+	// them on first use, then pin idx[] at pos[].
+	int set_attached(int count, const int* idx, const float* pos)
+	{
+		const int N = n;
+		if (att_active)
+			dev::k_set_w<<<blocks_for(N), kBlock, 0, stream>>>(N, pos_curr.p, inv_mass_saved.p, 0.0f);
+		if (count <= 0 || !idx || !pos) {
+			att_active = false;
+			CK(cudaGetLastError());
+			return 0;
+		}
+		if (!att_active) {
+			if (!inv_mass_saved.p) CK(inv_mass_saved.alloc(N));
+			dev::k_get_w<<<blocks_for(N), kBlock, 0, stream>>>(N, pos_curr.p, inv_mass_saved.p);
+		}
+		if (count > h_att_cap) {
+			CK(cudaStreamSynchronize(stream));
+			if (h_att_idx) cudaFreeHost(h_att_idx);
+			if (h_att_pos) cudaFreeHost(h_att_pos);
+			CK(cudaMallocHost(&h_att_idx, sizeof(int) * count));
+			CK(cudaMallocHost(&h_att_pos, sizeof(float) * 3 * count));
+			CK(att_idx.alloc(count));
+			CK(att_pos.alloc(3 * (size_t)count));
+			h_att_cap = count;
+		}
+		else CK(cudaStreamSynchronize(stream));   // the pinned staging buffers may still be in flight
+		memcpy(h_att_idx, idx, sizeof(int) * count);
+		memcpy(h_att_pos, pos, sizeof(float) * 3 * count);
+		CK(cudaMemcpyAsync(att_idx.p, h_att_idx, sizeof(int) * count, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(att_pos.p, h_att_pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
+		dev::k_attach<<<blocks_for(count), kBlock, 0, stream>>>(count, att_idx.p, att_pos.p, N, pos_curr.p, vel.p);
+		CK(cudaGetLastError());
+		att_active = true;
+		return 0;
+	}
+};
+
+static Engine* g_engine = nullptr;
+
+static Engine& engine()
+{
+	if (!g_engine) g_engine = new Engine();
+	return *g_engine;
+}
+
+}  // namespace xpbd
+
+using namespace xpbd;
+
+// ============================================================================
+// C ABI: the reference's entry points (xpbd_capi.cu:66-310); XPBD_API carries the
+// extern "C" linkage
+// ============================================================================
+
+XPBD_API const char* xpbd_last_error(void) { return g_err.c_str(); }
+
+XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const float* rots, const float* opacity, int e,
+	const int* edges, const float* rest, const float* stiff)
+{
+	Engine& E = engine();
+	E.free_device();
+	E.n = 0;
+	E.stepped = false;
+	if (n <= 0 || !pos || !scales || !rots || !opacity || e < 0 || (e > 0 && (!edges || !rest || !stiff)))
+		return fail("xpbd_create: invalid arguments");
+	E.n = n;
+	E.n_edges = e;
+	E.in_pos.assign(pos, pos + 3 * (size_t)n);
+	E.in_scales.assign(scales, scales + 3 * (size_t)n);
+	E.in_rots.assign(rots, rots + 4 * (size_t)n);
+	E.in_opacity.assign(opacity, opacity + n);
+	E.in_edges.assign(edges ? edges : (const int*)nullptr, edges ? edges + 2 * (size_t)e : (const int*)nullptr);
+	E.in_rest.assign(rest ? rest : (const float*)nullptr, rest ? rest + e : (const float*)nullptr);
+	E.in_stiff.assign(stiff ? stiff : (const float*)nullptr, stiff ? stiff + e : (const float*)nullptr);
+	if (E.ensure_stream()) return -1;
+	return 0;
+}
+
+XPBD_API void xpbd_destroy(void)
+{
+	S.kin_count = 0;
+	if (g_engine) {
+		g_engine->sync();
+		g_engine->free_device();
+		g_engine->n = 0;
+		g_engine->stepped = false;
+	}
+}
+
+XPBD_API int xpbd_count(void) { return g_engine ? g_engine->n : 0; }
+
+XPBD_API void xpbd_set_solver(int iters, float dt, float underRelax, float velDamping, float stiffnessScale,
+	float invMassScale, float distCompliance, float shapeCompliance, float shapeBlend, float angleCompliance,
+	float angleBlend)
+{
+	// setXPBDParams (forward.cu:4896-4922)
+	S.iters = iters < 1 ? 1 : iters;
+	S.dt = fmaxf(1e-5f, dt);
+	S.under_relax = fmaxf(0.0f, underRelax);
+	S.vel_damping = fmaxf(0.0f, velDamping);
+	S.stiffness_scale = fmaxf(0.0f, stiffnessScale);
+	S.inv_mass_scale = fmaxf(0.0f, invMassScale);
+	S.dist_compliance = fmaxf(0.0f, distCompliance);
+	S.shape_compliance = fmaxf(0.0f, shapeCompliance);
+	S.shape_blend = fminf(fmaxf(0.0f, shapeBlend), 1.0f);
+	S.angle_compliance = fmaxf(0.0f, angleCompliance);
+	S.angle_blend = fminf(fmaxf(0.0f, angleBlend), 1.0f);
+}
+
+XPBD_API void xpbd_set_constraints(int distance, int shape, int angle, int volume)
+{
+	S.use_distance = distance != 0;
+	S.use_shape = shape != 0;
+	S.use_angle = angle != 0;
+	S.use_volume = volume != 0;
+}
+
+XPBD_API void xpbd_set_volume(float compliance, int ringK, int maxMembers, int leaderMinHop)
+{
+	// setVolumeParams / setVolumeRingK / setVolumeLeaderParams (forward.cu:3849, 3934-3966)
+	S.vol_compliance = compliance;
+	S.ring_k = std::max(1, std::min(8, ringK));
+	S.max_members = std::max(8, std::min(8192, maxMembers));
+	S.leader_min_hop = std::max(1, std::min(8, leaderMinHop));
+	S.topo_dirty = true;
+}
+
+XPBD_API void xpbd_set_ground(int enabled, float ux, float uy, float uz, float height, float friction,
+	float restitution, float contactRadius, float contactSlop, float gravity)
+{
+	// setGroundParams (forward.cu:4430-4446)
+	float nx = ux, ny = uy, nz = uz;
+	const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+	if (!(len > 1e-8f) || !std::isfinite(len)) { nx = 0.0f; ny = 0.0f; nz = 1.0f; }
+	else { nx /= len; ny /= len; nz /= len; }
+	S.ground_n[0] = nx; S.ground_n[1] = ny; S.ground_n[2] = nz;
+	S.ground_on = enabled != 0;
+	S.ground_h = std::isfinite(height) ? height : 0.0f;
+	S.ground_friction = fmaxf(0.0f, friction);
+	S.ground_restitution = fminf(fmaxf(restitution, 0.0f), 1.0f);
+	S.ground_radius = fmaxf(0.0f, contactRadius);
+	S.ground_slop = fmaxf(0.0f, contactSlop);
+	S.ground_gravity = fmaxf(0.0f, gravity);
+}
+
+XPBD_API void xpbd_set_object_shape(float stiffness)
+{
+	float s = fminf(fmaxf(stiffness, 0.0f), 1.0f);
+	if (!std::isfinite(s)) s = 0.0f;
+	if (s > 0.0f && S.object_shape == 0.0f)
+		fprintf(stderr, "[xpbd_b200] object-level shape keeping is not implemented; stiffness %.3f ignored\n", s);
+	S.object_shape = s;
+}
+
+XPBD_API void xpbd_set_object_shape_gpu(int enabled) { (void)enabled; }
+
+XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses, const float* dims, float margin,
+	float friction)
+{
+	// setKinematicColliders (forward.cu:4478-4500)
+	if (count < 0) count = 0;
+	if (count > kMaxColliders) count = kMaxColliders;
+	const bool same = (count == S.kin_count);
+	for (int c = 0; c < count; ++c) {
+		KinCollider& K = S.kin[c];
+		const bool keep = same && K.type == types[c];
+		for (int a = 0; a < 9; ++a) K.Rp[a] = keep ? K.R[a] : poses[12 * c + a];
+		for (int a = 0; a < 3; ++a) K.tp[a] = keep ? K.t[a] : poses[12 * c + 9 + a];
+		K.type = types[c];
+		for (int a = 0; a < 9; ++a) K.R[a] = poses[12 * c + a];
+		for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
+	}
+	S.kin_count = count;
+	S.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
+	S.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
+}
+
+XPBD_API int xpbd_collider_stats(int* hits, float* push, float* centroid, int maxCount)
+{
+	// getKinematicColliderStats (forward.cu:4502-4519)
+	const int n = std::min(maxCount, S.kin_count);
+	if (n <= 0 || !g_engine || !g_engine->stepped) return 0;
+	if (g_engine->read_counters()) return 0;
+	const DevCounters& C = *g_engine->h_ctr;
+	for (int c = 0; c < n; ++c) {
+		if (hits) hits[c] = C.kin_hits[c];
+		const float* a = &C.kin_push[kColliderAcc * c];
+		for (int k = 0; k < 3; ++k) {
+			if (push) push[3 * c + k] = a[k];
+			if (centroid) centroid[3 * c + k] = (a[6] > 0.0f) ? a[3 + k] / a[6] : S.kin[c].t[k];
+		}
+	}
+	return n;
+}
+
+XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const float* center)
+{
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_add_rigid_velocity: no step yet");
+	Engine& E = *g_engine;
+	dev::k_add_rigid_velocity<<<Engine::blocks_for(E.n), kBlock, 0, E.stream>>>(E.n, E.pos_curr.p, E.vel.p,
+		make_float3(dv[0], dv[1], dv[2]), make_float3(dw[0], dw[1], dw[2]), make_float3(center[0], center[1], center[2]));
+	CK(cudaGetLastError());
+	return E.sync();
+}
+
+XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
+{
+	(void)tau; (void)radiusCap;
+	if (!g_engine || g_engine->n <= 0) return fail("xpbd_set_contact_shape: call xpbd_create first");
+	if (enabled) return fail("xpbd_set_contact_shape: ellipsoid contact shapes are not implemented");
+	return 0;
+}
+
+XPBD_API int xpbd_set_attached(int count, const int* idx, const float* pos, float weight)
+{
+	(void)weight;
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_set_attached: no step yet");
+	if (g_engine->set_attached(count, idx, pos)) return -1;
+	return 0;
+}
+
+XPBD_API void xpbd_set_self_collision(int enabled, float radiusScale, float excludeScale, int withinBody)
+{
+	// setSelfCollisionParams (forward.cu:4532-4540)
+	S.sc_enabled = enabled != 0;
+	S.sc_within = withinBody != 0;
+	S.sc_radius_scale = fminf(fmaxf(std::isfinite(radiusScale) ? radiusScale : 1.5f, 0.1f), 10.0f);
+	S.sc_exclude_scale = fminf(fmaxf(std::isfinite(excludeScale) ? excludeScale : 2.0f, 1.05f), 20.0f);
+}
+
+XPBD_API void xpbd_self_collision_stats(int* out)
+{
+	out[0] = out[1] = out[2] = 0;
+	if (!g_engine || !g_engine->stepped || !S.sc_enabled) return;
+	if (g_engine->read_counters()) return;
+	out[0] = (int)g_engine->h_ctr->sc_contacts;
+	out[1] = g_engine->n;
+	out[2] = (int)g_engine->h_ctr->sc_overflow;
+}
+
+XPBD_API void xpbd_set_shape_robust(int enabled) { S.shape_robust = enabled != 0; }
+
+XPBD_API int xpbd_step(void)
+{
+	if (!g_engine || g_engine->n <= 0) return fail("xpbd_step: call xpbd_create first");
+	if (g_engine->step_async()) return -1;
+	return g_engine->sync();
+}
+
+XPBD_API unsigned long long xpbd_positions_device(void)
+{
+	if (!g_engine || !g_engine->stepped) return 0ull;
+	return reinterpret_cast<unsigned long long>(g_engine->pos_out3.p);
+}
+
+XPBD_API int xpbd_positions_host(float* out, int n)
+{
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_positions_host: no step yet");
+	Engine& E = *g_engine;
+	if (!out || n != E.n) return fail("xpbd_positions_host: size mismatch");
+	CK(cudaMemcpy2DAsync(out, sizeof(float) * 3, E.pos_curr.p, sizeof(float4), sizeof(float) * 3, n,
+		cudaMemcpyDeviceToHost, E.stream));
+	return E.sync();
+}
+
+XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* hostQuats, int n)
+{
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_compute_shapes: no step yet");
+	Engine& E = *g_engine;
+	if (n != E.n) return fail("xpbd_compute_shapes: size mismatch");
+	CK(cudaMemsetAsync(&E.d_ctr->shapes_deformed, 0, sizeof(unsigned int) * 2, E.stream));
+	dev::k_deformed_shapes<<<Engine::blocks_for(n), kBlock, 0, E.stream>>>(n, E.pos_rest.p, E.pos_curr.p, E.off.p,
+		E.nbr.p, E.d_scales.p, E.d_rots.p, deformEps, E.d_out_scales.p, E.d_out_quats.p, E.d_ctr);
+	CK(cudaGetLastError());
+	if (hostScales)
+		CK(cudaMemcpyAsync(hostScales, E.d_out_scales.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, E.stream));
+	if (hostQuats)
+		CK(cudaMemcpyAsync(hostQuats, E.d_out_quats.p, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost, E.stream));
+	if (E.read_counters()) return -1;
+	return (int)E.h_ctr->shapes_deformed;
+}
+
+XPBD_API int xpbd_reset(void)
+{
+	// setAttachedParticles(0) then squashReset (forward.cu:4411-4427)
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_reset: no step yet");
+	Engine& E = *g_engine;
+	if (E.set_attached(0, nullptr, nullptr)) return -1;
+	std::vector<float4> p4(E.n);
+	for (int i = 0; i < E.n; ++i) p4[i] = make_float4(E.in_pos[3 * i], E.in_pos[3 * i + 1], E.in_pos[3 * i + 2], 1.0f);
+	CK(cudaMemcpyAsync(E.pos_curr.p, p4.data(), sizeof(float4) * E.n, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.pos_out3.p, E.in_pos.data(), sizeof(float) * 3 * E.n, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemsetAsync(E.vel.p, 0, E.vel.bytes(), E.stream));
+	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
+	return E.sync();
+}
+
+XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt)
+{
+	// groundLaunch (forward.cu:4551-4610): rest pose rotated about the centre of mass,
+	// rigid velocity field, inverse masses 1
+	if (!g_engine || !g_engine->stepped) return fail("xpbd_launch: no step yet");
+	Engine& E = *g_engine;
+	const int N = E.n;
+	double cx = 0.0, cy = 0.0, cz = 0.0;
+	for (int i = 0; i < N; ++i) { cx += E.in_pos[3 * i]; cy += E.in_pos[3 * i + 1]; cz += E.in_pos[3 * i + 2]; }
+	const float comX = float(cx / N), comY = float(cy / N), comZ = float(cz / N);
+	const float ax = tilt ? tilt[0] : 0.0f, ay = tilt ? tilt[1] : 0.0f, az = tilt ? tilt[2] : 0.0f;
+	const float th = sqrtf(ax * ax + ay * ay + az * az);
+	float R[9] = { 1, 0, 0, 0, 1, 0, 0, 0, 1 };
+	if (th > 1e-8f) {
+		const float kx = ax / th, ky = ay / th, kz = az / th;
+		const float s = sinf(th), c = cosf(th), t = 1.0f - c;
+		R[0] = c + t * kx * kx; R[1] = t * kx * ky - s * kz; R[2] = t * kx * kz + s * ky;
+		R[3] = t * ky * kx + s * kz; R[4] = c + t * ky * ky; R[5] = t * ky * kz - s * kx;
+		R[6] = t * kz * kx - s * ky; R[7] = t * kz * ky + s * kx; R[8] = c + t * kz * kz;
+	}
+	const float vx = lin ? lin[0] : 0.0f, vy = lin ? lin[1] : 0.0f, vz = lin ? lin[2] : 0.0f;
+	const float wx = ang ? ang[0] : 0.0f, wy = ang ? ang[1] : 0.0f, wz = ang ? ang[2] : 0.0f;
+	std::vector<float4> p4(N), v4(N);
+	std::vector<float> p3(3 * (size_t)N);
+	for (int i = 0; i < N; ++i) {
+		const float px = E.in_pos[3 * i] - comX, py = E.in_pos[3 * i + 1] - comY, pz = E.in_pos[3 * i + 2] - comZ;
+		const float rx = R[0] * px + R[1] * py + R[2] * pz;
+		const float ry = R[3] * px + R[4] * py + R[5] * pz;
+		const float rz = R[6] * px + R[7] * py + R[8] * pz;
+		p4[i] = make_float4(comX + rx, comY + ry, comZ + rz, 1.0f);
+		p3[3 * i] = p4[i].x; p3[3 * i + 1] = p4[i].y; p3[3 * i + 2] = p4[i].z;
+		v4[i] = make_float4(vx + (wy * rz - wz * ry), vy + (wz * rx - wx * rz), vz + (wx * ry - wy * rx), 0.0f);
+	}
+	CK(cudaMemcpyAsync(E.pos_curr.p, p4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.vel.p, v4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.pos_out3.p, p3.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
+	return E.sync();
+}
+
+XPBD_API int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo)
+{
+	(void)axis; (void)rampPerSec; (void)maxDispPct; (void)fromLo;
+	return fail("xpbd_press_start: the press harness is not implemented");
+}
+XPBD_API void xpbd_press_autolog(int enabled) { (void)enabled; }
+XPBD_API void xpbd_press_stop(void) {}
+XPBD_API int xpbd_press_state(float* lo, float* hi, float* cur, float* mx)
+{
+	if (lo) *lo = 0.0f;
+	if (hi) *hi = 0.0f;
+	if (cur) *cur = 0.0f;
+	if (mx) *mx = 0.0f;
+	return 0;
+}
+
+XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd)
+{
+	// setVolumeJStatsEnabled + getVolumeJVolumeWeighted (forward.cu:4081-4099)
+	S.jstats = enable != 0;
+	float m = 1.0f, s = 0.0f;
+	if (g_engine && g_engine->stepped && !g_engine->read_counters()) {
+		const double* a = g_engine->h_ctr->jstats;
+		if (a[0] > 0.0) {
+			const double mean = a[1] / a[0];
+			m = (float)mean;
+			s = (float)sqrt(fmax(0.0, a[2] / a[0] - mean * mean));
+		}
+	}
+	if (jvw) *jvw = m;
+	if (jvwStd) *jvwStd = s;
+}
+
+// ============================================================================
+// extensions (no counterpart in the reference ABI)
+// ============================================================================
+XPBD_API int xpbd_b200_set_stream(void* stream)
+{
+	Engine& E = engine();
+	if (E.own_stream && E.stream) {
+		cudaStreamSynchronize(E.stream);
+		cudaStreamDestroy(E.stream);
+	}
+	E.own_stream = false;
+	E.stream = static_cast<cudaStream_t>(stream);
+	if (E.graph_exec) { cudaGraphExecDestroy(E.graph_exec); E.graph_exec = nullptr; }
+	E.graph_key.clear();
+	if (!E.stream) return E.ensure_stream();
+	return 0;
+}
+
+XPBD_API int xpbd_b200_step_async(int substeps)
+{
+	if (!g_engine || g_engine->n <= 0) return fail("xpbd_b200_step_async: call xpbd_create first");
+	for (int s = 0; s < substeps; ++s)
+		if (g_engine->step_async()) return -1;
+	return 0;
+}
+
+XPBD_API int xpbd_b200_sync(void) { return g_engine ? g_engine->sync() : 0; }
+
+XPBD_API void xpbd_b200_set_gs(int distance, int volume)
+{
+	S.dist_gs = distance != 0;
+	S.vol_gs = volume != 0;
+}
+
+XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { S.warp_mode = std::max(0, std::min(2, mode)); }
+
+XPBD_API void xpbd_b200_set_graph(int enabled) { S.use_graph = enabled != 0; }
+
+XPBD_API int xpbd_b200_set_profiling(int enabled)
+{
+	Engine& E = engine();
+	if (E.profiling) E.profile_collect();
+	E.profiling = enabled != 0;
+	return 0;
+}
+
+XPBD_API int xpbd_b200_stage_times(double* ms, long long* counts, int max_stages)
+{
+	Engine& E = engine();
+	E.profile_collect();
+	const int k = std::min(max_stages, (int)ST_COUNT);
+	for (int s = 0; s < k; ++s) {
+		if (ms) ms[s] = E.prof_ms[s];
+		if (counts) counts[s] = E.prof_count[s];
+	}
+	return k;
+}
+
+XPBD_API void xpbd_b200_reset_stage_times(void)
+{
+	Engine& E = engine();
+	E.profile_collect();
+	for (int s = 0; s < ST_COUNT; ++s) { E.prof_ms[s] = 0.0; E.prof_count[s] = 0; }
+}
+
+XPBD_API const char* xpbd_b200_stage_name(int stage)
+{
+	return (stage >= 0 && stage < ST_COUNT) ? kStageNames[stage] : "";
+}
+
+XPBD_API long long xpbd_b200_launch_count(void) { return g_engine ? g_engine->launches : 0; }
+
+XPBD_API int xpbd_b200_sizes(long long* out)
+{
+	// [0] N, [1] directed edges, [2] cluster members, [3] reverse entries, [4] GS edges,
+	// [5] GS edge colours, [6] GS clusters, [7] GS cluster colours, [8] hash table, [9] candidates
+	for (int k = 0; k < 10; ++k) out[k] = 0;
+	if (!g_engine || !g_engine->built) return -1;
+	Engine& E = *g_engine;
+	out[0] = E.n;
+	out[1] = E.graph.off[E.n];
+	out[2] = E.clusters.vol_off.empty() ? 0 : E.clusters.vol_off[E.n];
+	out[3] = E.clusters.rev_off.empty() ? 0 : E.clusters.rev_off[E.n];
+	out[4] = (long long)E.coloring.edge.size();
+	out[5] = E.coloring.color_off.empty() ? 0 : (long long)E.coloring.color_off.size() - 1;
+	out[6] = (long long)E.clusters.gs_order.size();
+	out[7] = E.clusters.gs_color_off.empty() ? 0 : (long long)E.clusters.gs_color_off.size() - 1;
+	out[8] = E.sc_table;
+	if (E.sc_table && !E.read_counters()) out[9] = E.h_ctr->sc_contacts;
+	return 0;
+}
+
+namespace {
+template <typename T>
+int copy_dev(const T* src, long long count, T* out, long long cap, cudaStream_t st)
+{
+	if (!src || count < 0) return -1;
+	if (!out) return (int)count;
+	if (cap < count) return -1;
+	if (count > 0) {
+		if (cudaMemcpyAsync(out, src, sizeof(T) * (size_t)count, cudaMemcpyDeviceToHost, st) != cudaSuccess) return -1;
+		if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+	}
+	return (int)count;
+}
+template <typename T>
+int copy_host(const std::vector<T>& v, long long count, T* out, long long cap)
+{
+	if (count < 0 || (long long)v.size() < count) return -1;
+	if (!out) return (int)count;
+	if (cap < count) return -1;
+	std::copy(v.begin(), v.begin() + count, out);
+	return (int)count;
+}
+}  // namespace
+
+// Stage buffers by name, in the reference's layouts (counts per row instead of N+1
+// row starts, sorted hash order, candidate lists).  Count only when out == NULL.
+XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap)
+{
+	if (!g_engine || !g_engine->built) return -1;
+	Engine& E = *g_engine;
+	const int N = E.n;
+	const std::string s(name);
+	auto counts_of = [&](const std::vector<int>& off) {
+		std::vector<int> c(N);
+		for (int i = 0; i < N; ++i) c[i] = off[i + 1] - off[i];
+		return c;
+	};
+	if (s == "nbr_offset") return copy_host(E.graph.off, N, out, cap);
+	if (s == "nbr_count") return copy_host(counts_of(E.graph.off), N, out, cap);
+	if (s == "nbr_idx") return copy_host(E.graph.nbr, E.graph.off[N], out, cap);
+	if (s == "vol_offset") return copy_host(E.clusters.vol_off, N, out, cap);
+	if (s == "vol_count") return copy_host(counts_of(E.clusters.vol_off), N, out, cap);
+	if (s == "vol_idx") return copy_host(E.clusters.vol_idx, E.clusters.vol_off[N], out, cap);
+	if (s == "rev_offset") return copy_host(E.clusters.rev_off, N, out, cap);
+	if (s == "rev_count") return copy_host(counts_of(E.clusters.rev_off), N, out, cap);
+	if (s == "rev_idx") return copy_host(E.clusters.rev_idx, E.clusters.rev_off[N], out, cap);
+	if (s == "vol_gs_order") return copy_host(E.clusters.gs_order, (long long)E.clusters.gs_order.size(), out, cap);
+	if (s == "vol_gs_color_offset")
+		return copy_host(E.clusters.gs_color_off, (long long)E.clusters.gs_color_off.size(), out, cap);
+	if (s == "obj_id") return copy_host(E.obj_id, N, out, cap);
+	if (s == "mat_type") return copy_dev(E.mat_type.p, N, out, cap, E.stream);
+	if (s == "gs_edge" || s == "gs_color_offset") {
+		if (E.ensure_coloring()) return -1;
+		if (s == "gs_color_offset") return copy_host(E.coloring.color_off, (long long)E.coloring.color_off.size(), out, cap);
+		std::vector<int> flat(2 * E.coloring.edge.size());
+		for (size_t e = 0; e < E.coloring.edge.size(); ++e) { flat[2 * e] = E.coloring.edge[e].x; flat[2 * e + 1] = E.coloring.edge[e].y; }
+		return copy_host(flat, (long long)flat.size(), out, cap);
+	}
+	if (!E.sc_table) return -1;
+	if (s == "sc_keys") return copy_dev(reinterpret_cast<const int*>(E.sc_keys.p), N, out, cap, E.stream);
+	if (s == "sc_idx_sorted") return copy_dev(E.sc_idx_sorted.p, N, out, cap, E.stream);
+	if (s == "sc_count") return copy_dev(E.sc_counts.p, N, out, cap, E.stream);
+	if (s == "sc_contact") return copy_dev(E.sc_contacts.p, (long long)N * kSelfColMax, out, cap, E.stream);
+	if (s == "sc_keys_sorted" || s == "sc_cell_start" || s == "sc_cell_end") {
+		std::vector<int> start(E.sc_table + 2), keys(N), idx(N);
+		if (copy_dev(E.sc_start.p, E.sc_table + 2, start.data(), E.sc_table + 2, E.stream) < 0) return -1;
+		if (s == "sc_keys_sorted") {
+			if (copy_dev(reinterpret_cast<const int*>(E.sc_keys.p), N, keys.data(), N, E.stream) < 0) return -1;
+			if (copy_dev(E.sc_idx_sorted.p, N, idx.data(), N, E.stream) < 0) return -1;
+			std::vector<int> ks(N);
+			for (int t = 0; t < N; ++t) ks[t] = keys[idx[t]];
+			return copy_host(ks, N, out, cap);
+		}
+		std::vector<int> v(E.sc_table);
+		for (int k = 0; k < E.sc_table; ++k) {
+			const bool any = start[k + 1] > start[k];
+			v[k] = (s == "sc_cell_start") ? (any ? start[k] : -1) : (any ? start[k + 1] : -1);
+		}
+		return copy_host(v, E.sc_table, out, cap);
+	}
+	return -1;
+}
+
+XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
+{
+	if (!g_engine || !g_engine->built) return -1;
+	Engine& E = *g_engine;
+	const int N = E.n;
+	const std::string s(name);
+	if (s == "det_rest") return copy_dev(E.det_rest.p, N, out, cap, E.stream);
+	if (s == "sigma_rest") return copy_dev(E.sigma_rest.p, 6LL * N, out, cap, E.stream);
+	if (s == "v_rest") return copy_dev(E.v_rest.p, N, out, cap, E.stream);
+	if (s == "rest_len") return copy_dev(E.rest_len.p, N, out, cap, E.stream);
+	if (s == "gs_rest" || s == "gs_stiff") {
+		if (E.ensure_coloring()) return -1;
+		const auto& v = (s == "gs_rest") ? E.coloring.rest : E.coloring.stiff;
+		return copy_host(v, (long long)v.size(), out, cap);
+	}
+	if (s == "vel" || s == "inv_mass") {
+		std::vector<float4> tmp(N);
+		if (copy_dev(s == "vel" ? E.vel.p : E.pos_curr.p, N, tmp.data(), N, E.stream) < 0) return -1;
+		std::vector<float> v(s == "vel" ? 3 * (size_t)N : N);
+		for (int i = 0; i < N; ++i) {
+			if (s == "vel") { v[3 * i] = tmp[i].x; v[3 * i + 1] = tmp[i].y; v[3 * i + 2] = tmp[i].z; }
+			else v[i] = tmp[i].w;
+		}
+		return copy_host(v, (long long)v.size(), out, cap);
+	}
+	if (s == "self_col") {
+		if (!out) return 3;
+		if (cap < 3) return -1;
+		if (E.read_counters()) return -1;
+		out[0] = E.spacing;
+		out[1] = S.sc_radius_scale * E.spacing;
+		out[2] = E.h_ctr->sc_reach;
+		return 3;
+	}
+	return -1;
+}
+
+// The once-per-step self-collision build on caller-given start / predicted positions
+// (x[3N], p[3N]); the candidate total, or -1.  Used to check the hash, order and
+// candidate lists stage by stage.
+XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
+{
+	if (!g_engine || !g_engine->built || !x || !p) return fail("xpbd_b200_selfcol_build: no scene");
+	Engine& E = *g_engine;
+	if (E.ensure_selfcol()) return -1;
+	E.fill_params();
+	const int N = E.n;
+	std::vector<float4> a(N), b(N);
+	for (int i = 0; i < N; ++i) {
+		a[i] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 1.0f);
+		b[i] = make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 1.0f);
+	}
+	std::vector<float4> keep_curr(N), keep_next(N);
+	CK(cudaMemcpyAsync(keep_curr.data(), E.pos_curr.p, sizeof(float4) * N, cudaMemcpyDeviceToHost, E.stream));
+	CK(cudaMemcpyAsync(keep_next.data(), E.pos_next.p, sizeof(float4) * N, cudaMemcpyDeviceToHost, E.stream));
+	CK(cudaStreamSynchronize(E.stream));
+	CK(cudaMemcpyAsync(E.d_params, E.h_params, sizeof(StepParams), cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.pos_curr.p, a.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.pos_next.p, b.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemsetAsync(E.d_ctr, 0, sizeof(DevCounters), E.stream));
+	const dim3 B(kBlock), G = Engine::blocks_for(N);
+	const int buckets = E.sc_table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
+	CK(cudaMemsetAsync(E.sc_bucket.p, 0, E.sc_bucket.bytes(), E.stream));
+	CK(cudaMemsetAsync(E.sc_cursor.p, 0, E.sc_cursor.bytes(), E.stream));
+	dev::k_sc_disp<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.pos_next.p, E.d_ctr);
+	dev::k_sc_setup<<<1, 1, 0, E.stream>>>(E.d_params, E.d_ctr);
+	dev::k_sc_keys<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.d_ctr, (unsigned)(E.sc_table - 1), (unsigned)E.sc_table,
+		E.sc_keys.p, E.sc_bucket.p);
+	dev::k_scan_blocks<<<nb, 1024, 0, E.stream>>>(E.sc_bucket.p, E.sc_start.p, scan_n, E.sc_block_sums.p);
+	dev::k_scan_sums<<<1, 1024, 0, E.stream>>>(E.sc_block_sums.p, nb);
+	dev::k_scan_add<<<nb, 1024, 0, E.stream>>>(E.sc_start.p, scan_n, E.sc_block_sums.p);
+	dev::k_sc_scatter<<<G, B, 0, E.stream>>>(N, E.sc_keys.p, E.sc_start.p, E.sc_cursor.p, E.sc_idx_sorted.p);
+	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p);
+	dev::k_sc_build<<<G, B, 0, E.stream>>>(N, E.d_params, E.pos_curr.p, E.pos_next.p, E.pos_rest.p, E.sc_idx_sorted.p,
+		E.sc_start.p, (unsigned)(E.sc_table - 1), E.d_obj_id.p, E.d_ctr, E.sc_contacts.p, E.sc_counts.p);
+	CK(cudaGetLastError());
+	if (E.read_counters()) return -1;
+	// restore the solver state this stage check borrowed
+	CK(cudaMemcpyAsync(E.pos_curr.p, keep_curr.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaMemcpyAsync(E.pos_next.p, keep_next.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
+	CK(cudaStreamSynchronize(E.stream));
+	return (int)E.h_ctr->sc_contacts;
+}

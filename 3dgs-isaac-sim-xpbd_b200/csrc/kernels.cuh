@@ -1,0 +1,1786 @@
+// sm_100a kernels of the XPBD Gaussian-graph step.
+//
+// Every kernel restates one stage of the reference step (runXPBDSimulation,
+// forward.cu:12038-12751) with the same arithmetic order, so results stay within
+// FP32 rounding of the reference; the data layout is this library's own (float4
+// positions with the inverse mass in w, blackboard records as three float4, CSR row
+// starts with an N+1 sentinel, in-place distance multipliers).  None of these stages
+// is a dense contraction, so none uses tensor cores; each is bounded by HBM or L2
+// bandwidth (see the per-kernel notes).
+#pragma once
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "xpbd_internal.h"
+
+namespace xpbd {
+namespace dev {
+
+// ---------------------------------------------------------------------------
+// small helpers (forward.cu:4949-4969; glm mat3 is column-major: m[col][row])
+// ---------------------------------------------------------------------------
+struct M3 { float m[3][3]; };
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 mul3(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ bool fin3(float3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+__device__ __forceinline__ float comp(float3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+__device__ __forceinline__ float4 ld4(const float4* p, int i) { return __ldg(p + i); }
+
+__device__ __forceinline__ void m3_zero(M3& a)
+{
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) a.m[c][r] = 0.0f;
+}
+// A += outerProduct(p, q): O[c][r] = p[r] * q[c]
+__device__ __forceinline__ void m3_add_outer(M3& A, float3 p, float3 q)
+{
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) A.m[c][r] += comp(p, r) * comp(q, c);
+}
+__device__ __forceinline__ float3 m3_mulv(const M3& M, float3 v)
+{
+	return make_float3(M.m[0][0] * v.x + M.m[1][0] * v.y + M.m[2][0] * v.z,
+		M.m[0][1] * v.x + M.m[1][1] * v.y + M.m[2][1] * v.z,
+		M.m[0][2] * v.x + M.m[1][2] * v.y + M.m[2][2] * v.z);
+}
+__device__ __forceinline__ M3 m3_mul(const M3& A, const M3& B)
+{
+	M3 R;
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+			R.m[c][r] = A.m[0][r] * B.m[c][0] + A.m[1][r] * B.m[c][1] + A.m[2][r] * B.m[c][2];
+	return R;
+}
+__device__ __forceinline__ M3 m3_t(const M3& M)
+{
+	M3 T;
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) T.m[c][r] = M.m[r][c];
+	return T;
+}
+__device__ __forceinline__ float m3_det(const M3& M)
+{
+	const float(*m)[3] = M.m;
+	return +m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2])
+		- m[1][0] * (m[0][1] * m[2][2] - m[2][1] * m[0][2])
+		+ m[2][0] * (m[0][1] * m[1][2] - m[1][1] * m[0][2]);
+}
+__device__ __forceinline__ bool m3_finite(const M3& M)
+{
+	bool ok = true;
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) ok = ok && isfinite(M.m[c][r]);
+	return ok;
+}
+
+// adjugate inverse with an absolute determinant floor (forward.cu:1696-1719)
+__device__ __forceinline__ bool inverse3x3_safe(const M3& M, M3& inv, float eps_det)
+{
+	const float(*m)[3] = M.m;
+	const float a00 = m[0][0], a01 = m[0][1], a02 = m[0][2];
+	const float a10 = m[1][0], a11 = m[1][1], a12 = m[1][2];
+	const float a20 = m[2][0], a21 = m[2][1], a22 = m[2][2];
+	const float det = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) + a02 * (a10 * a21 - a11 * a20);
+	if (fabsf(det) < eps_det) return false;
+	const float invdet = 1.0f / det;
+	inv.m[0][0] = (a11 * a22 - a12 * a21) * invdet;
+	inv.m[0][1] = -(a01 * a22 - a02 * a21) * invdet;
+	inv.m[0][2] = (a01 * a12 - a02 * a11) * invdet;
+	inv.m[1][0] = -(a10 * a22 - a12 * a20) * invdet;
+	inv.m[1][1] = (a00 * a22 - a02 * a20) * invdet;
+	inv.m[1][2] = -(a00 * a12 - a02 * a10) * invdet;
+	inv.m[2][0] = (a10 * a21 - a11 * a20) * invdet;
+	inv.m[2][1] = -(a00 * a21 - a01 * a20) * invdet;
+	inv.m[2][2] = (a00 * a11 - a01 * a10) * invdet;
+	return true;
+}
+
+// cyclic-max float Jacobi, ascending eigenvalues, eigenvectors as glm columns
+// (jacobiEigenDecomposition3x3 + eigenDecomposition_glm, forward.cu:782-901)
+__device__ __noinline__ void eig_sym3f(const M3& Ag, float3& evals, M3& evecs)
+{
+	float A[3][3], V[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) { A[r][c] = Ag.m[c][r]; V[r][c] = (r == c) ? 1.0f : 0.0f; }
+	for (int iter = 0; iter < 50; ++iter) {
+		int p = 0, q = 1;
+		float maxOff = fabsf(A[0][1]);
+		if (fabsf(A[0][2]) > maxOff) { p = 0; q = 2; maxOff = fabsf(A[0][2]); }
+		if (fabsf(A[1][2]) > maxOff) { p = 1; q = 2; maxOff = fabsf(A[1][2]); }
+		if (maxOff < 1e-6f) break;
+		const float app = A[p][p], aqq = A[q][q], apq = A[p][q];
+		const float phi = 0.5f * (aqq - app) / (apq + 1e-20f);
+		const float t = (phi >= 0.0f) ? (1.0f / (phi + sqrtf(1.0f + phi * phi))) : (1.0f / (phi - sqrtf(1.0f + phi * phi)));
+		const float c = 1.0f / sqrtf(1.0f + t * t);
+		const float s = t * c;
+		A[p][p] = app - t * apq;
+		A[q][q] = aqq + t * apq;
+		A[p][q] = A[q][p] = 0.0f;
+		const int r = 3 - p - q;
+		const float arp = A[r][p], arq = A[r][q];
+		A[r][p] = A[p][r] = c * arp - s * arq;
+		A[r][q] = A[q][r] = c * arq + s * arp;
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) {
+			const float vrp = V[rr][p], vrq = V[rr][q];
+			V[rr][p] = c * vrp - s * vrq;
+			V[rr][q] = s * vrp + c * vrq;
+		}
+	}
+	float ev[3] = { A[0][0], A[1][1], A[2][2] };
+#pragma unroll
+	for (int i = 0; i < 2; ++i)
+#pragma unroll
+		for (int j = i + 1; j < 3; ++j)
+			if (ev[i] > ev[j]) {
+				const float te = ev[i]; ev[i] = ev[j]; ev[j] = te;
+#pragma unroll
+				for (int rr = 0; rr < 3; ++rr) { const float tv = V[rr][i]; V[rr][i] = V[rr][j]; V[rr][j] = tv; }
+			}
+	evals = make_float3(ev[0], ev[1], ev[2]);
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) evecs.m[c][rr] = V[rr][c];
+}
+
+// Sigma = s * SigmaHat, s = trace/3 (forward.cu:7666-7676)
+__device__ __forceinline__ bool sigma_scale_det(const M3& S, float& scale, float& det_hat)
+{
+	const float s = (S.m[0][0] + S.m[1][1] + S.m[2][2]) * (1.0f / 3.0f);
+	if (!isfinite(s) || s <= 1e-24f) return false;
+	M3 H;
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) H.m[c][r] = S.m[c][r] / s;
+	const float d = m3_det(H);
+	if (!isfinite(d) || d <= 1e-6f) return false;
+	scale = s;
+	det_hat = d;
+	return true;
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// ---------------------------------------------------------------------------
+// predict (forward.cu:5954-5979); also clears the volume multipliers of the step
+// (forward.cu:12058-12060).  HBM: 16+16 B read, 16+16 B written per Gaussian.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pos_curr, float4* __restrict__ pos_next, float4* __restrict__ vel,
+	float* __restrict__ lam_vol)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 x4 = pos_curr[i];
+	float4 v4 = vel[i];
+	const float dt = P->dt;
+	const float3 g = make_float3(P->gx, P->gy, P->gz);
+	if (lam_vol) lam_vol[i] = 0.0f;
+	if (x4.w > 0.0f) {
+		float3 v = add3(f3(v4), mul3(g, dt));
+		const float3 p = add3(f3(x4), mul3(v, dt));
+		pos_next[i] = make_float4(p.x, p.y, p.z, x4.w);
+		vel[i] = make_float4(v.x, v.y, v.z, 0.0f);
+	}
+	else {
+		pos_next[i] = x4;
+		vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// distance constraints, Jacobi (forward.cu:6484-6571).  One thread per Gaussian over
+// its CSR row; the multiplier of each directed edge is owned by that thread, so it is
+// updated in place (the reference ping-pongs two arrays; the value sequence per edge
+// is the same).  The first iteration of a step reads no multiplier (they start at 0)
+// and the last stores none (they are reset next step).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ off,
+	const int* __restrict__ nbr, const float* __restrict__ ndist, const float* __restrict__ nstiff,
+	float* __restrict__ lam, int read_lam, int write_lam)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	const float ims = P->inv_mass_scale, ss = P->stiffness_scale, gc = P->dist_compliance;
+	const float wi = p4.w * ims;
+	float3 accum = make_float3(0.0f, 0.0f, 0.0f);
+	int valid = 0;
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const int e0 = off[idx], e1 = off[idx + 1];
+	for (int edge = e0; edge < e1; ++edge) {
+		const int j = __ldg(nbr + edge);
+		float lambda = read_lam ? lam[edge] : 0.0f;
+		if (j < 0 || j >= n) continue;
+		const float4 q4 = ld4(pin, j);
+		const float3 diff = sub3(pi, f3(q4));
+		const float d = len3(diff);
+		if (d < 1e-7f) continue;
+		const float C = d - __ldg(ndist + edge);
+		const float3 grad = mul3(diff, 1.0f / d);
+		const float wj = q4.w * ims;
+		const float stiff = fmaxf(__ldg(nstiff + edge) * ss, 1e-6f);
+		const float alpha = gc / stiff;
+		const float alpha_tilde = alpha / dt2;
+		const float denom = (wi + wj) + alpha_tilde;
+		if (denom < 1e-8f) continue;
+		const float dl = (-C - alpha_tilde * lambda) / denom;
+		lambda += dl;
+		if (write_lam) lam[edge] = lambda;
+		if (wi > 0.0f) {
+			accum = add3(accum, mul3(grad, wi * dl));
+			valid++;
+		}
+	}
+	float3 out = pi;
+	if (wi > 0.0f && valid > 0) {
+		const float3 avg = mul3(accum, 1.0f / float(valid));
+		out = add3(pi, mul3(avg, P->under_relax));
+	}
+	pout[idx] = make_float4(out.x, out.y, out.z, p4.w);
+}
+
+// distance Gauss-Seidel, one colour: thread per undirected edge, in place
+// (forward.cu:6576-6621)
+__global__ void __launch_bounds__(kBlock) k_distance_gs(int begin, int count, int n, const StepParams* __restrict__ P,
+	float4* __restrict__ pos, const int2* __restrict__ edge, const float* __restrict__ rest,
+	const float* __restrict__ stiff, float* __restrict__ lam, int read_lam)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	const int e = begin + t;
+	const int2 ij = edge[e];
+	if (ij.x < 0 || ij.x >= n || ij.y < 0 || ij.y >= n) return;
+	const float4 a = pos[ij.x], b = pos[ij.y];
+	const float ims = P->inv_mass_scale;
+	const float wi = a.w * ims, wj = b.w * ims;
+	if (wi + wj <= 0.0f) return;
+	const float3 pi = f3(a), pj = f3(b);
+	const float3 diff = sub3(pi, pj);
+	const float d = len3(diff);
+	if (d < 1e-7f) return;
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float s = fmaxf(stiff[e] * P->stiffness_scale, 1e-6f);
+	const float alpha_tilde = (P->dist_compliance / s) / dt2;
+	const float denom = (wi + wj) + alpha_tilde;
+	if (denom < 1e-8f) return;
+	const float C = d - rest[e];
+	const float l = read_lam ? lam[e] : 0.0f;
+	const float dl = (-C - alpha_tilde * l) / denom;
+	lam[e] = l + dl;
+	const float3 nn = mul3(diff, 1.0f / d);
+	if (wi > 0.0f) { const float3 o = add3(pi, mul3(nn, wi * dl)); pos[ij.x] = make_float4(o.x, o.y, o.z, a.w); }
+	if (wj > 0.0f) { const float3 o = sub3(pj, mul3(nn, wj * dl)); pos[ij.y] = make_float4(o.x, o.y, o.z, b.w); }
+}
+
+// ---------------------------------------------------------------------------
+// volume: J and Sigma^-1 of one cluster covariance (forward.cu:8583-8620)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool cluster_j_sinv(const M3& Scur, float det_rest, float& J, float& C, M3& Sinv)
+{
+	float s_cur, det_hat;
+	if (!sigma_scale_det(Scur, s_cur, det_hat)) return false;
+	const float det_cur = s_cur * s_cur * s_cur * det_hat;
+	if (det_rest < 1e-30f) return false;
+	J = sqrtf(det_cur / det_rest);
+	if (!isfinite(J) || J <= 0.0f) return false;
+	if (J > 3.0f || J < 0.333f) J = fminf(3.0f, fmaxf(0.333f, J));
+	C = J - 1.0f;
+	if (fabsf(C) < 1e-4f) return false;
+	M3 Sreg = Scur;
+	if (det_hat < 0.2f) {
+		const float d = 0.06f * s_cur;
+		Sreg.m[0][0] += d; Sreg.m[1][1] += d; Sreg.m[2][2] += d;
+	}
+	return inverse3x3_safe(Sreg, Sinv, 1e-20f);
+}
+
+__device__ __forceinline__ void store_record(float4* rec, int idx, float3 c, float coef, const M3& S)
+{
+	rec[3 * idx + 0] = make_float4(c.x, c.y, c.z, coef);
+	rec[3 * idx + 1] = make_float4(S.m[0][0], S.m[1][1], S.m[2][2], S.m[1][0]);
+	rec[3 * idx + 2] = make_float4(S.m[2][0], S.m[2][1], 0.0f, 0.0f);
+}
+
+// Kernel A, one warp per cluster (forward.cu:8702-8863).  Lane L owns members
+// L, L+32, ...; their positions stay in registers across the centroid, covariance
+// and denominator passes (up to VC per lane), butterfly sums give every lane the
+// totals.  Reads per cluster: m member indices + m gathered positions (L2-resident).
+template <int VC>
+__global__ void __launch_bounds__(kBlock) k_volume_solve_warp(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, int read_lam)
+{
+	const int lane = threadIdx.x & 31;
+	const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (idx >= n) return;
+	if (mat_type[idx] != 0) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
+	const int off = voff[idx], cnt = voff[idx + 1] - off;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	float3 cache[VC];
+	float cw[VC];
+	int nc = 0, ucnt = 0;
+	float3 psum = make_float3(0.0f, 0.0f, 0.0f);
+	for (int k = lane; k < cnt; k += 32) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		const float4 q = ld4(pin, j);
+		psum = add3(psum, f3(q));
+		++ucnt;
+#pragma unroll
+		for (int t = 0; t < VC; ++t)
+			if (t == nc) { cache[t] = f3(q); cw[t] = q.w; }
+		if (nc < VC) ++nc;
+	}
+	const float sx = warp_sum(psum.x), sy = warp_sum(psum.y), sz = warp_sum(psum.z);
+	const int used = (int)(warp_sum((float)ucnt) + 0.5f);
+	if (used < 3) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
+	const float inv_n = 1.0f / (float)(used + 1);
+	const float3 c = make_float3((sx + pi.x) * inv_n, (sy + pi.y) * inv_n, (sz + pi.z) * inv_n);
+	float a00 = 0.f, a11 = 0.f, a22 = 0.f, a01 = 0.f, a02 = 0.f, a12 = 0.f;
+#pragma unroll
+	for (int t = 0; t < VC; ++t) {
+		if (t < nc) {
+			const float dx = cache[t].x - c.x, dy = cache[t].y - c.y, dz = cache[t].z - c.z;
+			a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+			a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+		}
+	}
+	if (ucnt > nc) {
+		int seen = 0;
+		for (int k = lane; k < cnt; k += 32) {
+			const int j = __ldg(vidx + off + k);
+			if (j < 0 || j >= n) continue;
+			if (seen++ < nc) continue;
+			const float3 q = f3(ld4(pin, j));
+			const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+			a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+			a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+		}
+	}
+	if (lane == 0) {
+		const float dx = pi.x - c.x, dy = pi.y - c.y, dz = pi.z - c.z;
+		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+	}
+	M3 S;
+	S.m[0][0] = warp_sum(a00) * inv_n;
+	S.m[1][1] = warp_sum(a11) * inv_n;
+	S.m[2][2] = warp_sum(a22) * inv_n;
+	const float s01 = warp_sum(a01) * inv_n, s02 = warp_sum(a02) * inv_n, s12 = warp_sum(a12) * inv_n;
+	S.m[0][1] = S.m[1][0] = s01;
+	S.m[0][2] = S.m[2][0] = s02;
+	S.m[1][2] = S.m[2][1] = s12;
+	float J, C;
+	M3 Sinv;
+	if (!cluster_j_sinv(S, __ldg(det_rest + idx), J, C, Sinv)) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
+	const float gs = J * inv_n;
+	const float ims = P->inv_mass_scale;
+	float dsum = 0.0f;
+#pragma unroll
+	for (int t = 0; t < VC; ++t) {
+		if (t < nc) {
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(cache[t].x - c.x, cache[t].y - c.y, cache[t].z - c.z)), gs);
+			dsum += (cw[t] * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+	}
+	if (ucnt > nc) {
+		int seen = 0;
+		for (int k = lane; k < cnt; k += 32) {
+			const int j = __ldg(vidx + off + k);
+			if (j < 0 || j >= n) continue;
+			if (seen++ < nc) continue;
+			const float4 q = ld4(pin, j);
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+			dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+	}
+	if (lane == 0) {
+		const float3 g = mul3(m3_mulv(Sinv, make_float3(pi.x - c.x, pi.y - c.y, pi.z - c.z)), gs);
+		dsum += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+	}
+	const float denom = warp_sum(dsum);
+	if (lane != 0) return;
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	lam_vol[idx] = lam + dl;
+	store_record(rec, idx, c, dl * gs, Sinv);
+}
+
+// Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
+__global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, int read_lam)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	rec[3 * idx].w = 0.0f;
+	if (mat_type[idx] != 0) return;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	const int off = voff[idx], cnt = voff[idx + 1] - off;
+	float3 c = pi;
+	int used = 0;
+	for (int k = 0; k < cnt; ++k) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		c = add3(c, f3(ld4(pin, j)));
+		++used;
+	}
+	if (used < 3) return;
+	const float inv_n = 1.0f / (float)(used + 1);
+	c = mul3(c, inv_n);
+	M3 S;
+	m3_zero(S);
+	{
+		const float3 d = sub3(pi, c);
+		m3_add_outer(S, d, d);
+	}
+	for (int k = 0; k < cnt; ++k) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		const float3 d = sub3(f3(ld4(pin, j)), c);
+		m3_add_outer(S, d, d);
+	}
+#pragma unroll
+	for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) S.m[cc][r] *= inv_n;
+	float J, C;
+	M3 Sinv;
+	if (!cluster_j_sinv(S, __ldg(det_rest + idx), J, C, Sinv)) return;
+	const float gs = J * inv_n;
+	const float ims = P->inv_mass_scale;
+	float denom = 0.0f;
+	{
+		const float3 g = mul3(m3_mulv(Sinv, sub3(pi, c)), gs);
+		denom += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+	}
+	for (int k = 0; k < cnt; ++k) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		const float4 q = ld4(pin, j);
+		const float3 g = mul3(m3_mulv(Sinv, sub3(f3(q), c)), gs);
+		denom += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+	}
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) return;
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) return;
+	lam_vol[idx] = lam + dl;
+	store_record(rec, idx, c, dl * gs, Sinv);
+}
+
+// one blackboard record applied to a node (forward.cu:9212-9222)
+__device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, int i, float3 pi, float wi, float3& dp)
+{
+	const float4 r0 = __ldg(rec + 3 * i);
+	const float coef = r0.w;
+	if (coef == 0.0f) return false;
+	const float4 r1 = __ldg(rec + 3 * i + 1);
+	const float4 r2 = __ldg(rec + 3 * i + 2);
+	M3 S;
+	S.m[0][0] = r1.x; S.m[1][1] = r1.y; S.m[2][2] = r1.z;
+	S.m[0][1] = S.m[1][0] = r1.w;
+	S.m[0][2] = S.m[2][0] = r2.x;
+	S.m[1][2] = S.m[2][1] = r2.y;
+	const float3 d = sub3(pi, make_float3(r0.x, r0.y, r0.z));
+	const float3 g = m3_mulv(S, d);
+	dp = make_float3(g.x * wi * coef, g.y * wi * coef, g.z * wi * coef);
+	return fin3(dp);
+}
+
+__device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl, float under_relax)
+{
+	if (rl > 1e-12f) {
+		const float max_step = 0.25f * rl;
+		const float len = len3(avg);
+		if (len > max_step && len > 1e-20f) avg = mul3(avg, max_step / len);
+	}
+	return add3(pi, mul3(avg, under_relax));
+}
+
+// Kernel B, one warp per node (forward.cu:9262-9323): mean over the clusters that
+// contain the node, step clamp 0.25 restLen, under-relaxation.  Reads per node: h
+// reverse indices + h gathered 48-byte records (L2-resident).
+__global__ void __launch_bounds__(kBlock) k_volume_gather_warp(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ rest_len)
+{
+	const int lane = threadIdx.x & 31;
+	const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if (idx >= n) return;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	const float wi = p4.w * P->inv_mass_scale;
+	if (wi <= 0.0f) { if (lane == 0) pout[idx] = p4; return; }
+	const int off = roff[idx], cnt = roff[idx + 1] - off;
+	float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+	int received = 0;
+	for (int k = lane; k < cnt; k += 32) {
+		const int i = __ldg(ridx + off + k);
+		if (i < 0 || i >= n) continue;
+		float3 dp;
+		if (!gather_one(rec, i, pi, wi, dp)) continue;
+		sum = add3(sum, dp);
+		++received;
+	}
+	const float sx = warp_sum(sum.x), sy = warp_sum(sum.y), sz = warp_sum(sum.z);
+	const int rc = (int)(warp_sum((float)received) + 0.5f);
+	if (lane != 0) return;
+	if (rc <= 0) { pout[idx] = p4; return; }
+	const float inv_rec = 1.0f / (float)rc;
+	const float3 avg = make_float3(sx * inv_rec, sy * inv_rec, sz * inv_rec);
+	if (!fin3(avg)) { pout[idx] = p4; return; }
+	const float3 o = gather_finish(pi, avg, __ldg(rest_len + idx), P->under_relax);
+	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
+}
+
+// Kernel B, one thread per node (forward.cu:9187-9243)
+__global__ void __launch_bounds__(kBlock) k_volume_gather_thread(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ rest_len)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	const float wi = p4.w * P->inv_mass_scale;
+	if (wi <= 0.0f) { pout[idx] = p4; return; }
+	float3 sum = make_float3(0.0f, 0.0f, 0.0f);
+	int received = 0;
+	for (int k = roff[idx]; k < roff[idx + 1]; ++k) {
+		const int i = __ldg(ridx + k);
+		if (i < 0 || i >= n) continue;
+		float3 dp;
+		if (!gather_one(rec, i, pi, wi, dp)) continue;
+		sum = add3(sum, dp);
+		++received;
+	}
+	if (received <= 0) { pout[idx] = p4; return; }
+	const float3 avg = mul3(sum, 1.0f / (float)received);
+	if (!fin3(avg)) { pout[idx] = p4; return; }
+	const float3 o = gather_finish(pi, avg, __ldg(rest_len + idx), P->under_relax);
+	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
+}
+
+// volume Gauss-Seidel, one colour: thread per cluster, members moved in place with no
+// averaging (forward.cu:9041-9183)
+__global__ void __launch_bounds__(64) k_volume_gs(int begin, int count, const int* __restrict__ order, int n,
+	const StepParams* __restrict__ P, float4* __restrict__ pos, const int* __restrict__ voff,
+	const int* __restrict__ vidx, const float* __restrict__ det_rest, const int* __restrict__ mat_type,
+	float* __restrict__ lam_vol, const float* __restrict__ rest_len, int read_lam)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	const int idx = order[begin + t];
+	if (idx < 0 || idx >= n) return;
+	if (mat_type[idx] != 0) return;
+	const float4 p4 = pos[idx];
+	const float3 pi = f3(p4);
+	const int off = voff[idx], cnt = voff[idx + 1] - off;
+	float3 c = pi;
+	int used = 0;
+	for (int k = 0; k < cnt; ++k) {
+		const int j = vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		c = add3(c, f3(pos[j]));
+		++used;
+	}
+	if (used < 3) return;
+	const float inv_n = 1.0f / (float)(used + 1);
+	c = mul3(c, inv_n);
+	M3 S;
+	m3_zero(S);
+	{
+		const float3 d = sub3(pi, c);
+		m3_add_outer(S, d, d);
+	}
+	for (int k = 0; k < cnt; ++k) {
+		const int j = vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		const float3 d = sub3(f3(pos[j]), c);
+		m3_add_outer(S, d, d);
+	}
+#pragma unroll
+	for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) S.m[cc][r] *= inv_n;
+	float J, C;
+	M3 Sinv;
+	if (!cluster_j_sinv(S, det_rest[idx], J, C, Sinv)) return;
+	const float gs = J * inv_n;
+	const float ims = P->inv_mass_scale;
+	float denom = 0.0f;
+	{
+		const float3 g = mul3(m3_mulv(Sinv, sub3(pi, c)), gs);
+		denom += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+	}
+	for (int k = 0; k < cnt; ++k) {
+		const int j = vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		const float4 q = pos[j];
+		const float3 g = mul3(m3_mulv(Sinv, sub3(f3(q), c)), gs);
+		denom += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+	}
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) return;
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) return;
+	lam_vol[idx] = lam + dl;
+	const float coef = dl * gs;
+	for (int k = -1; k < cnt; ++k) {
+		const int j = (k < 0) ? idx : vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		const float4 xj4 = pos[j];
+		const float wj = xj4.w * ims;
+		if (wj <= 0.0f) continue;
+		const float3 xj = f3(xj4);
+		const float3 g = m3_mulv(Sinv, sub3(xj, c));
+		float3 dp = make_float3(g.x * wj * coef, g.y * wj * coef, g.z * wj * coef);
+		if (!fin3(dp)) continue;
+		const float rl = rest_len[j];
+		if (rl > 1e-12f) {
+			const float max_step = 0.25f * rl;
+			const float len = len3(dp);
+			if (len > max_step && len > 1e-20f) dp = mul3(dp, max_step / len);
+		}
+		const float3 o = add3(xj, dp);
+		pos[j] = make_float4(o.x, o.y, o.z, xj4.w);
+	}
+}
+
+// rest covariance, determinant, volume, rest length, material class per cluster
+// (precomputeVolumeGaussianKernel, forward.cu:7691-7844; mixture rest off)
+__global__ void __launch_bounds__(kBlock) k_volume_rest(int n, const float4* __restrict__ rest,
+	const int* __restrict__ voff, const int* __restrict__ vidx, const int* __restrict__ goff,
+	const int* __restrict__ gnbr, float aniso, float* __restrict__ sigma_rest, float* __restrict__ det_rest,
+	float* __restrict__ v_rest, float* __restrict__ rest_len, int* __restrict__ mat_type)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	float* sig = sigma_rest + (size_t)idx * 6;
+	for (int k = 0; k < 6; ++k) sig[k] = 0.0f;
+	det_rest[idx] = 0.0f;
+	v_rest[idx] = 0.0f;
+	mat_type[idx] = 3;
+	const float3 p0 = f3(rest[idx]);
+	{
+		float dmin = FLT_MAX;
+		for (int e = goff[idx]; e < goff[idx + 1]; ++e) {
+			const int j = gnbr[e];
+			if (j < 0 || j >= n || j == idx) continue;
+			const float dl = len3(sub3(f3(rest[j]), p0));
+			if (dl > 1e-12f) dmin = fminf(dmin, dl);
+		}
+		rest_len[idx] = (dmin < FLT_MAX) ? dmin : 0.0f;
+	}
+	const int off = voff[idx], cnt = voff[idx + 1] - off;
+	if (cnt < 4) return;
+	float3 c = p0;
+	int used = 0;
+	for (int k = 0; k < cnt; ++k) {
+		const int j = vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		c = add3(c, f3(rest[j]));
+		++used;
+	}
+	if (used < 3) return;
+	const float inv_n = 1.0f / (float)(used + 1);
+	c = mul3(c, inv_n);
+	M3 S;
+	m3_zero(S);
+	{
+		const float3 d = sub3(p0, c);
+		m3_add_outer(S, d, d);
+	}
+	for (int k = 0; k < cnt; ++k) {
+		const int j = vidx[off + k];
+		if (j < 0 || j >= n) continue;
+		const float3 d = sub3(f3(rest[j]), c);
+		m3_add_outer(S, d, d);
+	}
+	for (int cc = 0; cc < 3; ++cc)
+		for (int r = 0; r < 3; ++r) S.m[cc][r] *= inv_n;
+	float s_rest, det_hat;
+	if (!sigma_scale_det(S, s_rest, det_hat)) { mat_type[idx] = 4; return; }
+	float3 eig;
+	M3 V;
+	eig_sym3f(S, eig, V);
+	const float lmax = fmaxf(eig.z, 1e-24f);
+	const float a1 = eig.x / lmax, a2 = eig.y / lmax;
+	if (a1 > aniso) mat_type[idx] = 0;
+	else if (a2 > aniso) mat_type[idx] = 1;
+	else mat_type[idx] = 2;
+	sig[0] = S.m[0][0]; sig[1] = S.m[1][1]; sig[2] = S.m[2][2];
+	sig[3] = S.m[1][0]; sig[4] = S.m[2][0]; sig[5] = S.m[2][1];
+	const float d = s_rest * s_rest * s_rest * det_hat;
+	det_rest[idx] = d;
+	v_rest[idx] = (4.0f / 3.0f) * 3.14159265f * sqrtf(fmaxf(d, 0.0f));
+}
+
+// ---------------------------------------------------------------------------
+// shape matching over {i} + 1-ring (forward.cu:6088-6383), FP64 polar rotation
+// (shapeMatchRotationDouble, forward.cu:5991-6086) or the float32 path
+// (forward.cu:6238-6319); XPBD pull toward the goal (forward.cu:4972-4988).
+// ---------------------------------------------------------------------------
+__device__ __noinline__ bool shape_rotation_double(const M3& A, M3& Rout)
+{
+	double a[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) a[r][c] = (double)A.m[c][r];
+	double m[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) m[r][c] = a[0][r] * a[0][c] + a[1][r] * a[1][c] + a[2][r] * a[2][c];
+	double v[3][3] = { { 1.0, 0.0, 0.0 }, { 0.0, 1.0, 0.0 }, { 0.0, 0.0, 1.0 } };
+	for (int iter = 0; iter < 50; ++iter) {
+		bool done = true;
+		int p = 0, q = 1;
+		double max_off = -1.0;
+#pragma unroll
+		for (int k = 0; k < 3; ++k) {
+			const int pk = (k == 2) ? 1 : 0, qk = (k == 0) ? 1 : 2;
+			const double off = fabs(m[pk][qk]);
+			if (off > 1e-12 * sqrt(fabs(m[pk][pk] * m[qk][qk])) + 1e-300) done = false;
+			if (off > max_off) { max_off = off; p = pk; q = qk; }
+		}
+		if (done) break;
+		const double app = m[p][p], aqq = m[q][q], apq = m[p][q];
+		const double phi = 0.5 * (aqq - app) / (apq + 1e-300);
+		const double t = (phi >= 0.0) ? 1.0 / (phi + sqrt(1.0 + phi * phi)) : 1.0 / (phi - sqrt(1.0 + phi * phi));
+		const double c = 1.0 / sqrt(1.0 + t * t);
+		const double s = t * c;
+		m[p][p] = app - t * apq;
+		m[q][q] = aqq + t * apq;
+		m[p][q] = m[q][p] = 0.0;
+		const int r = 3 - p - q;
+		const double arp = m[r][p], arq = m[r][q];
+		m[r][p] = m[p][r] = c * arp - s * arq;
+		m[r][q] = m[q][r] = c * arq + s * arp;
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) {
+			const double vrp = v[rr][p], vrq = v[rr][q];
+			v[rr][p] = c * vrp - s * vrq;
+			v[rr][q] = s * vrp + c * vrq;
+		}
+	}
+	double ev[3] = { m[0][0], m[1][1], m[2][2] };
+#pragma unroll
+	for (int i = 0; i < 2; ++i)
+#pragma unroll
+		for (int j = i + 1; j < 3; ++j)
+			if (ev[i] > ev[j]) {
+				const double te = ev[i]; ev[i] = ev[j]; ev[j] = te;
+#pragma unroll
+				for (int rr = 0; rr < 3; ++rr) { const double tv = v[rr][i]; v[rr][i] = v[rr][j]; v[rr][j] = tv; }
+			}
+	double S[3], Si[3];
+#pragma unroll
+	for (int i = 0; i < 3; ++i) S[i] = sqrt(ev[i] > 0.0 ? ev[i] : 0.0);
+	const double smax = (S[2] > 1e-300) ? S[2] : 1e-300;
+#pragma unroll
+	for (int i = 0; i < 3; ++i) Si[i] = (S[i] > 1e-12 * smax) ? 1.0 / S[i] : 0.0;
+	double u[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) u[r][c] = (a[r][0] * v[0][c] + a[r][1] * v[1][c] + a[r][2] * v[2][c]) * Si[c];
+	if (S[0] < 0.08 * smax) {
+		const double cx = u[1][1] * u[2][2] - u[2][1] * u[1][2];
+		const double cy = u[2][1] * u[0][2] - u[0][1] * u[2][2];
+		const double cz = u[0][1] * u[1][2] - u[1][1] * u[0][2];
+		const double len = sqrt(cx * cx + cy * cy + cz * cz);
+		if (!(len > 1e-7)) return false;
+		u[0][0] = cx / len; u[1][0] = cy / len; u[2][0] = cz / len;
+	}
+	double R[3][3];
+	for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) R[r][c] = u[r][0] * v[c][0] + u[r][1] * v[c][1] + u[r][2] * v[c][2];
+		const double det = R[0][0] * (R[1][1] * R[2][2] - R[1][2] * R[2][1])
+			- R[0][1] * (R[1][0] * R[2][2] - R[1][2] * R[2][0])
+			+ R[0][2] * (R[1][0] * R[2][1] - R[1][1] * R[2][0]);
+		if (det >= 0.0 || pass == 1) break;
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) u[rr][0] = -u[rr][0];
+	}
+	bool ok = true;
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) {
+			ok = ok && isfinite(R[r][c]);
+			Rout.m[c][r] = (float)R[r][c];
+		}
+	return ok;
+}
+
+__device__ __noinline__ bool shape_rotation_float(const M3& A, M3& Rout)
+{
+	const M3 AtA = m3_mul(m3_t(A), A);
+	float3 S2;
+	M3 V;
+	eig_sym3f(AtA, S2, V);
+	const float3 Sv = make_float3(sqrtf(fmaxf(0.0f, S2.x)), sqrtf(fmaxf(0.0f, S2.y)), sqrtf(fmaxf(0.0f, S2.z)));
+	if (!fin3(Sv)) return false;
+	M3 Si;
+	m3_zero(Si);
+	Si.m[0][0] = (Sv.x > 1e-7f) ? 1.0f / Sv.x : 0.0f;
+	Si.m[1][1] = (Sv.y > 1e-7f) ? 1.0f / Sv.y : 0.0f;
+	Si.m[2][2] = (Sv.z > 1e-7f) ? 1.0f / Sv.z : 0.0f;
+	M3 U = m3_mul(m3_mul(A, V), Si);
+	if (!m3_finite(U)) return false;
+	if (Sv.x < 0.08f * fmaxf(Sv.z, 1e-7f)) {
+		const float3 u1 = make_float3(U.m[1][0], U.m[1][1], U.m[1][2]);
+		const float3 u2 = make_float3(U.m[2][0], U.m[2][1], U.m[2][2]);
+		const float3 cr = make_float3(u1.y * u2.z - u2.y * u1.z, u1.z * u2.x - u2.z * u1.x, u1.x * u2.y - u2.x * u1.y);
+		const float l = sqrtf(dot3(cr, cr));
+		if (!(l > 1e-7f)) return false;
+		U.m[0][0] = cr.x / l; U.m[0][1] = cr.y / l; U.m[0][2] = cr.z / l;
+	}
+	const M3 Vt = m3_t(V);
+	M3 R = m3_mul(U, Vt);
+	if (!m3_finite(R)) return false;
+	if (m3_det(R) < 0.0f) {
+		U.m[0][0] *= -1.0f; U.m[0][1] *= -1.0f; U.m[0][2] *= -1.0f;
+		R = m3_mul(U, Vt);
+		if (!m3_finite(R)) return false;
+	}
+	Rout = R;
+	return true;
+}
+
+__global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
+	const int* __restrict__ off, const int* __restrict__ nbr, int robust)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const float4 p4 = ld4(pin, idx);
+	const float3 pi = f3(p4);
+	const float wi = p4.w * P->inv_mass_scale;
+	if (wi <= 0.0f) { pout[idx] = p4; return; }
+	const int e0 = off[idx], e1 = off[idx + 1];
+	const int cnt = e1 - e0;
+	if (cnt < 4) { pout[idx] = p4; return; }
+	const float3 ri = f3(ld4(rest, idx));
+	float3 com_rest = ri, com_curr = pi;
+	float cluster_count = 1.0f;
+	for (int e = e0; e < e1; ++e) {
+		const int j = __ldg(nbr + e);
+		if (j < 0 || j >= n) continue;
+		com_rest = add3(com_rest, f3(ld4(rest, j)));
+		com_curr = add3(com_curr, f3(ld4(pin, j)));
+		cluster_count += 1.0f;
+	}
+	if (cluster_count < 2.0f) { pout[idx] = p4; return; }
+	const float inv_c = 1.0f / cluster_count;
+	com_rest = mul3(com_rest, inv_c);
+	com_curr = mul3(com_curr, inv_c);
+	{
+		float3 dir_sum = make_float3(0.0f, 0.0f, 0.0f);
+		for (int e = e0; e < e1; ++e) {
+			const int j = __ldg(nbr + e);
+			if (j < 0 || j >= n) continue;
+			const float3 q = sub3(f3(ld4(rest, j)), com_rest);
+			const float len = len3(q);
+			if (len > 1e-7f) dir_sum = add3(dir_sum, mul3(q, 1.0f / len));
+		}
+		const float bias = len3(dir_sum) / fmaxf((float)cnt, 1.0f);
+		if (bias > 0.4f) { pout[idx] = p4; return; }
+	}
+	M3 A;
+	m3_zero(A);
+	m3_add_outer(A, sub3(pi, com_curr), sub3(ri, com_rest));
+	for (int e = e0; e < e1; ++e) {
+		const int j = __ldg(nbr + e);
+		if (j < 0 || j >= n) continue;
+		m3_add_outer(A, sub3(f3(ld4(pin, j)), com_curr), sub3(f3(ld4(rest, j)), com_rest));
+	}
+	float a_norm_sq = 0.0f;
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) a_norm_sq += A.m[c][r] * A.m[c][r];
+	const float a_norm = sqrtf(a_norm_sq);
+	if (!isfinite(a_norm) || a_norm < 1e-8f) { pout[idx] = p4; return; }
+#pragma unroll
+	for (int c = 0; c < 3; ++c)
+#pragma unroll
+		for (int r = 0; r < 3; ++r) A.m[c][r] /= a_norm;
+	M3 R;
+	const bool ok = robust ? shape_rotation_double(A, R) : shape_rotation_float(A, R);
+	if (!ok) { pout[idx] = p4; return; }
+	const float3 goal = add3(com_curr, m3_mulv(R, sub3(ri, com_rest)));
+	const float3 gd = sub3(goal, pi);
+	const float gd2 = dot3(gd, gd);
+	if (!isfinite(gd2) || gd2 < 1e-18f) { pout[idx] = p4; return; }
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_tilde = P->shape_compliance / dt2;
+	const float denom = wi + alpha_tilde;
+	if (denom < 1e-8f) { pout[idx] = p4; return; }
+	const float scale = P->shape_blend * (wi / denom);
+	const float3 o = add3(pi, mul3(sub3(goal, pi), scale));
+	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
+}
+
+// ---------------------------------------------------------------------------
+// per-Gaussian projections at the end of an iteration: self-collision apply
+// (forward.cu:7311-7322), kinematic colliders (forward.cu:7425-7518, point contact)
+// and the ground plane (forward.cu:7405-7421), fused in that order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
+	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
+	DevCounters* __restrict__ ctr, int count_hits)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	float4 p4 = pos[idx];
+	bool moved = false;
+	if (sc_count && sc_count[idx] > 0) {
+		const float4 d = sc_dp[idx];
+		p4.x = p4.x + d.x; p4.y = p4.y + d.y; p4.z = p4.z + d.z;
+		moved = true;
+	}
+	if (p4.w > 0.0f) {
+		float3 p = f3(p4);
+		const int nc = P->kin_count;
+		const float margin = P->kin_margin, mu = P->kin_friction;
+		const float reach = margin + 0.0f;
+		for (int c = 0; c < nc; ++c) {
+			const KinCollider& C = P->kin[c];
+			const float dx = p.x - C.t[0], dy = p.y - C.t[1], dz = p.z - C.t[2];
+			const float q0 = C.R[0] * dx + C.R[3] * dy + C.R[6] * dz;
+			const float q1 = C.R[1] * dx + C.R[4] * dy + C.R[7] * dz;
+			const float q2 = C.R[2] * dx + C.R[5] * dy + C.R[8] * dz;
+			float n0 = 0.0f, n1 = 0.0f, n2 = 1.0f, dist;
+			if (C.type == 1) {
+				const float a0 = fabsf(q0) - C.h[0], a1 = fabsf(q1) - C.h[1], a2 = fabsf(q2) - C.h[2];
+				if (a0 > 0.0f || a1 > 0.0f || a2 > 0.0f) {
+					const float o0 = fmaxf(a0, 0.0f), o1 = fmaxf(a1, 0.0f), o2 = fmaxf(a2, 0.0f);
+					dist = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+					if (dist >= reach) continue;
+					const float inv = 1.0f / fmaxf(dist, 1e-20f);
+					n0 = copysignf(o0 * inv, q0); n1 = copysignf(o1 * inv, q1); n2 = copysignf(o2 * inv, q2);
+				}
+				else {
+					if (a0 >= a1 && a0 >= a2) { dist = a0; n0 = (q0 >= 0.0f) ? 1.0f : -1.0f; n2 = 0.0f; }
+					else if (a1 >= a2) { dist = a1; n1 = (q1 >= 0.0f) ? 1.0f : -1.0f; n2 = 0.0f; }
+					else { dist = a2; n2 = (q2 >= 0.0f) ? 1.0f : -1.0f; }
+				}
+			}
+			else {
+				float e2 = q2;
+				if (C.type == 2) e2 = q2 - fminf(fmaxf(q2, -C.h[1]), C.h[1]);
+				const float r = sqrtf(q0 * q0 + q1 * q1 + e2 * e2);
+				dist = r - C.h[0];
+				if (dist >= reach) continue;
+				if (r > 1e-20f) { n0 = q0 / r; n1 = q1 / r; n2 = e2 / r; }
+			}
+			const float wx = C.R[0] * n0 + C.R[1] * n1 + C.R[2] * n2;
+			const float wy = C.R[3] * n0 + C.R[4] * n1 + C.R[5] * n2;
+			const float wz = C.R[6] * n0 + C.R[7] * n1 + C.R[8] * n2;
+			const float corr = margin - dist;
+			const float3 p_in = p;
+			p.x += wx * corr; p.y += wy * corr; p.z += wz * corr;
+			float3 dp = make_float3(wx * corr, wy * corr, wz * corr);
+			if (mu > 0.0f) {
+				const float ox = C.Rp[0] * q0 + C.Rp[1] * q1 + C.Rp[2] * q2 + C.tp[0];
+				const float oy = C.Rp[3] * q0 + C.Rp[4] * q1 + C.Rp[5] * q2 + C.tp[1];
+				const float oz = C.Rp[6] * q0 + C.Rp[7] * q1 + C.Rp[8] * q2 + C.tp[2];
+				const float4 x0 = pos_start[idx];
+				const float rx = (p.x - x0.x) - (p_in.x - ox), ry = (p.y - x0.y) - (p_in.y - oy),
+					rz = (p.z - x0.z) - (p_in.z - oz);
+				const float rn = rx * wx + ry * wy + rz * wz;
+				const float tx = rx - rn * wx, ty = ry - rn * wy, tz = rz - rn * wz;
+				const float lt = sqrtf(tx * tx + ty * ty + tz * tz);
+				if (lt > 1e-20f) {
+					const float k = fminf(1.0f, mu * corr / lt);
+					p.x -= k * tx; p.y -= k * ty; p.z -= k * tz;
+					dp.x -= k * tx; dp.y -= k * ty; dp.z -= k * tz;
+				}
+			}
+			moved = true;
+			float* acc = &ctr->kin_push[kColliderAcc * c];
+			const float w = sqrtf(dp.x * dp.x + dp.y * dp.y + dp.z * dp.z);
+			atomicAdd(&acc[0], dp.x);
+			atomicAdd(&acc[1], dp.y);
+			atomicAdd(&acc[2], dp.z);
+			atomicAdd(&acc[3], w * p.x);
+			atomicAdd(&acc[4], w * p.y);
+			atomicAdd(&acc[5], w * p.z);
+			atomicAdd(&acc[6], w);
+			if (count_hits) atomicAdd(&ctr->kin_hits[c], 1);
+		}
+		if (P->ground_on) {
+			const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane;
+			if (c < 0.0f) {
+				p = make_float3(p.x - c * P->gn[0], p.y - c * P->gn[1], p.z - c * P->gn[2]);
+				moved = true;
+			}
+		}
+		p4.x = p.x; p4.y = p.y; p4.z = p.z;
+	}
+	if (moved) pos[idx] = p4;
+}
+
+// ---------------------------------------------------------------------------
+// velocity commit (forward.cu:6623-6672) and its ground variant (forward.cu:7528-7599);
+// also refreshes the caller-layout float3 position mirror.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __restrict__ P,
+	float4* __restrict__ pos_curr, const float4* __restrict__ pfinal, float4* __restrict__ vel,
+	float* __restrict__ pos_out3)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const float4 x4 = pos_curr[idx];
+	const float4 p4 = pfinal[idx];
+	const float3 x = f3(x4), p = f3(p4);
+	const float w = p4.w;
+	const float dt = P->dt;
+	float3 v = make_float3(0.0f, 0.0f, 0.0f);
+	if (!P->ground_on) {
+		if (w > 0.0f) {
+			const float3 dx = sub3(p, x);
+			const float dx2 = dot3(dx, dx);
+			if (isfinite(dx2) && !(dx2 < 1e-18f)) {
+				v = mul3(dx, 1.0f / fmaxf(dt, 1e-8f));
+				const float damping = fminf(fmaxf(P->vel_damping, 0.0f), 1.0f);
+				v = mul3(v, 1.0f - damping);
+				if (!fin3(v) || dot3(v, v) < 1e-16f) v = make_float3(0.0f, 0.0f, 0.0f);
+			}
+		}
+	}
+	else if (w > 0.0f) {
+		const float3 v_pre = f3(vel[idx]);
+		const float3 dx = sub3(p, x);
+		const float dx2 = dot3(dx, dx);
+		if (isfinite(dx2)) {
+			v = (dx2 < 1e-18f) ? make_float3(0.0f, 0.0f, 0.0f) : mul3(dx, 1.0f / fmaxf(dt, 1e-8f));
+			const float3 nn = make_float3(P->gn[0], P->gn[1], P->gn[2]);
+			const float gap = nn.x * p.x + nn.y * p.y + nn.z * p.z - P->ground_plane;
+			if (gap <= P->ground_slop) {
+				const float vn = nn.x * v.x + nn.y * v.y + nn.z * v.z;
+				const float vn_pre = nn.x * v_pre.x + nn.y * v_pre.y + nn.z * v_pre.z;
+				float vn_new = vn, jn = 0.0f;
+				if (vn_pre < 0.0f) {
+					const float e = (-vn_pre <= P->resting_speed) ? 0.0f : P->ground_restitution;
+					vn_new = fmaxf(vn, -e * vn_pre);
+					jn = -(1.0f + e) * vn_pre;
+				}
+				float3 vt = make_float3(v.x - vn * nn.x, v.y - vn * nn.y, v.z - vn * nn.z);
+				const float vt_len = len3(vt);
+				const float dvt = P->ground_friction * jn;
+				if (vt_len <= dvt || vt_len < 1e-12f) vt = make_float3(0.0f, 0.0f, 0.0f);
+				else vt = mul3(vt, (vt_len - dvt) / vt_len);
+				v = make_float3(vt.x + vn_new * nn.x, vt.y + vn_new * nn.y, vt.z + vn_new * nn.z);
+			}
+			const float damping = fminf(fmaxf(P->vel_damping, 0.0f), 1.0f);
+			v = mul3(v, 1.0f - damping);
+			if (!fin3(v) || dot3(v, v) < 1e-16f) v = make_float3(0.0f, 0.0f, 0.0f);
+		}
+	}
+	vel[idx] = make_float4(v.x, v.y, v.z, 0.0f);
+	pos_curr[idx] = p4;
+	if (pos_out3) {
+		pos_out3[3 * idx + 0] = p.x;
+		pos_out3[3 * idx + 1] = p.y;
+		pos_out3[3 * idx + 2] = p.z;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// self-collision (forward.cu:6984-7322, 11796-11849), spatial hash of the step's start
+// positions, stable counting sort (same order as a stable radix sort of (key, index)),
+// per-particle candidate lists, and the two-phase per-iteration solve.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned int sc_hash(int cx, int cy, int cz, unsigned int mask)
+{
+	return (((unsigned int)cx * 73856093u) ^ ((unsigned int)cy * 19349663u) ^ ((unsigned int)cz * 83492791u)) & mask;
+}
+__device__ __forceinline__ int sc_cell(float v, float inv_cell)
+{
+	return (int)floorf(fminf(fmaxf(v * inv_cell, -1.0e9f), 1.0e9f));
+}
+
+// max predict displacement^2 (selfColDispKernel + DeviceReduce::Max)
+__global__ void __launch_bounds__(kBlock) k_sc_disp(int n, const float4* __restrict__ x, const float4* __restrict__ p,
+	DevCounters* __restrict__ ctr)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	float d2 = 0.0f;
+	if (i < n) {
+		const float4 a = x[i], b = p[i];
+		const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+		const float v = dx * dx + dy * dy + dz * dz;
+		d2 = isfinite(v) ? v : 0.0f;
+	}
+	for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+	__shared__ float smax[kBlock / 32];
+	if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = d2;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		float v = (threadIdx.x < blockDim.x / 32) ? smax[threadIdx.x] : 0.0f;
+		for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+		if (threadIdx.x == 0) atomicMax(&ctr->sc_max_disp2_bits, __float_as_uint(v));
+	}
+}
+
+// cell size = search + 2 max|p - x|, capped (forward.cu:11818-11831)
+__global__ void k_sc_setup(const StepParams* __restrict__ P, DevCounters* __restrict__ ctr)
+{
+	const float md2 = __uint_as_float(ctr->sc_max_disp2_bits);
+	const float md = (isfinite(md2) && md2 > 0.0f) ? sqrtf(md2) : 0.0f;
+	float reach = P->sc_search + 2.0f * md;
+	const float cap = P->sc_search_plus16dc;
+	if (reach > cap) reach = cap;
+	ctr->sc_reach = reach;
+	ctr->sc_inv_cell = 1.0f / reach;
+}
+
+// hash keys of start positions + bucket counts (selfColKeyKernel)
+__global__ void __launch_bounds__(kBlock) k_sc_keys(int n, const float4* __restrict__ x, const DevCounters* __restrict__ ctr,
+	unsigned int mask, unsigned int sentinel, unsigned int* __restrict__ keys, int* __restrict__ bucket)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 p = x[i];
+	const float inv_cell = ctr->sc_inv_cell;
+	unsigned int k = sentinel;
+	if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z))
+		k = sc_hash(sc_cell(p.x, inv_cell), sc_cell(p.y, inv_cell), sc_cell(p.z, inv_cell), mask);
+	keys[i] = k;
+	atomicAdd(&bucket[k], 1);
+}
+
+// exclusive scan of bucket counts, three phases (block sums, scan of sums, apply)
+__global__ void __launch_bounds__(1024) k_scan_blocks(const int* __restrict__ in, int* __restrict__ out, int n,
+	int* __restrict__ block_sums)
+{
+	__shared__ int s[1024];
+	const int i = blockIdx.x * 1024 + threadIdx.x;
+	const int v = (i < n) ? in[i] : 0;
+	s[threadIdx.x] = v;
+	__syncthreads();
+	for (int o = 1; o < 1024; o <<= 1) {
+		const int t = (threadIdx.x >= o) ? s[threadIdx.x - o] : 0;
+		__syncthreads();
+		s[threadIdx.x] += t;
+		__syncthreads();
+	}
+	if (i < n) out[i] = s[threadIdx.x] - v;
+	if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
+}
+__global__ void __launch_bounds__(1024) k_scan_sums(int* __restrict__ sums, int nb)
+{
+	// single block, sequential chunks of 1024
+	__shared__ int s[1024];
+	__shared__ int carry;
+	if (threadIdx.x == 0) carry = 0;
+	__syncthreads();
+	for (int base = 0; base < nb; base += 1024) {
+		const int i = base + threadIdx.x;
+		const int v = (i < nb) ? sums[i] : 0;
+		s[threadIdx.x] = v;
+		__syncthreads();
+		for (int o = 1; o < 1024; o <<= 1) {
+			const int t = (threadIdx.x >= o) ? s[threadIdx.x - o] : 0;
+			__syncthreads();
+			s[threadIdx.x] += t;
+			__syncthreads();
+		}
+		if (i < nb) sums[i] = s[threadIdx.x] - v + carry;
+		__syncthreads();
+		if (threadIdx.x == 0) carry += s[1023];
+		__syncthreads();
+	}
+}
+__global__ void __launch_bounds__(1024) k_scan_add(int* __restrict__ out, int n, const int* __restrict__ sums)
+{
+	const int i = blockIdx.x * 1024 + threadIdx.x;
+	if (i < n) out[i] += sums[blockIdx.x];
+}
+
+// scatter into buckets (unordered within a bucket)
+__global__ void __launch_bounds__(kBlock) k_sc_scatter(int n, const unsigned int* __restrict__ keys,
+	const int* __restrict__ start, int* __restrict__ cursor, int* __restrict__ idx_sorted)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const unsigned int k = keys[i];
+	const int pos = start[k] + atomicAdd(&cursor[k], 1);
+	idx_sorted[pos] = i;
+}
+
+// order each bucket by particle index (makes the sort stable); thread per bucket,
+// insertion sort for short buckets, rank counting for long ones
+__global__ void __launch_bounds__(kBlock) k_sc_order(int buckets, const int* __restrict__ start,
+	int* __restrict__ idx_sorted)
+{
+	const int b = blockIdx.x * blockDim.x + threadIdx.x;
+	if (b >= buckets) return;
+	const int s = start[b], e = start[b + 1];
+	const int len = e - s;
+	if (len <= 1) return;
+	if (len <= 64) {
+		int v[64];
+		for (int t = 0; t < len; ++t) v[t] = idx_sorted[s + t];
+		for (int t = 1; t < len; ++t) {
+			const int x = v[t];
+			int u = t - 1;
+			while (u >= 0 && v[u] > x) { v[u + 1] = v[u]; --u; }
+			v[u + 1] = x;
+		}
+		for (int t = 0; t < len; ++t) idx_sorted[s + t] = v[t];
+		return;
+	}
+	// long bucket: selection by rank into place, done in rounds of the minimum
+	// remaining value (bounded by len iterations, each O(len))
+	int last = -1;
+	for (int t = 0; t < len; ++t) {
+		int best = INT_MAX;
+		for (int u = t; u < len; ++u) {
+			const int x = idx_sorted[s + u];
+			if (x > last && x < best) best = x;
+		}
+		for (int u = t; u < len; ++u)
+			if (idx_sorted[s + u] == best) {
+				const int tmp = idx_sorted[s + t];
+				idx_sorted[s + t] = best;
+				idx_sorted[s + u] = tmp;
+				break;
+			}
+		last = best;
+	}
+}
+
+// per-particle candidate lists (selfColBuildKernel, forward.cu:7079-7180), within-body
+// pairs when enabled, no bounding-box activity filter (it needs object-mode boxes)
+__global__ void __launch_bounds__(kBlock) k_sc_build(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
+	const int* __restrict__ idx_sorted, const int* __restrict__ start, unsigned int mask,
+	const int* __restrict__ obj_id, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
+	int* __restrict__ counts)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 x = X[i], p = Pp[i];
+	int cnt = 0, over = 0;
+	if (isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+		const float inv_cell = ctr->sc_inv_cell;
+		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
+		const float fast_rel = P->sc_fast_rel;
+		const int within = P->sc_within;
+		const float4 q = rest[i];
+		const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
+		const int oi = obj_id[i];
+		const float search2 = search * search;
+		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+		int* out = contacts + (size_t)i * kSelfColMax;
+		unsigned int hs[27];
+		float prio[kSelfColMax];
+		int tier[kSelfColMax];
+		int nh = 0;
+		for (int oz = -1; oz <= 1; ++oz)
+			for (int oy = -1; oy <= 1; ++oy)
+				for (int ox = -1; ox <= 1; ++ox) {
+					const unsigned int h = sc_hash(cx + ox, cy + oy, cz + oz, mask);
+					bool dup = false;
+					for (int m = 0; m < nh; ++m) if (hs[m] == h) { dup = true; break; }
+					if (dup) continue;
+					hs[nh++] = h;
+					const int s = start[h], e = start[h + 1];
+					for (int t = s; t < e; ++t) {
+						const int j = idx_sorted[t];
+						if (j == i) continue;
+						const bool cross = obj_id[j] != oi;
+						if (!cross && !within) continue;
+						const float4 pj = Pp[j], qj = rest[j];
+						const float qx = q.x - qj.x, qy = q.y - qj.y, qz = q.z - qj.z;
+						const float q2 = qx * qx + qy * qy + qz * qz;
+						float pr;
+						int code = j;
+						if (cross) {
+							const float4 xj = X[j];
+							const float ex = x.x - xj.x, ey = x.y - xj.y, ez = x.z - xj.z;
+							const float dist_x = sqrtf(ex * ex + ey * ey + ez * ez);
+							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
+							const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
+							if (!(dist_x < search + rel)) continue;
+							if (!(q2 >= cross_excl2)) continue;
+							pr = dist_x - rel;
+							if (rel > fast_rel) code = -(j + 1);
+						}
+						else {
+							const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+							const float d2 = ex * ex + ey * ey + ez * ez;
+							if (!(d2 < search2)) continue;
+							if (!(q2 >= excl2)) continue;
+							pr = sqrtf(d2);
+						}
+						const int tr = cross ? 0 : 1;
+						if (cnt < kSelfColMax) {
+							out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
+						}
+						else {
+							int worst = 0;
+							for (int m = 1; m < kSelfColMax; ++m)
+								if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
+							if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
+								out[worst] = code; prio[worst] = pr; tier[worst] = tr;
+							}
+							++over;
+						}
+					}
+				}
+	}
+	counts[i] = cnt;
+	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
+	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
+}
+
+__device__ __forceinline__ bool sc_start_normal(float4 xi, float4 xj, float4 qi, float4 qj, float& nx, float& ny,
+	float& nz)
+{
+	nx = xi.x - xj.x; ny = xi.y - xj.y; nz = xi.z - xj.z;
+	float l2 = nx * nx + ny * ny + nz * nz;
+	if (!(l2 > 1e-24f)) {
+		nx = qi.x - qj.x; ny = qi.y - qj.y; nz = qi.z - qj.z;
+		l2 = nx * nx + ny * ny + nz * nz;
+		if (!(l2 > 1e-24f)) return false;
+	}
+	const float inv = 1.0f / sqrtf(l2);
+	nx *= inv; ny *= inv; nz *= inv;
+	return true;
+}
+
+// phase 1 of the per-iteration contact projection (selfColSolveKernel, forward.cu:7205-7308)
+__global__ void __launch_bounds__(kBlock) k_sc_solve(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pos, const float4* __restrict__ pos_start, const float4* __restrict__ rest,
+	const int* __restrict__ contacts, const int* __restrict__ counts, const DevCounters* __restrict__ ctr,
+	float4* __restrict__ dp_out)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (ctr->sc_contacts == 0u) return;
+	const int cnt = counts[i];
+	if (cnt <= 0) return;
+	const float dc = P->sc_dc;
+	const float ims = P->inv_mass_scale;
+	const float4 pi = pos[i];
+	const float wi = pi.w * ims;
+	float ax = 0.0f, ay = 0.0f, az = 0.0f;
+	int act = 0;
+	float cpx = 0.0f, cpy = 0.0f, cpz = 0.0f;
+	float sx = 0.0f, sy = 0.0f, sz = 0.0f, w_fast = 0.0f;
+	int n_fast = 0;
+	const int* list = contacts + (size_t)i * kSelfColMax;
+	const float4 xi = pos_start[i], qi = rest[i];
+	if (wi > 0.0f) {
+		const float dc2 = dc * dc;
+		for (int k = 0; k < cnt; ++k) {
+			const int code = list[k];
+			if (code < 0) {
+				const int j = -code - 1;
+				float nx, ny, nz;
+				if (!sc_start_normal(xi, pos_start[j], qi, rest[j], nx, ny, nz)) continue;
+				const float4 pj = pos[j];
+				const float proj = (pi.x - pj.x) * nx + (pi.y - pj.y) * ny + (pi.z - pj.z) * nz;
+				if (!(proj < dc)) continue;
+				const float pen = dc - proj;
+				sx += nx * pen; sy += ny * pen; sz += nz * pen;
+				const float wj = pj.w * ims;
+				w_fast += wi / (wi + wj);
+				++n_fast;
+				continue;
+			}
+			const int j = code;
+			const float4 pj = pos[j];
+			const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+			const float d2 = dx * dx + dy * dy + dz * dz;
+			if (!(d2 < dc2)) continue;
+			const float wj = pj.w * ims;
+			const float wr = wi / (wi + wj);
+			if (d2 < 1e-24f) {
+				const float4 qj = rest[j];
+				const float rx = qi.x - qj.x, ry = qi.y - qj.y, rz = qi.z - qj.z;
+				const float r2 = rx * rx + ry * ry + rz * rz;
+				if (!(r2 > 1e-24f)) continue;
+				const float s = dc * wr / sqrtf(r2);
+				ax += rx * s; ay += ry * s; az += rz * s;
+				++act;
+				continue;
+			}
+			const float d = sqrtf(d2);
+			const float s = (dc - d) / d * wr;
+			ax += dx * s; ay += dy * s; az += dz * s;
+			++act;
+		}
+	}
+	float3 out = (act > 0) ? make_float3(ax / act, ay / act, az / act) : make_float3(0.0f, 0.0f, 0.0f);
+	if (n_fast > 0) {
+		const float sl = sqrtf(sx * sx + sy * sy + sz * sz);
+		if (sl > 1e-20f) {
+			const float bx = sx / sl, by = sy / sl, bz = sz / sl;
+			float delta = 0.0f;
+			for (int k = 0; k < cnt; ++k) {
+				const int code = list[k];
+				if (code >= 0) continue;
+				const int j = -code - 1;
+				float nx, ny, nz;
+				if (!sc_start_normal(xi, pos_start[j], qi, rest[j], nx, ny, nz)) continue;
+				const float4 pj = pos[j];
+				const float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+				if (!(ddx * nx + ddy * ny + ddz * nz < dc)) continue;
+				const float pen = dc - (ddx * bx + ddy * by + ddz * bz);
+				if (pen > delta) delta = pen;
+			}
+			if (delta > 0.0f) {
+				const float sc = delta * (w_fast / (float)n_fast);
+				cpx = bx * sc; cpy = by * sc; cpz = bz * sc;
+				out = make_float3(out.x + cpx, out.y + cpy, out.z + cpz);
+			}
+		}
+	}
+	dp_out[i] = make_float4(out.x, out.y, out.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// pins (attachApplyKernel, forward.cu:6714-6725): inverse mass 0, position, zero velocity
+// ---------------------------------------------------------------------------
+__global__ void k_attach(int count, const int* __restrict__ idx, const float* __restrict__ pos, int n,
+	float4* __restrict__ pos_curr, float4* __restrict__ vel)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= count) return;
+	const int i = idx[k];
+	if (i < 0 || i >= n) return;
+	pos_curr[i] = make_float4(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2], 0.0f);
+	vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void k_get_w(int n, const float4* __restrict__ pos, float* __restrict__ w)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) w[i] = pos[i].w;
+}
+__global__ void k_set_w(int n, float4* __restrict__ pos, const float* __restrict__ w, float value)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) pos[i].w = w ? w[i] : value;
+}
+
+// addRigidVelocityAllKernel (forward.cu:6701-6712)
+__global__ void k_add_rigid_velocity(int n, const float4* __restrict__ pos, float4* __restrict__ vel, float3 dv,
+	float3 dw, float3 c)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 p = pos[i];
+	if (p.w <= 0.0f) return;
+	const float rx = p.x - c.x, ry = p.y - c.y, rz = p.z - c.z;
+	const float4 v = vel[i];
+	vel[i] = make_float4(v.x + dv.x + (dw.y * rz - dw.z * ry), v.y + dv.y + (dw.z * rx - dw.x * rz),
+		v.z + dv.z + (dw.x * ry - dw.y * rx), 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// volume-weighted J statistics (computeVolumeJKernel forward.cu:9428-9476 + the
+// host reduction forward.cu:12670-12689), reduced on the device in double
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_jstats(int n, const float4* __restrict__ pos, const int* __restrict__ voff,
+	const int* __restrict__ vidx, const float* __restrict__ det_rest, const int* __restrict__ mat_type,
+	const float* __restrict__ v_rest, DevCounters* __restrict__ ctr)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	double a = 0.0, b = 0.0, c2 = 0.0;
+	if (idx < n && mat_type[idx] == 0) {
+		float J = 1.0f;
+		const int off = voff[idx], cnt = voff[idx + 1] - off;
+		float3 c = f3(pos[idx]);
+		int used = 0;
+		for (int k = 0; k < cnt; ++k) {
+			const int j = vidx[off + k];
+			if (j < 0 || j >= n) continue;
+			c = add3(c, f3(pos[j]));
+			++used;
+		}
+		if (used >= 3) {
+			const float inv_n = 1.0f / (float)(used + 1);
+			c = mul3(c, inv_n);
+			M3 S;
+			m3_zero(S);
+			{
+				const float3 d = sub3(f3(pos[idx]), c);
+				m3_add_outer(S, d, d);
+			}
+			for (int k = 0; k < cnt; ++k) {
+				const int j = vidx[off + k];
+				if (j < 0 || j >= n) continue;
+				const float3 d = sub3(f3(pos[j]), c);
+				m3_add_outer(S, d, d);
+			}
+			for (int cc = 0; cc < 3; ++cc)
+				for (int r = 0; r < 3; ++r) S.m[cc][r] *= inv_n;
+			float s_cur, det_hat;
+			if (sigma_scale_det(S, s_cur, det_hat)) {
+				const float det_cur = s_cur * s_cur * s_cur * det_hat;
+				const float dr = det_rest[idx];
+				if (!(dr < 1e-30f)) {
+					const float Jc = sqrtf(det_cur / dr);
+					if (isfinite(Jc) && Jc > 0.0f) J = Jc;
+				}
+			}
+		}
+		const double v = (double)v_rest[idx];
+		if (v > 0.0 && isfinite(v)) { a = v; b = v * J; c2 = v * (double)J * J; }
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		a += __shfl_xor_sync(0xffffffffu, a, o);
+		b += __shfl_xor_sync(0xffffffffu, b, o);
+		c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+	}
+	if ((threadIdx.x & 31) == 0 && (a != 0.0 || b != 0.0)) {
+		atomicAdd(&ctr->jstats[0], a);
+		atomicAdd(&ctr->jstats[1], b);
+		atomicAdd(&ctr->jstats[2], c2);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// deformed Gaussian shapes (deformedShapeKernel, forward.cu:13063-13225; robust
+// F estimate forward.cu:450) with the FP64 Jacobi of symEig3Double (13022-13060)
+// ---------------------------------------------------------------------------
+__device__ __noinline__ void sym_eig3_double(double a[3][3], double ev[3], double V[3][3])
+{
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
+	for (int sweep = 0; sweep < 32; ++sweep) {
+		const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+		const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
+		if (off <= 1e-15 * diag + 1e-300) break;
+#pragma unroll
+		for (int k = 0; k < 3; ++k) {
+			const int p = (k == 2) ? 1 : 0, q = (k == 0) ? 1 : 2;
+			const double apq = a[p][q];
+			if (fabs(apq) <= 1e-300) continue;
+			const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+			const double t = ((theta >= 0.0) ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+			const double c = 1.0 / sqrt(t * t + 1.0);
+			const double s = t * c;
+#pragma unroll
+			for (int m = 0; m < 3; ++m) {
+				const double amp = a[m][p], amq = a[m][q];
+				a[m][p] = c * amp - s * amq;
+				a[m][q] = s * amp + c * amq;
+			}
+#pragma unroll
+			for (int m = 0; m < 3; ++m) {
+				const double apm = a[p][m], aqm = a[q][m];
+				a[p][m] = c * apm - s * aqm;
+				a[q][m] = s * apm + c * aqm;
+			}
+#pragma unroll
+			for (int m = 0; m < 3; ++m) {
+				const double vmp = V[m][p], vmq = V[m][q];
+				V[m][p] = c * vmp - s * vmq;
+				V[m][q] = s * vmp + c * vmq;
+			}
+		}
+	}
+	ev[0] = a[0][0]; ev[1] = a[1][1]; ev[2] = a[2][2];
+}
+
+__global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4* __restrict__ rest,
+	const float4* __restrict__ cur, const int* __restrict__ off, const int* __restrict__ nbr,
+	const float* __restrict__ scales, const float* __restrict__ rots, float deform_eps, float* __restrict__ out_scale,
+	float* __restrict__ out_quat, DevCounters* __restrict__ ctr)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float3 s0 = make_float3(scales[3 * i], scales[3 * i + 1], scales[3 * i + 2]);
+	const float4 q0 = make_float4(rots[4 * i], rots[4 * i + 1], rots[4 * i + 2], rots[4 * i + 3]);
+	const float3 x = f3(cur[i]), x0 = f3(rest[i]);
+	const float dxv = x.x - x0.x, dyv = x.y - x0.y, dzv = x.z - x0.z;
+	const float diff = sqrtf(dxv * dxv + dyv * dyv + dzv * dzv);
+	const int e0 = off[i], kn = off[i + 1] - e0;
+	bool deformed = false;
+	M3 Sigma;
+	m3_zero(Sigma);
+	if (diff > deform_eps && kn >= 3) {
+		M3 PPt, QPt;
+		m3_zero(PPt);
+		m3_zero(QPt);
+		for (int k = 0; k < kn; ++k) {
+			const int j = nbr[e0 + k];
+			if (j < 0 || j >= n) continue;
+			const float4 rj = rest[j], cj = cur[j];
+			const float3 p = make_float3(rj.x - x0.x, rj.y - x0.y, rj.z - x0.z);
+			const float3 q = make_float3(cj.x - x.x, cj.y - x.y, cj.z - x.z);
+			m3_add_outer(PPt, p, p);
+			m3_add_outer(QPt, q, p);
+		}
+		const float tr_p = PPt.m[0][0] + PPt.m[1][1] + PPt.m[2][2];
+		const float alpha = (tr_p > 0.0f) ? (tr_p * 1e-4f) : 1e-6f;
+#pragma unroll
+		for (int d = 0; d < 3; ++d) { PPt.m[d][d] = PPt.m[d][d] + alpha; QPt.m[d][d] = QPt.m[d][d] + alpha; }
+		const float sp = fmaxf((PPt.m[0][0] + PPt.m[1][1] + PPt.m[2][2]) * (1.0f / 3.0f), 1e-30f);
+		const float inv_sp = 1.0f / sp;
+		M3 Ph, inv_hat;
+#pragma unroll
+		for (int c = 0; c < 3; ++c)
+#pragma unroll
+			for (int r = 0; r < 3; ++r) Ph.m[c][r] = PPt.m[c][r] * inv_sp;
+		if (inverse3x3_safe(Ph, inv_hat, 1e-9f)) {
+			M3 inv_p;
+#pragma unroll
+			for (int c = 0; c < 3; ++c)
+#pragma unroll
+				for (int r = 0; r < 3; ++r) inv_p.m[c][r] = inv_hat.m[c][r] * inv_sp;
+			const M3 A = m3_mul(QPt, inv_p);
+			const M3 AtA = m3_mul(m3_t(A), A);
+			M3 V;
+			float3 S2;
+			eig_sym3f(AtA, S2, V);
+			float3 Sv = make_float3(sqrtf(fmaxf(0.0f, S2.x)), sqrtf(fmaxf(0.0f, S2.y)), sqrtf(fmaxf(0.0f, S2.z)));
+			Sv = make_float3(fminf(fmaxf(Sv.x, 1e-3f), 1.5f), fminf(fmaxf(Sv.y, 1e-3f), 1.5f), fminf(fmaxf(Sv.z, 1e-3f), 1.5f));
+			M3 Si;
+			m3_zero(Si);
+			Si.m[0][0] = (Sv.x > 1.0e-7f) ? 1.0f / Sv.x : 0.0f;
+			Si.m[1][1] = (Sv.y > 1.0e-7f) ? 1.0f / Sv.y : 0.0f;
+			Si.m[2][2] = (Sv.z > 1.0e-7f) ? 1.0f / Sv.z : 0.0f;
+			M3 U = m3_mul(m3_mul(A, V), Si);
+			const M3 Vt = m3_t(V);
+			M3 R = m3_mul(U, Vt);
+			if (m3_det(R) < 0.0f) {
+				U.m[0][0] *= -1.0f; U.m[0][1] *= -1.0f; U.m[0][2] *= -1.0f;
+				R = m3_mul(U, Vt);
+			}
+			M3 Sd;
+			m3_zero(Sd);
+			Sd.m[0][0] = Sv.x; Sd.m[1][1] = Sv.y; Sd.m[2][2] = Sv.z;
+			const M3 S_final = m3_mul(m3_mul(V, Sd), Vt);
+			M3 Sm;
+			m3_zero(Sm);
+			Sm.m[0][0] = s0.x; Sm.m[1][1] = s0.y; Sm.m[2][2] = s0.z;
+			const float r = q0.x, qx = q0.y, qy = q0.z, qz = q0.w;
+			M3 R0;
+			R0.m[0][0] = 1.f - 2.f * (qy * qy + qz * qz); R0.m[0][1] = 2.f * (qx * qy - r * qz);
+			R0.m[0][2] = 2.f * (qx * qz + r * qy);
+			R0.m[1][0] = 2.f * (qx * qy + r * qz); R0.m[1][1] = 1.f - 2.f * (qx * qx + qz * qz);
+			R0.m[1][2] = 2.f * (qy * qz - r * qx);
+			R0.m[2][0] = 2.f * (qx * qz - r * qy); R0.m[2][1] = 2.f * (qy * qz + r * qx);
+			R0.m[2][2] = 1.f - 2.f * (qx * qx + qy * qy);
+			const M3 M = m3_mul(m3_mul(m3_mul(Sm, R0), S_final), m3_t(R));
+			Sigma = m3_mul(m3_t(M), M);
+			deformed = m3_finite(Sigma);
+		}
+	}
+	const double tr = deformed ? ((double)Sigma.m[0][0] + Sigma.m[1][1] + Sigma.m[2][2]) : 0.0;
+	if (!deformed || !(tr > 0.0)) {
+		out_scale[3 * i + 0] = s0.x; out_scale[3 * i + 1] = s0.y; out_scale[3 * i + 2] = s0.z;
+		out_quat[4 * i + 0] = q0.x; out_quat[4 * i + 1] = q0.y; out_quat[4 * i + 2] = q0.z; out_quat[4 * i + 3] = q0.w;
+		atomicAdd(&ctr->shapes_kept, 1u);
+		return;
+	}
+	const double inv = 3.0 / tr;
+	double a[3][3];
+#pragma unroll
+	for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) a[rr][c] = 0.5 * ((double)Sigma.m[c][rr] + (double)Sigma.m[rr][c]) * inv;
+	double ev[3], E[3][3];
+	sym_eig3_double(a, ev, E);
+	const double det = E[0][0] * (E[1][1] * E[2][2] - E[1][2] * E[2][1])
+		- E[0][1] * (E[1][0] * E[2][2] - E[1][2] * E[2][0])
+		+ E[0][2] * (E[1][0] * E[2][1] - E[1][1] * E[2][0]);
+	if (det < 0.0) {
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) E[rr][2] = -E[rr][2];
+	}
+	const double s_floor = 1e-3 * (double)fmaxf(s0.x, fmaxf(s0.y, s0.z));
+#pragma unroll
+	for (int k = 0; k < 3; ++k) out_scale[3 * i + k] = (float)fmax(sqrt(fmax(ev[k], 0.0) / inv), s_floor);
+	double w, qxv, qyv, qzv;
+	const double t = E[0][0] + E[1][1] + E[2][2];
+	if (t > 0.0) {
+		const double s = 2.0 * sqrt(t + 1.0);
+		w = 0.25 * s; qxv = (E[2][1] - E[1][2]) / s; qyv = (E[0][2] - E[2][0]) / s; qzv = (E[1][0] - E[0][1]) / s;
+	}
+	else if (E[0][0] > E[1][1] && E[0][0] > E[2][2]) {
+		const double s = 2.0 * sqrt(1.0 + E[0][0] - E[1][1] - E[2][2]);
+		w = (E[2][1] - E[1][2]) / s; qxv = 0.25 * s; qyv = (E[0][1] + E[1][0]) / s; qzv = (E[0][2] + E[2][0]) / s;
+	}
+	else if (E[1][1] > E[2][2]) {
+		const double s = 2.0 * sqrt(1.0 + E[1][1] - E[0][0] - E[2][2]);
+		w = (E[0][2] - E[2][0]) / s; qxv = (E[0][1] + E[1][0]) / s; qyv = 0.25 * s; qzv = (E[1][2] + E[2][1]) / s;
+	}
+	else {
+		const double s = 2.0 * sqrt(1.0 + E[2][2] - E[0][0] - E[1][1]);
+		w = (E[1][0] - E[0][1]) / s; qxv = (E[0][2] + E[2][0]) / s; qyv = (E[1][2] + E[2][1]) / s; qzv = 0.25 * s;
+	}
+	const double qn = sqrt(w * w + qxv * qxv + qyv * qyv + qzv * qzv);
+	out_quat[4 * i + 0] = (float)(w / qn);
+	out_quat[4 * i + 1] = (float)(qxv / qn);
+	out_quat[4 * i + 2] = (float)(qyv / qn);
+	out_quat[4 * i + 3] = (float)(qzv / qn);
+	atomicAdd(&ctr->shapes_deformed, 1u);
+}
+
+}  // namespace dev
+}  // namespace xpbd

@@ -1,0 +1,208 @@
+"""Seeded synthetic Gaussian scenes and gripper scenarios.
+
+The reference ships no asset (its Wolf bundle is absent, docs/data.md:3) and no
+benchmark harness, so every workload here is generated: Gaussian centres uniform in
+an ellipsoid, random unit quaternions (w, x, y, z), log-normal scales, a symmetric
+k-NN distance graph with rest lengths taken from the initial pose, and one or two
+capsule grippers that pin their nearest Gaussians and move them per substep.
+
+The arrays match the inputs of ``xpbd_create`` (xpbd_capi.cu:71-102): ``pos[n,3]``,
+``scales[n,3]`` (activated), ``rots[n,4]`` (normalised, w,x,y,z), ``opacity[n]``
+(activated), undirected edges ``[e,2]`` with i<j, ``rest[e]``, ``stiff[e]``.
+"""
+import math
+
+import numpy as np
+
+DEFAULT_RADII = (1.0, 0.6, 0.4)
+
+
+def make_scene(n, seed=0, radii=DEFAULT_RADII, knn=8, centre=(0.0, 0.0, 0.0), opacity=0.9):
+    """One object: ``n`` Gaussians uniform in an ellipsoid with ``radii``.
+
+    Edges are the symmetric union of each centre's ``knn`` nearest neighbours,
+    deduplicated to i<j and sorted; rest = float32 |x_i - x_j|; stiffness 1.
+    """
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    u = rng.random(n) ** (1.0 / 3.0)
+    pos = (d * u[:, None] * np.asarray(radii, dtype=np.float64) + np.asarray(centre)).astype(np.float32)
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    scales = np.exp(rng.normal(-4.0, 0.3, (n, 3))).astype(np.float32)
+    k = min(knn + 1, n)
+    _, nn = cKDTree(pos.astype(np.float64)).query(pos.astype(np.float64), k=k)
+    nn = nn.reshape(n, k)
+    i = np.repeat(np.arange(n, dtype=np.int64), k - 1)
+    j = nn[:, 1:].reshape(-1).astype(np.int64)
+    a, b = np.minimum(i, j), np.maximum(i, j)
+    keep = a != b
+    key = np.unique(a[keep] * n + b[keep])
+    edges = np.stack([key // n, key % n], axis=1).astype(np.int32)
+    diff = pos[edges[:, 0]].astype(np.float64) - pos[edges[:, 1]].astype(np.float64)
+    rest = np.sqrt((diff * diff).sum(1)).astype(np.float32)
+    return {
+        "pos": np.ascontiguousarray(pos),
+        "scales": np.ascontiguousarray(scales),
+        "rots": np.ascontiguousarray(q.astype(np.float32)),
+        "opacity": np.full(n, opacity, dtype=np.float32),
+        "edges": np.ascontiguousarray(edges),
+        "rest": np.ascontiguousarray(rest),
+        "stiff": np.ones(len(edges), dtype=np.float32),
+    }
+
+
+def merge_scenes(parts):
+    """Concatenate independent objects into one scene (edges re-indexed)."""
+    out = {k: [] for k in ("pos", "scales", "rots", "opacity", "edges", "rest", "stiff")}
+    base = 0
+    for p in parts:
+        for k in ("pos", "scales", "rots", "opacity", "rest", "stiff"):
+            out[k].append(p[k])
+        out["edges"].append(p["edges"] + base)
+        base += p["pos"].shape[0]
+    return {k: np.ascontiguousarray(np.concatenate(v, axis=0)) for k, v in out.items()}
+
+
+def _rot_x(angle):
+    c, s = math.cos(angle), math.sin(angle)
+    return np.array([[1.0, 0.0, 0.0], [0.0, c, -s], [0.0, s, c]], dtype=np.float64)
+
+
+class Gripper:
+    """A capsule (radius, half-length along local z) that pins the ``count`` Gaussians
+    nearest to ``centre`` and moves them rigidly: translation ``velocity`` per frame,
+    rotation ``twist`` radians per frame about the world x axis through its centre."""
+
+    def __init__(self, pos, centre, count=200, velocity=(0.01, 0.0, 0.0), twist=0.0,
+                 radius=0.05, half_length=0.05):
+        self.centre = np.asarray(centre, dtype=np.float64)
+        d2 = ((pos.astype(np.float64) - self.centre) ** 2).sum(1)
+        count = min(count, len(pos))
+        self.idx = np.sort(np.argsort(d2, kind="stable")[:count]).astype(np.int32)
+        self.rel = pos[self.idx].astype(np.float64) - self.centre
+        self.velocity = np.asarray(velocity, dtype=np.float64)
+        self.twist = float(twist)
+        self.radius = radius
+        self.half_length = half_length
+
+    def pose(self, t):
+        """(R 3x3, centre 3) after ``t`` frames."""
+        return _rot_x(self.twist * t), self.centre + self.velocity * t
+
+    def targets(self, t):
+        R, c = self.pose(t)
+        return (c + self.rel @ R.T).astype(np.float32)
+
+    def collider(self, t):
+        R, c = self.pose(t)
+        return 2, np.concatenate([R.reshape(-1), c]).astype(np.float32), \
+            np.array([self.radius, self.half_length, 0.0], np.float32)
+
+
+class Scenario:
+    """Drives any object with the ``XPBD`` method set through ``frames`` 60 Hz frames of
+    ``substeps`` solver steps each (one ``xpbd_step`` per substep, dt = 1/(60*substeps)).
+
+    Before every substep the grippers' capsules are re-posed and their pinned Gaussians
+    re-targeted by linear interpolation of the per-frame motion.  The reference rejects
+    ``xpbd_set_attached`` before the first step (xpbd_capi.cu:169), so pins start with the
+    second substep on every backend alike.
+    """
+
+    def __init__(self, scene, grippers, substeps=10, iters=4, shape=True, volume=True, self_collision=False,
+                 within_body=True, ring_k=3, max_members=64, leader_min_hop=1, dist_compliance=1e-6,
+                 vol_compliance=1e-5, shape_compliance=1e-5, under_relax=0.6, vel_damping=0.01,
+                 shape_robust=True, frame_dt=1.0 / 60.0):
+        self.scene = scene
+        self.grippers = list(grippers)
+        self.substeps = substeps
+        self.iters = iters
+        self.shape = shape
+        self.volume = volume
+        self.self_collision = self_collision
+        self.within_body = within_body
+        self.ring_k = ring_k
+        self.max_members = max_members
+        self.leader_min_hop = leader_min_hop
+        self.dist_compliance = dist_compliance
+        self.vol_compliance = vol_compliance
+        self.shape_compliance = shape_compliance
+        self.under_relax = under_relax
+        self.vel_damping = vel_damping
+        self.shape_robust = shape_robust
+        self.dt = frame_dt / substeps
+        self.k = 0
+
+    @property
+    def n(self):
+        return self.scene["pos"].shape[0]
+
+    def setup(self, solver):
+        solver.create(self.scene)
+        solver.set_solver(iters=self.iters, dt=self.dt, under_relax=self.under_relax,
+                          vel_damping=self.vel_damping, dist_compliance=self.dist_compliance,
+                          shape_compliance=self.shape_compliance)
+        solver.set_constraints(distance=True, shape=self.shape, angle=False, volume=self.volume)
+        solver.set_volume(self.vol_compliance, self.ring_k, self.max_members, self.leader_min_hop)
+        solver.set_shape_robust(self.shape_robust)
+        solver.set_self_collision(self.self_collision, 1.5, 2.0, self.within_body)
+        solver.volume_stats(False)
+        self.k = 0
+
+    def pins(self, t):
+        if not self.grippers:
+            return None, None
+        idx = np.concatenate([g.idx for g in self.grippers])
+        pos = np.concatenate([g.targets(t) for g in self.grippers], axis=0)
+        return idx, pos
+
+    def colliders(self, t):
+        cols = [g.collider(t) for g in self.grippers]
+        if not cols:
+            return [], np.zeros((0, 12), np.float32), np.zeros((0, 3), np.float32)
+        return [c[0] for c in cols], np.stack([c[1] for c in cols]), np.stack([c[2] for c in cols])
+
+    def advance(self, solver, count):
+        """Run ``count`` substeps."""
+        for _ in range(count):
+            t = (self.k + 1) / self.substeps
+            if self.grippers:
+                types, poses, dims = self.colliders(t)
+                solver.set_colliders(types, poses, dims, 0.0, 0.0)
+                if self.k > 0:
+                    idx, pos = self.pins(t)
+                    solver.set_attached(idx, pos, 1.0)
+            solver.step()
+            self.k += 1
+
+
+def plain_scene_scenario(n=20000, seed=0, **kw):
+    """The plain small-scene workload: one object, two capsule grippers at the x extremes
+    (+-0.9, 0, 0), each pinning its 200 nearest Gaussians; both translate +0.01 x per frame."""
+    scene = make_scene(n, seed)
+    pins = kw.pop("pins", 200)
+    grippers = [Gripper(scene["pos"], (-0.9, 0.0, 0.0), pins, (0.01, 0.0, 0.0)),
+                Gripper(scene["pos"], (0.9, 0.0, 0.0), pins, (0.01, 0.0, 0.0))]
+    return Scenario(scene, grippers, **kw)
+
+
+def large_scene_scenario(n=1_000_000, seed=0, **kw):
+    """The large single-scene workload: grippers pull apart (+-0.01 x per frame) while each
+    twists 1 degree per frame about x; self-collision on (within-body pairs)."""
+    scene = kw.pop("scene", None) or make_scene(n, seed)
+    pins = kw.pop("pins", 200)
+    deg = math.radians(1.0)
+    grippers = [Gripper(scene["pos"], (-0.9, 0.0, 0.0), pins, (-0.01, 0.0, 0.0), -deg),
+                Gripper(scene["pos"], (0.9, 0.0, 0.0), pins, (0.01, 0.0, 0.0), deg)]
+    kw.setdefault("self_collision", True)
+    kw.setdefault("within_body", True)
+    return Scenario(scene, grippers, **kw)
+
+
+def bbox_diagonal(pos):
+    p = np.asarray(pos, dtype=np.float64)
+    return float(np.linalg.norm(p.max(0) - p.min(0)))

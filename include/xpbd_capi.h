@@ -1,0 +1,144 @@
+/*
+ * C ABI of the B200 XPBD Gaussian-graph solver (libxpbd_b200.so).
+ *
+ * The first group is a drop-in for the reference's singleton C ABI: the same 29
+ * symbols, argument meanings, clamping and error behaviour as native/xpbd_capi.cu of
+ * minn-k/3dgs-isaac-sim-xpbd, so that its src/xpbd_bridge.py loads this library through
+ * XPBD_DLL unchanged.  Each declaration names the reference entry point it replaces
+ * (file:line in that project).  Conventions, as in the reference:
+ *   - all pointers are caller-owned host memory, copied during the call;
+ *   - int functions return 0 (or a count) on success and -1 on failure, with the
+ *     message in xpbd_last_error() (xpbd_capi.cu:31-43);
+ *   - void setters cannot fail and clamp their inputs;
+ *   - xpbd_set_attached / positions / shapes / reset / launch / add_rigid_velocity need
+ *     one xpbd_step first (the graph is uploaded by the first step, xpbd_capi.cu:169);
+ *   - xpbd_step blocks until the GPU has finished the step (xpbd_capi.cu:223).
+ *   - Gaussian order is the caller's (PLY/USD) order; positions are float3[n],
+ *     quaternions (w, x, y, z).
+ *
+ * The second group (xpbd_b200_*) has no counterpart in the reference ABI.
+ */
+#ifndef XPBD_B200_CAPI_H
+#define XPBD_B200_CAPI_H
+
+#ifdef __cplusplus
+#define XPBD_API extern "C" __attribute__((visibility("default")))
+#else
+#define XPBD_API __attribute__((visibility("default")))
+#endif
+
+/* ---- reference entry points (native/xpbd_capi.cu) ---------------------- */
+
+/* xpbd_capi.cu:66 — message of the last failed call */
+XPBD_API const char* xpbd_last_error(void);
+/* xpbd_capi.cu:71-102 — n Gaussians (pos[3n], activated scales[3n], normalised
+ * rots[4n] w,x,y,z, activated opacity[n]) and e undirected edges (edges[2e], rest[e],
+ * stiff[e]).  Frees any previous scene. */
+XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const float* rots, const float* opacity,
+	int e, const int* edges, const float* rest, const float* stiff);
+/* xpbd_capi.cu:104-109 — frees the scene and clears colliders and pins */
+XPBD_API void xpbd_destroy(void);
+/* xpbd_capi.cu:111 */
+XPBD_API int xpbd_count(void);
+/* xpbd_capi.cu:113-119 — iterations per step, dt, Jacobi under-relaxation, velocity
+ * damping, stiffness / inverse-mass scales, distance / shape compliance, shape blend,
+ * angle compliance / blend (angle constraint: accepted, not solved — as in the runtime) */
+XPBD_API void xpbd_set_solver(int iters, float dt, float underRelax, float velDamping, float stiffnessScale,
+	float invMassScale, float distCompliance, float shapeCompliance, float shapeBlend, float angleCompliance,
+	float angleBlend);
+/* xpbd_capi.cu:121-127 */
+XPBD_API void xpbd_set_constraints(int distance, int shape, int angle, int volume);
+/* xpbd_capi.cu:130-137 — volume compliance, cluster ring k, member cap, leader spacing;
+ * clusters are rebuilt at the next step */
+XPBD_API void xpbd_set_volume(float compliance, int ringK, int maxMembers, int leaderMinHop);
+/* xpbd_capi.cu:140-145 — ground plane (point contact) and gravity along -up */
+XPBD_API void xpbd_set_ground(int enabled, float ux, float uy, float uz, float height, float friction,
+	float restitution, float contactRadius, float contactSlop, float gravity);
+/* xpbd_capi.cu:148 — object-level shape keeping: accepted, not implemented (a warning
+ * is printed when a positive stiffness is set) */
+XPBD_API void xpbd_set_object_shape(float stiffness);
+/* xpbd_capi.cu:151 — accepted, no effect */
+XPBD_API void xpbd_set_object_shape_gpu(int enabled);
+/* xpbd_capi.cu:154-158 — up to 32 kinematic colliders: types (0 sphere, 1 box,
+ * 2 capsule), poses[12 count] (row-major local->world R, centre), dims[3 count] */
+XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses, const float* dims, float margin,
+	float friction);
+/* xpbd_capi.cu:161-164 — per collider of the last step: hits, pushed displacement sum,
+ * contact centroid; returns the number filled */
+XPBD_API int xpbd_collider_stats(int* hits, float* push, float* centroid, int maxCount);
+/* xpbd_capi.cu:167-172 — adds dv + dw x (x - center) to every free Gaussian's velocity */
+XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const float* center);
+/* xpbd_capi.cu:179-191 — ellipsoid contact shapes: 0 accepted; enabling returns -1
+ * (not implemented) */
+XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap);
+/* xpbd_capi.cu:195-200 — pins idx[count] at pos[3 count] (inverse mass 0, velocity 0);
+ * count 0 releases; the previous pins' inverse masses are restored first */
+XPBD_API int xpbd_set_attached(int count, const int* idx, const float* pos, float weight);
+/* xpbd_capi.cu:203-206 — spatial-hash self-collision */
+XPBD_API void xpbd_set_self_collision(int enabled, float radiusScale, float excludeScale, int withinBody);
+/* xpbd_capi.cu:209-212 — out[0] candidates, out[1] active particles, out[2] over-cap
+ * replacements, of the last step */
+XPBD_API void xpbd_self_collision_stats(int* out);
+/* xpbd_capi.cu:215 — shape-matching rotation: 1 FP64 polar (default), 0 FP32 path */
+XPBD_API void xpbd_set_shape_robust(int enabled);
+/* xpbd_capi.cu:218-225 — one solver step; blocks until done */
+XPBD_API int xpbd_step(void);
+/* xpbd_capi.cu:228-232 — device pointer to the committed positions, float3[n], valid
+ * until the next create/destroy; 0 before the first step */
+XPBD_API unsigned long long xpbd_positions_device(void);
+/* xpbd_capi.cu:235-243 */
+XPBD_API int xpbd_positions_host(float* out, int n);
+/* xpbd_capi.cu:248-260 — deformed Gaussian scales[3n] / quats[4n] (either may be NULL);
+ * returns the number of Gaussians whose shape changed, or -1 */
+XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* hostQuats, int n);
+/* xpbd_capi.cu:263-269 — back to rest, zero velocity, pins released */
+XPBD_API int xpbd_reset(void);
+/* xpbd_capi.cu:272-276 — rest pose rotated by tilt (axis * angle) about the centre of
+ * mass, velocity lin + ang x (x - com) */
+XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt);
+/* xpbd_capi.cu:281-288 — press harness: not implemented, returns -1 */
+XPBD_API int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo);
+/* xpbd_capi.cu:291 */
+XPBD_API void xpbd_press_autolog(int enabled);
+/* xpbd_capi.cu:294 */
+XPBD_API void xpbd_press_stop(void);
+/* xpbd_capi.cu:297-303 — returns 0 (no press active) */
+XPBD_API int xpbd_press_state(float* lo, float* hi, float* curDisp, float* maxDisp);
+/* xpbd_capi.cu:306-310 — enables per-step volume-weighted J statistics and returns
+ * the last ones computed (mean, std) */
+XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd);
+
+/* ---- extensions (no counterpart in the reference ABI) ------------------- */
+
+/* Run the engine on a caller-owned cudaStream_t (NULL: the library's own stream). */
+XPBD_API int xpbd_b200_set_stream(void* stream);
+/* Enqueue `substeps` steps without waiting for them. */
+XPBD_API int xpbd_b200_step_async(int substeps);
+/* Wait for the engine's stream. */
+XPBD_API int xpbd_b200_sync(void);
+/* Gauss-Seidel colour sweeps for the distance / volume constraints instead of the
+ * Jacobi default (the reference's forward.cu:3780-3812 toggles). */
+XPBD_API void xpbd_b200_set_gs(int distance, int volume);
+/* Volume kernel shape: 0 auto (warp per cluster when mean members >= 40), 1 thread, 2 warp. */
+XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
+/* 1 (default): replay each step from a captured CUDA graph; 0: launch kernel by kernel. */
+XPBD_API void xpbd_b200_set_graph(int enabled);
+/* Per-kernel CUDA-event timing of subsequent steps (launches then go kernel by kernel). */
+XPBD_API int xpbd_b200_set_profiling(int enabled);
+/* Accumulated per-stage milliseconds and launch counts; returns the number of stages. */
+XPBD_API int xpbd_b200_stage_times(double* ms, long long* counts, int max_stages);
+XPBD_API void xpbd_b200_reset_stage_times(void);
+XPBD_API const char* xpbd_b200_stage_name(int stage);
+/* Kernels launched by the engine since load (graph replays count every kernel node). */
+XPBD_API long long xpbd_b200_launch_count(void);
+/* Topology sizes after the first step: N, edges, cluster members, reverse entries, GS
+ * edges, GS edge colours, GS clusters, GS cluster colours, hash table, candidates. */
+XPBD_API int xpbd_b200_sizes(long long* out);
+/* Stage buffers by name, for parity checks (count only when out is NULL). */
+XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap);
+XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap);
+/* The once-per-step self-collision build on given start / predicted positions
+ * (x[3n], p[3n]); returns the candidate total.  Solver state is left unchanged. */
+XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p);
+
+#endif

@@ -1,0 +1,169 @@
+"""Shared test utilities: library paths, stage accessors, comparison metrics."""
+import ctypes
+import importlib
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+pkg = importlib.import_module("3dgs-isaac-sim-xpbd_b200")
+scenes = pkg.scenes
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libxpbd_ref.so")
+B200_SO = pkg.library_path()
+
+# tolerances (fraction of the scene's bounding-box diagonal)
+TOL_1STEP = 1e-5
+TOL_100STEP = 1e-4
+
+
+def ensure_oracle():
+    if not os.path.isfile(ORACLE_SO):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    return ORACLE_SO
+
+
+def cuda_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+class Staged(pkg.bridge.XPBD):
+    """XPBD bridge plus the stage accessors of the oracle (oracle_*), the product
+    library (xpbd_b200_debug_*) or the reference shim (refshim_*)."""
+
+    def __init__(self, path, prefix):
+        super().__init__(path)
+        L = self.lib
+        self.prefix = prefix
+        names = {"oracle": ("oracle_int", "oracle_float", "oracle_selfcol_build"),
+                 "b200": ("xpbd_b200_debug_int", "xpbd_b200_debug_float", "xpbd_b200_selfcol_build"),
+                 "ref": ("refshim_int", "refshim_float", "refshim_selfcol_build")}[prefix]
+        self._int, self._float, self._scb = (getattr(L, n) for n in names)
+        for f in (self._int, self._float):
+            f.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong]
+            f.restype = ctypes.c_int
+        self._scb.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._scb.restype = ctypes.c_int
+        if prefix == "oracle":
+            L.oracle_set_gs.argtypes = [ctypes.c_int, ctypes.c_int]
+            L.oracle_set_volume_warp_mode.argtypes = [ctypes.c_int]
+            L.oracle_set_threads.argtypes = [ctypes.c_int]
+        elif prefix == "b200":
+            L.xpbd_b200_set_gs.argtypes = [ctypes.c_int, ctypes.c_int]
+            L.xpbd_b200_set_volume_warp_mode.argtypes = [ctypes.c_int]
+            L.xpbd_b200_set_graph.argtypes = [ctypes.c_int]
+        else:
+            L.refshim_set_gs.argtypes = [ctypes.c_int, ctypes.c_int]
+
+    def ints(self, name):
+        n = self._int(name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(max(n, 1), np.int32)
+        assert self._int(name.encode(), out.ctypes.data, out.size) == n
+        return out[:n].copy()
+
+    def floats(self, name):
+        n = self._float(name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(max(n, 1), np.float32)
+        assert self._float(name.encode(), out.ctypes.data, out.size) == n
+        return out[:n].copy()
+
+    def selfcol_build(self, x, p):
+        x = np.ascontiguousarray(x, np.float32)
+        p = np.ascontiguousarray(p, np.float32)
+        return self._scb(x.ctypes.data, p.ctypes.data)
+
+    def set_gs(self, dist, vol):
+        fn = {"oracle": "oracle_set_gs", "b200": "xpbd_b200_set_gs", "ref": "refshim_set_gs"}[self.prefix]
+        getattr(self.lib, fn)(int(dist), int(vol))
+
+
+def oracle():
+    return Staged(ensure_oracle(), "oracle")
+
+
+def b200():
+    return Staged(B200_SO, "b200")
+
+
+def load_golden(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def golden_scene(g):
+    return {k[3:]: g[k] for k in g.files if k.startswith("in_")}
+
+
+def scenario_for(case):
+    """The scenario each golden case was generated with (tests/golden/make_golden.py)."""
+    if case.startswith("plain_n4000"):
+        kw = {}
+        if case.endswith("_k1"):
+            kw["ring_k"] = 1
+        if case.endswith("_fpolar"):
+            kw["shape_robust"] = False
+        return scenes.plain_scene_scenario(4000, 3, pins=40, **kw)
+    if case == "plain_n20000":
+        return scenes.plain_scene_scenario(20000, 0)
+    if case == "selfcol_blobs":
+        return scenes.Scenario(*two_blob_scene(), self_collision=True, within_body=True)
+    raise KeyError(case)
+
+
+def two_blob_scene(n_each=1500):
+    a = scenes.make_scene(n_each, 11, radii=(0.3, 0.3, 0.3), centre=(-0.35, 0.0, 0.0))
+    b = scenes.make_scene(n_each, 12, radii=(0.3, 0.3, 0.3), centre=(0.35, 0.0, 0.0))
+    sc = scenes.merge_scenes([a, b])
+    grippers = [scenes.Gripper(sc["pos"], (-0.55, 0.0, 0.0), 60, (0.03, 0.0, 0.0)),
+                scenes.Gripper(sc["pos"], (0.55, 0.0, 0.0), 60, (-0.03, 0.0, 0.0))]
+    return sc, grippers
+
+
+def max_err_over_diag(a, b, diag):
+    return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max() / diag)
+
+
+def covariances(scales, quats):
+    """Sigma = R diag(s^2) R^T per Gaussian from (w, x, y, z) quaternions; invariant to the
+    eigenvector sign and order choices of the shape writeback."""
+    s = np.asarray(scales, np.float64)
+    w, x, y, z = np.asarray(quats, np.float64).T
+    R = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+                  np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+                  np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+    return np.einsum("nij,nj,nkj->nik", R, s * s, R)
+
+
+def covariance_rel_err(sa, qa, sb, qb):
+    A, B = covariances(sa, qa), covariances(sb, qb)
+    return np.linalg.norm((A - B).reshape(-1, 9), axis=1) / np.linalg.norm(B.reshape(-1, 9), axis=1)
+
+
+def cells_equal(start_a, end_a, start_b, end_b):
+    """Cell ranges compared where a cell is occupied (the reference leaves stale ends in
+    empty cells, forward.cu:11838)."""
+    start_a, start_b = np.asarray(start_a), np.asarray(start_b)
+    if not np.array_equal(start_a, start_b):
+        return False
+    occ = start_a >= 0
+    return bool(np.array_equal(np.asarray(end_a)[occ], np.asarray(end_b)[occ]))
+
+
+def contacts_equal(count_a, list_a, count_b, list_b):
+    ca, cb = np.asarray(count_a), np.asarray(count_b)
+    if not np.array_equal(ca, cb):
+        return False
+    la, lb = np.asarray(list_a).reshape(-1, 32), np.asarray(list_b).reshape(-1, 32)
+    for i in np.nonzero(ca)[0]:
+        if not np.array_equal(la[i, :ca[i]], lb[i, :ca[i]]):
+            return False
+    return True

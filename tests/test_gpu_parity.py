@@ -1,0 +1,195 @@
+"""Parity of the B200 library (CUDA kernels through the C ABI) with the reference.
+
+Same bar as the oracle: integer artefacts bit-exact against the reference's own
+golden vectors, FP32 positions within 1e-5 of the bbox diagonal after 1 step and
+1e-4 after 100, deformed-shape covariances within 1e-3 (p99).  Cross-checks against
+the CPU oracle cover states the golden files do not hold.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+GRAPH_INT = ["nbr_offset", "nbr_count", "nbr_idx", "vol_offset", "vol_count", "vol_idx", "rev_offset", "rev_count",
+             "rev_idx", "mat_type", "gs_edge", "gs_color_offset", "vol_gs_order", "vol_gs_color_offset"]
+GRAPH_FLOAT = ["det_rest", "sigma_rest", "v_rest", "rest_len", "gs_rest", "gs_stiff"]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not H.cuda_available():
+        pytest.fail("a CUDA device is required for the gpu tests")
+    b = H.b200()
+    yield b
+    b.destroy()
+
+
+@pytest.mark.parametrize("case", ["graph_n3000_r1", "graph_n3000_r2", "graph_n3000_k1"])
+def test_cluster_topology_bit_exact(lib, case):
+    g = H.load_golden(case)
+    sc = H.golden_scene(g)
+    s = H.scenes.Scenario(sc, [], ring_k=int(g["ring_k"]), max_members=int(g["cap"]),
+                          leader_min_hop=int(g["leader"]))
+    s.setup(lib)
+    lib.step()
+    for name in GRAPH_INT:
+        np.testing.assert_array_equal(lib.ints(name), g[name], err_msg=name)
+    for name in GRAPH_FLOAT:
+        a, b = lib.floats(name), g[name]
+        assert a.shape == b.shape, name
+        np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-6 * float(np.abs(b).max()), err_msg=name)
+    assert H.max_err_over_diag(lib.positions(), g["pos_step1"], H.scenes.bbox_diagonal(sc["pos"])) < H.TOL_1STEP
+
+
+@pytest.mark.parametrize("case", ["plain_n4000", "plain_n4000_k1", "plain_n4000_fpolar", "plain_n4000_gs"])
+def test_scenario_positions(lib, case):
+    g = H.load_golden(case)
+    s = H.scenario_for(case)
+    s.setup(lib)
+    lib.set_gs(*((1, 1) if case.endswith("_gs") else (0, 0)))
+    lib.volume_stats(True)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    done = 0
+    for c in g["checkpoints"]:
+        s.advance(lib, int(c) - done)
+        done = int(c)
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(lib.positions(), g[f"pos_{c}"], diag) < tol, c
+        np.testing.assert_allclose(lib.volume_stats(True), g[f"jvw_{c}"], rtol=1e-4, atol=1e-6)
+        hits, _, _ = lib.collider_stats(2)
+        np.testing.assert_array_equal(hits, g[f"col_hits_{c}"])
+    sc_, q_, k_ = lib.shapes(float(g["deform_eps"]))
+    assert k_ == int(g["shape_deformed"])
+    rel = H.covariance_rel_err(sc_, q_, g["shape_scales"], g["shape_quats"])
+    assert np.percentile(rel, 99) < 1e-3 and rel.max() < 1e-2
+    lib.set_gs(0, 0)
+
+
+def test_plain_small_scene_100_frames(lib):
+    """The 20,000-Gaussian plain workload end to end: 100 frames x 10 substeps."""
+    g = H.load_golden("plain_n20000")
+    s = H.scenario_for("plain_n20000")
+    s.setup(lib)
+    lib.volume_stats(True)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    done = 0
+    for c in g["checkpoints"]:
+        s.advance(lib, int(c) - done)
+        done = int(c)
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(lib.positions(), g[f"pos_{c}"], diag) < tol, c
+    sc_, q_, k_ = lib.shapes(float(g["deform_eps"]))
+    rel = H.covariance_rel_err(sc_, q_, g["shape_scales"], g["shape_quats"])
+    assert np.percentile(rel, 99) < 1e-3
+
+
+def test_self_collision(lib):
+    g = H.load_golden("selfcol_blobs")
+    s = H.scenario_for("selfcol_blobs")
+    s.setup(lib)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    s.advance(lib, 1)
+    assert H.max_err_over_diag(lib.positions(), g["pos_1"], diag) < H.TOL_1STEP
+    s.advance(lib, 49)
+    assert H.max_err_over_diag(lib.positions(), g["pos_50"], diag) < H.TOL_100STEP
+    assert lib.self_collision_stats()[0] == int(g["sc_stats_50"][0])
+    total = lib.selfcol_build(g["stage_x"], g["stage_p"])
+    assert total == int(g["stage_total"])
+    np.testing.assert_array_equal(lib.floats("self_col"), g["self_col_params"])
+    for name in ["sc_keys", "sc_keys_sorted", "sc_idx_sorted", "sc_count", "obj_id"]:
+        np.testing.assert_array_equal(lib.ints(name), g[name], err_msg=name)
+    assert H.cells_equal(lib.ints("sc_cell_start"), lib.ints("sc_cell_end"), g["sc_cell_start"], g["sc_cell_end"])
+    assert H.contacts_equal(lib.ints("sc_count"), lib.ints("sc_contact"), g["sc_count"], g["sc_contact"])
+
+
+def test_ground_launch_reset(lib):
+    g = H.load_golden("misc_n2000")
+    sc = H.golden_scene(g)
+    s = H.scenes.Scenario(sc, [])
+    lib.set_colliders([], [], [])
+    s.setup(lib)
+    diag = H.scenes.bbox_diagonal(sc["pos"])
+    lib.step()
+    lib.set_ground(True, (0.0, 0.0, 1.0), -0.45, 0.5, 0.3, 0.0, 0.0, 9.8)
+    lib.launch((0.0, 0.0, -1.0), (0.0, 0.0, 2.0), (0.3, 0.0, 0.0))
+    assert H.max_err_over_diag(lib.positions(), g["pos_launch"], diag) < 1e-7
+    k = 0
+    for c in (1, 30, 90):
+        while k < c:
+            lib.step()
+            k += 1
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(lib.positions(), g[f"pos_ground_{c}"], diag) < tol, c
+    lib.reset()
+    np.testing.assert_array_equal(lib.positions(), g["pos_reset"])
+    lib.step()
+    assert H.max_err_over_diag(lib.positions(), g["pos_after_reset_step"], diag) < H.TOL_1STEP
+    lib.set_ground(False, (0.0, 0.0, 1.0), 0.0, 0.5, 0.3, 0.0, 0.0, 0.0)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_volume_kernel_shapes_agree_with_oracle(lib, mode):
+    """Thread- and warp-per-cluster volume kernels against the oracle in the same mode."""
+    orc = H.oracle()
+    out = {}
+    for name, solver in (("b200", lib), ("oracle", orc)):
+        s = H.scenes.plain_scene_scenario(3000, 8, pins=30)
+        s.setup(solver)
+        if name == "b200":
+            solver.lib.xpbd_b200_set_volume_warp_mode(mode)
+        else:
+            solver.lib.oracle_set_volume_warp_mode(mode)
+        s.advance(solver, 20)
+        out[name] = solver.positions()
+    lib.lib.xpbd_b200_set_volume_warp_mode(0)
+    orc.lib.oracle_set_volume_warp_mode(0)
+    orc.destroy()
+    diag = H.scenes.bbox_diagonal(out["oracle"])
+    assert H.max_err_over_diag(out["b200"], out["oracle"], diag) < H.TOL_100STEP
+
+
+def test_graph_replay_matches_eager(lib):
+    out = []
+    for graph in (1, 0):
+        lib.lib.xpbd_b200_set_graph(graph)
+        s = H.scenes.plain_scene_scenario(2000, 4, pins=20)
+        s.setup(lib)
+        s.advance(lib, 15)
+        out.append(lib.positions())
+    lib.lib.xpbd_b200_set_graph(1)
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_positions_device_pointer(lib):
+    """xpbd_positions_device returns float3[n] committed positions (xpbd_capi.cu:228-232)."""
+    cudart = pytest.importorskip("cuda.bindings.runtime")
+    s = H.scenes.plain_scene_scenario(1000, 6, pins=10)
+    s.setup(lib)
+    assert lib.positions_device_ptr() == 0
+    s.advance(lib, 3)
+    ptr = lib.positions_device_ptr()
+    assert ptr != 0
+    host = np.empty((1000, 3), np.float32)
+    err, = cudart.cudaMemcpy(host.ctypes.data, ptr, host.nbytes, cudart.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert int(err) == 0
+    np.testing.assert_array_equal(host, lib.positions())
+
+
+def test_error_behaviour(lib):
+    lib.destroy()
+    assert lib.lib.xpbd_step() == -1
+    assert "create" in lib.last_error()
+    sc = H.scenes.make_scene(300, 2)
+    lib.create(sc)
+    with pytest.raises(RuntimeError, match="no step yet"):
+        lib.positions()
+    with pytest.raises(RuntimeError, match="no step yet"):
+        lib.set_attached([0], [[0.0, 0.0, 0.0]])
+    lib.step()
+    with pytest.raises(RuntimeError, match="size mismatch"):
+        lib._check(lib.lib.xpbd_positions_host(np.zeros(3, np.float32), 1), "xpbd_positions_host")
+    with pytest.raises(RuntimeError, match="not implemented"):
+        lib.set_contact_shape(1)
+    lib.destroy()
