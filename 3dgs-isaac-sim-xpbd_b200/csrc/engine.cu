@@ -92,6 +92,7 @@ struct Settings {
 	int kin_count = 0;
 	float kin_margin = 0.0f, kin_friction = 0.0f;
 	bool use_graph = true;
+	bool reorder = true;             // Morton order inside the engine (results unchanged)
 };
 static Settings S;
 
@@ -111,7 +112,8 @@ public:
 	bool built = false, stepped = false;
 	int generation = 0;
 
-	// ---- host topology ----
+	// ---- host topology (caller index space) and the internal order ----
+	std::vector<int> perm, inv;
 	HostGraph graph;
 	HostClusters clusters;
 	HostEdgeColoring coloring;
@@ -133,18 +135,24 @@ public:
 	DBuf<float> gs_rest, gs_stiff, gs_lam;
 	DBuf<unsigned int> sc_keys;
 	DBuf<int> sc_bucket, sc_start, sc_cursor, sc_idx_sorted, sc_contacts, sc_counts, sc_block_sums, d_obj_id;
-	DBuf<float4> sc_dp;
+	DBuf<float4> sc_dp, sc_sp, sc_sr, sc_sx;
 	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
+	DBuf<int> d_perm;
 	DBuf<int> att_idx;
 	DBuf<float> att_pos;
 	bool att_active = false;
 	StepParams* d_params = nullptr;
-	StepParams* h_params = nullptr;
+	StepParams* h_params = nullptr;      // current ring slot
+	static constexpr int kParamSlots = 8;
+	StepParams* h_param_ring = nullptr;  // pinned; a slot is rewritten only after its copy ran
+	cudaEvent_t param_ev[kParamSlots] = {};
+	int param_next = 0;
 	DevCounters* d_ctr = nullptr;
 	DevCounters* h_ctr = nullptr;
-	int* h_att_idx = nullptr;
-	float* h_att_pos = nullptr;
-	int h_att_cap = 0;
+	static constexpr int kStagingSlots = 4;
+	struct Staging { int* idx = nullptr; float* pos = nullptr; int cap = 0; cudaEvent_t ev = nullptr; };
+	Staging staging[kStagingSlots];
+	int staging_next = 0;
 
 	// ---- execution ----
 	cudaStream_t stream = nullptr;
@@ -170,13 +178,18 @@ public:
 		graph_key.clear();
 		free_device();
 		if (d_params) cudaFree(d_params);
-		if (h_params) cudaFreeHost(h_params);
+		for (auto& e : param_ev) if (e) { cudaEventSynchronize(e); cudaEventDestroy(e); e = nullptr; }
+		if (h_param_ring) cudaFreeHost(h_param_ring);
+		h_param_ring = nullptr;
 		if (d_ctr) cudaFree(d_ctr);
 		if (h_ctr) cudaFreeHost(h_ctr);
-		if (h_att_idx) cudaFreeHost(h_att_idx);
-		if (h_att_pos) cudaFreeHost(h_att_pos);
+		for (auto& st : staging) {
+			if (st.ev) cudaEventSynchronize(st.ev), cudaEventDestroy(st.ev);
+			if (st.idx) cudaFreeHost(st.idx);
+			if (st.pos) cudaFreeHost(st.pos);
+			st = Staging();
+		}
 		d_params = nullptr; h_params = nullptr; d_ctr = nullptr; h_ctr = nullptr;
-		h_att_idx = nullptr; h_att_pos = nullptr; h_att_cap = 0;
 		for (auto& e : event_pool) cudaEventDestroy(e);
 		event_pool.clear();
 		prof_records.clear();
@@ -194,8 +207,9 @@ public:
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
 		sc_contacts.release(); sc_counts.release(); sc_block_sums.release(); d_obj_id.release(); sc_dp.release();
+		sc_sp.release(); sc_sr.release(); sc_sx.release();
 		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
-		att_idx.release(); att_pos.release();
+		att_idx.release(); att_pos.release(); d_perm.release();
 		att_active = false;
 		coloring_built = false;
 		sc_table = 0;
@@ -210,7 +224,9 @@ public:
 		}
 		if (!d_params) {
 			CK(cudaMalloc(&d_params, sizeof(StepParams)));
-			CK(cudaMallocHost(&h_params, sizeof(StepParams)));
+			CK(cudaMallocHost(&h_param_ring, sizeof(StepParams) * kParamSlots));
+			for (auto& e : param_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+			h_params = h_param_ring;
 			CK(cudaMalloc(&d_ctr, sizeof(DevCounters)));
 			CK(cudaMallocHost(&h_ctr, sizeof(DevCounters)));
 			CK(cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), stream));
@@ -220,6 +236,90 @@ public:
 	}
 
 	// ------------------------------------------------------------------ build
+	// Internal order: device slot r holds the caller's Gaussian perm[r] (Morton order of the
+	// rest positions, so that graph, cluster and hash-cell neighbours sit close in memory);
+	// inv[perm[r]] = r.  Every topology is built in the caller's index space — the
+	// reference's construction order is index-dependent — and only then relabelled, with
+	// every list keeping its order, so the kernels see exactly the reference's sequences.
+	void compute_order()
+	{
+		perm.resize(n);
+		inv.resize(n);
+		for (int i = 0; i < n; ++i) perm[i] = i;
+		if (S.reorder && n > 1) {
+			float lo[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, hi[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+			for (int i = 0; i < n; ++i)
+				for (int a = 0; a < 3; ++a) {
+					const float v = in_pos[3 * i + a];
+					if (std::isfinite(v)) { lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
+				}
+			std::vector<unsigned long long> code(n);
+			auto spread = [](unsigned long long v) {
+				v &= 0x1fffffull;
+				v = (v | v << 32) & 0x1f00000000ffffull;
+				v = (v | v << 16) & 0x1f0000ff0000ffull;
+				v = (v | v << 8) & 0x100f00f00f00f00full;
+				v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+				v = (v | v << 2) & 0x1249249249249249ull;
+				return v;
+			};
+			for (int i = 0; i < n; ++i) {
+				unsigned long long c = 0;
+				for (int a = 0; a < 3; ++a) {
+					const float ext = hi[a] > lo[a] ? hi[a] - lo[a] : 1.0f;
+					float u = (in_pos[3 * i + a] - lo[a]) / ext;
+					if (!std::isfinite(u)) u = 0.0f;
+					u = std::min(std::max(u, 0.0f), 1.0f);
+					c |= spread((unsigned long long)(u * 2097151.0f)) << a;
+				}
+				code[i] = c;
+			}
+			std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return code[a] < code[b]; });
+		}
+		for (int r = 0; r < n; ++r) inv[perm[r]] = r;
+	}
+
+	// caller-order CSR (off[N+1], idx) -> internal order, neighbour order kept
+	void relabel_csr(const std::vector<int>& off_o, const std::vector<int>& idx_o, std::vector<int>& off_i,
+		std::vector<int>& idx_i, std::vector<int>* src_pos = nullptr) const
+	{
+		off_i.assign(n + 1, 0);
+		for (int r = 0; r < n; ++r) off_i[r + 1] = off_i[r] + (off_o[perm[r] + 1] - off_o[perm[r]]);
+		idx_i.resize(std::max(off_i[n], 1));
+		if (src_pos) src_pos->resize(std::max(off_i[n], 1));
+		for (int r = 0; r < n; ++r) {
+			const int o = perm[r];
+			for (int e = off_o[o], d = off_i[r]; e < off_o[o + 1]; ++e, ++d) {
+				const int j = idx_o[e];
+				idx_i[d] = (j >= 0 && j < n) ? inv[j] : j;
+				if (src_pos) (*src_pos)[d] = e;
+			}
+		}
+	}
+
+	template <typename T>
+	std::vector<T> to_internal(const T* src, int width) const
+	{
+		std::vector<T> out((size_t)n * width);
+		for (int r = 0; r < n; ++r)
+			for (int a = 0; a < width; ++a) out[(size_t)r * width + a] = src[(size_t)perm[r] * width + a];
+		return out;
+	}
+
+	int upload_positions(const float* pos3, const float* vel3)
+	{
+		std::vector<float4> p4(n), v4(n);
+		for (int r = 0; r < n; ++r) {
+			const int o = perm[r];
+			p4[r] = make_float4(pos3[3 * o], pos3[3 * o + 1], pos3[3 * o + 2], 1.0f);
+			v4[r] = vel3 ? make_float4(vel3[3 * o], vel3[3 * o + 1], vel3[3 * o + 2], 0.0f) : make_float4(0, 0, 0, 0);
+		}
+		CK(cudaMemcpyAsync(pos_curr.p, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(vel.p, v4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(pos_out3.p, pos3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+		return sync();
+	}
+
 	// ensureChainmailGPU (forward.cu:10519-10845): graph upload, colourings, clusters
 	int build()
 	{
@@ -228,35 +328,56 @@ public:
 		graph_key.clear();
 		if (ensure_stream()) return -1;
 		build_graph(n, n_edges, in_edges.data(), in_rest.data(), in_stiff.data(), graph);
+		compute_order();
 		const int m = graph.off[n];
-		std::vector<float4> p4(n);
-		for (int i = 0; i < n; ++i) p4[i] = make_float4(in_pos[3 * i], in_pos[3 * i + 1], in_pos[3 * i + 2], 1.0f);
+		CK(d_perm.alloc(n));
+		CK(cudaMemcpyAsync(d_perm.p, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
 		CK(pos_curr.alloc(n)); CK(pos_next.alloc(n)); CK(pos_tmp.alloc(n)); CK(vel.alloc(n)); CK(pos_rest.alloc(n));
 		CK(pos_out3.alloc(3 * (size_t)n));
-		CK(cudaMemcpyAsync(pos_curr.p, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
-		for (auto& v : p4) v.w = 0.0f;
-		CK(cudaMemcpyAsync(pos_rest.p, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
-		CK(cudaMemsetAsync(vel.p, 0, vel.bytes(), stream));
-		CK(cudaMemcpyAsync(pos_out3.p, in_pos.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
-		CK(off.alloc(n + 1)); CK(nbr.alloc(std::max(m, 1))); CK(ndist.alloc(std::max(m, 1)));
-		CK(nstiff.alloc(std::max(m, 1))); CK(lam.alloc(std::max(m, 1)));
-		CK(cudaMemcpyAsync(off.p, graph.off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
-		if (m > 0) {
-			CK(cudaMemcpyAsync(nbr.p, graph.nbr.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
-			CK(cudaMemcpyAsync(ndist.p, graph.ndist.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
-			CK(cudaMemcpyAsync(nstiff.p, graph.nstiff.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
+		{
+			std::vector<float4> r4(n);
+			for (int r = 0; r < n; ++r) {
+				const int o = perm[r];
+				r4[r] = make_float4(in_pos[3 * o], in_pos[3 * o + 1], in_pos[3 * o + 2], 0.0f);
+			}
+			CK(cudaMemcpyAsync(pos_rest.p, r4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, stream));
+		}
+		if (upload_positions(in_pos.data(), nullptr)) return -1;
+		{
+			std::vector<int> off_i, nbr_i, src;
+			relabel_csr(graph.off, graph.nbr, off_i, nbr_i, &src);
+			std::vector<float> nd(std::max(m, 1)), ns(std::max(m, 1));
+			for (int e = 0; e < m; ++e) { nd[e] = graph.ndist[src[e]]; ns[e] = graph.nstiff[src[e]]; }
+			CK(off.alloc(n + 1)); CK(nbr.alloc(std::max(m, 1))); CK(ndist.alloc(std::max(m, 1)));
+			CK(nstiff.alloc(std::max(m, 1))); CK(lam.alloc(std::max(m, 1)));
+			CK(cudaMemcpyAsync(off.p, off_i.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+			if (m > 0) {
+				CK(cudaMemcpyAsync(nbr.p, nbr_i.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
+				CK(cudaMemcpyAsync(ndist.p, nd.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
+				CK(cudaMemcpyAsync(nstiff.p, ns.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
+			}
+			CK(cudaStreamSynchronize(stream));
 		}
 		CK(d_scales.alloc(3 * (size_t)n)); CK(d_rots.alloc(4 * (size_t)n));
 		CK(d_out_scales.alloc(3 * (size_t)n)); CK(d_out_quats.alloc(4 * (size_t)n));
-		CK(cudaMemcpyAsync(d_scales.p, in_scales.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
-		CK(cudaMemcpyAsync(d_rots.p, in_rots.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, stream));
+		{
+			const auto sc = to_internal(in_scales.data(), 3);
+			const auto rt = to_internal(in_rots.data(), 4);
+			CK(cudaMemcpyAsync(d_scales.p, sc.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(d_rots.p, rt.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, stream));
+			CK(cudaStreamSynchronize(stream));
+		}
 		CK(det_rest.alloc(n)); CK(v_rest.alloc(n)); CK(rest_len.alloc(n)); CK(sigma_rest.alloc(6 * (size_t)n));
 		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * (size_t)n));
 		CK(cudaMemsetAsync(rec.p, 0, rec.bytes(), stream));
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		build_components(graph, 50, obj_id, num_objects);
-		CK(d_obj_id.alloc(n));
-		CK(cudaMemcpyAsync(d_obj_id.p, obj_id.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+		{
+			const auto oi = to_internal(obj_id.data(), 1);
+			CK(d_obj_id.alloc(n));
+			CK(cudaMemcpyAsync(d_obj_id.p, oi.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+			CK(cudaStreamSynchronize(stream));
+		}
 		spacing = graph_spacing(graph);
 		S.topo_dirty = false;
 		if (rebuild_clusters()) return -1;
@@ -270,23 +391,28 @@ public:
 	int rebuild_clusters()
 	{
 		build_clusters(graph, in_pos.data(), S.ring_k, S.max_members, S.leader_min_hop, clusters);
-		const size_t nv = std::max<size_t>(clusters.vol_idx.size(), 1), nr = std::max<size_t>(clusters.rev_idx.size(), 1);
-		CK(vol_off.alloc(n + 1)); CK(vol_idx.alloc(nv)); CK(rev_off.alloc(n + 1)); CK(rev_idx.alloc(nr));
-		CK(cudaMemcpyAsync(vol_off.p, clusters.vol_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
-		CK(cudaMemcpyAsync(vol_idx.p, clusters.vol_idx.data(), sizeof(int) * clusters.vol_idx.size(), cudaMemcpyHostToDevice, stream));
-		CK(cudaMemcpyAsync(rev_off.p, clusters.rev_off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
-		CK(cudaMemcpyAsync(rev_idx.p, clusters.rev_idx.data(), sizeof(int) * clusters.rev_idx.size(), cudaMemcpyHostToDevice, stream));
+		std::vector<int> voff_i, vidx_i, roff_i, ridx_i;
+		relabel_csr(clusters.vol_off, clusters.vol_idx, voff_i, vidx_i);
+		relabel_csr(clusters.rev_off, clusters.rev_idx, roff_i, ridx_i);
+		CK(vol_off.alloc(n + 1)); CK(vol_idx.alloc(vidx_i.size())); CK(rev_off.alloc(n + 1)); CK(rev_idx.alloc(ridx_i.size()));
+		CK(cudaMemcpyAsync(vol_off.p, voff_i.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(vol_idx.p, vidx_i.data(), sizeof(int) * vidx_i.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(rev_off.p, roff_i.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(rev_idx.p, ridx_i.data(), sizeof(int) * ridx_i.size(), cudaMemcpyHostToDevice, stream));
 		vol_gs_order.release();
-		if (!clusters.gs_order.empty()) {
-			CK(vol_gs_order.alloc(clusters.gs_order.size()));
-			CK(cudaMemcpyAsync(vol_gs_order.p, clusters.gs_order.data(), sizeof(int) * clusters.gs_order.size(),
-				cudaMemcpyHostToDevice, stream));
+		std::vector<int> order_i(clusters.gs_order.size());
+		for (size_t t = 0; t < order_i.size(); ++t) order_i[t] = inv[clusters.gs_order[t]];
+		if (!order_i.empty()) {
+			CK(vol_gs_order.alloc(order_i.size()));
+			CK(cudaMemcpyAsync(vol_gs_order.p, order_i.data(), sizeof(int) * order_i.size(), cudaMemcpyHostToDevice,
+				stream));
 		}
 		const int blocks = (n + kBlock - 1) / kBlock;
 		dev::k_volume_rest<<<blocks, kBlock, 0, stream>>>(n, pos_rest.p, vol_off.p, vol_idx.p, off.p, nbr.p,
 			S.vol_aniso, sigma_rest.p, det_rest.p, v_rest.p, rest_len.p, mat_type.p);
 		CK(cudaGetLastError());
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
+		CK(cudaStreamSynchronize(stream));
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
 		graph_key.clear();
 		++generation;
@@ -298,15 +424,19 @@ public:
 		if (coloring_built) return 0;
 		build_edge_coloring(graph, coloring);
 		const size_t ne = coloring.edge.size();
+		std::vector<int2> e_i(std::max<size_t>(ne, 1));
+		for (size_t e = 0; e < ne; ++e) e_i[e] = make_int2(inv[coloring.edge[e].x], inv[coloring.edge[e].y]);
 		CK(gs_edge.alloc(std::max<size_t>(ne, 1))); CK(gs_rest.alloc(std::max<size_t>(ne, 1)));
 		CK(gs_stiff.alloc(std::max<size_t>(ne, 1))); CK(gs_lam.alloc(std::max<size_t>(ne, 1)));
 		if (ne) {
-			CK(cudaMemcpyAsync(gs_edge.p, coloring.edge.data(), sizeof(int2) * ne, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(gs_edge.p, e_i.data(), sizeof(int2) * ne, cudaMemcpyHostToDevice, stream));
 			CK(cudaMemcpyAsync(gs_rest.p, coloring.rest.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, stream));
 			CK(cudaMemcpyAsync(gs_stiff.p, coloring.stiff.data(), sizeof(float) * ne, cudaMemcpyHostToDevice, stream));
 		}
 		CK(cudaStreamSynchronize(stream));
 		coloring_built = true;
+		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		graph_key.clear();
 		return 0;
 	}
 
@@ -320,12 +450,23 @@ public:
 		const int buckets = table + 1;   // + sentinel bucket
 		CK(sc_keys.alloc(n)); CK(sc_bucket.alloc(buckets + 1)); CK(sc_start.alloc(buckets + 1));
 		CK(sc_cursor.alloc(buckets)); CK(sc_idx_sorted.alloc(n)); CK(sc_contacts.alloc((size_t)n * kSelfColMax));
-		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
+		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
 		CK(cudaMemsetAsync(sc_counts.p, 0, sc_counts.bytes(), stream));
 		return 0;
 	}
 
 	// ------------------------------------------------------------------ params
+	int upload_params()
+	{
+		CK(cudaEventSynchronize(param_ev[param_next]));
+		h_params = h_param_ring + param_next;
+		fill_params();
+		CK(cudaMemcpyAsync(d_params, h_params, sizeof(StepParams), cudaMemcpyHostToDevice, stream));
+		CK(cudaEventRecord(param_ev[param_next], stream));
+		param_next = (param_next + 1) % kParamSlots;
+		return 0;
+	}
+
 	void fill_params()
 	{
 		StepParams& P = *h_params;
@@ -381,7 +522,7 @@ public:
 
 	std::vector<long long> topology_key() const
 	{
-		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), use_warp(),
+		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), vol_lanes(), gather_lanes(),
 			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table };
 	}
@@ -417,6 +558,32 @@ public:
 		return dim3((unsigned)((items + per_block - 1) / per_block));
 	}
 
+	void enqueue_sc_candidates(dim3 G, dim3 B)
+	{
+		launch(ST_SC_BUILD, G, B, dev::k_sc_pack, n, (const int*)sc_idx_sorted.p, (const float4*)pos_curr.p,
+			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)d_obj_id.p, sc_sp.p, sc_sr.p, sc_sx.p);
+		launch(ST_SC_BUILD, G, B, dev::k_sc_build_sorted, n, (const StepParams*)d_params, (const float4*)pos_curr.p,
+			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p, (const int*)sc_start.p,
+			(unsigned)(sc_table - 1), (const int*)d_obj_id.p, (const float4*)sc_sp.p, (const float4*)sc_sr.p,
+			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p);
+	}
+
+	// volume kernel shapes: lanes per cluster (Kernel A) and per node (Kernel B);
+	// 0 = one thread per cluster / node
+	int vol_lanes() const
+	{
+		if (S.warp_mode == 2) return 32;
+		if (S.warp_mode == 1) return 0;
+		return clusters.avg_members >= 40.0f ? 8 : 4;
+	}
+	int gather_lanes() const
+	{
+		if (S.warp_mode == 2) return 32;
+		if (S.warp_mode == 1) return 0;
+		const double h = clusters.rev_off.empty() ? 0.0 : (double)clusters.rev_off[n] / std::max(n, 1);
+		return h >= 40.0 ? 8 : 4;
+	}
+
 	// one step's kernel sequence (the body of runXPBDSimulation)
 	int enqueue_step()
 	{
@@ -444,15 +611,12 @@ public:
 			launch(ST_SC_BUILD, G, B, dev::k_sc_scatter, N, (const unsigned*)sc_keys.p, (const int*)sc_start.p,
 				sc_cursor.p, sc_idx_sorted.p);
 			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
-				sc_idx_sorted.p);
-			launch(ST_SC_BUILD, G, B, dev::k_sc_build, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
-				(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p,
-				(const int*)sc_start.p, (unsigned)(sc_table - 1), (const int*)d_obj_id.p, d_ctr, sc_contacts.p,
-				sc_counts.p);
+				sc_idx_sorted.p, (const int*)d_perm.p);
+			enqueue_sc_candidates(G, B);
 		}
 		float4* pin = pos_next.p;
 		float4* pout = pos_tmp.p;
-		const bool dgs = dist_gs_on(), vgs = vol_gs_on(), warp = use_warp();
+		const bool dgs = dist_gs_on(), vgs = vol_gs_on();
 		const bool project = S.kin_count > 0 || S.ground_on || sc;
 		for (int it = 0; it < S.iters; ++it) {
 			const int first = (it == 0), last = (it == S.iters - 1);
@@ -483,22 +647,37 @@ public:
 					}
 				}
 				else {
-					if (warp)
-						launch(ST_VOL_SOLVE, GW, B, dev::k_volume_solve_warp<8>, N, (const StepParams*)d_params,
-							(const float4*)pin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, first ? 0 : 1);
+					const int la = vol_lanes(), lb = gather_lanes();
+					const int rl = first ? 0 : 1;
+					const StepParams* dp = d_params;
+					const float4* cpin = pin;
+					if (la == 32)
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 32), B, dev::k_volume_solve_group<32, 8>, N, dp, cpin,
+							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
+							lam_vol.p, rec.p, rl);
+					else if (la == 8)
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_group<8, 8>, N, dp, cpin,
+							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
+							lam_vol.p, rec.p, rl);
+					else if (la == 4)
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_group<4, 4>, N, dp, cpin,
+							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
+							lam_vol.p, rec.p, rl);
 					else
-						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, (const StepParams*)d_params,
-							(const float4*)pin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, first ? 0 : 1);
-					if (warp)
-						launch(ST_VOL_GATHER, GW, B, dev::k_volume_gather_warp, N, (const StepParams*)d_params,
-							(const float4*)pin, pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p,
-							(const float*)rest_len.p);
+						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
+							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
+					if (lb == 32)
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, N, dp, cpin,
+							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+					else if (lb == 8)
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
+							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+					else if (lb == 4)
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B, dev::k_volume_gather_group<4>, N, dp, cpin,
+							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
 					else
-						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, (const StepParams*)d_params,
-							(const float4*)pin, pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p,
-							(const float*)rest_len.p);
+						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
+							(const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
 					std::swap(pin, pout);
 				}
 			}
@@ -516,7 +695,7 @@ public:
 					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0);
 		}
 		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
-			vel.p, pos_out3.p);
+			vel.p, pos_out3.p, (const int*)d_perm.p);
 		if (S.jstats) {
 			CK(cudaMemsetAsync(d_ctr->jstats, 0, sizeof(double) * 3, stream));
 			launch(ST_JSTATS, G, B, dev::k_jstats, N, (const float4*)pos_curr.p, (const int*)vol_off.p,
@@ -539,8 +718,7 @@ public:
 		}
 		if (S.use_distance && S.dist_gs && ensure_coloring()) return -1;
 		if (S.sc_enabled && ensure_selfcol()) return -1;
-		fill_params();
-		CK(cudaMemcpyAsync(d_params, h_params, sizeof(StepParams), cudaMemcpyHostToDevice, stream));
+		if (upload_params()) return -1;
 		if (profiling || !S.use_graph) {
 			if (enqueue_step()) return -1;
 		}
@@ -614,21 +792,31 @@ public:
 			if (!inv_mass_saved.p) CK(inv_mass_saved.alloc(N));
 			dev::k_get_w<<<blocks_for(N), kBlock, 0, stream>>>(N, pos_curr.p, inv_mass_saved.p);
 		}
-		if (count > h_att_cap) {
-			CK(cudaStreamSynchronize(stream));
-			if (h_att_idx) cudaFreeHost(h_att_idx);
-			if (h_att_pos) cudaFreeHost(h_att_pos);
-			CK(cudaMallocHost(&h_att_idx, sizeof(int) * count));
-			CK(cudaMallocHost(&h_att_pos, sizeof(float) * 3 * count));
+		// targets go through a small ring of pinned staging slots; a slot is reused only
+		// after the event recorded behind its last copy has completed
+		if ((int)att_idx.n < count) {
 			CK(att_idx.alloc(count));
 			CK(att_pos.alloc(3 * (size_t)count));
-			h_att_cap = count;
 		}
-		else CK(cudaStreamSynchronize(stream));   // the pinned staging buffers may still be in flight
-		memcpy(h_att_idx, idx, sizeof(int) * count);
-		memcpy(h_att_pos, pos, sizeof(float) * 3 * count);
-		CK(cudaMemcpyAsync(att_idx.p, h_att_idx, sizeof(int) * count, cudaMemcpyHostToDevice, stream));
-		CK(cudaMemcpyAsync(att_pos.p, h_att_pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
+		Staging& st = staging[staging_next];
+		staging_next = (staging_next + 1) % kStagingSlots;
+		if (st.ev) CK(cudaEventSynchronize(st.ev));
+		else CK(cudaEventCreateWithFlags(&st.ev, cudaEventDisableTiming));
+		if (count > st.cap) {
+			if (st.idx) cudaFreeHost(st.idx);
+			if (st.pos) cudaFreeHost(st.pos);
+			st.idx = nullptr;
+			st.pos = nullptr;
+			st.cap = 0;
+			CK(cudaMallocHost(&st.idx, sizeof(int) * count));
+			CK(cudaMallocHost(&st.pos, sizeof(float) * 3 * count));
+			st.cap = count;
+		}
+		for (int k = 0; k < count; ++k) st.idx[k] = (idx[k] >= 0 && idx[k] < N) ? inv[idx[k]] : -1;
+		memcpy(st.pos, pos, sizeof(float) * 3 * count);
+		CK(cudaMemcpyAsync(att_idx.p, st.idx, sizeof(int) * count, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(att_pos.p, st.pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
+		CK(cudaEventRecord(st.ev, stream));
 		dev::k_attach<<<blocks_for(count), kBlock, 0, stream>>>(count, att_idx.p, att_pos.p, N, pos_curr.p, vel.p);
 		CK(cudaGetLastError());
 		att_active = true;
@@ -859,8 +1047,7 @@ XPBD_API int xpbd_positions_host(float* out, int n)
 	if (!g_engine || !g_engine->stepped) return fail("xpbd_positions_host: no step yet");
 	Engine& E = *g_engine;
 	if (!out || n != E.n) return fail("xpbd_positions_host: size mismatch");
-	CK(cudaMemcpy2DAsync(out, sizeof(float) * 3, E.pos_curr.p, sizeof(float4), sizeof(float) * 3, n,
-		cudaMemcpyDeviceToHost, E.stream));
+	CK(cudaMemcpyAsync(out, E.pos_out3.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, E.stream));
 	return E.sync();
 }
 
@@ -871,7 +1058,7 @@ XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* host
 	if (n != E.n) return fail("xpbd_compute_shapes: size mismatch");
 	CK(cudaMemsetAsync(&E.d_ctr->shapes_deformed, 0, sizeof(unsigned int) * 2, E.stream));
 	dev::k_deformed_shapes<<<Engine::blocks_for(n), kBlock, 0, E.stream>>>(n, E.pos_rest.p, E.pos_curr.p, E.off.p,
-		E.nbr.p, E.d_scales.p, E.d_rots.p, deformEps, E.d_out_scales.p, E.d_out_quats.p, E.d_ctr);
+		E.nbr.p, E.d_scales.p, E.d_rots.p, deformEps, E.d_out_scales.p, E.d_out_quats.p, E.d_ctr, E.d_perm.p);
 	CK(cudaGetLastError());
 	if (hostScales)
 		CK(cudaMemcpyAsync(hostScales, E.d_out_scales.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, E.stream));
@@ -887,13 +1074,8 @@ XPBD_API int xpbd_reset(void)
 	if (!g_engine || !g_engine->stepped) return fail("xpbd_reset: no step yet");
 	Engine& E = *g_engine;
 	if (E.set_attached(0, nullptr, nullptr)) return -1;
-	std::vector<float4> p4(E.n);
-	for (int i = 0; i < E.n; ++i) p4[i] = make_float4(E.in_pos[3 * i], E.in_pos[3 * i + 1], E.in_pos[3 * i + 2], 1.0f);
-	CK(cudaMemcpyAsync(E.pos_curr.p, p4.data(), sizeof(float4) * E.n, cudaMemcpyHostToDevice, E.stream));
-	CK(cudaMemcpyAsync(E.pos_out3.p, E.in_pos.data(), sizeof(float) * 3 * E.n, cudaMemcpyHostToDevice, E.stream));
-	CK(cudaMemsetAsync(E.vel.p, 0, E.vel.bytes(), E.stream));
 	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
-	return E.sync();
+	return E.upload_positions(E.in_pos.data(), nullptr);
 }
 
 XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt)
@@ -918,22 +1100,17 @@ XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt)
 	}
 	const float vx = lin ? lin[0] : 0.0f, vy = lin ? lin[1] : 0.0f, vz = lin ? lin[2] : 0.0f;
 	const float wx = ang ? ang[0] : 0.0f, wy = ang ? ang[1] : 0.0f, wz = ang ? ang[2] : 0.0f;
-	std::vector<float4> p4(N), v4(N);
-	std::vector<float> p3(3 * (size_t)N);
+	std::vector<float> p3(3 * (size_t)N), v3(3 * (size_t)N);
 	for (int i = 0; i < N; ++i) {
 		const float px = E.in_pos[3 * i] - comX, py = E.in_pos[3 * i + 1] - comY, pz = E.in_pos[3 * i + 2] - comZ;
 		const float rx = R[0] * px + R[1] * py + R[2] * pz;
 		const float ry = R[3] * px + R[4] * py + R[5] * pz;
 		const float rz = R[6] * px + R[7] * py + R[8] * pz;
-		p4[i] = make_float4(comX + rx, comY + ry, comZ + rz, 1.0f);
-		p3[3 * i] = p4[i].x; p3[3 * i + 1] = p4[i].y; p3[3 * i + 2] = p4[i].z;
-		v4[i] = make_float4(vx + (wy * rz - wz * ry), vy + (wz * rx - wx * rz), vz + (wx * ry - wy * rx), 0.0f);
+		p3[3 * i] = comX + rx; p3[3 * i + 1] = comY + ry; p3[3 * i + 2] = comZ + rz;
+		v3[3 * i] = vx + (wy * rz - wz * ry); v3[3 * i + 1] = vy + (wz * rx - wx * rz); v3[3 * i + 2] = vz + (wx * ry - wy * rx);
 	}
-	CK(cudaMemcpyAsync(E.pos_curr.p, p4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
-	CK(cudaMemcpyAsync(E.vel.p, v4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
-	CK(cudaMemcpyAsync(E.pos_out3.p, p3.data(), sizeof(float) * 3 * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
-	return E.sync();
+	return E.upload_positions(p3.data(), v3.data());
 }
 
 XPBD_API int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo)
@@ -1006,6 +1183,8 @@ XPBD_API void xpbd_b200_set_gs(int distance, int volume)
 XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { S.warp_mode = std::max(0, std::min(2, mode)); }
 
 XPBD_API void xpbd_b200_set_graph(int enabled) { S.use_graph = enabled != 0; }
+
+XPBD_API void xpbd_b200_set_reorder(int enabled) { S.reorder = enabled != 0; }
 
 XPBD_API int xpbd_b200_set_profiling(int enabled)
 {
@@ -1083,6 +1262,20 @@ int copy_host(const std::vector<T>& v, long long count, T* out, long long cap)
 	std::copy(v.begin(), v.begin() + count, out);
 	return (int)count;
 }
+// device array in internal order -> caller order (rows of `width`)
+template <typename T>
+int dev_to_caller(const Engine& E, const T* src, int width, T* out, long long cap)
+{
+	const long long count = (long long)E.n * width;
+	if (!src) return -1;
+	if (!out) return (int)count;
+	if (cap < count) return -1;
+	std::vector<T> tmp(count);
+	if (copy_dev(src, count, tmp.data(), count, E.stream) < 0) return -1;
+	for (int r = 0; r < E.n; ++r)
+		for (int a = 0; a < width; ++a) out[(size_t)E.perm[r] * width + a] = tmp[(size_t)r * width + a];
+	return (int)count;
+}
 }  // namespace
 
 // Stage buffers by name, in the reference's layouts (counts per row instead of N+1
@@ -1111,7 +1304,7 @@ XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap)
 	if (s == "vol_gs_color_offset")
 		return copy_host(E.clusters.gs_color_off, (long long)E.clusters.gs_color_off.size(), out, cap);
 	if (s == "obj_id") return copy_host(E.obj_id, N, out, cap);
-	if (s == "mat_type") return copy_dev(E.mat_type.p, N, out, cap, E.stream);
+	if (s == "mat_type") return dev_to_caller(E, E.mat_type.p, 1, out, cap);
 	if (s == "gs_edge" || s == "gs_color_offset") {
 		if (E.ensure_coloring()) return -1;
 		if (s == "gs_color_offset") return copy_host(E.coloring.color_off, (long long)E.coloring.color_off.size(), out, cap);
@@ -1120,10 +1313,24 @@ XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap)
 		return copy_host(flat, (long long)flat.size(), out, cap);
 	}
 	if (!E.sc_table) return -1;
-	if (s == "sc_keys") return copy_dev(reinterpret_cast<const int*>(E.sc_keys.p), N, out, cap, E.stream);
-	if (s == "sc_idx_sorted") return copy_dev(E.sc_idx_sorted.p, N, out, cap, E.stream);
-	if (s == "sc_count") return copy_dev(E.sc_counts.p, N, out, cap, E.stream);
-	if (s == "sc_contact") return copy_dev(E.sc_contacts.p, (long long)N * kSelfColMax, out, cap, E.stream);
+	if (s == "sc_keys") return dev_to_caller(E, reinterpret_cast<const int*>(E.sc_keys.p), 1, out, cap);
+	if (s == "sc_count") return dev_to_caller(E, E.sc_counts.p, 1, out, cap);
+	if (s == "sc_idx_sorted") {
+		const int r = copy_dev(E.sc_idx_sorted.p, N, out, cap, E.stream);
+		if (r > 0 && out)
+			for (int t = 0; t < N; ++t) out[t] = E.perm[out[t]];
+		return r;
+	}
+	if (s == "sc_contact") {
+		const int r = dev_to_caller(E, E.sc_contacts.p, kSelfColMax, out, cap);
+		if (r > 0 && out)
+			for (long long t = 0; t < (long long)N * kSelfColMax; ++t) {
+				const int c = out[t];
+				if (c >= 0 && c < N) out[t] = E.perm[c];
+				else if (c < 0 && -c - 1 < N) out[t] = -(E.perm[-c - 1] + 1);
+			}
+		return r;
+	}
 	if (s == "sc_keys_sorted" || s == "sc_cell_start" || s == "sc_cell_end") {
 		std::vector<int> start(E.sc_table + 2), keys(N), idx(N);
 		if (copy_dev(E.sc_start.p, E.sc_table + 2, start.data(), E.sc_table + 2, E.stream) < 0) return -1;
@@ -1150,10 +1357,10 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 	Engine& E = *g_engine;
 	const int N = E.n;
 	const std::string s(name);
-	if (s == "det_rest") return copy_dev(E.det_rest.p, N, out, cap, E.stream);
-	if (s == "sigma_rest") return copy_dev(E.sigma_rest.p, 6LL * N, out, cap, E.stream);
-	if (s == "v_rest") return copy_dev(E.v_rest.p, N, out, cap, E.stream);
-	if (s == "rest_len") return copy_dev(E.rest_len.p, N, out, cap, E.stream);
+	if (s == "det_rest") return dev_to_caller(E, E.det_rest.p, 1, out, cap);
+	if (s == "sigma_rest") return dev_to_caller(E, E.sigma_rest.p, 6, out, cap);
+	if (s == "v_rest") return dev_to_caller(E, E.v_rest.p, 1, out, cap);
+	if (s == "rest_len") return dev_to_caller(E, E.rest_len.p, 1, out, cap);
 	if (s == "gs_rest" || s == "gs_stiff") {
 		if (E.ensure_coloring()) return -1;
 		const auto& v = (s == "gs_rest") ? E.coloring.rest : E.coloring.stiff;
@@ -1163,9 +1370,10 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 		std::vector<float4> tmp(N);
 		if (copy_dev(s == "vel" ? E.vel.p : E.pos_curr.p, N, tmp.data(), N, E.stream) < 0) return -1;
 		std::vector<float> v(s == "vel" ? 3 * (size_t)N : N);
-		for (int i = 0; i < N; ++i) {
-			if (s == "vel") { v[3 * i] = tmp[i].x; v[3 * i + 1] = tmp[i].y; v[3 * i + 2] = tmp[i].z; }
-			else v[i] = tmp[i].w;
+		for (int r = 0; r < N; ++r) {
+			const int i = E.perm[r];
+			if (s == "vel") { v[3 * i] = tmp[r].x; v[3 * i + 1] = tmp[r].y; v[3 * i + 2] = tmp[r].z; }
+			else v[i] = tmp[r].w;
 		}
 		return copy_host(v, (long long)v.size(), out, cap);
 	}
@@ -1189,18 +1397,18 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	if (!g_engine || !g_engine->built || !x || !p) return fail("xpbd_b200_selfcol_build: no scene");
 	Engine& E = *g_engine;
 	if (E.ensure_selfcol()) return -1;
-	E.fill_params();
+	if (E.upload_params()) return -1;
 	const int N = E.n;
 	std::vector<float4> a(N), b(N);
-	for (int i = 0; i < N; ++i) {
-		a[i] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 1.0f);
-		b[i] = make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 1.0f);
+	for (int r = 0; r < N; ++r) {
+		const int i = E.perm[r];
+		a[r] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 1.0f);
+		b[r] = make_float4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 1.0f);
 	}
 	std::vector<float4> keep_curr(N), keep_next(N);
 	CK(cudaMemcpyAsync(keep_curr.data(), E.pos_curr.p, sizeof(float4) * N, cudaMemcpyDeviceToHost, E.stream));
 	CK(cudaMemcpyAsync(keep_next.data(), E.pos_next.p, sizeof(float4) * N, cudaMemcpyDeviceToHost, E.stream));
 	CK(cudaStreamSynchronize(E.stream));
-	CK(cudaMemcpyAsync(E.d_params, E.h_params, sizeof(StepParams), cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemcpyAsync(E.pos_curr.p, a.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemcpyAsync(E.pos_next.p, b.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemsetAsync(E.d_ctr, 0, sizeof(DevCounters), E.stream));
@@ -1216,9 +1424,8 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	dev::k_scan_sums<<<1, 1024, 0, E.stream>>>(E.sc_block_sums.p, nb);
 	dev::k_scan_add<<<nb, 1024, 0, E.stream>>>(E.sc_start.p, scan_n, E.sc_block_sums.p);
 	dev::k_sc_scatter<<<G, B, 0, E.stream>>>(N, E.sc_keys.p, E.sc_start.p, E.sc_cursor.p, E.sc_idx_sorted.p);
-	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p);
-	dev::k_sc_build<<<G, B, 0, E.stream>>>(N, E.d_params, E.pos_curr.p, E.pos_next.p, E.pos_rest.p, E.sc_idx_sorted.p,
-		E.sc_start.p, (unsigned)(E.sc_table - 1), E.d_obj_id.p, E.d_ctr, E.sc_contacts.p, E.sc_counts.p);
+	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p, E.d_perm.p);
+	E.enqueue_sc_candidates(G, B);
 	CK(cudaGetLastError());
 	if (E.read_counters()) return -1;
 	// restore the solver state this stage check borrowed

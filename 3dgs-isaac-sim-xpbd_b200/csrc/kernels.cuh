@@ -330,28 +330,45 @@ __device__ __forceinline__ void store_record(float4* rec, int idx, float3 c, flo
 	rec[3 * idx + 2] = make_float4(S.m[2][0], S.m[2][1], 0.0f, 0.0f);
 }
 
-// Kernel A, one warp per cluster (forward.cu:8702-8863).  Lane L owns members
-// L, L+32, ...; their positions stay in registers across the centroid, covariance
-// and denominator passes (up to VC per lane), butterfly sums give every lane the
-// totals.  Reads per cluster: m member indices + m gathered positions (L2-resident).
-template <int VC>
-__global__ void __launch_bounds__(kBlock) k_volume_solve_warp(int n, const StepParams* __restrict__ P,
+// Kernel A on groups of S lanes per cluster (32/S clusters per warp).  Lane L of a group
+// owns members L, L+S, ...; their positions stay in registers (VC slots) across the
+// centroid, covariance and denominator passes, and butterfly sums inside the group give
+// every lane the totals.  S = 32 is the reference's warp kernel with its exact summation
+// order (forward.cu:8702-8863); smaller S runs the same operations with the per-cluster
+// serial 3x3 work (J, Sigma^-1) shared by fewer lanes, i.e. more clusters per warp
+// instruction.  No lane leaves before the last shuffle, so groups may diverge freely.
+// Reads per cluster: m member indices (coalesced runs of S) + m gathered positions.
+template <int S>
+__device__ __forceinline__ float group_sum(float v)
+{
+#pragma unroll
+	for (int o = S / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+template <int S, int VC>
+__global__ void __launch_bounds__(kBlock) k_volume_solve_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, int read_lam)
 {
-	const int lane = threadIdx.x & 31;
-	const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-	if (idx >= n) return;
-	if (mat_type[idx] != 0) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
-	const int off = voff[idx], cnt = voff[idx + 1] - off;
-	const float4 p4 = ld4(pin, idx);
+	const int sl = threadIdx.x & (S - 1);
+	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const bool in_range = idx < n;
+	bool valid = in_range && mat_type[idx] == 0;
+	int off = 0, cnt = 0;
+	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (valid) {
+		off = voff[idx];
+		cnt = voff[idx + 1] - off;
+		p4 = ld4(pin, idx);
+	}
 	const float3 pi = f3(p4);
 	float3 cache[VC];
 	float cw[VC];
 	int nc = 0, ucnt = 0;
 	float3 psum = make_float3(0.0f, 0.0f, 0.0f);
-	for (int k = lane; k < cnt; k += 32) {
+	for (int k = sl; k < cnt; k += S) {
 		const int j = __ldg(vidx + off + k);
 		if (j < 0 || j >= n) continue;
 		const float4 q = ld4(pin, j);
@@ -362,9 +379,9 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_warp(int n, const StepP
 			if (t == nc) { cache[t] = f3(q); cw[t] = q.w; }
 		if (nc < VC) ++nc;
 	}
-	const float sx = warp_sum(psum.x), sy = warp_sum(psum.y), sz = warp_sum(psum.z);
-	const int used = (int)(warp_sum((float)ucnt) + 0.5f);
-	if (used < 3) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
+	const float sx = group_sum<S>(psum.x), sy = group_sum<S>(psum.y), sz = group_sum<S>(psum.z);
+	const int used = (int)(group_sum<S>((float)ucnt) + 0.5f);
+	valid = valid && used >= 3;
 	const float inv_n = 1.0f / (float)(used + 1);
 	const float3 c = make_float3((sx + pi.x) * inv_n, (sy + pi.y) * inv_n, (sz + pi.z) * inv_n);
 	float a00 = 0.f, a11 = 0.f, a22 = 0.f, a01 = 0.f, a02 = 0.f, a12 = 0.f;
@@ -378,7 +395,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_warp(int n, const StepP
 	}
 	if (ucnt > nc) {
 		int seen = 0;
-		for (int k = lane; k < cnt; k += 32) {
+		for (int k = sl; k < cnt; k += S) {
 			const int j = __ldg(vidx + off + k);
 			if (j < 0 || j >= n) continue;
 			if (seen++ < nc) continue;
@@ -388,49 +405,53 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_warp(int n, const StepP
 			a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
 		}
 	}
-	if (lane == 0) {
+	if (sl == 0) {
 		const float dx = pi.x - c.x, dy = pi.y - c.y, dz = pi.z - c.z;
 		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
 		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
 	}
-	M3 S;
-	S.m[0][0] = warp_sum(a00) * inv_n;
-	S.m[1][1] = warp_sum(a11) * inv_n;
-	S.m[2][2] = warp_sum(a22) * inv_n;
-	const float s01 = warp_sum(a01) * inv_n, s02 = warp_sum(a02) * inv_n, s12 = warp_sum(a12) * inv_n;
-	S.m[0][1] = S.m[1][0] = s01;
-	S.m[0][2] = S.m[2][0] = s02;
-	S.m[1][2] = S.m[2][1] = s12;
-	float J, C;
+	M3 Sm;
+	Sm.m[0][0] = group_sum<S>(a00) * inv_n;
+	Sm.m[1][1] = group_sum<S>(a11) * inv_n;
+	Sm.m[2][2] = group_sum<S>(a22) * inv_n;
+	const float s01 = group_sum<S>(a01) * inv_n, s02 = group_sum<S>(a02) * inv_n, s12 = group_sum<S>(a12) * inv_n;
+	Sm.m[0][1] = Sm.m[1][0] = s01;
+	Sm.m[0][2] = Sm.m[2][0] = s02;
+	Sm.m[1][2] = Sm.m[2][1] = s12;
+	float J = 1.0f, C = 0.0f;
 	M3 Sinv;
-	if (!cluster_j_sinv(S, __ldg(det_rest + idx), J, C, Sinv)) { if (lane == 0) rec[3 * idx].w = 0.0f; return; }
+	m3_zero(Sinv);
+	if (valid) valid = cluster_j_sinv(Sm, __ldg(det_rest + idx), J, C, Sinv);
 	const float gs = J * inv_n;
 	const float ims = P->inv_mass_scale;
 	float dsum = 0.0f;
+	if (valid) {
 #pragma unroll
-	for (int t = 0; t < VC; ++t) {
-		if (t < nc) {
-			const float3 g = mul3(m3_mulv(Sinv, make_float3(cache[t].x - c.x, cache[t].y - c.y, cache[t].z - c.z)), gs);
-			dsum += (cw[t] * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		for (int t = 0; t < VC; ++t) {
+			if (t < nc) {
+				const float3 g = mul3(m3_mulv(Sinv, make_float3(cache[t].x - c.x, cache[t].y - c.y, cache[t].z - c.z)), gs);
+				dsum += (cw[t] * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+			}
+		}
+		if (ucnt > nc) {
+			int seen = 0;
+			for (int k = sl; k < cnt; k += S) {
+				const int j = __ldg(vidx + off + k);
+				if (j < 0 || j >= n) continue;
+				if (seen++ < nc) continue;
+				const float4 q = ld4(pin, j);
+				const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+				dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+			}
+		}
+		if (sl == 0) {
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(pi.x - c.x, pi.y - c.y, pi.z - c.z)), gs);
+			dsum += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
 		}
 	}
-	if (ucnt > nc) {
-		int seen = 0;
-		for (int k = lane; k < cnt; k += 32) {
-			const int j = __ldg(vidx + off + k);
-			if (j < 0 || j >= n) continue;
-			if (seen++ < nc) continue;
-			const float4 q = ld4(pin, j);
-			const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
-			dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
-		}
-	}
-	if (lane == 0) {
-		const float3 g = mul3(m3_mulv(Sinv, make_float3(pi.x - c.x, pi.y - c.y, pi.z - c.z)), gs);
-		dsum += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
-	}
-	const float denom = warp_sum(dsum);
-	if (lane != 0) return;
+	const float denom = group_sum<S>(dsum);
+	if (sl != 0 || !in_range) return;
+	if (!valid) { rec[3 * idx].w = 0.0f; return; }
 	const float dt = P->dt;
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const float alpha_t = P->vol_compliance / dt2;
@@ -541,24 +562,32 @@ __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl,
 	return add3(pi, mul3(avg, under_relax));
 }
 
-// Kernel B, one warp per node (forward.cu:9262-9323): mean over the clusters that
-// contain the node, step clamp 0.25 restLen, under-relaxation.  Reads per node: h
-// reverse indices + h gathered 48-byte records (L2-resident).
-__global__ void __launch_bounds__(kBlock) k_volume_gather_warp(int n, const StepParams* __restrict__ P,
+// Kernel B on groups of S lanes per node (forward.cu:9262-9323 with S = 32): mean over
+// the clusters that contain the node, step clamp 0.25 restLen, under-relaxation.  Reads
+// per node: h reverse indices + h gathered 48-byte records (L2-resident).
+template <int S>
+__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ rest_len)
 {
-	const int lane = threadIdx.x & 31;
-	const int idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-	if (idx >= n) return;
-	const float4 p4 = ld4(pin, idx);
+	const int sl = threadIdx.x & (S - 1);
+	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const bool in_range = idx < n;
+	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	int off = 0, cnt = 0;
+	float wi = 0.0f;
+	if (in_range) {
+		p4 = ld4(pin, idx);
+		wi = p4.w * P->inv_mass_scale;
+		if (wi > 0.0f) {
+			off = roff[idx];
+			cnt = roff[idx + 1] - off;
+		}
+	}
 	const float3 pi = f3(p4);
-	const float wi = p4.w * P->inv_mass_scale;
-	if (wi <= 0.0f) { if (lane == 0) pout[idx] = p4; return; }
-	const int off = roff[idx], cnt = roff[idx + 1] - off;
 	float3 sum = make_float3(0.0f, 0.0f, 0.0f);
 	int received = 0;
-	for (int k = lane; k < cnt; k += 32) {
+	for (int k = sl; k < cnt; k += S) {
 		const int i = __ldg(ridx + off + k);
 		if (i < 0 || i >= n) continue;
 		float3 dp;
@@ -566,10 +595,10 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_warp(int n, const Step
 		sum = add3(sum, dp);
 		++received;
 	}
-	const float sx = warp_sum(sum.x), sy = warp_sum(sum.y), sz = warp_sum(sum.z);
-	const int rc = (int)(warp_sum((float)received) + 0.5f);
-	if (lane != 0) return;
-	if (rc <= 0) { pout[idx] = p4; return; }
+	const float sx = group_sum<S>(sum.x), sy = group_sum<S>(sum.y), sz = group_sum<S>(sum.z);
+	const int rc = (int)(group_sum<S>((float)received) + 0.5f);
+	if (sl != 0 || !in_range) return;
+	if (!(wi > 0.0f) || rc <= 0) { pout[idx] = p4; return; }
 	const float inv_rec = 1.0f / (float)rc;
 	const float3 avg = make_float3(sx * inv_rec, sy * inv_rec, sz * inv_rec);
 	if (!fin3(avg)) { pout[idx] = p4; return; }
@@ -1082,7 +1111,7 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __restrict__ P,
 	float4* __restrict__ pos_curr, const float4* __restrict__ pfinal, float4* __restrict__ vel,
-	float* __restrict__ pos_out3)
+	float* __restrict__ pos_out3, const int* __restrict__ perm)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1136,9 +1165,10 @@ __global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __
 	vel[idx] = make_float4(v.x, v.y, v.z, 0.0f);
 	pos_curr[idx] = p4;
 	if (pos_out3) {
-		pos_out3[3 * idx + 0] = p.x;
-		pos_out3[3 * idx + 1] = p.y;
-		pos_out3[3 * idx + 2] = p.z;
+		const size_t o = 3 * (size_t)(perm ? perm[idx] : idx);
+		pos_out3[o + 0] = p.x;
+		pos_out3[o + 1] = p.y;
+		pos_out3[o + 2] = p.z;
 	}
 }
 
@@ -1265,45 +1295,40 @@ __global__ void __launch_bounds__(kBlock) k_sc_scatter(int n, const unsigned int
 	idx_sorted[pos] = i;
 }
 
-// order each bucket by particle index (makes the sort stable); thread per bucket,
-// insertion sort for short buckets, rank counting for long ones
+// order each bucket by the particles' caller indices (perm maps the internal slot to
+// it), which makes the counting sort equal to a stable sort of (key, caller index) —
+// the reference's order; thread per bucket, insertion sort for short buckets, repeated
+// minimum selection for long ones
 __global__ void __launch_bounds__(kBlock) k_sc_order(int buckets, const int* __restrict__ start,
-	int* __restrict__ idx_sorted)
+	int* __restrict__ idx_sorted, const int* __restrict__ perm)
 {
 	const int b = blockIdx.x * blockDim.x + threadIdx.x;
 	if (b >= buckets) return;
 	const int s = start[b], e = start[b + 1];
 	const int len = e - s;
 	if (len <= 1) return;
-	if (len <= 64) {
-		int v[64];
-		for (int t = 0; t < len; ++t) v[t] = idx_sorted[s + t];
+	if (len <= 32) {
+		int v[32], key[32];
+		for (int t = 0; t < len; ++t) { v[t] = idx_sorted[s + t]; key[t] = perm ? perm[v[t]] : v[t]; }
 		for (int t = 1; t < len; ++t) {
-			const int x = v[t];
+			const int x = v[t], kx = key[t];
 			int u = t - 1;
-			while (u >= 0 && v[u] > x) { v[u + 1] = v[u]; --u; }
+			while (u >= 0 && key[u] > kx) { v[u + 1] = v[u]; key[u + 1] = key[u]; --u; }
 			v[u + 1] = x;
+			key[u + 1] = kx;
 		}
 		for (int t = 0; t < len; ++t) idx_sorted[s + t] = v[t];
 		return;
 	}
-	// long bucket: selection by rank into place, done in rounds of the minimum
-	// remaining value (bounded by len iterations, each O(len))
-	int last = -1;
-	for (int t = 0; t < len; ++t) {
-		int best = INT_MAX;
-		for (int u = t; u < len; ++u) {
-			const int x = idx_sorted[s + u];
-			if (x > last && x < best) best = x;
+	for (int t = 0; t < len - 1; ++t) {
+		int best = t, bk = perm ? perm[idx_sorted[s + t]] : idx_sorted[s + t];
+		for (int u = t + 1; u < len; ++u) {
+			const int k = perm ? perm[idx_sorted[s + u]] : idx_sorted[s + u];
+			if (k < bk) { bk = k; best = u; }
 		}
-		for (int u = t; u < len; ++u)
-			if (idx_sorted[s + u] == best) {
-				const int tmp = idx_sorted[s + t];
-				idx_sorted[s + t] = best;
-				idx_sorted[s + u] = tmp;
-				break;
-			}
-		last = best;
+		const int tmp = idx_sorted[s + t];
+		idx_sorted[s + t] = idx_sorted[s + best];
+		idx_sorted[s + best] = tmp;
 	}
 }
 
@@ -1355,6 +1380,112 @@ __global__ void __launch_bounds__(kBlock) k_sc_build(int n, const StepParams* __
 						int code = j;
 						if (cross) {
 							const float4 xj = X[j];
+							const float ex = x.x - xj.x, ey = x.y - xj.y, ez = x.z - xj.z;
+							const float dist_x = sqrtf(ex * ex + ey * ey + ez * ez);
+							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
+							const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
+							if (!(dist_x < search + rel)) continue;
+							if (!(q2 >= cross_excl2)) continue;
+							pr = dist_x - rel;
+							if (rel > fast_rel) code = -(j + 1);
+						}
+						else {
+							const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+							const float d2 = ex * ex + ey * ey + ez * ez;
+							if (!(d2 < search2)) continue;
+							if (!(q2 >= excl2)) continue;
+							pr = sqrtf(d2);
+						}
+						const int tr = cross ? 0 : 1;
+						if (cnt < kSelfColMax) {
+							out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
+						}
+						else {
+							int worst = 0;
+							for (int m = 1; m < kSelfColMax; ++m)
+								if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
+							if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
+								out[worst] = code; prio[worst] = pr; tier[worst] = tr;
+							}
+							++over;
+						}
+					}
+				}
+	}
+	counts[i] = cnt;
+	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
+	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
+}
+
+// Cell-ordered copies of what the candidate scan reads per neighbour: predicted
+// position + object id, rest position + particle index, start position.  One pass,
+// 48 B per particle written; the scan then reads each cell's particles contiguously.
+__global__ void __launch_bounds__(kBlock) k_sc_pack(int n, const int* __restrict__ idx_sorted,
+	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
+	const int* __restrict__ obj_id, float4* __restrict__ sp, float4* __restrict__ sr, float4* __restrict__ sx)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const int j = idx_sorted[t];
+	const float4 p = Pp[j], q = rest[j], x = X[j];
+	sp[t] = make_float4(p.x, p.y, p.z, __int_as_float(obj_id[j]));
+	sr[t] = make_float4(q.x, q.y, q.z, __int_as_float(j));
+	sx[t] = x;
+}
+
+// Candidate lists with particles visited in cell order (thread t builds the list of
+// particle idx_sorted[t], so a warp scans overlapping cells) and neighbours read from
+// the cell-ordered copies.  Same cells, same visiting order and same tests as
+// k_sc_build / selfColBuildKernel (forward.cu:7079-7180), hence identical lists.
+__global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
+	const int* __restrict__ idx_sorted, const int* __restrict__ start, unsigned int mask,
+	const int* __restrict__ obj_id, const float4* __restrict__ sp, const float4* __restrict__ sr,
+	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
+	int* __restrict__ counts)
+{
+	const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t0 >= n) return;
+	const int i = idx_sorted[t0];
+	const float4 x = X[i], p = Pp[i];
+	int cnt = 0, over = 0;
+	if (isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+		const float inv_cell = ctr->sc_inv_cell;
+		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
+		const float fast_rel = P->sc_fast_rel;
+		const int within = P->sc_within;
+		const float4 q = rest[i];
+		const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
+		const int oi = obj_id[i];
+		const float search2 = search * search;
+		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+		int* out = contacts + (size_t)i * kSelfColMax;
+		unsigned int hs[27];
+		float prio[kSelfColMax];
+		int tier[kSelfColMax];
+		int nh = 0;
+		for (int oz = -1; oz <= 1; ++oz)
+			for (int oy = -1; oy <= 1; ++oy)
+				for (int ox = -1; ox <= 1; ++ox) {
+					const unsigned int h = sc_hash(cx + ox, cy + oy, cz + oz, mask);
+					bool dup = false;
+					for (int m = 0; m < nh; ++m) if (hs[m] == h) { dup = true; break; }
+					if (dup) continue;
+					hs[nh++] = h;
+					const int s = start[h], e = start[h + 1];
+					for (int t = s; t < e; ++t) {
+						const float4 rj = sr[t];
+						const int j = __float_as_int(rj.w);
+						if (j == i) continue;
+						const float4 pj = sp[t];
+						const bool cross = __float_as_int(pj.w) != oi;
+						if (!cross && !within) continue;
+						const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
+						const float q2 = qx * qx + qy * qy + qz * qz;
+						float pr;
+						int code = j;
+						if (cross) {
+							const float4 xj = sx[t];
 							const float ex = x.x - xj.x, ey = x.y - xj.y, ez = x.z - xj.z;
 							const float dist_x = sqrtf(ex * ex + ey * ey + ez * ez);
 							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
@@ -1649,10 +1780,11 @@ __device__ __noinline__ void sym_eig3_double(double a[3][3], double ev[3], doubl
 __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4* __restrict__ rest,
 	const float4* __restrict__ cur, const int* __restrict__ off, const int* __restrict__ nbr,
 	const float* __restrict__ scales, const float* __restrict__ rots, float deform_eps, float* __restrict__ out_scale,
-	float* __restrict__ out_quat, DevCounters* __restrict__ ctr)
+	float* __restrict__ out_quat, DevCounters* __restrict__ ctr, const int* __restrict__ perm)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
+	const int o = perm ? perm[i] : i;   // output slot in the caller's order
 	const float3 s0 = make_float3(scales[3 * i], scales[3 * i + 1], scales[3 * i + 2]);
 	const float4 q0 = make_float4(rots[4 * i], rots[4 * i + 1], rots[4 * i + 2], rots[4 * i + 3]);
 	const float3 x = f3(cur[i]), x0 = f3(rest[i]);
@@ -1733,8 +1865,8 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 	}
 	const double tr = deformed ? ((double)Sigma.m[0][0] + Sigma.m[1][1] + Sigma.m[2][2]) : 0.0;
 	if (!deformed || !(tr > 0.0)) {
-		out_scale[3 * i + 0] = s0.x; out_scale[3 * i + 1] = s0.y; out_scale[3 * i + 2] = s0.z;
-		out_quat[4 * i + 0] = q0.x; out_quat[4 * i + 1] = q0.y; out_quat[4 * i + 2] = q0.z; out_quat[4 * i + 3] = q0.w;
+		out_scale[3 * o + 0] = s0.x; out_scale[3 * o + 1] = s0.y; out_scale[3 * o + 2] = s0.z;
+		out_quat[4 * o + 0] = q0.x; out_quat[4 * o + 1] = q0.y; out_quat[4 * o + 2] = q0.z; out_quat[4 * o + 3] = q0.w;
 		atomicAdd(&ctr->shapes_kept, 1u);
 		return;
 	}
@@ -1755,7 +1887,7 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 	}
 	const double s_floor = 1e-3 * (double)fmaxf(s0.x, fmaxf(s0.y, s0.z));
 #pragma unroll
-	for (int k = 0; k < 3; ++k) out_scale[3 * i + k] = (float)fmax(sqrt(fmax(ev[k], 0.0) / inv), s_floor);
+	for (int k = 0; k < 3; ++k) out_scale[3 * o + k] = (float)fmax(sqrt(fmax(ev[k], 0.0) / inv), s_floor);
 	double w, qxv, qyv, qzv;
 	const double t = E[0][0] + E[1][1] + E[2][2];
 	if (t > 0.0) {
@@ -1775,10 +1907,10 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 		w = (E[1][0] - E[0][1]) / s; qxv = (E[0][2] + E[2][0]) / s; qyv = (E[1][2] + E[2][1]) / s; qzv = 0.25 * s;
 	}
 	const double qn = sqrt(w * w + qxv * qxv + qyv * qyv + qzv * qzv);
-	out_quat[4 * i + 0] = (float)(w / qn);
-	out_quat[4 * i + 1] = (float)(qxv / qn);
-	out_quat[4 * i + 2] = (float)(qyv / qn);
-	out_quat[4 * i + 3] = (float)(qzv / qn);
+	out_quat[4 * o + 0] = (float)(w / qn);
+	out_quat[4 * o + 1] = (float)(qxv / qn);
+	out_quat[4 * o + 2] = (float)(qyv / qn);
+	out_quat[4 * o + 3] = (float)(qzv / qn);
 	atomicAdd(&ctr->shapes_deformed, 1u);
 }
 

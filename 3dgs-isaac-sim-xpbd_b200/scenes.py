@@ -74,15 +74,23 @@ def _rot_x(angle):
 
 class Gripper:
     """A capsule (radius, half-length along local z) that pins the ``count`` Gaussians
-    nearest to ``centre`` and moves them rigidly: translation ``velocity`` per frame,
-    rotation ``twist`` radians per frame about the world x axis through its centre."""
+    nearest to ``centre`` (or, with ``pin_radius``, every Gaussian that close to its axis)
+    and moves them rigidly: translation ``velocity`` per frame, rotation ``twist`` radians
+    per frame about the world x axis through its centre."""
 
     def __init__(self, pos, centre, count=200, velocity=(0.01, 0.0, 0.0), twist=0.0,
-                 radius=0.05, half_length=0.05):
+                 radius=0.05, half_length=0.05, pin_radius=None):
         self.centre = np.asarray(centre, dtype=np.float64)
-        d2 = ((pos.astype(np.float64) - self.centre) ** 2).sum(1)
-        count = min(count, len(pos))
-        self.idx = np.sort(np.argsort(d2, kind="stable")[:count]).astype(np.int32)
+        p = pos.astype(np.float64) - self.centre
+        if pin_radius is None:
+            d2 = (p ** 2).sum(1)
+            count = min(count, len(pos))
+            self.idx = np.sort(np.argsort(d2, kind="stable")[:count]).astype(np.int32)
+        else:
+            # every Gaussian within pin_radius of the capsule's axis segment (local z)
+            z = np.clip(p[:, 2], -half_length, half_length)
+            d2 = p[:, 0] ** 2 + p[:, 1] ** 2 + (p[:, 2] - z) ** 2
+            self.idx = np.nonzero(d2 <= pin_radius * pin_radius)[0].astype(np.int32)
         self.rel = pos[self.idx].astype(np.float64) - self.centre
         self.velocity = np.asarray(velocity, dtype=np.float64)
         self.twist = float(twist)
@@ -192,12 +200,13 @@ def plain_scene_scenario(n=20000, seed=0, **kw):
 
 def large_scene_scenario(n=1_000_000, seed=0, **kw):
     """The large single-scene workload: grippers pull apart (+-0.01 x per frame) while each
-    twists 1 degree per frame about x; self-collision on (within-body pairs)."""
+    twists 1 degree per frame about x; self-collision on (within-body pairs).  Each gripper
+    pins every Gaussian inside its capsule (radius 0.05 + 10 %), so no free Gaussian starts
+    inside a collider at any scene size."""
     scene = kw.pop("scene", None) or make_scene(n, seed)
-    pins = kw.pop("pins", 200)
     deg = math.radians(1.0)
-    grippers = [Gripper(scene["pos"], (-0.9, 0.0, 0.0), pins, (-0.01, 0.0, 0.0), -deg),
-                Gripper(scene["pos"], (0.9, 0.0, 0.0), pins, (0.01, 0.0, 0.0), deg)]
+    grippers = [Gripper(scene["pos"], (-0.9, 0.0, 0.0), 0, (-0.01, 0.0, 0.0), -deg, pin_radius=0.055),
+                Gripper(scene["pos"], (0.9, 0.0, 0.0), 0, (0.01, 0.0, 0.0), deg, pin_radius=0.055)]
     kw.setdefault("self_collision", True)
     kw.setdefault("within_body", True)
     return Scenario(scene, grippers, **kw)

@@ -1,0 +1,354 @@
+"""Throughput benchmark of the XPBD Gaussian-graph step (one JSON line on rank 0).
+
+Workload (default): the large single scene — 1,000,000 Gaussians (ellipsoid, 8-NN
+graph, 64-member volume clusters, shape matching, spatial-hash self-collision), two
+capsule grippers pulling apart while twisting; one bench "step" is one 60 Hz frame =
+10 solver substeps x 4 iterations.  Metric: Gaussian-substeps per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config large|plain]
+
+value     device-resident throughput: frames enqueued through the library's async API,
+          timed with CUDA events on the engine's stream (pins/colliders re-posed per
+          substep from host, as a caller does);
+e2e       the same frames through the reference-facing C ABI (xpbd_set_colliders /
+          xpbd_set_attached / blocking xpbd_step per substep, xpbd_positions_host per frame);
+roofline  the dominant kernel's algorithmic bytes / its mean CUDA-event duration over
+          the timed region, against the measured HBM copy bandwidth;
+cpu_baseline  the CPU oracle (OpenMP, all host cores) on a bounded sample.
+
+--impl reference times the reference's CPU path.  The reference has no CPU XPBD
+solver, so this is the C restatement oracle/liboracle.so with all host threads; each
+"step" is one substep of the same workload.  Multi-GPU (torchrun): every rank runs an
+independent replica (the step has no exchange), barrier + max over ranks.
+"""
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+pkg = importlib.import_module("3dgs-isaac-sim-xpbd_b200")
+scenes = pkg.scenes
+
+METRIC = "XPBD substeps/s at 1M Gaussians (Gaussian-substeps/s)"
+UNIT = "Gaussian-substeps/s"
+SUBSTEPS = 10
+ITERS = 4
+
+
+def workload(config):
+    if config == "plain":
+        return "plain 20k: 20,000 Gaussians, 2 pinned capsule grippers, 10 substeps x 4 iterations", \
+            lambda: scenes.plain_scene_scenario(20000, 0)
+    return ("large 1M: 1,000,000 Gaussians, 8-NN graph, 64-member clusters (k=3), shape matching, "
+            "spatial-hash self-collision, 2 twisting grippers, 10 substeps x 4 iterations"), \
+        lambda: scenes.large_scene_scenario(1_000_000, 0)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def bind_ext(L):
+    L.xpbd_b200_set_stream.argtypes = [ctypes.c_void_p]
+    L.xpbd_b200_step_async.argtypes = [ctypes.c_int]
+    L.xpbd_b200_set_profiling.argtypes = [ctypes.c_int]
+    L.xpbd_b200_stage_times.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    L.xpbd_b200_stage_name.restype = ctypes.c_char_p
+    L.xpbd_b200_stage_name.argtypes = [ctypes.c_int]
+    L.xpbd_b200_launch_count.restype = ctypes.c_longlong
+    L.xpbd_b200_sizes.argtypes = [ctypes.c_void_p]
+
+
+def run_frames(solver, scen, frames, blocking):
+    """Advance `frames` frames; pins and colliders re-posed before every substep."""
+    for _ in range(frames):
+        for _ in range(SUBSTEPS):
+            t = (scen.k + 1) / scen.substeps
+            types, poses, dims = scen.colliders(t)
+            solver.set_colliders(types, poses, dims, 0.0, 0.0)
+            if scen.k > 0:                             # pins need one step first (xpbd_capi.cu:169)
+                idx, pos = scen.pins(t)
+                solver.set_attached(idx, pos, 1.0)
+            if blocking:
+                solver.step()
+            else:
+                solver.lib.xpbd_b200_step_async(1)
+            scen.k += 1
+
+
+def algorithmic_bytes(stage, sizes, n):
+    """Bytes one launch of `stage` must move, counting each array of the data model once
+    (FP32/int32): the per-Gaussian figures of the measurement plan."""
+    m_dir = sizes[1] / n           # mean directed degree
+    members = sizes[2] / n         # mean cluster members (leader excluded)
+    rev = sizes[3] / n             # mean reverse-list length
+    per = {
+        "distance": 28 + 20 * m_dir,
+        "volume_solve": 4 * members + 56,
+        "volume_gather": 4 * rev + 80,
+        "shape": 48 + 4 * m_dir,
+        "project": 28,
+        "predict": 52,
+        "velocity": 48,
+    }.get(stage)
+    return None if per is None else per * n
+
+
+def bench_b200(args, rank, world):
+    import torch
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    name, make = workload(args.config)
+    scen = make()
+    n = scen.n
+    x = pkg.XPBD()
+    bind_ext(x.lib)
+    stream = torch.cuda.Stream()
+    x.lib.xpbd_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    scen.setup(x)
+    run_frames(x, scen, 1, blocking=True)            # upload + build (not timed)
+    with torch.cuda.stream(stream):
+        run_frames(x, scen, args.warmup, blocking=False)
+        torch.cuda.synchronize()
+        sizes = np.zeros(10, np.int64)
+        x.lib.xpbd_b200_sizes(sizes.ctypes.data)
+
+        # ---- timed region: device-resident throughput, per-kernel events on ----
+        x.lib.xpbd_b200_reset_stage_times()
+        x.lib.xpbd_b200_set_profiling(1)
+        launches0 = x.lib.xpbd_b200_launch_count()
+        clocks = Clocks(torch.cuda.current_device())
+        clocks.start()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        run_frames(x, scen, args.steps, blocking=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        clk = clocks.stop()
+        ms = ev0.elapsed_time(ev1)
+        launches = x.lib.xpbd_b200_launch_count() - launches0
+        x.lib.xpbd_b200_set_profiling(0)
+        st_ms = np.zeros(16)
+        st_cnt = np.zeros(16, np.int64)
+        k = x.lib.xpbd_b200_stage_times(st_ms.ctypes.data, st_cnt.ctypes.data, 16)
+        stages = {x.lib.xpbd_b200_stage_name(s).decode(): (float(st_ms[s]), int(st_cnt[s])) for s in range(k)
+                  if st_cnt[s]}
+
+    # ---- e2e: reference ABI, host buffers, blocking step, positions read per frame ----
+    x.lib.xpbd_b200_set_stream(None)
+    e2e_frames = max(1, min(args.steps, 5))
+    pos_bytes = n * 3 * 4
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_frames):
+        run_frames(x, scen, 1, blocking=True)
+        x.positions()
+    e2e_s = time.perf_counter() - t0
+    h2d = SUBSTEPS * (len(scen.pins(0.0)[0]) * 16 + len(scen.grippers) * 64)
+
+    if world > 1:
+        t = torch.tensor([ms, e2e_s * 1e3], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    else:
+        e2e_ms = e2e_s * 1e3
+    if rank != 0:
+        x.destroy()
+        return None
+
+    units = n * SUBSTEPS * args.steps * world
+    value = units / (ms / 1e3)
+    dom = max(stages.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_cnt) = dom
+    peak, peak_kind = peaks()
+    algo = algorithmic_bytes(dom_name, sizes, n)
+    achieved = (algo / (dom_ms / dom_cnt / 1e3) / 1e9) if algo else None
+    traffic = traffic_estimate(dom_name, n)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid scene; no public dataset)",
+        "config": {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": ITERS,
+                   "graph_edges_directed": int(sizes[1]), "cluster_members": int(sizes[2]),
+                   "hash_table": int(sizes[8]), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (working set > 2 GB per replica)"},
+        "e2e": {"value": n * SUBSTEPS * e2e_frames * world / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": pos_bytes, "frames": e2e_frames},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
+                     "mean_launch_ms": dom_ms / dom_cnt},
+        "stages_ms_per_step": {k2: v[0] / args.steps for k2, v in sorted(stages.items(), key=lambda kv: -kv[1][0])},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, scen_maker=make)
+    x.destroy()
+    return line
+
+
+def traffic_estimate(stage, n):
+    """DRAM bytes per launch from the committed ncu summary of this kernel, scaled to n."""
+    path = os.path.join(ROOT, "profiles", "dram_per_gaussian.json")
+    if not os.path.isfile(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    per = d.get(stage)
+    return None if per is None else per * n
+
+
+def cpu_baseline(args, scen_maker, substeps=None):
+    """The oracle on the host cores: the same workload, a bounded number of substeps."""
+    lib = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.isfile(lib):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    o = pkg.bridge.XPBD(lib)
+    o.lib.oracle_get_threads.restype = ctypes.c_int
+    scen = scen_maker()
+    scen.setup(o)
+    scen.advance(o, 1)                          # build (not timed)
+    k = substeps or args.cpu_substeps
+    t0 = time.perf_counter()
+    scen.advance(o, k)
+    dt = time.perf_counter() - t0
+    cores = int(o.lib.oracle_get_threads())
+    o.destroy()
+    return {"value": scen.n * k / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{k} substeps of the same {scen.n}-Gaussian workload after its upload"}
+
+
+def bench_reference(args, rank, world):
+    if rank != 0:
+        return None
+    name, make = workload(args.config)
+    steps = args.steps
+    warm = args.warmup
+    lib = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.isfile(lib):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    o = pkg.bridge.XPBD(lib)
+    o.lib.oracle_get_threads.restype = ctypes.c_int
+    scen = make()
+    scen.setup(o)
+    scen.advance(o, 1 + min(warm, 1))
+    t0 = time.perf_counter()
+    scen.advance(o, steps)
+    dt = time.perf_counter() - t0
+    cores = int(o.lib.oracle_get_threads())
+    value = scen.n * steps / dt
+    o.destroy()
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid scene)",
+            "config": {"workload": name, "step": "one substep (CPU sample of the workload)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{steps} substeps of the {scen.n}-Gaussian workload"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="large", choices=["large", "plain"])
+    ap.add_argument("--cpu-substeps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "b200":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() and args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        line = bench_reference(args, rank, world) if args.impl == "reference" else bench_b200(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1 and args.impl == "b200":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -119,10 +119,15 @@ XPBD_API int xpbd_b200_sync(void);
 /* Gauss-Seidel colour sweeps for the distance / volume constraints instead of the
  * Jacobi default (the reference's forward.cu:3780-3812 toggles). */
 XPBD_API void xpbd_b200_set_gs(int distance, int volume);
-/* Volume kernel shape: 0 auto (warp per cluster when mean members >= 40), 1 thread, 2 warp. */
+/* Volume kernel shape: 0 auto (8 lanes per cluster / node when clusters average >= 40
+ * members, else 4), 1 one thread per cluster (the reference's thread kernels' summation
+ * order), 2 one warp per cluster (its warp kernels' order). */
 XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
 /* 1 (default): replay each step from a captured CUDA graph; 0: launch kernel by kernel. */
 XPBD_API void xpbd_b200_set_graph(int enabled);
+/* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
+ * ABI; results identical); 0: caller order.  Takes effect at the next upload. */
+XPBD_API void xpbd_b200_set_reorder(int enabled);
 /* Per-kernel CUDA-event timing of subsequent steps (launches then go kernel by kernel). */
 XPBD_API int xpbd_b200_set_profiling(int enabled);
 /* Accumulated per-stage milliseconds and launch counts; returns the number of stages. */

@@ -150,6 +150,26 @@ def test_volume_kernel_shapes_agree_with_oracle(lib, mode):
     assert H.max_err_over_diag(out["b200"], out["oracle"], diag) < H.TOL_100STEP
 
 
+def test_internal_order_does_not_change_results(lib):
+    """Morton order inside the engine reproduces the caller-order run bit for bit: every
+    list (neighbours, members, clusters per node, hash-cell order) keeps its order."""
+    import ctypes
+    lib.lib.xpbd_b200_set_reorder.argtypes = [ctypes.c_int]
+    out = []
+    for reorder in (1, 0):
+        lib.lib.xpbd_b200_set_reorder(reorder)
+        s = H.scenario_for("selfcol_blobs")
+        s.setup(lib)
+        s.advance(lib, 30)
+        sc_, q_, _ = lib.shapes(1e-3)
+        out.append((lib.positions(), sc_, q_, lib.ints("sc_idx_sorted"), lib.ints("sc_count"),
+                    lib.ints("sc_contact")))
+    lib.lib.xpbd_b200_set_reorder(1)
+    for a, b in zip(out[0][:5], out[1][:5]):
+        np.testing.assert_array_equal(a, b)
+    assert H.contacts_equal(out[0][4], out[0][5], out[1][4], out[1][5])
+
+
 def test_graph_replay_matches_eager(lib):
     out = []
     for graph in (1, 0):
