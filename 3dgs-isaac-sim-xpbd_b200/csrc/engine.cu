@@ -93,6 +93,7 @@ struct Settings {
 	float kin_margin = 0.0f, kin_friction = 0.0f;
 	bool use_graph = true;
 	bool reorder = true;             // Morton order inside the engine (results unchanged)
+	int lanes_a = 0, lanes_b = 0;    // volume kernel lanes per cluster / node (0 = automatic)
 };
 static Settings S;
 
@@ -120,6 +121,7 @@ public:
 	bool coloring_built = false;
 	std::vector<int> obj_id;
 	int num_objects = 0;
+	bool single_object = true;
 	float spacing = 0.0f;
 	int sc_table = 0;
 
@@ -372,6 +374,7 @@ public:
 		CK(cudaMemsetAsync(rec.p, 0, rec.bytes(), stream));
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		build_components(graph, 50, obj_id, num_objects);
+		single_object = std::all_of(obj_id.begin(), obj_id.end(), [&](int v) { return v == obj_id[0]; });
 		{
 			const auto oi = to_internal(obj_id.data(), 1);
 			CK(d_obj_id.alloc(n));
@@ -508,6 +511,7 @@ public:
 		P.sc_fast_rel = S.sc_fast_rel * dc;
 		P.sc_search_plus16dc = search + 16.0f * dc;
 		P.sc_within = S.sc_within ? 1 : 0;
+		P.sc_single_object = single_object ? 1 : 0;
 	}
 
 	bool use_warp() const
@@ -574,12 +578,14 @@ public:
 	{
 		if (S.warp_mode == 2) return 32;
 		if (S.warp_mode == 1) return 0;
+		if (S.lanes_a > 0) return S.lanes_a;
 		return clusters.avg_members >= 40.0f ? 8 : 4;
 	}
 	int gather_lanes() const
 	{
 		if (S.warp_mode == 2) return 32;
 		if (S.warp_mode == 1) return 0;
+		if (S.lanes_b > 0) return S.lanes_b;
 		const double h = clusters.rev_off.empty() ? 0.0 : (double)clusters.rev_off[n] / std::max(n, 1);
 		return h >= 40.0 ? 8 : 4;
 	}
@@ -656,13 +662,17 @@ public:
 							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
 							lam_vol.p, rec.p, rl);
 					else if (la == 8)
-						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_group<8, 8>, N, dp, cpin,
-							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
-							lam_vol.p, rec.p, rl);
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_slots<8, 8, true>, N, dp,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 4)
-						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_group<4, 4>, N, dp, cpin,
-							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
-							lam_vol.p, rec.p, rl);
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_slots<4, 16, false>, N, dp,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+					else if (la == 2)
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 2), B, dev::k_volume_solve_slots<2, 32, false>, N, dp,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else
 						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
 							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
@@ -1185,6 +1195,13 @@ XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { S.warp_mode = std::max(
 XPBD_API void xpbd_b200_set_graph(int enabled) { S.use_graph = enabled != 0; }
 
 XPBD_API void xpbd_b200_set_reorder(int enabled) { S.reorder = enabled != 0; }
+
+XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes)
+{
+	auto ok = [](int v) { return v == 0 || v == 2 || v == 4 || v == 8 || v == 32; };
+	S.lanes_a = ok(solve_lanes) ? solve_lanes : 0;
+	S.lanes_b = (ok(gather_lanes) && gather_lanes != 2) ? gather_lanes : 0;
+}
 
 XPBD_API int xpbd_b200_set_profiling(int enabled)
 {

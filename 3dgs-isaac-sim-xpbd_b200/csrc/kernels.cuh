@@ -464,6 +464,136 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_group(int n, const Step
 	store_record(rec, idx, c, dl * gs, Sinv);
 }
 
+// Kernel A with static register slots: lane sl of an S-lane group owns members
+// sl + t*S (t < NS) in fixed registers (index, and the position when CP), so the three
+// passes over a cluster need no dynamic indexing; members past S*NS are streamed from
+// memory in each pass.  Same per-lane order and arithmetic as k_volume_solve_group.
+template <int S, int NS, bool CP>
+__global__ void __launch_bounds__(kBlock) k_volume_solve_slots(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, int read_lam)
+{
+	const int sl = threadIdx.x & (S - 1);
+	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const bool in_range = idx < n;
+	bool valid = in_range && mat_type[idx] == 0;
+	int off = 0, cnt = 0;
+	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (valid) {
+		off = voff[idx];
+		cnt = voff[idx + 1] - off;
+		p4 = ld4(pin, idx);
+	}
+	const float3 pi = f3(p4);
+	int jj[NS];
+	float4 qq[CP ? NS : 1];
+	int ucnt = 0;
+	float3 psum = make_float3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+	for (int t = 0; t < NS; ++t) {
+		const int k = sl + t * S;
+		int j = -1;
+		if (k < cnt) {
+			j = __ldg(vidx + off + k);
+			if (j >= n) j = -1;
+		}
+		jj[t] = j;
+	}
+#pragma unroll
+	for (int t = 0; t < NS; ++t) {
+		if (jj[t] >= 0) {
+			const float4 q = ld4(pin, jj[t]);
+			if (CP) qq[t] = q;
+			psum = add3(psum, f3(q));
+			++ucnt;
+		}
+	}
+	for (int k = sl + NS * S; k < cnt; k += S) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		psum = add3(psum, f3(ld4(pin, j)));
+		++ucnt;
+	}
+	const float sx = group_sum<S>(psum.x), sy = group_sum<S>(psum.y), sz = group_sum<S>(psum.z);
+	const int used = (int)(group_sum<S>((float)ucnt) + 0.5f);
+	valid = valid && used >= 3;
+	const float inv_n = 1.0f / (float)(used + 1);
+	const float3 c = make_float3((sx + pi.x) * inv_n, (sy + pi.y) * inv_n, (sz + pi.z) * inv_n);
+	float a00 = 0.f, a11 = 0.f, a22 = 0.f, a01 = 0.f, a02 = 0.f, a12 = 0.f;
+#pragma unroll
+	for (int t = 0; t < NS; ++t) {
+		if (jj[t] >= 0) {
+			const float4 q = CP ? qq[t] : ld4(pin, jj[t]);
+			const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+			a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+			a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+		}
+	}
+	for (int k = sl + NS * S; k < cnt; k += S) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		const float3 q = f3(ld4(pin, j));
+		const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+	}
+	if (sl == 0) {
+		const float dx = pi.x - c.x, dy = pi.y - c.y, dz = pi.z - c.z;
+		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+	}
+	M3 Sm;
+	Sm.m[0][0] = group_sum<S>(a00) * inv_n;
+	Sm.m[1][1] = group_sum<S>(a11) * inv_n;
+	Sm.m[2][2] = group_sum<S>(a22) * inv_n;
+	const float s01 = group_sum<S>(a01) * inv_n, s02 = group_sum<S>(a02) * inv_n, s12 = group_sum<S>(a12) * inv_n;
+	Sm.m[0][1] = Sm.m[1][0] = s01;
+	Sm.m[0][2] = Sm.m[2][0] = s02;
+	Sm.m[1][2] = Sm.m[2][1] = s12;
+	float J = 1.0f, C = 0.0f;
+	M3 Sinv;
+	m3_zero(Sinv);
+	if (valid) valid = cluster_j_sinv(Sm, __ldg(det_rest + idx), J, C, Sinv);
+	const float gs = J * inv_n;
+	const float ims = P->inv_mass_scale;
+	float dsum = 0.0f;
+	if (valid) {
+#pragma unroll
+		for (int t = 0; t < NS; ++t) {
+			if (jj[t] >= 0) {
+				const float4 q = CP ? qq[t] : ld4(pin, jj[t]);
+				const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+				dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+			}
+		}
+		for (int k = sl + NS * S; k < cnt; k += S) {
+			const int j = __ldg(vidx + off + k);
+			if (j < 0 || j >= n) continue;
+			const float4 q = ld4(pin, j);
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+			dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+		if (sl == 0) {
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(pi.x - c.x, pi.y - c.y, pi.z - c.z)), gs);
+			dsum += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+	}
+	const float denom = group_sum<S>(dsum);
+	if (sl != 0 || !in_range) return;
+	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	lam_vol[idx] = lam + dl;
+	store_record(rec, idx, c, dl * gs, Sinv);
+}
+
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
 __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
@@ -798,7 +928,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_rest(int n, const float4* __r
 // (shapeMatchRotationDouble, forward.cu:5991-6086) or the float32 path
 // (forward.cu:6238-6319); XPBD pull toward the goal (forward.cu:4972-4988).
 // ---------------------------------------------------------------------------
-__device__ __noinline__ bool shape_rotation_double(const M3& A, M3& Rout)
+__device__ __forceinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 {
 	double a[3][3];
 #pragma unroll
@@ -819,7 +949,8 @@ __device__ __noinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 		for (int k = 0; k < 3; ++k) {
 			const int pk = (k == 2) ? 1 : 0, qk = (k == 0) ? 1 : 2;
 			const double off = fabs(m[pk][qk]);
-			if (off > 1e-12 * sqrt(fabs(m[pk][pk] * m[qk][qk])) + 1e-300) done = false;
+			// off > 1e-12 sqrt(|a_pp a_qq|) + 1e-300, compared in squares (no square root)
+			if (off > 1e-300 && off * off > 1e-24 * fabs(m[pk][pk] * m[qk][qk])) done = false;
 			if (off > max_off) { max_off = off; p = pk; q = qk; }
 		}
 		if (done) break;
@@ -1428,8 +1559,8 @@ __global__ void __launch_bounds__(kBlock) k_sc_pack(int n, const int* __restrict
 	if (t >= n) return;
 	const int j = idx_sorted[t];
 	const float4 p = Pp[j], q = rest[j], x = X[j];
-	sp[t] = make_float4(p.x, p.y, p.z, __int_as_float(obj_id[j]));
-	sr[t] = make_float4(q.x, q.y, q.z, __int_as_float(j));
+	sp[t] = make_float4(p.x, p.y, p.z, __int_as_float(j));
+	sr[t] = make_float4(q.x, q.y, q.z, __int_as_float(obj_id[j]));
 	sx[t] = x;
 }
 
@@ -1454,6 +1585,9 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
 		const float fast_rel = P->sc_fast_rel;
 		const int within = P->sc_within;
+		// when every particle carries the same object id there are no cross-object pairs,
+		// and a same-object neighbour outside the search radius is rejected right away
+		const bool single_object = P->sc_single_object != 0;
 		const float4 q = rest[i];
 		const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
 		const int oi = obj_id[i];
@@ -1474,11 +1608,17 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 					hs[nh++] = h;
 					const int s = start[h], e = start[h + 1];
 					for (int t = s; t < e; ++t) {
-						const float4 rj = sr[t];
-						const int j = __float_as_int(rj.w);
-						if (j == i) continue;
+						// predicted position + index first: most neighbours fail the distance
+						// test, so the rest position / object id is read only for the others
 						const float4 pj = sp[t];
-						const bool cross = __float_as_int(pj.w) != oi;
+						const int j = __float_as_int(pj.w);
+						if (j == i) continue;
+						const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+						const float d2 = ex * ex + ey * ey + ez * ez;
+						const bool near_same = d2 < search2;
+						if (!near_same && single_object) continue;
+						const float4 rj = sr[t];
+						const bool cross = __float_as_int(rj.w) != oi;
 						if (!cross && !within) continue;
 						const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
 						const float q2 = qx * qx + qy * qy + qz * qz;
@@ -1486,8 +1626,8 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 						int code = j;
 						if (cross) {
 							const float4 xj = sx[t];
-							const float ex = x.x - xj.x, ey = x.y - xj.y, ez = x.z - xj.z;
-							const float dist_x = sqrtf(ex * ex + ey * ey + ez * ez);
+							const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
+							const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
 							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
 							const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
 							if (!(dist_x < search + rel)) continue;
@@ -1496,9 +1636,7 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 							if (rel > fast_rel) code = -(j + 1);
 						}
 						else {
-							const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-							const float d2 = ex * ex + ey * ey + ez * ez;
-							if (!(d2 < search2)) continue;
+							if (!near_same) continue;
 							if (!(q2 >= excl2)) continue;
 							pr = sqrtf(d2);
 						}

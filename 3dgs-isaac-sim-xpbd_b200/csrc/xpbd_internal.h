@@ -57,7 +57,8 @@ struct StepParams {
 	float kin_margin, kin_friction;
 	float sc_dc, sc_search, sc_excl2, sc_cross_excl2, sc_fast_rel, sc_search_plus16dc;
 	int sc_within;
-	int pad[3];
+	int sc_single_object;           // every particle has the same object id
+	int pad[2];
 	KinCollider kin[kMaxColliders];
 };
 
