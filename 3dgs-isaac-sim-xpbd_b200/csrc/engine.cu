@@ -579,15 +579,14 @@ public:
 		if (S.warp_mode == 2) return 32;
 		if (S.warp_mode == 1) return 0;
 		if (S.lanes_a > 0) return S.lanes_a;
-		return clusters.avg_members >= 40.0f ? 8 : 4;
+		return 4;   // measured best on B200 for 10-64 members (sweep of 2/4/8/32)
 	}
 	int gather_lanes() const
 	{
 		if (S.warp_mode == 2) return 32;
 		if (S.warp_mode == 1) return 0;
 		if (S.lanes_b > 0) return S.lanes_b;
-		const double h = clusters.rev_off.empty() ? 0.0 : (double)clusters.rev_off[n] / std::max(n, 1);
-		return h >= 40.0 ? 8 : 4;
+		return 4;
 	}
 
 	// one step's kernel sequence (the body of runXPBDSimulation)

@@ -119,8 +119,8 @@ XPBD_API int xpbd_b200_sync(void);
 /* Gauss-Seidel colour sweeps for the distance / volume constraints instead of the
  * Jacobi default (the reference's forward.cu:3780-3812 toggles). */
 XPBD_API void xpbd_b200_set_gs(int distance, int volume);
-/* Volume kernel shape: 0 auto (8 lanes per cluster / node when clusters average >= 40
- * members, else 4), 1 one thread per cluster (the reference's thread kernels' summation
+/* Volume kernel shape: 0 auto (4 lanes per cluster / node, or xpbd_b200_set_volume_lanes),
+ * 1 one thread per cluster (the reference's thread kernels' summation
  * order), 2 one warp per cluster (its warp kernels' order). */
 XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
 /* Lanes per cluster for the volume solve (2, 4, 8, 32) and per node for the volume
