@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1449,4 +1450,167 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	CK(cudaMemcpyAsync(E.pos_next.p, keep_next.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaStreamSynchronize(E.stream));
 	return (int)E.h_ctr->sc_contacts;
+}
+
+// ============================================================================
+// Allocation-free self-collision candidate build
+//
+// For callers that may not allocate device memory: a host application that owns the
+// whole device heap (a simulator that hands plug-ins its buffers and forbids
+// cudaMalloc, whose implicit device synchronisation would stall its frame), or code
+// running where allocation is not allowed at all.  The caller passes inputs and
+// outputs in its own device memory; every scratch buffer of the build (hash keys,
+// bucket counts and starts, the ordered index, the cell-ordered copies, counters and
+// the step constants) lives in one file-scope __device__ array sized for
+// kStaticMaxN particles, which every GPU that loads this library holds until exit.
+// ============================================================================
+namespace xpbd {
+namespace noalloc {
+
+constexpr int kStaticMaxN = 65536;
+
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+constexpr int table_for(int n)
+{
+	int t = 1024;
+	while (t < 2 * n) t <<= 1;
+	return t;
+}
+constexpr int kTable = table_for(kStaticMaxN);              // 131072
+constexpr int kBuckets = kTable + 1;                        // + sentinel bucket
+constexpr int kScanN = kBuckets + 1;
+constexpr int kScanBlocks = (kScanN + 1023) / 1024;
+// byte offsets inside the scratch array
+constexpr size_t kOffParams = 0;
+constexpr size_t kOffCtr = align256(kOffParams + sizeof(StepParams));
+constexpr size_t kOffKeys = align256(kOffCtr + sizeof(DevCounters));
+constexpr size_t kOffBucket = align256(kOffKeys + sizeof(unsigned int) * kStaticMaxN);
+constexpr size_t kOffStart = align256(kOffBucket + sizeof(int) * kScanN);
+constexpr size_t kOffCursor = align256(kOffStart + sizeof(int) * kScanN);
+constexpr size_t kOffSorted = align256(kOffCursor + sizeof(int) * kBuckets);
+constexpr size_t kOffSums = align256(kOffSorted + sizeof(int) * kStaticMaxN);
+constexpr size_t kOffObj = align256(kOffSums + sizeof(int) * (kScanBlocks + 1));
+constexpr size_t kOffSp = align256(kOffObj + sizeof(int) * kStaticMaxN);
+constexpr size_t kOffSr = align256(kOffSp + sizeof(float4) * kStaticMaxN);
+constexpr size_t kOffSx = align256(kOffSr + sizeof(float4) * kStaticMaxN);
+constexpr size_t kScratchBytes = align256(kOffSx + sizeof(float4) * kStaticMaxN);   // about 5.4 MB
+
+static __device__ __align__(256) unsigned char g_selfcol_scratch[kScratchBytes];
+
+// Device address of g_selfcol_scratch, looked up once per device with that device
+// current (the host-side symbol is only a stand-in, never a device address).
+constexpr int kMaxDevices = 64;
+static unsigned char* g_scratch_addr[kMaxDevices] = {};
+static std::mutex g_scratch_mutex;
+
+static int scratch_for_current_device(unsigned char** out)
+{
+	int dev = 0;
+	CK(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= kMaxDevices) return fail("selfcol static: device ordinal %d out of range", dev);
+	std::lock_guard<std::mutex> lock(g_scratch_mutex);
+	if (!g_scratch_addr[dev]) {
+		void* p = nullptr;
+		CK(cudaGetSymbolAddress(&p, g_selfcol_scratch));
+		g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+	}
+	*out = g_scratch_addr[dev];
+	return 0;
+}
+
+}  // namespace noalloc
+}  // namespace xpbd
+
+// Self-collision candidate lists (the once-per-step build of the solver step,
+// forward.cu:11796-11849) for n <= 65,536 particles, with no device allocation.
+//
+//   x, p, rest  device float4[n]: start positions, predicted positions, rest positions
+//               (w ignored)
+//   obj_id      device int[n] object id per particle, or NULL (one object)
+//   spacing, radius_scale, exclude_scale, within_body
+//               as for xpbd_set_self_collision; spacing is the median shortest graph
+//               edge (contact distance = radius_scale * spacing)
+//   contacts    device int[32 n] out: candidate codes, j or -(j + 1) for fast
+//               cross-object pairs, first counts[i] valid per particle
+//   counts      device int[n] out
+//   total       device int out (candidate total), or NULL
+//   stream      cudaStream_t to run on (NULL: legacy default stream)
+//
+// Returns 0 once the work is enqueued, -1 with xpbd_last_error() on bad arguments or a
+// CUDA error.  All scratch sits in one static device array per GPU, reused by every call:
+// calls that overlap on the GPU (different streams, or several host threads) race on it
+// and must be serialised by the caller.  The first call on a device looks up the array's
+// device address; make that first call outside any CUDA stream capture.
+XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const float* p, const float* rest,
+	const int* obj_id, float spacing, float radius_scale, float exclude_scale, int within_body, int* contacts,
+	int* counts, int* total, void* stream)
+{
+	using namespace xpbd::noalloc;
+	if (n <= 0 || n > kStaticMaxN)
+		return fail("xpbd_b200_selfcol_candidates_static: n = %d outside 1..%d (the static scratch limit)", n,
+			kStaticMaxN);
+	if (!x || !p || !rest || !contacts || !counts)
+		return fail("xpbd_b200_selfcol_candidates_static: null input or output pointer");
+	if (!(spacing > 0.0f) || !std::isfinite(spacing))
+		return fail("xpbd_b200_selfcol_candidates_static: spacing must be positive");
+	unsigned char* base = nullptr;
+	if (scratch_for_current_device(&base)) return -1;
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	auto* d_params = reinterpret_cast<StepParams*>(base + kOffParams);
+	auto* d_ctr = reinterpret_cast<DevCounters*>(base + kOffCtr);
+	auto* keys = reinterpret_cast<unsigned int*>(base + kOffKeys);
+	auto* bucket = reinterpret_cast<int*>(base + kOffBucket);
+	auto* start = reinterpret_cast<int*>(base + kOffStart);
+	auto* cursor = reinterpret_cast<int*>(base + kOffCursor);
+	auto* sorted = reinterpret_cast<int*>(base + kOffSorted);
+	auto* sums = reinterpret_cast<int*>(base + kOffSums);
+	auto* obj0 = reinterpret_cast<int*>(base + kOffObj);
+	auto* sp = reinterpret_cast<float4*>(base + kOffSp);
+	auto* sr = reinterpret_cast<float4*>(base + kOffSr);
+	auto* sx = reinterpret_cast<float4*>(base + kOffSx);
+	// step constants as the solver derives them (forward.cu:4532-4540, 11798-11831)
+	StepParams hp;
+	memset(&hp, 0, sizeof(hp));
+	const float rs = fminf(fmaxf(std::isfinite(radius_scale) ? radius_scale : 1.5f, 0.1f), 10.0f);
+	const float es = fminf(fmaxf(std::isfinite(exclude_scale) ? exclude_scale : 2.0f, 1.05f), 20.0f);
+	const float dc = rs * spacing;
+	const float search = 1.5f * dc;
+	const float excl = es * dc;
+	hp.sc_dc = dc;
+	hp.sc_search = search;
+	hp.sc_excl2 = excl * excl;
+	hp.sc_cross_excl2 = dc * dc;
+	hp.sc_fast_rel = 0.0f * dc;
+	hp.sc_search_plus16dc = search + 16.0f * dc;
+	hp.sc_within = within_body ? 1 : 0;
+	hp.sc_single_object = obj_id ? 0 : 1;
+	// everything the build accumulates into starts from zero on every call
+	CK(cudaMemcpyAsync(d_params, &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st));
+	CK(cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), st));
+	CK(cudaMemsetAsync(bucket, 0, sizeof(int) * kScanN, st));
+	CK(cudaMemsetAsync(cursor, 0, sizeof(int) * kBuckets, st));
+	if (!obj_id) {
+		CK(cudaMemsetAsync(obj0, 0, sizeof(int) * n, st));
+		obj_id = obj0;
+	}
+	const int table = table_for(n), buckets = table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
+	const auto* X = reinterpret_cast<const float4*>(x);
+	const auto* Pp = reinterpret_cast<const float4*>(p);
+	const auto* R = reinterpret_cast<const float4*>(rest);
+	const dim3 B(kBlock), G((n + kBlock - 1) / kBlock);
+	dev::k_sc_disp<<<G, B, 0, st>>>(n, X, Pp, d_ctr);
+	dev::k_sc_setup<<<1, 1, 0, st>>>(d_params, d_ctr);
+	dev::k_sc_keys<<<G, B, 0, st>>>(n, X, d_ctr, (unsigned)(table - 1), (unsigned)table, keys, bucket);
+	dev::k_scan_blocks<<<nb, 1024, 0, st>>>(bucket, start, scan_n, sums);
+	dev::k_scan_sums<<<1, 1024, 0, st>>>(sums, nb);
+	dev::k_scan_add<<<nb, 1024, 0, st>>>(start, scan_n, sums);
+	dev::k_sc_scatter<<<G, B, 0, st>>>(n, keys, start, cursor, sorted);
+	dev::k_sc_order<<<(buckets + kBlock - 1) / kBlock, B, 0, st>>>(buckets, start, sorted, (const int*)nullptr);
+	dev::k_sc_pack<<<G, B, 0, st>>>(n, sorted, X, Pp, R, obj_id, sp, sr, sx);
+	dev::k_sc_build_sorted<<<G, B, 0, st>>>(n, d_params, X, Pp, R, sorted, start, (unsigned)(table - 1), obj_id, sp,
+		sr, sx, d_ctr, contacts, counts);
+	if (total)
+		CK(cudaMemcpyAsync(total, &d_ctr->sc_contacts, sizeof(int), cudaMemcpyDeviceToDevice, st));
+	CK(cudaGetLastError());
+	return 0;
 }

@@ -149,4 +149,19 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap);
  * (x[3n], p[3n]); returns the candidate total.  Solver state is left unchanged. */
 XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p);
 
+/* No counterpart in the reference: the once-per-step self-collision candidate build on
+ * caller-owned device buffers, for callers that cannot allocate device memory (a host
+ * application that owns the device heap and forbids cudaMalloc, whose implicit
+ * synchronisation would stall its frame).  All scratch lives in one static device array
+ * sized for n <= 65,536 particles (about 5.4 MB, held by every GPU that loads the library
+ * until exit); larger n is rejected with -1.  x, p, rest: device float4[n] (start,
+ * predicted and rest positions, w ignored); obj_id: device int[n] or NULL (one object);
+ * spacing and the scales as for xpbd_set_self_collision; outputs contacts int[32 n],
+ * counts int[n] and optionally total int[1], all device memory; runs on `stream`.
+ * Calls share the scratch and must not overlap on the GPU; the first call on a device
+ * looks up the array's address and should come before any stream capture. */
+XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const float* p, const float* rest,
+	const int* obj_id, float spacing, float radius_scale, float exclude_scale, int within_body, int* contacts,
+	int* counts, int* total, void* stream);
+
 #endif
