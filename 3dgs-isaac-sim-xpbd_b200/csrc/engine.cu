@@ -666,6 +666,10 @@ public:
 							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 4)
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4, dev::kSmemBlock), dim3(dev::kSmemBlock),
+							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx.p,
+							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
+					else if (la == 3)   // 4 lanes, positions re-read from L1 instead of shared memory
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_slots<4, 16, false>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
@@ -1198,9 +1202,9 @@ XPBD_API void xpbd_b200_set_reorder(int enabled) { S.reorder = enabled != 0; }
 
 XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes)
 {
-	auto ok = [](int v) { return v == 0 || v == 2 || v == 4 || v == 8 || v == 32; };
+	auto ok = [](int v) { return v == 0 || v == 2 || v == 3 || v == 4 || v == 8 || v == 32; };
 	S.lanes_a = ok(solve_lanes) ? solve_lanes : 0;
-	S.lanes_b = (ok(gather_lanes) && gather_lanes != 2) ? gather_lanes : 0;
+	S.lanes_b = (ok(gather_lanes) && gather_lanes != 2 && gather_lanes != 3) ? gather_lanes : 0;
 }
 
 XPBD_API int xpbd_b200_set_profiling(int enabled)

@@ -594,6 +594,143 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_slots(int n, const Step
 	store_record(rec, idx, c, dl * gs, Sinv);
 }
 
+// Kernel A with the members' positions staged in shared memory: pass 1 gathers each
+// lane's NS members once (L2/L1) and parks them in a per-thread column of shared memory
+// (slot t of thread x at [t][x], so a warp's accesses are conflict-free); the covariance
+// and denominator passes read them back from there instead of re-gathering.  Same
+// per-lane order and arithmetic as k_volume_solve_slots.  Block size must be kSmemBlock.
+constexpr int kSmemBlock = 128;
+template <int S, int NS>
+__global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, int read_lam)
+{
+	__shared__ float4 stage[NS][kSmemBlock];
+	const int tx = threadIdx.x;
+	const int sl = tx & (S - 1);
+	const int idx = (int)(((long long)blockIdx.x * kSmemBlock + tx) / S);
+	const bool in_range = idx < n;
+	bool valid = in_range && mat_type[idx] == 0;
+	int off = 0, cnt = 0;
+	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (valid) {
+		off = voff[idx];
+		cnt = voff[idx + 1] - off;
+		p4 = ld4(pin, idx);
+	}
+	const float3 pi = f3(p4);
+	unsigned int live = 0u;   // bit t: slot t holds a member
+	int ucnt = 0;
+	float3 psum = make_float3(0.0f, 0.0f, 0.0f);
+	{
+		int jj[NS];
+#pragma unroll
+		for (int t = 0; t < NS; ++t) {
+			const int k = sl + t * S;
+			int j = -1;
+			if (k < cnt) {
+				j = __ldg(vidx + off + k);
+				if (j >= n) j = -1;
+			}
+			jj[t] = j;
+		}
+#pragma unroll
+		for (int t = 0; t < NS; ++t) {
+			if (jj[t] >= 0) {
+				const float4 q = ld4(pin, jj[t]);
+				stage[t][tx] = q;
+				live |= 1u << t;
+				psum = add3(psum, f3(q));
+				++ucnt;
+			}
+		}
+	}
+	for (int k = sl + NS * S; k < cnt; k += S) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		psum = add3(psum, f3(ld4(pin, j)));
+		++ucnt;
+	}
+	const float sx = group_sum<S>(psum.x), sy = group_sum<S>(psum.y), sz = group_sum<S>(psum.z);
+	const int used = (int)(group_sum<S>((float)ucnt) + 0.5f);
+	valid = valid && used >= 3;
+	const float inv_n = 1.0f / (float)(used + 1);
+	const float3 c = make_float3((sx + pi.x) * inv_n, (sy + pi.y) * inv_n, (sz + pi.z) * inv_n);
+	float a00 = 0.f, a11 = 0.f, a22 = 0.f, a01 = 0.f, a02 = 0.f, a12 = 0.f;
+#pragma unroll
+	for (int t = 0; t < NS; ++t) {
+		if (live & (1u << t)) {
+			const float4 q = stage[t][tx];
+			const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+			a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+			a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+		}
+	}
+	for (int k = sl + NS * S; k < cnt; k += S) {
+		const int j = __ldg(vidx + off + k);
+		if (j < 0 || j >= n) continue;
+		const float3 q = f3(ld4(pin, j));
+		const float dx = q.x - c.x, dy = q.y - c.y, dz = q.z - c.z;
+		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+	}
+	if (sl == 0) {
+		const float dx = pi.x - c.x, dy = pi.y - c.y, dz = pi.z - c.z;
+		a00 += dx * dx; a11 += dy * dy; a22 += dz * dz;
+		a01 += dx * dy; a02 += dx * dz; a12 += dy * dz;
+	}
+	M3 Sm;
+	Sm.m[0][0] = group_sum<S>(a00) * inv_n;
+	Sm.m[1][1] = group_sum<S>(a11) * inv_n;
+	Sm.m[2][2] = group_sum<S>(a22) * inv_n;
+	const float s01 = group_sum<S>(a01) * inv_n, s02 = group_sum<S>(a02) * inv_n, s12 = group_sum<S>(a12) * inv_n;
+	Sm.m[0][1] = Sm.m[1][0] = s01;
+	Sm.m[0][2] = Sm.m[2][0] = s02;
+	Sm.m[1][2] = Sm.m[2][1] = s12;
+	float J = 1.0f, C = 0.0f;
+	M3 Sinv;
+	m3_zero(Sinv);
+	if (valid) valid = cluster_j_sinv(Sm, __ldg(det_rest + idx), J, C, Sinv);
+	const float gs = J * inv_n;
+	const float ims = P->inv_mass_scale;
+	float dsum = 0.0f;
+	if (valid) {
+#pragma unroll
+		for (int t = 0; t < NS; ++t) {
+			if (live & (1u << t)) {
+				const float4 q = stage[t][tx];
+				const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+				dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+			}
+		}
+		for (int k = sl + NS * S; k < cnt; k += S) {
+			const int j = __ldg(vidx + off + k);
+			if (j < 0 || j >= n) continue;
+			const float4 q = ld4(pin, j);
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(q.x - c.x, q.y - c.y, q.z - c.z)), gs);
+			dsum += (q.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+		if (sl == 0) {
+			const float3 g = mul3(m3_mulv(Sinv, make_float3(pi.x - c.x, pi.y - c.y, pi.z - c.z)), gs);
+			dsum += (p4.w * ims) * (g.x * g.x + g.y * g.y + g.z * g.z);
+		}
+	}
+	const float denom = group_sum<S>(dsum);
+	if (sl != 0 || !in_range) return;
+	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	lam_vol[idx] = lam + dl;
+	store_record(rec, idx, c, dl * gs, Sinv);
+}
+
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
 __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
