@@ -7,13 +7,15 @@ and hand-written sm_100a CUDA kernels).  This package only locates and binds it:
   (src/xpbd_bridge.py:45-271), bound to this package's library by default;
 * ``library_path()`` — the in-tree library path (the value to put in ``XPBD_DLL``
   for the reference's own bridge);
-* ``scenes`` — seeded synthetic workloads.
+* ``scenes`` — seeded synthetic workloads;
+* ``batch`` — many independent objects packed into one scene;
+* ``serve`` — continuous-batching session loop over resident engine instances.
 
 There is no CPU fallback: constructing ``XPBD`` without the built library raises.
 """
 import os
 
-from . import bridge, scenes  # noqa: F401
+from . import batch, bridge, scenes, serve  # noqa: F401
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libxpbd_b200.so"

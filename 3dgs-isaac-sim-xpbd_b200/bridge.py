@@ -77,15 +77,59 @@ def bind_abi(lib):
     return L
 
 
+class _Selected:
+    """Forwards ABI calls to a library after selecting one engine handle for the thread."""
+
+    def __init__(self, lib, handle):
+        self._lib = lib
+        self._handle = handle
+
+    def __getattr__(self, name):
+        f = getattr(self._lib, name)
+        if not callable(f) or name.startswith("xpbd_b200_engine_"):
+            return f
+        lib, handle = self._lib, self._handle
+
+        def call(*args):
+            lib.xpbd_b200_engine_select(handle)
+            return f(*args)
+        return call
+
+
+_LIBS = {}
+
+
+def load(dll_path):
+    """One ctypes handle per library path (every XPBD object shares it)."""
+    path = os.path.abspath(dll_path)
+    if path not in _LIBS:
+        if not os.path.isfile(path):
+            raise FileNotFoundError(f"XPBD library not found: {path}")
+        _LIBS[path] = bind_abi(ctypes.CDLL(path))
+    return _LIBS[path]
+
+
 class XPBD:
-    """One solver instance behind the singleton ``xpbd_*`` ABI of ``dll_path``."""
+    """One solver instance behind the ``xpbd_*`` ABI of ``dll_path``: the library's
+    singleton, or — with ``instance=True`` on a library exporting the engine-handle
+    extension — a separate resident engine of its own."""
 
     SPHERE, BOX, CAPSULE = 0, 1, 2
 
-    def __init__(self, dll_path):
-        if not os.path.isfile(dll_path):
-            raise FileNotFoundError(f"XPBD library not found: {dll_path}")
-        self.lib = bind_abi(ctypes.CDLL(dll_path))
+    def __init__(self, dll_path, instance=False):
+        lib = load(dll_path)
+        self.handle = None
+        if instance:
+            lib.xpbd_b200_engine_new.restype = ctypes.c_void_p
+            lib.xpbd_b200_engine_free.argtypes = [ctypes.c_void_p]
+            lib.xpbd_b200_engine_select.argtypes = [ctypes.c_void_p]
+            self.handle = lib.xpbd_b200_engine_new()
+            if not self.handle:
+                raise MemoryError("xpbd_b200_engine_new failed")
+            self.lib = _Selected(lib, self.handle)
+        else:
+            self.lib = lib
+        self.raw = lib
         self.path = dll_path
         self.has_attach = hasattr(self.lib, "xpbd_set_attached")
         self.has_contact_shape = hasattr(self.lib, "xpbd_set_contact_shape")
@@ -237,3 +281,10 @@ class XPBD:
     def destroy(self):
         self.lib.xpbd_destroy()
         self.n = 0
+
+    def close(self):
+        """Release a separate engine (instance=True); the singleton stays."""
+        self.destroy()
+        if self.handle:
+            self.raw.xpbd_b200_engine_free(self.handle)
+            self.handle = None

@@ -28,7 +28,7 @@
 
 namespace xpbd {
 
-static std::string g_err;
+static thread_local std::string g_err;
 
 static int fail(const char* fmt, ...)
 {
@@ -90,13 +90,17 @@ struct Settings {
 	float object_shape = 0.0f;
 	bool jstats = true;
 	KinCollider kin[kMaxColliders];
+	int kin_obj[kMaxColliders];      // object each collider acts on (-1: every Gaussian)
 	int kin_count = 0;
 	float kin_margin = 0.0f, kin_friction = 0.0f;
 	bool use_graph = true;
 	bool reorder = true;             // Morton order inside the engine (results unchanged)
 	int lanes_a = 0, lanes_b = 0;    // volume kernel lanes per cluster / node (0 = automatic)
+	Settings()
+	{
+		for (auto& v : kin_obj) v = -1;
+	}
 };
-static Settings S;
 
 enum Stage {
 	ST_PREDICT, ST_DISTANCE, ST_VOL_SOLVE, ST_VOL_GATHER, ST_VOL_GS, ST_SHAPE, ST_SC_BUILD, ST_SC_SOLVE,
@@ -107,6 +111,8 @@ static const char* kStageNames[ST_COUNT] = { "predict", "distance", "volume_solv
 
 class Engine {
 public:
+	// solver settings of this instance (the reference keeps one global set)
+	Settings S;
 	// ---- created inputs (caller order) ----
 	int n = 0, n_edges = 0;
 	std::vector<float> in_pos, in_scales, in_rots, in_opacity, in_rest, in_stiff;
@@ -501,6 +507,11 @@ public:
 		P.kin_margin = S.kin_margin;
 		P.kin_friction = S.kin_friction;
 		memcpy(P.kin, S.kin, sizeof(KinCollider) * S.kin_count);
+		P.kin_filtered = 0;
+		for (int c = 0; c < S.kin_count; ++c) {
+			P.kin[c].obj = S.kin_obj[c];
+			if (S.kin_obj[c] >= 0) P.kin_filtered = 1;
+		}
 		// selfColBuild constants (forward.cu:11798-11831), host float arithmetic
 		const float dc = S.sc_radius_scale * spacing;
 		const float search = S.sc_search_scale * dc;
@@ -706,7 +717,8 @@ public:
 					(const int*)sc_counts.p, (const DevCounters*)d_ctr, sc_dp.p);
 			if (project)
 				launch(ST_PROJECT, G, B, dev::k_project, N, (const StepParams*)d_params, pin, (const float4*)pos_curr.p,
-					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0);
+					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0,
+					(const int*)d_obj_id.p);
 		}
 		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
 			vel.p, pos_out3.p, (const int*)d_perm.p);
@@ -763,6 +775,7 @@ public:
 
 	int sync()
 	{
+		if (!stream) return 0;
 		CK(cudaStreamSynchronize(stream));
 		CK(cudaGetLastError());
 		return 0;
@@ -838,13 +851,20 @@ public:
 	}
 };
 
-static Engine* g_engine = nullptr;
+// The reference ABI addresses one solver instance.  Here it addresses the calling
+// thread's current engine: the process-wide default, or one selected with
+// xpbd_b200_engine_select (several resident scenes, one per session).
+static Engine* g_default_engine = nullptr;
+static thread_local Engine* t_current_engine = nullptr;
 
-static Engine& engine()
+static Engine* cur_engine()
 {
-	if (!g_engine) g_engine = new Engine();
-	return *g_engine;
+	if (t_current_engine) return t_current_engine;
+	if (!g_default_engine) g_default_engine = new Engine();
+	return g_default_engine;
 }
+
+static Engine& engine() { return *cur_engine(); }
 
 }  // namespace xpbd
 
@@ -881,51 +901,51 @@ XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const flo
 
 XPBD_API void xpbd_destroy(void)
 {
-	S.kin_count = 0;
-	if (g_engine) {
-		g_engine->sync();
-		g_engine->free_device();
-		g_engine->n = 0;
-		g_engine->stepped = false;
+	engine().S.kin_count = 0;
+	{
+		cur_engine()->sync();
+		cur_engine()->free_device();
+		cur_engine()->n = 0;
+		cur_engine()->stepped = false;
 	}
 }
 
-XPBD_API int xpbd_count(void) { return g_engine ? g_engine->n : 0; }
+XPBD_API int xpbd_count(void) { return cur_engine()->n; }
 
 XPBD_API void xpbd_set_solver(int iters, float dt, float underRelax, float velDamping, float stiffnessScale,
 	float invMassScale, float distCompliance, float shapeCompliance, float shapeBlend, float angleCompliance,
 	float angleBlend)
 {
 	// setXPBDParams (forward.cu:4896-4922)
-	S.iters = iters < 1 ? 1 : iters;
-	S.dt = fmaxf(1e-5f, dt);
-	S.under_relax = fmaxf(0.0f, underRelax);
-	S.vel_damping = fmaxf(0.0f, velDamping);
-	S.stiffness_scale = fmaxf(0.0f, stiffnessScale);
-	S.inv_mass_scale = fmaxf(0.0f, invMassScale);
-	S.dist_compliance = fmaxf(0.0f, distCompliance);
-	S.shape_compliance = fmaxf(0.0f, shapeCompliance);
-	S.shape_blend = fminf(fmaxf(0.0f, shapeBlend), 1.0f);
-	S.angle_compliance = fmaxf(0.0f, angleCompliance);
-	S.angle_blend = fminf(fmaxf(0.0f, angleBlend), 1.0f);
+	engine().S.iters = iters < 1 ? 1 : iters;
+	engine().S.dt = fmaxf(1e-5f, dt);
+	engine().S.under_relax = fmaxf(0.0f, underRelax);
+	engine().S.vel_damping = fmaxf(0.0f, velDamping);
+	engine().S.stiffness_scale = fmaxf(0.0f, stiffnessScale);
+	engine().S.inv_mass_scale = fmaxf(0.0f, invMassScale);
+	engine().S.dist_compliance = fmaxf(0.0f, distCompliance);
+	engine().S.shape_compliance = fmaxf(0.0f, shapeCompliance);
+	engine().S.shape_blend = fminf(fmaxf(0.0f, shapeBlend), 1.0f);
+	engine().S.angle_compliance = fmaxf(0.0f, angleCompliance);
+	engine().S.angle_blend = fminf(fmaxf(0.0f, angleBlend), 1.0f);
 }
 
 XPBD_API void xpbd_set_constraints(int distance, int shape, int angle, int volume)
 {
-	S.use_distance = distance != 0;
-	S.use_shape = shape != 0;
-	S.use_angle = angle != 0;
-	S.use_volume = volume != 0;
+	engine().S.use_distance = distance != 0;
+	engine().S.use_shape = shape != 0;
+	engine().S.use_angle = angle != 0;
+	engine().S.use_volume = volume != 0;
 }
 
 XPBD_API void xpbd_set_volume(float compliance, int ringK, int maxMembers, int leaderMinHop)
 {
 	// setVolumeParams / setVolumeRingK / setVolumeLeaderParams (forward.cu:3849, 3934-3966)
-	S.vol_compliance = compliance;
-	S.ring_k = std::max(1, std::min(8, ringK));
-	S.max_members = std::max(8, std::min(8192, maxMembers));
-	S.leader_min_hop = std::max(1, std::min(8, leaderMinHop));
-	S.topo_dirty = true;
+	engine().S.vol_compliance = compliance;
+	engine().S.ring_k = std::max(1, std::min(8, ringK));
+	engine().S.max_members = std::max(8, std::min(8192, maxMembers));
+	engine().S.leader_min_hop = std::max(1, std::min(8, leaderMinHop));
+	engine().S.topo_dirty = true;
 }
 
 XPBD_API void xpbd_set_ground(int enabled, float ux, float uy, float uz, float height, float friction,
@@ -936,23 +956,23 @@ XPBD_API void xpbd_set_ground(int enabled, float ux, float uy, float uz, float h
 	const float len = sqrtf(nx * nx + ny * ny + nz * nz);
 	if (!(len > 1e-8f) || !std::isfinite(len)) { nx = 0.0f; ny = 0.0f; nz = 1.0f; }
 	else { nx /= len; ny /= len; nz /= len; }
-	S.ground_n[0] = nx; S.ground_n[1] = ny; S.ground_n[2] = nz;
-	S.ground_on = enabled != 0;
-	S.ground_h = std::isfinite(height) ? height : 0.0f;
-	S.ground_friction = fmaxf(0.0f, friction);
-	S.ground_restitution = fminf(fmaxf(restitution, 0.0f), 1.0f);
-	S.ground_radius = fmaxf(0.0f, contactRadius);
-	S.ground_slop = fmaxf(0.0f, contactSlop);
-	S.ground_gravity = fmaxf(0.0f, gravity);
+	engine().S.ground_n[0] = nx; engine().S.ground_n[1] = ny; engine().S.ground_n[2] = nz;
+	engine().S.ground_on = enabled != 0;
+	engine().S.ground_h = std::isfinite(height) ? height : 0.0f;
+	engine().S.ground_friction = fmaxf(0.0f, friction);
+	engine().S.ground_restitution = fminf(fmaxf(restitution, 0.0f), 1.0f);
+	engine().S.ground_radius = fmaxf(0.0f, contactRadius);
+	engine().S.ground_slop = fmaxf(0.0f, contactSlop);
+	engine().S.ground_gravity = fmaxf(0.0f, gravity);
 }
 
 XPBD_API void xpbd_set_object_shape(float stiffness)
 {
 	float s = fminf(fmaxf(stiffness, 0.0f), 1.0f);
 	if (!std::isfinite(s)) s = 0.0f;
-	if (s > 0.0f && S.object_shape == 0.0f)
+	if (s > 0.0f && engine().S.object_shape == 0.0f)
 		fprintf(stderr, "[xpbd_b200] object-level shape keeping is not implemented; stiffness %.3f ignored\n", s);
-	S.object_shape = s;
+	engine().S.object_shape = s;
 }
 
 XPBD_API void xpbd_set_object_shape_gpu(int enabled) { (void)enabled; }
@@ -963,9 +983,9 @@ XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses
 	// setKinematicColliders (forward.cu:4478-4500)
 	if (count < 0) count = 0;
 	if (count > kMaxColliders) count = kMaxColliders;
-	const bool same = (count == S.kin_count);
+	const bool same = (count == engine().S.kin_count);
 	for (int c = 0; c < count; ++c) {
-		KinCollider& K = S.kin[c];
+		KinCollider& K = engine().S.kin[c];
 		const bool keep = same && K.type == types[c];
 		for (int a = 0; a < 9; ++a) K.Rp[a] = keep ? K.R[a] : poses[12 * c + a];
 		for (int a = 0; a < 3; ++a) K.tp[a] = keep ? K.t[a] : poses[12 * c + 9 + a];
@@ -973,24 +993,25 @@ XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses
 		for (int a = 0; a < 9; ++a) K.R[a] = poses[12 * c + a];
 		for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
 	}
-	S.kin_count = count;
-	S.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
-	S.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
+	for (int c = 0; c < count; ++c) engine().S.kin_obj[c] = -1;
+	engine().S.kin_count = count;
+	engine().S.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
+	engine().S.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
 }
 
 XPBD_API int xpbd_collider_stats(int* hits, float* push, float* centroid, int maxCount)
 {
 	// getKinematicColliderStats (forward.cu:4502-4519)
-	const int n = std::min(maxCount, S.kin_count);
-	if (n <= 0 || !g_engine || !g_engine->stepped) return 0;
-	if (g_engine->read_counters()) return 0;
-	const DevCounters& C = *g_engine->h_ctr;
+	const int n = std::min(maxCount, engine().S.kin_count);
+	if (n <= 0 || !cur_engine()->stepped) return 0;
+	if (cur_engine()->read_counters()) return 0;
+	const DevCounters& C = *cur_engine()->h_ctr;
 	for (int c = 0; c < n; ++c) {
 		if (hits) hits[c] = C.kin_hits[c];
 		const float* a = &C.kin_push[kColliderAcc * c];
 		for (int k = 0; k < 3; ++k) {
 			if (push) push[3 * c + k] = a[k];
-			if (centroid) centroid[3 * c + k] = (a[6] > 0.0f) ? a[3 + k] / a[6] : S.kin[c].t[k];
+			if (centroid) centroid[3 * c + k] = (a[6] > 0.0f) ? a[3 + k] / a[6] : engine().S.kin[c].t[k];
 		}
 	}
 	return n;
@@ -998,8 +1019,8 @@ XPBD_API int xpbd_collider_stats(int* hits, float* push, float* centroid, int ma
 
 XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const float* center)
 {
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_add_rigid_velocity: no step yet");
-	Engine& E = *g_engine;
+	if (!cur_engine()->stepped) return fail("xpbd_add_rigid_velocity: no step yet");
+	Engine& E = *cur_engine();
 	dev::k_add_rigid_velocity<<<Engine::blocks_for(E.n), kBlock, 0, E.stream>>>(E.n, E.pos_curr.p, E.vel.p,
 		make_float3(dv[0], dv[1], dv[2]), make_float3(dw[0], dw[1], dw[2]), make_float3(center[0], center[1], center[2]));
 	CK(cudaGetLastError());
@@ -1009,7 +1030,7 @@ XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const flo
 XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 {
 	(void)tau; (void)radiusCap;
-	if (!g_engine || g_engine->n <= 0) return fail("xpbd_set_contact_shape: call xpbd_create first");
+	if (cur_engine()->n <= 0) return fail("xpbd_set_contact_shape: call xpbd_create first");
 	if (enabled) return fail("xpbd_set_contact_shape: ellipsoid contact shapes are not implemented");
 	return 0;
 }
@@ -1017,49 +1038,49 @@ XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 XPBD_API int xpbd_set_attached(int count, const int* idx, const float* pos, float weight)
 {
 	(void)weight;
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_set_attached: no step yet");
-	if (g_engine->set_attached(count, idx, pos)) return -1;
+	if (!cur_engine()->stepped) return fail("xpbd_set_attached: no step yet");
+	if (cur_engine()->set_attached(count, idx, pos)) return -1;
 	return 0;
 }
 
 XPBD_API void xpbd_set_self_collision(int enabled, float radiusScale, float excludeScale, int withinBody)
 {
 	// setSelfCollisionParams (forward.cu:4532-4540)
-	S.sc_enabled = enabled != 0;
-	S.sc_within = withinBody != 0;
-	S.sc_radius_scale = fminf(fmaxf(std::isfinite(radiusScale) ? radiusScale : 1.5f, 0.1f), 10.0f);
-	S.sc_exclude_scale = fminf(fmaxf(std::isfinite(excludeScale) ? excludeScale : 2.0f, 1.05f), 20.0f);
+	engine().S.sc_enabled = enabled != 0;
+	engine().S.sc_within = withinBody != 0;
+	engine().S.sc_radius_scale = fminf(fmaxf(std::isfinite(radiusScale) ? radiusScale : 1.5f, 0.1f), 10.0f);
+	engine().S.sc_exclude_scale = fminf(fmaxf(std::isfinite(excludeScale) ? excludeScale : 2.0f, 1.05f), 20.0f);
 }
 
 XPBD_API void xpbd_self_collision_stats(int* out)
 {
 	out[0] = out[1] = out[2] = 0;
-	if (!g_engine || !g_engine->stepped || !S.sc_enabled) return;
-	if (g_engine->read_counters()) return;
-	out[0] = (int)g_engine->h_ctr->sc_contacts;
-	out[1] = g_engine->n;
-	out[2] = (int)g_engine->h_ctr->sc_overflow;
+	if (!cur_engine()->stepped || !engine().S.sc_enabled) return;
+	if (cur_engine()->read_counters()) return;
+	out[0] = (int)cur_engine()->h_ctr->sc_contacts;
+	out[1] = cur_engine()->n;
+	out[2] = (int)cur_engine()->h_ctr->sc_overflow;
 }
 
-XPBD_API void xpbd_set_shape_robust(int enabled) { S.shape_robust = enabled != 0; }
+XPBD_API void xpbd_set_shape_robust(int enabled) { engine().S.shape_robust = enabled != 0; }
 
 XPBD_API int xpbd_step(void)
 {
-	if (!g_engine || g_engine->n <= 0) return fail("xpbd_step: call xpbd_create first");
-	if (g_engine->step_async()) return -1;
-	return g_engine->sync();
+	if (cur_engine()->n <= 0) return fail("xpbd_step: call xpbd_create first");
+	if (cur_engine()->step_async()) return -1;
+	return cur_engine()->sync();
 }
 
 XPBD_API unsigned long long xpbd_positions_device(void)
 {
-	if (!g_engine || !g_engine->stepped) return 0ull;
-	return reinterpret_cast<unsigned long long>(g_engine->pos_out3.p);
+	if (!cur_engine()->stepped) return 0ull;
+	return reinterpret_cast<unsigned long long>(cur_engine()->pos_out3.p);
 }
 
 XPBD_API int xpbd_positions_host(float* out, int n)
 {
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_positions_host: no step yet");
-	Engine& E = *g_engine;
+	if (!cur_engine()->stepped) return fail("xpbd_positions_host: no step yet");
+	Engine& E = *cur_engine();
 	if (!out || n != E.n) return fail("xpbd_positions_host: size mismatch");
 	CK(cudaMemcpyAsync(out, E.pos_out3.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, E.stream));
 	return E.sync();
@@ -1067,8 +1088,8 @@ XPBD_API int xpbd_positions_host(float* out, int n)
 
 XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* hostQuats, int n)
 {
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_compute_shapes: no step yet");
-	Engine& E = *g_engine;
+	if (!cur_engine()->stepped) return fail("xpbd_compute_shapes: no step yet");
+	Engine& E = *cur_engine();
 	if (n != E.n) return fail("xpbd_compute_shapes: size mismatch");
 	CK(cudaMemsetAsync(&E.d_ctr->shapes_deformed, 0, sizeof(unsigned int) * 2, E.stream));
 	dev::k_deformed_shapes<<<Engine::blocks_for(n), kBlock, 0, E.stream>>>(n, E.pos_rest.p, E.pos_curr.p, E.off.p,
@@ -1085,8 +1106,8 @@ XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* host
 XPBD_API int xpbd_reset(void)
 {
 	// setAttachedParticles(0) then squashReset (forward.cu:4411-4427)
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_reset: no step yet");
-	Engine& E = *g_engine;
+	if (!cur_engine()->stepped) return fail("xpbd_reset: no step yet");
+	Engine& E = *cur_engine();
 	if (E.set_attached(0, nullptr, nullptr)) return -1;
 	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
 	return E.upload_positions(E.in_pos.data(), nullptr);
@@ -1096,8 +1117,8 @@ XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt)
 {
 	// groundLaunch (forward.cu:4551-4610): rest pose rotated about the centre of mass,
 	// rigid velocity field, inverse masses 1
-	if (!g_engine || !g_engine->stepped) return fail("xpbd_launch: no step yet");
-	Engine& E = *g_engine;
+	if (!cur_engine()->stepped) return fail("xpbd_launch: no step yet");
+	Engine& E = *cur_engine();
 	const int N = E.n;
 	double cx = 0.0, cy = 0.0, cz = 0.0;
 	for (int i = 0; i < N; ++i) { cx += E.in_pos[3 * i]; cy += E.in_pos[3 * i + 1]; cz += E.in_pos[3 * i + 2]; }
@@ -1146,10 +1167,10 @@ XPBD_API int xpbd_press_state(float* lo, float* hi, float* cur, float* mx)
 XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd)
 {
 	// setVolumeJStatsEnabled + getVolumeJVolumeWeighted (forward.cu:4081-4099)
-	S.jstats = enable != 0;
+	engine().S.jstats = enable != 0;
 	float m = 1.0f, s = 0.0f;
-	if (g_engine && g_engine->stepped && !g_engine->read_counters()) {
-		const double* a = g_engine->h_ctr->jstats;
+	if (cur_engine()->stepped && !cur_engine()->read_counters()) {
+		const double* a = cur_engine()->h_ctr->jstats;
 		if (a[0] > 0.0) {
 			const double mean = a[1] / a[0];
 			m = (float)mean;
@@ -1163,6 +1184,28 @@ XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd)
 // ============================================================================
 // extensions (no counterpart in the reference ABI)
 // ============================================================================
+XPBD_API int xpbd_b200_set_collider_objects(int count, const int* obj)
+{
+	Settings& st = engine().S;
+	if (count != st.kin_count || (count > 0 && !obj))
+		return fail("xpbd_b200_set_collider_objects: %d filters for %d colliders", count, st.kin_count);
+	for (int c = 0; c < count; ++c) st.kin_obj[c] = obj[c] < 0 ? -1 : obj[c];
+	return 0;
+}
+
+XPBD_API void* xpbd_b200_engine_new(void) { return new (std::nothrow) Engine(); }
+
+XPBD_API void xpbd_b200_engine_free(void* handle)
+{
+	Engine* e = static_cast<Engine*>(handle);
+	if (!e || e == g_default_engine) return;
+	if (t_current_engine == e) t_current_engine = nullptr;
+	e->sync();
+	delete e;
+}
+
+XPBD_API void xpbd_b200_engine_select(void* handle) { t_current_engine = static_cast<Engine*>(handle); }
+
 XPBD_API int xpbd_b200_set_stream(void* stream)
 {
 	Engine& E = engine();
@@ -1180,31 +1223,31 @@ XPBD_API int xpbd_b200_set_stream(void* stream)
 
 XPBD_API int xpbd_b200_step_async(int substeps)
 {
-	if (!g_engine || g_engine->n <= 0) return fail("xpbd_b200_step_async: call xpbd_create first");
+	if (cur_engine()->n <= 0) return fail("xpbd_b200_step_async: call xpbd_create first");
 	for (int s = 0; s < substeps; ++s)
-		if (g_engine->step_async()) return -1;
+		if (cur_engine()->step_async()) return -1;
 	return 0;
 }
 
-XPBD_API int xpbd_b200_sync(void) { return g_engine ? g_engine->sync() : 0; }
+XPBD_API int xpbd_b200_sync(void) { return cur_engine()->stream ? cur_engine()->sync() : 0; }
 
 XPBD_API void xpbd_b200_set_gs(int distance, int volume)
 {
-	S.dist_gs = distance != 0;
-	S.vol_gs = volume != 0;
+	engine().S.dist_gs = distance != 0;
+	engine().S.vol_gs = volume != 0;
 }
 
-XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { S.warp_mode = std::max(0, std::min(2, mode)); }
+XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { engine().S.warp_mode = std::max(0, std::min(2, mode)); }
 
-XPBD_API void xpbd_b200_set_graph(int enabled) { S.use_graph = enabled != 0; }
+XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled != 0; }
 
-XPBD_API void xpbd_b200_set_reorder(int enabled) { S.reorder = enabled != 0; }
+XPBD_API void xpbd_b200_set_reorder(int enabled) { engine().S.reorder = enabled != 0; }
 
 XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes)
 {
 	auto ok = [](int v) { return v == 0 || v == 2 || v == 3 || v == 4 || v == 8 || v == 32; };
-	S.lanes_a = ok(solve_lanes) ? solve_lanes : 0;
-	S.lanes_b = (ok(gather_lanes) && gather_lanes != 2 && gather_lanes != 3) ? gather_lanes : 0;
+	engine().S.lanes_a = ok(solve_lanes) ? solve_lanes : 0;
+	engine().S.lanes_b = (ok(gather_lanes) && gather_lanes != 2 && gather_lanes != 3) ? gather_lanes : 0;
 }
 
 XPBD_API int xpbd_b200_set_profiling(int enabled)
@@ -1239,15 +1282,15 @@ XPBD_API const char* xpbd_b200_stage_name(int stage)
 	return (stage >= 0 && stage < ST_COUNT) ? kStageNames[stage] : "";
 }
 
-XPBD_API long long xpbd_b200_launch_count(void) { return g_engine ? g_engine->launches : 0; }
+XPBD_API long long xpbd_b200_launch_count(void) { return cur_engine()->launches; }
 
 XPBD_API int xpbd_b200_sizes(long long* out)
 {
 	// [0] N, [1] directed edges, [2] cluster members, [3] reverse entries, [4] GS edges,
 	// [5] GS edge colours, [6] GS clusters, [7] GS cluster colours, [8] hash table, [9] candidates
 	for (int k = 0; k < 10; ++k) out[k] = 0;
-	if (!g_engine || !g_engine->built) return -1;
-	Engine& E = *g_engine;
+	if (!cur_engine()->built) return -1;
+	Engine& E = *cur_engine();
 	out[0] = E.n;
 	out[1] = E.graph.off[E.n];
 	out[2] = E.clusters.vol_off.empty() ? 0 : E.clusters.vol_off[E.n];
@@ -1303,8 +1346,8 @@ int dev_to_caller(const Engine& E, const T* src, int width, T* out, long long ca
 // row starts, sorted hash order, candidate lists).  Count only when out == NULL.
 XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap)
 {
-	if (!g_engine || !g_engine->built) return -1;
-	Engine& E = *g_engine;
+	if (!cur_engine()->built) return -1;
+	Engine& E = *cur_engine();
 	const int N = E.n;
 	const std::string s(name);
 	auto counts_of = [&](const std::vector<int>& off) {
@@ -1374,8 +1417,8 @@ XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap)
 
 XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 {
-	if (!g_engine || !g_engine->built) return -1;
-	Engine& E = *g_engine;
+	if (!cur_engine()->built) return -1;
+	Engine& E = *cur_engine();
 	const int N = E.n;
 	const std::string s(name);
 	if (s == "det_rest") return dev_to_caller(E, E.det_rest.p, 1, out, cap);
@@ -1403,7 +1446,7 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 		if (cap < 3) return -1;
 		if (E.read_counters()) return -1;
 		out[0] = E.spacing;
-		out[1] = S.sc_radius_scale * E.spacing;
+		out[1] = engine().S.sc_radius_scale * E.spacing;
 		out[2] = E.h_ctr->sc_reach;
 		return 3;
 	}
@@ -1415,8 +1458,8 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 // candidate lists stage by stage.
 XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 {
-	if (!g_engine || !g_engine->built || !x || !p) return fail("xpbd_b200_selfcol_build: no scene");
-	Engine& E = *g_engine;
+	if (!cur_engine()->built || !x || !p) return fail("xpbd_b200_selfcol_build: no scene");
+	Engine& E = *cur_engine();
 	if (E.ensure_selfcol()) return -1;
 	if (E.upload_params()) return -1;
 	const int N = E.n;

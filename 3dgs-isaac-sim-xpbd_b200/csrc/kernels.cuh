@@ -1280,7 +1280,7 @@ __global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams*
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
 	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
-	DevCounters* __restrict__ ctr, int count_hits)
+	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1296,8 +1296,10 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 		const int nc = P->kin_count;
 		const float margin = P->kin_margin, mu = P->kin_friction;
 		const float reach = margin + 0.0f;
+		const int my_obj = (P->kin_filtered && obj_id) ? obj_id[idx] : -1;
 		for (int c = 0; c < nc; ++c) {
 			const KinCollider& C = P->kin[c];
+			if (C.obj >= 0 && C.obj != my_obj) continue;
 			const float dx = p.x - C.t[0], dy = p.y - C.t[1], dz = p.z - C.t[2];
 			const float q0 = C.R[0] * dx + C.R[3] * dy + C.R[6] * dz;
 			const float q1 = C.R[1] * dx + C.R[4] * dy + C.R[7] * dz;

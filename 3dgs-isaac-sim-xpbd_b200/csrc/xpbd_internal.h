@@ -34,6 +34,7 @@ struct KinCollider {                // forward.cu:129-136
 	int type;
 	float Rp[9];
 	float tp[3];
+	int obj;                        // object it acts on, -1 every Gaussian (batched scenes)
 };
 
 // Step parameters read by every kernel from device memory, so that one captured
@@ -58,7 +59,8 @@ struct StepParams {
 	float sc_dc, sc_search, sc_excl2, sc_cross_excl2, sc_fast_rel, sc_search_plus16dc;
 	int sc_within;
 	int sc_single_object;           // every particle has the same object id
-	int pad[2];
+	int kin_filtered;               // some collider acts on one object only
+	int pad;
 	KinCollider kin[kMaxColliders];
 };
 

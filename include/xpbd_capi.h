@@ -110,6 +110,16 @@ XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd);
 
 /* ---- extensions (no counterpart in the reference ABI) ------------------- */
 
+/* Independent solver instances: a new engine (own scene, settings and stream), its
+ * release, and the choice of the engine that the reference entry points above act on
+ * from the calling thread (NULL: the process-wide default engine). */
+XPBD_API void* xpbd_b200_engine_new(void);
+XPBD_API void xpbd_b200_engine_free(void* handle);
+XPBD_API void xpbd_b200_engine_select(void* handle);
+/* Restrict each collider of the last xpbd_set_colliders call to one object (graph
+ * component id, as numbered by first Gaussian; -1 = every Gaussian), so that objects
+ * packed into one scene are gripped independently. */
+XPBD_API int xpbd_b200_set_collider_objects(int count, const int* obj);
 /* Run the engine on a caller-owned cudaStream_t (NULL: the library's own stream). */
 XPBD_API int xpbd_b200_set_stream(void* stream);
 /* Enqueue `substeps` steps without waiting for them. */

@@ -1,0 +1,62 @@
+"""Batched objects and served sessions give each object / session the result it has alone."""
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+batch = H.pkg.batch
+serve = H.pkg.serve
+
+
+def test_batched_objects_match_alone():
+    objs = batch.make_objects(count=4, seed=3, n_min=1500, n_max=4000)
+    lib = H.b200()
+    b = batch.Batch(objs)
+    b.setup(lib)
+    b.advance(lib, 20)
+    together = b.split(lib.positions())
+    for k, (sc, grs) in enumerate(objs):
+        s = batch.ObjectScenario(sc, grs)
+        s.setup(lib)
+        s.advance(lib, 20)
+        np.testing.assert_array_equal(lib.positions(), together[k], err_msg=f"object {k}")
+    lib.destroy()
+
+
+def test_engine_instances_are_independent():
+    a = H.pkg.bridge.XPBD(H.B200_SO, instance=True)
+    b = H.pkg.bridge.XPBD(H.B200_SO, instance=True)
+    sa = H.scenes.plain_scene_scenario(2500, 11, pins=20)
+    sb = H.scenes.plain_scene_scenario(1800, 12, pins=20)
+    sa.setup(a)
+    sb.setup(b)
+    for _ in range(12):          # interleaved
+        sa.advance(a, 1)
+        sb.advance(b, 1)
+    pa, pb = a.positions(), b.positions()
+    a.close()
+    b.close()
+    c = H.pkg.bridge.XPBD(H.B200_SO, instance=True)
+    for s, expect in ((H.scenes.plain_scene_scenario(2500, 11, pins=20), pa),
+                      (H.scenes.plain_scene_scenario(1800, 12, pins=20), pb)):
+        s.setup(c)
+        s.advance(c, 12)
+        np.testing.assert_array_equal(c.positions(), expect)
+    c.close()
+
+
+def test_served_sessions_match_alone():
+    sessions = [(0.0, 3000, 3, 101), (0.0, 5000, 2, 202), (0.01, 2000, 4, 303)]
+    stats = serve.run_served(H.B200_SO, sessions, budget_bytes=1e12)
+    assert stats["sessions"] == 3 and stats["steps"] == 9
+    done = {s.sid: s for s in stats["sessions_done"]}
+    for k, (a, n, frames, seed) in enumerate(sessions):
+        alone = serve.Session(k, a, n, frames, seed)
+        alone.admit(H.B200_SO)
+        while alone.frames_left > 0:
+            alone.enqueue_frame()
+        alone.solver.lib.xpbd_b200_sync()
+        np.testing.assert_array_equal(alone.solver.positions(), done[k].final)
+        alone.close(keep_result=False)
