@@ -5,7 +5,7 @@ objects are separate graph components, so K objects concatenated into one scene 
 advanced by the same launches as one object — one graph-captured kernel sequence per
 substep covers them all, whatever their sizes.  Objects keep their own coordinates
 (they may overlap in space); each object's grippers act only on that object
-(xpbd_b200_set_collider_objects), self-collision and ground stay off, so every
+(xpbd_b200_set_colliders_many binds every collider to its object), self-collision and ground stay off, so every
 object's trajectory is the one it has alone, bit for bit (tests/test_gpu_batch.py).
 """
 import ctypes
@@ -74,10 +74,13 @@ class Batch(scenes.Scenario):
 
     def colliders_posed(self, solver, t):
         types, poses, dims = self.colliders(t)
-        solver.set_colliders(types, poses, dims, 0.0, 0.0)
+        types = np.ascontiguousarray(np.asarray(types, np.int32))
+        poses = np.ascontiguousarray(np.asarray(poses, np.float32).reshape(-1))
+        dims = np.ascontiguousarray(np.asarray(dims, np.float32).reshape(-1))
         L = solver.lib
-        L.xpbd_b200_set_collider_objects.argtypes = [ctypes.c_int, ctypes.c_void_p]
-        rc = L.xpbd_b200_set_collider_objects(len(self.owner), self.owner.ctypes.data)
+        L.xpbd_b200_set_colliders_many.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_float] * 2
+        rc = L.xpbd_b200_set_colliders_many(len(types), types.ctypes.data, poses.ctypes.data, dims.ctypes.data,
+                                            self.owner.ctypes.data, 0.0, 0.0)
         if rc != 0:
             raise RuntimeError(solver.last_error())
 
@@ -85,7 +88,7 @@ class Batch(scenes.Scenario):
         for _ in range(count):
             t = (self.k + 1) / self.substeps
             self.colliders_posed(solver, t)
-            if self.k > 0:
+            if self.k > 0 and self.grippers:
                 idx, pos = self.pins(t)
                 solver.set_attached(idx, pos, 1.0)
             if blocking:

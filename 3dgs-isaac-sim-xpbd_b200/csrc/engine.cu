@@ -91,6 +91,7 @@ struct Settings {
 	bool jstats = true;
 	KinCollider kin[kMaxColliders];
 	int kin_obj[kMaxColliders];      // object each collider acts on (-1: every Gaussian)
+	std::vector<KinCollider> kin_ext; // batched colliders (any number), each bound to one object
 	int kin_count = 0;
 	float kin_margin = 0.0f, kin_friction = 0.0f;
 	bool use_graph = true;
@@ -147,6 +148,10 @@ public:
 	DBuf<float4> sc_dp, sc_sp, sc_sr, sc_sx;
 	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
 	DBuf<int> d_perm;
+	DBuf<KinCollider> d_kin_ext;
+	DBuf<int2> d_kin_range;
+	std::vector<KinCollider> h_kin_sorted;
+	std::vector<int2> h_kin_range;
 	DBuf<int> att_idx;
 	DBuf<float> att_pos;
 	bool att_active = false;
@@ -218,7 +223,7 @@ public:
 		sc_contacts.release(); sc_counts.release(); sc_block_sums.release(); d_obj_id.release(); sc_dp.release();
 		sc_sp.release(); sc_sr.release(); sc_sx.release();
 		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
-		att_idx.release(); att_pos.release(); d_perm.release();
+		att_idx.release(); att_pos.release(); d_perm.release(); d_kin_ext.release(); d_kin_range.release();
 		att_active = false;
 		coloring_built = false;
 		sc_table = 0;
@@ -477,6 +482,37 @@ public:
 		return 0;
 	}
 
+	// batched colliders: stable-sorted by object, one [begin, end) range per object id
+	int upload_ext_colliders()
+	{
+		if (S.kin_ext.empty()) return 0;
+		const int count = (int)S.kin_ext.size();
+		int objects = 0;
+		for (const auto& k : S.kin_ext) objects = std::max(objects, k.obj + 1);
+		h_kin_sorted.assign(S.kin_ext.begin(), S.kin_ext.end());
+		std::stable_sort(h_kin_sorted.begin(), h_kin_sorted.end(),
+			[](const KinCollider& a, const KinCollider& b) { return a.obj < b.obj; });
+		h_kin_range.assign(std::max(objects, 1), make_int2(0, 0));
+		for (int c = 0; c < count; ++c) {
+			const int o = h_kin_sorted[c].obj;
+			if (o < 0) continue;
+			if (h_kin_range[o].y == 0) h_kin_range[o].x = c;
+			h_kin_range[o].y = c + 1;
+			h_kin_sorted[c].obj = -1;   // selected by range; no per-collider filter on the device
+		}
+		if ((int)d_kin_ext.n < count || (int)d_kin_range.n < (int)h_kin_range.size()) {
+			CK(cudaStreamSynchronize(stream));
+			CK(d_kin_ext.alloc(std::max<size_t>(count, 64)));
+			CK(d_kin_range.alloc(std::max<size_t>(h_kin_range.size(), 64)));
+			if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+			graph_key.clear();
+		}
+		CK(cudaMemcpyAsync(d_kin_ext.p, h_kin_sorted.data(), sizeof(KinCollider) * count, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(d_kin_range.p, h_kin_range.data(), sizeof(int2) * h_kin_range.size(),
+			cudaMemcpyHostToDevice, stream));
+		return 0;
+	}
+
 	void fill_params()
 	{
 		StepParams& P = *h_params;
@@ -508,6 +544,7 @@ public:
 		P.kin_friction = S.kin_friction;
 		memcpy(P.kin, S.kin, sizeof(KinCollider) * S.kin_count);
 		P.kin_filtered = 0;
+		P.kin_ext_ranges = (int)h_kin_range.size();
 		for (int c = 0; c < S.kin_count; ++c) {
 			P.kin[c].obj = S.kin_obj[c];
 			if (S.kin_obj[c] >= 0) P.kin_filtered = 1;
@@ -540,6 +577,7 @@ public:
 	{
 		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), vol_lanes(), gather_lanes(),
 			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
+			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table };
 	}
 
@@ -634,7 +672,7 @@ public:
 		float4* pin = pos_next.p;
 		float4* pout = pos_tmp.p;
 		const bool dgs = dist_gs_on(), vgs = vol_gs_on();
-		const bool project = S.kin_count > 0 || S.ground_on || sc;
+		const bool project = S.kin_count > 0 || !S.kin_ext.empty() || S.ground_on || sc;
 		for (int it = 0; it < S.iters; ++it) {
 			const int first = (it == 0), last = (it == S.iters - 1);
 			if (dgs) {
@@ -718,7 +756,8 @@ public:
 			if (project)
 				launch(ST_PROJECT, G, B, dev::k_project, N, (const StepParams*)d_params, pin, (const float4*)pos_curr.p,
 					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0,
-					(const int*)d_obj_id.p);
+					(const int*)d_obj_id.p, S.kin_ext.empty() ? (const KinCollider*)nullptr : (const KinCollider*)d_kin_ext.p,
+					(const int2*)d_kin_range.p);
 		}
 		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
 			vel.p, pos_out3.p, (const int*)d_perm.p);
@@ -744,6 +783,7 @@ public:
 		}
 		if (S.use_distance && S.dist_gs && ensure_coloring()) return -1;
 		if (S.sc_enabled && ensure_selfcol()) return -1;
+		if (upload_ext_colliders()) return -1;   // sets the object ranges fill_params reads
 		if (upload_params()) return -1;
 		if (profiling || !S.use_graph) {
 			if (enqueue_step()) return -1;
@@ -994,6 +1034,7 @@ XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses
 		for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
 	}
 	for (int c = 0; c < count; ++c) engine().S.kin_obj[c] = -1;
+	engine().S.kin_ext.clear();
 	engine().S.kin_count = count;
 	engine().S.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
 	engine().S.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
@@ -1190,6 +1231,32 @@ XPBD_API int xpbd_b200_set_collider_objects(int count, const int* obj)
 	if (count != st.kin_count || (count > 0 && !obj))
 		return fail("xpbd_b200_set_collider_objects: %d filters for %d colliders", count, st.kin_count);
 	for (int c = 0; c < count; ++c) st.kin_obj[c] = obj[c] < 0 ? -1 : obj[c];
+	return 0;
+}
+
+XPBD_API int xpbd_b200_set_colliders_many(int count, const int* types, const float* poses, const float* dims,
+	const int* obj, float margin, float friction)
+{
+	Settings& st = engine().S;
+	if (count < 0 || (count > 0 && (!types || !poses || !dims || !obj)))
+		return fail("xpbd_b200_set_colliders_many: invalid arguments");
+	const bool same = (count == (int)st.kin_ext.size());
+	std::vector<KinCollider> next(count);
+	for (int c = 0; c < count; ++c) {
+		KinCollider& K = next[c];
+		const KinCollider* prev = same ? &st.kin_ext[c] : nullptr;
+		const bool keep = prev && prev->type == types[c];
+		for (int a = 0; a < 9; ++a) K.Rp[a] = keep ? prev->R[a] : poses[12 * c + a];
+		for (int a = 0; a < 3; ++a) K.tp[a] = keep ? prev->t[a] : poses[12 * c + 9 + a];
+		K.type = types[c];
+		for (int a = 0; a < 9; ++a) K.R[a] = poses[12 * c + a];
+		for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
+		K.obj = obj[c] < 0 ? -1 : obj[c];
+	}
+	st.kin_ext.swap(next);
+	st.kin_count = 0;
+	st.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
+	st.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
 	return 0;
 }
 

@@ -1280,7 +1280,8 @@ __global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams*
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
 	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
-	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id)
+	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id,
+	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1293,12 +1294,24 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 	}
 	if (p4.w > 0.0f) {
 		float3 p = f3(p4);
-		const int nc = P->kin_count;
 		const float margin = P->kin_margin, mu = P->kin_friction;
 		const float reach = margin + 0.0f;
-		const int my_obj = (P->kin_filtered && obj_id) ? obj_id[idx] : -1;
-		for (int c = 0; c < nc; ++c) {
-			const KinCollider& C = P->kin[c];
+		const int my_obj = ((P->kin_filtered || ext_kin) && obj_id) ? obj_id[idx] : -1;
+		// colliders: the reference's list (with optional per-collider object filter), or the
+		// batched list sorted by object, of which only this object's range is visited
+		const KinCollider* cols = P->kin;
+		int c0 = 0, c1 = P->kin_count;
+		if (ext_kin) {
+			cols = ext_kin;
+			c0 = c1 = 0;
+			if (my_obj >= 0 && my_obj < P->kin_ext_ranges) {
+				const int2 r = ext_range[my_obj];
+				c0 = r.x;
+				c1 = r.y;
+			}
+		}
+		for (int c = c0; c < c1; ++c) {
+			const KinCollider& C = cols[c];
 			if (C.obj >= 0 && C.obj != my_obj) continue;
 			const float dx = p.x - C.t[0], dy = p.y - C.t[1], dz = p.z - C.t[2];
 			const float q0 = C.R[0] * dx + C.R[3] * dy + C.R[6] * dz;
@@ -1333,8 +1346,10 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 			const float wz = C.R[6] * n0 + C.R[7] * n1 + C.R[8] * n2;
 			const float corr = margin - dist;
 			const float3 p_in = p;
-			p.x += wx * corr; p.y += wy * corr; p.z += wz * corr;
-			float3 dp = make_float3(wx * corr, wy * corr, wz * corr);
+			// explicit roundings: the batched-list and reference-list paths of this loop
+			// must round identically, whatever the compiler fuses in each
+			float3 dp = make_float3(__fmul_rn(wx, corr), __fmul_rn(wy, corr), __fmul_rn(wz, corr));
+			p.x = __fadd_rn(p.x, dp.x); p.y = __fadd_rn(p.y, dp.y); p.z = __fadd_rn(p.z, dp.z);
 			if (mu > 0.0f) {
 				const float ox = C.Rp[0] * q0 + C.Rp[1] * q1 + C.Rp[2] * q2 + C.tp[0];
 				const float oy = C.Rp[3] * q0 + C.Rp[4] * q1 + C.Rp[5] * q2 + C.tp[1];
@@ -1347,21 +1362,24 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 				const float lt = sqrtf(tx * tx + ty * ty + tz * tz);
 				if (lt > 1e-20f) {
 					const float k = fminf(1.0f, mu * corr / lt);
-					p.x -= k * tx; p.y -= k * ty; p.z -= k * tz;
-					dp.x -= k * tx; dp.y -= k * ty; dp.z -= k * tz;
+					const float fx = __fmul_rn(k, tx), fy = __fmul_rn(k, ty), fz = __fmul_rn(k, tz);
+					p.x = __fsub_rn(p.x, fx); p.y = __fsub_rn(p.y, fy); p.z = __fsub_rn(p.z, fz);
+					dp.x = __fsub_rn(dp.x, fx); dp.y = __fsub_rn(dp.y, fy); dp.z = __fsub_rn(dp.z, fz);
 				}
 			}
 			moved = true;
-			float* acc = &ctr->kin_push[kColliderAcc * c];
-			const float w = sqrtf(dp.x * dp.x + dp.y * dp.y + dp.z * dp.z);
-			atomicAdd(&acc[0], dp.x);
-			atomicAdd(&acc[1], dp.y);
-			atomicAdd(&acc[2], dp.z);
-			atomicAdd(&acc[3], w * p.x);
-			atomicAdd(&acc[4], w * p.y);
-			atomicAdd(&acc[5], w * p.z);
-			atomicAdd(&acc[6], w);
-			if (count_hits) atomicAdd(&ctr->kin_hits[c], 1);
+			if (!ext_kin) {   // per-collider statistics cover the reference's list only
+				float* acc = &ctr->kin_push[kColliderAcc * c];
+				const float w = sqrtf(dp.x * dp.x + dp.y * dp.y + dp.z * dp.z);
+				atomicAdd(&acc[0], dp.x);
+				atomicAdd(&acc[1], dp.y);
+				atomicAdd(&acc[2], dp.z);
+				atomicAdd(&acc[3], w * p.x);
+				atomicAdd(&acc[4], w * p.y);
+				atomicAdd(&acc[5], w * p.z);
+				atomicAdd(&acc[6], w);
+				if (count_hits) atomicAdd(&ctr->kin_hits[c], 1);
+			}
 		}
 		if (P->ground_on) {
 			const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane;

@@ -60,7 +60,7 @@ struct StepParams {
 	int sc_within;
 	int sc_single_object;           // every particle has the same object id
 	int kin_filtered;               // some collider acts on one object only
-	int pad;
+	int kin_ext_ranges;             // objects with a range in the batched collider list
 	KinCollider kin[kMaxColliders];
 };
 

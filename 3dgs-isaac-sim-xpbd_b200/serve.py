@@ -86,8 +86,8 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
     resident = []
     resident_bytes = [0.0]
     lock = threading.Lock()
-    admitted_ids = set()
     stop = threading.Event()
+    queued = [0]                # sessions handed to the admission thread
     backlog = queue.Queue()
 
     def admitter():
@@ -104,7 +104,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
     waiting = collections.deque()
     done, work, ticks = [], 0, 0
     sid = 0
-    while arrivals or waiting or resident or not backlog.empty() or not ready.empty():
+    while arrivals or waiting or resident or queued[0] > len(done):
         now = time.perf_counter() - t0
         if max_wall and now > max_wall:
             break
@@ -120,6 +120,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                     break
                 resident_bytes[0] += need
             backlog.put(waiting.popleft())
+            queued[0] += 1
         while not ready.empty():
             s = ready.get()
             s.pending_since = time.perf_counter()

@@ -120,6 +120,12 @@ XPBD_API void xpbd_b200_engine_select(void* handle);
  * component id, as numbered by first Gaussian; -1 = every Gaussian), so that objects
  * packed into one scene are gripped independently. */
 XPBD_API int xpbd_b200_set_collider_objects(int count, const int* obj);
+/* Colliders for scenes that pack many objects: any number of colliders (same layout as
+ * xpbd_set_colliders), each bound to one object id obj[c]; a Gaussian is tested only
+ * against its own object's colliders.  Replaces the xpbd_set_colliders list (and is
+ * replaced by the next xpbd_set_colliders call); xpbd_collider_stats does not cover it. */
+XPBD_API int xpbd_b200_set_colliders_many(int count, const int* types, const float* poses, const float* dims,
+	const int* obj, float margin, float friction);
 /* Run the engine on a caller-owned cudaStream_t (NULL: the library's own stream). */
 XPBD_API int xpbd_b200_set_stream(void* stream);
 /* Enqueue `substeps` steps without waiting for them. */
