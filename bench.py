@@ -5,7 +5,8 @@ graph, 64-member volume clusters, shape matching, spatial-hash self-collision), 
 capsule grippers pulling apart while twisting; one bench "step" is one 60 Hz frame =
 10 solver substeps x 4 iterations.  Metric: Gaussian-substeps per second.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config large|plain]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--config large|plain|batched|served] [--gaussians N]
 
 value     device-resident throughput: frames enqueued through the library's async API,
           timed with CUDA events on the engine's stream (pins/colliders re-posed per
@@ -44,13 +45,17 @@ SUBSTEPS = 10
 ITERS = 4
 
 
-def workload(config):
+def workload(config, gaussians=None):
+    """(name, scenario factory) of a single-scene workload; `gaussians` shrinks or grows
+    the scene (profiler captures use a small case of the same workload)."""
     if config == "plain":
-        return "plain 20k: 20,000 Gaussians, 2 pinned capsule grippers, 10 substeps x 4 iterations", \
-            lambda: scenes.plain_scene_scenario(20000, 0)
-    return ("large 1M: 1,000,000 Gaussians, 8-NN graph, 64-member clusters (k=3), shape matching, "
+        n = gaussians or 20000
+        return f"plain: {n} Gaussians, 2 pinned capsule grippers, 10 substeps x 4 iterations", \
+            lambda: scenes.plain_scene_scenario(n, 0)
+    n = gaussians or 1_000_000
+    return (f"large: {n} Gaussians, 8-NN graph, 64-member clusters (k=3), shape matching, "
             "spatial-hash self-collision, 2 twisting grippers, 10 substeps x 4 iterations"), \
-        lambda: scenes.large_scene_scenario(1_000_000, 0)
+        lambda: scenes.large_scene_scenario(n, 0)
 
 
 def peaks():
@@ -160,11 +165,21 @@ def algorithmic_bytes(stage, sizes, n):
     return None if per is None else per * n
 
 
+def max_over_ranks(values, world, device):
+    """Element-wise maximum of `values` over all ranks (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def bench_b200(args, rank, world):
     import torch
 
     torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
-    name, make = workload(args.config)
+    name, make = workload(args.config, args.gaussians)
     scen = make()
     n = scen.n
     x = pkg.XPBD()
@@ -217,12 +232,7 @@ def bench_b200(args, rank, world):
     e2e_s = time.perf_counter() - t0
     h2d = SUBSTEPS * (len(scen.pins(0.0)[0]) * 16 + len(scen.grippers) * 64)
 
-    if world > 1:
-        t = torch.tensor([ms, e2e_s * 1e3], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    else:
-        e2e_ms = e2e_s * 1e3
+    ms, e2e_ms = max_over_ranks([ms, e2e_s * 1e3], world, "cuda")
     if rank != 0:
         x.destroy()
         return None
@@ -355,7 +365,7 @@ def bench_served(args, rank, world):
 def bench_reference(args, rank, world):
     if rank != 0:
         return None
-    name, make = workload(args.config)
+    name, make = workload(args.config, args.gaussians)
     steps = args.steps
     warm = args.warmup
     lib = os.path.join(ROOT, "oracle", "liboracle.so")
@@ -390,6 +400,8 @@ def main():
     ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gaussians", type=int, default=None,
+                    help="scene size of the large/plain workload (default 1,000,000 / 20,000)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

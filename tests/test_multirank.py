@@ -1,0 +1,58 @@
+"""Multi-rank paths of bench.py on CPU: gloo process group, world size 2."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import torch.multiprocessing as mp
+
+import helpers as H
+
+ROOT = H.ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _max_worker(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        out[rank] = bench.max_over_ranks([1.0 + rank, 10.0 - rank, 0.5 * rank], world, "cpu")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_max_worker, args=(world, port, out), nprocs=world, join=True)
+        got = dict(out)
+    assert got[0] == got[1] == [2.0, 10.0, 0.5]
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    """`--impl reference` with two ranks: rank 0 alone times the CPU path and prints one
+    JSON line; the other rank exits 0 without work."""
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+           "--impl", "reference", "--config", "plain", "--gaussians", "1500", "--steps", "2", "--warmup", "1"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
