@@ -134,7 +134,7 @@ public:
 	int sc_table = 0;
 
 	// ---- device state ----
-	DBuf<float4> pos_curr, pos_next, pos_tmp, vel, pos_rest;
+	DBuf<float4> pos_curr, pos_next, pos_tmp, vel, pos_rest, shape_rest;
 	DBuf<float> pos_out3;
 	DBuf<int> off, nbr;
 	DBuf<float> ndist, nstiff, lam;
@@ -215,6 +215,7 @@ public:
 	void free_device()
 	{
 		pos_curr.release(); pos_next.release(); pos_tmp.release(); vel.release(); pos_rest.release();
+		shape_rest.release();
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
@@ -370,6 +371,9 @@ public:
 				CK(cudaMemcpyAsync(ndist.p, nd.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
 				CK(cudaMemcpyAsync(nstiff.p, ns.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
 			}
+			CK(shape_rest.alloc(n));
+			dev::k_shape_rest<<<blocks_for(n), kBlock, 0, stream>>>(n, pos_rest.p, off.p, nbr.p, shape_rest.p);
+			CK(cudaGetLastError());
 			CK(cudaStreamSynchronize(stream));
 		}
 		CK(d_scales.alloc(3 * (size_t)n)); CK(d_rots.alloc(4 * (size_t)n));
@@ -745,8 +749,14 @@ public:
 				}
 			}
 			if (S.use_shape) {
-				launch(ST_SHAPE, G, B, dev::k_shape_match, N, (const StepParams*)d_params, (const float4*)pin, pout,
-					(const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p, S.shape_robust ? 1 : 0);
+				if (S.shape_robust)
+					launch(ST_SHAPE, G, B, dev::k_shape_match<true>, N, (const StepParams*)d_params, (const float4*)pin,
+						pout, (const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p,
+						(const float4*)shape_rest.p);
+				else
+					launch(ST_SHAPE, G, B, dev::k_shape_match<false>, N, (const StepParams*)d_params, (const float4*)pin,
+						pout, (const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p,
+						(const float4*)shape_rest.p);
 				std::swap(pin, pout);
 			}
 			if (sc)
@@ -1506,6 +1516,13 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 			if (s == "vel") { v[3 * i] = tmp[r].x; v[3 * i + 1] = tmp[r].y; v[3 * i + 2] = tmp[r].z; }
 			else v[i] = tmp[r].w;
 		}
+		return copy_host(v, (long long)v.size(), out, cap);
+	}
+	if (s == "cluster_coef") {   // the last iteration's per-cluster coefficient (0: inactive)
+		std::vector<float4> tmp(3 * (size_t)N);
+		if (copy_dev(E.rec.p, 3LL * N, tmp.data(), 3LL * N, E.stream) < 0) return -1;
+		std::vector<float> v(N);
+		for (int r = 0; r < N; ++r) v[E.perm[r]] = tmp[3 * (size_t)r].w;
 		return copy_host(v, (long long)v.size(), out, cap);
 	}
 	if (s == "self_col") {

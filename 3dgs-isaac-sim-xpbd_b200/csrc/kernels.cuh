@@ -1065,6 +1065,31 @@ __global__ void __launch_bounds__(kBlock) k_volume_rest(int n, const float4* __r
 // (shapeMatchRotationDouble, forward.cu:5991-6086) or the float32 path
 // (forward.cu:6238-6319); XPBD pull toward the goal (forward.cu:4972-4988).
 // ---------------------------------------------------------------------------
+// One cyclic-Jacobi rotation zeroing m[p][q] (p < q compile-time constants, so m and v
+// stay in registers; a run-time pivot index would put them in local memory).
+template <int p, int q>
+__device__ __forceinline__ void jacobi_rotate_d(double (&m)[3][3], double (&v)[3][3])
+{
+	constexpr int r = 3 - p - q;
+	const double app = m[p][p], aqq = m[q][q], apq = m[p][q];
+	const double phi = 0.5 * (aqq - app) / (apq + 1e-300);
+	const double t = (phi >= 0.0) ? 1.0 / (phi + sqrt(1.0 + phi * phi)) : 1.0 / (phi - sqrt(1.0 + phi * phi));
+	const double c = 1.0 / sqrt(1.0 + t * t);
+	const double s = t * c;
+	m[p][p] = app - t * apq;
+	m[q][q] = aqq + t * apq;
+	m[p][q] = m[q][p] = 0.0;
+	const double arp = m[r][p], arq = m[r][q];
+	m[r][p] = m[p][r] = c * arp - s * arq;
+	m[r][q] = m[q][r] = c * arq + s * arp;
+#pragma unroll
+	for (int rr = 0; rr < 3; ++rr) {
+		const double vrp = v[rr][p], vrq = v[rr][q];
+		v[rr][p] = c * vrp - s * vrq;
+		v[rr][q] = s * vrp + c * vrq;
+	}
+}
+
 __device__ __forceinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 {
 	double a[3][3];
@@ -1080,7 +1105,7 @@ __device__ __forceinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 	double v[3][3] = { { 1.0, 0.0, 0.0 }, { 0.0, 1.0, 0.0 }, { 0.0, 0.0, 1.0 } };
 	for (int iter = 0; iter < 50; ++iter) {
 		bool done = true;
-		int p = 0, q = 1;
+		int piv = 0;   // 0: (0,1), 1: (0,2), 2: (1,2)
 		double max_off = -1.0;
 #pragma unroll
 		for (int k = 0; k < 3; ++k) {
@@ -1088,27 +1113,12 @@ __device__ __forceinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 			const double off = fabs(m[pk][qk]);
 			// off > 1e-12 sqrt(|a_pp a_qq|) + 1e-300, compared in squares (no square root)
 			if (off > 1e-300 && off * off > 1e-24 * fabs(m[pk][pk] * m[qk][qk])) done = false;
-			if (off > max_off) { max_off = off; p = pk; q = qk; }
+			if (off > max_off) { max_off = off; piv = k; }
 		}
 		if (done) break;
-		const double app = m[p][p], aqq = m[q][q], apq = m[p][q];
-		const double phi = 0.5 * (aqq - app) / (apq + 1e-300);
-		const double t = (phi >= 0.0) ? 1.0 / (phi + sqrt(1.0 + phi * phi)) : 1.0 / (phi - sqrt(1.0 + phi * phi));
-		const double c = 1.0 / sqrt(1.0 + t * t);
-		const double s = t * c;
-		m[p][p] = app - t * apq;
-		m[q][q] = aqq + t * apq;
-		m[p][q] = m[q][p] = 0.0;
-		const int r = 3 - p - q;
-		const double arp = m[r][p], arq = m[r][q];
-		m[r][p] = m[p][r] = c * arp - s * arq;
-		m[r][q] = m[q][r] = c * arq + s * arp;
-#pragma unroll
-		for (int rr = 0; rr < 3; ++rr) {
-			const double vrp = v[rr][p], vrq = v[rr][q];
-			v[rr][p] = c * vrp - s * vrq;
-			v[rr][q] = s * vrp + c * vrq;
-		}
+		if (piv == 0) jacobi_rotate_d<0, 1>(m, v);
+		else if (piv == 1) jacobi_rotate_d<0, 2>(m, v);
+		else jacobi_rotate_d<1, 2>(m, v);
 	}
 	double ev[3] = { m[0][0], m[1][1], m[2][2] };
 #pragma unroll
@@ -1198,9 +1208,52 @@ __device__ __noinline__ bool shape_rotation_float(const M3& A, M3& Rout)
 	return true;
 }
 
-__global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams* __restrict__ P,
+// Rest-state part of shape matching, fixed for the life of the graph: the rest centroid
+// of {i} + 1-ring, 1 / member count, and the skips that depend only on the rest pose and
+// the topology (fewer than 4 neighbours, boundary bias > 0.4; forward.cu:6116-6176).
+// out[i] = (rest centroid, 1 / count), or w = -1 when node i is never shape-matched.
+__global__ void __launch_bounds__(kBlock) k_shape_rest(int n, const float4* __restrict__ rest,
+	const int* __restrict__ off, const int* __restrict__ nbr, float4* __restrict__ out)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const float4 skip = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+	const int e0 = off[idx], e1 = off[idx + 1];
+	const int cnt = e1 - e0;
+	if (cnt < 4) { out[idx] = skip; return; }
+	float3 com_rest = f3(ld4(rest, idx));
+	float cluster_count = 1.0f;
+	for (int e = e0; e < e1; ++e) {
+		const int j = __ldg(nbr + e);
+		if (j < 0 || j >= n) continue;
+		com_rest = add3(com_rest, f3(ld4(rest, j)));
+		cluster_count += 1.0f;
+	}
+	if (cluster_count < 2.0f) { out[idx] = skip; return; }
+	const float inv_c = 1.0f / cluster_count;
+	com_rest = mul3(com_rest, inv_c);
+	float3 dir_sum = make_float3(0.0f, 0.0f, 0.0f);
+	for (int e = e0; e < e1; ++e) {
+		const int j = __ldg(nbr + e);
+		if (j < 0 || j >= n) continue;
+		const float3 q = sub3(f3(ld4(rest, j)), com_rest);
+		const float len = len3(q);
+		if (len > 1e-7f) dir_sum = add3(dir_sum, mul3(q, 1.0f / len));
+	}
+	const float bias = len3(dir_sum) / fmaxf((float)cnt, 1.0f);
+	if (bias > 0.4f) { out[idx] = skip; return; }
+	out[idx] = make_float4(com_rest.x, com_rest.y, com_rest.z, inv_c);
+}
+
+// Per-iteration shape matching: current centroid, A = sum (p - c)(q - c_rest)^T over
+// {i} + 1-ring, normalised, rotation by polar decomposition (FP64 Jacobi when ROBUST,
+// else float), goal projection.  The rest-only terms come from k_shape_rest.  Three
+// blocks per SM (80 registers, a few spilled) hide more of the FP64 Jacobi chain's
+// latency than two (measured 1.3 -> 1.05 ms per substep at 1M).
+template <bool ROBUST>
+__global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
-	const int* __restrict__ off, const int* __restrict__ nbr, int robust)
+	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1208,35 +1261,18 @@ __global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams*
 	const float3 pi = f3(p4);
 	const float wi = p4.w * P->inv_mass_scale;
 	if (wi <= 0.0f) { pout[idx] = p4; return; }
+	const float4 sr = ld4(shape_rest, idx);
+	if (!(sr.w > 0.0f)) { pout[idx] = p4; return; }
 	const int e0 = off[idx], e1 = off[idx + 1];
-	const int cnt = e1 - e0;
-	if (cnt < 4) { pout[idx] = p4; return; }
 	const float3 ri = f3(ld4(rest, idx));
-	float3 com_rest = ri, com_curr = pi;
-	float cluster_count = 1.0f;
+	const float3 com_rest = f3(sr);
+	float3 com_curr = pi;
 	for (int e = e0; e < e1; ++e) {
 		const int j = __ldg(nbr + e);
 		if (j < 0 || j >= n) continue;
-		com_rest = add3(com_rest, f3(ld4(rest, j)));
 		com_curr = add3(com_curr, f3(ld4(pin, j)));
-		cluster_count += 1.0f;
 	}
-	if (cluster_count < 2.0f) { pout[idx] = p4; return; }
-	const float inv_c = 1.0f / cluster_count;
-	com_rest = mul3(com_rest, inv_c);
-	com_curr = mul3(com_curr, inv_c);
-	{
-		float3 dir_sum = make_float3(0.0f, 0.0f, 0.0f);
-		for (int e = e0; e < e1; ++e) {
-			const int j = __ldg(nbr + e);
-			if (j < 0 || j >= n) continue;
-			const float3 q = sub3(f3(ld4(rest, j)), com_rest);
-			const float len = len3(q);
-			if (len > 1e-7f) dir_sum = add3(dir_sum, mul3(q, 1.0f / len));
-		}
-		const float bias = len3(dir_sum) / fmaxf((float)cnt, 1.0f);
-		if (bias > 0.4f) { pout[idx] = p4; return; }
-	}
+	com_curr = mul3(com_curr, sr.w);
 	M3 A;
 	m3_zero(A);
 	m3_add_outer(A, sub3(pi, com_curr), sub3(ri, com_rest));
@@ -1257,7 +1293,7 @@ __global__ void __launch_bounds__(kBlock) k_shape_match(int n, const StepParams*
 #pragma unroll
 		for (int r = 0; r < 3; ++r) A.m[c][r] /= a_norm;
 	M3 R;
-	const bool ok = robust ? shape_rotation_double(A, R) : shape_rotation_float(A, R);
+	const bool ok = ROBUST ? shape_rotation_double(A, R) : shape_rotation_float(A, R);
 	if (!ok) { pout[idx] = p4; return; }
 	const float3 goal = add3(com_curr, m3_mulv(R, sub3(ri, com_rest)));
 	const float3 gd = sub3(goal, pi);
@@ -1732,9 +1768,11 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
 	int* __restrict__ counts)
 {
-	const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t0 >= n) return;
-	const int i = idx_sorted[t0];
+	// thread i builds the list of particle i: particles are numbered along a Morton curve
+	// of their rest positions, so a warp's particles share most of their 27 cells (same
+	// loop trip counts, same neighbour rows); the list itself does not depend on who builds it
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
 	const float4 x = X[i], p = Pp[i];
 	int cnt = 0, over = 0;
 	if (isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
@@ -1751,18 +1789,27 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 		const float search2 = search * search;
 		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
 		int* out = contacts + (size_t)i * kSelfColMax;
-		unsigned int hs[27];
 		float prio[kSelfColMax];
 		int tier[kSelfColMax];
-		int nh = 0;
+		// a cell whose hash repeats an earlier one of the 27 is skipped (forward.cu:7116-7123);
+		// a 64-bit filter on the low hash bits settles almost every cell without comparing,
+		// the rest recompute the earlier hashes
+		unsigned long long seen = 0ull;
+		int kc = 0;
 		for (int oz = -1; oz <= 1; ++oz)
 			for (int oy = -1; oy <= 1; ++oy)
-				for (int ox = -1; ox <= 1; ++ox) {
+				for (int ox = -1; ox <= 1; ++ox, ++kc) {
 					const unsigned int h = sc_hash(cx + ox, cy + oy, cz + oz, mask);
-					bool dup = false;
-					for (int m = 0; m < nh; ++m) if (hs[m] == h) { dup = true; break; }
-					if (dup) continue;
-					hs[nh++] = h;
+					const unsigned long long bit = 1ull << (h & 63u);
+					if (seen & bit) {
+						bool dup = false;
+						for (int m = 0; m < kc && !dup; ++m) {
+							const int mz = m / 9 - 1, my = (m / 3) % 3 - 1, mx = m % 3 - 1;
+							dup = sc_hash(cx + mx, cy + my, cz + mz, mask) == h;
+						}
+						if (dup) continue;
+					}
+					seen |= bit;
 					const int s = start[h], e = start[h + 1];
 					for (int t = s; t < e; ++t) {
 						// predicted position + index first: most neighbours fail the distance
