@@ -97,6 +97,8 @@ struct Settings {
 	bool use_graph = true;
 	bool reorder = true;             // Morton order inside the engine (results unchanged)
 	int lanes_a = 0, lanes_b = 0;    // volume kernel lanes per cluster / node (0 = automatic)
+	dev::CmMaterial cm{ 1.0f, 0.1f, 0.1f, 0.1f, 1.0f, 1 };   // ChainMail material (forward.cu:66-71)
+	bool cm_frontier = true;         // ChainMail sweeps on work lists (false: every sweep dense)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -135,6 +137,14 @@ public:
 
 	// ---- device state ----
 	DBuf<float4> pos_curr, pos_next, pos_tmp, vel, pos_rest, shape_rest;
+	// ChainMail: (arrival time, density), sweep flags / marks / work list / scratch, seeds
+	DBuf<float2> cm_td;
+	DBuf<unsigned char> cm_flag;
+	DBuf<unsigned int> cm_mark;
+	DBuf<int> cm_work, cm_seed_idx;
+	DBuf<float4> cm_spos;
+	DBuf<float> cm_stime, cm_seed_delta, cm_time_out;
+	DBuf<dev::CmState> cm_state;
 	DBuf<float> pos_out3;
 	DBuf<int> off, nbr;
 	DBuf<float> ndist, nstiff, lam;
@@ -216,6 +226,8 @@ public:
 	{
 		pos_curr.release(); pos_next.release(); pos_tmp.release(); vel.release(); pos_rest.release();
 		shape_rest.release();
+		cm_td.release(); cm_flag.release(); cm_mark.release(); cm_work.release(); cm_seed_idx.release();
+		cm_spos.release(); cm_stime.release(); cm_seed_delta.release(); cm_time_out.release(); cm_state.release();
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
@@ -436,6 +448,79 @@ public:
 		graph_key.clear();
 		++generation;
 		return 0;
+	}
+
+	// ------------------------------------------------------------------ ChainMail
+	// ensureChainmailGPU's time / density upload (forward.cu:10679-10698, 10826): every
+	// arrival time 1e9 (not reached), density = opacity.  Allocated on first use.
+	int ensure_chainmail()
+	{
+		if (cm_td.p) return 0;
+		const auto dens = to_internal(in_opacity.data(), 1);
+		std::vector<float2> td(n);
+		for (int i = 0; i < n; ++i) td[i] = make_float2(1e9f, dens[i]);
+		CK(cm_td.alloc(n)); CK(cm_flag.alloc(n)); CK(cm_mark.alloc((n + 31) / 32)); CK(cm_work.alloc(n));
+		CK(cm_spos.alloc(n)); CK(cm_stime.alloc(n)); CK(cm_time_out.alloc(n)); CK(cm_state.alloc(1));
+		CK(cudaMemcpyAsync(cm_td.p, td.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemsetAsync(cm_flag.p, 0, cm_flag.bytes(), stream));
+		CK(cudaMemsetAsync(cm_mark.p, 0, cm_mark.bytes(), stream));
+		CK(cudaMemsetAsync(cm_state.p, 0, cm_state.bytes(), stream));
+		return sync();
+	}
+
+	int cm_publish(float* time_out)
+	{
+		dev::k_cm_publish<<<blocks_for(n), kBlock, 0, stream>>>(n, pos_curr.p, cm_td.p, d_perm.p, pos_out3.p, time_out);
+		CK(cudaGetLastError());
+		return 0;
+	}
+
+	int chainmail_seed(int count, const int* idx, const float* delta)
+	{
+		if (ensure_chainmail()) return -1;
+		if (count == 0) return 0;
+		std::vector<int> ii(count);
+		for (int k = 0; k < count; ++k) ii[k] = inv[idx[k]];
+		if ((int)cm_seed_idx.n < count) { CK(cm_seed_idx.alloc(count)); CK(cm_seed_delta.alloc(3 * (size_t)count)); }
+		CK(cudaMemcpyAsync(cm_seed_idx.p, ii.data(), sizeof(int) * count, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(cm_seed_delta.p, delta, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
+		dev::k_cm_seed<<<1, 1, 0, stream>>>(count, cm_seed_idx.p, cm_seed_delta.p, pos_curr.p, cm_td.p, cm_flag.p,
+			cm_state.p);
+		CK(cudaGetLastError());
+		if (cm_publish(nullptr)) return -1;
+		return sync();
+	}
+
+	// runChainmailGPU, dense path (forward.cu:12901-12999): prop_iters propagation
+	// sweeps (frontier form), relax_iters relax sweeps and the closing relax sweep
+	int chainmail_run(int prop_iters, int relax_iters, float strength, float stiffness, float damping)
+	{
+		if (ensure_chainmail()) return -1;
+		const dev::CmMaterial M = S.cm;
+		const dim3 B(kBlock);
+		const dim3 G = blocks_for(n);
+		const dim3 GS(std::min<unsigned>(G.x, 148u * 8u));   // grid-stride kernels
+		for (int it = 0; it < prop_iters; ++it) {
+			dev::k_cm_begin<<<1, 1, 0, stream>>>(n, S.cm_frontier ? n / 4 : -1, cm_state.p);
+			dev::k_cm_expand<<<GS, B, 0, stream>>>(n, off.p, nbr.p, cm_flag.p, cm_mark.p, cm_work.p, cm_state.p);
+			dev::k_cm_sweep<<<GS, B, 0, stream>>>(n, pos_curr.p, cm_td.p, off.p, nbr.p, ndist.p, nstiff.p, cm_work.p,
+				cm_state.p, M, strength, cm_spos.p, cm_stime.p);
+			dev::k_cm_commit<<<GS, B, 0, stream>>>(n, pos_curr.p, cm_td.p, cm_work.p, cm_spos.p, cm_stime.p, cm_flag.p,
+				cm_mark.p, cm_state.p);
+			launches += 4;
+		}
+		float4* a = pos_curr.p;
+		float4* b = pos_tmp.p;
+		for (int it = 0; it <= relax_iters; ++it) {
+			dev::k_cm_relax<<<G, B, 0, stream>>>(n, a, b, cm_td.p, off.p, nbr.p, ndist.p, nstiff.p, M, stiffness, damping);
+			++launches;
+			std::swap(a, b);
+		}
+		if (a != pos_curr.p)
+			CK(cudaMemcpyAsync(pos_curr.p, a, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream));
+		CK(cudaGetLastError());
+		if (cm_publish(cm_time_out.p)) return -1;
+		return sync();
 	}
 
 	int ensure_coloring()
@@ -1268,6 +1353,53 @@ XPBD_API int xpbd_b200_set_colliders_many(int count, const int* types, const flo
 	st.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
 	st.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
 	return 0;
+}
+
+// ChainMail (forward.cu:12808-13006).  The reference's C ABI cannot reach it: xpbd_create
+// forces XPBD mode (xpbd_capi.cu:98); these expose its GPU path on the same scene.
+XPBD_API void xpbd_b200_chainmail_set_material(float global_scale, float air, float skin, float bone,
+	int use_edge_stiffness, float edge_influence)
+{
+	// setChainmailMaterialParams (forward.cu:4844-4858)
+	dev::CmMaterial& M = engine().S.cm;
+	M.global = fmaxf(1e-4f, global_scale);
+	M.air = fmaxf(1e-4f, air);
+	M.skin = fmaxf(1e-4f, skin);
+	M.bone = fmaxf(1e-4f, bone);
+	M.use_edge = use_edge_stiffness != 0;
+	M.influence = fmaxf(0.0f, edge_influence);
+}
+
+XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled) { engine().S.cm_frontier = enabled != 0; }
+
+XPBD_API int xpbd_b200_chainmail_seed(int count, const int* idx, const float* delta)
+{
+	Engine& E = *cur_engine();
+	if (!E.stepped) return fail("xpbd_b200_chainmail_seed: no step yet");
+	if (count < 0 || (count > 0 && (!idx || !delta))) return fail("xpbd_b200_chainmail_seed: invalid arguments");
+	for (int k = 0; k < count; ++k)
+		if (idx[k] < 0 || idx[k] >= E.n) return fail("xpbd_b200_chainmail_seed: index %d out of range", idx[k]);
+	return E.chainmail_seed(count, idx, delta);
+}
+
+XPBD_API int xpbd_b200_chainmail_run(int prop_iters, int relax_iters, float prop_strength, float relax_stiffness,
+	float relax_damping)
+{
+	Engine& E = *cur_engine();
+	if (!E.stepped) return fail("xpbd_b200_chainmail_run: no step yet");
+	if (prop_iters < 0 || relax_iters < 0) return fail("xpbd_b200_chainmail_run: negative iteration count");
+	return E.chainmail_run(prop_iters, relax_iters, prop_strength, relax_stiffness, relax_damping);
+}
+
+XPBD_API int xpbd_b200_chainmail_times(float* out, int n)
+{
+	Engine& E = *cur_engine();
+	if (!E.stepped || !out || n < E.n) return fail("xpbd_b200_chainmail_times: invalid arguments");
+	if (E.ensure_chainmail()) return -1;
+	if (E.cm_publish(E.cm_time_out.p)) return -1;
+	CK(cudaMemcpyAsync(out, E.cm_time_out.p, sizeof(float) * E.n, cudaMemcpyDeviceToHost, E.stream));
+	if (E.sync()) return -1;
+	return E.n;
 }
 
 XPBD_API void* xpbd_b200_engine_new(void) { return new (std::nothrow) Engine(); }

@@ -2256,5 +2256,288 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 	atomicAdd(&ctr->shapes_deformed, 1u);
 }
 
+// ===========================================================================
+// ChainMail displacement propagation (runChainmailGPU's dense path,
+// forward.cu:12808-13006): arrival-time sweeps that move each Gaussian toward the
+// neighbour that reached it first, then relax sweeps.
+//
+// Layout: td[i] = (arrival time, density) as one float2, so a neighbour costs one
+// 8-byte load; positions are the engine's float4 (inverse mass in w, untouched).
+//
+// Propagation runs as a frontier sweep.  A Gaussian can change in a sweep only if a
+// neighbour's arrival time dropped in the sweep before (otherwise its time is already
+// no later than every neighbour's offer, so the reference kernel writes its input back
+// unchanged), so each sweep visits only the neighbours of the Gaussians flagged in the
+// previous one: k_cm_expand turns the flags into a work list (warp ballots give one
+// atomic per warp), k_cm_sweep computes the reference kernel's output for the listed
+// Gaussians from the unchanged state, k_cm_commit writes back the ones that improved
+// and flags them for the next sweep.  The result equals the reference's dense Jacobi
+// sweep exactly; when a quarter of the Gaussians are flagged the list is replaced by
+// all Gaussians.
+// ===========================================================================
+constexpr float kCmAir = 0.13f, kCmSkin = 0.45f, kCmBone = 0.75f;   // forward.h:63-65
+
+struct CmMaterial {                 // setChainmailMaterialParams (forward.cu:4844-4858)
+	float global, air, skin, bone, influence;
+	int use_edge;
+};
+
+struct CmState {                    // device-side sweep bookkeeping
+	int pending;                    // Gaussians flagged by the last sweep or by seeds
+	int work;                       // entries in the work list of this sweep
+	int dense;                      // this sweep visits every Gaussian
+	int pad;
+};
+
+// cm_getConstraint (forward.cu:5221-5264): axis tolerance of a density class
+__device__ __forceinline__ float cm_axis_tol(const CmMaterial& M, float density)
+{
+	const float c = (density < kCmAir) ? M.air : ((density < kCmSkin) ? M.skin : M.bone);
+	return c * fmaxf(1e-4f, M.global);
+}
+
+// cm_edgeScaleFromStiff (forward.cu:5266-5278)
+__device__ __forceinline__ float cm_edge_scale(const CmMaterial& M, float stiff)
+{
+	if (!M.use_edge || M.influence <= 0.0f) return 1.0f;
+	const float s = fminf(fmaxf(stiff, 0.05f), 1.0f);
+	const float t = (s - 0.05f) / 0.95f;
+	const float scale = 1.0f + M.influence * (t * 2.0f - 1.0f);
+	return fminf(fmaxf(scale, 0.1f), 4.0f);
+}
+
+__device__ __forceinline__ float cm_class_time(float d)
+{
+	return (d < kCmAir) ? 1.0f : ((d < kCmSkin) ? 0.3f : ((d < kCmBone) ? 0.05f : 0.005f));
+}
+
+// cm_propagationTime (forward.cu:5280-5293)
+__device__ __forceinline__ float cm_link_time(float d0, float d1)
+{
+	return (cm_class_time(d0) + cm_class_time(d1)) * 0.5f;
+}
+
+// cm_correctionFromNeighbor (forward.cu:5295-5330)
+__device__ __forceinline__ float3 cm_correction(const CmMaterial& M, float3 epos, float3 npos, float targ, float ndens,
+	float stiff)
+{
+	const float dx = cm_axis_tol(M, ndens);
+	const float edge_scale = cm_edge_scale(M, stiff);
+	const float3 dir = sub3(epos, npos);
+	const float len = len3(dir);
+	if (len < 1e-6f) return make_float3(0.0f, 0.0f, 0.0f);
+	const float inv_len = 1.0f / len;
+	const float3 nd = mul3(dir, inv_len);
+	if (len < targ - dx) return mul3(nd, ((targ - dx) - len) * edge_scale);
+	if (len > targ + dx) return mul3(nd, -((len - (targ + dx)) * edge_scale));
+	return make_float3(0.0f, 0.0f, 0.0f);
+}
+
+// seeds, in order (applySeedCommandsKernel, forward.cu:5907-5924): move by delta, arrival
+// time 0, flagged for the next sweep
+__global__ void k_cm_seed(int count, const int* __restrict__ idx, const float* __restrict__ delta,
+	float4* __restrict__ pos, float2* __restrict__ td, unsigned char* __restrict__ flag, CmState* __restrict__ st)
+{
+	if (blockIdx.x != 0 || threadIdx.x != 0) return;
+	for (int k = 0; k < count; ++k) {
+		const int i = idx[k];
+		float4 p = pos[i];
+		p.x = p.x + delta[3 * k]; p.y = p.y + delta[3 * k + 1]; p.z = p.z + delta[3 * k + 2];
+		pos[i] = p;
+		td[i].x = 0.0f;
+		if (!flag[i]) { flag[i] = 1; ++st->pending; }
+	}
+}
+
+// start of a sweep: dense when more than `dense_above` Gaussians are flagged
+__global__ void k_cm_begin(int n, int dense_above, CmState* __restrict__ st)
+{
+	const int dense = st->pending > dense_above;
+	st->dense = dense;
+	st->work = dense ? n : 0;
+	st->pending = 0;
+}
+
+// Work list of this sweep: the neighbours of every flagged Gaussian, each once (a bit
+// per Gaussian in `mark`), appended with one atomic per warp; clears the flags.  The
+// lanes of a warp walk the rows of the warp's flagged Gaussians together.
+__global__ void __launch_bounds__(kBlock) k_cm_expand(int n, const int* __restrict__ off, const int* __restrict__ nbr,
+	unsigned char* __restrict__ flag, unsigned int* __restrict__ mark, int* __restrict__ work, CmState* __restrict__ st)
+{
+	const bool dense = st->dense != 0;
+	const int lane = threadIdx.x & 31;
+	const int stride = gridDim.x * blockDim.x;
+	for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+		const int i = base + lane;
+		const bool pending = i < n && flag[i];
+		if (pending) flag[i] = 0;
+		if (dense) continue;
+		unsigned int todo = __ballot_sync(0xffffffffu, pending);
+		while (todo) {
+			const int p = base + __ffs(todo) - 1;
+			todo &= todo - 1;
+			const int e1 = off[p + 1];
+			for (int e0 = off[p]; e0 < e1; e0 += 32) {
+				const int e = e0 + lane;
+				bool fresh = false;
+				int j = 0;
+				if (e < e1) {
+					j = __ldg(nbr + e);
+					if (j >= 0 && j < n) {
+						const unsigned int bit = 1u << (j & 31);
+						fresh = (atomicOr(mark + (j >> 5), bit) & bit) == 0u;
+					}
+				}
+				const unsigned int fm = __ballot_sync(0xffffffffu, fresh);
+				if (fm) {
+					int at = 0;
+					if (lane == 0) at = atomicAdd(&st->work, __popc(fm));
+					at = __shfl_sync(0xffffffffu, at, 0);
+					if (fresh) work[at + __popc(fm & ((1u << lane) - 1u))] = j;
+				}
+			}
+		}
+	}
+}
+
+// chainmailPropagateKernelBest (forward.cu:5396-5464) for the listed Gaussians: the
+// earliest arrival through any neighbour; when it beats the Gaussian's own time, one
+// correction toward the neighbour it came through.  Reads the state only; results go
+// to per-entry scratch (Jacobi: every entry sees the state before this sweep).
+__global__ void __launch_bounds__(kBlock) k_cm_sweep(int n, const float4* __restrict__ pos,
+	const float2* __restrict__ td, const int* __restrict__ off, const int* __restrict__ nbr,
+	const float* __restrict__ ndist, const float* __restrict__ nstiff, const int* __restrict__ work,
+	const CmState* __restrict__ st, CmMaterial M, float strength, float4* __restrict__ out_pos,
+	float* __restrict__ out_time)
+{
+	const int cnt = st->work;
+	const bool dense = st->dense != 0;
+	const int stride = gridDim.x * blockDim.x;
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += stride) {
+		const int i = dense ? k : work[k];
+		const float4 e4 = ld4(pos, i);
+		const float2 me = td[i];
+		const float edens = me.y, tcur = me.x;
+		float best_time = tcur, best_dist = 0.0f, best_dens = 0.0f;
+		int best = -1;
+		const int e0 = off[i], e1 = off[i + 1];
+		for (int e = e0; e < e1; ++e) {
+			const int j = __ldg(nbr + e);
+			const float2 o = td[j];
+			const float cand = o.x + cm_link_time(edens, o.y);
+			if (cand < best_time) { best_time = cand; best = j; best_dist = __ldg(ndist + e); best_dens = o.y; }
+		}
+		float4 out = e4;
+		if (best >= 0 && best_time < tcur) {
+			float stiff = 1.0f;
+			for (int e = e0; e < e1; ++e)
+				if (__ldg(nbr + e) == best) { stiff = __ldg(nstiff + e); break; }
+			const float3 epos = f3(e4);
+			const float3 corr = cm_correction(M, epos, f3(ld4(pos, best)), best_dist, best_dens, stiff);
+			if (len3(corr) > 0.0f) {
+				const float3 o = add3(epos, mul3(corr, strength));
+				out = make_float4(o.x, o.y, o.z, e4.w);
+			}
+		}
+		out_pos[k] = out;
+		out_time[k] = best_time;
+	}
+}
+
+// Writes back the entries whose arrival time dropped, flags them for the next sweep and
+// clears the work-list marks.
+__global__ void __launch_bounds__(kBlock) k_cm_commit(int n, float4* __restrict__ pos, float2* __restrict__ td,
+	const int* __restrict__ work, const float4* __restrict__ out_pos, const float* __restrict__ out_time,
+	unsigned char* __restrict__ flag, unsigned int* __restrict__ mark, CmState* __restrict__ st)
+{
+	const int cnt = st->work;
+	const bool dense = st->dense != 0;
+	const int lane = threadIdx.x & 31;
+	const int stride = gridDim.x * blockDim.x;
+	for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cnt; base += stride) {
+		const int k = base + lane;
+		bool improved = false;
+		if (k < cnt) {
+			const int i = dense ? k : work[k];
+			if (!dense) atomicAnd(mark + (i >> 5), ~(1u << (i & 31)));
+			const float t = out_time[k];
+			if (t < td[i].x) {
+				pos[i] = out_pos[k];
+				td[i].x = t;
+				flag[i] = 1;
+				improved = true;
+			}
+		}
+		const unsigned int fm = __ballot_sync(0xffffffffu, improved);
+		if (fm && lane == 0) atomicAdd(&st->pending, __popc(fm));
+	}
+}
+
+// chainmailRelaxKernel (forward.cu:5466-5559): every Gaussian toward the rest lengths of
+// its edges, mean correction clamped to 1.5 x the mean rest length, stiffness, damping.
+__global__ void __launch_bounds__(kBlock) k_cm_relax(int n, const float4* __restrict__ pin, float4* __restrict__ pout,
+	const float2* __restrict__ td, const int* __restrict__ off, const int* __restrict__ nbr,
+	const float* __restrict__ ndist, const float* __restrict__ nstiff, CmMaterial M, float stiffness, float damping)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 e4 = ld4(pin, i);
+	const float3 epos = f3(e4);
+	const float etol = cm_axis_tol(M, td[i].y);
+	float3 acc = make_float3(0.0f, 0.0f, 0.0f);
+	int corr_count = 0, dist_count = 0;
+	float sum_target = 0.0f;
+	const int e0 = off[i], e1 = off[i + 1];
+	for (int e = e0; e < e1; ++e) {
+		const int j = __ldg(nbr + e);
+		const float3 npos = f3(ld4(pin, j));
+		const float ntol = cm_axis_tol(M, td[j].y);
+		const float edge_scale = cm_edge_scale(M, __ldg(nstiff + e));
+		const float targ = __ldg(ndist + e);
+		const float tol = (0.0000001f * (etol + ntol)) / edge_scale;
+		const float3 dir = sub3(npos, epos);
+		const float len = len3(dir);
+		if (len < 1e-6f) continue;
+		const float inv_len = 1.0f / len;
+		const float3 nd = mul3(dir, inv_len);
+		if (len < targ - tol) {
+			acc = sub3(acc, mul3(nd, ((targ - tol) - len) * edge_scale));
+			corr_count++;
+		}
+		else if (len > targ + tol) {
+			acc = add3(acc, mul3(nd, (len - (targ + tol)) * edge_scale));
+			corr_count++;
+		}
+		sum_target += targ;
+		dist_count++;
+	}
+	if (corr_count > 0) {
+		float3 avg = mul3(acc, 1.0f / (float)corr_count);
+		float max_step = 0.6f;
+		if (dist_count > 0) max_step = 1.5f * (sum_target / (float)dist_count);
+		const float cl = len3(avg);
+		if (cl > 1e-6f && cl > max_step) avg = mul3(avg, max_step / cl);
+		const float3 corrected = add3(epos, mul3(avg, stiffness));
+		const float3 o = add3(epos, mul3(sub3(corrected, epos), 1.0f - damping));
+		pout[i] = make_float4(o.x, o.y, o.z, e4.w);
+	}
+	else {
+		pout[i] = e4;
+	}
+}
+
+// arrival times (caller order) and the caller-order position mirror after a run
+__global__ void __launch_bounds__(kBlock) k_cm_publish(int n, const float4* __restrict__ pos,
+	const float2* __restrict__ td, const int* __restrict__ perm, float* __restrict__ pos_out3,
+	float* __restrict__ time_out)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const int o = perm ? perm[i] : i;
+	const float4 p = pos[i];
+	if (pos_out3) { pos_out3[3 * (size_t)o] = p.x; pos_out3[3 * (size_t)o + 1] = p.y; pos_out3[3 * (size_t)o + 2] = p.z; }
+	if (time_out) time_out[o] = td[i].x;
+}
+
 }  // namespace dev
 }  // namespace xpbd

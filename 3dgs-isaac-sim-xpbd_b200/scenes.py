@@ -215,3 +215,42 @@ def large_scene_scenario(n=1_000_000, seed=0, **kw):
 def bbox_diagonal(pos):
     p = np.asarray(pos, dtype=np.float64)
     return float(np.linalg.norm(p.max(0) - p.min(0)))
+
+
+# ---------------------------------------------------------------------------
+# ChainMail workload (forward.cu:12808-13006): a displacement wave from seeds
+# ---------------------------------------------------------------------------
+CHAINMAIL_DEFAULTS = dict(prop_iters=20, relax_iters=5, prop_strength=0.5, relax_stiffness=0.99,
+                          relax_damping=0.1)   # the reference's tunables (forward.cu:60-64)
+
+
+def chainmail_scene(n=4000, seed=21):
+    """The config-0 ellipsoid with opacity uniform in [0.02, 1): densities fall in all four
+    ChainMail classes (air < 0.13 <= skin < 0.45 <= 0.75 <= bone, forward.h:63-65)."""
+    sc = make_scene(n, seed)
+    sc["opacity"] = np.random.default_rng(seed + 7).uniform(0.02, 1.0, n).astype(np.float32)
+    return sc
+
+
+def chainmail_script(solver, sc, record, push=1.0):
+    """Create, one solver step (graph upload), reset to rest; then two waves:
+    run 1 — 30 seeds at the -x end pushed +0.02 x, the reference's default sweeps;
+    run 2 — 15 seeds at the +x end pushed (-0.015, 0.005, 0), other material constants,
+    3 propagation + 2 relax sweeps (the first wave is still travelling).
+    ``record(tag)`` is called after each run; ``push`` scales both seed displacements."""
+    solver.create(sc)
+    solver.step()
+    solver.reset()
+    pos = sc["pos"].astype(np.float64)
+    left = np.argsort(np.linalg.norm(pos - np.array([-0.9, 0.0, 0.0]), axis=1), kind="stable")[:30]
+    right = np.argsort(np.linalg.norm(pos - np.array([0.9, 0.0, 0.0]), axis=1), kind="stable")[:15]
+    solver.chainmail_set_material()
+    solver.chainmail_seed(left, np.tile(np.float32([0.02 * push, 0.0, 0.0]), (len(left), 1)))
+    solver.chainmail_run(**CHAINMAIL_DEFAULTS)
+    record("run1")
+    solver.chainmail_set_material(2.0, 0.2, 0.05, 0.02, True, 0.5)
+    solver.chainmail_seed(right, np.tile(np.float32([-0.015 * push, 0.005 * push, 0.0]), (len(right), 1)))
+    solver.chainmail_run(3, 2, 0.5, 0.99, 0.1)
+    record("run2")
+    solver.chainmail_set_material()
+

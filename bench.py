@@ -6,7 +6,7 @@ capsule grippers pulling apart while twisting; one bench "step" is one 60 Hz fra
 10 solver substeps x 4 iterations.  Metric: Gaussian-substeps per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config large|plain|batched|served] [--gaussians N]
+                  [--config large|plain|batched|served|chainmail] [--gaussians N]
 
 value     device-resident throughput: frames enqueued through the library's async API,
           timed with CUDA events on the engine's stream (pins/colliders re-posed per
@@ -340,6 +340,112 @@ def bench_batched(args, rank, world):
             "speedup_vs_plain": plain_s / batched_s}
 
 
+def chainmail_seeds(scen_pos, k):
+    """Step k's seeds: the 30 Gaussians nearest one x end (alternating), pushed inward by
+    about one graph spacing."""
+    side = -1.0 if k % 2 == 0 else 1.0
+    d = np.linalg.norm(scen_pos - np.array([0.9 * side, 0.0, 0.0]), axis=1)
+    idx = np.argpartition(d, 30)[:30].astype(np.int32)
+    delta = np.tile(np.float32([-0.005 * side, 0.0, 0.0]), (30, 1))
+    return idx, delta
+
+
+def bench_chainmail(args, rank, world):
+    """ChainMail on the large scene: one step = seeds + one run of the reference's default
+    sweeps (20 propagation + 5 relax + 1 closing relax, forward.cu:60-64, 12808-13006)."""
+    import torch
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    n = args.gaussians or 1_000_000
+    sc = scenes.chainmail_scene(n, 0)
+    pos64 = sc["pos"].astype(np.float64)
+    x = pkg.XPBD()
+    bind_ext(x.lib)
+    L = x.lib
+    stream = torch.cuda.Stream()
+    L.xpbd_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    x.create(sc)
+    x.step()
+    x.reset()
+    cm = scenes.CHAINMAIL_DEFAULTS
+    sweeps = cm["prop_iters"] + cm["relax_iters"] + 1
+    seeds = [chainmail_seeds(pos64, k) for k in range(args.warmup + args.steps)]
+    for k in range(args.warmup):
+        x.chainmail_seed(*seeds[k])
+        x.chainmail_run(**cm)
+    launches0 = L.xpbd_b200_launch_count()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.warmup, args.warmup + args.steps):
+        x.chainmail_seed(*seeds[k])
+        x.chainmail_run(**cm)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = L.xpbd_b200_launch_count() - launches0
+    # the dense relax sweep alone (the dominant kernel): 1 + r sweeps per call
+    r = 20
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    x.chainmail_run(0, r - 1, 0.5, 0.99, 0.1)
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    relax_ms = ev2.elapsed_time(ev3) / r
+    sizes = np.zeros(10, np.int64)
+    L.xpbd_b200_sizes(sizes.ctypes.data)
+    d = sizes[1] / n
+    relax_bytes = (44 + 12 * d) * n          # pos in/out, (time, density), row offsets; nbr, rest, stiffness per edge
+    peak, peak_kind = peaks()
+    achieved = relax_bytes / (relax_ms / 1e3) / 1e9
+    # e2e: blocking C ABI on the library's own stream, seeds from host, positions read back per step
+    L.xpbd_b200_set_stream(None)
+    e2e_steps = min(args.steps, 5)
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        x.chainmail_seed(*seeds[k])
+        x.chainmail_run(**cm)
+        x.positions()
+    e2e_s = time.perf_counter() - t0
+    x.destroy()
+    unit = "Gaussian-sweeps/s"
+    line = {
+        "metric": "ChainMail Gaussian-sweeps/s at 1M Gaussians", "value": n * sweeps * args.steps / (ms / 1e3),
+        "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid scene, opacity uniform in [0.02, 1))",
+        "config": {"workload": f"chainmail: {n} Gaussians, 30 seeds per step, 20 propagation + 6 relax sweeps",
+                   "n_gaussians": n, "sweeps_per_step": sweeps, "l2": "inputs larger than L2"},
+        "e2e": {"value": n * sweeps * e2e_steps / e2e_s, "unit": unit, "h2d_bytes_per_step": 30 * 16,
+                "d2h_bytes_per_step": n * 12, "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "chainmail_relax", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": relax_bytes, "mean_launch_ms": relax_ms},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        lib = os.path.join(ROOT, "oracle", "liboracle.so")
+        o = pkg.bridge.XPBD(lib)
+        o.lib.oracle_get_threads.restype = ctypes.c_int
+        o.create(sc)
+        o.step()
+        o.reset()
+        k = 2
+        t1 = time.perf_counter()
+        for j in range(k):
+            o.chainmail_seed(*seeds[j])
+            o.chainmail_run(**cm)
+        dt = time.perf_counter() - t1
+        line["cpu_baseline"] = {"value": n * sweeps * k / dt, "unit": unit, "cores": int(o.lib.oracle_get_threads()),
+                                "kind": "port", "sample": f"{k} steps of the same {n}-Gaussian workload"}
+        o.destroy()
+    return line
+
+
 def bench_served(args, rank, world):
     """Poisson session arrivals served with continuous batching, against one session at a
     time.  Arrival rate and sizes are scaled to what the host-side topology build admits
@@ -397,7 +503,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served"])
+    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gaussians", type=int, default=None,
@@ -421,6 +527,8 @@ def main():
             line = bench_batched(args, rank, world)
         elif args.config == "served":
             line = bench_served(args, rank, world)
+        elif args.config == "chainmail":
+            line = bench_chainmail(args, rank, world)
         else:
             line = bench_b200(args, rank, world)
         if line is not None:

@@ -110,6 +110,25 @@ XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd);
 
 /* ---- extensions (no counterpart in the reference ABI) ------------------- */
 
+/* ChainMail displacement propagation (runChainmailGPU, forward.cu:12808-13006; the
+ * reference's C ABI cannot reach it because xpbd_create forces XPBD mode,
+ * xpbd_capi.cu:98).  Material constants as setChainmailMaterialParams
+ * (forward.cu:4844-4858). */
+XPBD_API void xpbd_b200_chainmail_set_material(float global_scale, float air, float skin, float bone,
+	int use_edge_stiffness, float edge_influence);
+/* Seeds start a wave: Gaussian idx[k] moves by delta[3k..3k+2] and its arrival time
+ * becomes 0 (applySeedCommandsKernel, forward.cu:5907-5924), in order.  After a step. */
+XPBD_API int xpbd_b200_chainmail_seed(int count, const int* idx, const float* delta);
+/* prop_iters propagation sweeps, relax_iters relax sweeps and one closing relax sweep on
+ * the current positions (the reference's dense path; its defaults 20, 5, 0.5, 0.99, 0.1). */
+XPBD_API int xpbd_b200_chainmail_run(int prop_iters, int relax_iters, float prop_strength, float relax_stiffness,
+	float relax_damping);
+/* Propagation sweeps on work lists of the Gaussians next to the last sweep's changes (1,
+ * default) or over every Gaussian (0).  The results are identical. */
+XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled);
+/* Arrival times (caller order; 1e9 where the wave has not arrived); returns N or -1. */
+XPBD_API int xpbd_b200_chainmail_times(float* out, int n);
+
 /* Independent solver instances: a new engine (own scene, settings and stream), its
  * release, and the choice of the engine that the reference entry points above act on
  * from the calling thread (NULL: the process-wide default engine). */

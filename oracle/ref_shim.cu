@@ -145,6 +145,7 @@ __attribute__((visibility("default"))) int refshim_float(const char* name, float
 	if (s == "pos_next") return copy_out(reinterpret_cast<const float*>(d_pos_next), 3LL * N, out, cap);
 	if (s == "inv_mass") return copy_out(d_invMass, N, out, cap);
 	if (s == "cluster_coef") return copy_out(d_volClusterCoef, N, out, cap);
+	if (s == "cm_time") return copy_out(d_time_curr, N, out, cap);
 	if (s == "self_col") {
 		// [0] spacing, [1] contact distance d_c, [2] cell size (reach)
 		if (!out) return 3;
@@ -155,6 +156,54 @@ __attribute__((visibility("default"))) int refshim_float(const char* name, float
 		return 3;
 	}
 	return -1;
+}
+
+// ChainMail (forward.cu:12808-13006): not reachable through xpbd_capi.cu, which forces
+// XPBD mode (xpbd_capi.cu:98).  These drive the reference's own seed kernel and its
+// runChainmailGPU on the graph a first xpbd_step uploaded.
+__attribute__((visibility("default"))) void refshim_chainmail_set_material(float global_scale, float air, float skin,
+	float bone, int use_edge_stiffness, float edge_influence)
+{
+	FORWARD::setChainmailMaterialParams(global_scale, air, skin, bone, use_edge_stiffness != 0, edge_influence);
+}
+
+// applySeedCommandsKernel (forward.cu:5907-5924): seeds move by delta, arrival time 0.
+__attribute__((visibility("default"))) int refshim_chainmail_seed(int count, const int* idx, const float* delta)
+{
+	const int N = cm_num_elements;
+	if (N <= 0 || !d_pos_curr || !d_time_curr || count < 0) return -1;
+	if (count == 0) return 0;
+	int* di = nullptr;
+	float3* dd = nullptr;
+	cudaMalloc(&di, sizeof(int) * count);
+	cudaMalloc(&dd, sizeof(float3) * count);
+	cudaMemcpy(di, idx, sizeof(int) * count, cudaMemcpyHostToDevice);
+	cudaMemcpy(dd, delta, sizeof(float3) * count, cudaMemcpyHostToDevice);
+	applySeedCommandsKernel<<<(count + 255) / 256, 256>>>(count, di, dd, d_pos_curr, d_time_curr, (int*)nullptr);
+	cudaDeviceSynchronize();
+	cudaFree(di);
+	cudaFree(dd);
+	return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// runChainmailGPU's dense path (no active map, no inertia: the reference defaults,
+// forward.cu:47 and 73).  Its ChainMail argument only supplies the element count here
+// (no host upload or download), so a placeholder with N elements is passed.
+__attribute__((visibility("default"))) int refshim_chainmail_run(int prop_iters, int relax_iters, float prop_strength,
+	float relax_stiffness, float relax_damping)
+{
+	const int N = cm_num_elements;
+	if (N <= 0 || !d_pos_curr || !d_time_curr) return -1;
+	static FORWARD::ChainMail placeholder;
+	if ((int)placeholder.numElements() != N)
+		placeholder.loadGraph(placeholder, std::vector<FORWARD::Pos>(N, FORWARD::Pos(0.0f)), std::vector<FORWARD::Edge>(),
+			std::vector<float>(N, 0.0f));
+	g_useActiveMap = false;
+	g_cmInertiaGain = 0.0f;
+	runChainmailGPU(placeholder, prop_iters, relax_iters, prop_strength, relax_stiffness, relax_damping, false, false,
+		nullptr);
+	cudaDeviceSynchronize();
+	return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 }  // extern "C"

@@ -279,6 +279,8 @@ static struct {
 	int obj_k;
 	/* J stats */
 	float jvw_mean, jvw_std;
+	/* ChainMail arrival times (forward.cu:3542; 1e9 = not reached, forward.cu:2717) */
+	float *cm_time, *cm_time_next;
 } S;
 
 /* parameters: file statics of forward.cu with their defaults (forward.cu:53-92, 224-265, 300-361) */
@@ -327,7 +329,7 @@ static void free_state(void)
 {
 	FREE(S.off); FREE(S.cnt); FREE(S.nbr); FREE(S.ndist); FREE(S.nstiff);
 	FREE(S.pos_curr); FREE(S.pos_next); FREE(S.pos_tmp); FREE(S.pos_rest); FREE(S.vel);
-	FREE(S.inv_mass); FREE(S.density); FREE(S.lam_a); FREE(S.lam_b);
+	FREE(S.inv_mass); FREE(S.density); FREE(S.lam_a); FREE(S.lam_b); FREE(S.cm_time); FREE(S.cm_time_next);
 	FREE(S.vol_off); FREE(S.vol_cnt); FREE(S.vol_idx); FREE(S.rev_off); FREE(S.rev_cnt); FREE(S.rev_idx);
 	FREE(S.sigma_rest); FREE(S.det_rest); FREE(S.v_rest); FREE(S.rest_len); FREE(S.lam_vol); FREE(S.mat_type);
 	FREE(S.cl_c); FREE(S.cl_sinv); FREE(S.cl_coef); FREE(S.vol_gs_order); FREE(S.vol_gs_color_off);
@@ -843,6 +845,9 @@ static void ensure_built(void)
 		S.inv_mass[i] = 1.0f;
 		S.density[i] = S.opacity[i];
 	}
+	S.cm_time = malloc(sizeof(float) * N);
+	S.cm_time_next = malloc(sizeof(float) * N);
+	for (int i = 0; i < N; ++i) S.cm_time[i] = 1e9f;
 	const int M = S.m > 0 ? S.m : 1;
 	S.lam_a = calloc(M, sizeof(float));
 	S.lam_b = calloc(M, sizeof(float));
@@ -2712,6 +2717,211 @@ EXPORT int oracle_float(const char* name, float* out, long long cap)
 		return 3;
 	}
 	return -1;
+}
+
+/* ------------------------------------------------------------------------- */
+/* ChainMail displacement propagation (runChainmailGPU, forward.cu:12808-13006, */
+/* the dense path: no active map, no inertia)                                 */
+/* ------------------------------------------------------------------------- */
+/* material controls (forward.cu:66-71 defaults, setChainmailMaterialParams 4844-4858) */
+static struct {
+	float global, air, skin, bone, influence;
+	int use_edge;
+} CM = { 1.0f, 0.1f, 0.1f, 0.1f, 1.0f, 1 };
+
+#define CM_AIR 0.13f   /* forward.h:63-65 */
+#define CM_SKIN 0.45f
+#define CM_BONE 0.75f
+
+/* cm_getConstraint (forward.cu:5221-5264): the axis tolerance of a density class */
+static float cm_axis_tol(float density)
+{
+	float c;
+	if (density < CM_AIR) c = CM.air;
+	else if (density < CM_SKIN) c = CM.skin;
+	else c = CM.bone;
+	const float scale = fmaxf(1e-4f, CM.global);
+	return c * scale;
+}
+
+/* cm_edgeScaleFromStiff (forward.cu:5266-5278) */
+static float cm_edge_scale(float stiff)
+{
+	if (!CM.use_edge || CM.influence <= 0.0f) return 1.0f;
+	const float s = fminf(fmaxf(stiff, 0.05f), 1.0f);
+	const float t = (s - 0.05f) / 0.95f;
+	const float scale = 1.0f + CM.influence * (t * 2.0f - 1.0f);
+	return fminf(fmaxf(scale, 0.1f), 4.0f);
+}
+
+/* cm_propagationTime (forward.cu:5280-5293) */
+static float cm_link_time(float d0, float d1)
+{
+	float et, nt;
+	if (d0 < CM_AIR) et = 1.0f;
+	else if (d0 < CM_SKIN) et = 0.3f;
+	else if (d0 < CM_BONE) et = 0.05f;
+	else et = 0.005f;
+	if (d1 < CM_AIR) nt = 1.0f;
+	else if (d1 < CM_SKIN) nt = 0.3f;
+	else if (d1 < CM_BONE) nt = 0.05f;
+	else nt = 0.005f;
+	return (et + nt) * 0.5f;
+}
+
+/* cm_correctionFromNeighbor (forward.cu:5295-5330) */
+static f3 cm_correction(f3 epos, f3 npos, float targ, float ndens, float stiff)
+{
+	const float dx = cm_axis_tol(ndens);
+	const float edge_scale = cm_edge_scale(stiff);
+	const f3 dir = f3_sub(epos, npos);
+	const float len = f3_len(dir);
+	if (len < 1e-6f) return mk3(0.0f, 0.0f, 0.0f);
+	const float inv_len = 1.0f / len;
+	const f3 nd = f3_mul(dir, inv_len);
+	if (len < targ - dx) {
+		const float delta = (targ - dx) - len;
+		return f3_mul(nd, delta * edge_scale);
+	}
+	if (len > targ + dx) {
+		const float delta = len - (targ + dx);
+		return f3_mul(nd, -(delta * edge_scale));
+	}
+	return mk3(0.0f, 0.0f, 0.0f);
+}
+
+/* chainmailPropagateKernelBest (forward.cu:5396-5464): the fastest neighbour only */
+static void cm_propagate(const f3* pin, f3* pout, const float* tin, float* tout, float strength)
+{
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+	for (int i = 0; i < S.n; ++i) {
+		const f3 epos = pin[i];
+		const float edens = S.density[i];
+		const float tcur = tin[i];
+		float best_time = tcur, best_dist = 0.0f, best_dens = 0.0f;
+		int best = -1;
+		const int off = S.off[i], cnt = S.cnt[i];
+		for (int k = 0; k < cnt; ++k) {
+			const int j = S.nbr[off + k];
+			const float nd = S.density[j];
+			const float cand = tin[j] + cm_link_time(edens, nd);
+			if (cand < best_time) { best_time = cand; best = j; best_dist = S.ndist[off + k]; best_dens = nd; }
+		}
+		f3 out = epos;
+		if (best >= 0 && best_time < tcur) {
+			float stiff = 1.0f;
+			for (int k = 0; k < cnt; ++k)
+				if (S.nbr[off + k] == best) { stiff = S.nstiff[off + k]; break; }
+			const f3 corr = cm_correction(epos, pin[best], best_dist, best_dens, stiff);
+			if (f3_len(corr) > 0.0f) out = f3_add(epos, f3_mul(corr, strength));
+		}
+		pout[i] = out;
+		tout[i] = best_time;
+	}
+}
+
+/* chainmailRelaxKernel (forward.cu:5466-5559) */
+static void cm_relax(const f3* pin, f3* pout, float stiffness, float damping)
+{
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+	for (int i = 0; i < S.n; ++i) {
+		const f3 epos = pin[i];
+		const float etol = cm_axis_tol(S.density[i]);
+		f3 acc = mk3(0.0f, 0.0f, 0.0f);
+		int corr_count = 0, dist_count = 0;
+		float sum_target = 0.0f;
+		const int off = S.off[i], cnt = S.cnt[i];
+		for (int k = 0; k < cnt; ++k) {
+			const int j = S.nbr[off + k];
+			const f3 npos = pin[j];
+			const float ntol = cm_axis_tol(S.density[j]);
+			const float edge_scale = cm_edge_scale(S.nstiff[off + k]);
+			const float targ = S.ndist[off + k];
+			const float tol = (0.0000001f * (etol + ntol)) / edge_scale;
+			const f3 dir = f3_sub(npos, epos);
+			const float len = f3_len(dir);
+			if (len < 1e-6f) continue;
+			const float inv_len = 1.0f / len;
+			const f3 nd = f3_mul(dir, inv_len);
+			if (len < targ - tol) {
+				const float delta = (targ - tol) - len;
+				acc = f3_sub(acc, f3_mul(nd, delta * edge_scale));
+				corr_count++;
+			}
+			else if (len > targ + tol) {
+				const float delta = len - (targ + tol);
+				acc = f3_add(acc, f3_mul(nd, delta * edge_scale));
+				corr_count++;
+			}
+			sum_target += targ;
+			dist_count++;
+		}
+		if (corr_count > 0) {
+			f3 avg = f3_mul(acc, 1.0f / (float)corr_count);
+			float max_step = 0.6f;
+			if (dist_count > 0) max_step = 1.5f * (sum_target / (float)dist_count);
+			const float cl = f3_len(avg);
+			if (cl > 1e-6f && cl > max_step) avg = f3_mul(avg, max_step / cl);
+			const f3 corrected = f3_add(epos, f3_mul(avg, stiffness));
+			pout[i] = f3_add(epos, f3_mul(f3_sub(corrected, epos), 1.0f - damping));
+		}
+		else {
+			pout[i] = epos;
+		}
+	}
+}
+
+EXPORT void oracle_chainmail_set_material(float global_scale, float air, float skin, float bone, int use_edge_stiffness,
+	float edge_influence)
+{
+	CM.global = fmaxf(1e-4f, global_scale);
+	CM.air = fmaxf(1e-4f, air);
+	CM.skin = fmaxf(1e-4f, skin);
+	CM.bone = fmaxf(1e-4f, bone);
+	CM.use_edge = use_edge_stiffness != 0;
+	CM.influence = fmaxf(0.0f, edge_influence);
+}
+
+/* applySeedCommandsKernel (forward.cu:5907-5924): seeds move by delta and start the wave
+ * (arrival time 0); applied in order */
+EXPORT int oracle_chainmail_seed(int count, const int* idx, const float* delta)
+{
+	if (!S.stepped) return fail("oracle_chainmail_seed: no step yet");
+	if (count < 0 || (count > 0 && (!idx || !delta))) return fail("oracle_chainmail_seed: invalid arguments");
+	for (int k = 0; k < count; ++k)
+		if (idx[k] < 0 || idx[k] >= S.n) return fail("oracle_chainmail_seed: index out of range");
+	for (int k = 0; k < count; ++k) {
+		const int id = idx[k];
+		S.pos_curr[id] = f3_add(S.pos_curr[id], mk3(delta[3 * k], delta[3 * k + 1], delta[3 * k + 2]));
+		S.cm_time[id] = 0.0f;
+	}
+	return 0;
+}
+
+/* runChainmailGPU dense path (forward.cu:12901-12999): prop_iters propagation sweeps,
+ * relax_iters relax sweeps, then one more relax sweep */
+EXPORT int oracle_chainmail_run(int prop_iters, int relax_iters, float prop_strength, float relax_stiffness,
+	float relax_damping)
+{
+	if (!S.stepped) return fail("oracle_chainmail_run: no step yet");
+	if (prop_iters < 0 || relax_iters < 0) return fail("oracle_chainmail_run: negative iteration count");
+	for (int it = 0; it < prop_iters; ++it) {
+		cm_propagate(S.pos_curr, S.pos_next, S.cm_time, S.cm_time_next, prop_strength);
+		f3* t = S.pos_curr; S.pos_curr = S.pos_next; S.pos_next = t;
+		float* u = S.cm_time; S.cm_time = S.cm_time_next; S.cm_time_next = u;
+	}
+	for (int it = 0; it <= relax_iters; ++it) {
+		cm_relax(S.pos_curr, S.pos_next, relax_stiffness, relax_damping);
+		f3* t = S.pos_curr; S.pos_curr = S.pos_next; S.pos_next = t;
+	}
+	return 0;
+}
+
+EXPORT int oracle_chainmail_times(float* out, int n)
+{
+	if (!S.built || !out || n < S.n) return fail("oracle_chainmail_times: invalid arguments");
+	memcpy(out, S.cm_time, sizeof(float) * S.n);
+	return S.n;
 }
 
 EXPORT int oracle_selfcol_build(const float* x, const float* p)

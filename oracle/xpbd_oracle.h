@@ -43,6 +43,14 @@ int oracle_float(const char* name, float* out, long long cap);
 void oracle_sizes(long long* out);
 /* The once-per-step self-collision build on given start / predicted positions. */
 int oracle_selfcol_build(const float* x, const float* p);
+/* ChainMail propagation (forward.cu:12808-13006, dense path): material controls,
+ * seeds (move + arrival time 0), prop_iters + relax_iters + 1 sweeps, arrival times. */
+void oracle_chainmail_set_material(float global_scale, float air, float skin, float bone, int use_edge_stiffness,
+	float edge_influence);
+int oracle_chainmail_seed(int count, const int* idx, const float* delta);
+int oracle_chainmail_run(int prop_iters, int relax_iters, float prop_strength, float relax_stiffness,
+	float relax_damping);
+int oracle_chainmail_times(float* out, int n);
 
 #ifdef __cplusplus
 }

@@ -177,6 +177,19 @@ def misc_case(ref):
     return out
 
 
+def chainmail_case(ref):
+    """ChainMail waves through the reference's runChainmailGPU (forward.cu:12808-13006)."""
+    sc = scenes.chainmail_scene(4000, 21)
+    out = scene_arrays(sc)
+
+    def record(tag):
+        out[f"pos_{tag}"] = ref.positions()
+        out[f"time_{tag}"] = ref.chainmail_times()
+
+    scenes.chainmail_script(ref, sc, record)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -184,7 +197,7 @@ def main():
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     names = ["graph_n3000_r1", "graph_n3000_r2", "graph_n3000_k1", "plain_n4000", "plain_n4000_k1",
-             "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000"]
+             "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000", "chainmail_n4000"]
     if not args.only:
         # One process per case: the reference keeps its solver state in file-static globals.
         import subprocess
@@ -210,6 +223,7 @@ def main():
         "plain_n20000": lambda: scenario_case(ref, scenes.plain_scene_scenario(20000, 0), [1, 100, 1000]),
         "selfcol_blobs": lambda: selfcol_case(ref),
         "misc_n2000": lambda: misc_case(ref),
+        "chainmail_n4000": lambda: chainmail_case(ref),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only.split(","):

@@ -197,6 +197,58 @@ def test_positions_device_pointer(lib):
     np.testing.assert_array_equal(host, lib.positions())
 
 
+def _chainmail_run(solver, sc, push=1.0):
+    res = {}
+
+    def record(tag):
+        res[tag] = (solver.positions(), solver.chainmail_times())
+    H.scenes.chainmail_script(solver, sc, record, push)
+    return res
+
+
+def test_chainmail_matches_reference(lib):
+    """ChainMail frontier sweeps against the reference's dense sweeps: arrival times
+    bit-exact, positions within the 1-step tolerance."""
+    g = H.load_golden("chainmail_n4000")
+    res = _chainmail_run(lib, H.golden_scene(g))
+    diag = H.scenes.bbox_diagonal(g["pos_run1"])
+    for tag in ("run1", "run2"):
+        pos, t = res[tag]
+        np.testing.assert_array_equal(t, g[f"time_{tag}"])
+        assert H.max_err_over_diag(pos, g[f"pos_{tag}"], diag) < H.TOL_1STEP
+
+
+def test_chainmail_frontier_equals_dense(lib):
+    """Work-list sweeps touch only the Gaussians next to the last sweep's changes; the
+    others would write their input back, so the result is the dense sweeps' bit for bit."""
+    import ctypes
+    lib.lib.xpbd_b200_chainmail_set_frontier.argtypes = [ctypes.c_int]
+    sc = H.scenes.chainmail_scene(200000, 5)
+    out = []
+    for frontier in (1, 0):
+        lib.lib.xpbd_b200_chainmail_set_frontier(frontier)
+        out.append(_chainmail_run(lib, sc, push=0.25))
+    lib.lib.xpbd_b200_chainmail_set_frontier(1)
+    for tag in ("run1", "run2"):
+        np.testing.assert_array_equal(out[0][tag][1], out[1][tag][1])
+        np.testing.assert_array_equal(out[0][tag][0], out[1][tag][0])
+    assert (out[0]["run1"][1] < 1e8).sum() > 1000
+
+
+def test_chainmail_large_scene_matches_oracle(lib):
+    """200,000 Gaussians, seeds pushed by about one spacing: arrival times bit-exact and
+    positions within the 1-step tolerance of the oracle's dense sweeps."""
+    sc = H.scenes.chainmail_scene(200000, 5)
+    got = _chainmail_run(lib, sc, push=0.25)
+    orc = H.oracle()
+    want = _chainmail_run(orc, sc, push=0.25)
+    orc.destroy()
+    diag = H.scenes.bbox_diagonal(sc["pos"])
+    for tag in ("run1", "run2"):
+        np.testing.assert_array_equal(got[tag][1], want[tag][1])
+        assert H.max_err_over_diag(got[tag][0], want[tag][0], diag) < H.TOL_1STEP
+
+
 def test_error_behaviour(lib):
     lib.destroy()
     assert lib.lib.xpbd_step() == -1

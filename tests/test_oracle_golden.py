@@ -156,3 +156,26 @@ def test_error_behaviour(orc):
     with pytest.raises(RuntimeError, match="size mismatch"):
         orc._check(orc.lib.xpbd_positions_host(np.zeros(3, np.float32), 1), "xpbd_positions_host")
     orc.destroy()
+
+
+def _chainmail_run(solver, sc):
+    res = {}
+
+    def record(tag):
+        res[tag] = (solver.positions(), solver.chainmail_times())
+    H.scenes.chainmail_script(solver, sc, record)
+    return res
+
+
+def test_chainmail_matches_reference(orc):
+    """ChainMail waves (runChainmailGPU, forward.cu:12808-13006): arrival times are sums and
+    comparisons only, so bit-exact; positions within the 1-step tolerance."""
+    g = H.load_golden("chainmail_n4000")
+    sc = H.golden_scene(g)
+    res = _chainmail_run(orc, sc)
+    diag = H.scenes.bbox_diagonal(g["pos_run1"])
+    for tag in ("run1", "run2"):
+        pos, t = res[tag]
+        np.testing.assert_array_equal(t, g[f"time_{tag}"])
+        assert H.max_err_over_diag(pos, g[f"pos_{tag}"], diag) < H.TOL_1STEP
+    assert (g["time_run1"] < 1e8).sum() > 1000   # the wave travelled
