@@ -161,6 +161,9 @@ class Scenario:
         solver.volume_stats(False)
         self.k = 0
 
+    def has_pins(self):
+        return any(len(g.idx) for g in self.grippers)
+
     def pins(self, t):
         if not self.grippers:
             return None, None
@@ -181,7 +184,7 @@ class Scenario:
             if self.grippers:
                 types, poses, dims = self.colliders(t)
                 solver.set_colliders(types, poses, dims, 0.0, 0.0)
-                if self.k > 0:
+                if self.k > 0 and self.has_pins():
                     idx, pos = self.pins(t)
                     solver.set_attached(idx, pos, 1.0)
             solver.step()
@@ -210,6 +213,44 @@ def large_scene_scenario(n=1_000_000, seed=0, **kw):
     kw.setdefault("self_collision", True)
     kw.setdefault("within_body", True)
     return Scenario(scene, grippers, **kw)
+
+
+class Plate:
+    """A box collider (type 1, half extents ``half``) whose inner face starts at height
+    ``face`` on the ``side`` (+1 above, -1 below) of the z axis and moves toward z = 0 by
+    ``speed`` per frame until it has travelled ``travel``; it pins nothing."""
+
+    def __init__(self, side, face, speed, travel, half=(1.6, 1.6, 0.05)):
+        self.side, self.face, self.speed, self.travel = float(side), float(face), float(speed), float(travel)
+        self.half = np.asarray(half, dtype=np.float32)
+        self.idx = np.zeros(0, np.int32)
+
+    def centre(self, t):
+        inner = self.face - min(self.speed * t, self.travel)
+        return np.array([0.0, 0.0, self.side * (inner + float(self.half[2]))])
+
+    def targets(self, t):
+        return np.zeros((0, 3), np.float32)
+
+    def collider(self, t):
+        return 1, np.concatenate([np.eye(3).reshape(-1), self.centre(t)]).astype(np.float32), self.half
+
+
+def dense_contact_scenario(n=4_000_000, seed=0, **kw):
+    """The dense-contact stress workload: 12-NN graph, 128-member clusters, two parallel
+    plates (box colliders) normal to the thinnest axis (z) closing at 0.005 per frame in
+    all (each plate 0.0025) until the gap is 40 % of the initial thickness, then holding;
+    self-collision on; 10 substeps x 20 iterations per frame."""
+    scene = kw.pop("scene", None) or make_scene(n, seed, knn=12)
+    z = scene["pos"][:, 2].astype(np.float64)
+    thick = float(z.max() - z.min())
+    travel = 0.5 * 0.6 * thick
+    plates = [Plate(+1.0, float(z.max()), 0.0025, travel), Plate(-1.0, float(-z.min()), 0.0025, travel)]
+    kw.setdefault("self_collision", True)
+    kw.setdefault("within_body", True)
+    kw.setdefault("iters", 20)
+    kw.setdefault("max_members", 128)
+    return Scenario(scene, plates, **kw)
 
 
 def bbox_diagonal(pos):

@@ -6,7 +6,8 @@ capsule grippers pulling apart while twisting; one bench "step" is one 60 Hz fra
 10 solver substeps x 4 iterations.  Metric: Gaussian-substeps per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config large|plain|batched|served|chainmail] [--gaussians N]
+                  [--config large|plain|batched|served|chainmail|dense]
+                  [--gaussians N]
 
 value     device-resident throughput: frames enqueued through the library's async API,
           timed with CUDA events on the engine's stream (pins/colliders re-posed per
@@ -48,6 +49,11 @@ ITERS = 4
 def workload(config, gaussians=None):
     """(name, scenario factory) of a single-scene workload; `gaussians` shrinks or grows
     the scene (profiler captures use a small case of the same workload)."""
+    if config == "dense":
+        n = gaussians or 4_000_000
+        return (f"dense contact: {n} Gaussians, 12-NN graph, 128-member clusters (k=3), shape matching, "
+                "self-collision, two plates closing 0.005 per frame, 10 substeps x 20 iterations"), \
+            lambda: scenes.dense_contact_scenario(n, 0)
     if config == "plain":
         n = gaussians or 20000
         return f"plain: {n} Gaussians, 2 pinned capsule grippers, 10 substeps x 4 iterations", \
@@ -137,7 +143,7 @@ def run_frames(solver, scen, frames, blocking):
             t = (scen.k + 1) / scen.substeps
             types, poses, dims = scen.colliders(t)
             solver.set_colliders(types, poses, dims, 0.0, 0.0)
-            if scen.k > 0:                             # pins need one step first (xpbd_capi.cu:169)
+            if scen.k > 0 and scen.has_pins():         # pins need one step first (xpbd_capi.cu:169)
                 idx, pos = scen.pins(t)
                 solver.set_attached(idx, pos, 1.0)
             if blocking:
@@ -246,10 +252,10 @@ def bench_b200(args, rank, world):
     achieved = (algo / (dom_ms / dom_cnt / 1e3) / 1e9) if algo else None
     traffic = traffic_estimate(dom_name, n)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric_for(args.config, n), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid scene; no public dataset)",
-        "config": {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": ITERS,
+        "config": {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": scen.iters,
                    "graph_edges_directed": int(sizes[1]), "cluster_members": int(sizes[2]),
                    "hash_table": int(sizes[8]), "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (working set > 2 GB per replica)"},
@@ -263,10 +269,48 @@ def bench_b200(args, rank, world):
         "stages_ms_per_step": {k2: v[0] / args.steps for k2, v in sorted(stages.items(), key=lambda kv: -kv[1][0])},
         "clocks": clk,
     }
+    line["residuals_fp64"] = residuals_fp64(x, scen)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, scen_maker=make)
     x.destroy()
     return line
+
+
+def metric_for(config, n):
+    if config == "large" and n == 1_000_000:
+        return METRIC
+    what = {"dense": "dense contact, 20 iterations", "plain": "plain scene"}.get(config, config)
+    return f"XPBD substeps/s at {n} Gaussians, {what} (Gaussian-substeps/s)"
+
+
+def residuals_fp64(x, scen):
+    """Constraint residuals of the final state evaluated in FP64 on the host: relative
+    distance error |l - l0| / l0 over every edge, and the volume ratio J over every
+    cluster (the reference's volume statistics, one more substep with them on)."""
+    pos = x.positions().astype(np.float64)
+    e = scen.scene["edges"]
+    rest = scen.scene["rest"].astype(np.float64)
+    ln = np.linalg.norm(pos[e[:, 0]] - pos[e[:, 1]], axis=1)
+    rel = np.abs(ln - rest) / np.maximum(rest, 1e-12)
+    x.volume_stats(True)
+    run_frames_substeps(x, scen, 1)
+    jm, js = x.volume_stats(True)
+    x.volume_stats(False)
+    return {"distance_rel_mean": float(rel.mean()), "distance_rel_p99": float(np.percentile(rel, 99)),
+            "distance_rel_max": float(rel.max()), "volume_J_mean": float(jm), "volume_J_std": float(js),
+            "note": "FP32 solver state, residuals in FP64"}
+
+
+def run_frames_substeps(solver, scen, count):
+    for _ in range(count):
+        t = (scen.k + 1) / scen.substeps
+        types, poses, dims = scen.colliders(t)
+        solver.set_colliders(types, poses, dims, 0.0, 0.0)
+        if scen.has_pins():
+            idx, pos = scen.pins(t)
+            solver.set_attached(idx, pos, 1.0)
+        solver.step()
+        scen.k += 1
 
 
 def traffic_estimate(stage, n):
@@ -503,7 +547,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail"])
+    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail", "dense"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gaussians", type=int, default=None,

@@ -249,6 +249,24 @@ def test_chainmail_large_scene_matches_oracle(lib):
         assert H.max_err_over_diag(got[tag][0], want[tag][0], diag) < H.TOL_1STEP
 
 
+def test_dense_contact_scenario_matches_oracle(lib):
+    """The dense-contact workload's settings at a small size: 12-NN graph, 128-member
+    clusters, 20 iterations, two closing box plates, self-collision."""
+    out = {}
+    orc = H.oracle()
+    for name, solver in (("b200", lib), ("oracle", orc)):
+        s = H.scenes.dense_contact_scenario(8000, 3)
+        s.setup(solver)
+        s.advance(solver, 1)
+        out[name, 1] = solver.positions()
+        s.advance(solver, 9)
+        out[name, 10] = solver.positions()
+    orc.destroy()
+    diag = H.scenes.bbox_diagonal(out["oracle", 1])
+    assert H.max_err_over_diag(out["b200", 1], out["oracle", 1], diag) < H.TOL_1STEP
+    assert H.max_err_over_diag(out["b200", 10], out["oracle", 10], diag) < H.TOL_100STEP
+
+
 def test_error_behaviour(lib):
     lib.destroy()
     assert lib.lib.xpbd_step() == -1

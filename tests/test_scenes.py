@@ -43,3 +43,19 @@ def test_gripper_motion():
     np.testing.assert_allclose(d0, d1, atol=1e-5)
     typ, pose, dims = gr.collider(10.0)
     assert typ == 2 and pose.shape == (12,) and dims[0] == 0.05
+
+
+def test_dense_contact_plates_close_then_hold():
+    s = H.scenes.dense_contact_scenario(3000, 1)
+    assert s.iters == 20 and s.max_members == 128 and s.self_collision
+    top, bottom = s.grippers
+    z = s.scene["pos"][:, 2]
+    thick = float(z.max() - z.min())
+    gap = lambda t: (top.centre(t)[2] - top.half[2]) - (bottom.centre(t)[2] + bottom.half[2])
+    assert abs(gap(0) - thick) < 1e-6
+    assert abs(gap(10) - (thick - 0.05)) < 1e-6            # 0.005 per frame
+    assert abs(gap(1000) - 0.4 * thick) < 1e-6             # stops at 40 %
+    assert not s.has_pins()
+    types, poses, dims = s.colliders(0.0)
+    assert list(types) == [1, 1] and poses.shape == (2, 12)
+
