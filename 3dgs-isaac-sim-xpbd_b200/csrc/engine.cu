@@ -803,6 +803,11 @@ public:
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_slots<8, 8, true>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+					else if (la == 4 && S.lanes_a == 0 && clusters.avg_members > 64.0f)
+						// more than 64 members: 8 lanes x 16 staged slots hold up to 128
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8, dev::kSmemBlock), dim3(dev::kSmemBlock),
+							dev::k_volume_solve_smem<8, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx.p,
+							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 4)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4, dev::kSmemBlock), dim3(dev::kSmemBlock),
 							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx.p,
