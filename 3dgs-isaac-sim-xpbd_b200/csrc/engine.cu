@@ -99,6 +99,7 @@ struct Settings {
 	int lanes_a = 0, lanes_b = 0;    // volume kernel lanes per cluster / node (0 = automatic)
 	dev::CmMaterial cm{ 1.0f, 0.1f, 0.1f, 0.1f, 1.0f, 1 };   // ChainMail material (forward.cu:66-71)
 	bool cm_frontier = true;         // ChainMail sweeps on work lists (false: every sweep dense)
+	bool obj_gpu = true;             // object mode's weighted device fit (xpbd_set_object_shape_gpu)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -145,6 +146,16 @@ public:
 	DBuf<float4> cm_spos;
 	DBuf<float> cm_stime, cm_seed_delta, cm_time_out;
 	DBuf<dev::CmState> cm_state;
+	// object mode: rest offsets q (FP64, internal order), per-object rest centroid, sum q,
+	// count, previous centroid, fit parameters, centroid move, block partials, fit weights,
+	// boxes; self-collision active set, cross-object corrections and their frame sums
+	DBuf<double> obj_q, obj_shift, obj_sumq, obj_partial;
+	DBuf<float> obj_c0, obj_params, obj_disp, obj_w, obj_boxes, push_partial, push_T;
+	DBuf<int> obj_count;
+	DBuf<unsigned char> sc_active;
+	DBuf<float4> sc_cross, sc_accum;
+	bool obj_shift_valid = false;    // a previous object step set the centroids (boxes usable)
+	bool last_sc_limited = false;    // the last step's self-collision build used the box filter
 	DBuf<float> pos_out3;
 	DBuf<int> off, nbr;
 	DBuf<float> ndist, nstiff, lam;
@@ -228,6 +239,10 @@ public:
 		shape_rest.release();
 		cm_td.release(); cm_flag.release(); cm_mark.release(); cm_work.release(); cm_seed_idx.release();
 		cm_spos.release(); cm_stime.release(); cm_seed_delta.release(); cm_time_out.release(); cm_state.release();
+		obj_q.release(); obj_shift.release(); obj_sumq.release(); obj_partial.release(); obj_c0.release();
+		obj_params.release(); obj_disp.release(); obj_w.release(); obj_boxes.release(); push_partial.release();
+		push_T.release(); obj_count.release(); sc_active.release(); sc_cross.release(); sc_accum.release();
+		obj_shift_valid = false;
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
@@ -409,6 +424,7 @@ public:
 			CK(cudaMemcpyAsync(d_obj_id.p, oi.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
 			CK(cudaStreamSynchronize(stream));
 		}
+		if (build_object_cache()) return -1;
 		spacing = graph_spacing(graph);
 		S.topo_dirty = false;
 		if (rebuild_clusters()) return -1;
@@ -448,6 +464,101 @@ public:
 		graph_key.clear();
 		++generation;
 		return 0;
+	}
+
+	// ------------------------------------------------------------------ object mode
+	// objectEnsureRestCache (forward.cu:11376-11440): per object (graph component of at
+	// least 50) the rest centroid c0 (FP64 sums in caller order, stored as float), the rest
+	// offsets q = rest - c0 (float difference widened to FP64), sum q and the count; the
+	// previous centroid starts at c0.
+	int build_object_cache()
+	{
+		const int K = num_objects;
+		if (K <= 0) return 0;
+		std::vector<double> sum(3 * (size_t)K, 0.0);
+		std::vector<int> cnt(K, 0);
+		for (int i = 0; i < n; ++i) {
+			const int id = obj_id[i];
+			if (id < 0) continue;
+			for (int a = 0; a < 3; ++a) sum[3 * id + a] += in_pos[3 * i + a];
+			++cnt[id];
+		}
+		std::vector<float> c0(3 * (size_t)K);
+		std::vector<double> shift(3 * (size_t)K);
+		for (int k = 0; k < K; ++k)
+			for (int a = 0; a < 3; ++a) {
+				c0[3 * k + a] = (float)(sum[3 * k + a] / std::max(cnt[k], 1));
+				shift[3 * k + a] = (double)c0[3 * k + a];
+			}
+		std::vector<double> q(3 * (size_t)n, 0.0), sumq(3 * (size_t)K, 0.0);
+		for (int i = 0; i < n; ++i) {
+			const int id = obj_id[i];
+			if (id < 0) continue;
+			const int r = inv[i];
+			for (int a = 0; a < 3; ++a) {
+				const double v = (double)(in_pos[3 * i + a] - c0[3 * id + a]);
+				q[3 * (size_t)r + a] = v;
+				sumq[3 * id + a] += v;
+			}
+		}
+		CK(obj_q.alloc(3 * (size_t)n)); CK(obj_shift.alloc(3 * (size_t)K)); CK(obj_sumq.alloc(3 * (size_t)K));
+		CK(obj_c0.alloc(3 * (size_t)K)); CK(obj_count.alloc(K)); CK(obj_params.alloc(16 * (size_t)K));
+		CK(obj_disp.alloc(K)); CK(obj_w.alloc(n)); CK(obj_boxes.alloc(6 * (size_t)K)); CK(push_T.alloc(4 * (size_t)K));
+		CK(obj_partial.alloc((size_t)blocks_for(n).x * K * 16));
+		CK(push_partial.alloc((size_t)blocks_for(n).x * K * 4));
+		CK(cudaMemcpyAsync(obj_q.p, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(obj_shift.p, shift.data(), sizeof(double) * shift.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(obj_sumq.p, sumq.data(), sizeof(double) * sumq.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(obj_c0.p, c0.data(), sizeof(float) * c0.size(), cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(obj_count.p, cnt.data(), sizeof(int) * K, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemsetAsync(obj_params.p, 0, obj_params.bytes(), stream));
+		CK(cudaMemsetAsync(obj_disp.p, 0, obj_disp.bytes(), stream));
+		dev::k_fill<<<blocks_for(n), kBlock, 0, stream>>>(n, obj_w.p, 1.0f);
+		CK(cudaGetLastError());
+		obj_shift_valid = false;
+		return sync();
+	}
+
+	bool object_on() const { return S.object_shape > 0.0f && num_objects > 0; }
+	// the self-collision build keeps only Gaussians near another object (forward.cu:11808-11816)
+	bool sc_limited() const
+	{
+		return selfcol_on() && object_on() && !S.sc_within && obj_shift_valid && num_objects >= 1 &&
+			num_objects <= dev::kObjMaxK;
+	}
+	bool obj_push() const { return selfcol_on() && object_on(); }
+
+	int ensure_sc_object_buffers()
+	{
+		if (!obj_push()) return 0;
+		if (!sc_active.p) CK(sc_active.alloc(n));
+		if (!sc_cross.p) CK(sc_cross.alloc(n));
+		if (!sc_accum.p) CK(sc_accum.alloc(n));
+		return 0;
+	}
+
+	// object shape keeping after predict (forward.cu:12141-12166, device path 11671-11702);
+	// the weighted fit while Gaussians are pinned, the plain fit otherwise or with more
+	// than 64 objects (where the reference fits on the host)
+	void enqueue_object_step(dim3 G, dim3 B)
+	{
+		const int K = num_objects;
+		const bool weighted = att_active && S.obj_gpu && K <= dev::kObjMaxK;
+		const int stride = weighted ? 16 : 12;
+		for (int k0 = 0; k0 < K; k0 += dev::kObjMaxK)
+			launch(ST_PREDICT, G, B, dev::k_obj_accum, n, (const float4*)pos_next.p, (const int*)d_obj_id.p,
+				(const double*)obj_q.p, (const double*)obj_shift.p, K, k0, std::min(dev::kObjMaxK, K - k0),
+				weighted ? (const float*)obj_w.p : (const float*)nullptr, stride, obj_partial.p);
+		launch(ST_PREDICT, dim3(K), dim3(256), dev::k_obj_solve, (int)G.x, K, (const double*)obj_partial.p, stride,
+			(const int*)obj_count.p, (const double*)obj_sumq.p, (const float*)obj_c0.p, obj_shift.p, obj_params.p,
+			obj_disp.p);
+		if (selfcol_on() && K <= dev::kObjMaxK) {
+			launch(ST_PREDICT, dim3((6 * K + 255) / 256), dim3(256), dev::k_obj_boxes_init, K, obj_boxes.p);
+			launch(ST_PREDICT, G, B, dev::k_obj_boxes, n, (const float4*)pos_next.p, (const int*)d_obj_id.p, K,
+				obj_boxes.p);
+		}
+		launch(ST_PREDICT, G, B, dev::k_obj_match, n, pos_next.p, (const float4*)pos_rest.p, (const int*)d_obj_id.p,
+			(const float*)obj_params.p, S.object_shape);
 	}
 
 	// ------------------------------------------------------------------ ChainMail
@@ -667,7 +778,8 @@ public:
 		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), vol_lanes(), gather_lanes(),
 			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
-			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table };
+			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
+			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -701,14 +813,14 @@ public:
 		return dim3((unsigned)((items + per_block - 1) / per_block));
 	}
 
-	void enqueue_sc_candidates(dim3 G, dim3 B)
+	void enqueue_sc_candidates(dim3 G, dim3 B, const unsigned char* active)
 	{
 		launch(ST_SC_BUILD, G, B, dev::k_sc_pack, n, (const int*)sc_idx_sorted.p, (const float4*)pos_curr.p,
 			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)d_obj_id.p, sc_sp.p, sc_sr.p, sc_sx.p);
 		launch(ST_SC_BUILD, G, B, dev::k_sc_build_sorted, n, (const StepParams*)d_params, (const float4*)pos_curr.p,
 			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p, (const int*)sc_start.p,
 			(unsigned)(sc_table - 1), (const int*)d_obj_id.p, (const float4*)sc_sp.p, (const float4*)sc_sr.p,
-			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p);
+			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p, active);
 	}
 
 	// volume kernel shapes: lanes per cluster (Kernel A) and per node (Kernel B);
@@ -738,14 +850,20 @@ public:
 		CK(cudaMemsetAsync(d_ctr, 0, offsetof(DevCounters, jstats), stream));
 		launch(ST_PREDICT, G, B, dev::k_predict, N, (const StepParams*)d_params, (const float4*)pos_curr.p, pos_next.p,
 			vel.p, S.use_volume ? lam_vol.p : (float*)nullptr);
+		if (object_on()) enqueue_object_step(G, B);
+		const unsigned char* active = sc_limited() ? (const unsigned char*)sc_active.p : nullptr;
 		if (sc) {
+			if (active)
+				launch(ST_SC_BUILD, G, B, dev::k_sc_active, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
+					(const float4*)pos_next.p, (const int*)d_obj_id.p, (const float*)obj_boxes.p,
+					(const float*)obj_disp.p, num_objects, sc_active.p, d_ctr);
 			const int buckets = sc_table + 1;
 			CK(cudaMemsetAsync(sc_bucket.p, 0, sc_bucket.bytes(), stream));
 			CK(cudaMemsetAsync(sc_cursor.p, 0, sc_cursor.bytes(), stream));
-			launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr, active);
 			launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
 			launch(ST_SC_BUILD, G, B, dev::k_sc_keys, N, (const float4*)pos_curr.p, (const DevCounters*)d_ctr,
-				(unsigned)(sc_table - 1), (unsigned)sc_table, sc_keys.p, sc_bucket.p);
+				(unsigned)(sc_table - 1), (unsigned)sc_table, sc_keys.p, sc_bucket.p, active);
 			const int scan_n = buckets + 1;
 			const int nb = (scan_n + 1023) / 1024;
 			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_blocks, (const int*)sc_bucket.p, sc_start.p, scan_n,
@@ -756,7 +874,8 @@ public:
 				sc_cursor.p, sc_idx_sorted.p);
 			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
 				sc_idx_sorted.p, (const int*)d_perm.p);
-			enqueue_sc_candidates(G, B);
+			enqueue_sc_candidates(G, B, active);
+			if (obj_push()) CK(cudaMemsetAsync(sc_accum.p, 0, sc_accum.bytes(), stream));
 		}
 		float4* pin = pos_next.p;
 		float4* pout = pos_tmp.p;
@@ -852,12 +971,23 @@ public:
 			if (sc)
 				launch(ST_SC_SOLVE, G, B, dev::k_sc_solve, N, (const StepParams*)d_params, (const float4*)pin,
 					(const float4*)pos_curr.p, (const float4*)pos_rest.p, (const int*)sc_contacts.p,
-					(const int*)sc_counts.p, (const DevCounters*)d_ctr, sc_dp.p);
+					(const int*)sc_counts.p, (const DevCounters*)d_ctr, sc_dp.p,
+					obj_push() ? sc_cross.p : (float4*)nullptr);
 			if (project)
 				launch(ST_PROJECT, G, B, dev::k_project, N, (const StepParams*)d_params, pin, (const float4*)pos_curr.p,
 					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0,
 					(const int*)d_obj_id.p, S.kin_ext.empty() ? (const KinCollider*)nullptr : (const KinCollider*)d_kin_ext.p,
-					(const int2*)d_kin_range.p);
+					(const int2*)d_kin_range.p, (const float4*)sc_cross.p, obj_push() ? sc_accum.p : (float4*)nullptr);
+		}
+		if (obj_push()) {   // contact push (forward.cu:12587-12597)
+			const int K = num_objects;
+			for (int k0 = 0; k0 < K; k0 += dev::kObjMaxK)
+				launch(ST_PROJECT, G, B, dev::k_obj_push_sum, N, (const int*)d_obj_id.p, (const float4*)sc_accum.p, K, k0,
+					std::min(dev::kObjMaxK, K - k0), (const DevCounters*)d_ctr, push_partial.p);
+			launch(ST_PROJECT, dim3((K + 63) / 64), dim3(64), dev::k_obj_push_solve, (int)G.x, K,
+				(const float*)push_partial.p, (const DevCounters*)d_ctr, S.object_shape, push_T.p);
+			launch(ST_PROJECT, G, B, dev::k_obj_push_apply, N, (const StepParams*)d_params, (const int*)d_obj_id.p,
+				(const float4*)sc_accum.p, (const float*)push_T.p, (const DevCounters*)d_ctr, pin);
 		}
 		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
 			vel.p, pos_out3.p, (const int*)d_perm.p);
@@ -883,6 +1013,8 @@ public:
 		}
 		if (S.use_distance && S.dist_gs && ensure_coloring()) return -1;
 		if (S.sc_enabled && ensure_selfcol()) return -1;
+		if (ensure_sc_object_buffers()) return -1;
+		const bool sc_limited_now = sc_limited();
 		if (upload_ext_colliders()) return -1;   // sets the object ranges fill_params reads
 		if (upload_params()) return -1;
 		if (profiling || !S.use_graph) {
@@ -909,6 +1041,8 @@ public:
 			CK(cudaGraphLaunch(graph_exec, stream));
 			launches += graph_kernels;
 		}
+		last_sc_limited = sc_limited_now;
+		if (object_on()) obj_shift_valid = true;
 		stepped = true;
 		return 0;
 	}
@@ -945,7 +1079,7 @@ public:
 	// ------------------------------------------------------------------ attach
 	// setAttachedParticles (forward.cu:6759-6788): restore the saved inverse masses, save
 	// them on first use, then pin idx[] at pos[].
-	int set_attached(int count, const int* idx, const float* pos)
+	int set_attached(int count, const int* idx, const float* pos, float weight = 1.0f)
 	{
 		const int N = n;
 		if (att_active)
@@ -984,7 +1118,10 @@ public:
 		CK(cudaMemcpyAsync(att_idx.p, st.idx, sizeof(int) * count, cudaMemcpyHostToDevice, stream));
 		CK(cudaMemcpyAsync(att_pos.p, st.pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
 		CK(cudaEventRecord(st.ev, stream));
-		dev::k_attach<<<blocks_for(count), kBlock, 0, stream>>>(count, att_idx.p, att_pos.p, N, pos_curr.p, vel.p);
+		float* w = (object_on() && obj_w.p) ? obj_w.p : nullptr;
+		if (w) dev::k_fill<<<blocks_for(N), kBlock, 0, stream>>>(N, w, 1.0f);
+		dev::k_attach<<<blocks_for(count), kBlock, 0, stream>>>(count, att_idx.p, att_pos.p, N, pos_curr.p, vel.p, w,
+			fmaxf(weight, 1.0f));
 		CK(cudaGetLastError());
 		att_active = true;
 		return 0;
@@ -1108,14 +1245,16 @@ XPBD_API void xpbd_set_ground(int enabled, float ux, float uy, float uz, float h
 
 XPBD_API void xpbd_set_object_shape(float stiffness)
 {
+	// setObjectModeParams(stiffness, no body contact, components >= 50) (xpbd_capi.cu:148,
+	// forward.cu:4464-4477)
 	float s = fminf(fmaxf(stiffness, 0.0f), 1.0f);
 	if (!std::isfinite(s)) s = 0.0f;
-	if (s > 0.0f && engine().S.object_shape == 0.0f)
-		fprintf(stderr, "[xpbd_b200] object-level shape keeping is not implemented; stiffness %.3f ignored\n", s);
 	engine().S.object_shape = s;
 }
 
-XPBD_API void xpbd_set_object_shape_gpu(int enabled) { (void)enabled; }
+// setObjectShapeGPU (forward.cu:4521): 1 = the weighted device fit while Gaussians are
+// pinned (default); 0 = the plain fit always (the reference's host path)
+XPBD_API void xpbd_set_object_shape_gpu(int enabled) { engine().S.obj_gpu = enabled != 0; }
 
 XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses, const float* dims, float margin,
 	float friction)
@@ -1178,9 +1317,8 @@ XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 
 XPBD_API int xpbd_set_attached(int count, const int* idx, const float* pos, float weight)
 {
-	(void)weight;
 	if (!cur_engine()->stepped) return fail("xpbd_set_attached: no step yet");
-	if (cur_engine()->set_attached(count, idx, pos)) return -1;
+	if (cur_engine()->set_attached(count, idx, pos, weight)) return -1;
 	return 0;
 }
 
@@ -1199,7 +1337,7 @@ XPBD_API void xpbd_self_collision_stats(int* out)
 	if (!cur_engine()->stepped || !engine().S.sc_enabled) return;
 	if (cur_engine()->read_counters()) return;
 	out[0] = (int)cur_engine()->h_ctr->sc_contacts;
-	out[1] = cur_engine()->n;
+	out[1] = cur_engine()->last_sc_limited ? (int)cur_engine()->h_ctr->sc_active : cur_engine()->n;
 	out[2] = (int)cur_engine()->h_ctr->sc_overflow;
 }
 
@@ -1701,16 +1839,16 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	const int buckets = E.sc_table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
 	CK(cudaMemsetAsync(E.sc_bucket.p, 0, E.sc_bucket.bytes(), E.stream));
 	CK(cudaMemsetAsync(E.sc_cursor.p, 0, E.sc_cursor.bytes(), E.stream));
-	dev::k_sc_disp<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.pos_next.p, E.d_ctr);
+	dev::k_sc_disp<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.pos_next.p, E.d_ctr, nullptr);
 	dev::k_sc_setup<<<1, 1, 0, E.stream>>>(E.d_params, E.d_ctr);
 	dev::k_sc_keys<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.d_ctr, (unsigned)(E.sc_table - 1), (unsigned)E.sc_table,
-		E.sc_keys.p, E.sc_bucket.p);
+		E.sc_keys.p, E.sc_bucket.p, nullptr);
 	dev::k_scan_blocks<<<nb, 1024, 0, E.stream>>>(E.sc_bucket.p, E.sc_start.p, scan_n, E.sc_block_sums.p);
 	dev::k_scan_sums<<<1, 1024, 0, E.stream>>>(E.sc_block_sums.p, nb);
 	dev::k_scan_add<<<nb, 1024, 0, E.stream>>>(E.sc_start.p, scan_n, E.sc_block_sums.p);
 	dev::k_sc_scatter<<<G, B, 0, E.stream>>>(N, E.sc_keys.p, E.sc_start.p, E.sc_cursor.p, E.sc_idx_sorted.p);
 	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p, E.d_perm.p);
-	E.enqueue_sc_candidates(G, B);
+	E.enqueue_sc_candidates(G, B, nullptr);
 	CK(cudaGetLastError());
 	if (E.read_counters()) return -1;
 	// restore the solver state this stage check borrowed
@@ -1866,9 +2004,9 @@ XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const fl
 	const auto* Pp = reinterpret_cast<const float4*>(p);
 	const auto* R = reinterpret_cast<const float4*>(rest);
 	const dim3 B(kBlock), G((n + kBlock - 1) / kBlock);
-	dev::k_sc_disp<<<G, B, 0, st>>>(n, X, Pp, d_ctr);
+	dev::k_sc_disp<<<G, B, 0, st>>>(n, X, Pp, d_ctr, nullptr);
 	dev::k_sc_setup<<<1, 1, 0, st>>>(d_params, d_ctr);
-	dev::k_sc_keys<<<G, B, 0, st>>>(n, X, d_ctr, (unsigned)(table - 1), (unsigned)table, keys, bucket);
+	dev::k_sc_keys<<<G, B, 0, st>>>(n, X, d_ctr, (unsigned)(table - 1), (unsigned)table, keys, bucket, nullptr);
 	dev::k_scan_blocks<<<nb, 1024, 0, st>>>(bucket, start, scan_n, sums);
 	dev::k_scan_sums<<<1, 1024, 0, st>>>(sums, nb);
 	dev::k_scan_add<<<nb, 1024, 0, st>>>(start, scan_n, sums);
@@ -1876,7 +2014,7 @@ XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const fl
 	dev::k_sc_order<<<(buckets + kBlock - 1) / kBlock, B, 0, st>>>(buckets, start, sorted, (const int*)nullptr);
 	dev::k_sc_pack<<<G, B, 0, st>>>(n, sorted, X, Pp, R, obj_id, sp, sr, sx);
 	dev::k_sc_build_sorted<<<G, B, 0, st>>>(n, d_params, X, Pp, R, sorted, start, (unsigned)(table - 1), obj_id, sp,
-		sr, sx, d_ctr, contacts, counts);
+		sr, sx, d_ctr, contacts, counts, nullptr);
 	if (total)
 		CK(cudaMemcpyAsync(total, &d_ctr->sc_contacts, sizeof(int), cudaMemcpyDeviceToDevice, st));
 	CK(cudaGetLastError());

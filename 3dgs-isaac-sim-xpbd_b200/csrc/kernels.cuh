@@ -1317,7 +1317,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
 	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
 	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id,
-	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range)
+	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range, const float4* __restrict__ sc_dp_cross,
+	float4* __restrict__ sc_accum)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1327,6 +1328,12 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 		const float4 d = sc_dp[idx];
 		p4.x = p4.x + d.x; p4.y = p4.y + d.y; p4.z = p4.z + d.z;
 		moved = true;
+		if (sc_accum) {   // the frame's cross-object part, for the contact push (forward.cu:7311-7322)
+			const float4 c = sc_dp_cross[idx];
+			float4 a = sc_accum[idx];
+			a.x = a.x + c.x; a.y = a.y + c.y; a.z = a.z + c.z;
+			sc_accum[idx] = a;
+		}
 	}
 	if (p4.w > 0.0f) {
 		float3 p = f3(p4);
@@ -1512,11 +1519,11 @@ __device__ __forceinline__ int sc_cell(float v, float inv_cell)
 
 // max predict displacement^2 (selfColDispKernel + DeviceReduce::Max)
 __global__ void __launch_bounds__(kBlock) k_sc_disp(int n, const float4* __restrict__ x, const float4* __restrict__ p,
-	DevCounters* __restrict__ ctr)
+	DevCounters* __restrict__ ctr, const unsigned char* __restrict__ active)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	float d2 = 0.0f;
-	if (i < n) {
+	if (i < n && (!active || active[i])) {
 		const float4 a = x[i], b = p[i];
 		const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
 		const float v = dx * dx + dy * dy + dz * dz;
@@ -1547,14 +1554,15 @@ __global__ void k_sc_setup(const StepParams* __restrict__ P, DevCounters* __rest
 
 // hash keys of start positions + bucket counts (selfColKeyKernel)
 __global__ void __launch_bounds__(kBlock) k_sc_keys(int n, const float4* __restrict__ x, const DevCounters* __restrict__ ctr,
-	unsigned int mask, unsigned int sentinel, unsigned int* __restrict__ keys, int* __restrict__ bucket)
+	unsigned int mask, unsigned int sentinel, unsigned int* __restrict__ keys, int* __restrict__ bucket,
+	const unsigned char* __restrict__ active)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const float4 p = x[i];
 	const float inv_cell = ctr->sc_inv_cell;
 	unsigned int k = sentinel;
-	if (isfinite(p.x) && isfinite(p.y) && isfinite(p.z))
+	if ((!active || active[i]) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z))
 		k = sc_hash(sc_cell(p.x, inv_cell), sc_cell(p.y, inv_cell), sc_cell(p.z, inv_cell), mask);
 	keys[i] = k;
 	atomicAdd(&bucket[k], 1);
@@ -1656,91 +1664,6 @@ __global__ void __launch_bounds__(kBlock) k_sc_order(int buckets, const int* __r
 	}
 }
 
-// per-particle candidate lists (selfColBuildKernel, forward.cu:7079-7180), within-body
-// pairs when enabled, no bounding-box activity filter (it needs object-mode boxes)
-__global__ void __launch_bounds__(kBlock) k_sc_build(int n, const StepParams* __restrict__ P,
-	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
-	const int* __restrict__ idx_sorted, const int* __restrict__ start, unsigned int mask,
-	const int* __restrict__ obj_id, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
-	int* __restrict__ counts)
-{
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	const float4 x = X[i], p = Pp[i];
-	int cnt = 0, over = 0;
-	if (isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
-		const float inv_cell = ctr->sc_inv_cell;
-		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
-		const float fast_rel = P->sc_fast_rel;
-		const int within = P->sc_within;
-		const float4 q = rest[i];
-		const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
-		const int oi = obj_id[i];
-		const float search2 = search * search;
-		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
-		int* out = contacts + (size_t)i * kSelfColMax;
-		unsigned int hs[27];
-		float prio[kSelfColMax];
-		int tier[kSelfColMax];
-		int nh = 0;
-		for (int oz = -1; oz <= 1; ++oz)
-			for (int oy = -1; oy <= 1; ++oy)
-				for (int ox = -1; ox <= 1; ++ox) {
-					const unsigned int h = sc_hash(cx + ox, cy + oy, cz + oz, mask);
-					bool dup = false;
-					for (int m = 0; m < nh; ++m) if (hs[m] == h) { dup = true; break; }
-					if (dup) continue;
-					hs[nh++] = h;
-					const int s = start[h], e = start[h + 1];
-					for (int t = s; t < e; ++t) {
-						const int j = idx_sorted[t];
-						if (j == i) continue;
-						const bool cross = obj_id[j] != oi;
-						if (!cross && !within) continue;
-						const float4 pj = Pp[j], qj = rest[j];
-						const float qx = q.x - qj.x, qy = q.y - qj.y, qz = q.z - qj.z;
-						const float q2 = qx * qx + qy * qy + qz * qz;
-						float pr;
-						int code = j;
-						if (cross) {
-							const float4 xj = X[j];
-							const float ex = x.x - xj.x, ey = x.y - xj.y, ez = x.z - xj.z;
-							const float dist_x = sqrtf(ex * ex + ey * ey + ez * ez);
-							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
-							const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
-							if (!(dist_x < search + rel)) continue;
-							if (!(q2 >= cross_excl2)) continue;
-							pr = dist_x - rel;
-							if (rel > fast_rel) code = -(j + 1);
-						}
-						else {
-							const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-							const float d2 = ex * ex + ey * ey + ez * ez;
-							if (!(d2 < search2)) continue;
-							if (!(q2 >= excl2)) continue;
-							pr = sqrtf(d2);
-						}
-						const int tr = cross ? 0 : 1;
-						if (cnt < kSelfColMax) {
-							out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
-						}
-						else {
-							int worst = 0;
-							for (int m = 1; m < kSelfColMax; ++m)
-								if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
-							if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
-								out[worst] = code; prio[worst] = pr; tier[worst] = tr;
-							}
-							++over;
-						}
-					}
-				}
-	}
-	counts[i] = cnt;
-	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
-	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
-}
-
 // Cell-ordered copies of what the candidate scan reads per neighbour: predicted
 // position + object id, rest position + particle index, start position.  One pass,
 // 48 B per particle written; the scan then reads each cell's particles contiguously.
@@ -1766,7 +1689,7 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 	const int* __restrict__ idx_sorted, const int* __restrict__ start, unsigned int mask,
 	const int* __restrict__ obj_id, const float4* __restrict__ sp, const float4* __restrict__ sr,
 	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
-	int* __restrict__ counts)
+	int* __restrict__ counts, const unsigned char* __restrict__ active)
 {
 	// thread i builds the list of particle i: particles are numbered along a Morton curve
 	// of their rest positions, so a warp's particles share most of their 27 cells (same
@@ -1775,7 +1698,8 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 	if (i >= n) return;
 	const float4 x = X[i], p = Pp[i];
 	int cnt = 0, over = 0;
-	if (isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+	if ((!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) &&
+		isfinite(p.z)) {
 		const float inv_cell = ctr->sc_inv_cell;
 		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
 		const float fast_rel = P->sc_fast_rel;
@@ -1884,7 +1808,7 @@ __device__ __forceinline__ bool sc_start_normal(float4 xi, float4 xj, float4 qi,
 __global__ void __launch_bounds__(kBlock) k_sc_solve(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pos, const float4* __restrict__ pos_start, const float4* __restrict__ rest,
 	const int* __restrict__ contacts, const int* __restrict__ counts, const DevCounters* __restrict__ ctr,
-	float4* __restrict__ dp_out)
+	float4* __restrict__ dp_out, float4* __restrict__ dp_cross)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
@@ -1969,13 +1893,14 @@ __global__ void __launch_bounds__(kBlock) k_sc_solve(int n, const StepParams* __
 		}
 	}
 	dp_out[i] = make_float4(out.x, out.y, out.z, 0.0f);
+	if (dp_cross) dp_cross[i] = make_float4(cpx, cpy, cpz, 0.0f);
 }
 
 // ---------------------------------------------------------------------------
 // pins (attachApplyKernel, forward.cu:6714-6725): inverse mass 0, position, zero velocity
 // ---------------------------------------------------------------------------
 __global__ void k_attach(int count, const int* __restrict__ idx, const float* __restrict__ pos, int n,
-	float4* __restrict__ pos_curr, float4* __restrict__ vel)
+	float4* __restrict__ pos_curr, float4* __restrict__ vel, float* __restrict__ obj_w, float weight)
 {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k >= count) return;
@@ -1983,6 +1908,13 @@ __global__ void k_attach(int count, const int* __restrict__ idx, const float* __
 	if (i < 0 || i >= n) return;
 	pos_curr[i] = make_float4(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2], 0.0f);
 	vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (obj_w) obj_w[i] = weight;   // rigid-fit weight of object mode (forward.cu:6724)
+}
+
+__global__ void k_fill(int n, float* __restrict__ a, float v)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) a[i] = v;
 }
 
 __global__ void k_get_w(int n, const float4* __restrict__ pos, float* __restrict__ w)
@@ -2254,6 +2186,328 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 	out_quat[4 * o + 2] = (float)(qyv / qn);
 	out_quat[4 * o + 3] = (float)(qzv / qn);
 	atomicAdd(&ctr->shapes_deformed, 1u);
+}
+
+// ===========================================================================
+// Object mode: rigid shape keeping per object (graph component of at least 50
+// Gaussians), once per step right after predict (forward.cu:12141-12166, the device path
+// 6829-6958 and 11671-11702).  The per-object sums are in FP64 like the reference's; they
+// are reduced in a fixed order (block partials, then one block per object) instead of
+// with atomics, so a run repeats bit for bit.
+// ===========================================================================
+constexpr int kObjMaxK = 64;   // objects with the device path (OBJ_GPU_MAX_K, forward.cu:192)
+
+// objectShapeAccumKernel (forward.cu:6829-6885): per Gaussian of an object, d = p - s
+// (s: the object's previous centroid) and d q^T (q = rest - rest centroid); with
+// attachment weights (stride 16) every term times w, plus w and w q.  Writes the block's
+// sums of objects k0 .. k0 + kc - 1 (kc <= 64) to partial[block][object][stride].
+__global__ void __launch_bounds__(kBlock) k_obj_accum(int n, const float4* __restrict__ pos,
+	const int* __restrict__ obj_id, const double* __restrict__ q3, const double* __restrict__ shift, int K, int k0,
+	int kc, const float* __restrict__ weight, int stride, double* __restrict__ partial)
+{
+	__shared__ double sh[kObjMaxK * 16];
+	for (int t = threadIdx.x; t < kc * stride; t += blockDim.x) sh[t] = 0.0;
+	__syncthreads();
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	const int gid = (idx < n) ? obj_id[idx] : -1;
+	const int id = (gid >= k0 && gid < k0 + kc) ? gid - k0 : -1;   // index within this chunk
+	double v[16];
+#pragma unroll
+	for (int k = 0; k < 16; ++k) v[k] = 0.0;
+	if (id >= 0) {
+		const float4 p = pos[idx];
+		const double dx = (double)p.x - shift[3 * gid], dy = (double)p.y - shift[3 * gid + 1],
+			dz = (double)p.z - shift[3 * gid + 2];
+		const double qx = q3[3 * (size_t)idx], qy = q3[3 * (size_t)idx + 1], qz = q3[3 * (size_t)idx + 2];
+		v[0] = dx; v[1] = dy; v[2] = dz;
+		v[3] = dx * qx; v[4] = dx * qy; v[5] = dx * qz;
+		v[6] = dy * qx; v[7] = dy * qy; v[8] = dy * qz;
+		v[9] = dz * qx; v[10] = dz * qy; v[11] = dz * qz;
+		if (weight) {
+			const double w = (double)weight[idx];
+#pragma unroll
+			for (int k = 0; k < 12; ++k) v[k] *= w;
+			v[12] = w; v[13] = w * qx; v[14] = w * qy; v[15] = w * qz;
+		}
+	}
+	const unsigned int full = 0xffffffffu;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int id0 = __shfl_sync(full, id, 0);
+	const bool uniform = __all_sync(full, id == id0);
+	if (uniform && id0 >= 0) {
+		for (int k = 0; k < stride; ++k)
+			for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(full, v[k], o);
+	}
+	// warps add their sums one after another (fixed order); a warp spanning objects adds
+	// lane by lane
+	for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+		if (warp == w) {
+			if (uniform) {
+				if (lane == 0 && id0 >= 0)
+					for (int k = 0; k < stride; ++k) sh[id0 * stride + k] += v[k];
+			}
+			else {
+				for (int l = 0; l < 32; ++l) {
+					const int idl = __shfl_sync(full, id, l);
+					for (int k = 0; k < stride; ++k) {
+						const double vl = __shfl_sync(full, v[k], l);
+						if (lane == 0 && idl >= 0) sh[idl * stride + k] += vl;
+					}
+				}
+			}
+		}
+		__syncthreads();
+	}
+	for (int t = threadIdx.x; t < kc * stride; t += blockDim.x)
+		partial[((size_t)blockIdx.x * K + k0) * stride + t] = sh[t];
+}
+
+// objectShapeSolveKernel (forward.cu:6887-6958), one block per object: the block sums
+// the partials in order, then one thread forms c = s + sum d / W, A = sum d q^T - (c - s)
+// (sum q)^T, normalises it (Frobenius), takes its rotation with the FP64 polar
+// decomposition of shape matching, and writes params = (rest centroid, c, R row-major,
+// valid); s becomes c and disp the centroid's move.
+__global__ void __launch_bounds__(256) k_obj_solve(int blocks, int K, const double* __restrict__ partial, int stride,
+	const int* __restrict__ count, const double* __restrict__ sumq, const float* __restrict__ c0,
+	double* __restrict__ shift, float* __restrict__ params, float* __restrict__ disp)
+{
+	const int k = blockIdx.x;
+	__shared__ double red[256];
+	__shared__ double S[16];
+	for (int c = 0; c < stride; ++c) {
+		double acc = 0.0;
+		for (int b = threadIdx.x; b < blocks; b += blockDim.x) acc += partial[((size_t)b * K + k) * stride + c];
+		red[threadIdx.x] = acc;
+		__syncthreads();
+		for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+			if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+			__syncthreads();
+		}
+		if (threadIdx.x == 0) S[c] = red[0];
+		__syncthreads();
+	}
+	if (threadIdx.x != 0) return;
+	float* Pk = params + 16 * k;
+	const int n = count[k];
+	if (n < 4) { Pk[15] = 0.0f; disp[k] = 0.0f; return; }
+	const bool wOn = (stride == 16);
+	const double W = wOn ? S[12] : (double)n;
+	if (!(W > 0.0)) { Pk[15] = 0.0f; disp[k] = 0.0f; return; }
+	const double inv = 1.0 / W;
+	const double dc[3] = { S[0] * inv, S[1] * inv, S[2] * inv };
+	const double* sq = wOn ? &S[13] : &sumq[3 * k];
+	double a[9];
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c) a[3 * r + c] = S[3 + 3 * r + c] - dc[r] * sq[c];
+	double now[3];
+	for (int t = 0; t < 3; ++t) {
+		now[t] = shift[3 * k + t] + dc[t];
+		shift[3 * k + t] = now[t];
+	}
+	disp[k] = (float)sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+	double fn = 0.0;
+	for (int t = 0; t < 9; ++t) fn += a[t] * a[t];
+	fn = sqrt(fn);
+	if (!(fn > 1e-300) || !isfinite(fn)) { Pk[15] = 0.0f; return; }
+	M3 A;
+	for (int r = 0; r < 3; ++r)
+		for (int c = 0; c < 3; ++c) A.m[c][r] = (float)(a[3 * r + c] / fn);
+	M3 R;
+	if (!shape_rotation_double(A, R)) { Pk[15] = 0.0f; return; }
+	for (int t = 0; t < 3; ++t) {
+		Pk[t] = wOn ? (float)((double)c0[3 * k + t] + S[13 + t] * inv) : c0[3 * k + t];
+		Pk[3 + t] = (float)now[t];
+		for (int cc = 0; cc < 3; ++cc) Pk[6 + 3 * t + cc] = R.m[cc][t];
+	}
+	Pk[15] = 1.0f;
+}
+
+// objectShapeMatchKernel (forward.cu:6801-6827): p += s (c + R (x_rest - c0) - p) for the
+// free Gaussians of valid objects
+__global__ void __launch_bounds__(kBlock) k_obj_match(int n, float4* __restrict__ pos, const float4* __restrict__ rest,
+	const int* __restrict__ obj_id, const float* __restrict__ params, float s)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= n) return;
+	const int id = obj_id[idx];
+	const float4 p = pos[idx];
+	if (id < 0 || p.w <= 0.0f) return;
+	const float* Pk = params + 16 * id;
+	if (Pk[15] == 0.0f) return;
+	const float4 r = rest[idx];
+	const float qx = r.x - Pk[0], qy = r.y - Pk[1], qz = r.z - Pk[2];
+	const float gx = Pk[3] + Pk[6] * qx + Pk[7] * qy + Pk[8] * qz;
+	const float gy = Pk[4] + Pk[9] * qx + Pk[10] * qy + Pk[11] * qz;
+	const float gz = Pk[5] + Pk[12] * qx + Pk[13] * qy + Pk[14] * qz;
+	pos[idx] = make_float4(p.x + s * (gx - p.x), p.y + s * (gy - p.y), p.z + s * (gz - p.z), p.w);
+}
+
+// object bounding boxes of the predicted positions (objectBoxesKernel, forward.cu:6960-6981):
+// float min / max through integer atomics on the bits, block-local first
+__device__ __forceinline__ void obj_atomic_min(float* a, float v)
+{
+	v += 0.0f;
+	if (v >= 0.0f) atomicMin((int*)a, __float_as_int(v));
+	else atomicMax((unsigned int*)a, __float_as_uint(v));
+}
+__device__ __forceinline__ void obj_atomic_max(float* a, float v)
+{
+	v += 0.0f;
+	if (v >= 0.0f) atomicMax((int*)a, __float_as_int(v));
+	else atomicMin((unsigned int*)a, __float_as_uint(v));
+}
+
+__global__ void k_obj_boxes_init(int K, float* __restrict__ boxes)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < 6 * K) boxes[t] = ((t % 6) < 3) ? FLT_MAX : -FLT_MAX;
+}
+
+__global__ void __launch_bounds__(kBlock) k_obj_boxes(int n, const float4* __restrict__ pos,
+	const int* __restrict__ obj_id, int K, float* __restrict__ boxes)
+{
+	__shared__ float sh[kObjMaxK * 6];
+	for (int t = threadIdx.x; t < K * 6; t += blockDim.x) sh[t] = ((t % 6) < 3) ? FLT_MAX : -FLT_MAX;
+	__syncthreads();
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx < n) {
+		const int id = obj_id[idx];
+		const float4 p = pos[idx];
+		if (id >= 0 && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)) {
+			float* b = &sh[6 * id];
+			obj_atomic_min(&b[0], p.x); obj_atomic_min(&b[1], p.y); obj_atomic_min(&b[2], p.z);
+			obj_atomic_max(&b[3], p.x); obj_atomic_max(&b[4], p.y); obj_atomic_max(&b[5], p.z);
+		}
+	}
+	__syncthreads();
+	for (int t = threadIdx.x; t < K * 6; t += blockDim.x) {
+		const float v = sh[t];
+		if (v == FLT_MAX || v == -FLT_MAX) continue;
+		if ((t % 6) < 3) obj_atomic_min(&boxes[t], v);
+		else obj_atomic_max(&boxes[t], v);
+	}
+}
+
+// selfColActiveKernel (forward.cu:6998-7029): with same-object contacts off, only Gaussians
+// whose start or predicted position lies in another object's box (grown by search + 2 x
+// the largest centroid move + 2 dc) enter the hash grid; Gaussians of no object always do
+__global__ void __launch_bounds__(kBlock) k_sc_active(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ x, const float4* __restrict__ p, const int* __restrict__ obj_id,
+	const float* __restrict__ boxes, const float* __restrict__ disp, int K, unsigned char* __restrict__ active,
+	DevCounters* __restrict__ ctr)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	float md = 0.0f;
+	for (int k = 0; k < K; ++k) md = fmaxf(md, disp[k]);
+	const float inflate = P->sc_search + 2.0f * md + 2.0f * P->sc_dc;
+	const int id = obj_id[i];
+	unsigned char a = 0;
+	if (id < 0) {
+		a = 1;
+	}
+	else {
+		const float4 pp = p[i], xx = x[i];
+		for (int k = 0; k < K; ++k) {
+			if (k == id) continue;
+			const float* b = &boxes[6 * k];
+			const float lx = b[0] - inflate, ly = b[1] - inflate, lz = b[2] - inflate;
+			const float hx = b[3] + inflate, hy = b[4] + inflate, hz = b[5] + inflate;
+			const bool inP = pp.x >= lx && pp.x <= hx && pp.y >= ly && pp.y <= hy && pp.z >= lz && pp.z <= hz;
+			const bool inX = xx.x >= lx && xx.x <= hx && xx.y >= ly && xx.y <= hy && xx.z >= lz && xx.z <= hz;
+			if (inP || inX) { a = 1; break; }
+		}
+	}
+	active[i] = a;
+	const unsigned int m = __ballot_sync(__activemask(), a != 0);
+	if (m && (threadIdx.x & 31) == __ffs(__activemask()) - 1) atomicAdd(&ctr->sc_active, __popc(m));
+}
+
+// Contact push (objectContactPush, forward.cu:11858-11890; kernels 7326-7354): per object,
+// the mean of the frame's cross-object corrections over the Gaussians that received one,
+// times the shape stiffness, is added to the object's other free Gaussians.  Block
+// partials of (sum, count) in a fixed order, then one thread per object.
+__global__ void __launch_bounds__(kBlock) k_obj_push_sum(int n, const int* __restrict__ obj_id,
+	const float4* __restrict__ accum, int K, int k0, int kc, const DevCounters* __restrict__ ctr,
+	float* __restrict__ partial)
+{
+	__shared__ float sh[kObjMaxK * 4];
+	if (ctr->sc_contacts == 0u) return;
+	for (int t = threadIdx.x; t < kc * 4; t += blockDim.x) sh[t] = 0.0f;
+	__syncthreads();
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	int id = -1;
+	float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (idx < n) {
+		const int gid = obj_id[idx];
+		id = (gid >= k0 && gid < k0 + kc) ? gid - k0 : -1;
+		a = accum[idx];
+		if (!(a.x * a.x + a.y * a.y + a.z * a.z > 1e-30f)) id = -1;
+	}
+	const unsigned int full = 0xffffffffu;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+		if (warp == w) {
+			for (int l = 0; l < 32; ++l) {
+				const int idl = __shfl_sync(full, id, l);
+				const float ax = __shfl_sync(full, a.x, l), ay = __shfl_sync(full, a.y, l), az = __shfl_sync(full, a.z, l);
+				if (lane == 0 && idl >= 0) {
+					float* S = &sh[4 * idl];
+					S[0] += ax; S[1] += ay; S[2] += az; S[3] += 1.0f;
+				}
+			}
+		}
+		__syncthreads();
+	}
+	for (int t = threadIdx.x; t < kc * 4; t += blockDim.x) partial[((size_t)blockIdx.x * K + k0) * 4 + t] = sh[t];
+}
+
+__global__ void k_obj_push_solve(int blocks, int K, const float* __restrict__ partial, const DevCounters* __restrict__ ctr,
+	float s, float* __restrict__ T)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= K) return;
+	T[4 * k + 3] = 0.0f;
+	if (ctr->sc_contacts == 0u) return;
+	float sum[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+	for (int b = 0; b < blocks; ++b)
+		for (int c = 0; c < 4; ++c) sum[c] += partial[((size_t)b * K + k) * 4 + c];
+	const float cnt = sum[3];
+	if (!(cnt > 0.0f)) return;
+	const float sc = s / cnt;
+	const float tx = sum[0] * sc, ty = sum[1] * sc, tz = sum[2] * sc;
+	if (!isfinite(tx) || !isfinite(ty) || !isfinite(tz)) return;
+	T[4 * k] = tx; T[4 * k + 1] = ty; T[4 * k + 2] = tz; T[4 * k + 3] = 1.0f;
+}
+
+// objectPushApplyKernel (forward.cu:7341-7354), then the ground plane again
+// (groundProjectKernel, forward.cu:7405-7421) when it is on
+__global__ void __launch_bounds__(kBlock) k_obj_push_apply(int n, const StepParams* __restrict__ P,
+	const int* __restrict__ obj_id, const float4* __restrict__ accum, const float* __restrict__ T,
+	const DevCounters* __restrict__ ctr, float4* __restrict__ pos)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	if (ctr->sc_contacts == 0u) return;
+	float4 p = pos[i];
+	if (p.w <= 0.0f) return;
+	bool moved = false;
+	const int id = obj_id[i];
+	if (id >= 0 && T[4 * id + 3] != 0.0f) {
+		const float4 a = accum[i];
+		if (!(a.x * a.x + a.y * a.y + a.z * a.z > 1e-30f)) {
+			p.x = p.x + T[4 * id]; p.y = p.y + T[4 * id + 1]; p.z = p.z + T[4 * id + 2];
+			moved = true;
+		}
+	}
+	if (P->ground_on) {
+		const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane;
+		if (c < 0.0f) {
+			p.x = p.x - c * P->gn[0]; p.y = p.y - c * P->gn[1]; p.z = p.z - c * P->gn[2];
+			moved = true;
+		}
+	}
+	if (moved) pos[i] = p;
 }
 
 // ===========================================================================

@@ -73,7 +73,7 @@ struct DevCounters {
 	float sc_reach;
 	unsigned int shapes_deformed;
 	unsigned int shapes_kept;
-	unsigned int pad;
+	unsigned int sc_active;         // Gaussians in the grid when the object box filter is on ([2])
 	int kin_hits[kMaxColliders];
 	float kin_push[kMaxColliders * kColliderAcc];
 	double jstats[3];               // sum V, sum V J, sum V J^2

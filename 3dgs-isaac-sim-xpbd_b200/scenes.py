@@ -124,8 +124,9 @@ class Scenario:
     def __init__(self, scene, grippers, substeps=10, iters=4, shape=True, volume=True, self_collision=False,
                  within_body=True, ring_k=3, max_members=64, leader_min_hop=1, dist_compliance=1e-6,
                  vol_compliance=1e-5, shape_compliance=1e-5, under_relax=0.6, vel_damping=0.01,
-                 shape_robust=True, frame_dt=1.0 / 60.0):
+                 shape_robust=True, frame_dt=1.0 / 60.0, object_shape=0.0):
         self.scene = scene
+        self.object_shape = object_shape
         self.grippers = list(grippers)
         self.substeps = substeps
         self.iters = iters
@@ -158,6 +159,7 @@ class Scenario:
         solver.set_volume(self.vol_compliance, self.ring_k, self.max_members, self.leader_min_hop)
         solver.set_shape_robust(self.shape_robust)
         solver.set_self_collision(self.self_collision, 1.5, 2.0, self.within_body)
+        solver.set_object_shape(self.object_shape)   # settings outlive create / destroy: always set
         solver.volume_stats(False)
         self.k = 0
 

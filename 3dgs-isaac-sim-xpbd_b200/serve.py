@@ -42,18 +42,25 @@ class Session:
     def __init__(self, sid, arrival, n, frames, seed, substeps=10, iters=4):
         self.sid, self.arrival, self.frames_left, self.seed = sid, arrival, frames, seed
         self.frames_total = frames
-        rng = np.random.default_rng(seed)
-        radii = tuple(float(r) for r in rng.uniform(0.3, 1.5, 3))
-        sc = scenes.make_scene(n, seed, radii=radii)
-        vel = (float(rng.uniform(0.002, 0.01)), 0.0, 0.0)
-        g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, math.radians(float(rng.uniform(-1, 1))))
-        self.scen = scenes.Scenario(sc, [g], substeps=substeps, iters=iters)
+        self.substeps, self.iters = substeps, iters
         self.n = n
+        self.scen = None
         self.solver = None
         self.pending_since = None
         self.latencies = []
 
+    def prepare(self):
+        """The session's scene and gripper stream (host work, done by the admission thread)."""
+        rng = np.random.default_rng(self.seed)
+        radii = tuple(float(r) for r in rng.uniform(0.3, 1.5, 3))
+        sc = scenes.make_scene(self.n, self.seed, radii=radii)
+        vel = (float(rng.uniform(0.002, 0.01)), 0.0, 0.0)
+        g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, math.radians(float(rng.uniform(-1, 1))))
+        self.scen = scenes.Scenario(sc, [g], substeps=self.substeps, iters=self.iters)
+
     def admit(self, lib_path):
+        if self.scen is None:
+            self.prepare()
         self.solver = bridge.XPBD(lib_path, instance=True)
         self.scen.setup(self.solver)
         self.scen.advance(self.solver, 1)          # upload + topology build (first substep)

@@ -281,6 +281,15 @@ static struct {
 	float jvw_mean, jvw_std;
 	/* ChainMail arrival times (forward.cu:3542; 1e9 = not reached, forward.cu:2717) */
 	float *cm_time, *cm_time_next;
+	/* object mode (forward.cu:164-209, 11376-11440): rest cache, fit state, boxes, weights,
+	 * the frame's cross-object self-collision corrections, the self-collision active set */
+	int obj_cache;
+	float *obj_c0, *obj_params, *obj_disp, *obj_boxes, *obj_w;
+	double *obj_q, *obj_sumq, *obj_shift;
+	int* obj_count;
+	int obj_shift_valid;
+	f3* obj_accum;
+	unsigned char* sc_act;
 } S;
 
 /* parameters: file statics of forward.cu with their defaults (forward.cu:53-92, 224-265, 300-361) */
@@ -330,6 +339,9 @@ static void free_state(void)
 	FREE(S.off); FREE(S.cnt); FREE(S.nbr); FREE(S.ndist); FREE(S.nstiff);
 	FREE(S.pos_curr); FREE(S.pos_next); FREE(S.pos_tmp); FREE(S.pos_rest); FREE(S.vel);
 	FREE(S.inv_mass); FREE(S.density); FREE(S.lam_a); FREE(S.lam_b); FREE(S.cm_time); FREE(S.cm_time_next);
+	FREE(S.obj_c0); FREE(S.obj_params); FREE(S.obj_disp); FREE(S.obj_boxes); FREE(S.obj_w); FREE(S.obj_q);
+	FREE(S.obj_sumq); FREE(S.obj_shift); FREE(S.obj_count); FREE(S.obj_accum); FREE(S.sc_act);
+	S.obj_cache = 0; S.obj_shift_valid = 0;
 	FREE(S.vol_off); FREE(S.vol_cnt); FREE(S.vol_idx); FREE(S.rev_off); FREE(S.rev_cnt); FREE(S.rev_idx);
 	FREE(S.sigma_rest); FREE(S.det_rest); FREE(S.v_rest); FREE(S.rest_len); FREE(S.lam_vol); FREE(S.mat_type);
 	FREE(S.cl_c); FREE(S.cl_sinv); FREE(S.cl_coef); FREE(S.vol_gs_order); FREE(S.vol_gs_color_off);
@@ -1858,9 +1870,10 @@ static int sc_build_one(int i, const f3* X, const f3* Pp, float invCell, unsigne
 	return cnt;
 }
 
-/* selfColBuild (forward.cu:11796-11849), within-body / no activity filter (the activity box
- * filter needs object-mode boxes, which the oracle does not restate) */
-static void sc_build(const f3* X, const f3* Pp)
+/* selfColBuild (forward.cu:11796-11849); with `limited`, only the Gaussians near another
+ * object's box take part (object mode, cross-object contacts only; forward.cu:11808-11816) */
+static void sc_active_set(const f3* X, const f3* Pp, float search, float dc);
+static void sc_build_active(const f3* X, const f3* Pp, int limited)
 {
 	const int N = S.n;
 	sc_ensure_spacing();
@@ -1870,8 +1883,14 @@ static void sc_build(const f3* X, const f3* Pp)
 	ensure_components();
 	const float search = P.sc_search_scale * dc;
 	const float excl = P.sc_exclude_scale * dc;
+	const unsigned char* act = NULL;
+	if (limited) {
+		sc_active_set(X, Pp, search, dc);
+		act = S.sc_act;
+	}
 	float maxDisp2 = 0.0f;
 	for (int i = 0; i < N; ++i) {
+		if (act && !act[i]) continue;
 		const float dx = Pp[i].x - X[i].x, dy = Pp[i].y - X[i].y, dz = Pp[i].z - X[i].z;
 		const float d2 = dx * dx + dy * dy + dz * dz;
 		const float v = isfinite(d2) ? d2 : 0.0f;
@@ -1887,7 +1906,7 @@ static void sc_build(const f3* X, const f3* Pp)
 	const unsigned int sentinel = (unsigned int)S.sc_table;
 	for (int i = 0; i < N; ++i) {
 		const f3 p = X[i];
-		if (!f3_finite(p)) { S.sc_keys[i] = sentinel; continue; }
+		if ((act && !act[i]) || !f3_finite(p)) { S.sc_keys[i] = sentinel; continue; }
 		S.sc_keys[i] = sc_hash(sc_cell(p.x, invCell), sc_cell(p.y, invCell), sc_cell(p.z, invCell), mask);
 	}
 	/* stable counting sort by key = CUB's stable radix sort of (key, i) pairs */
@@ -1912,13 +1931,18 @@ static void sc_build(const f3* X, const f3* Pp)
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : total, over) num_threads(nthreads())
 	for (int i = 0; i < N; ++i) {
 		int ov = 0;
+		if (act && !act[i]) { S.sc_count[i] = 0; continue; }
 		total += sc_build_one(i, X, Pp, invCell, mask, search, excl * excl, dc * dc, P.sc_fast_rel * dc, &ov);
 		over += ov;
 	}
 	S.sc_contacts = (int)total;
 	S.sc_overflow = (int)over;
-	S.sc_active = N;
+	int na = N;
+	if (act) { na = 0; for (int i = 0; i < N; ++i) na += act[i] ? 1 : 0; }
+	S.sc_active = na;
 }
+
+static void sc_build(const f3* X, const f3* Pp) { sc_build_active(X, Pp, 0); }
 
 /* selfColStartNormal (forward.cu:7183-7197) */
 static inline int sc_start_normal(f3 xi, f3 xj, f3 qi, f3 qj, float* nx, float* ny, float* nz)
@@ -1936,7 +1960,7 @@ static inline int sc_start_normal(f3 xi, f3 xj, f3 qi, f3 qj, float* nx, float* 
 }
 
 /* selfColSolveKernel + selfColApplyKernel (forward.cu:7205-7322) */
-static void sc_solve_apply(f3* pos)
+static void sc_solve_apply(f3* pos, f3* accum)
 {
 	const int N = S.n;
 	const float dc = P.sc_radius_scale * S.sc_spacing;
@@ -2026,6 +2050,7 @@ static void sc_solve_apply(f3* pos)
 	for (int i = 0; i < N; ++i) {
 		if (S.sc_count[i] <= 0) continue;
 		pos[i] = f3_add(pos[i], S.sc_dp[i]);
+		if (accum) accum[i] = f3_add(accum[i], S.sc_dp_cross[i]);
 	}
 }
 
@@ -2082,6 +2107,214 @@ static void volume_j_stats(void)
 }
 
 /* ------------------------------------------------------------------------- */
+/* object mode: rigid shape keeping per object after predict                  */
+/* (forward.cu:12141-12166; device path 6801-6958, 11671-11702)               */
+/* ------------------------------------------------------------------------- */
+#define OBJ_MAX_K 64   /* OBJ_GPU_MAX_K (forward.cu:192) */
+static int g_obj_gpu = 1;  /* g_objShapeGPU (forward.cu:193) */
+
+/* objectEnsureRestCache (forward.cu:11376-11440) */
+static void obj_ensure_cache(void)
+{
+	if (S.obj_cache) return;
+	ensure_components();
+	const int N = S.n, K = S.obj_k;
+	double* sum = calloc(3 * (size_t)(K > 0 ? K : 1), sizeof(double));
+	S.obj_count = calloc(K > 0 ? K : 1, sizeof(int));
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0) continue;
+		sum[3 * id] += S.pos_rest[i].x; sum[3 * id + 1] += S.pos_rest[i].y; sum[3 * id + 2] += S.pos_rest[i].z;
+		S.obj_count[id]++;
+	}
+	S.obj_c0 = malloc(sizeof(float) * 3 * (K > 0 ? K : 1));
+	S.obj_shift = malloc(sizeof(double) * 3 * (K > 0 ? K : 1));
+	for (int k = 0; k < K; ++k)
+		for (int a = 0; a < 3; ++a) {
+			const int c = S.obj_count[k] > 0 ? S.obj_count[k] : 1;
+			S.obj_c0[3 * k + a] = (float)(sum[3 * k + a] / c);
+			S.obj_shift[3 * k + a] = (double)S.obj_c0[3 * k + a];
+		}
+	free(sum);
+	S.obj_q = calloc(3 * (size_t)N, sizeof(double));
+	S.obj_sumq = calloc(3 * (size_t)(K > 0 ? K : 1), sizeof(double));
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0) continue;
+		S.obj_q[3 * i] = (double)(S.pos_rest[i].x - S.obj_c0[3 * id]);
+		S.obj_q[3 * i + 1] = (double)(S.pos_rest[i].y - S.obj_c0[3 * id + 1]);
+		S.obj_q[3 * i + 2] = (double)(S.pos_rest[i].z - S.obj_c0[3 * id + 2]);
+		for (int a = 0; a < 3; ++a) S.obj_sumq[3 * id + a] += S.obj_q[3 * i + a];
+	}
+	S.obj_params = calloc(16 * (size_t)(K > 0 ? K : 1), sizeof(float));
+	S.obj_disp = calloc(K > 0 ? K : 1, sizeof(float));
+	S.obj_boxes = calloc(6 * (size_t)(K > 0 ? K : 1), sizeof(float));
+	S.obj_accum = calloc(N, sizeof(f3));
+	S.sc_act = calloc(N, 1);
+	if (!S.obj_w) {
+		S.obj_w = malloc(sizeof(float) * N);
+		for (int i = 0; i < N; ++i) S.obj_w[i] = 1.0f;
+	}
+	S.obj_shift_valid = 0;
+	S.obj_cache = 1;
+}
+
+static int object_on(void) { return P.obj_shape > 0.0f && S.obj_k > 0; }
+static int object_on_ensure(void)
+{
+	if (!(P.obj_shape > 0.0f)) return 0;
+	obj_ensure_cache();
+	return object_on();
+}
+
+/* objectShapeAccumKernel + objectShapeSolveKernel + objectBoxesKernel +
+ * objectShapeMatchKernel, in that order, on the predicted positions */
+static void object_step(f3* pos)
+{
+	const int N = S.n, K = S.obj_k;
+	const int wOn = S.att_active && g_obj_gpu && K <= OBJ_MAX_K;
+	const int stride = wOn ? 16 : 12;
+	double* sums = calloc((size_t)K * 16, sizeof(double));
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0) continue;
+		const f3 p = pos[i];
+		const double dx = (double)p.x - S.obj_shift[3 * id], dy = (double)p.y - S.obj_shift[3 * id + 1],
+			dz = (double)p.z - S.obj_shift[3 * id + 2];
+		const double qx = S.obj_q[3 * i], qy = S.obj_q[3 * i + 1], qz = S.obj_q[3 * i + 2];
+		double v[16] = { dx, dy, dz, dx * qx, dx * qy, dx * qz, dy * qx, dy * qy, dy * qz, dz * qx, dz * qy, dz * qz,
+			0, 0, 0, 0 };
+		if (wOn) {
+			const double w = (double)S.obj_w[i];
+			for (int k = 0; k < 12; ++k) v[k] *= w;
+			v[12] = w; v[13] = w * qx; v[14] = w * qy; v[15] = w * qz;
+		}
+		for (int k = 0; k < stride; ++k) sums[16 * id + k] += v[k];
+	}
+	for (int k = 0; k < K; ++k) {
+		const double* Sk = &sums[16 * k];
+		float* Pk = &S.obj_params[16 * k];
+		const int n = S.obj_count[k];
+		if (n < 4) { Pk[15] = 0.0f; S.obj_disp[k] = 0.0f; continue; }
+		const double W = wOn ? Sk[12] : (double)n;
+		if (!(W > 0.0)) { Pk[15] = 0.0f; S.obj_disp[k] = 0.0f; continue; }
+		const double inv = 1.0 / W;
+		const double dc[3] = { Sk[0] * inv, Sk[1] * inv, Sk[2] * inv };
+		const double* sq = wOn ? &Sk[13] : &S.obj_sumq[3 * k];
+		double a[9];
+		for (int r = 0; r < 3; ++r)
+			for (int c = 0; c < 3; ++c) a[3 * r + c] = Sk[3 + 3 * r + c] - dc[r] * sq[c];
+		double now[3];
+		for (int t = 0; t < 3; ++t) { now[t] = S.obj_shift[3 * k + t] + dc[t]; S.obj_shift[3 * k + t] = now[t]; }
+		S.obj_disp[k] = (float)sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+		double fn = 0.0;
+		for (int t = 0; t < 9; ++t) fn += a[t] * a[t];
+		fn = sqrt(fn);
+		if (!(fn > 1e-300) || !isfinite(fn)) { Pk[15] = 0.0f; continue; }
+		m3 A, R;
+		for (int r = 0; r < 3; ++r)
+			for (int c = 0; c < 3; ++c) A.m[c][r] = (float)(a[3 * r + c] / fn);
+		if (!shape_rotation_double(&A, &R)) { Pk[15] = 0.0f; continue; }
+		for (int t = 0; t < 3; ++t) {
+			Pk[t] = wOn ? (float)((double)S.obj_c0[3 * k + t] + Sk[13 + t] * inv) : S.obj_c0[3 * k + t];
+			Pk[3 + t] = (float)now[t];
+			for (int cc = 0; cc < 3; ++cc) Pk[6 + 3 * t + cc] = R.m[cc][t];
+		}
+		Pk[15] = 1.0f;
+	}
+	free(sums);
+	if (P.sc_enabled && K <= OBJ_MAX_K) {
+		for (int k = 0; k < K; ++k)
+			for (int a = 0; a < 6; ++a) S.obj_boxes[6 * k + a] = (a < 3) ? FLT_MAX : -FLT_MAX;
+		for (int i = 0; i < N; ++i) {
+			const int id = S.obj_id[i];
+			const f3 p = pos[i];
+			if (id < 0 || !f3_finite(p)) continue;
+			float* b = &S.obj_boxes[6 * id];
+			b[0] = fminf(b[0], p.x); b[1] = fminf(b[1], p.y); b[2] = fminf(b[2], p.z);
+			b[3] = fmaxf(b[3], p.x); b[4] = fmaxf(b[4], p.y); b[5] = fmaxf(b[5], p.z);
+		}
+	}
+	const float s = P.obj_shape;
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0 || S.inv_mass[i] <= 0.0f) continue;
+		const float* Pk = &S.obj_params[16 * id];
+		if (Pk[15] == 0.0f) continue;
+		const f3 r = S.pos_rest[i], p = pos[i];
+		const float qx = r.x - Pk[0], qy = r.y - Pk[1], qz = r.z - Pk[2];
+		const float gx = Pk[3] + Pk[6] * qx + Pk[7] * qy + Pk[8] * qz;
+		const float gy = Pk[4] + Pk[9] * qx + Pk[10] * qy + Pk[11] * qz;
+		const float gz = Pk[5] + Pk[12] * qx + Pk[13] * qy + Pk[14] * qz;
+		pos[i] = mk3(p.x + s * (gx - p.x), p.y + s * (gy - p.y), p.z + s * (gz - p.z));
+	}
+}
+
+/* selfColActiveKernel (forward.cu:6998-7029) */
+static void sc_active_set(const f3* X, const f3* Pp, float search, float dc)
+{
+	const int K = S.obj_k;
+	float md = 0.0f;
+	for (int k = 0; k < K; ++k) md = fmaxf(md, S.obj_disp[k]);
+	const float inflate = search + 2.0f * md + 2.0f * dc;
+	for (int i = 0; i < S.n; ++i) {
+		const int id = S.obj_id[i];
+		unsigned char a = 0;
+		if (id < 0) a = 1;
+		else {
+			const f3 p = Pp[i], x = X[i];
+			for (int k = 0; k < K; ++k) {
+				if (k == id) continue;
+				const float* b = &S.obj_boxes[6 * k];
+				const float lx = b[0] - inflate, ly = b[1] - inflate, lz = b[2] - inflate;
+				const float hx = b[3] + inflate, hy = b[4] + inflate, hz = b[5] + inflate;
+				const int inP = p.x >= lx && p.x <= hx && p.y >= ly && p.y <= hy && p.z >= lz && p.z <= hz;
+				const int inX = x.x >= lx && x.x <= hx && x.y >= ly && x.y <= hy && x.z >= lz && x.z <= hz;
+				if (inP || inX) { a = 1; break; }
+			}
+		}
+		S.sc_act[i] = a;
+	}
+}
+
+/* objectContactPush (forward.cu:11858-11890) and the ground re-projection after it
+ * (forward.cu:12587-12597) */
+static void object_contact_push(f3* pos)
+{
+	const int N = S.n, K = S.obj_k;
+	float* sums = calloc((size_t)K * 4, sizeof(float));
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0) continue;
+		const f3 a = S.obj_accum[i];
+		if (!(a.x * a.x + a.y * a.y + a.z * a.z > 1e-30f)) continue;
+		float* Sm = &sums[4 * id];
+		Sm[0] += a.x; Sm[1] += a.y; Sm[2] += a.z; Sm[3] += 1.0f;
+	}
+	float* T = calloc((size_t)K * 4, sizeof(float));
+	for (int k = 0; k < K; ++k) {
+		const float n = sums[4 * k + 3];
+		if (!(n > 0.0f)) continue;
+		const float sc = P.obj_shape / n;
+		const float tx = sums[4 * k] * sc, ty = sums[4 * k + 1] * sc, tz = sums[4 * k + 2] * sc;
+		if (!isfinite(tx) || !isfinite(ty) || !isfinite(tz)) continue;
+		T[4 * k] = tx; T[4 * k + 1] = ty; T[4 * k + 2] = tz; T[4 * k + 3] = 1.0f;
+	}
+	for (int i = 0; i < N; ++i) {
+		const int id = S.obj_id[i];
+		if (id < 0 || S.inv_mass[i] <= 0.0f) continue;
+		const float* Tk = &T[4 * id];
+		if (Tk[3] == 0.0f) continue;
+		const f3 a = S.obj_accum[i];
+		if (a.x * a.x + a.y * a.y + a.z * a.z > 1e-30f) continue;
+		pos[i] = mk3(pos[i].x + Tk[0], pos[i].y + Tk[1], pos[i].z + Tk[2]);
+	}
+	free(sums);
+	free(T);
+	if (P.ground_on) ground_project(pos);
+}
+
+/* ------------------------------------------------------------------------- */
 /* one step: runXPBDSimulation (forward.cu:12038-12751) via stepPhysicsOnly  */
 /* (forward.cu:13253-13264)                                                   */
 /* ------------------------------------------------------------------------- */
@@ -2102,10 +2335,18 @@ static void run_step(void)
 	if (distGS) memset(S.gs_lam, 0, sizeof(float) * S.gs_nedges);
 	const int groundOn = P.ground_on;
 	predict(gravity, dt);
+	const int objOn = object_on_ensure();
+	int limited = 0;
+	if (objOn) {
+		limited = P.sc_enabled && !P.sc_within && S.obj_shift_valid && S.obj_k >= 1 && S.obj_k <= OBJ_MAX_K;
+		object_step(S.pos_next);
+		S.obj_shift_valid = 1;
+	}
 	int scContacts = 0;
 	if (P.sc_enabled) {
-		sc_build(S.pos_curr, S.pos_next);
+		sc_build_active(S.pos_curr, S.pos_next, limited);
 		scContacts = S.sc_contacts;
+		if (objOn && scContacts > 0) memset(S.obj_accum, 0, sizeof(f3) * N);
 	}
 	else S.sc_contacts = 0;
 	if (P.kin_count > 0) {
@@ -2141,10 +2382,11 @@ static void run_step(void)
 			shape_matching(pin, pout, dt);
 			f3* t = pin; pin = pout; pout = t;
 		}
-		if (P.sc_enabled && scContacts > 0) sc_solve_apply(pin);
+		if (P.sc_enabled && scContacts > 0) sc_solve_apply(pin, objOn ? S.obj_accum : NULL);
 		if (P.kin_count > 0) colliders_project(pin, it == P.iters - 1);
 		if (groundOn) ground_project(pin);
 	}
+	if (objOn && P.sc_enabled && scContacts > 0) object_contact_push(pin);
 	velocity_commit(pin, dt, groundOn);
 	if (P.jstats && P.use_volume >= 0) volume_j_stats();
 }
@@ -2248,14 +2490,16 @@ EXPORT void xpbd_set_ground(int enabled, float ux, float uy, float uz, float hei
 	P.ground_gravity = fmaxf(0.0f, gravity);
 }
 
+/* setObjectModeParams(stiffness, no body contact, 50) (xpbd_capi.cu:148, forward.cu:4464-4477) */
 EXPORT void xpbd_set_object_shape(float stiffness)
 {
 	float s = fminf(fmaxf(stiffness, 0.0f), 1.0f);
 	if (!isfinite(s)) s = 0.0f;
-	P.obj_shape = s; /* object mode is outside the restatement */
+	P.obj_shape = s;
 }
 
-EXPORT void xpbd_set_object_shape_gpu(int enabled) { (void)enabled; }
+/* setObjectShapeGPU (forward.cu:4521): the weighted fit while pinned (1) or the plain fit */
+EXPORT void xpbd_set_object_shape_gpu(int enabled) { g_obj_gpu = enabled != 0; }
 
 /* setKinematicColliders (forward.cu:4478-4500) */
 EXPORT void xpbd_set_colliders(int count, const int* types, const float* poses, const float* dims, float margin,
@@ -2320,7 +2564,6 @@ EXPORT int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 /* setAttachedParticles + attachApplyKernel (forward.cu:6714-6725, 6759-6788) */
 EXPORT int xpbd_set_attached(int count, const int* idx, const float* pos, float weight)
 {
-	(void)weight;
 	if (!S.stepped) return fail("xpbd_set_attached: no step yet");
 	const int N = S.n;
 	if (S.att_active) memcpy(S.inv_mass, S.inv_mass_saved, sizeof(float) * N);
@@ -2329,12 +2572,16 @@ EXPORT int xpbd_set_attached(int count, const int* idx, const float* pos, float 
 		if (!S.inv_mass_saved) S.inv_mass_saved = malloc(sizeof(float) * N);
 		memcpy(S.inv_mass_saved, S.inv_mass, sizeof(float) * N);
 	}
+	/* rigid-fit weights of object mode: 1, pinned max(weight, 1) (forward.cu:6774, 6724) */
+	if (!S.obj_w) S.obj_w = malloc(sizeof(float) * N);
+	for (int i = 0; i < N; ++i) S.obj_w[i] = 1.0f;
 	for (int k = 0; k < count; ++k) {
 		const int i = idx[k];
 		if (i < 0 || i >= N) continue;
 		S.inv_mass[i] = 0.0f;
 		S.pos_curr[i] = mk3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]);
 		S.vel[i] = mk3(0, 0, 0);
+		S.obj_w[i] = fmaxf(weight, 1.0f);
 	}
 	S.att_active = 1;
 	return 0;

@@ -177,6 +177,15 @@ def misc_case(ref):
     return out
 
 
+def object_blobs_case(ref):
+    """Object mode (forward.cu:12141-12166) on two objects pushed together by pinned
+    grippers: weighted rigid fit, cross-object self-collision limited to the boxes of the
+    other object, contact push."""
+    sc, grippers = two_blob_scene()
+    scen = scenes.Scenario(sc, grippers, self_collision=True, within_body=False, object_shape=0.9)
+    return scenario_case(ref, scen, [1, 10, 30])
+
+
 def chainmail_case(ref):
     """ChainMail waves through the reference's runChainmailGPU (forward.cu:12808-13006)."""
     sc = scenes.chainmail_scene(4000, 21)
@@ -197,7 +206,8 @@ def main():
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     names = ["graph_n3000_r1", "graph_n3000_r2", "graph_n3000_k1", "plain_n4000", "plain_n4000_k1",
-             "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000", "chainmail_n4000"]
+             "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000", "chainmail_n4000", "object_blobs",
+             "object_plain_n4000"]
     if not args.only:
         # One process per case: the reference keeps its solver state in file-static globals.
         import subprocess
@@ -224,6 +234,9 @@ def main():
         "selfcol_blobs": lambda: selfcol_case(ref),
         "misc_n2000": lambda: misc_case(ref),
         "chainmail_n4000": lambda: chainmail_case(ref),
+        "object_blobs": lambda: object_blobs_case(ref),
+        "object_plain_n4000": lambda: scenario_case(
+            ref, scenes.plain_scene_scenario(4000, 3, pins=40, object_shape=0.9), [1, 10, 100]),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only.split(","):

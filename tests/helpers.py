@@ -116,6 +116,10 @@ def scenario_for(case):
         return scenes.plain_scene_scenario(20000, 0)
     if case == "selfcol_blobs":
         return scenes.Scenario(*two_blob_scene(), self_collision=True, within_body=True)
+    if case == "object_blobs":
+        return scenes.Scenario(*two_blob_scene(), self_collision=True, within_body=False, object_shape=0.9)
+    if case == "object_plain_n4000":
+        return scenes.plain_scene_scenario(4000, 3, pins=40, object_shape=0.9)
     raise KeyError(case)
 
 

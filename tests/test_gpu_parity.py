@@ -43,7 +43,8 @@ def test_cluster_topology_bit_exact(lib, case):
     assert H.max_err_over_diag(lib.positions(), g["pos_step1"], H.scenes.bbox_diagonal(sc["pos"])) < H.TOL_1STEP
 
 
-@pytest.mark.parametrize("case", ["plain_n4000", "plain_n4000_k1", "plain_n4000_fpolar", "plain_n4000_gs"])
+@pytest.mark.parametrize("case", ["plain_n4000", "plain_n4000_k1", "plain_n4000_fpolar", "plain_n4000_gs",
+                                  "object_plain_n4000"])
 def test_scenario_positions(lib, case):
     g = H.load_golden(case)
     s = H.scenario_for(case)
@@ -283,3 +284,25 @@ def test_error_behaviour(lib):
     with pytest.raises(RuntimeError, match="not implemented"):
         lib.set_contact_shape(1)
     lib.destroy()
+
+
+def test_object_mode_two_objects(lib):
+    """Object mode on two objects pushed together: rigid fit weighted by the pins, cross-object
+    self-collision limited to the other object's box, contact push (forward.cu:12141-12166,
+    11796-11849, 12587-12597)."""
+    g = H.load_golden("object_blobs")
+    s = H.scenario_for("object_blobs")
+    s.setup(lib)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    done = 0
+    for c in g["checkpoints"]:
+        s.advance(lib, int(c) - done)
+        done = int(c)
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(lib.positions(), g[f"pos_{c}"], diag) < tol, c
+        st = lib.self_collision_stats()
+        ref = g[f"sc_stats_{c}"]
+        assert abs(st[1] - int(ref[1])) <= max(5, 0.01 * int(ref[1])), (c, st, ref)   # active Gaussians
+    assert int(g["sc_stats_30"][1]) < len(g["in_pos"])   # the box filter left some out
+    lib.set_object_shape(0.0)
+

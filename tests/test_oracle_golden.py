@@ -39,7 +39,8 @@ def test_cluster_topology_bit_exact(orc, case):
     assert H.max_err_over_diag(orc.positions(), g["pos_step1"], H.scenes.bbox_diagonal(sc["pos"])) < H.TOL_1STEP
 
 
-@pytest.mark.parametrize("case", ["plain_n4000", "plain_n4000_k1", "plain_n4000_fpolar", "plain_n4000_gs"])
+@pytest.mark.parametrize("case", ["plain_n4000", "plain_n4000_k1", "plain_n4000_fpolar", "plain_n4000_gs",
+                                  "object_plain_n4000"])
 def test_scenario_positions(orc, case):
     g = H.load_golden(case)
     s = H.scenario_for(case)
@@ -179,3 +180,25 @@ def test_chainmail_matches_reference(orc):
         np.testing.assert_array_equal(t, g[f"time_{tag}"])
         assert H.max_err_over_diag(pos, g[f"pos_{tag}"], diag) < H.TOL_1STEP
     assert (g["time_run1"] < 1e8).sum() > 1000   # the wave travelled
+
+
+def test_object_mode_two_objects(orc):
+    """Object mode on two objects pushed together: rigid fit weighted by the pins, cross-object
+    self-collision limited to the other object's box, contact push (forward.cu:12141-12166,
+    11796-11849, 12587-12597)."""
+    g = H.load_golden("object_blobs")
+    s = H.scenario_for("object_blobs")
+    s.setup(orc)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    done = 0
+    for c in g["checkpoints"]:
+        s.advance(orc, int(c) - done)
+        done = int(c)
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(orc.positions(), g[f"pos_{c}"], diag) < tol, c
+        st = orc.self_collision_stats()
+        ref = g[f"sc_stats_{c}"]
+        assert abs(st[1] - int(ref[1])) <= max(5, 0.01 * int(ref[1])), (c, st, ref)   # active Gaussians
+    assert int(g["sc_stats_30"][1]) < len(g["in_pos"])   # the box filter left some out
+    orc.set_object_shape(0.0)
+
