@@ -126,6 +126,7 @@ public:
 
 	// ---- host topology (caller index space) and the internal order ----
 	std::vector<int> perm, inv;
+	std::vector<unsigned long long> lcode;   // Morton code in its component's box, per caller index
 	HostGraph graph;
 	HostClusters clusters;
 	HostEdgeColoring coloring;
@@ -160,6 +161,7 @@ public:
 	DBuf<int> off, nbr;
 	DBuf<float> ndist, nstiff, lam;
 	DBuf<int> vol_off, vol_idx, rev_off, rev_idx, mat_type, vol_gs_order;
+	DBuf<int> vol_idx_s, rev_idx_s;  // the same lists, rows sorted along the Morton curve
 	DBuf<float> det_rest, v_rest, rest_len, sigma_rest, lam_vol;
 	DBuf<float4> rec;
 	DBuf<int2> gs_edge;
@@ -245,6 +247,7 @@ public:
 		obj_shift_valid = false;
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
+		vol_idx_s.release(); rev_idx_s.release();
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
@@ -283,6 +286,29 @@ public:
 	// inv[perm[r]] = r.  Every topology is built in the caller's index space — the
 	// reference's construction order is index-dependent — and only then relabelled, with
 	// every list keeping its order, so the kernels see exactly the reference's sequences.
+	// 63-bit Morton code of each Gaussian's rest position within the box `lo`..`hi`
+	static unsigned long long morton_code(const float* p, const float* lo, const float* hi)
+	{
+		auto spread = [](unsigned long long v) {
+			v &= 0x1fffffull;
+			v = (v | v << 32) & 0x1f00000000ffffull;
+			v = (v | v << 16) & 0x1f0000ff0000ffull;
+			v = (v | v << 8) & 0x100f00f00f00f00full;
+			v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+			v = (v | v << 2) & 0x1249249249249249ull;
+			return v;
+		};
+		unsigned long long c = 0;
+		for (int a = 0; a < 3; ++a) {
+			const float ext = hi[a] > lo[a] ? hi[a] - lo[a] : 1.0f;
+			float u = (p[a] - lo[a]) / ext;
+			if (!std::isfinite(u)) u = 0.0f;
+			u = std::min(std::max(u, 0.0f), 1.0f);
+			c |= spread((unsigned long long)(u * 2097151.0f)) << a;
+		}
+		return c;
+	}
+
 	void compute_order()
 	{
 		perm.resize(n);
@@ -296,29 +322,36 @@ public:
 					if (std::isfinite(v)) { lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
 				}
 			std::vector<unsigned long long> code(n);
-			auto spread = [](unsigned long long v) {
-				v &= 0x1fffffull;
-				v = (v | v << 32) & 0x1f00000000ffffull;
-				v = (v | v << 16) & 0x1f0000ff0000ffull;
-				v = (v | v << 8) & 0x100f00f00f00f00full;
-				v = (v | v << 4) & 0x10c30c30c30c30c3ull;
-				v = (v | v << 2) & 0x1249249249249249ull;
-				return v;
-			};
-			for (int i = 0; i < n; ++i) {
-				unsigned long long c = 0;
-				for (int a = 0; a < 3; ++a) {
-					const float ext = hi[a] > lo[a] ? hi[a] - lo[a] : 1.0f;
-					float u = (in_pos[3 * i + a] - lo[a]) / ext;
-					if (!std::isfinite(u)) u = 0.0f;
-					u = std::min(std::max(u, 0.0f), 1.0f);
-					c |= spread((unsigned long long)(u * 2097151.0f)) << a;
-				}
-				code[i] = c;
-			}
+			for (int i = 0; i < n; ++i) code[i] = morton_code(&in_pos[3 * i], lo, hi);
 			std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return code[a] < code[b]; });
 		}
 		for (int r = 0; r < n; ++r) inv[perm[r]] = r;
+		// Morton code within each connected component's own box: orders the rows of the
+		// 4- and 8-lane volume lists the same way whatever the renumbering and whatever
+		// other objects share the scene
+		std::vector<int> parent(n);
+		for (int i = 0; i < n; ++i) parent[i] = i;
+		auto root = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
+		for (int i = 0; i < n; ++i)
+			for (int e = graph.off[i]; e < graph.off[i + 1]; ++e) {
+				const int j = graph.nbr[e];
+				if (j < 0 || j >= n) continue;
+				const int ri = root(i), rj = root(j);
+				if (ri != rj) parent[ri] = rj;
+			}
+		std::vector<float> clo(3 * (size_t)n, FLT_MAX), chi(3 * (size_t)n, -FLT_MAX);
+		for (int i = 0; i < n; ++i) {
+			const int r = root(i);
+			for (int a = 0; a < 3; ++a) {
+				const float v = in_pos[3 * i + a];
+				if (std::isfinite(v)) { clo[3 * r + a] = std::min(clo[3 * r + a], v); chi[3 * r + a] = std::max(chi[3 * r + a], v); }
+			}
+		}
+		lcode.resize(n);
+		for (int i = 0; i < n; ++i) {
+			const int r = root(i);
+			lcode[i] = morton_code(&in_pos[3 * i], &clo[3 * r], &chi[3 * r]);
+		}
 	}
 
 	// caller-order CSR (off[N+1], idx) -> internal order, neighbour order kept
@@ -446,6 +479,27 @@ public:
 		CK(cudaMemcpyAsync(vol_idx.p, vidx_i.data(), sizeof(int) * vidx_i.size(), cudaMemcpyHostToDevice, stream));
 		CK(cudaMemcpyAsync(rev_off.p, roff_i.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
 		CK(cudaMemcpyAsync(rev_idx.p, ridx_i.data(), sizeof(int) * ridx_i.size(), cudaMemcpyHostToDevice, stream));
+		{
+			// copies of both lists with every row sorted along the Morton curve of the component
+			// (caller index breaking ties), for the 4- and 8-lane kernels: the lanes of a cluster
+			// read neighbouring Gaussians (fewer cache lines per warp load)
+			auto sorted_rows = [&](const std::vector<int>& off_i, std::vector<int> idx_i) {
+				auto key = [&](int a) {   // (code in the component's box, caller index); invalid last
+					if (a < 0 || a >= n) return std::make_pair(~0ull, INT_MAX);
+					return std::make_pair(lcode[perm[a]], perm[a]);
+				};
+				for (int r = 0; r < n; ++r)
+					std::sort(idx_i.begin() + off_i[r], idx_i.begin() + off_i[r + 1],
+						[&](int a, int b) { return key(a) < key(b); });
+				return idx_i;
+			};
+			const auto vs = sorted_rows(voff_i, vidx_i);
+			const auto rs = sorted_rows(roff_i, ridx_i);
+			CK(vol_idx_s.alloc(vs.size())); CK(rev_idx_s.alloc(rs.size()));
+			CK(cudaMemcpyAsync(vol_idx_s.p, vs.data(), sizeof(int) * vs.size(), cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(rev_idx_s.p, rs.data(), sizeof(int) * rs.size(), cudaMemcpyHostToDevice, stream));
+			CK(cudaStreamSynchronize(stream));
+		}
 		vol_gs_order.release();
 		std::vector<int> order_i(clusters.gs_order.size());
 		for (size_t t = 0; t < order_i.size(); ++t) order_i[t] = inv[clusters.gs_order[t]];
@@ -925,11 +979,11 @@ public:
 					else if (la == 4 && S.lanes_a == 0 && clusters.avg_members > 64.0f)
 						// more than 64 members: 8 lanes x 16 staged slots hold up to 128
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8, dev::kSmemBlock), dim3(dev::kSmemBlock),
-							dev::k_volume_solve_smem<8, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx.p,
+							dev::k_volume_solve_smem<8, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p,
 							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 4)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4, dev::kSmemBlock), dim3(dev::kSmemBlock),
-							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx.p,
+							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p,
 							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 3)   // 4 lanes, positions re-read from L1 instead of shared memory
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_slots<4, 16, false>, N, dp,
@@ -950,7 +1004,7 @@ public:
 							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B, dev::k_volume_gather_group<4>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)rest_len.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
 							(const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
