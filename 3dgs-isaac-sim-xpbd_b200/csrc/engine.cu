@@ -974,7 +974,7 @@ public:
 							lam_vol.p, rec.p, rl);
 					else if (la == 8)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_slots<8, 8, true>, N, dp,
-							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 4 && S.lanes_a == 0 && clusters.avg_members > 64.0f)
 						// more than 64 members: 8 lanes x 16 staged slots hold up to 128
@@ -987,11 +987,11 @@ public:
 							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 3)   // 4 lanes, positions re-read from L1 instead of shared memory
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_slots<4, 16, false>, N, dp,
-							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else if (la == 2)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 2), B, dev::k_volume_solve_slots<2, 32, false>, N, dp,
-							cpin, (const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p,
+							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
 					else
 						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
@@ -1001,7 +1001,7 @@ public:
 							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
 					else if (lb == 8)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B, dev::k_volume_gather_group<4>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)rest_len.p);
