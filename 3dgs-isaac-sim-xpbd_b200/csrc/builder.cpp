@@ -137,8 +137,9 @@ void members_of(const HostGraph& g, const float* rest, int i, int k, int cap, Sc
 	}
 }
 
-void color_clusters(int n, const std::vector<std::vector<int>>& members, const std::vector<char>& leader,
-	HostClusters& out)
+// members_of_leader(l) -> (pointer, count) of leader l's member list
+template <typename Members>
+void color_clusters(int n, const Members& members_of_leader, const std::vector<char>& leader, HostClusters& out)
 {
 	out.gs_order.clear();
 	out.gs_color_off.clear();
@@ -164,8 +165,11 @@ void color_clusters(int n, const std::vector<std::vector<int>>& members, const s
 			}
 		};
 		forbid(l);
-		for (int j : members[l])
+		const auto ml = members_of_leader(l);
+		for (int t = 0; t < ml.second; ++t) {
+			const int j = ml.first[t];
 			if (j >= 0 && j < n) forbid(j);
+		}
 		int c = 0;
 		while (c < num_colors && stamp[c] == l) ++c;
 		color[l] = c;
@@ -181,7 +185,63 @@ void color_clusters(int n, const std::vector<std::vector<int>>& members, const s
 		if (leader[l]) out.gs_order[fill[color[l]]++] = l;
 }
 
+// Member CSR, transposed membership (leader self entry first, then clusters in leader
+// order) and the cluster colouring, from the leaders' member lists.
+template <typename Members>
+void finish_clusters(int n, const Members& members_of_leader, const std::vector<char>& leader, HostClusters& out)
+{
+	out.vol_off.assign(n + 1, 0);
+	for (int i = 0; i < n; ++i) out.vol_off[i + 1] = out.vol_off[i] + members_of_leader(i).second;
+	out.vol_idx.resize(std::max(out.vol_off[n], 1));
+	for (int i = 0; i < n; ++i) {
+		const auto mi = members_of_leader(i);
+		std::copy(mi.first, mi.first + mi.second, out.vol_idx.begin() + out.vol_off[i]);
+	}
+	std::vector<int> rc(n, 0);
+	for (int i = 0; i < n; ++i) rc[i] += leader[i] ? 1 : 0;
+	for (int i = 0; i < n; ++i) {
+		const auto mi = members_of_leader(i);
+		for (int t = 0; t < mi.second; ++t) ++rc[mi.first[t]];
+	}
+	out.rev_off.assign(n + 1, 0);
+	for (int i = 0; i < n; ++i) out.rev_off[i + 1] = out.rev_off[i] + rc[i];
+	out.rev_idx.resize(std::max(out.rev_off[n], 1));
+	std::vector<int> cur(out.rev_off.begin(), out.rev_off.end() - 1);
+	for (int i = 0; i < n; ++i)
+		if (leader[i]) out.rev_idx[cur[i]++] = i;
+	for (int i = 0; i < n; ++i) {
+		const auto mi = members_of_leader(i);
+		for (int t = 0; t < mi.second; ++t) out.rev_idx[cur[mi.first[t]]++] = i;
+	}
+	out.avg_members = out.leaders > 0 ? (float)((double)out.vol_off[n] / out.leaders) : 0.0f;
+	color_clusters(n, members_of_leader, leader, out);
+}
+
 }  // namespace
+
+void build_clusters_from_members(const HostGraph& g, const float* rest, int ring_k, int cap, const int* flat,
+	const int* counts, HostClusters& out)
+{
+	// every Gaussian is a leader (leader spacing 1); lists with count -1 are built here
+	const int n = g.n;
+	std::vector<char> leader(n, 1);
+	out.leaders = n;
+	std::vector<std::vector<int>> host_lists;
+	std::vector<int> host_at(n, -1);
+	{
+		Scratch sc(n);
+		for (int i = 0; i < n; ++i)
+			if (counts[i] < 0) {
+				host_at[i] = (int)host_lists.size();
+				host_lists.emplace_back();
+				members_of(g, rest, i, ring_k, cap, sc, host_lists.back());
+			}
+	}
+	finish_clusters(n, [&](int i) {
+		if (host_at[i] >= 0) return std::make_pair((const int*)host_lists[host_at[i]].data(), (int)host_lists[host_at[i]].size());
+		return std::make_pair(flat + (size_t)i * cap, counts[i]);
+	}, leader, out);
+}
 
 void build_clusters(const HostGraph& g, const float* rest, int ring_k, int cap, int leader_min_hop, HostClusters& out)
 {
@@ -255,26 +315,8 @@ void build_clusters(const HostGraph& g, const float* rest, int ring_k, int cap, 
 		}
 		out.leaders = count;
 	}
-	out.vol_off.assign(n + 1, 0);
-	for (int i = 0; i < n; ++i) out.vol_off[i + 1] = out.vol_off[i] + (int)members[i].size();
-	out.vol_idx.resize(std::max(out.vol_off[n], 1));
-	for (int i = 0; i < n; ++i)
-		std::copy(members[i].begin(), members[i].end(), out.vol_idx.begin() + out.vol_off[i]);
-	// transposed membership: leader self entry first, then clusters in leader order
-	std::vector<int> rc(n, 0);
-	for (int i = 0; i < n; ++i) rc[i] += leader[i] ? 1 : 0;
-	for (int i = 0; i < n; ++i)
-		for (int j : members[i]) ++rc[j];
-	out.rev_off.assign(n + 1, 0);
-	for (int i = 0; i < n; ++i) out.rev_off[i + 1] = out.rev_off[i] + rc[i];
-	out.rev_idx.resize(std::max(out.rev_off[n], 1));
-	std::vector<int> cur(out.rev_off.begin(), out.rev_off.end() - 1);
-	for (int i = 0; i < n; ++i)
-		if (leader[i]) out.rev_idx[cur[i]++] = i;
-	for (int i = 0; i < n; ++i)
-		for (int j : members[i]) out.rev_idx[cur[j]++] = i;
-	out.avg_members = out.leaders > 0 ? (float)((double)out.vol_off[n] / out.leaders) : 0.0f;
-	color_clusters(n, members, leader, out);
+	finish_clusters(n, [&](int i) { return std::make_pair((const int*)members[i].data(), (int)members[i].size()); },
+		leader, out);
 }
 
 void build_edge_coloring(const HostGraph& g, HostEdgeColoring& out)

@@ -10,7 +10,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdarg>
@@ -20,6 +22,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/xpbd_capi.h"
@@ -47,6 +50,26 @@ static int fail(const char* fmt, ...)
 		if (e_ != cudaSuccess) return fail("%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
 			__FILE__, __LINE__);                                                           \
 	} while (0)
+
+// fn(begin, end) over [0, n) in chunks on all host threads (upload-time host work)
+template <typename F>
+void parallel_for(int n, F fn)
+{
+	const int workers = std::max(1, std::min<int>(std::thread::hardware_concurrency(), 64));
+	if (n < 4096 || workers == 1) { fn(0, n); return; }
+	std::atomic<int> next{ 0 };
+	const int chunk = std::max(1024, n / (workers * 8));
+	std::vector<std::thread> pool;
+	for (int w = 0; w < workers; ++w)
+		pool.emplace_back([&]() {
+			for (;;) {
+				const int b = next.fetch_add(chunk);
+				if (b >= n) break;
+				fn(b, std::min(n, b + chunk));
+			}
+		});
+	for (auto& t : pool) t.join();
+}
 
 template <typename T>
 struct DBuf {
@@ -100,6 +123,7 @@ struct Settings {
 	dev::CmMaterial cm{ 1.0f, 0.1f, 0.1f, 0.1f, 1.0f, 1 };   // ChainMail material (forward.cu:66-71)
 	bool cm_frontier = true;         // ChainMail sweeps on work lists (false: every sweep dense)
 	bool obj_gpu = true;             // object mode's weighted device fit (xpbd_set_object_shape_gpu)
+	bool gpu_builder = true;         // cluster members (BFS + farthest point) built on the GPU
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -157,6 +181,16 @@ public:
 	DBuf<float4> sc_cross, sc_accum;
 	bool obj_shift_valid = false;    // a previous object step set the centroids (boxes usable)
 	bool last_sc_limited = false;    // the last step's self-collision build used the box filter
+	// wall-clock milliseconds of the upload phases (debug_float "build_ms"): graph, order,
+	// state upload, cluster members, cluster lists, sorted copies, rest state, the rest
+	double build_ms[8] = {};
+	std::chrono::steady_clock::time_point build_t0;
+	void build_mark(int phase)
+	{
+		const auto t = std::chrono::steady_clock::now();
+		build_ms[phase] += std::chrono::duration<double, std::milli>(t - build_t0).count();
+		build_t0 = t;
+	}
 	DBuf<float> pos_out3;
 	DBuf<int> off, nbr;
 	DBuf<float> ndist, nstiff, lam;
@@ -362,14 +396,16 @@ public:
 		for (int r = 0; r < n; ++r) off_i[r + 1] = off_i[r] + (off_o[perm[r] + 1] - off_o[perm[r]]);
 		idx_i.resize(std::max(off_i[n], 1));
 		if (src_pos) src_pos->resize(std::max(off_i[n], 1));
-		for (int r = 0; r < n; ++r) {
-			const int o = perm[r];
-			for (int e = off_o[o], d = off_i[r]; e < off_o[o + 1]; ++e, ++d) {
-				const int j = idx_o[e];
-				idx_i[d] = (j >= 0 && j < n) ? inv[j] : j;
-				if (src_pos) (*src_pos)[d] = e;
+		parallel_for(n, [&](int r0, int r1) {
+			for (int r = r0; r < r1; ++r) {
+				const int o = perm[r];
+				for (int e = off_o[o], d = off_i[r]; e < off_o[o + 1]; ++e, ++d) {
+					const int j = idx_o[e];
+					idx_i[d] = (j >= 0 && j < n) ? inv[j] : j;
+					if (src_pos) (*src_pos)[d] = e;
+				}
 			}
-		}
+		});
 	}
 
 	template <typename T>
@@ -398,12 +434,16 @@ public:
 	// ensureChainmailGPU (forward.cu:10519-10845): graph upload, colourings, clusters
 	int build()
 	{
+		for (double& v : build_ms) v = 0.0;
+		build_t0 = std::chrono::steady_clock::now();
 		free_device();
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
 		graph_key.clear();
 		if (ensure_stream()) return -1;
 		build_graph(n, n_edges, in_edges.data(), in_rest.data(), in_stiff.data(), graph);
+		build_mark(0);
 		compute_order();
+		build_mark(1);
 		const int m = graph.off[n];
 		CK(d_perm.alloc(n));
 		CK(cudaMemcpyAsync(d_perm.p, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
@@ -464,13 +504,20 @@ public:
 		CK(cudaStreamSynchronize(stream));
 		++generation;
 		built = true;
+		build_mark(7);
 		return 0;
 	}
 
 	// rebuildVolumeClusters (forward.cu:9814-10403): host BFS/FPS, then rest covariance on the GPU
 	int rebuild_clusters()
 	{
-		build_clusters(graph, in_pos.data(), S.ring_k, S.max_members, S.leader_min_hop, clusters);
+		build_mark(2);
+		if (S.gpu_builder && S.leader_min_hop <= 1 && n > 0) {
+			if (build_members_gpu()) return -1;
+		}
+		else
+			build_clusters(graph, in_pos.data(), S.ring_k, S.max_members, S.leader_min_hop, clusters);
+		build_mark(4);
 		std::vector<int> voff_i, vidx_i, roff_i, ridx_i;
 		relabel_csr(clusters.vol_off, clusters.vol_idx, voff_i, vidx_i);
 		relabel_csr(clusters.rev_off, clusters.rev_idx, roff_i, ridx_i);
@@ -483,22 +530,29 @@ public:
 			// copies of both lists with every row sorted along the Morton curve of the component
 			// (caller index breaking ties), for the 4- and 8-lane kernels: the lanes of a cluster
 			// read neighbouring Gaussians (fewer cache lines per warp load)
+			std::vector<unsigned long long> kcode(n);
+			for (int r = 0; r < n; ++r) kcode[r] = lcode[perm[r]];
 			auto sorted_rows = [&](const std::vector<int>& off_i, std::vector<int> idx_i) {
-				auto key = [&](int a) {   // (code in the component's box, caller index); invalid last
-					if (a < 0 || a >= n) return std::make_pair(~0ull, INT_MAX);
-					return std::make_pair(lcode[perm[a]], perm[a]);
+				// (code in the component's box, caller index); invalid entries last
+				auto less = [&](int a, int b) {
+					const bool va = a >= 0 && a < n, vb = b >= 0 && b < n;
+					if (!va || !vb) return va && !vb;
+					if (kcode[a] != kcode[b]) return kcode[a] < kcode[b];
+					return perm[a] < perm[b];
 				};
-				for (int r = 0; r < n; ++r)
-					std::sort(idx_i.begin() + off_i[r], idx_i.begin() + off_i[r + 1],
-						[&](int a, int b) { return key(a) < key(b); });
+				parallel_for(n, [&](int r0, int r1) {
+					for (int r = r0; r < r1; ++r) std::sort(idx_i.begin() + off_i[r], idx_i.begin() + off_i[r + 1], less);
+				});
 				return idx_i;
 			};
+			build_mark(4);
 			const auto vs = sorted_rows(voff_i, vidx_i);
 			const auto rs = sorted_rows(roff_i, ridx_i);
 			CK(vol_idx_s.alloc(vs.size())); CK(rev_idx_s.alloc(rs.size()));
 			CK(cudaMemcpyAsync(vol_idx_s.p, vs.data(), sizeof(int) * vs.size(), cudaMemcpyHostToDevice, stream));
 			CK(cudaMemcpyAsync(rev_idx_s.p, rs.data(), sizeof(int) * rs.size(), cudaMemcpyHostToDevice, stream));
 			CK(cudaStreamSynchronize(stream));
+			build_mark(5);
 		}
 		vol_gs_order.release();
 		std::vector<int> order_i(clusters.gs_order.size());
@@ -517,6 +571,7 @@ public:
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
 		graph_key.clear();
 		++generation;
+		build_mark(6);
 		return 0;
 	}
 
@@ -686,6 +741,33 @@ public:
 		CK(cudaGetLastError());
 		if (cm_publish(cm_time_out.p)) return -1;
 		return sync();
+	}
+
+	// k-ring BFS + farthest-point members of every leader on the GPU (caller index space),
+	// then the CSRs and colouring on the host (builder.cpp)
+	int build_members_gpu()
+	{
+		const int cap = std::max(1, S.max_members);
+		const int m = graph.off[n];
+		DBuf<int> d_off, d_nbr, d_members, d_counts;
+		DBuf<float> d_rest3;
+		CK(d_off.alloc(n + 1)); CK(d_nbr.alloc(std::max(m, 1))); CK(d_rest3.alloc(3 * (size_t)n));
+		CK(d_members.alloc((size_t)n * cap)); CK(d_counts.alloc(n));
+		CK(cudaMemcpyAsync(d_off.p, graph.off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
+		if (m > 0) CK(cudaMemcpyAsync(d_nbr.p, graph.nbr.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
+		CK(cudaMemcpyAsync(d_rest3.p, in_pos.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
+		CK(cudaFuncSetAttribute(dev::k_build_members, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dev::kBuildSmem));
+		const int blocks = std::min((n + dev::kBuildWarps - 1) / dev::kBuildWarps, 148 * 16);
+		dev::k_build_members<<<blocks, dev::kBuildWarps * 32, dev::kBuildSmem, stream>>>(n, d_off.p, d_nbr.p, d_rest3.p,
+			S.ring_k, cap, d_members.p, d_counts.p);
+		CK(cudaGetLastError());
+		std::vector<int> flat((size_t)n * cap), counts(n);
+		CK(cudaMemcpyAsync(counts.data(), d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+		CK(cudaMemcpyAsync(flat.data(), d_members.p, sizeof(int) * (size_t)n * cap, cudaMemcpyDeviceToHost, stream));
+		CK(cudaStreamSynchronize(stream));
+		build_mark(3);
+		build_clusters_from_members(graph, in_pos.data(), S.ring_k, cap, flat.data(), counts.data(), clusters);
+		return 0;
 	}
 
 	int ensure_coloring()
@@ -1569,6 +1651,8 @@ XPBD_API void xpbd_b200_chainmail_set_material(float global_scale, float air, fl
 
 XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled) { engine().S.cm_frontier = enabled != 0; }
 
+XPBD_API void xpbd_b200_set_gpu_builder(int enabled) { engine().S.gpu_builder = enabled != 0; }
+
 XPBD_API int xpbd_b200_chainmail_seed(int count, const int* idx, const float* delta)
 {
 	Engine& E = *cur_engine();
@@ -1846,6 +1930,10 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 			else v[i] = tmp[r].w;
 		}
 		return copy_host(v, (long long)v.size(), out, cap);
+	}
+	if (s == "build_ms") {
+		const std::vector<float> v(E.build_ms, E.build_ms + 8);
+		return copy_host(v, 8, out, cap);
 	}
 	if (s == "cluster_coef") {   // the last iteration's per-cluster coefficient (0: inactive)
 		std::vector<float4> tmp(3 * (size_t)N);

@@ -2189,6 +2189,162 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 }
 
 // ===========================================================================
+// Upload-time cluster builder on the GPU (every Gaussian a leader): k-ring BFS and the
+// farthest-point subsample of rebuildVolumeClusters (forward.cu:9814-10033), one warp
+// per leader, in the caller's index space.  Same visiting order, same candidate order,
+// same float distances (explicit roundings, as the host computes them) and the same
+// first-maximum ties as the host builder, so the member lists are identical.  A leader
+// whose ball exceeds kBallCap candidates is flagged and built on the host.
+// ===========================================================================
+constexpr int kBallCap = 1024;        // BFS candidates a warp holds
+constexpr int kBallSet = 2048;        // visited-set slots (open addressing, power of two)
+constexpr int kBuildWarps = 4;        // warps per block
+constexpr size_t kBuildSmem = (size_t)kBuildWarps * (kBallCap * 8 + kBallSet * 4);
+
+__device__ __forceinline__ float build_dist2(const float* __restrict__ a, const float* __restrict__ b)
+{
+	const float dx = __fsub_rn(a[0], b[0]), dy = __fsub_rn(a[1], b[1]), dz = __fsub_rn(a[2], b[2]);
+	return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ unsigned int build_slot(int j) { return ((unsigned int)j * 2654435761u) & (kBallSet - 1); }
+
+__device__ __forceinline__ bool build_set_has(const int* set, int j)
+{
+	for (unsigned int h = build_slot(j), t = 0; t < kBallSet; ++t, h = (h + 1) & (kBallSet - 1)) {
+		const int v = set[h];
+		if (v == j) return true;
+		if (v == -1) return false;
+	}
+	return false;
+}
+
+__device__ __forceinline__ void build_set_put(int* set, int j)
+{
+	for (unsigned int h = build_slot(j), t = 0; t < kBallSet; ++t, h = (h + 1) & (kBallSet - 1)) {
+		const int old = atomicCAS(&set[h], -1, j);
+		if (old == -1 || old == j) return;
+	}
+}
+
+// warp-wide (value, index) maximum, lowest index among equal values
+__device__ __forceinline__ void build_argmax(float& v, int& m)
+{
+	for (int o = 16; o > 0; o >>= 1) {
+		const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
+		const int m2 = __shfl_xor_sync(0xffffffffu, m, o);
+		if (v2 > v || (v2 == v && m2 >= 0 && (m < 0 || m2 < m))) { v = v2; m = m2; }
+	}
+}
+
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_members(int n, const int* __restrict__ off,
+	const int* __restrict__ nbr, const float* __restrict__ rest3, int ring_k, int cap, int* __restrict__ members,
+	int* __restrict__ counts)
+{
+	extern __shared__ int build_sm[];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	int* col = build_sm + w * (kBallCap * 2 + kBallSet);
+	float* md = reinterpret_cast<float*>(col + kBallCap);
+	int* set = col + 2 * kBallCap;
+	const unsigned int lt = (1u << lane) - 1u;
+	for (int i = blockIdx.x * kBuildWarps + w; i < n; i += gridDim.x * kBuildWarps) {
+		int count = 0;
+		bool overflow = false;
+		if (ring_k <= 1) {
+			for (int e0 = off[i]; e0 < off[i + 1] && !overflow; e0 += 32) {
+				const int e = e0 + lane;
+				int j = -1;
+				if (e < off[i + 1]) j = nbr[e];
+				const bool ok = j >= 0 && j < n && j != i;
+				const unsigned int m = __ballot_sync(0xffffffffu, ok);
+				const int pos = count + __popc(m & lt);
+				if (ok && pos < kBallCap) col[pos] = j;
+				count += __popc(m);
+				if (count > kBallCap) overflow = true;
+			}
+		}
+		else {
+			for (int t = lane; t < kBallSet; t += 32) set[t] = -1;
+			__syncwarp();
+			if (lane == 0) build_set_put(set, i);
+			__syncwarp();
+			int fs = 0, fe = 0;          // frontier = col[fs, fe); the leader alone at depth 0
+			for (int d = 0; d < ring_k && !overflow; ++d) {
+				if (d > 0 && fs == fe) break;
+				const int next = count;
+				const int nf = (d == 0) ? 1 : fe - fs;
+				for (int q = 0; q < nf && !overflow; ++q) {
+					const int f = (d == 0) ? i : col[fs + q];
+					const int r1 = off[f + 1];
+					for (int e0 = off[f]; e0 < r1 && !overflow; e0 += 32) {
+						const int e = e0 + lane;
+						int j = -1;
+						if (e < r1) j = nbr[e];
+						bool fresh = j >= 0 && j < n;
+						// repeated entries in one row: only the first lane's counts
+						const unsigned int same = __match_any_sync(0xffffffffu, j);
+						if ((same & lt) != 0u) fresh = false;
+						if (fresh && build_set_has(set, j)) fresh = false;
+						const unsigned int m = __ballot_sync(0xffffffffu, fresh);
+						const int pos = count + __popc(m & lt);
+						if (fresh && pos < kBallCap) { col[pos] = j; build_set_put(set, j); }
+						count += __popc(m);
+						if (count > kBallCap) overflow = true;
+						__syncwarp();
+					}
+				}
+				fs = next;
+				fe = count;
+			}
+		}
+		__syncwarp();
+		int* out = members + (size_t)i * cap;
+		if (overflow) {
+			if (lane == 0) counts[i] = -1;   // built on the host
+		}
+		else if (count <= cap) {
+			for (int t = lane; t < count; t += 32) out[t] = col[t];
+			if (lane == 0) counts[i] = count;
+		}
+		else {
+			// farthest point: start at the candidate farthest from the leader; each pick
+			// lowers the others' distance-to-picked; next = first maximum; taken = -1
+			const float* ci = rest3 + 3 * (size_t)i;
+			float bv = -1.0f;
+			int bm = -1;
+			for (int t = lane; t < count; t += 32) {
+				const float dd = build_dist2(rest3 + 3 * (size_t)col[t], ci);
+				md[t] = dd;
+				if (dd > bv) { bv = dd; bm = t; }
+			}
+			build_argmax(bv, bm);
+			int cur = bm, picks = 0;
+			for (int t = 0; t < cap; ++t) {
+				__syncwarp();
+				if (lane == 0) { out[t] = col[cur]; md[cur] = -1.0f; }
+				++picks;
+				__syncwarp();
+				const float* cp = rest3 + 3 * (size_t)col[cur];
+				float nv = -1.0f;
+				int nm = -1;
+				for (int u = lane; u < count; u += 32) {
+					float v = md[u];
+					if (v < 0.0f) continue;
+					const float dd = build_dist2(rest3 + 3 * (size_t)col[u], cp);
+					if (dd < v) { v = dd; md[u] = dd; }
+					if (v > nv) { nv = v; nm = u; }
+				}
+				build_argmax(nv, nm);
+				if (nm < 0) break;
+				cur = nm;
+			}
+			if (lane == 0) counts[i] = picks;
+		}
+		__syncwarp();
+	}
+}
+
+// ===========================================================================
 // Object mode: rigid shape keeping per object (graph component of at least 50
 // Gaussians), once per step right after predict (forward.cu:12141-12166, the device path
 // 6829-6958 and 11671-11702).  The per-object sums are in FP64 like the reference's; they

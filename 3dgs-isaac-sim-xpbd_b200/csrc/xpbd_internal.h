@@ -109,6 +109,10 @@ struct HostEdgeColoring {
 void build_graph(int n, int e, const int* edges, const float* rest, const float* stiff, HostGraph& g);
 void build_clusters(const HostGraph& g, const float* rest_pos3, int ring_k, int cap, int leader_min_hop,
 	HostClusters& out);
+// the same for leader spacing 1 from member lists built on the GPU: flat[i * cap ...],
+// counts[i] entries each, or -1 where the host builds leader i's list
+void build_clusters_from_members(const HostGraph& g, const float* rest_pos3, int ring_k, int cap, const int* flat,
+	const int* counts, HostClusters& out);
 void build_edge_coloring(const HostGraph& g, HostEdgeColoring& out);
 void build_components(const HostGraph& g, int min_component, std::vector<int>& obj_id, int& num_objects);
 float graph_spacing(const HostGraph& g);

@@ -126,6 +126,10 @@ XPBD_API int xpbd_b200_chainmail_run(int prop_iters, int relax_iters, float prop
 /* Propagation sweeps on work lists of the Gaussians next to the last sweep's changes (1,
  * default) or over every Gaussian (0).  The results are identical. */
 XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled);
+/* Build the volume clusters' member lists (k-ring BFS and farthest-point subsample,
+ * forward.cu:9814-10033) on the GPU (1, default; leader spacing 1 only) or on the host
+ * (0).  The lists are identical either way; takes effect at the next upload or rebuild. */
+XPBD_API void xpbd_b200_set_gpu_builder(int enabled);
 /* Arrival times (caller order; 1e9 where the wave has not arrived); returns N or -1. */
 XPBD_API int xpbd_b200_chainmail_times(float* out, int n);
 

@@ -175,6 +175,27 @@ def test_internal_order_does_not_change_results(lib):
     assert H.contacts_equal(out[0][4], out[0][5], out[1][4], out[1][5])
 
 
+@pytest.mark.parametrize("knn,ring,cap", [(8, 3, 64), (8, 1, 64), (12, 3, 128), (8, 6, 64)])
+def test_gpu_cluster_builder_matches_host(lib, knn, ring, cap):
+    """Member lists built on the GPU (BFS + farthest point, one warp per leader) equal the
+    host builder's, and so the reference's (the golden topology tests use the GPU path);
+    ring 6 sends the leaders whose ball exceeds the GPU's 1024 candidates to the host."""
+    import ctypes
+    lib.lib.xpbd_b200_set_gpu_builder.argtypes = [ctypes.c_int]
+    sc = H.scenes.make_scene(6000, 9, knn=knn)
+    out = []
+    for gpu in (1, 0):
+        lib.lib.xpbd_b200_set_gpu_builder(gpu)
+        s = H.scenes.Scenario(sc, [], ring_k=ring, max_members=cap)
+        s.setup(lib)
+        s.advance(lib, 1)
+        out.append({k: lib.ints(k) for k in ("vol_offset", "vol_count", "vol_idx", "rev_offset", "rev_count", "rev_idx")})
+    lib.lib.xpbd_b200_set_gpu_builder(1)
+    for k in out[0]:
+        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
+    assert out[0]["vol_count"].max() == min(cap, out[0]["vol_count"].max())
+
+
 def test_graph_replay_matches_eager(lib):
     out = []
     for graph in (1, 0):
