@@ -266,48 +266,41 @@ class XPBD:
     # ---- ChainMail (forward.cu:12808-13006; not in the reference C ABI) ----
     # The product exports xpbd_b200_chainmail_*, the oracle oracle_chainmail_* and the
     # reference shim refshim_chainmail_*; the first present is used.
-    def _cm(self, name):
+    def _cm(self, name, argtypes, restype):
         for prefix in ("xpbd_b200_", "oracle_", "refshim_"):
             f = getattr(self.raw, prefix + name, None)
             if f is not None:
+                f.argtypes = argtypes       # on the ctypes function; self.lib may be an engine proxy
+                f.restype = restype
                 return prefix, getattr(self.lib, prefix + name)
         raise AttributeError(f"{self.path} has no ChainMail entry point {name}")
 
     def chainmail_set_material(self, global_scale=1.0, air=0.1, skin=0.1, bone=0.1, use_edge_stiffness=True,
                                edge_influence=1.0):
-        _, f = self._cm("chainmail_set_material")
-        f.argtypes = [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.c_float]
-        f.restype = None
+        _, f = self._cm("chainmail_set_material", [ctypes.c_float] * 4 + [ctypes.c_int, ctypes.c_float], None)
         f(global_scale, air, skin, bone, int(use_edge_stiffness), edge_influence)
 
     def chainmail_seed(self, idx, delta):
         """Seeds start the wave: each moves by its delta (K, 3) and gets arrival time 0."""
         idx = np.ascontiguousarray(idx, dtype=np.int32).reshape(-1)
         delta = np.ascontiguousarray(delta, dtype=np.float32).reshape(-1, 3)
-        _, f = self._cm("chainmail_seed")
-        f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
-        f.restype = ctypes.c_int
+        _, f = self._cm("chainmail_seed", [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int)
         self._check(f(len(idx), idx.ctypes.data, delta.ctypes.data), "chainmail_seed")
 
     def chainmail_run(self, prop_iters=20, relax_iters=5, prop_strength=0.5, relax_stiffness=0.99, relax_damping=0.1):
         """Propagation and relax sweeps; defaults are the reference's (forward.cu:60-64)."""
-        _, f = self._cm("chainmail_run")
-        f.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 3
-        f.restype = ctypes.c_int
+        _, f = self._cm("chainmail_run", [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 3, ctypes.c_int)
         self._check(f(prop_iters, relax_iters, prop_strength, relax_stiffness, relax_damping), "chainmail_run")
 
     def chainmail_times(self):
         """Arrival times (N,), 1e9 where the wave has not arrived."""
         out = np.zeros(max(self.n, 1), np.float32)
         if hasattr(self.raw, "refshim_float") and not hasattr(self.raw, "xpbd_b200_chainmail_times"):
-            f = self.lib.refshim_float
-            f.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong]
-            f.restype = ctypes.c_int
-            got = f(b"cm_time", out.ctypes.data, out.size)
+            self.raw.refshim_float.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong]
+            self.raw.refshim_float.restype = ctypes.c_int
+            got = self.lib.refshim_float(b"cm_time", out.ctypes.data, out.size)
         else:
-            _, f = self._cm("chainmail_times")
-            f.argtypes = [ctypes.c_void_p, ctypes.c_int]
-            f.restype = ctypes.c_int
+            _, f = self._cm("chainmail_times", [ctypes.c_void_p, ctypes.c_int], ctypes.c_int)
             got = f(out.ctypes.data, out.size)
         if got != self.n:
             raise RuntimeError(f"chainmail_times: {self.last_error()}")

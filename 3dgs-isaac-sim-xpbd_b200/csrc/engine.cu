@@ -1719,6 +1719,26 @@ XPBD_API int xpbd_b200_step_async(int substeps)
 	return 0;
 }
 
+// k substeps in one call, each preceded by what a caller sets per substep: the colliders'
+// poses (the reference list: types / dims fixed, poses[s * 12 * ncol ...]) and, after the
+// first step, the pinned Gaussians' targets (targets[s * 3 * npins ...], weight 1).  The
+// same as xpbd_set_colliders + xpbd_set_attached + xpbd_b200_step_async(1) per substep.
+XPBD_API int xpbd_b200_step_substeps(int k, int ncol, const int* types, const float* poses, const float* dims,
+	float margin, float friction, int npins, const int* idx, const float* targets)
+{
+	Engine& E = *cur_engine();
+	if (E.n <= 0) return fail("xpbd_b200_step_substeps: call xpbd_create first");
+	if (k < 0 || ncol < 0 || npins < 0 || (ncol > 0 && (!types || !poses || !dims)) ||
+		(npins > 0 && (!idx || !targets)))
+		return fail("xpbd_b200_step_substeps: invalid arguments");
+	for (int s = 0; s < k; ++s) {
+		if (ncol > 0) xpbd_set_colliders(ncol, types, poses + (size_t)s * 12 * ncol, dims, margin, friction);
+		if (npins > 0 && E.stepped && E.set_attached(npins, idx, targets + (size_t)s * 3 * npins, 1.0f)) return -1;
+		if (E.step_async()) return -1;
+	}
+	return 0;
+}
+
 XPBD_API int xpbd_b200_sync(void) { return cur_engine()->stream ? cur_engine()->sync() : 0; }
 
 XPBD_API void xpbd_b200_set_gs(int distance, int volume)

@@ -10,6 +10,7 @@ The arrays match the inputs of ``xpbd_create`` (xpbd_capi.cu:71-102): ``pos[n,3]
 ``scales[n,3]`` (activated), ``rots[n,4]`` (normalised, w,x,y,z), ``opacity[n]``
 (activated), undirected edges ``[e,2]`` with i<j, ``rest[e]``, ``stiff[e]``.
 """
+import ctypes
 import math
 
 import numpy as np
@@ -178,6 +179,36 @@ class Scenario:
         if not cols:
             return [], np.zeros((0, 12), np.float32), np.zeros((0, 3), np.float32)
         return [c[0] for c in cols], np.stack([c[1] for c in cols]), np.stack([c[2] for c in cols])
+
+    def frame_inputs(self, count):
+        """The next ``count`` substeps' collider poses (count, K, 12) and pin targets
+        (count, P, 3), with the collider types and dims and the pinned indices."""
+        ts = [(self.k + 1 + s) / self.substeps for s in range(count)]
+        types, _, dims = self.colliders(ts[0])
+        poses = np.stack([self.colliders(t)[1] for t in ts]).astype(np.float32) if self.grippers \
+            else np.zeros((count, 0, 12), np.float32)
+        if self.has_pins():
+            idx = np.concatenate([g.idx for g in self.grippers]).astype(np.int32)
+            targets = np.stack([np.concatenate([g.targets(t) for g in self.grippers], axis=0) for t in ts])
+        else:
+            idx, targets = np.zeros(0, np.int32), np.zeros((count, 0, 3), np.float32)
+        return (np.asarray(types, np.int32), np.ascontiguousarray(poses), np.asarray(dims, np.float32).reshape(-1, 3),
+                idx, np.ascontiguousarray(targets, np.float32))
+
+    def advance_async(self, solver, count):
+        """Enqueue ``count`` substeps with one library call (xpbd_b200_step_substeps)."""
+        types, poses, dims, idx, targets = self.frame_inputs(count)
+        raw = getattr(solver, "raw", solver.lib).xpbd_b200_step_substeps   # the ctypes function itself
+        raw.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                        ctypes.c_float, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        raw.restype = ctypes.c_int
+        f = solver.lib.xpbd_b200_step_substeps   # through the engine selection of an instance
+        dims = np.ascontiguousarray(dims)
+        rc = f(count, len(types), types.ctypes.data, poses.ctypes.data, dims.ctypes.data, 0.0, 0.0, len(idx),
+               idx.ctypes.data, targets.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(solver.last_error())
+        self.k += count
 
     def advance(self, solver, count):
         """Run ``count`` substeps."""

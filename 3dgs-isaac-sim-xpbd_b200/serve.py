@@ -58,6 +58,11 @@ class Session:
         g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, math.radians(float(rng.uniform(-1, 1))))
         self.scen = scenes.Scenario(sc, [g], substeps=self.substeps, iters=self.iters)
 
+    def fresh_scenario(self):
+        """A copy of the prepared scenario at frame 0 (same scene arrays)."""
+        sc = self.scen
+        return scenes.Scenario(sc.scene, sc.grippers, substeps=self.substeps, iters=self.iters)
+
     def admit(self, lib_path):
         if self.scen is None:
             self.prepare()
@@ -66,15 +71,8 @@ class Session:
         self.scen.advance(self.solver, 1)          # upload + topology build (first substep)
 
     def enqueue_frame(self):
-        s, x = self.scen, self.solver
-        for _ in range(s.substeps):
-            t = (s.k + 1) / s.substeps
-            types, poses, dims = s.colliders(t)
-            x.set_colliders(types, poses, dims, 0.0, 0.0)
-            idx, pos = s.pins(t)
-            x.set_attached(idx, pos, 1.0)
-            x.lib.xpbd_b200_step_async(1)
-            s.k += 1
+        """The next frame's substeps, with their collider poses and pin targets, in one call."""
+        self.scen.advance_async(self.solver, self.scen.substeps)
         self.frames_left -= 1
 
     def close(self, keep_result=True):
@@ -85,8 +83,19 @@ class Session:
             self.solver = None
 
 
+def prepare_sessions(sessions):
+    """Session objects with their scenes generated (the request payloads a server receives)."""
+    out = []
+    for k, (a, n, frames, seed) in enumerate(sessions):
+        s = Session(k, a, n, frames, seed)
+        s.prepare()
+        out.append(s)
+    return out
+
+
 def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=None):
-    """Serve `sessions` (from make_sessions) with continuous batching.  Returns stats."""
+    """Serve `sessions` (tuples from make_sessions, or prepared Session objects) with
+    continuous batching.  Returns stats."""
     t0 = time.perf_counter()
     arrivals = collections.deque(sessions)
     ready = queue.Queue()
@@ -115,9 +124,13 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
         now = time.perf_counter() - t0
         if max_wall and now > max_wall:
             break
-        while arrivals and arrivals[0][0] * time_scale <= now:
-            a, n, frames, seed = arrivals.popleft()
-            waiting.append(Session(sid, a * time_scale, n, frames, seed))
+        while arrivals and _arrival(arrivals[0]) * time_scale <= now:
+            item = arrivals.popleft()
+            if isinstance(item, Session):
+                waiting.append(item)
+            else:
+                a, n, frames, seed = item
+                waiting.append(Session(sid, a * time_scale, n, frames, seed))
             sid += 1
         # admission by resident-byte budget, in arrival order
         while waiting:
@@ -163,14 +176,23 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "sessions_done": done}
 
 
+def _arrival(item):
+    return item.arrival if isinstance(item, Session) else item[0]
+
+
 def run_plain(lib_path, sessions, max_wall=None):
     """One session at a time, start to finish, on one engine (no overlap)."""
     t0 = time.perf_counter()
     work, lats, count = 0, [], 0
-    for k, (a, n, frames, seed) in enumerate(sessions):
+    for k, item in enumerate(sessions):
         if max_wall and time.perf_counter() - t0 > max_wall:
             break
-        s = Session(k, a, n, frames, seed)
+        if isinstance(item, Session):
+            s = Session(item.sid, item.arrival, item.n, item.frames_total, item.seed)
+            s.scen = item.fresh_scenario()
+        else:
+            a, n, frames, seed = item
+            s = Session(k, a, n, frames, seed)
         s.admit(lib_path)
         while s.frames_left > 0:
             t1 = time.perf_counter()

@@ -153,6 +153,12 @@ XPBD_API int xpbd_b200_set_colliders_many(int count, const int* types, const flo
 XPBD_API int xpbd_b200_set_stream(void* stream);
 /* Enqueue `substeps` steps without waiting for them. */
 XPBD_API int xpbd_b200_step_async(int substeps);
+/* k substeps in one call, each preceded by its collider poses (poses[s * 12 * ncol ...],
+ * types and dims fixed) and, after the first step, its pin targets
+ * (targets[s * 3 * npins ...]): xpbd_set_colliders + xpbd_set_attached +
+ * xpbd_b200_step_async(1) per substep, without a call per substep. */
+XPBD_API int xpbd_b200_step_substeps(int k, int ncol, const int* types, const float* poses, const float* dims,
+	float margin, float friction, int npins, const int* idx, const float* targets);
 /* Wait for the engine's stream. */
 XPBD_API int xpbd_b200_sync(void);
 /* Gauss-Seidel colour sweeps for the distance / volume constraints instead of the

@@ -196,6 +196,22 @@ def test_gpu_cluster_builder_matches_host(lib, knn, ring, cap):
     assert out[0]["vol_count"].max() == min(cap, out[0]["vol_count"].max())
 
 
+def test_frame_call_matches_per_substep_calls(lib):
+    """xpbd_b200_step_substeps (one call per frame) = set_colliders + set_attached + step per substep."""
+    out = []
+    for frame_call in (True, False):
+        s = H.scenes.plain_scene_scenario(2500, 8, pins=30)
+        s.setup(lib)
+        s.advance(lib, 1)
+        if frame_call:
+            s.advance_async(lib, 10)
+            s.advance_async(lib, 7)
+        else:
+            s.advance(lib, 17)
+        out.append(lib.positions())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
 def test_graph_replay_matches_eager(lib):
     out = []
     for graph in (1, 0):
