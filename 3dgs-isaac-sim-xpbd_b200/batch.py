@@ -42,6 +42,26 @@ def make_objects(count=64, seed=0, n_min=2000, n_max=200000, radius_range=(0.3, 
     return objs
 
 
+def object_cost(scene, cap=64):
+    """Per-step work of an object: Gaussians x (mean directed degree + cluster members)."""
+    n = scene["pos"].shape[0]
+    return n * (2.0 * len(scene["edges"]) / max(n, 1) + cap)
+
+
+def partition(objects, ranks, cap=64):
+    """Objects split over `ranks` GPUs (longest-processing-time greedy bin packing on
+    object_cost): returns one list of object indices per rank, each in input order.
+    Objects are independent, so the ranks share nothing during the step."""
+    order = sorted(range(len(objects)), key=lambda k: (-object_cost(objects[k][0], cap), k))
+    load = [0.0] * ranks
+    bins = [[] for _ in range(ranks)]
+    for k in order:
+        r = min(range(ranks), key=lambda q: (load[q], q))
+        bins[r].append(k)
+        load[r] += object_cost(objects[k][0], cap)
+    return [sorted(b) for b in bins]
+
+
 class ObjectScenario(scenes.Scenario):
     """One object of a batch run on its own (the reference's one-scene-per-instance form)."""
 

@@ -362,14 +362,19 @@ def bench_batched(args, rank, world):
     import torch
 
     batch = pkg.batch
-    objs = batch.make_objects(64, seed=0)
-    total = sum(sc["pos"].shape[0] for sc, _ in objs)
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    all_objs = batch.make_objects(64, seed=0)
+    total = sum(sc["pos"].shape[0] for sc, _ in all_objs)
+    mine = batch.partition(all_objs, world)[rank]          # this rank's objects (no exchange)
+    objs = [all_objs[k] for k in mine]
     x = pkg.XPBD()
     bind_ext(x.lib)
     b = batch.Batch(objs)
     b.setup(x)
     b.advance(x, SUBSTEPS * (1 + args.warmup))
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     b.advance(x, SUBSTEPS * args.steps, blocking=False)
     x.lib.xpbd_b200_sync()
@@ -384,13 +389,17 @@ def bench_batched(args, rank, world):
         s.advance(x, SUBSTEPS * args.steps)
         plain_s += time.perf_counter() - t1
     x.destroy()
+    batched_s, plain_s = max_over_ranks([batched_s, plain_s], world, "cuda")
+    if rank != 0:
+        return None
     units = total * SUBSTEPS * args.steps
     return {"metric": "batched XPBD Gaussian-substeps/s (64 objects)", "value": units / batched_s, "unit": UNIT,
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_s / args.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_s / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (64 seeded ellipsoid objects)",
             "config": {"workload": f"batched: 64 objects, {total} Gaussians, 10 substeps x 4 iterations",
-                       "objects": 64, "n_gaussians": total},
+                       "objects": 64, "n_gaussians": total,
+                       "parallelism": f"objects bin-packed over {world} GPU(s), no exchange"},
             "plain": {"value": units / plain_s, "unit": UNIT, "ms_per_step": plain_s / args.steps * 1e3,
                       "form": "the same objects stepped one at a time, one scene per engine"},
             "speedup_vs_plain": plain_s / batched_s}

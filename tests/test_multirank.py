@@ -56,3 +56,38 @@ def test_reference_arm_under_torchrun_prints_once():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def _partition_worker(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import importlib
+    batch = importlib.import_module("3dgs-isaac-sim-xpbd_b200").batch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        objs = batch.make_objects(count=9, seed=4, n_min=300, n_max=3000)
+        mine = batch.partition(objs, world)[rank]
+        got = [None] * world
+        dist.all_gather_object(got, mine)
+        out[rank] = (got, [batch.object_cost(objs[k][0]) for k in range(len(objs))])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batched_partition_gloo():
+    """Each rank derives the same object partition: disjoint, covering, load-balanced."""
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_partition_worker, args=(world, port, out), nprocs=world, join=True)
+        got = dict(out)
+    parts, cost = got[0]
+    assert got[1][0] == parts
+    flat = sorted(k for p in parts for k in p)
+    assert flat == list(range(len(cost)))
+    loads = [sum(cost[k] for k in p) for p in parts]
+    assert max(loads) - min(loads) <= max(cost)
