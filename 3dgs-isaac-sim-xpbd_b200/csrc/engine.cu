@@ -1653,6 +1653,30 @@ XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled) { engine().S.cm_fron
 
 XPBD_API void xpbd_b200_set_gpu_builder(int enabled) { engine().S.gpu_builder = enabled != 0; }
 
+// exportPhysicsGraph (forward.cu:4612-4663): the directed graph and rest positions as an
+// APGGRPH1 file, in the order given to xpbd_create (the reference writes its viewer's
+// internal order; tools/import_graph.py renumbers either by matching positions)
+XPBD_API int xpbd_b200_export_graph(const char* path)
+{
+	Engine& E = *cur_engine();
+	if (!E.built || !path) return fail("xpbd_b200_export_graph: no graph yet (create and step first)");
+	const int N = E.n, M = E.graph.off[N];
+	std::vector<int> cnt(N);
+	for (int i = 0; i < N; ++i) cnt[i] = E.graph.off[i + 1] - E.graph.off[i];
+	FILE* f = fopen(path, "wb");
+	if (!f) return fail("xpbd_b200_export_graph: cannot open %s", path);
+	bool ok = fwrite("APGGRPH1", 1, 8, f) == 8;
+	ok = ok && fwrite(&N, sizeof(int), 1, f) == 1 && fwrite(&M, sizeof(int), 1, f) == 1;
+	ok = ok && fwrite(E.in_pos.data(), sizeof(float), 3 * (size_t)N, f) == 3 * (size_t)N;
+	ok = ok && fwrite(E.graph.off.data(), sizeof(int), N, f) == (size_t)N;
+	ok = ok && fwrite(cnt.data(), sizeof(int), N, f) == (size_t)N;
+	ok = ok && fwrite(E.graph.nbr.data(), sizeof(int), M, f) == (size_t)M;
+	ok = ok && fwrite(E.graph.ndist.data(), sizeof(float), M, f) == (size_t)M;
+	ok = ok && fwrite(E.graph.nstiff.data(), sizeof(float), M, f) == (size_t)M;
+	ok = (fclose(f) == 0) && ok;
+	return ok ? 0 : fail("xpbd_b200_export_graph: write failed: %s", path);
+}
+
 XPBD_API int xpbd_b200_chainmail_seed(int count, const int* idx, const float* delta)
 {
 	Engine& E = *cur_engine();

@@ -130,6 +130,9 @@ XPBD_API void xpbd_b200_chainmail_set_frontier(int enabled);
  * forward.cu:9814-10033) on the GPU (1, default; leader spacing 1 only) or on the host
  * (0).  The lists are identical either way; takes effect at the next upload or rebuild. */
 XPBD_API void xpbd_b200_set_gpu_builder(int enabled);
+/* The graph as an APGGRPH1 file (exportPhysicsGraph, forward.cu:4612-4663), in the
+ * order given to xpbd_create; after the first step.  0 or -1. */
+XPBD_API int xpbd_b200_export_graph(const char* path);
 /* Arrival times (caller order; 1e9 where the wave has not arrived); returns N or -1. */
 XPBD_API int xpbd_b200_chainmail_times(float* out, int n);
 

@@ -212,6 +212,22 @@ def test_frame_call_matches_per_substep_calls(lib):
     np.testing.assert_array_equal(out[0], out[1])
 
 
+def test_export_graph(lib, tmp_path):
+    """xpbd_b200_export_graph writes the APGGRPH1 graph in xpbd_create's order."""
+    import ctypes
+    lib.lib.xpbd_b200_export_graph.argtypes = [ctypes.c_char_p]
+    sc = H.scenes.make_scene(1500, 6)
+    s = H.scenes.Scenario(sc, [])
+    s.setup(lib)
+    s.advance(lib, 1)
+    path = tmp_path / "g.bin"
+    assert lib.lib.xpbd_b200_export_graph(str(path).encode()) == 0
+    n, m, g = H.pkg.graph_io.read_graph(path)
+    np.testing.assert_array_equal(g["pos"], sc["pos"])
+    for k, v in zip(("offset", "count", "idx", "dist", "stiff"), H.pkg.graph_io.scene_csr(sc)):
+        np.testing.assert_array_equal(g[k], v, err_msg=k)
+
+
 def test_graph_replay_matches_eager(lib):
     out = []
     for graph in (1, 0):
