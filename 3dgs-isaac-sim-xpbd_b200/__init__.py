@@ -10,13 +10,14 @@ and hand-written sm_100a CUDA kernels).  This package only locates and binds it:
 * ``scenes`` — seeded synthetic workloads;
 * ``batch`` — many independent objects packed into one scene;
 * ``serve`` — continuous-batching session loop over resident engine instances;
-* ``graph_io`` — APGGRPH1 graphs, graph ``.npz`` renumbering, 3DGS PLY, runtime inputs.
+* ``graph_io`` — APGGRPH1 graphs, graph ``.npz`` renumbering, 3DGS PLY, runtime inputs;
+* ``splat`` — cameras for the splatting pass (``XPBD.render``).
 
 There is no CPU fallback: constructing ``XPBD`` without the built library raises.
 """
 import os
 
-from . import batch, bridge, graph_io, scenes, serve  # noqa: F401
+from . import batch, bridge, graph_io, scenes, serve, splat  # noqa: F401
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_NAME = "libxpbd_b200.so"

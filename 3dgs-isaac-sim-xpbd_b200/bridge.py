@@ -306,6 +306,65 @@ class XPBD:
             raise RuntimeError(f"chainmail_times: {self.last_error()}")
         return out[:self.n]
 
+    # ---- splatting into a device image (the viewer's rasteriser; library only) ----
+    def _ext(self, name, argtypes, restype):
+        f = getattr(self.raw, "xpbd_b200_" + name, None)
+        if f is None:
+            raise AttributeError(f"{self.path} has no entry point xpbd_b200_{name}")
+        f.argtypes = argtypes
+        f.restype = restype
+        return getattr(self.lib, "xpbd_b200_" + name)
+
+    def render_set_colors(self, colors, sh_degree=-1):
+        """RGB (N, 3) with sh_degree -1, else SH coefficients (N, (d+1)^2, 3)."""
+        c = np.ascontiguousarray(colors, dtype=np.float32)
+        f = self._ext("render_set_colors", [ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int)
+        self._check(f(self.n, int(sh_degree), c.ctypes.data), "render_set_colors")
+        self._keep_colors = c
+
+    def render_set_options(self, antialiasing=False, box=None, pick=False):
+        f = self._ext("render_set_options", [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int], None)
+        if box is None:
+            f(int(antialiasing), None, None, int(pick))
+        else:
+            lo = np.ascontiguousarray(box[0], dtype=np.float32)
+            hi = np.ascontiguousarray(box[1], dtype=np.float32)
+            f(int(antialiasing), lo.ctypes.data, hi.ctypes.data, int(pick))
+
+    def render_set_floor(self, visible, origin=(0.0, 0.0, 0.0), checker=1.0, fade_radius=10.0):
+        o = np.ascontiguousarray(origin, dtype=np.float32)
+        f = self._ext("render_set_floor", [ctypes.c_int, ctypes.c_void_p, ctypes.c_float, ctypes.c_float], None)
+        f(int(visible), o.ctypes.data, float(checker), float(fade_radius))
+
+    def render(self, cam, deform_eps=1e-2, bg=(0.0, 0.0, 0.0), scale_modifier=1.0, to_host=True):
+        """One frame of the current state through ``cam`` (splat.Camera).  Returns
+        (image (3, H, W) float32 or None, number of (tile, Gaussian) pairs)."""
+        f = self._ext("render", [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 4
+                      + [ctypes.c_void_p, ctypes.c_void_p], ctypes.c_longlong)
+        bgv = np.ascontiguousarray(bg, dtype=np.float32)
+        out = np.empty((3, cam.height, cam.width), np.float32) if to_host else None
+        m = f(cam.view.ctypes.data, cam.proj.ctypes.data, cam.campos.ctypes.data, cam.width, cam.height,
+              cam.tan_fovx, cam.tan_fovy, float(scale_modifier), float(deform_eps), bgv.ctypes.data,
+              out.ctypes.data if to_host else None)
+        if m < 0:
+            self._check(-1, "render")
+        return out, int(m)
+
+    def render_device_ptr(self):
+        return int(self._ext("render_device", [], ctypes.c_ulonglong)())
+
+    def render_aux(self, width, height, pick=False):
+        """final_T (H, W), n_contrib (H, W), picked ids (H, W) or None, radii (N,)."""
+        f = self._ext("render_aux", [ctypes.c_void_p] * 3 + [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int],
+                      ctypes.c_int)
+        ft = np.empty((height, width), np.float32)
+        nc = np.empty((height, width), np.int32)
+        pk = np.empty((height, width), np.int32) if pick else None
+        radii = np.empty(self.n, np.int32)
+        self._check(f(ft.ctypes.data, nc.ctypes.data, pk.ctypes.data if pick else None, width * height,
+                      radii.ctypes.data, self.n), "render_aux")
+        return ft, nc, pk, radii
+
     def press_start(self, axis, ramp_per_sec, max_disp_pct, from_lo):
         self._check(self.lib.xpbd_press_start(int(axis), float(ramp_per_sec), float(max_disp_pct), int(from_lo)),
                     "xpbd_press_start")

@@ -25,8 +25,12 @@
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "../../include/xpbd_capi.h"
 #include "kernels.cuh"
+#include "render.cuh"
 #include "xpbd_internal.h"
 
 namespace xpbd {
@@ -132,10 +136,11 @@ struct Settings {
 
 enum Stage {
 	ST_PREDICT, ST_DISTANCE, ST_VOL_SOLVE, ST_VOL_GATHER, ST_VOL_GS, ST_SHAPE, ST_SC_BUILD, ST_SC_SOLVE,
-	ST_PROJECT, ST_VELOCITY, ST_JSTATS, ST_OTHER, ST_COUNT
+	ST_PROJECT, ST_VELOCITY, ST_JSTATS, ST_OTHER, ST_RENDER_PREPARE, ST_RENDER_SORT, ST_RENDER_TILES, ST_COUNT
 };
 static const char* kStageNames[ST_COUNT] = { "predict", "distance", "volume_solve", "volume_gather", "volume_gs",
-	"shape", "selfcol_build", "selfcol_solve", "project", "velocity", "jstats", "other" };
+	"shape", "selfcol_build", "selfcol_solve", "project", "velocity", "jstats", "other", "render_prepare",
+	"render_sort", "render_tiles" };
 
 class Engine {
 public:
@@ -179,6 +184,43 @@ public:
 	DBuf<int> obj_count;
 	DBuf<unsigned char> sc_active;
 	DBuf<float4> sc_cross, sc_accum;
+	// splatting (xpbd_b200_render*): per-Gaussian projection, depth order, tile pairs,
+	// tile ranges, the image and its per-pixel extras; colours and options outlive frames
+	struct Render {
+		DBuf<float2> xy;
+		DBuf<float4> conic, rgb;
+		DBuf<int4> rect;
+		DBuf<unsigned int> dkey, dkey_s, tkey, tkey_s;
+		DBuf<int> iota, order, radii, touched, val, val_s, n_contrib, pick;
+		DBuf<int2> ranges;
+		DBuf<float> image, final_T, colors, opacity, rest_sc, rest_q;
+		DBuf<long long> cnt, offs;
+		DBuf<unsigned char> temp;
+		long long* h_total = nullptr;   // pinned: pair count of the frame
+		std::vector<float> h_colors;    // caller order; uploaded on the next frame
+		int sh_deg = -1, sh_coeffs = 0;
+		bool colors_dirty = false;
+		int antialias = 0, pick_on = 0;
+		bool box_on = false;
+		float box_lo[3] = {}, box_hi[3] = {};
+		bool floor_on = false;
+		float floor_origin[3] = {}, floor_checker = 1.0f, floor_fade = 10.0f;
+		int W = 0, H = 0;
+		long long pairs = 0;
+		void release()
+		{
+			xy.release(); conic.release(); rgb.release(); rect.release(); dkey.release(); dkey_s.release();
+			tkey.release(); tkey_s.release(); iota.release(); order.release(); radii.release(); touched.release();
+			cnt.release(); offs.release(); val.release(); val_s.release(); n_contrib.release(); pick.release();
+			ranges.release(); image.release(); final_T.release(); colors.release(); opacity.release();
+			rest_sc.release(); rest_q.release(); temp.release();
+			if (h_total) cudaFreeHost(h_total);
+			h_total = nullptr;
+			colors_dirty = !h_colors.empty();
+			W = H = 0;
+			pairs = 0;
+		}
+	} rs;
 	bool obj_shift_valid = false;    // a previous object step set the centroids (boxes usable)
 	bool last_sc_limited = false;    // the last step's self-collision build used the box filter
 	// wall-clock milliseconds of the upload phases (debug_float "build_ms"): graph, order,
@@ -289,6 +331,7 @@ public:
 		sc_sp.release(); sc_sr.release(); sc_sx.release();
 		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
 		att_idx.release(); att_pos.release(); d_perm.release(); d_kin_ext.release(); d_kin_range.release();
+		rs.release();
 		att_active = false;
 		coloring_built = false;
 		sc_table = 0;
@@ -1279,6 +1322,203 @@ static Engine* cur_engine()
 
 static Engine& engine() { return *cur_engine(); }
 
+// Tangent basis of the floor: the world axis least parallel to n, made orthogonal to n,
+// and n x t1 (the reference viewer's checker axes, forward.cu:284-297).
+static void floor_basis(const float n[3], float t1[3], float t2[3])
+{
+	float a[3] = { 0.0f, 0.0f, 0.0f };
+	const float ax = fabsf(n[0]), ay = fabsf(n[1]), az = fabsf(n[2]);
+	a[(ax <= ay && ax <= az) ? 0 : (ay <= az ? 1 : 2)] = 1.0f;
+	const float d = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+	float x = a[0] - d * n[0], y = a[1] - d * n[1], z = a[2] - d * n[2];
+	const float len = sqrtf(x * x + y * y + z * z);
+	if (len > 1e-12f) { x /= len; y /= len; z /= len; }
+	t1[0] = x; t1[1] = y; t1[2] = z;
+	t2[0] = n[1] * z - n[2] * y;
+	t2[1] = n[2] * x - n[0] * z;
+	t2[2] = n[0] * y - n[1] * x;
+}
+
+// One splatted frame of the current positions (Rasterizer::forward,
+// rasterizer_impl.cu:201-470, without the solver step that the reference runs inside
+// its preprocess).  Shapes: the deformed scales / quaternions of xpbd_compute_shapes
+// when deform_eps >= 0, the created ones otherwise.  Returns the (tile, Gaussian) pair
+// count, the reference's num_rendered.
+static long long render_frame(Engine& E, const float* view, const float* proj, const float* campos, int W, int H,
+	float tan_fovx, float tan_fovy, float scale_mod, float deform_eps, const float* bg, float* out)
+{
+	if (!E.stepped) return fail("xpbd_b200_render: no step yet");
+	if (!view || !proj || !campos || W <= 0 || H <= 0 || !(tan_fovx > 0.0f) || !(tan_fovy > 0.0f))
+		return fail("xpbd_b200_render: invalid camera");
+	auto& R = E.rs;
+	const int n = E.n;
+	if (R.h_colors.empty()) return fail("xpbd_b200_render: no colours (xpbd_b200_render_set_colors)");
+	cudaStream_t st = E.stream;
+	const int tiles_x = (W + dev::kTile - 1) / dev::kTile, tiles_y = (H + dev::kTile - 1) / dev::kTile;
+	const int tiles = tiles_x * tiles_y;
+	if ((long long)W * H > (1LL << 30)) return fail("xpbd_b200_render: image too large");
+	// per-Gaussian buffers, created shapes and opacity (caller order), colours
+	if (R.xy.n != (size_t)n) {
+		CK(R.xy.alloc(n)); CK(R.conic.alloc(n)); CK(R.rgb.alloc(n)); CK(R.rect.alloc(n));
+		CK(R.dkey.alloc(n)); CK(R.dkey_s.alloc(n)); CK(R.iota.alloc(n)); CK(R.order.alloc(n));
+		CK(R.radii.alloc(n)); CK(R.touched.alloc(n)); CK(R.cnt.alloc(n)); CK(R.offs.alloc((size_t)n + 1));
+		CK(R.opacity.alloc(n));
+		CK(cudaMemcpyAsync(R.opacity.p, E.in_opacity.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+		dev::k_iota<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.iota.p);
+		CK(cudaGetLastError());
+		++E.launches;
+	}
+	if (!R.h_total) CK(cudaMallocHost(reinterpret_cast<void**>(&R.h_total), sizeof(long long)));
+	if (R.colors_dirty || R.colors.n != R.h_colors.size()) {
+		CK(R.colors.alloc(R.h_colors.size()));
+		CK(cudaMemcpyAsync(R.colors.p, R.h_colors.data(), sizeof(float) * R.h_colors.size(), cudaMemcpyHostToDevice,
+			st));
+		R.colors_dirty = false;
+	}
+	// stage timings under xpbd_b200_set_profiling (render_prepare / _sort / _tiles)
+	auto seg_begin = [&]() -> cudaEvent_t {
+		cudaEvent_t a = nullptr;
+		if (E.profiling) {
+			a = E.next_event();
+			cudaEventRecord(a, st);
+		}
+		return a;
+	};
+	auto seg_end = [&](int stage, cudaEvent_t a) {
+		if (!E.profiling) return;
+		cudaEvent_t b = E.next_event();
+		cudaEventRecord(b, st);
+		E.prof_records.push_back({ stage, a, b });
+	};
+	cudaEvent_t seg = seg_begin();
+	const float* sc;
+	const float* q;
+	if (deform_eps >= 0.0f) {
+		CK(cudaMemsetAsync(&E.d_ctr->shapes_deformed, 0, sizeof(unsigned int) * 2, st));
+		dev::k_deformed_shapes<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, E.pos_rest.p, E.pos_curr.p, E.off.p,
+			E.nbr.p, E.d_scales.p, E.d_rots.p, deform_eps, E.d_out_scales.p, E.d_out_quats.p, E.d_ctr, E.d_perm.p);
+		CK(cudaGetLastError());
+		++E.launches;
+		sc = E.d_out_scales.p;
+		q = E.d_out_quats.p;
+	} else {
+		if (R.rest_sc.n != 3 * (size_t)n) {
+			CK(R.rest_sc.alloc(3 * (size_t)n)); CK(R.rest_q.alloc(4 * (size_t)n));
+			CK(cudaMemcpyAsync(R.rest_sc.p, E.in_scales.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+			CK(cudaMemcpyAsync(R.rest_q.p, E.in_rots.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, st));
+		}
+		sc = R.rest_sc.p;
+		q = R.rest_q.p;
+	}
+	if (R.W != W || R.H != H) {
+		CK(R.image.alloc(3 * (size_t)W * H)); CK(R.final_T.alloc((size_t)W * H)); CK(R.n_contrib.alloc((size_t)W * H));
+		CK(R.pick.alloc((size_t)W * H)); CK(R.ranges.alloc(tiles));
+		R.W = W;
+		R.H = H;
+	}
+	dev::RenderFrame F;
+	memset(&F, 0, sizeof(F));
+	memcpy(F.view, view, sizeof(F.view));
+	memcpy(F.proj, proj, sizeof(F.proj));
+	memcpy(F.campos, campos, sizeof(F.campos));
+	F.tan_fovx = tan_fovx;
+	F.tan_fovy = tan_fovy;
+	F.focal_x = W / (2.0f * tan_fovx);
+	F.focal_y = H / (2.0f * tan_fovy);
+	F.scale_mod = scale_mod;
+	for (int k = 0; k < 3; ++k) {
+		F.box_lo[k] = R.box_on ? R.box_lo[k] : -FLT_MAX;
+		F.box_hi[k] = R.box_on ? R.box_hi[k] : FLT_MAX;
+		F.bg[k] = bg ? bg[k] : 0.0f;
+	}
+	F.W = W; F.H = H; F.tiles_x = tiles_x; F.tiles_y = tiles_y;
+	F.sh_deg = R.sh_deg;
+	F.sh_coeffs = R.sh_coeffs;
+	F.antialias = R.antialias;
+	F.pick = R.pick_on;
+	if (R.floor_on) {
+		// renderCUDA's checker floor under the solver's ground plane (FORWARD::render,
+		// forward.cu:2663-2680)
+		const float* gn = E.S.ground_n;
+		float t1[3], t2[3];
+		floor_basis(gn, t1, t2);
+		const float inv_checker = 1.0f / fmaxf(R.floor_checker, 1e-8f);
+		F.floor_on = 1;
+		for (int k = 0; k < 3; ++k) {
+			F.fl_cam[k] = campos[k];
+			F.fl_rx[k] = view[4 * k] * tan_fovx;
+			F.fl_ry[k] = view[4 * k + 1] * tan_fovy;
+			F.fl_rz[k] = view[4 * k + 2];
+			F.fl_n[k] = gn[k];
+			F.fl_t1[k] = t1[k] * inv_checker;
+			F.fl_t2[k] = t2[k] * inv_checker;
+			F.fl_origin[k] = R.floor_origin[k];
+		}
+		F.fl_camh = gn[0] * campos[0] + gn[1] * campos[1] + gn[2] * campos[2] - E.S.ground_h;
+		F.fl_pix = 2.0f * tan_fovy / (float)H * inv_checker;
+		F.fl_inv_fade2 = 1.0f / fmaxf(R.floor_fade * R.floor_fade, 1e-12f);
+	}
+	// 1. project every Gaussian
+	dev::k_splat_prepare<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, F, E.pos_out3.p, sc, q, R.opacity.p,
+		R.colors.p, R.xy.p, R.conic.p, R.rgb.p, R.dkey.p, R.radii.p, R.rect.p, R.touched.p);
+	CK(cudaGetLastError());
+	seg_end(ST_RENDER_PREPARE, seg);
+	seg = seg_begin();
+	// 2. depth order (stable), tile counts in that order, their prefix sums
+	size_t need = 0, t1b = 0, t2b = 0;
+	CK(cub::DeviceRadixSort::SortPairs(nullptr, t1b, R.dkey.p, R.dkey_s.p, R.iota.p, R.order.p, n, 0, 32, st));
+	CK(cub::DeviceScan::InclusiveSum(nullptr, t2b, R.cnt.p, R.offs.p + 1, n, st));
+	need = std::max(t1b, t2b);
+	if (R.temp.n < need) CK(R.temp.alloc(need));
+	CK(cub::DeviceRadixSort::SortPairs(R.temp.p, t1b, R.dkey.p, R.dkey_s.p, R.iota.p, R.order.p, n, 0, 32, st));
+	dev::k_splat_counts<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.order.p, R.touched.p, R.cnt.p);
+	CK(cudaGetLastError());
+	CK(cudaMemsetAsync(R.offs.p, 0, sizeof(long long), st));
+	CK(cub::DeviceScan::InclusiveSum(R.temp.p, t2b, R.cnt.p, R.offs.p + 1, n, st));
+	CK(cudaMemcpyAsync(R.h_total, R.offs.p + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
+	CK(cudaStreamSynchronize(st));
+	const long long m = *R.h_total;
+	if (m < 0 || m > INT_MAX) return fail("xpbd_b200_render: %lld tile pairs (limit %d)", m, INT_MAX);
+	E.launches += 2;
+	// 3. (tile, Gaussian) pairs in depth order, stable sort by tile, tile ranges
+	CK(cudaMemsetAsync(R.ranges.p, 0, sizeof(int2) * tiles, st));
+	if (m > 0) {
+		if (R.tkey.n < (size_t)m) {
+			const size_t cap = (size_t)m + m / 4;
+			CK(R.tkey.alloc(cap)); CK(R.tkey_s.alloc(cap)); CK(R.val.alloc(cap)); CK(R.val_s.alloc(cap));
+		}
+		dev::k_splat_pairs<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.order.p, R.offs.p, R.rect.p, tiles_x,
+			R.tkey.p, R.val.p);
+		CK(cudaGetLastError());
+		int bits = 1;
+		while ((1LL << bits) < tiles) ++bits;
+		size_t t3b = 0;
+		CK(cub::DeviceRadixSort::SortPairs(nullptr, t3b, R.tkey.p, R.tkey_s.p, R.val.p, R.val_s.p, (int)m, 0, bits,
+			st));
+		if (R.temp.n < t3b) CK(R.temp.alloc(t3b));
+		CK(cub::DeviceRadixSort::SortPairs(R.temp.p, t3b, R.tkey.p, R.tkey_s.p, R.val.p, R.val_s.p, (int)m, 0, bits,
+			st));
+		dev::k_splat_ranges<<<(int)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>((int)m, R.tkey_s.p, R.ranges.p);
+		CK(cudaGetLastError());
+		E.launches += 2;
+	}
+	seg_end(ST_RENDER_SORT, seg);
+	seg = seg_begin();
+	// 4. composite every tile
+	if (R.pick_on) CK(cudaMemsetAsync(R.pick.p, 0xff, sizeof(int) * (size_t)W * H, st));
+	dev::k_splat_tiles<<<dim3(tiles_x, tiles_y), dev::kTilePix, 0, st>>>(F, R.ranges.p, R.val_s.p, R.xy.p,
+		R.conic.p, R.rgb.p, R.image.p, R.final_T.p, R.n_contrib.p, R.pick.p);
+	CK(cudaGetLastError());
+	++E.launches;
+	seg_end(ST_RENDER_TILES, seg);
+	R.pairs = m;
+	if (out) {
+		CK(cudaMemcpyAsync(out, R.image.p, sizeof(float) * 3 * (size_t)W * H, cudaMemcpyDeviceToHost, st));
+		CK(cudaStreamSynchronize(st));
+	}
+	return m;
+}
+
 }  // namespace xpbd
 
 using namespace xpbd;
@@ -1305,6 +1545,8 @@ XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const flo
 	E.in_scales.assign(scales, scales + 3 * (size_t)n);
 	E.in_rots.assign(rots, rots + 4 * (size_t)n);
 	E.in_opacity.assign(opacity, opacity + n);
+	E.rs.h_colors.clear();
+	E.rs.colors_dirty = false;
 	E.in_edges.assign(edges ? edges : (const int*)nullptr, edges ? edges + 2 * (size_t)e : (const int*)nullptr);
 	E.in_rest.assign(rest ? rest : (const float*)nullptr, rest ? rest + e : (const float*)nullptr);
 	E.in_stiff.assign(stiff ? stiff : (const float*)nullptr, stiff ? stiff + e : (const float*)nullptr);
@@ -1656,6 +1898,73 @@ XPBD_API void xpbd_b200_set_gpu_builder(int enabled) { engine().S.gpu_builder = 
 // exportPhysicsGraph (forward.cu:4612-4663): the directed graph and rest positions as an
 // APGGRPH1 file, in the order given to xpbd_create (the reference writes its viewer's
 // internal order; tools/import_graph.py renumbers either by matching positions)
+XPBD_API int xpbd_b200_render_set_colors(int n, int sh_degree, const float* data)
+{
+	// colours of the splatting pass: RGB per Gaussian (sh_degree -1, the reference's
+	// colors_precomp) or (sh_degree + 1)^2 RGB spherical-harmonic coefficients per
+	// Gaussian ([n][coeffs][3], the reference's shs) evaluated toward the camera
+	Engine& E = *cur_engine();
+	if (E.n <= 0 || n != E.n) return fail("xpbd_b200_render_set_colors: size mismatch (create first)");
+	if (!data || sh_degree < -1 || sh_degree > 3) return fail("xpbd_b200_render_set_colors: invalid arguments");
+	const int coeffs = sh_degree < 0 ? 1 : (sh_degree + 1) * (sh_degree + 1);
+	E.rs.h_colors.assign(data, data + (size_t)3 * coeffs * n);
+	E.rs.sh_deg = sh_degree;
+	E.rs.sh_coeffs = coeffs;
+	E.rs.colors_dirty = true;
+	return 0;
+}
+
+XPBD_API void xpbd_b200_render_set_options(int antialiasing, const float* box_min, const float* box_max, int pick)
+{
+	auto& R = cur_engine()->rs;
+	R.antialias = antialiasing != 0;
+	R.pick_on = pick != 0;
+	R.box_on = box_min && box_max;
+	for (int k = 0; k < 3; ++k) {
+		R.box_lo[k] = R.box_on ? box_min[k] : 0.0f;
+		R.box_hi[k] = R.box_on ? box_max[k] : 0.0f;
+	}
+}
+
+XPBD_API void xpbd_b200_render_set_floor(int visible, const float* origin, float checker, float fade_radius)
+{
+	// setGroundRender (forward.cu:4448-4462); the plane is the solver's ground
+	auto& R = cur_engine()->rs;
+	R.floor_on = visible != 0 && origin;
+	if (!R.floor_on) return;
+	for (int k = 0; k < 3; ++k) R.floor_origin[k] = origin[k];
+	R.floor_checker = fmaxf(checker, 1e-8f);
+	R.floor_fade = fmaxf(fade_radius, 1e-8f);
+}
+
+XPBD_API long long xpbd_b200_render(const float* view, const float* proj, const float* campos, int width, int height,
+	float tan_fovx, float tan_fovy, float scale_modifier, float deform_eps, const float* bg, float* out)
+{
+	return render_frame(*cur_engine(), view, proj, campos, width, height, tan_fovx, tan_fovy, scale_modifier,
+		deform_eps, bg, out);
+}
+
+XPBD_API unsigned long long xpbd_b200_render_device(void)
+{
+	return reinterpret_cast<unsigned long long>(cur_engine()->rs.image.p);
+}
+
+XPBD_API int xpbd_b200_render_aux(float* final_T, int* n_contrib, int* pick, long long npix, int* radii, int n)
+{
+	Engine& E = *cur_engine();
+	auto& R = E.rs;
+	if (!R.image.p) return fail("xpbd_b200_render_aux: no frame yet");
+	const long long np = (long long)R.W * R.H;
+	if ((final_T || n_contrib || pick) && npix != np) return fail("xpbd_b200_render_aux: %lld pixels, not %lld", npix, np);
+	if (radii && n != E.n) return fail("xpbd_b200_render_aux: size mismatch");
+	if (pick && !R.pick_on) return fail("xpbd_b200_render_aux: picking is off");
+	if (final_T) CK(cudaMemcpyAsync(final_T, R.final_T.p, sizeof(float) * np, cudaMemcpyDeviceToHost, E.stream));
+	if (n_contrib) CK(cudaMemcpyAsync(n_contrib, R.n_contrib.p, sizeof(int) * np, cudaMemcpyDeviceToHost, E.stream));
+	if (pick) CK(cudaMemcpyAsync(pick, R.pick.p, sizeof(int) * np, cudaMemcpyDeviceToHost, E.stream));
+	if (radii) CK(cudaMemcpyAsync(radii, R.radii.p, sizeof(int) * E.n, cudaMemcpyDeviceToHost, E.stream));
+	return E.sync();
+}
+
 XPBD_API int xpbd_b200_export_graph(const char* path)
 {
 	Engine& E = *cur_engine();

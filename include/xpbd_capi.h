@@ -136,6 +136,32 @@ XPBD_API int xpbd_b200_export_graph(const char* path);
 /* Arrival times (caller order; 1e9 where the wave has not arrived); returns N or -1. */
 XPBD_API int xpbd_b200_chainmail_times(float* out, int n);
 
+/* ---- Splatting of the current Gaussians into a device image (the viewer's 3DGS
+ * rasteriser, CudaRasterizer::Rasterizer::forward, rasterizer_impl.cu:201-470, with
+ * preprocessCUDA / renderCUDA, forward.cu:1919-2650), no graphics API. ---- */
+/* Colours: sh_degree -1 -> RGB per Gaussian (colors_precomp); 0..3 -> (d+1)^2 RGB
+ * spherical-harmonic coefficients per Gaussian, [n][coeffs][3] (shs).  After
+ * xpbd_create; kept until the next create.  0 or -1. */
+XPBD_API int xpbd_b200_render_set_colors(int n, int sh_degree, const float* data);
+/* antialiasing (the reference's flag), an optional crop box (boxmin/boxmax; NULL = none)
+ * and per-pixel picking of the first Gaussian with alpha > 0.1 (id_buffer). */
+XPBD_API void xpbd_b200_render_set_options(int antialiasing, const float* box_min, const float* box_max, int pick);
+/* Checker floor in place of the background under the solver's ground plane
+ * (setGroundRender, forward.cu:4448-4462). */
+XPBD_API void xpbd_b200_render_set_floor(int visible, const float* origin, float checker, float fade_radius);
+/* One frame: view / proj column-major 4x4 (world->view, world->clip), camera position,
+ * image size, tan of the half fields of view, scale modifier; deform_eps >= 0 renders
+ * the deformed shapes of xpbd_compute_shapes(deform_eps), < 0 the created ones; bg
+ * RGB (NULL = black); out (3 x H x W floats, channel-major, NULL = keep on the device).
+ * Returns the number of (tile, Gaussian) pairs (num_rendered) or -1. */
+XPBD_API long long xpbd_b200_render(const float* view, const float* proj, const float* campos, int width, int height,
+	float tan_fovx, float tan_fovy, float scale_modifier, float deform_eps, const float* bg, float* out);
+/* Device pointer of the last image (float, 3 x H x W). */
+XPBD_API unsigned long long xpbd_b200_render_device(void);
+/* Last frame's final transmittance, contributor count and picked Gaussian per pixel
+ * (-1 none; picking on) and the screen radius per Gaussian (0 culled); NULL skips one. */
+XPBD_API int xpbd_b200_render_aux(float* final_T, int* n_contrib, int* pick, long long npix, int* radii, int n);
+
 /* Independent solver instances: a new engine (own scene, settings and stream), its
  * release, and the choice of the engine that the reference entry points above act on
  * from the calling thread (NULL: the process-wide default engine). */

@@ -13,6 +13,8 @@
 // element count (or -1 when the buffer does not exist or is too small).
 #include "forward.cu"
 
+#include <cub/device/device_scan.cuh>
+
 namespace {
 template <typename T>
 int copy_out(const T* dev, long long count, T* host, long long cap)
@@ -204,6 +206,229 @@ __attribute__((visibility("default"))) int refshim_chainmail_run(int prop_iters,
 		nullptr);
 	cudaDeviceSynchronize();
 	return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+
+// ---- the viewer's rasteriser on explicit inputs ----
+// The reference's own preprocessCUDA (forward.cu:1919-2467; demo modes off, no
+// neighbour graph, so the given shapes are used as they are) and renderCUDA
+// (forward.cu:2469-2650, through FORWARD::render), with the binning steps of
+// Rasterizer::forward (rasterizer_impl.cu:330-370: inclusive scan of touched tiles,
+// pair keys tile << 32 | depth written in Gaussian order, cub stable radix sort over
+// 32 + bits(tiles) bits, tile ranges) done by the small kernels below.
+namespace refrender {
+
+// the reference's bit count of the tile id (getHigherMsb, rasterizer_impl.cu:34-49 is
+// file-local there): the smallest b with n >> b == 0
+int getHigherMsb(uint32_t n)
+{
+	int b = 0;
+	while (b < 32 && (n >> b)) ++b;
+	return b;
+}
+
+__global__ void pairs_kernel(int P, const float2* xy, const float* depth, const uint32_t* incl, const int* radii,
+	dim3 grid, uint64_t* keys, uint32_t* vals)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= P || radii[i] <= 0) return;
+	uint32_t at = i == 0 ? 0 : incl[i - 1];
+	uint2 lo, hi;
+	getRect(xy[i], radii[i], lo, hi, grid);
+	for (unsigned y = lo.y; y < hi.y; ++y)
+		for (unsigned x = lo.x; x < hi.x; ++x) {
+			keys[at] = ((uint64_t)(y * grid.x + x) << 32) | __float_as_uint(depth[i]);
+			vals[at] = (uint32_t)i;
+			++at;
+		}
+}
+
+__global__ void ranges_kernel(int L, const uint64_t* keys, uint2* ranges)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= L) return;
+	const uint32_t t = (uint32_t)(keys[k] >> 32);
+	if (k == 0 || (uint32_t)(keys[k - 1] >> 32) != t) ranges[t].x = k;
+	if (k == L - 1 || (uint32_t)(keys[k + 1] >> 32) != t) ranges[t].y = k + 1;
+}
+
+struct Frame {
+	int P = 0, D = 0, M = 0, W = 0, H = 0, sh = -1, aa = 0;
+	dim3 grid, block;
+	float tan_fovx = 0, tan_fovy = 0, focal_x = 0, focal_y = 0, scale_mod = 1;
+	float3 bmin, bmax;
+	float *pos = nullptr, *sc = nullptr, *rot = nullptr, *op = nullptr, *col = nullptr, *view = nullptr,
+		*proj = nullptr, *cam = nullptr, *depth = nullptr, *cov = nullptr, *rgb = nullptr, *T = nullptr,
+		*out = nullptr, *bg = nullptr;
+	float2* xy = nullptr;
+	float4* con = nullptr;
+	int *radii = nullptr, *pick = nullptr;
+	uint32_t *touched = nullptr, *incl = nullptr, *vals = nullptr, *vals_s = nullptr, *contrib = nullptr;
+	uint64_t *keys = nullptr, *keys_s = nullptr;
+	uint2* ranges = nullptr;
+	bool* clamped = nullptr;
+	void* temp = nullptr;
+	size_t temp_bytes = 0;
+	long long cap = 0, L = 0;
+
+	// one frame on resident inputs; returns the pair count
+	long long run()
+	{
+		preprocessCUDA<NUM_CHANNELS><<<(P + 255) / 256, 256>>>(P, D, M, pos, pos, nullptr, nullptr, nullptr, nullptr,
+			(const glm::vec3*)sc, scale_mod, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f,
+			(const glm::vec4*)rot, op, sh < 0 ? nullptr : col, clamped, nullptr, sh < 0 ? col : nullptr, view, proj,
+			(const glm::vec3*)cam, W, H, tan_fovx, tan_fovy, focal_x, focal_y, radii, xy, depth, cov, rgb, con, grid,
+			touched, false, nullptr, bmin, bmax, aa != 0, 0.0f, false, false, false, nullptr, 0.0f, nullptr);
+		size_t need = 0;
+		cub::DeviceScan::InclusiveSum(nullptr, need, touched, incl, P);
+		grow(need);
+		cub::DeviceScan::InclusiveSum(temp, need, touched, incl, P);
+		uint32_t total = 0;
+		cudaMemcpy(&total, incl + P - 1, 4, cudaMemcpyDeviceToHost);
+		L = total;
+		const int tiles = grid.x * grid.y;
+		cudaMemset(ranges, 0, sizeof(uint2) * tiles);
+		if (L > 0) {
+			if (L > cap) {
+				cudaFree(keys); cudaFree(keys_s); cudaFree(vals); cudaFree(vals_s);
+				cap = L + L / 4;
+				cudaMalloc(&keys, 8 * cap); cudaMalloc(&keys_s, 8 * cap);
+				cudaMalloc(&vals, 4 * cap); cudaMalloc(&vals_s, 4 * cap);
+			}
+			pairs_kernel<<<(P + 255) / 256, 256>>>(P, xy, depth, incl, radii, grid, keys, vals);
+			const int bit = getHigherMsb(tiles);
+			cub::DeviceRadixSort::SortPairs(nullptr, need, keys, keys_s, vals, vals_s, (int)L, 0, 32 + bit);
+			grow(need);
+			cub::DeviceRadixSort::SortPairs(temp, need, keys, keys_s, vals, vals_s, (int)L, 0, 32 + bit);
+			ranges_kernel<<<(int)((L + 255) / 256), 256>>>((int)L, keys_s, ranges);
+		}
+		if (pick) cudaMemset(pick, 0xff, 4 * (size_t)W * H);
+		FORWARD::render(grid, block, ranges, vals_s, W, H, xy, sh < 0 ? col : rgb, con, T, contrib, bg, out, pick);
+		return L;
+	}
+
+	void grow(size_t need)
+	{
+		if (need <= temp_bytes) return;
+		cudaFree(temp);
+		cudaMalloc(&temp, need);
+		temp_bytes = need;
+	}
+
+	void release()
+	{
+		void* bufs[] = { pos, sc, rot, op, col, view, proj, cam, depth, cov, rgb, T, out, bg, xy, con, radii, pick,
+			touched, incl, vals, vals_s, contrib, keys, keys_s, ranges, clamped, temp };
+		for (void* b : bufs)
+			if (b) cudaFree(b);
+	}
+};
+
+}  // namespace refrender
+
+static long long ref_render(int P, const float* pos, const float* scales, const float* rots, const float* opacity,
+	const float* colors, int sh_degree, const float* view, const float* proj, const float* campos, int W, int H,
+	float tan_fovx, float tan_fovy, float scale_mod, int antialias, const float* box_lo, const float* box_hi,
+	const float* bg, int pick, const float* floor_p, float* out, float* final_T_out, int* n_contrib_out, int* pick_out,
+	int* radii_out, int reps, float* ms_per_frame)
+{
+	if (P <= 0 || W <= 0 || H <= 0) return -1;
+	refrender::Frame F;
+	F.P = P; F.W = W; F.H = H; F.sh = sh_degree; F.aa = antialias;
+	F.D = sh_degree < 0 ? 0 : sh_degree;
+	F.M = sh_degree < 0 ? 0 : (sh_degree + 1) * (sh_degree + 1);
+	F.grid = dim3((W + BLOCK_X - 1) / BLOCK_X, (H + BLOCK_Y - 1) / BLOCK_Y, 1);
+	F.block = dim3(BLOCK_X, BLOCK_Y, 1);
+	F.tan_fovx = tan_fovx; F.tan_fovy = tan_fovy;
+	F.focal_y = H / (2.0f * tan_fovy); F.focal_x = W / (2.0f * tan_fovx);
+	F.scale_mod = scale_mod;
+	F.bmin = box_lo ? make_float3(box_lo[0], box_lo[1], box_lo[2]) : make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+	F.bmax = box_hi ? make_float3(box_hi[0], box_hi[1], box_hi[2]) : make_float3(FLT_MAX, FLT_MAX, FLT_MAX);
+	const size_t ncol = sh_degree < 0 ? 3 * (size_t)P : 3 * (size_t)F.M * P;
+	const int tiles = F.grid.x * F.grid.y;
+	const size_t np = (size_t)W * H;
+	cudaMalloc(&F.pos, 12 * (size_t)P); cudaMalloc(&F.sc, 12 * (size_t)P); cudaMalloc(&F.rot, 16 * (size_t)P);
+	cudaMalloc(&F.op, 4 * (size_t)P); cudaMalloc(&F.col, 4 * ncol); cudaMalloc(&F.view, 64); cudaMalloc(&F.proj, 64);
+	cudaMalloc(&F.cam, 12); cudaMalloc(&F.depth, 4 * (size_t)P); cudaMalloc(&F.cov, 24 * (size_t)P);
+	cudaMalloc(&F.rgb, 12 * (size_t)P); cudaMalloc(&F.xy, 8 * (size_t)P); cudaMalloc(&F.con, 16 * (size_t)P);
+	cudaMalloc(&F.radii, 4 * (size_t)P); cudaMalloc(&F.touched, 4 * (size_t)P); cudaMalloc(&F.incl, 4 * (size_t)P);
+	cudaMalloc(&F.clamped, 3 * (size_t)P); cudaMalloc(&F.ranges, sizeof(uint2) * tiles);
+	cudaMalloc(&F.T, 4 * np); cudaMalloc(&F.contrib, 4 * np); cudaMalloc(&F.out, 12 * np); cudaMalloc(&F.bg, 12);
+	if (pick) cudaMalloc(&F.pick, 4 * np);
+	cudaMemcpy(F.pos, pos, 12 * (size_t)P, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.sc, scales, 12 * (size_t)P, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.rot, rots, 16 * (size_t)P, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.op, opacity, 4 * (size_t)P, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.col, colors, 4 * ncol, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.view, view, 64, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.proj, proj, 64, cudaMemcpyHostToDevice);
+	cudaMemcpy(F.cam, campos, 12, cudaMemcpyHostToDevice);
+	const float zero3[3] = { 0.0f, 0.0f, 0.0f };
+	cudaMemcpy(F.bg, bg ? bg : zero3, 12, cudaMemcpyHostToDevice);
+	// checker floor: the solver's ground statics plus setGroundRender, restored after
+	const float keepN[3] = { g_groundN[0], g_groundN[1], g_groundN[2] };
+	const float keepH = g_groundHeight;
+	if (floor_p) {
+		for (int k = 0; k < 3; ++k) g_groundN[k] = floor_p[k];
+		g_groundHeight = floor_p[3];
+		FORWARD::setGroundRender(true, floor_p + 4, floor_p[7], floor_p[8], view, campos, tan_fovx, tan_fovy);
+	}
+	long long L = F.run();
+	if (reps > 0 && ms_per_frame) {
+		cudaEvent_t a, b;
+		cudaEventCreate(&a);
+		cudaEventCreate(&b);
+		cudaDeviceSynchronize();
+		cudaEventRecord(a);
+		for (int r = 0; r < reps; ++r) L = F.run();
+		cudaEventRecord(b);
+		cudaEventSynchronize(b);
+		float ms = 0.0f;
+		cudaEventElapsedTime(&ms, a, b);
+		*ms_per_frame = ms / reps;
+		cudaEventDestroy(a);
+		cudaEventDestroy(b);
+	}
+	cudaDeviceSynchronize();
+	if (floor_p) {
+		FORWARD::setGroundRender(false, nullptr, 1.0f, 1.0f, nullptr, nullptr, 1.0f, 1.0f);
+		for (int k = 0; k < 3; ++k) g_groundN[k] = keepN[k];
+		g_groundHeight = keepH;
+	}
+	const bool ok = cudaGetLastError() == cudaSuccess;
+	if (out) cudaMemcpy(out, F.out, 12 * np, cudaMemcpyDeviceToHost);
+	if (final_T_out) cudaMemcpy(final_T_out, F.T, 4 * np, cudaMemcpyDeviceToHost);
+	if (n_contrib_out) cudaMemcpy(n_contrib_out, F.contrib, 4 * np, cudaMemcpyDeviceToHost);
+	if (pick_out && pick) cudaMemcpy(pick_out, F.pick, 4 * np, cudaMemcpyDeviceToHost);
+	if (radii_out) cudaMemcpy(radii_out, F.radii, 4 * (size_t)P, cudaMemcpyDeviceToHost);
+	F.release();
+	return ok ? L : -1;
+}
+
+// One frame (sh_degree -1: colours are RGB, colors_precomp; else SH coefficients
+// [n][(d+1)^2][3]; floor_p NULL or {normal[3], height, origin[3], checker, fade}).
+// Returns the pair count (num_rendered).
+__attribute__((visibility("default"))) long long refshim_render(int P, const float* pos, const float* scales,
+	const float* rots, const float* opacity, const float* colors, int sh_degree, const float* view, const float* proj,
+	const float* campos, int W, int H, float tan_fovx, float tan_fovy, float scale_mod, int antialias,
+	const float* box_lo, const float* box_hi, const float* bg, int pick, const float* floor_p, float* out,
+	float* final_T_out, int* n_contrib_out, int* pick_out, int* radii_out)
+{
+	return ref_render(P, pos, scales, rots, opacity, colors, sh_degree, view, proj, campos, W, H, tan_fovx, tan_fovy,
+		scale_mod, antialias, box_lo, box_hi, bg, pick, floor_p, out, final_T_out, n_contrib_out, pick_out, radii_out,
+		0, nullptr);
+}
+
+// The same frame repeated reps times on resident inputs: milliseconds per frame
+// (CUDA events around preprocess + scan + pair keys + sort + ranges + render, the
+// pair-count readback included as in Rasterizer::forward).
+__attribute__((visibility("default"))) long long refshim_render_timed(int P, const float* pos, const float* scales,
+	const float* rots, const float* opacity, const float* colors, int sh_degree, const float* view, const float* proj,
+	const float* campos, int W, int H, float tan_fovx, float tan_fovy, int reps, float* ms_per_frame)
+{
+	return ref_render(P, pos, scales, rots, opacity, colors, sh_degree, view, proj, campos, W, H, tan_fovx, tan_fovy,
+		1.0f, 0, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, reps,
+		ms_per_frame);
 }
 
 }  // extern "C"

@@ -51,6 +51,17 @@ int oracle_chainmail_seed(int count, const int* idx, const float* delta);
 int oracle_chainmail_run(int prop_iters, int relax_iters, float prop_strength, float relax_stiffness,
 	float relax_damping);
 int oracle_chainmail_times(float* out, int n);
+/* Stateless 3DGS forward rasteriser (render_oracle.c): explicit positions, scales,
+ * quaternions (w, x, y, z), opacities and colours (RGB when sh_degree is -1, else
+ * [n][(d+1)^2][3] SH coefficients); camera as the library's xpbd_b200_render; box_lo /
+ * box_hi NULL for no crop box; floor_p NULL or {normal[3], height, origin[3], checker,
+ * fade radius}.  out is 3 x H x W; final_T, n_contrib, picked (H x W) and radii (n) may
+ * be NULL.  Returns the (tile, Gaussian) pair count. */
+long long oracle_render(int n, const float* pos, const float* scales, const float* quats, const float* opacity,
+	const float* colors, int sh_degree, const float* view, const float* proj, const float* campos, int W, int H,
+	float tan_fovx, float tan_fovy, float scale_mod, int antialias, const float* box_lo, const float* box_hi,
+	const float* bg, int pick, const float* floor_p, float* out, float* final_T, int* n_contrib, int* picked,
+	int* radii);
 
 #ifdef __cplusplus
 }

@@ -171,3 +171,46 @@ def contacts_equal(count_a, list_a, count_b, list_b):
         if not np.array_equal(la[i, :ca[i]], lb[i, :ca[i]]):
             return False
     return True
+
+
+# ---------------------------------------------------------------- splatting checkers
+def cpu_render(fn, pos, scales, quats, opacity, colors, sh_degree, cam, scale_mod=1.0, antialias=False, box=None,
+               bg=(0.0, 0.0, 0.0), pick=False, floor=None):
+    """One frame through a stateless rasteriser with the oracle_render / refshim_render
+    signature.  floor: None or (normal[3], height, origin[3], checker, fade)."""
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)   # noqa: E731
+    P = ctypes.c_void_p
+    fn.argtypes = ([ctypes.c_int] + [P] * 5 + [ctypes.c_int] + [P] * 3 + [ctypes.c_int, ctypes.c_int]
+                   + [ctypes.c_float] * 3 + [ctypes.c_int] + [P] * 3 + [ctypes.c_int] + [P] * 6)
+    fn.restype = ctypes.c_longlong
+    n, W, H = len(pos), cam.width, cam.height
+    arrs = [f32(pos), f32(scales), f32(quats), f32(opacity), f32(colors)]
+    lo, hi = (f32(box[0]), f32(box[1])) if box is not None else (None, None)
+    bgv = f32(bg)
+    fl = None
+    if floor is not None:
+        fl = f32(list(floor[0]) + [floor[1]] + list(floor[2]) + [floor[3], floor[4]])
+    out = np.zeros((3, H, W), np.float32)
+    ft = np.zeros((H, W), np.float32)
+    nc = np.zeros((H, W), np.int32)
+    pk = np.full((H, W), -1, np.int32)
+    radii = np.zeros(n, np.int32)
+    ptr = lambda a: None if a is None else a.ctypes.data   # noqa: E731
+    m = fn(n, *[a.ctypes.data for a in arrs], int(sh_degree), cam.view.ctypes.data, cam.proj.ctypes.data,
+           cam.campos.ctypes.data, W, H, cam.tan_fovx, cam.tan_fovy, float(scale_mod), int(antialias), ptr(lo),
+           ptr(hi), bgv.ctypes.data, int(pick), ptr(fl), out.ctypes.data, ft.ctypes.data, nc.ctypes.data,
+           pk.ctypes.data, radii.ctypes.data)
+    if m < 0:
+        raise RuntimeError("render failed")
+    return {"image": out, "final_T": ft, "n_contrib": nc, "pick": pk, "radii": radii, "pairs": int(m)}
+
+
+def oracle_render(*args, **kw):
+    lib = ctypes.CDLL(ensure_oracle())
+    return cpu_render(lib.oracle_render, *args, **kw)
+
+
+def image_diff(a, b):
+    """(max |a-b|, mean |a-b|, fraction of values with |a-b| > 1e-3)."""
+    d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+    return float(d.max()), float(d.mean()), float((d > 1e-3).mean())

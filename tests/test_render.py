@@ -1,0 +1,276 @@
+"""Splatting pass (xpbd_b200_render): the library's rasteriser against the oracle's
+restatement (render_oracle.c) and the reference's own preprocessCUDA / renderCUDA
+(refshim_render, and the golden frames it produced, tests/golden/render_ref.npz).
+
+Tolerances.  Both sides compute in FP32 with different contraction (FMA) and exp
+implementations, so a Gaussian whose alpha lands within an ulp of 1/255, or whose
+radius lands on an integer, can switch between the two; each switch moves a few pixels
+by at most that Gaussian's 3-sigma alpha (< 0.012).  The tests therefore bound the
+maximum pixel difference by 0.05, the mean by 2e-5 and the fraction of values off by
+more than 1e-3 by 0.2 %; radii and per-pixel contributor counts must agree for at least
+99.9 % / 99 % of entries and the pair count within 0.1 %.
+"""
+import ctypes
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+import helpers
+
+pkg = importlib.import_module("3dgs-isaac-sim-xpbd_b200")
+Camera = pkg.splat.Camera
+
+MAX_DIFF, MEAN_DIFF, FRAC_OFF = 0.05, 2e-5, 2e-3
+
+
+def assert_frames_close(a, b, what, contrib=True):
+    mx, mean, frac = helpers.image_diff(a["image"], b["image"])
+    assert mx <= MAX_DIFF and mean <= MEAN_DIFF and frac <= FRAC_OFF, \
+        f"{what}: image max {mx:.3e}, mean {mean:.3e}, off {frac:.2e}"
+    mx, mean, frac = helpers.image_diff(a["final_T"], b["final_T"])
+    assert mx <= MAX_DIFF and frac <= FRAC_OFF, f"{what}: final_T max {mx:.3e}, off {frac:.2e}"
+    ra, rb = np.asarray(a["radii"]), np.asarray(b["radii"])
+    assert (ra == rb).mean() >= 0.999, f"{what}: radii agree for {(ra == rb).mean():.4f}"
+    pa, pb = a["pairs"], b["pairs"]
+    assert abs(pa - pb) <= max(2, 1e-3 * max(pa, pb)), f"{what}: pairs {pa} vs {pb}"
+    if contrib:
+        ca, cb = np.asarray(a["n_contrib"]), np.asarray(b["n_contrib"])
+        assert (ca == cb).mean() >= 0.99, f"{what}: n_contrib agree for {(ca == cb).mean():.4f}"
+
+
+def small_set(n=800, seed=5, sh_degree=-1):
+    sc = pkg.scenes.make_scene(n, seed, radii=(0.5, 0.35, 0.3))
+    return sc, pkg.splat.synthetic_colors(n, sh_degree, seed + 1)
+
+
+# ------------------------------------------------------------------ oracle on the CPU
+def test_oracle_single_gaussian_symmetric():
+    cam = Camera.look_at((0, -3, 0), (0, 0, 0), (0, 0, 1), 64, 48)
+    r = helpers.oracle_render(np.zeros((1, 3)), np.full((1, 3), 0.1), [[1, 0, 0, 0]], [0.9], [[1, 0.5, 0.25]], -1,
+                              cam, bg=(0, 0, 1))
+    img = r["image"]
+    # centre of the image at pixel (31.5, 23.5): mirror symmetric about it
+    assert np.allclose(img[:, :, :32], img[:, :, 32:][:, :, ::-1], atol=1e-6)
+    assert np.allclose(img[:, :24, :], img[:, 24:, :][:, ::-1, :], atol=1e-6)
+    a = img[0, 23, 31]                                           # alpha near the centre (red 1)
+    assert a > 0.8 and abs(img[1, 23, 31] - 0.5 * a) < 1e-6 and abs(img[2, 23, 31] - (0.25 * a + (1 - a))) < 1e-6
+    assert np.allclose(img[:, 0, 0], (0, 0, 1), atol=1e-6)        # background in a corner
+    assert r["pairs"] >= 1 and r["radii"][0] > 0
+
+
+def test_oracle_front_gaussian_occludes():
+    cam = Camera.look_at((0, -3, 0), (0, 0, 0), (0, 0, 1), 32, 32)
+    pos = [[0, 0.5, 0], [0, -0.5, 0]]          # the second one is nearer the camera
+    sc = np.full((2, 3), 0.3)
+    q = [[1, 0, 0, 0]] * 2
+    r = helpers.oracle_render(pos, sc, q, [0.99, 0.99], [[0, 1, 0], [1, 0, 0]], -1, cam)
+    c = r["image"][:, 15, 15]
+    assert c[0] > 0.9 and c[1] < 0.1, c
+
+
+def test_oracle_culling_behind_camera_and_box():
+    cam = Camera.look_at((0, -3, 0), (0, 0, 0), (0, 0, 1), 32, 32)
+    pos = [[0, -4, 0], [0, 0, 0]]
+    r = helpers.oracle_render(pos, np.full((2, 3), 0.1), [[1, 0, 0, 0]] * 2, [0.9, 0.9], [[1, 1, 1]] * 2, -1, cam)
+    assert r["radii"][0] == 0 and r["radii"][1] > 0
+    r = helpers.oracle_render(pos, np.full((2, 3), 0.1), [[1, 0, 0, 0]] * 2, [0.9, 0.9], [[1, 1, 1]] * 2, -1, cam,
+                              box=((0.5, 0.5, 0.5), (1, 1, 1)))
+    assert (r["radii"] == 0).all() and r["pairs"] == 0
+    assert np.allclose(r["image"], 0.0) and np.allclose(r["final_T"], 1.0)
+
+
+def test_oracle_sh_degree0_equals_rgb():
+    sc, rgb = small_set(300, 7)
+    sh = ((rgb - 0.5) / 0.28209479177387814)[:, None, :]
+    cam = Camera.framing(sc["pos"], 48, 40)
+    a = helpers.oracle_render(sc["pos"], sc["scales"], sc["rots"], sc["opacity"], rgb, -1, cam)
+    b = helpers.oracle_render(sc["pos"], sc["scales"], sc["rots"], sc["opacity"], sh, 0, cam)
+    assert helpers.image_diff(a["image"], b["image"])[0] < 1e-5
+
+
+def golden_ref():
+    path = os.path.join(helpers.GOLDEN, "render_ref.npz")
+    if not os.path.isfile(path):
+        pytest.skip("render_ref.npz not generated")
+    return np.load(path)
+
+
+def golden_case_frames(g, fn):
+    mk = importlib.import_module("golden.make_render_golden")
+    for name, n, seed, deg, W, H, direction, aa, box, pick, floor in mk.CASES:
+        sc, colors, cam = mk.case_inputs(n, seed, deg, W, H, direction)
+        bx = ((-0.3, -0.5, -0.5), (0.3, 0.5, 0.5)) if box else None
+        fl = ((0.0, 0.0, 1.0), -0.4, (0.0, 0.0, -0.4), 0.15, 3.0) if floor else None
+        ref = {k.split("/", 1)[1]: g[k] for k in g.files if k.startswith(name + "/")}
+        ref["pairs"] = int(ref["pairs"])
+        got = fn(sc, colors, deg, cam, aa, bx, pick, fl)
+        yield name, ref, got
+
+
+def test_oracle_matches_reference_golden():
+    """The restatement against frames of the reference's own kernels (pins the oracle)."""
+    g = golden_ref()
+
+    def run(sc, colors, deg, cam, aa, bx, pick, fl):
+        return helpers.oracle_render(sc["pos"], sc["scales"], sc["rots"], sc["opacity"], colors, deg, cam,
+                                     antialias=aa, box=bx, bg=(0.1, 0.2, 0.3), pick=pick, floor=fl)
+
+    for name, ref, got in golden_case_frames(g, run):
+        assert_frames_close(got, ref, f"oracle vs reference golden [{name}]")
+        # on these frames the restatement reproduces the reference exactly in every
+        # integer artefact and to 1e-5 in colour and transmittance
+        assert helpers.image_diff(got["image"], ref["image"])[0] <= 1e-5, name
+        assert helpers.image_diff(got["final_T"], ref["final_T"])[0] <= 1e-5, name
+        assert got["pairs"] == ref["pairs"], name
+        assert np.array_equal(got["radii"], ref["radii"]), name
+        assert np.array_equal(got["n_contrib"], ref["n_contrib"]), name
+        assert np.array_equal(got["pick"], ref["pick"]), name
+
+
+# -------------------------------------------------------------- the library on the GPU
+def stepped_solver(n=2000, steps=5, seed=3):
+    scen = pkg.scenes.plain_scene_scenario(n, seed, pins=20)
+    s = pkg.bridge.XPBD(helpers.B200_SO)
+    scen.setup(s)
+    scen.advance(s, steps)
+    return s, scen
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("deg,aa", [(-1, False), (3, True), (1, False)])
+def test_render_matches_oracle(deg, aa):
+    s, scen = stepped_solver()
+    try:
+        pos = s.positions()
+        sc, q, _ = s.shapes(1e-2)
+        colors = pkg.splat.synthetic_colors(s.n, deg, 9)
+        s.render_set_colors(colors, deg)
+        s.render_set_options(antialiasing=aa, pick=True)
+        s.render_set_floor(False)
+        for W, H, direction in ((160, 120, (0.3, -1.0, 0.5)), (100, 37, (-1.0, 0.2, -0.3))):
+            cam = Camera.framing(pos, W, H, direction=direction)
+            img, m = s.render(cam, deform_eps=1e-2, bg=(0.1, 0.2, 0.3))
+            ft, nc, pk, radii = s.render_aux(W, H, pick=True)
+            got = {"image": img, "final_T": ft, "n_contrib": nc, "radii": radii, "pairs": m}
+            ref = helpers.oracle_render(pos, sc, q, s_opacity(scen), colors, deg, cam, antialias=aa,
+                                        bg=(0.1, 0.2, 0.3), pick=True)
+            assert_frames_close(got, ref, f"library vs oracle deg={deg} {W}x{H}")
+            assert (pk == ref["pick"]).mean() >= 0.99
+    finally:
+        s.destroy()
+
+
+def s_opacity(scen):
+    return np.asarray(scen.scene["opacity"], np.float32)
+
+
+@pytest.mark.gpu
+def test_render_box_floor_and_rest_shapes():
+    s, scen = stepped_solver(1500, 3, seed=4)
+    try:
+        pos = s.positions()
+        colors = pkg.splat.synthetic_colors(s.n, -1, 2)
+        s.render_set_colors(colors)
+        lo, hi = pos.min(0), pos.max(0)
+        mid = 0.5 * (lo + hi)
+        box = (lo, np.array([mid[0], hi[1], hi[2]], np.float32))
+        s.render_set_options(box=box)
+        s.set_ground(True, (0, 0, 1), float(lo[2]) - 0.05)
+        s.render_set_floor(True, origin=(0, 0, float(lo[2]) - 0.05), checker=0.1, fade_radius=3.0)
+        cam = Camera.framing(pos, 128, 96, direction=(0.3, -1.0, -0.7))
+        img, m = s.render(cam, deform_eps=-1.0, bg=(0.2, 0.2, 0.2))
+        ft, nc, _, radii = s.render_aux(128, 96)
+        got = {"image": img, "final_T": ft, "n_contrib": nc, "radii": radii, "pairs": m}
+        sce = scen.scene
+        ref = helpers.oracle_render(pos, sce["scales"], sce["rots"], sce["opacity"], colors, -1, cam, box=box,
+                                    bg=(0.2, 0.2, 0.2),
+                                    floor=((0, 0, 1), float(lo[2]) - 0.05, (0, 0, float(lo[2]) - 0.05), 0.1, 3.0))
+        assert_frames_close(got, ref, "library vs oracle, box + floor + created shapes")
+        assert (radii[pos[:, 0] > hi[0]] == 0).all()
+    finally:
+        s.destroy()
+
+
+@pytest.mark.gpu
+def test_render_edge_cases():
+    s, scen = stepped_solver(600, 1, seed=6)
+    try:
+        pos = s.positions()
+        s.render_set_colors(pkg.splat.synthetic_colors(s.n, -1, 1))
+        s.render_set_options()
+        s.render_set_floor(False)      # options outlive create, like the solver settings
+        # camera looking away: nothing drawn, the image is the background
+        c = pos.mean(0)
+        cam = Camera.look_at(c + np.array([0, -3, 0]), c + np.array([0, -6, 0]), (0, 0, 1), 40, 30)
+        img, m = s.render(cam, bg=(0.3, 0.4, 0.5))
+        assert m == 0 and np.allclose(img, np.array([0.3, 0.4, 0.5])[:, None, None])
+        # one pixel, and an image narrower than a tile
+        for W, H in ((1, 1), (7, 33)):
+            cam = Camera.framing(pos, W, H)
+            img, m = s.render(cam, deform_eps=-1.0)
+            ref = helpers.oracle_render(pos, scen.scene["scales"], scen.scene["rots"], scen.scene["opacity"],
+                                        pkg.splat.synthetic_colors(s.n, -1, 1), -1, cam)
+            assert abs(m - ref["pairs"]) <= 2
+            assert helpers.image_diff(img, ref["image"])[0] <= MAX_DIFF
+        # invalid camera and missing colours fail loudly
+        with pytest.raises(RuntimeError):
+            s.render(Camera(0, 0, cam.view, cam.proj, cam.campos, 0.5, 0.5))
+    finally:
+        s.destroy()
+
+
+@pytest.mark.gpu
+def test_render_matches_reference_kernels():
+    """The library against the reference's own preprocessCUDA / renderCUDA, live."""
+    if not os.path.isfile(helpers.REF_SO):
+        pytest.skip("reference build absent")
+    lib = ctypes.CDLL(helpers.REF_SO)
+    s, scen = stepped_solver(2500, 4, seed=8)
+    try:
+        pos = s.positions()
+        for deg, aa in ((-1, False), (3, True)):
+            colors = pkg.splat.synthetic_colors(s.n, deg, 3)
+            s.render_set_colors(colors, deg)
+            s.render_set_options(antialiasing=aa)
+            s.render_set_floor(False)
+            cam = Camera.framing(pos, 144, 112, direction=(0.5, -1.0, 0.3))
+            img, m = s.render(cam, deform_eps=-1.0, bg=(0.1, 0.2, 0.3))
+            ft, nc, _, radii = s.render_aux(144, 112)
+            got = {"image": img, "final_T": ft, "n_contrib": nc, "radii": radii, "pairs": m}
+            sce = scen.scene
+            ref = helpers.cpu_render(lib.refshim_render, pos, sce["scales"], sce["rots"], sce["opacity"], colors, deg,
+                                     cam, antialias=aa, bg=(0.1, 0.2, 0.3))
+            assert_frames_close(got, ref, f"library vs reference kernels deg={deg}")
+    finally:
+        s.destroy()
+
+
+@pytest.mark.gpu
+def test_library_matches_reference_golden():
+    g = golden_ref()
+    lib_path = helpers.B200_SO
+
+    def run(sc, colors, deg, cam, aa, bx, pick, fl):
+        s = pkg.bridge.XPBD(lib_path)
+        try:
+            s.set_constraints(distance=False, shape=False, angle=False, volume=False)
+            s.create({**sc, "edges": np.zeros((0, 2), np.int32), "rest": np.zeros(0, np.float32),
+                      "stiff": np.zeros(0, np.float32)})
+            if fl is not None:
+                s.set_ground(True, fl[0], fl[1])
+            s.render_set_colors(colors, deg)
+            s.render_set_options(antialiasing=aa, box=bx, pick=pick)
+            s.render_set_floor(fl is not None, *(fl[2:] if fl is not None else ()))
+            img, m = s.render(cam, deform_eps=-1.0, bg=(0.1, 0.2, 0.3))
+            ft, nc, pk, radii = s.render_aux(cam.width, cam.height, pick=pick)
+            return {"image": img, "final_T": ft, "n_contrib": nc, "radii": radii, "pairs": m,
+                    "pick": pk if pick else None}
+        finally:
+            s.destroy()
+
+    for name, ref, got in golden_case_frames(g, run):
+        assert_frames_close(got, ref, f"library vs reference golden [{name}]")
+        if got["pick"] is not None:
+            assert (got["pick"] == ref["pick"]).mean() >= 0.99
