@@ -190,11 +190,14 @@ public:
 		DBuf<float2> xy;
 		DBuf<float4> conic, rgb;
 		DBuf<int4> rect;
-		DBuf<unsigned int> dkey, dkey_s, tkey, tkey_s;
-		DBuf<int> iota, order, radii, touched, val, val_s, n_contrib, pick;
+		DBuf<unsigned int> dkey, dkey_s;
+		DBuf<unsigned char> tkey, tkey_s;   // tile keys, 16-bit when the tile count allows, else 32-bit
+		DBuf<int> iota, order, radii, touched, val, val_s, n_contrib, pick, torder;
 		DBuf<int2> ranges;
 		DBuf<float> image, final_T, colors, opacity, rest_sc, rest_q;
 		DBuf<long long> cnt, offs;
+		DBuf<unsigned long long> d_total;
+		cudaEvent_t ev_total = nullptr;
 		DBuf<unsigned char> temp;
 		long long* h_total = nullptr;   // pinned: pair count of the frame
 		std::vector<float> h_colors;    // caller order; uploaded on the next frame
@@ -210,12 +213,16 @@ public:
 		void release()
 		{
 			xy.release(); conic.release(); rgb.release(); rect.release(); dkey.release(); dkey_s.release();
-			tkey.release(); tkey_s.release(); iota.release(); order.release(); radii.release(); touched.release();
+			tkey.release(); tkey_s.release(); torder.release();
+			iota.release(); order.release(); radii.release(); touched.release();
 			cnt.release(); offs.release(); val.release(); val_s.release(); n_contrib.release(); pick.release();
 			ranges.release(); image.release(); final_T.release(); colors.release(); opacity.release();
 			rest_sc.release(); rest_q.release(); temp.release();
 			if (h_total) cudaFreeHost(h_total);
 			h_total = nullptr;
+			d_total.release();
+			if (ev_total) cudaEventDestroy(ev_total);
+			ev_total = nullptr;
 			colors_dirty = !h_colors.empty();
 			W = H = 0;
 			pairs = 0;
@@ -1339,6 +1346,36 @@ static void floor_basis(const float n[3], float t1[3], float t2[3])
 	t2[2] = n[0] * y - n[1] * x;
 }
 
+// Pairs of the frame (m > 0) in depth order, stable-sorted by tile key (Key: 16 or
+// 32 bits), then the tile ranges.
+template <typename Key>
+static int render_bin(Engine& E, long long m, int tiles_x, int tiles)
+{
+	auto& R = E.rs;
+	cudaStream_t st = E.stream;
+	const int n = E.n;
+	if (R.tkey.n < sizeof(Key) * (size_t)m || R.val.n < (size_t)m) {
+		const size_t cap = (size_t)m + m / 4;
+		CK(R.tkey.alloc(cap * sizeof(Key))); CK(R.tkey_s.alloc(cap * sizeof(Key)));
+		CK(R.val.alloc(cap)); CK(R.val_s.alloc(cap));
+	}
+	Key* tk = reinterpret_cast<Key*>(R.tkey.p);
+	Key* tks = reinterpret_cast<Key*>(R.tkey_s.p);
+	dev::k_splat_pairs<Key><<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.order.p, R.offs.p, R.rect.p, tiles_x, tk,
+		R.val.p);
+	CK(cudaGetLastError());
+	int bits = 1;
+	while ((1LL << bits) < tiles) ++bits;
+	size_t t3b = 0;
+	CK(cub::DeviceRadixSort::SortPairs(nullptr, t3b, tk, tks, R.val.p, R.val_s.p, (int)m, 0, bits, st));
+	if (R.temp.n < t3b) CK(R.temp.alloc(t3b));
+	CK(cub::DeviceRadixSort::SortPairs(R.temp.p, t3b, tk, tks, R.val.p, R.val_s.p, (int)m, 0, bits, st));
+	dev::k_splat_ranges<Key><<<Engine::blocks_for(tiles), kBlock, 0, st>>>(tiles, (int)m, tks, R.ranges.p);
+	CK(cudaGetLastError());
+	E.launches += 2;
+	return 0;
+}
+
 // One splatted frame of the current positions (Rasterizer::forward,
 // rasterizer_impl.cu:201-470, without the solver step that the reference runs inside
 // its preprocess).  Shapes: the deformed scales / quaternions of xpbd_compute_shapes
@@ -1362,7 +1399,7 @@ static long long render_frame(Engine& E, const float* view, const float* proj, c
 		CK(R.xy.alloc(n)); CK(R.conic.alloc(n)); CK(R.rgb.alloc(n)); CK(R.rect.alloc(n));
 		CK(R.dkey.alloc(n)); CK(R.dkey_s.alloc(n)); CK(R.iota.alloc(n)); CK(R.order.alloc(n));
 		CK(R.radii.alloc(n)); CK(R.touched.alloc(n)); CK(R.cnt.alloc(n)); CK(R.offs.alloc((size_t)n + 1));
-		CK(R.opacity.alloc(n));
+		CK(R.opacity.alloc(n)); CK(R.d_total.alloc(1));
 		CK(cudaMemcpyAsync(R.opacity.p, E.in_opacity.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
 		dev::k_iota<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.iota.p);
 		CK(cudaGetLastError());
@@ -1413,6 +1450,7 @@ static long long render_frame(Engine& E, const float* view, const float* proj, c
 	if (R.W != W || R.H != H) {
 		CK(R.image.alloc(3 * (size_t)W * H)); CK(R.final_T.alloc((size_t)W * H)); CK(R.n_contrib.alloc((size_t)W * H));
 		CK(R.pick.alloc((size_t)W * H)); CK(R.ranges.alloc(tiles));
+		CK(R.torder.alloc(tiles));
 		R.W = W;
 		R.H = H;
 	}
@@ -1464,7 +1502,14 @@ static long long render_frame(Engine& E, const float* view, const float* proj, c
 	CK(cudaGetLastError());
 	seg_end(ST_RENDER_PREPARE, seg);
 	seg = seg_begin();
-	// 2. depth order (stable), tile counts in that order, their prefix sums
+	// 2. the pair count goes to the host while the GPU sorts by depth and scans the
+	// tile counts in that order; the host waits for it only before the pair stage
+	CK(cudaMemsetAsync(R.d_total.p, 0, sizeof(unsigned long long), st));
+	dev::k_splat_total<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.touched.p, R.d_total.p);
+	CK(cudaGetLastError());
+	CK(cudaMemcpyAsync(R.h_total, R.d_total.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
+	if (!R.ev_total) CK(cudaEventCreateWithFlags(&R.ev_total, cudaEventDisableTiming));
+	CK(cudaEventRecord(R.ev_total, st));
 	size_t need = 0, t1b = 0, t2b = 0;
 	CK(cub::DeviceRadixSort::SortPairs(nullptr, t1b, R.dkey.p, R.dkey_s.p, R.iota.p, R.order.p, n, 0, 32, st));
 	CK(cub::DeviceScan::InclusiveSum(nullptr, t2b, R.cnt.p, R.offs.p + 1, n, st));
@@ -1475,38 +1520,26 @@ static long long render_frame(Engine& E, const float* view, const float* proj, c
 	CK(cudaGetLastError());
 	CK(cudaMemsetAsync(R.offs.p, 0, sizeof(long long), st));
 	CK(cub::DeviceScan::InclusiveSum(R.temp.p, t2b, R.cnt.p, R.offs.p + 1, n, st));
-	CK(cudaMemcpyAsync(R.h_total, R.offs.p + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
-	CK(cudaStreamSynchronize(st));
+	E.launches += 3;
+	CK(cudaEventSynchronize(R.ev_total));
 	const long long m = *R.h_total;
 	if (m < 0 || m > INT_MAX) return fail("xpbd_b200_render: %lld tile pairs (limit %d)", m, INT_MAX);
-	E.launches += 2;
-	// 3. (tile, Gaussian) pairs in depth order, stable sort by tile, tile ranges
+	// 3. (tile, Gaussian) pairs in depth order, stable sort by tile, tile ranges, and
+	// the tiles ordered longest list first for the compositing launch
 	CK(cudaMemsetAsync(R.ranges.p, 0, sizeof(int2) * tiles, st));
 	if (m > 0) {
-		if (R.tkey.n < (size_t)m) {
-			const size_t cap = (size_t)m + m / 4;
-			CK(R.tkey.alloc(cap)); CK(R.tkey_s.alloc(cap)); CK(R.val.alloc(cap)); CK(R.val_s.alloc(cap));
-		}
-		dev::k_splat_pairs<<<Engine::blocks_for(n), kBlock, 0, st>>>(n, R.order.p, R.offs.p, R.rect.p, tiles_x,
-			R.tkey.p, R.val.p);
-		CK(cudaGetLastError());
-		int bits = 1;
-		while ((1LL << bits) < tiles) ++bits;
-		size_t t3b = 0;
-		CK(cub::DeviceRadixSort::SortPairs(nullptr, t3b, R.tkey.p, R.tkey_s.p, R.val.p, R.val_s.p, (int)m, 0, bits,
-			st));
-		if (R.temp.n < t3b) CK(R.temp.alloc(t3b));
-		CK(cub::DeviceRadixSort::SortPairs(R.temp.p, t3b, R.tkey.p, R.tkey_s.p, R.val.p, R.val_s.p, (int)m, 0, bits,
-			st));
-		dev::k_splat_ranges<<<(int)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>((int)m, R.tkey_s.p, R.ranges.p);
-		CK(cudaGetLastError());
-		E.launches += 2;
+		const bool narrow = tiles <= 65536;
+		if (narrow ? render_bin<unsigned short>(E, m, tiles_x, tiles) : render_bin<unsigned int>(E, m, tiles_x, tiles))
+			return -1;
 	}
+	dev::k_tile_order<<<1, 1024, 0, st>>>(tiles, R.ranges.p, R.torder.p);
+	CK(cudaGetLastError());
+	++E.launches;
 	seg_end(ST_RENDER_SORT, seg);
 	seg = seg_begin();
 	// 4. composite every tile
 	if (R.pick_on) CK(cudaMemsetAsync(R.pick.p, 0xff, sizeof(int) * (size_t)W * H, st));
-	dev::k_splat_tiles<<<dim3(tiles_x, tiles_y), dev::kTilePix, 0, st>>>(F, R.ranges.p, R.val_s.p, R.xy.p,
+	dev::k_splat_tiles<<<tiles, dev::kTileThreads, 0, st>>>(F, R.torder.p, R.ranges.p, R.val_s.p, R.xy.p,
 		R.conic.p, R.rgb.p, R.image.p, R.final_T.p, R.n_contrib.p, R.pick.p);
 	CK(cudaGetLastError());
 	++E.launches;

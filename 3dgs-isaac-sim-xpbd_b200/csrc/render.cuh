@@ -177,7 +177,24 @@ __global__ void __launch_bounds__(kBlock) k_splat_prepare(int n, RenderFrame F, 
 		float dx = p.x - F.campos[0], dy = p.y - F.campos[1], dz = p.z - F.campos[2];
 		const float len = sqrtf(dx * dx + dy * dy + dz * dz);
 		dx /= len; dy /= len; dz /= len;
-		col = sh_color(F.sh_deg, colors + (size_t)3 * F.sh_coeffs * i, make_float3(dx, dy, dz));
+		const float* src = colors + (size_t)3 * F.sh_coeffs * i;
+		float c[48];
+		if (F.sh_deg == 3 || F.sh_deg == 1) {
+			// 192 or 48 bytes per Gaussian: 16-byte aligned rows, read as float4
+			const float4* s4 = reinterpret_cast<const float4*>(src);
+			const int n4 = F.sh_deg == 3 ? 12 : 3;
+#pragma unroll
+			for (int k = 0; k < 12; ++k)
+				if (k < n4) {
+					const float4 v = __ldg(s4 + k);
+					c[4 * k] = v.x; c[4 * k + 1] = v.y; c[4 * k + 2] = v.z; c[4 * k + 3] = v.w;
+				}
+		} else {
+#pragma unroll
+			for (int k = 0; k < 27; ++k)
+				if (k < 3 * F.sh_coeffs) c[k] = __ldg(src + k);
+		}
+		col = sh_color(F.sh_deg, c, make_float3(dx, dy, dz));
 	} else {
 		col = make_float3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]);
 	}
@@ -188,6 +205,23 @@ __global__ void __launch_bounds__(kBlock) k_splat_prepare(int n, RenderFrame F, 
 	radii[i] = radius;
 	rect[i] = make_int4(x0, y0, x1, y1);
 	touched[i] = cnt;
+}
+
+// total tiles touched (the pair count), accumulated into *total (zeroed before)
+__global__ void __launch_bounds__(kBlock) k_splat_total(int n, const int* __restrict__ touched,
+	unsigned long long* __restrict__ total)
+{
+	__shared__ unsigned long long s_part[kBlock / 32];
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long v = i < n ? (unsigned long long)touched[i] : 0ull;
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		unsigned long long t = 0;
+		for (int w = 0; w < kBlock / 32; ++w) t += s_part[w];
+		if (t) atomicAdd(total, t);
+	}
 }
 
 __global__ void __launch_bounds__(kBlock) k_iota(int n, int* __restrict__ a)
@@ -204,94 +238,148 @@ __global__ void __launch_bounds__(kBlock) k_splat_counts(int n, const int* __res
 	if (k < n) cnt[k] = touched[order[k]];
 }
 
-// one (tile, Gaussian) pair per touched tile, Gaussians in depth order
+// One (tile, Gaussian) pair per touched tile, Gaussians in depth order, tiles of a
+// Gaussian row by row.  A warp takes 32 consecutive Gaussians of the depth order and
+// writes their pairs together, lane j the j-th pair of each 32, so that the stores of
+// a warp are consecutive; each lane finds the Gaussian owning its pair by a binary
+// search over the warp's prefix offsets (shuffles).
+template <typename Key>
 __global__ void __launch_bounds__(kBlock) k_splat_pairs(int n, const int* __restrict__ order,
-	const long long* __restrict__ offs, const int4* __restrict__ rect, int tiles_x, unsigned int* __restrict__ tkey,
+	const long long* __restrict__ offs, const int4* __restrict__ rect, int tiles_x, Key* __restrict__ tkey,
 	int* __restrict__ val)
 {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= n) return;
-	long long at = offs[k];
-	if (offs[k + 1] == at) return;
-	const int g = order[k];
-	const int4 r = rect[g];
-	for (int y = r.y; y < r.w; ++y)
-		for (int x = r.x; x < r.z; ++x) {
-			tkey[at] = (unsigned int)(y * tiles_x + x);
-			val[at] = g;
-			++at;
+	const int lane = threadIdx.x & 31;
+	if (k - lane >= n) return;                       // whole warp past the end
+	const long long s0 = offs[min(k, n)];
+	const long long e0 = k < n ? offs[k + 1] : s0;
+	int g = 0;
+	int4 r = make_int4(0, 0, 1, 1);
+	if (e0 > s0) {
+		g = order[k];
+		r = rect[g];
+	}
+	const long long base = __shfl_sync(0xffffffffu, s0, 0);
+	const long long total = __shfl_sync(0xffffffffu, e0, 31) - base;
+	const int loc = (int)(s0 - base);                // this lane's first pair within the warp's run
+	for (long long p0 = 0; p0 < total; p0 += 32) {
+		const int p = (int)p0 + lane;
+		int owner = 0;                               // largest lane whose run starts at or before p
+		for (int step = 16; step > 0; step >>= 1) {
+			const int cand = owner + step;
+			const int lc = __shfl_sync(0xffffffffu, loc, cand & 31);
+			if (cand < 32 && lc <= p) owner = cand;
 		}
+		const int o_loc = __shfl_sync(0xffffffffu, loc, owner);
+		const int o_g = __shfl_sync(0xffffffffu, g, owner);
+		const int o_x0 = __shfl_sync(0xffffffffu, r.x, owner);
+		const int o_y0 = __shfl_sync(0xffffffffu, r.y, owner);
+		const int o_x1 = __shfl_sync(0xffffffffu, r.z, owner);
+		if (p < total) {
+			const int li = p - o_loc, w = o_x1 - o_x0;
+			const int y = o_y0 + li / w, x = o_x0 + li % w;
+			tkey[base + p] = (Key)(y * tiles_x + x);
+			val[base + p] = o_g;
+		}
+	}
 }
 
-// [start, end) of every tile in the sorted pair list (ranges zeroed before)
-__global__ void __launch_bounds__(kBlock) k_splat_ranges(int m, const unsigned int* __restrict__ tkey,
+// [start, end) of every tile in the sorted pair list: two lower-bound searches per tile
+template <typename Key>
+__global__ void __launch_bounds__(kBlock) k_splat_ranges(int tiles, int m, const Key* __restrict__ tkey,
 	int2* __restrict__ ranges)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= m) return;
-	const unsigned int tile = tkey[t];
-	if (t == 0 || tkey[t - 1] != tile) ranges[tile].x = t;
-	if (t == m - 1 || tkey[t + 1] != tile) ranges[tile].y = t + 1;
+	if (t >= tiles) return;
+	int bounds[2];
+	for (int h = 0; h < 2; ++h) {
+		const unsigned int want = (unsigned int)(t + h);
+		int lo = 0, hi = m;
+		while (lo < hi) {
+			const int mid = (lo + hi) >> 1;
+			if ((unsigned int)tkey[mid] < want) lo = mid + 1;
+			else hi = mid;
+		}
+		bounds[h] = lo;
+	}
+	ranges[t] = make_int2(bounds[0], bounds[1]);
 }
 
-// One block per 16x16 tile, one thread per pixel.
-__global__ void __launch_bounds__(kTilePix) k_splat_tiles(RenderFrame F, const int2* __restrict__ ranges,
-	const int* __restrict__ val, const float2* __restrict__ xy, const float4* __restrict__ conic_op,
-	const float4* __restrict__ rgb, float* __restrict__ out, float* __restrict__ final_T,
-	int* __restrict__ n_contrib, int* __restrict__ pick)
+// Launch order of the compositing blocks: tiles by list length, longest first, in
+// power-of-two classes (the order inside a class is free: it changes no result).
+// One block.
+__global__ void __launch_bounds__(1024) k_tile_order(int tiles, const int2* __restrict__ ranges,
+	int* __restrict__ order)
 {
-	__shared__ int s_id[kTilePix];
-	__shared__ float2 s_xy[kTilePix];
-	__shared__ float4 s_co[kTilePix];
-	const int tile = blockIdx.y * F.tiles_x + blockIdx.x;
-	const int pxi = blockIdx.x * kTile + (int)threadIdx.x % kTile;
-	const int pyi = blockIdx.y * kTile + (int)threadIdx.x / kTile;
-	const bool inside = pxi < F.W && pyi < F.H;
-	const float fx = (float)pxi, fy = (float)pyi;
-	const int2 r = ranges[tile];
-	float T = 1.0f;
-	float cr = 0.0f, cg = 0.0f, cbl = 0.0f;
-	int contributor = 0, last = 0, picked = -1;
-	bool done = !inside;
-	int todo = r.y - r.x;
-	for (int base = r.x; base < r.y; base += kTilePix, todo -= kTilePix) {
-		if (__syncthreads_count(done) == kTilePix) break;
-		const int k = base + (int)threadIdx.x;
-		if (k < r.y) {
-			const int g = val[k];
-			s_id[threadIdx.x] = g;
-			s_xy[threadIdx.x] = xy[g];
-			s_co[threadIdx.x] = conic_op[g];
-		}
-		__syncthreads();
-		const int cnt = min(kTilePix, todo);
-		for (int j = 0; !done && j < cnt; ++j) {
-			++contributor;
-			const float2 c = s_xy[j];
-			const float4 co = s_co[j];
-			const float dx = c.x - fx, dy = c.y - fy;
-			const float power = -0.5f * (co.x * dx * dx + co.z * dy * dy) - co.y * dx * dy;
-			if (power > 0.0f) continue;
-			const float alpha = fminf(0.99f, co.w * expf(power));
-			if (alpha < 1.0f / 255.0f) continue;
-			if (F.pick && picked == -1 && alpha > 0.1f) picked = s_id[j];
-			const float tn = T * (1.0f - alpha);
-			if (tn < 0.0001f) { done = true; continue; }
-			const float4 col = rgb[s_id[j]];
-			const float w = alpha * T;
-			cr += col.x * w;
-			cg += col.y * w;
-			cbl += col.z * w;
-			T = tn;
-			last = contributor;
+	__shared__ int s_count[33], s_start[33];
+	if (threadIdx.x < 33) s_count[threadIdx.x] = 0;
+	__syncthreads();
+	for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+		const int2 r = ranges[t];
+		const int len = r.y - r.x;
+		atomicAdd(&s_count[len > 0 ? 32 - __clz(len) : 0], 1);
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		int at = 0;
+		for (int c = 32; c >= 0; --c) {
+			s_start[c] = at;
+			at += s_count[c];
 		}
 	}
-	if (!inside) return;
-	const size_t pix = (size_t)pyi * F.W + pxi, plane = (size_t)F.W * F.H;
-	final_T[pix] = T;
-	n_contrib[pix] = last;
+	__syncthreads();
+	for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+		const int2 r = ranges[t];
+		const int len = r.y - r.x;
+		order[atomicAdd(&s_start[len > 0 ? 32 - __clz(len) : 0], 1)] = t;
+	}
+}
+
+// True unless the Gaussian (centre c, conic co.xyz, opacity co.w) stays below alpha
+// 1/255 at every pixel centre of [x0, x1] x [y0, y1]: the minimum of the quadratic form
+// over the rectangle (a continuous bound, so no larger than at the pixel centres),
+// compared with 2 ln(255 o) plus a margin far above FP32 rounding.  Indefinite conics
+// are always kept.
+__device__ __forceinline__ bool splat_reaches(float2 c, float4 co, float x0, float x1, float y0, float y1)
+{
+	const float a = co.x, b = co.y, cc = co.z, o = co.w;
+	if (o < 1.0f / 255.0f) return false;             // alpha <= o everywhere
+	if (!(a > 0.0f && cc > 0.0f && a * cc - b * b > 0.0f)) return true;
+	if (c.x >= x0 && c.x <= x1 && c.y >= y0 && c.y <= y1) return true;
+	const float t = 2.0f * logf(255.0f * o) * 1.002f + 0.02f;
+	float qmin = FLT_MAX;
+	// edges x = x0, x1 (d = centre - pixel, dy over [c.y - y1, c.y - y0])
+	for (int e = 0; e < 2; ++e) {
+		const float dx = c.x - (e ? x1 : x0);
+		const float dy = fminf(c.y - y0, fmaxf(c.y - y1, -b * dx / cc));
+		qmin = fminf(qmin, a * dx * dx + 2.0f * b * dx * dy + cc * dy * dy);
+	}
+	for (int e = 0; e < 2; ++e) {
+		const float dy = c.y - (e ? y1 : y0);
+		const float dx = fminf(c.x - x0, fmaxf(c.x - x1, -b * dy / a));
+		qmin = fminf(qmin, a * dx * dx + 2.0f * b * dx * dy + cc * dy * dy);
+	}
+	return qmin <= t;
+}
+
+// Front-to-back state of one pixel (renderCUDA's per-thread registers).
+struct PixelAcc {
+	float T = 1.0f, r = 0.0f, g = 0.0f, b = 0.0f;
+	int last = 0, picked = -1;
+	bool done = false;
+};
+
+// Writes one pixel: colour over the background (or the checker floor where it shows),
+// transmittance, contributor count and picked Gaussian.
+__device__ __forceinline__ void splat_finish(const RenderFrame& F, int px, int py, const PixelAcc& P,
+	float* __restrict__ out, float* __restrict__ final_T, int* __restrict__ n_contrib, int* __restrict__ pick)
+{
+	const size_t pix = (size_t)py * F.W + px, plane = (size_t)F.W * F.H;
+	const float fx = (float)px, fy = (float)py;
+	final_T[pix] = P.T;
+	n_contrib[pix] = P.last;
 	float bgc[3] = { F.bg[0], F.bg[1], F.bg[2] };
-	if (F.floor_on && T > (1.0f / 255.0f) && F.fl_camh > 0.0f) {
+	if (F.floor_on && P.T > (1.0f / 255.0f) && F.fl_camh > 0.0f) {
 		// ray through the pixel against the ground plane; checker cells faded with distance
 		const float ndcx = (2.0f * fx + 1.0f) / (float)F.W - 1.0f;
 		const float ndcy = (2.0f * fy + 1.0f) / (float)F.H - 1.0f;
@@ -317,10 +405,163 @@ __global__ void __launch_bounds__(kTilePix) k_splat_tiles(RenderFrame F, const i
 			}
 		}
 	}
-	out[pix] = cr + T * bgc[0];
-	out[plane + pix] = cg + T * bgc[1];
-	out[2 * plane + pix] = cbl + T * bgc[2];
-	if (F.pick && picked != -1) pick[pix] = picked;
+	out[pix] = P.r + P.T * bgc[0];
+	out[plane + pix] = P.g + P.T * bgc[1];
+	out[2 * plane + pix] = P.b + P.T * bgc[2];
+	if (F.pick && P.picked != -1) pick[pix] = P.picked;
+}
+
+// One block of 128 threads per 16x16 tile, tiles launched longest list first
+// (tile_order): warp w owns the 8x8 quadrant (w % 2, w / 2), each lane two horizontally
+// adjacent pixels of it, and the four warps run without block barriers (their reads of
+// the tile's list meet in the SM's L1).  A warp walks the tile's list 64 entries a step,
+// two per lane, software-pipelined: the list indices of step s + 2 and the centre,
+// conic and colour of step s + 1 are in flight while step s is tested and blended, so
+// the dependent index -> Gaussian gathers of a long list do not serialise.  Each entry
+// is tested against the quadrant (splat_reaches); survivors are packed into the warp's
+// shared-memory slots with their list position and the pixels visit them in list
+// order, two Gaussians per iteration (their alphas are independent of T).  A Gaussian
+// left out would have been skipped at each of the quadrant's pixels and the position
+// is carried along, so colour, transmittance, contributor count and pick equal those
+// of the full list.
+constexpr int kTileThreads = 128;
+constexpr int kSpan = 64;
+
+struct SplatEntry {
+	int g;
+	float2 c;
+	float4 co, col;
+};
+
+__device__ __forceinline__ void splat_fetch(SplatEntry& e, int g, const float2* __restrict__ xy,
+	const float4* __restrict__ conic_op, const float4* __restrict__ rgb)
+{
+	e.g = g;
+	e.c = xy[g];
+	e.co = conic_op[g];
+	e.col = rgb[g];
+}
+
+// alpha of a Gaussian at a pixel, or 0 where renderCUDA skips it (power > 0 or
+// alpha < 1/255)
+__device__ __forceinline__ float splat_alpha(float fx, float fy, float2 c, float4 co)
+{
+	const float dx = c.x - fx, dy = c.y - fy;
+	const float power = -0.5f * (co.x * dx * dx + co.z * dy * dy) - co.y * dx * dy;
+	if (power > 0.0f) return 0.0f;
+	const float alpha = fminf(0.99f, co.w * expf(power));
+	return alpha < 1.0f / 255.0f ? 0.0f : alpha;
+}
+
+// Front-to-back step of one pixel over one Gaussian (renderCUDA's inner loop): stop
+// before T drops below 1e-4, otherwise accumulate colour and record the contributor's
+// list position.
+__device__ __forceinline__ void splat_apply(PixelAcc& P, float alpha, float4 col, int id, int rank, bool pick_on)
+{
+	if (P.done || alpha == 0.0f) return;
+	if (pick_on && P.picked == -1 && alpha > 0.1f) P.picked = id;
+	const float tn = P.T * (1.0f - alpha);
+	if (tn < 0.0001f) { P.done = true; return; }
+	const float w = alpha * P.T;
+	P.r += col.x * w;
+	P.g += col.y * w;
+	P.b += col.z * w;
+	P.T = tn;
+	P.last = rank + 1;
+}
+
+__global__ void __launch_bounds__(kTileThreads) k_splat_tiles(RenderFrame F, const int* __restrict__ tile_order,
+	const int2* __restrict__ ranges, const int* __restrict__ val, const float2* __restrict__ xy,
+	const float4* __restrict__ conic_op, const float4* __restrict__ rgb, float* __restrict__ out,
+	float* __restrict__ final_T, int* __restrict__ n_contrib, int* __restrict__ pick)
+{
+	constexpr int kWarps = kTileThreads / 32;
+	__shared__ float4 s_co[kWarps][kSpan], s_rgb[kWarps][kSpan];
+	__shared__ float2 s_xy[kWarps][kSpan];
+	__shared__ int s_id[kWarps][kSpan], s_rank[kWarps][kSpan];
+	const int tile = tile_order[blockIdx.x];
+	const int bx = tile % F.tiles_x, by = tile / F.tiles_x;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int qx = bx * kTile + (warp & 1) * 8, qy = by * kTile + (warp >> 1) * 8;
+	const int qx1 = min(qx + 7, F.W - 1), qy1 = min(qy + 7, F.H - 1);
+	const int px = qx + (lane & 3) * 2, py = qy + (lane >> 2);
+	const bool in0 = px < F.W && py < F.H, in1 = px + 1 < F.W && py < F.H;
+	const float fx0 = (float)px, fx1 = (float)(px + 1), fy = (float)py;
+	const float rx0 = (float)qx, rx1 = (float)qx1, ry0 = (float)qy, ry1 = (float)qy1;
+	const bool pick_on = F.pick != 0;
+	PixelAcc A, B;
+	A.done = !in0;
+	B.done = !in1;
+	if (qx <= qx1 && qy <= qy1) {
+		const int2 r = ranges[tile];
+		SplatEntry cur[2], nxt[2];
+		int nv[2];
+		// prologue: step 0 gathered, step 1 indices loaded
+#pragma unroll
+		for (int e = 0; e < 2; ++e) {
+			const int k = r.x + lane + 32 * e;
+			cur[e].g = -1;
+			if (k < r.y) splat_fetch(cur[e], val[k], xy, conic_op, rgb);
+			nv[e] = k + kSpan < r.y ? val[k + kSpan] : -1;
+		}
+		for (int base = r.x; base < r.y; base += kSpan) {
+			if (__all_sync(0xffffffffu, A.done && B.done)) break;
+			// in flight: gathers of step + 1, indices of step + 2
+#pragma unroll
+			for (int e = 0; e < 2; ++e) {
+				nxt[e].g = -1;
+				if (nv[e] >= 0) splat_fetch(nxt[e], nv[e], xy, conic_op, rgb);
+				const int k2 = base + lane + 32 * e + 2 * kSpan;
+				nv[e] = k2 < r.y ? val[k2] : -1;
+			}
+			bool keep[2];
+#pragma unroll
+			for (int e = 0; e < 2; ++e)
+				keep[e] = cur[e].g >= 0 && splat_reaches(cur[e].c, cur[e].co, rx0, rx1, ry0, ry1);
+			const unsigned b0 = __ballot_sync(0xffffffffu, keep[0]);
+			const unsigned b1 = __ballot_sync(0xffffffffu, keep[1]);
+			const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+			for (int e = 0; e < 2; ++e)
+				if (keep[e]) {
+					const int at = e == 0 ? __popc(b0 & lt) : __popc(b0) + __popc(b1 & lt);
+					s_xy[warp][at] = cur[e].c;
+					s_co[warp][at] = cur[e].co;
+					s_rgb[warp][at] = cur[e].col;
+					s_id[warp][at] = cur[e].g;
+					s_rank[warp][at] = base - r.x + lane + 32 * e;
+				}
+			__syncwarp();
+			const int kept = __popc(b0) + __popc(b1);
+			int j = 0;
+			for (; j + 1 < kept && !(A.done && B.done); j += 2) {
+				const float2 c0 = s_xy[warp][j], c1 = s_xy[warp][j + 1];
+				const float4 q0 = s_co[warp][j], q1 = s_co[warp][j + 1];
+				const float a0 = splat_alpha(fx0, fy, c0, q0), b0a = splat_alpha(fx1, fy, c0, q0);
+				const float a1 = splat_alpha(fx0, fy, c1, q1), b1a = splat_alpha(fx1, fy, c1, q1);
+				const float4 col0 = s_rgb[warp][j], col1 = s_rgb[warp][j + 1];
+				const int id0 = s_id[warp][j], id1 = s_id[warp][j + 1];
+				const int rk0 = s_rank[warp][j], rk1 = s_rank[warp][j + 1];
+				splat_apply(A, a0, col0, id0, rk0, pick_on);
+				splat_apply(B, b0a, col0, id0, rk0, pick_on);
+				splat_apply(A, a1, col1, id1, rk1, pick_on);
+				splat_apply(B, b1a, col1, id1, rk1, pick_on);
+			}
+			if (j < kept && !(A.done && B.done)) {
+				const float2 c0 = s_xy[warp][j];
+				const float4 q0 = s_co[warp][j];
+				const float4 col0 = s_rgb[warp][j];
+				const int id0 = s_id[warp][j], rk0 = s_rank[warp][j];
+				splat_apply(A, splat_alpha(fx0, fy, c0, q0), col0, id0, rk0, pick_on);
+				splat_apply(B, splat_alpha(fx1, fy, c0, q0), col0, id0, rk0, pick_on);
+			}
+			__syncwarp();
+#pragma unroll
+			for (int e = 0; e < 2; ++e) cur[e] = nxt[e];
+		}
+	}
+	if (in0) splat_finish(F, px, py, A, out, final_T, n_contrib, pick);
+	if (in1) splat_finish(F, px + 1, py, B, out, final_T, n_contrib, pick);
 }
 
 }  // namespace dev

@@ -6,7 +6,7 @@ capsule grippers pulling apart while twisting; one bench "step" is one 60 Hz fra
 10 solver substeps x 4 iterations.  Metric: Gaussian-substeps per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config large|plain|batched|served|chainmail|dense]
+                  [--config large|plain|batched|served|chainmail|dense|render]
                   [--gaussians N]
 
 value     device-resident throughput: frames enqueued through the library's async API
@@ -92,14 +92,17 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.first = threading.Event()
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
+            self.first.wait(3.0)      # sampling is running before the timed region starts
         except OSError:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
 
     def stop(self):
         if not self.proc:
@@ -511,6 +514,151 @@ def bench_chainmail(args, rank, world):
     return line
 
 
+RENDER_W, RENDER_H, RENDER_SH = 1920, 1080, 3
+
+
+def render_inputs(n):
+    """The splatting workload: the large scene after 5 solver frames (grippers pulling
+    and twisting), SH degree-3 colours, a camera framing the object at 1920x1080."""
+    scen = scenes.large_scene_scenario(n, 0)
+    colors = pkg.splat.synthetic_colors(n, RENDER_SH, 1)
+    return scen, colors
+
+
+def oracle_render_fn():
+    lib_path = os.path.join(ROOT, "oracle", "liboracle.so")
+    if not os.path.isfile(lib_path):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    f = ctypes.CDLL(lib_path).oracle_render
+    P = ctypes.c_void_p
+    f.argtypes = ([ctypes.c_int] + [P] * 5 + [ctypes.c_int] + [P] * 3 + [ctypes.c_int, ctypes.c_int]
+                  + [ctypes.c_float] * 3 + [ctypes.c_int] + [P] * 3 + [ctypes.c_int] + [P] * 6)
+    f.restype = ctypes.c_longlong
+    return f
+
+
+def oracle_render_sample(pos, sc, q, op, colors, cam):
+    """One frame of the CPU restatement (single thread); returns seconds."""
+    f = oracle_render_fn()
+    a = [np.ascontiguousarray(v, dtype=np.float32) for v in (pos, sc, q, op, colors)]
+    out = np.empty((3, cam.height, cam.width), np.float32)
+    t0 = time.perf_counter()
+    f(len(pos), *[v.ctypes.data for v in a], RENDER_SH, cam.view.ctypes.data, cam.proj.ctypes.data,
+      cam.campos.ctypes.data, cam.width, cam.height, cam.tan_fovx, cam.tan_fovy, 1.0, 0, None, None, None, 0, None,
+      out.ctypes.data, None, None, None, None)
+    return time.perf_counter() - t0
+
+
+def bench_render(args, rank, world):
+    """Splatting (xpbd_b200_render): one step = one 1920x1080 frame of the deformed
+    Gaussians (1-ring deformation fit, EWA projection, depth + tile binning, tile
+    compositing), image left in device memory."""
+    import torch
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    n = args.gaussians or 1_000_000
+    scen, colors = render_inputs(n)
+    x = pkg.XPBD()
+    bind_ext(x.lib)
+    L = x.lib
+    stream = torch.cuda.Stream()
+    L.xpbd_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    scen.setup(x)
+    scen.advance(x, 5)
+    pos = x.positions()
+    x.render_set_colors(colors, RENDER_SH)
+    x.render_set_options()
+    x.render_set_floor(False)
+    cam = pkg.splat.Camera.framing(pos, RENDER_W, RENDER_H)
+    eps = 1e-2
+    for _ in range(args.warmup):
+        x.render(cam, deform_eps=eps, to_host=False)
+    launches0 = L.xpbd_b200_launch_count()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        _, pairs = x.render(cam, deform_eps=eps, to_host=False)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = L.xpbd_b200_launch_count() - launches0
+    # stage times: the same frames with an event pair around each stage
+    L.xpbd_b200_set_profiling(1)
+    L.xpbd_b200_reset_stage_times()
+    for _ in range(args.steps):
+        x.render(cam, deform_eps=eps, to_host=False)
+    st_ms, st_cnt = np.zeros(16), np.zeros(16, np.int64)
+    k = L.xpbd_b200_stage_times(st_ms.ctypes.data, st_cnt.ctypes.data, 16)
+    stages = {L.xpbd_b200_stage_name(i).decode(): st_ms[i] / args.steps for i in range(k) if st_cnt[i]}
+    L.xpbd_b200_set_profiling(0)
+    visible = int((x.render_aux(RENDER_W, RENDER_H)[3] > 0).sum())
+    # the tile compositing kernel: per launch it reads each pair's index, centre, conic
+    # and colour (4 + 8 + 16 + 16 B) and the tile ranges, and writes 3 colour planes,
+    # transmittance and contributor count per pixel (20 B)
+    npix = RENDER_W * RENDER_H
+    tiles_bytes = pairs * 44 + npix * 20 + 8 * ((RENDER_W + 15) // 16) * ((RENDER_H + 15) // 16)
+    tiles_ms = stages.get("render_tiles", float("nan"))
+    peak, peak_kind = peaks()
+    achieved = tiles_bytes / (tiles_ms / 1e3) / 1e9
+    # e2e: blocking C ABI, the image read back to host memory every frame
+    L.xpbd_b200_set_stream(None)
+    e2e_steps = min(args.steps, 10)
+    x.render(cam, deform_eps=eps, to_host=True)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        x.render(cam, deform_eps=eps, to_host=True)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    sc, q, _ = x.shapes(eps)
+    op = np.asarray(scen.scene["opacity"], np.float32)
+    x.destroy()
+    unit = "frames/s"
+    line = {
+        "metric": "splatted frames/s of 1M deformed Gaussians at 1920x1080 (SH degree 3)", "value": 1e3 / ms,
+        "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid scene after 5 solver frames, seeded SH coefficients)",
+        "config": {"workload": f"render: {n} Gaussians, {RENDER_W}x{RENDER_H}, SH degree {RENDER_SH}, "
+                               f"deformed shapes (deform_eps {eps})",
+                   "n_gaussians": n, "visible": visible, "pairs": int(pairs),
+                   "l2": "inputs larger than L2 (1M Gaussians x 300 B + 13M pairs)"},
+        "stages_ms": stages,
+        "e2e": {"value": 1.0 / e2e_s, "unit": unit, "h2d_bytes_per_step": 4 * 35,
+                "d2h_bytes_per_step": 12 * npix, "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "splat_tiles", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": tiles_bytes, "mean_launch_ms": tiles_ms,
+                     "note": "compositing is bound by the per pixel-Gaussian exp/FMA work, not by DRAM"},
+        "clocks": clk,
+    }
+    ref_so = os.path.join(ROOT, "oracle", "_ref", "libxpbd_ref.so")
+    if os.path.isfile(ref_so):
+        f = ctypes.CDLL(ref_so).refshim_render_timed
+        P = ctypes.c_void_p
+        f.argtypes = ([ctypes.c_int] + [P] * 5 + [ctypes.c_int] + [P] * 3 + [ctypes.c_int, ctypes.c_int]
+                      + [ctypes.c_float] * 2 + [ctypes.c_int, P])
+        f.restype = ctypes.c_longlong
+        out = ctypes.c_float(0.0)
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (pos, sc, q, op, colors)]
+        m_ref = f(n, *[v.ctypes.data for v in a], RENDER_SH, cam.view.ctypes.data, cam.proj.ctypes.data,
+                  cam.campos.ctypes.data, RENDER_W, RENDER_H, cam.tan_fovx, cam.tan_fovy, args.steps,
+                  ctypes.byref(out))
+        line["reference_gpu"] = {"ms_per_frame": out.value, "pairs": int(m_ref), "speedup": out.value / ms,
+                                 "form": "the reference's preprocessCUDA + renderCUDA with cub scan / radix sort "
+                                         "binning on the same inputs (shapes given, no physics)"}
+    if not args.no_cpu_baseline:
+        cs = pkg.splat.Camera.framing(pos, RENDER_W // 4, RENDER_H // 4)
+        dt = oracle_render_sample(pos, sc, q, op, colors, cs)
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": unit, "cores": 1, "kind": "port",
+                                "sample": f"one {cs.width}x{cs.height} frame of the same {n} Gaussians "
+                                          "(a quarter of the width and height)"}
+    return line
+
+
 def bench_served(args, rank, world):
     """Poisson session arrivals served with continuous batching, against one session at a
     time.  Arrival rate and sizes are scaled to what the host-side topology build admits
@@ -540,6 +688,8 @@ def bench_served(args, rank, world):
 def bench_reference(args, rank, world):
     if rank != 0:
         return None
+    if args.config == "render":
+        return bench_reference_render(args)
     name, make = workload(args.config, args.gaussians)
     steps = args.steps
     warm = args.warmup
@@ -566,13 +716,34 @@ def bench_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def bench_reference_render(args):
+    """CPU arm of the render config: the restatement (the reference has no CPU
+    rasteriser), one 480x270 frame of the same Gaussians per step."""
+    n = args.gaussians or 1_000_000
+    scen, colors = render_inputs(n)
+    sc = scen.scene
+    cam = pkg.splat.Camera.framing(sc["pos"], RENDER_W // 4, RENDER_H // 4)
+    steps = max(1, min(args.steps, 3))
+    total = sum(oracle_render_sample(sc["pos"], sc["scales"], sc["rots"], sc["opacity"], colors, cam)
+                for _ in range(steps))
+    value = steps / total
+    return {"impl": "reference", "metric": "splatted frames/s of 1M deformed Gaussians at 1920x1080 (SH degree 3)",
+            "value": value, "unit": "frames/s", "n_gpus": 1, "steps": steps, "warmup": 0,
+            "ms_per_step": total / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded ellipsoid scene, created shapes)",
+            "config": {"workload": f"render: {n} Gaussians, {cam.width}x{cam.height} CPU sample"},
+            "cpu_baseline": {"value": value, "unit": "frames/s", "cores": 1, "kind": "port",
+                             "sample": f"{steps} frames at {cam.width}x{cam.height}"},
+            "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail", "dense"])
+    ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail", "dense", "render"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gaussians", type=int, default=None,
@@ -598,6 +769,8 @@ def main():
             line = bench_served(args, rank, world)
         elif args.config == "chainmail":
             line = bench_chainmail(args, rank, world)
+        elif args.config == "render":
+            line = bench_render(args, rank, world)
         else:
             line = bench_b200(args, rank, world)
         if line is not None:

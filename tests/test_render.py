@@ -258,6 +258,7 @@ def test_library_matches_reference_golden():
             s.set_constraints(distance=False, shape=False, angle=False, volume=False)
             s.create({**sc, "edges": np.zeros((0, 2), np.int32), "rest": np.zeros(0, np.float32),
                       "stiff": np.zeros(0, np.float32)})
+            s.step()                   # no constraints, no velocity: positions stay as created
             if fl is not None:
                 s.set_ground(True, fl[0], fl[1])
             s.render_set_colors(colors, deg)
