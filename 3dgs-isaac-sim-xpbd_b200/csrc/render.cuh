@@ -411,20 +411,20 @@ __device__ __forceinline__ void splat_finish(const RenderFrame& F, int px, int p
 	if (F.pick && P.picked != -1) pick[pix] = P.picked;
 }
 
-// One block of 128 threads per 16x16 tile, tiles launched longest list first
-// (tile_order): warp w owns the 8x8 quadrant (w % 2, w / 2), each lane two horizontally
-// adjacent pixels of it, and the four warps run without block barriers (their reads of
-// the tile's list meet in the SM's L1).  A warp walks the tile's list 64 entries a step,
-// two per lane, software-pipelined: the list indices of step s + 2 and the centre,
-// conic and colour of step s + 1 are in flight while step s is tested and blended, so
-// the dependent index -> Gaussian gathers of a long list do not serialise.  Each entry
-// is tested against the quadrant (splat_reaches); survivors are packed into the warp's
+// One block of 256 threads per 16x16 tile, tiles launched longest list first
+// (tile_order): warp w owns the 8x4 region ((w % 2) * 8, (w / 2) * 4), one pixel per
+// lane, and the eight warps run without block barriers (their reads of the tile's list
+// meet in the SM's L1).  A warp walks the tile's list 64 entries a step, two per lane,
+// software-pipelined: the list indices of step s + 2 and the centre, conic and colour
+// of step s + 1 are in flight while step s is tested and blended, so the dependent
+// index -> Gaussian gathers of a long list do not serialise.  Each entry is tested
+// against the warp's region (splat_reaches); survivors are packed into the warp's
 // shared-memory slots with their list position and the pixels visit them in list
 // order, two Gaussians per iteration (their alphas are independent of T).  A Gaussian
-// left out would have been skipped at each of the quadrant's pixels and the position
-// is carried along, so colour, transmittance, contributor count and pick equal those
-// of the full list.
-constexpr int kTileThreads = 128;
+// left out would have been skipped at each of the region's pixels and the position is
+// carried along, so colour, transmittance, contributor count and pick equal those of
+// the full list.
+constexpr int kTileThreads = 256;
 constexpr int kSpan = 64;
 
 struct SplatEntry {
@@ -470,7 +470,7 @@ __device__ __forceinline__ void splat_apply(PixelAcc& P, float alpha, float4 col
 	P.last = rank + 1;
 }
 
-__global__ void __launch_bounds__(kTileThreads) k_splat_tiles(RenderFrame F, const int* __restrict__ tile_order,
+__global__ void __launch_bounds__(kTileThreads, 3) k_splat_tiles(RenderFrame F, const int* __restrict__ tile_order,
 	const int2* __restrict__ ranges, const int* __restrict__ val, const float2* __restrict__ xy,
 	const float4* __restrict__ conic_op, const float4* __restrict__ rgb, float* __restrict__ out,
 	float* __restrict__ final_T, int* __restrict__ n_contrib, int* __restrict__ pick)
@@ -482,16 +482,15 @@ __global__ void __launch_bounds__(kTileThreads) k_splat_tiles(RenderFrame F, con
 	const int tile = tile_order[blockIdx.x];
 	const int bx = tile % F.tiles_x, by = tile / F.tiles_x;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int qx = bx * kTile + (warp & 1) * 8, qy = by * kTile + (warp >> 1) * 8;
-	const int qx1 = min(qx + 7, F.W - 1), qy1 = min(qy + 7, F.H - 1);
-	const int px = qx + (lane & 3) * 2, py = qy + (lane >> 2);
-	const bool in0 = px < F.W && py < F.H, in1 = px + 1 < F.W && py < F.H;
-	const float fx0 = (float)px, fx1 = (float)(px + 1), fy = (float)py;
+	const int qx = bx * kTile + (warp & 1) * 8, qy = by * kTile + (warp >> 1) * 4;
+	const int qx1 = min(qx + 7, F.W - 1), qy1 = min(qy + 3, F.H - 1);
+	const int px = qx + (lane & 7), py = qy + (lane >> 3);
+	const bool inside = px < F.W && py < F.H;
+	const float fx = (float)px, fy = (float)py;
 	const float rx0 = (float)qx, rx1 = (float)qx1, ry0 = (float)qy, ry1 = (float)qy1;
 	const bool pick_on = F.pick != 0;
-	PixelAcc A, B;
-	A.done = !in0;
-	B.done = !in1;
+	PixelAcc A;
+	A.done = !inside;
 	if (qx <= qx1 && qy <= qy1) {
 		const int2 r = ranges[tile];
 		SplatEntry cur[2], nxt[2];
@@ -505,7 +504,7 @@ __global__ void __launch_bounds__(kTileThreads) k_splat_tiles(RenderFrame F, con
 			nv[e] = k + kSpan < r.y ? val[k + kSpan] : -1;
 		}
 		for (int base = r.x; base < r.y; base += kSpan) {
-			if (__all_sync(0xffffffffu, A.done && B.done)) break;
+			if (__all_sync(0xffffffffu, A.done)) break;
 			// in flight: gathers of step + 1, indices of step + 2
 #pragma unroll
 			for (int e = 0; e < 2; ++e) {
@@ -534,34 +533,21 @@ __global__ void __launch_bounds__(kTileThreads) k_splat_tiles(RenderFrame F, con
 			__syncwarp();
 			const int kept = __popc(b0) + __popc(b1);
 			int j = 0;
-			for (; j + 1 < kept && !(A.done && B.done); j += 2) {
-				const float2 c0 = s_xy[warp][j], c1 = s_xy[warp][j + 1];
-				const float4 q0 = s_co[warp][j], q1 = s_co[warp][j + 1];
-				const float a0 = splat_alpha(fx0, fy, c0, q0), b0a = splat_alpha(fx1, fy, c0, q0);
-				const float a1 = splat_alpha(fx0, fy, c1, q1), b1a = splat_alpha(fx1, fy, c1, q1);
-				const float4 col0 = s_rgb[warp][j], col1 = s_rgb[warp][j + 1];
-				const int id0 = s_id[warp][j], id1 = s_id[warp][j + 1];
-				const int rk0 = s_rank[warp][j], rk1 = s_rank[warp][j + 1];
-				splat_apply(A, a0, col0, id0, rk0, pick_on);
-				splat_apply(B, b0a, col0, id0, rk0, pick_on);
-				splat_apply(A, a1, col1, id1, rk1, pick_on);
-				splat_apply(B, b1a, col1, id1, rk1, pick_on);
+			for (; j + 1 < kept && !A.done; j += 2) {
+				const float a0 = splat_alpha(fx, fy, s_xy[warp][j], s_co[warp][j]);
+				const float a1 = splat_alpha(fx, fy, s_xy[warp][j + 1], s_co[warp][j + 1]);
+				splat_apply(A, a0, s_rgb[warp][j], s_id[warp][j], s_rank[warp][j], pick_on);
+				splat_apply(A, a1, s_rgb[warp][j + 1], s_id[warp][j + 1], s_rank[warp][j + 1], pick_on);
 			}
-			if (j < kept && !(A.done && B.done)) {
-				const float2 c0 = s_xy[warp][j];
-				const float4 q0 = s_co[warp][j];
-				const float4 col0 = s_rgb[warp][j];
-				const int id0 = s_id[warp][j], rk0 = s_rank[warp][j];
-				splat_apply(A, splat_alpha(fx0, fy, c0, q0), col0, id0, rk0, pick_on);
-				splat_apply(B, splat_alpha(fx1, fy, c0, q0), col0, id0, rk0, pick_on);
-			}
+			if (j < kept && !A.done)
+				splat_apply(A, splat_alpha(fx, fy, s_xy[warp][j], s_co[warp][j]), s_rgb[warp][j], s_id[warp][j],
+					s_rank[warp][j], pick_on);
 			__syncwarp();
 #pragma unroll
 			for (int e = 0; e < 2; ++e) cur[e] = nxt[e];
 		}
 	}
-	if (in0) splat_finish(F, px, py, A, out, final_T, n_contrib, pick);
-	if (in1) splat_finish(F, px + 1, py, B, out, final_T, n_contrib, pick);
+	if (inside) splat_finish(F, px, py, A, out, final_T, n_contrib, pick);
 }
 
 }  // namespace dev
