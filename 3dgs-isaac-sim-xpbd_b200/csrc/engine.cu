@@ -187,7 +187,7 @@ public:
 	// splatting (xpbd_b200_render*): per-Gaussian projection, depth order, tile pairs,
 	// tile ranges, the image and its per-pixel extras; colours and options outlive frames
 	struct Render {
-		DBuf<float2> xy;
+		DBuf<float4> xy;     // pixel centre and the half widths of the alpha >= 1/255 box
 		DBuf<float4> conic, rgb;
 		DBuf<int4> rect;
 		DBuf<unsigned int> dkey, dkey_s;

@@ -89,7 +89,7 @@ __device__ __forceinline__ float3 sh_color(int deg, const float* __restrict__ c,
 // culled), radius and tile rectangle.  Quaternions are (w, x, y, z), used as given.
 __global__ void __launch_bounds__(kBlock) k_splat_prepare(int n, RenderFrame F, const float* __restrict__ pos,
 	const float* __restrict__ scales, const float* __restrict__ quats, const float* __restrict__ opacity,
-	const float* __restrict__ colors, float2* __restrict__ xy, float4* __restrict__ conic_op,
+	const float* __restrict__ colors, float4* __restrict__ xy, float4* __restrict__ conic_op,
 	float4* __restrict__ rgb, unsigned int* __restrict__ dkey, int* __restrict__ radii, int4* __restrict__ rect,
 	int* __restrict__ touched)
 {
@@ -198,8 +198,21 @@ __global__ void __launch_bounds__(kBlock) k_splat_prepare(int n, RenderFrame F, 
 	} else {
 		col = make_float3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]);
 	}
-	xy[i] = make_float2(px, py);
-	conic_op[i] = make_float4(cc * idet, -cb * idet, ca * idet, opacity[i] * aa);
+	// half widths of the box outside which alpha stays below 1/255: the ellipse
+	// d^T Q d <= 2 ln(255 o) (Q the conic, Q^-1 the low-passed 2D covariance) has the
+	// axis-aligned half widths sqrt(t cov_xx), sqrt(t cov_yy); the margins keep the
+	// compositing kernel's region test conservative under FP32 rounding
+	const float o_eff = opacity[i] * aa;
+	float ex = -1.0f, ey = -1.0f;
+	if (!(det > 0.0f)) {
+		ex = ey = FLT_MAX;
+	} else if (o_eff >= 1.0f / 255.0f) {
+		const float t = 2.0f * logf(255.0f * o_eff) * 1.002f + 0.02f;
+		ex = sqrtf(t * ca) * 1.001f + 0.01f;
+		ey = sqrtf(t * cc) * 1.001f + 0.01f;
+	}
+	xy[i] = make_float4(px, py, ex, ey);
+	conic_op[i] = make_float4(cc * idet, -cb * idet, ca * idet, o_eff);
 	rgb[i] = make_float4(col.x, col.y, col.z, 0.0f);
 	dkey[i] = __float_as_uint(vz);   // positive floats order as unsigned integers
 	radii[i] = radius;
@@ -335,31 +348,14 @@ __global__ void __launch_bounds__(1024) k_tile_order(int tiles, const int2* __re
 	}
 }
 
-// True unless the Gaussian (centre c, conic co.xyz, opacity co.w) stays below alpha
-// 1/255 at every pixel centre of [x0, x1] x [y0, y1]: the minimum of the quadratic form
-// over the rectangle (a continuous bound, so no larger than at the pixel centres),
-// compared with 2 ln(255 o) plus a margin far above FP32 rounding.  Indefinite conics
-// are always kept.
-__device__ __forceinline__ bool splat_reaches(float2 c, float4 co, float x0, float x1, float y0, float y1)
+// False when the Gaussian (c = centre x, y and the half widths of its alpha >= 1/255
+// box) cannot reach alpha 1/255 at any pixel centre of [x0, x1] x [y0, y1]: the
+// rectangle's nearest point is outside the box.  Conservative by construction of the
+// half widths.
+__device__ __forceinline__ bool splat_reaches(float4 c, float x0, float x1, float y0, float y1)
 {
-	const float a = co.x, b = co.y, cc = co.z, o = co.w;
-	if (o < 1.0f / 255.0f) return false;             // alpha <= o everywhere
-	if (!(a > 0.0f && cc > 0.0f && a * cc - b * b > 0.0f)) return true;
-	if (c.x >= x0 && c.x <= x1 && c.y >= y0 && c.y <= y1) return true;
-	const float t = 2.0f * logf(255.0f * o) * 1.002f + 0.02f;
-	float qmin = FLT_MAX;
-	// edges x = x0, x1 (d = centre - pixel, dy over [c.y - y1, c.y - y0])
-	for (int e = 0; e < 2; ++e) {
-		const float dx = c.x - (e ? x1 : x0);
-		const float dy = fminf(c.y - y0, fmaxf(c.y - y1, -b * dx / cc));
-		qmin = fminf(qmin, a * dx * dx + 2.0f * b * dx * dy + cc * dy * dy);
-	}
-	for (int e = 0; e < 2; ++e) {
-		const float dy = c.y - (e ? y1 : y0);
-		const float dx = fminf(c.x - x0, fmaxf(c.x - x1, -b * dy / a));
-		qmin = fminf(qmin, a * dx * dx + 2.0f * b * dx * dy + cc * dy * dy);
-	}
-	return qmin <= t;
+	const float nx = fminf(fmaxf(c.x, x0), x1), ny = fminf(fmaxf(c.y, y0), y1);
+	return fabsf(c.x - nx) <= c.z && fabsf(c.y - ny) <= c.w;
 }
 
 // Front-to-back state of one pixel (renderCUDA's per-thread registers).
@@ -418,7 +414,8 @@ __device__ __forceinline__ void splat_finish(const RenderFrame& F, int px, int p
 // software-pipelined: the list indices of step s + 2 and the centre, conic and colour
 // of step s + 1 are in flight while step s is tested and blended, so the dependent
 // index -> Gaussian gathers of a long list do not serialise.  Each entry is tested
-// against the warp's region (splat_reaches); survivors are packed into the warp's
+// against the warp's region (splat_reaches: the box outside which its alpha stays
+// below 1/255, computed in k_splat_prepare); survivors are packed into the warp's
 // shared-memory slots with their list position and the pixels visit them in list
 // order, two Gaussians per iteration (their alphas are independent of T).  A Gaussian
 // left out would have been skipped at each of the region's pixels and the position is
@@ -429,11 +426,11 @@ constexpr int kSpan = 64;
 
 struct SplatEntry {
 	int g;
-	float2 c;
+	float4 c;
 	float4 co, col;
 };
 
-__device__ __forceinline__ void splat_fetch(SplatEntry& e, int g, const float2* __restrict__ xy,
+__device__ __forceinline__ void splat_fetch(SplatEntry& e, int g, const float4* __restrict__ xy,
 	const float4* __restrict__ conic_op, const float4* __restrict__ rgb)
 {
 	e.g = g;
@@ -471,7 +468,7 @@ __device__ __forceinline__ void splat_apply(PixelAcc& P, float alpha, float4 col
 }
 
 __global__ void __launch_bounds__(kTileThreads, 3) k_splat_tiles(RenderFrame F, const int* __restrict__ tile_order,
-	const int2* __restrict__ ranges, const int* __restrict__ val, const float2* __restrict__ xy,
+	const int2* __restrict__ ranges, const int* __restrict__ val, const float4* __restrict__ xy,
 	const float4* __restrict__ conic_op, const float4* __restrict__ rgb, float* __restrict__ out,
 	float* __restrict__ final_T, int* __restrict__ n_contrib, int* __restrict__ pick)
 {
@@ -516,7 +513,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_splat_tiles(RenderFrame F, 
 			bool keep[2];
 #pragma unroll
 			for (int e = 0; e < 2; ++e)
-				keep[e] = cur[e].g >= 0 && splat_reaches(cur[e].c, cur[e].co, rx0, rx1, ry0, ry1);
+				keep[e] = cur[e].g >= 0 && splat_reaches(cur[e].c, rx0, rx1, ry0, ry1);
 			const unsigned b0 = __ballot_sync(0xffffffffu, keep[0]);
 			const unsigned b1 = __ballot_sync(0xffffffffu, keep[1]);
 			const unsigned lt = (1u << lane) - 1u;
@@ -524,7 +521,7 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_splat_tiles(RenderFrame F, 
 			for (int e = 0; e < 2; ++e)
 				if (keep[e]) {
 					const int at = e == 0 ? __popc(b0 & lt) : __popc(b0) + __popc(b1 & lt);
-					s_xy[warp][at] = cur[e].c;
+					s_xy[warp][at] = make_float2(cur[e].c.x, cur[e].c.y);
 					s_co[warp][at] = cur[e].co;
 					s_rgb[warp][at] = cur[e].col;
 					s_id[warp][at] = cur[e].g;
