@@ -168,6 +168,7 @@ public:
 
 	// ---- device state ----
 	DBuf<float4> pos_curr, pos_next, pos_tmp, vel, pos_rest, shape_rest;
+	DBuf<float4> shape_q;    // per Gaussian: eigenvector frame of its last FP64 polar decomposition
 	// ChainMail: (arrival time, density), sweep flags / marks / work list / scratch, seeds
 	DBuf<float2> cm_td;
 	DBuf<unsigned char> cm_flag;
@@ -321,7 +322,7 @@ public:
 	void free_device()
 	{
 		pos_curr.release(); pos_next.release(); pos_tmp.release(); vel.release(); pos_rest.release();
-		shape_rest.release();
+		shape_rest.release(); shape_q.release();
 		cm_td.release(); cm_flag.release(); cm_mark.release(); cm_work.release(); cm_seed_idx.release();
 		cm_spos.release(); cm_stime.release(); cm_seed_delta.release(); cm_time_out.release(); cm_state.release();
 		obj_q.release(); obj_shift.release(); obj_sumq.release(); obj_partial.release(); obj_c0.release();
@@ -521,7 +522,8 @@ public:
 				CK(cudaMemcpyAsync(ndist.p, nd.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
 				CK(cudaMemcpyAsync(nstiff.p, ns.data(), sizeof(float) * m, cudaMemcpyHostToDevice, stream));
 			}
-			CK(shape_rest.alloc(n));
+			CK(shape_rest.alloc(n)); CK(shape_q.alloc(n));
+			CK(cudaMemsetAsync(shape_q.p, 0, shape_q.bytes(), stream));   // zero = identity start
 			dev::k_shape_rest<<<blocks_for(n), kBlock, 0, stream>>>(n, pos_rest.p, off.p, nbr.p, shape_rest.p);
 			CK(cudaGetLastError());
 			CK(cudaStreamSynchronize(stream));
@@ -1147,11 +1149,11 @@ public:
 				if (S.shape_robust)
 					launch(ST_SHAPE, G, B, dev::k_shape_match<true>, N, (const StepParams*)d_params, (const float4*)pin,
 						pout, (const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p,
-						(const float4*)shape_rest.p);
+						(const float4*)shape_rest.p, shape_q.p);
 				else
 					launch(ST_SHAPE, G, B, dev::k_shape_match<false>, N, (const StepParams*)d_params, (const float4*)pin,
 						pout, (const float4*)pos_rest.p, (const int*)off.p, (const int*)nbr.p,
-						(const float4*)shape_rest.p);
+						(const float4*)shape_rest.p, shape_q.p);
 				std::swap(pin, pout);
 			}
 			if (sc)

@@ -1173,6 +1173,140 @@ __device__ __forceinline__ bool shape_rotation_double(const M3& A, M3& Rout)
 	return ok;
 }
 
+// shape_rotation_double with the Jacobi started from the eigenvector frame of this
+// Gaussian's previous call (warm, a unit quaternion; all zero = identity) and that
+// frame stored back.  The polar factor R = U V^T is unique for a non-singular A, so the
+// start changes only where the iteration stops, not what it converges to (the same
+// 1e-12 relative off-diagonal test); successive calls of one Gaussian see nearly the
+// same A, which leaves one or two rotations instead of a full cold run.
+__device__ __forceinline__ bool shape_rotation_double_warm(const M3& A, M3& Rout, float4& warm)
+{
+	double a[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) a[r][c] = (double)A.m[c][r];
+	double m[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) m[r][c] = a[0][r] * a[0][c] + a[1][r] * a[1][c] + a[2][r] * a[2][c];
+	double v[3][3] = { { 1.0, 0.0, 0.0 }, { 0.0, 1.0, 0.0 }, { 0.0, 0.0, 1.0 } };
+	{
+		double qw = warm.x, qx = warm.y, qy = warm.z, qz = warm.w;
+		const double qn = qw * qw + qx * qx + qy * qy + qz * qz;
+		if (qn > 0.5) {
+			const double inv = 1.0 / sqrt(qn);
+			qw *= inv; qx *= inv; qy *= inv; qz *= inv;
+			v[0][0] = 1.0 - 2.0 * (qy * qy + qz * qz); v[0][1] = 2.0 * (qx * qy - qw * qz);
+			v[0][2] = 2.0 * (qx * qz + qw * qy);
+			v[1][0] = 2.0 * (qx * qy + qw * qz); v[1][1] = 1.0 - 2.0 * (qx * qx + qz * qz);
+			v[1][2] = 2.0 * (qy * qz - qw * qx);
+			v[2][0] = 2.0 * (qx * qz - qw * qy); v[2][1] = 2.0 * (qy * qz + qw * qx);
+			v[2][2] = 1.0 - 2.0 * (qx * qx + qy * qy);
+			// m <- V^T m V
+			double t[3][3];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c) t[r][c] = m[r][0] * v[0][c] + m[r][1] * v[1][c] + m[r][2] * v[2][c];
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+#pragma unroll
+				for (int c = 0; c < 3; ++c) m[r][c] = v[0][r] * t[0][c] + v[1][r] * t[1][c] + v[2][r] * t[2][c];
+		}
+	}
+	for (int iter = 0; iter < 50; ++iter) {
+		bool done = true;
+		int piv = 0;   // 0: (0,1), 1: (0,2), 2: (1,2)
+		double max_off = -1.0;
+#pragma unroll
+		for (int k = 0; k < 3; ++k) {
+			const int pk = (k == 2) ? 1 : 0, qk = (k == 0) ? 1 : 2;
+			const double off = fabs(m[pk][qk]);
+			// off > 1e-12 sqrt(|a_pp a_qq|) + 1e-300, compared in squares (no square root)
+			if (off > 1e-300 && off * off > 1e-24 * fabs(m[pk][pk] * m[qk][qk])) done = false;
+			if (off > max_off) { max_off = off; piv = k; }
+		}
+		if (done) break;
+		if (piv == 0) jacobi_rotate_d<0, 1>(m, v);
+		else if (piv == 1) jacobi_rotate_d<0, 2>(m, v);
+		else jacobi_rotate_d<1, 2>(m, v);
+	}
+	{
+		// the converged frame (a proper rotation: products of rotations), as a unit
+		// quaternion for the next call (largest-component extraction)
+		const double tr = v[0][0] + v[1][1] + v[2][2];
+		double qw, qx, qy, qz;
+		if (tr > 0.0) {
+			const double s2 = 2.0 * sqrt(1.0 + tr);
+			qw = 0.25 * s2; qx = (v[2][1] - v[1][2]) / s2; qy = (v[0][2] - v[2][0]) / s2; qz = (v[1][0] - v[0][1]) / s2;
+		} else if (v[0][0] > v[1][1] && v[0][0] > v[2][2]) {
+			const double s2 = 2.0 * sqrt(fmax(1.0 + v[0][0] - v[1][1] - v[2][2], 1e-30));
+			qw = (v[2][1] - v[1][2]) / s2; qx = 0.25 * s2; qy = (v[0][1] + v[1][0]) / s2; qz = (v[0][2] + v[2][0]) / s2;
+		} else if (v[1][1] > v[2][2]) {
+			const double s2 = 2.0 * sqrt(fmax(1.0 + v[1][1] - v[0][0] - v[2][2], 1e-30));
+			qw = (v[0][2] - v[2][0]) / s2; qx = (v[0][1] + v[1][0]) / s2; qy = 0.25 * s2; qz = (v[1][2] + v[2][1]) / s2;
+		} else {
+			const double s2 = 2.0 * sqrt(fmax(1.0 + v[2][2] - v[0][0] - v[1][1], 1e-30));
+			qw = (v[1][0] - v[0][1]) / s2; qx = (v[0][2] + v[2][0]) / s2; qy = (v[1][2] + v[2][1]) / s2; qz = 0.25 * s2;
+		}
+		warm = isfinite(qw + qx + qy + qz) ? make_float4((float)qw, (float)qx, (float)qy, (float)qz)
+			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	}
+	double ev[3] = { m[0][0], m[1][1], m[2][2] };
+#pragma unroll
+	for (int i = 0; i < 2; ++i)
+#pragma unroll
+		for (int j = i + 1; j < 3; ++j)
+			if (ev[i] > ev[j]) {
+				const double te = ev[i]; ev[i] = ev[j]; ev[j] = te;
+#pragma unroll
+				for (int rr = 0; rr < 3; ++rr) { const double tv = v[rr][i]; v[rr][i] = v[rr][j]; v[rr][j] = tv; }
+			}
+	double S[3], Si[3];
+#pragma unroll
+	for (int i = 0; i < 3; ++i) S[i] = sqrt(ev[i] > 0.0 ? ev[i] : 0.0);
+	const double smax = (S[2] > 1e-300) ? S[2] : 1e-300;
+#pragma unroll
+	for (int i = 0; i < 3; ++i) Si[i] = (S[i] > 1e-12 * smax) ? 1.0 / S[i] : 0.0;
+	double u[3][3];
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) u[r][c] = (a[r][0] * v[0][c] + a[r][1] * v[1][c] + a[r][2] * v[2][c]) * Si[c];
+	if (S[0] < 0.08 * smax) {
+		const double cx = u[1][1] * u[2][2] - u[2][1] * u[1][2];
+		const double cy = u[2][1] * u[0][2] - u[0][1] * u[2][2];
+		const double cz = u[0][1] * u[1][2] - u[1][1] * u[0][2];
+		const double len = sqrt(cx * cx + cy * cy + cz * cz);
+		if (!(len > 1e-7)) return false;
+		u[0][0] = cx / len; u[1][0] = cy / len; u[2][0] = cz / len;
+	}
+	double R[3][3];
+	for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) R[r][c] = u[r][0] * v[c][0] + u[r][1] * v[c][1] + u[r][2] * v[c][2];
+		const double det = R[0][0] * (R[1][1] * R[2][2] - R[1][2] * R[2][1])
+			- R[0][1] * (R[1][0] * R[2][2] - R[1][2] * R[2][0])
+			+ R[0][2] * (R[1][0] * R[2][1] - R[1][1] * R[2][0]);
+		if (det >= 0.0 || pass == 1) break;
+#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) u[rr][0] = -u[rr][0];
+	}
+	bool ok = true;
+#pragma unroll
+	for (int r = 0; r < 3; ++r)
+#pragma unroll
+		for (int c = 0; c < 3; ++c) {
+			ok = ok && isfinite(R[r][c]);
+			Rout.m[c][r] = (float)R[r][c];
+		}
+	return ok;
+}
+
 __device__ __noinline__ bool shape_rotation_float(const M3& A, M3& Rout)
 {
 	const M3 AtA = m3_mul(m3_t(A), A);
@@ -1253,7 +1387,8 @@ __global__ void __launch_bounds__(kBlock) k_shape_rest(int n, const float4* __re
 template <bool ROBUST>
 __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
-	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest)
+	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest,
+	float4* __restrict__ shape_q)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1293,7 +1428,15 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 #pragma unroll
 		for (int r = 0; r < 3; ++r) A.m[c][r] /= a_norm;
 	M3 R;
-	const bool ok = ROBUST ? shape_rotation_double(A, R) : shape_rotation_float(A, R);
+	bool ok;
+	if (ROBUST) {
+		float4 q = shape_q[idx];
+		ok = shape_rotation_double_warm(A, R, q);
+		shape_q[idx] = q;
+	}
+	else {
+		ok = shape_rotation_float(A, R);
+	}
 	if (!ok) { pout[idx] = p4; return; }
 	const float3 goal = add3(com_curr, m3_mulv(R, sub3(ri, com_rest)));
 	const float3 gd = sub3(goal, pi);
