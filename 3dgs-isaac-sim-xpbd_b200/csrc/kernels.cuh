@@ -1858,74 +1858,95 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 		int* out = contacts + (size_t)i * kSelfColMax;
 		float prio[kSelfColMax];
 		int tier[kSelfColMax];
-		// a cell whose hash repeats an earlier one of the 27 is skipped (forward.cu:7116-7123);
-		// a 64-bit filter on the low hash bits settles almost every cell without comparing,
-		// the rest recompute the earlier hashes
-		unsigned long long seen = 0ull;
-		int kc = 0;
-		for (int oz = -1; oz <= 1; ++oz)
-			for (int oy = -1; oy <= 1; ++oy)
-				for (int ox = -1; ox <= 1; ++ox, ++kc) {
-					const unsigned int h = sc_hash(cx + ox, cy + oy, cz + oz, mask);
-					const unsigned long long bit = 1ull << (h & 63u);
-					if (seen & bit) {
-						bool dup = false;
-						for (int m = 0; m < kc && !dup; ++m) {
-							const int mz = m / 9 - 1, my = (m / 3) % 3 - 1, mx = m % 3 - 1;
-							dup = sc_hash(cx + mx, cy + my, cz + mz, mask) == h;
-						}
-						if (dup) continue;
-					}
-					seen |= bit;
-					const int s = start[h], e = start[h + 1];
-					for (int t = s; t < e; ++t) {
-						// predicted position + index first: most neighbours fail the distance
-						// test, so the rest position / object id is read only for the others
-						const float4 pj = sp[t];
-						const int j = __float_as_int(pj.w);
-						if (j == i) continue;
-						const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-						const float d2 = ex * ex + ey * ey + ez * ez;
-						const bool near_same = d2 < search2;
-						if (!near_same && single_object) continue;
-						const float4 rj = sr[t];
-						const bool cross = __float_as_int(rj.w) != oi;
-						if (!cross && !within) continue;
-						const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
-						const float q2 = qx * qx + qy * qy + qz * qz;
-						float pr;
-						int code = j;
-						if (cross) {
-							const float4 xj = sx[t];
-							const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
-							const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
-							const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
-							const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
-							if (!(dist_x < search + rel)) continue;
-							if (!(q2 >= cross_excl2)) continue;
-							pr = dist_x - rel;
-							if (rel > fast_rel) code = -(j + 1);
-						}
-						else {
-							if (!near_same) continue;
-							if (!(q2 >= excl2)) continue;
-							pr = sqrtf(d2);
-						}
-						const int tr = cross ? 0 : 1;
-						if (cnt < kSelfColMax) {
-							out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
-						}
-						else {
-							int worst = 0;
-							for (int m = 1; m < kSelfColMax; ++m)
-								if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
-							if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
-								out[worst] = code; prio[worst] = pr; tier[worst] = tr;
-							}
-							++over;
-						}
-					}
+		// the 27 cells in the reference's order (z, y, x nested, kc = 9 (z+1) + 3 (y+1) +
+		// (x+1)); a cell whose hash repeats an earlier one of the 27 is skipped
+		// (forward.cu:7116-7123).  A 64-bit filter on the low hash bits settles almost
+		// every cell without comparing, the rest recompute the earlier hashes.
+		unsigned int use = 0u;
+		{
+			unsigned long long seen = 0ull;
+			for (int kc = 0; kc < 27; ++kc) {
+				const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
+				const unsigned long long bit = 1ull << (h & 63u);
+				if (seen & bit) {
+					bool dup = false;
+					for (int m = 0; m < kc && !dup; ++m)
+						dup = sc_hash(cx + m % 3 - 1, cy + (m / 3) % 3 - 1, cz + m / 9 - 1, mask) == h;
+					if (dup) continue;
 				}
+				seen |= bit;
+				use |= 1u << kc;
+			}
+		}
+		// the used cells in order, the next cell's bucket range loaded while the current
+		// cell's entries are tested
+		int kc = use ? __ffs(use) - 1 : 27;
+		int cs = 0, ce = 0;
+		if (kc < 27) {
+			const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
+			cs = start[h];
+			ce = start[h + 1];
+		}
+		while (kc < 27) {
+			const unsigned int later = use & ~((2u << kc) - 1u);
+			const int kn = later ? __ffs(later) - 1 : 27;
+			int ns = 0, ne = 0;
+			if (kn < 27) {
+				const unsigned int hn = sc_hash(cx + kn % 3 - 1, cy + (kn / 3) % 3 - 1, cz + kn / 9 - 1, mask);
+				ns = start[hn];
+				ne = start[hn + 1];
+			}
+			for (int t = cs; t < ce; ++t) {
+				// predicted position + index first: most neighbours fail the distance
+				// test, so the rest position / object id is read only for the others
+				const float4 pj = sp[t];
+				const int j = __float_as_int(pj.w);
+				if (j == i) continue;
+				const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+				const float d2 = ex * ex + ey * ey + ez * ez;
+				const bool near_same = d2 < search2;
+				if (!near_same && single_object) continue;
+				const float4 rj = sr[t];
+				const bool cross = __float_as_int(rj.w) != oi;
+				if (!cross && !within) continue;
+				const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
+				const float q2 = qx * qx + qy * qy + qz * qz;
+				float pr;
+				int code = j;
+				if (cross) {
+					const float4 xj = sx[t];
+					const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
+					const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
+					const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
+					const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
+					if (!(dist_x < search + rel)) continue;
+					if (!(q2 >= cross_excl2)) continue;
+					pr = dist_x - rel;
+					if (rel > fast_rel) code = -(j + 1);
+				}
+				else {
+					if (!near_same) continue;
+					if (!(q2 >= excl2)) continue;
+					pr = sqrtf(d2);
+				}
+				const int tr = cross ? 0 : 1;
+				if (cnt < kSelfColMax) {
+					out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
+				}
+				else {
+					int worst = 0;
+					for (int m = 1; m < kSelfColMax; ++m)
+						if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
+					if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
+						out[worst] = code; prio[worst] = pr; tier[worst] = tr;
+					}
+					++over;
+				}
+			}
+			kc = kn;
+			cs = ns;
+			ce = ne;
+		}
 	}
 	counts[i] = cnt;
 	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
