@@ -172,7 +172,7 @@ def algorithmic_bytes(stage, sizes, n):
         "distance": 28 + 20 * m_dir,
         "volume_solve": 4 * members + 56,
         "volume_gather": 4 * rev + 80,
-        "shape": 48 + 4 * m_dir,
+        "shape": 48 + 4 * m_dir + 32,   # + the warm-start eigenvector frame, read and written
         "project": 28,
         "predict": 52,
         "velocity": 48,
