@@ -235,22 +235,20 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 	const float dt = P->dt;
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const int e0 = off[idx], e1 = off[idx + 1];
-	for (int edge = e0; edge < e1; ++edge) {
-		const int j = __ldg(nbr + edge);
-		float lambda = read_lam ? lam[edge] : 0.0f;
-		if (j < 0 || j >= n) continue;
-		const float4 q4 = ld4(pin, j);
+	// one edge of the row: its neighbour's position and its own multiplier, rest length
+	// and stiffness already loaded
+	auto edge_step = [&](int edge, float4 q4, float lambda, float rest, float stiff_e) {
 		const float3 diff = sub3(pi, f3(q4));
 		const float d = len3(diff);
-		if (d < 1e-7f) continue;
-		const float C = d - __ldg(ndist + edge);
+		if (d < 1e-7f) return;
+		const float C = d - rest;
 		const float3 grad = mul3(diff, 1.0f / d);
 		const float wj = q4.w * ims;
-		const float stiff = fmaxf(__ldg(nstiff + edge) * ss, 1e-6f);
+		const float stiff = fmaxf(stiff_e * ss, 1e-6f);
 		const float alpha = gc / stiff;
 		const float alpha_tilde = alpha / dt2;
 		const float denom = (wi + wj) + alpha_tilde;
-		if (denom < 1e-8f) continue;
+		if (denom < 1e-8f) return;
 		const float dl = (-C - alpha_tilde * lambda) / denom;
 		lambda += dl;
 		if (write_lam) lam[edge] = lambda;
@@ -258,6 +256,26 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 			accum = add3(accum, mul3(grad, wi * dl));
 			valid++;
 		}
+	};
+	// two edges per trip: their loads are in flight together; edges are applied in row
+	// order, so the result is that of the one-at-a-time loop bit for bit
+	int edge = e0;
+	for (; edge + 1 < e1; edge += 2) {
+		const int j0 = __ldg(nbr + edge), j1 = __ldg(nbr + edge + 1);
+		const float l0 = read_lam ? lam[edge] : 0.0f, l1 = read_lam ? lam[edge + 1] : 0.0f;
+		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
+		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
+		if (ok0) q0 = ld4(pin, j0);
+		if (ok1) q1 = ld4(pin, j1);
+		const float r0 = __ldg(ndist + edge), r1 = __ldg(ndist + edge + 1);
+		const float s0 = __ldg(nstiff + edge), s1 = __ldg(nstiff + edge + 1);
+		if (ok0) edge_step(edge, q0, l0, r0, s0);
+		if (ok1) edge_step(edge + 1, q1, l1, r1, s1);
+	}
+	if (edge < e1) {
+		const int j = __ldg(nbr + edge);
+		const float lambda = read_lam ? lam[edge] : 0.0f;
+		if (j >= 0 && j < n) edge_step(edge, ld4(pin, j), lambda, __ldg(ndist + edge), __ldg(nstiff + edge));
 	}
 	float3 out = pi;
 	if (wi > 0.0f && valid > 0) {
@@ -800,6 +818,22 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const Ste
 	store_record(rec, idx, c, dl * gs, Sinv);
 }
 
+// one blackboard record (already loaded) applied to a node (forward.cu:9212-9222)
+__device__ __forceinline__ bool gather_rec(float4 r0, float4 r1, float4 r2, float3 pi, float wi, float3& dp)
+{
+	const float coef = r0.w;
+	if (coef == 0.0f) return false;
+	M3 S;
+	S.m[0][0] = r1.x; S.m[1][1] = r1.y; S.m[2][2] = r1.z;
+	S.m[0][1] = S.m[1][0] = r1.w;
+	S.m[0][2] = S.m[2][0] = r2.x;
+	S.m[1][2] = S.m[2][1] = r2.y;
+	const float3 d = sub3(pi, make_float3(r0.x, r0.y, r0.z));
+	const float3 g = m3_mulv(S, d);
+	dp = make_float3(g.x * wi * coef, g.y * wi * coef, g.z * wi * coef);
+	return fin3(dp);
+}
+
 // one blackboard record applied to a node (forward.cu:9212-9222)
 __device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, int i, float3 pi, float wi, float3& dp)
 {
@@ -854,13 +888,27 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 	const float3 pi = f3(p4);
 	float3 sum = make_float3(0.0f, 0.0f, 0.0f);
 	int received = 0;
-	for (int k = sl; k < cnt; k += S) {
-		const int i = __ldg(ridx + off + k);
-		if (i < 0 || i >= n) continue;
+	// two records per trip: both index loads, then all six record loads, are in flight
+	// together (the loop is latency bound); records are applied in list order, as in
+	// the one-at-a-time loop, so the sum is the same bit for bit
+	int k = sl;
+	for (; k + S < cnt; k += 2 * S) {
+		const int i0 = __ldg(ridx + off + k), i1 = __ldg(ridx + off + k + S);
+		const bool ok0 = i0 >= 0 && i0 < n, ok1 = i1 >= 0 && i1 < n;
+		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, c0 = a0, a1 = a0, b1 = a0, c1 = a0;
+		if (ok0) { a0 = __ldg(rec + 3 * i0); b0 = __ldg(rec + 3 * i0 + 1); c0 = __ldg(rec + 3 * i0 + 2); }
+		if (ok1) { a1 = __ldg(rec + 3 * i1); b1 = __ldg(rec + 3 * i1 + 1); c1 = __ldg(rec + 3 * i1 + 2); }
 		float3 dp;
-		if (!gather_one(rec, i, pi, wi, dp)) continue;
-		sum = add3(sum, dp);
-		++received;
+		if (ok0 && gather_rec(a0, b0, c0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
+		if (ok1 && gather_rec(a1, b1, c1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
+	}
+	if (k < cnt) {
+		const int i = __ldg(ridx + off + k);
+		float3 dp;
+		if (i >= 0 && i < n && gather_one(rec, i, pi, wi, dp)) {
+			sum = add3(sum, dp);
+			++received;
+		}
 	}
 	const float sx = group_sum<S>(sum.x), sy = group_sum<S>(sum.y), sz = group_sum<S>(sum.z);
 	const int rc = (int)(group_sum<S>((float)received) + 0.5f);
