@@ -1449,20 +1449,40 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 	const int e0 = off[idx], e1 = off[idx + 1];
 	const float3 ri = f3(ld4(rest, idx));
 	const float3 com_rest = f3(sr);
+	// both neighbour loops take two neighbours per trip (loads in flight together) and
+	// add them in row order, as the one-at-a-time loops do
 	float3 com_curr = pi;
-	for (int e = e0; e < e1; ++e) {
+	int e = e0;
+	for (; e + 1 < e1; e += 2) {
+		const int j0 = __ldg(nbr + e), j1 = __ldg(nbr + e + 1);
+		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
+		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
+		if (ok0) q0 = ld4(pin, j0);
+		if (ok1) q1 = ld4(pin, j1);
+		if (ok0) com_curr = add3(com_curr, f3(q0));
+		if (ok1) com_curr = add3(com_curr, f3(q1));
+	}
+	if (e < e1) {
 		const int j = __ldg(nbr + e);
-		if (j < 0 || j >= n) continue;
-		com_curr = add3(com_curr, f3(ld4(pin, j)));
+		if (j >= 0 && j < n) com_curr = add3(com_curr, f3(ld4(pin, j)));
 	}
 	com_curr = mul3(com_curr, sr.w);
 	M3 A;
 	m3_zero(A);
 	m3_add_outer(A, sub3(pi, com_curr), sub3(ri, com_rest));
-	for (int e = e0; e < e1; ++e) {
+	e = e0;
+	for (; e + 1 < e1; e += 2) {
+		const int j0 = __ldg(nbr + e), j1 = __ldg(nbr + e + 1);
+		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
+		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0, r0 = q0, r1 = q0;
+		if (ok0) { q0 = ld4(pin, j0); r0 = ld4(rest, j0); }
+		if (ok1) { q1 = ld4(pin, j1); r1 = ld4(rest, j1); }
+		if (ok0) m3_add_outer(A, sub3(f3(q0), com_curr), sub3(f3(r0), com_rest));
+		if (ok1) m3_add_outer(A, sub3(f3(q1), com_curr), sub3(f3(r1), com_rest));
+	}
+	if (e < e1) {
 		const int j = __ldg(nbr + e);
-		if (j < 0 || j >= n) continue;
-		m3_add_outer(A, sub3(f3(ld4(pin, j)), com_curr), sub3(f3(ld4(rest, j)), com_rest));
+		if (j >= 0 && j < n) m3_add_outer(A, sub3(f3(ld4(pin, j)), com_curr), sub3(f3(ld4(rest, j)), com_rest));
 	}
 	float a_norm_sq = 0.0f;
 #pragma unroll
