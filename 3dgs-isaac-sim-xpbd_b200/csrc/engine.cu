@@ -1102,7 +1102,12 @@ public:
 					const int rl = first ? 0 : 1;
 					const StepParams* dp = d_params;
 					const float4* cpin = pin;
-					if (la == 32)
+					if (la == 4 && S.lanes_a == 0)
+						// automatic: one pass over the members, 4 lanes per cluster
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_onepass<4>, N, dp, cpin,
+							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
+							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+					else if (la == 32)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 32), B, dev::k_volume_solve_group<32, 8>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
 							lam_vol.p, rec.p, rl);

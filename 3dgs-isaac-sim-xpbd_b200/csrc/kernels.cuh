@@ -749,6 +749,115 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 	store_record(rec, idx, c, dl * gs, Sinv);
 }
 
+// Kernel A in one pass over the members (S lanes per cluster, members L, L+S, ... of
+// the Morton-sorted list on lane L, two in flight per trip): each lane accumulates,
+// relative to the leader's position, the count, first and second moments of its
+// members and the same moments weighted by inverse mass.  The centred covariance
+//   Sigma = (1 / (m+1)) sum (q - c)(q - c)^T = sum d d^T / (m+1) - c' c'^T
+// (d = q - p_leader, c' = c - p_leader, the leader's d = 0) and the denominator
+//   sum w |g Sinv (q - c)|^2 = g^2 tr(Sinv^2 W),  W = sum w (d - c')(d - c')^T
+// follow from them, so the member positions are read once and nothing is staged.
+// Members lie within a few graph spacings of their leader, which keeps the
+// cancellation in the moment form small; the result equals the two-pass form
+// (forward.cu:8531-8664) to FP32 rounding.
+template <int S>
+__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, int read_lam)
+{
+	const int sl = threadIdx.x & (S - 1);
+	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const bool in_range = idx < n;
+	bool valid = in_range && mat_type[idx] == 0;
+	int off = 0, cnt = 0;
+	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (valid) {
+		off = voff[idx];
+		cnt = voff[idx + 1] - off;
+		p4 = ld4(pin, idx);
+	}
+	const float3 pi = f3(p4);
+	const float ims = P->inv_mass_scale;
+	// m[0..9]: count, d, d d^T (xx yy zz xy xz yz); m[10..19]: the same weighted by w
+	float m[20];
+#pragma unroll
+	for (int t = 0; t < 20; ++t) m[t] = 0.0f;
+	auto add = [&](float4 q) {
+		const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z, w = q.w * ims;
+		m[0] += 1.0f; m[1] += dx; m[2] += dy; m[3] += dz;
+		m[4] += dx * dx; m[5] += dy * dy; m[6] += dz * dz; m[7] += dx * dy; m[8] += dx * dz; m[9] += dy * dz;
+		m[10] += w; m[11] += w * dx; m[12] += w * dy; m[13] += w * dz;
+		m[14] += w * dx * dx; m[15] += w * dy * dy; m[16] += w * dz * dz;
+		m[17] += w * dx * dy; m[18] += w * dx * dz; m[19] += w * dy * dz;
+	};
+	int k = sl;
+	for (; k + S < cnt; k += 2 * S) {
+		const int j0 = __ldg(vidx + off + k), j1 = __ldg(vidx + off + k + S);
+		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
+		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
+		if (ok0) q0 = ld4(pin, j0);
+		if (ok1) q1 = ld4(pin, j1);
+		if (ok0) add(q0);
+		if (ok1) add(q1);
+	}
+	if (k < cnt) {
+		const int j = __ldg(vidx + off + k);
+		if (j >= 0 && j < n) add(ld4(pin, j));
+	}
+#pragma unroll
+	for (int t = 0; t < 20; ++t) m[t] = group_sum<S>(m[t]);
+	const int used = (int)(m[0] + 0.5f);
+	valid = valid && used >= 3;
+	const float inv_n = 1.0f / (float)(used + 1);
+	const float cx = m[1] * inv_n, cy = m[2] * inv_n, cz = m[3] * inv_n;   // c - p_leader
+	const float3 c = make_float3(pi.x + cx, pi.y + cy, pi.z + cz);
+	M3 Sm;
+	Sm.m[0][0] = m[4] * inv_n - cx * cx;
+	Sm.m[1][1] = m[5] * inv_n - cy * cy;
+	Sm.m[2][2] = m[6] * inv_n - cz * cz;
+	Sm.m[0][1] = Sm.m[1][0] = m[7] * inv_n - cx * cy;
+	Sm.m[0][2] = Sm.m[2][0] = m[8] * inv_n - cx * cz;
+	Sm.m[1][2] = Sm.m[2][1] = m[9] * inv_n - cy * cz;
+	if (sl != 0 || !in_range) return;
+	float J = 1.0f, C = 0.0f;
+	M3 Sinv;
+	m3_zero(Sinv);
+	if (valid) valid = cluster_j_sinv(Sm, __ldg(det_rest + idx), J, C, Sinv);
+	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	const float gs = J * inv_n;
+	// W over members and leader (weight w_leader, d = 0)
+	const float wl = p4.w * ims;
+	const float ws = m[10] + wl;
+	float W[3][3];
+	const float wd[3] = { m[11], m[12], m[13] }, cc[3] = { cx, cy, cz };
+	const float wdd[3][3] = { { m[14], m[17], m[18] }, { m[17], m[15], m[19] }, { m[18], m[19], m[16] } };
+#pragma unroll
+	for (int a = 0; a < 3; ++a)
+#pragma unroll
+		for (int b = 0; b < 3; ++b) W[a][b] = wdd[a][b] - cc[a] * wd[b] - wd[a] * cc[b] + ws * cc[a] * cc[b];
+	// tr(Sinv^2 W) = sum_ab (Sinv^2)_ab W_ab
+	float dsum = 0.0f;
+#pragma unroll
+	for (int a = 0; a < 3; ++a)
+#pragma unroll
+		for (int b = 0; b < 3; ++b) {
+			const float s2 = Sinv.m[a][0] * Sinv.m[0][b] + Sinv.m[a][1] * Sinv.m[1][b] + Sinv.m[a][2] * Sinv.m[2][b];
+			dsum += s2 * W[a][b];
+		}
+	const float denom = gs * gs * dsum;
+	const float dt = P->dt;
+	const float dt2 = fmaxf(dt * dt, 1e-8f);
+	const float alpha_t = P->vol_compliance / dt2;
+	const float den = denom + alpha_t;
+	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	const float lam = read_lam ? lam_vol[idx] : 0.0f;
+	const float dl = (-C - alpha_t * lam) / den;
+	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	lam_vol[idx] = lam + dl;
+	store_record(rec, idx, c, dl * gs, Sinv);
+}
+
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
 __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
