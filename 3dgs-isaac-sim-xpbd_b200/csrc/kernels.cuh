@@ -1558,41 +1558,46 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 	const int e0 = off[idx], e1 = off[idx + 1];
 	const float3 ri = f3(ld4(rest, idx));
 	const float3 com_rest = f3(sr);
-	// both neighbour loops take two neighbours per trip (loads in flight together) and
-	// add them in row order, as the one-at-a-time loops do
-	float3 com_curr = pi;
-	int e = e0;
-	for (; e + 1 < e1; e += 2) {
-		const int j0 = __ldg(nbr + e), j1 = __ldg(nbr + e + 1);
-		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
-		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
-		if (ok0) q0 = ld4(pin, j0);
-		if (ok1) q1 = ld4(pin, j1);
-		if (ok0) com_curr = add3(com_curr, f3(q0));
-		if (ok1) com_curr = add3(com_curr, f3(q1));
-	}
-	if (e < e1) {
-		const int j = __ldg(nbr + e);
-		if (j >= 0 && j < n) com_curr = add3(com_curr, f3(ld4(pin, j)));
-	}
-	com_curr = mul3(com_curr, sr.w);
+	// one pass over the 1-ring, two neighbours per trip (loads in flight together):
+	// the current centroid's sum in row order (as the two-pass form computes it) and,
+	// relative to the Gaussian itself (dq = q - p_i, dr = r - r_i), the sums of dq, dr
+	// and dq dr^T.  With cq = com - p_i and cr = com_rest - r_i,
+	//   A = sum_k (q_k - com)(r_k - com_rest)^T = sum dq dr^T - cq (sum dr)^T - (sum dq) cr^T
+	//       + (m+1) cq cr^T
+	// over the Gaussian and its m neighbours (the Gaussian's own dq = dr = 0); the
+	// neighbours lie within a spacing or two, so the shifted moments lose little to
+	// cancellation (equal to the two-pass sums to FP32 rounding).
+	float3 sq = pi, sdq = make_float3(0.0f, 0.0f, 0.0f), sdr = sdq;
+	float count = 1.0f;
 	M3 A;
 	m3_zero(A);
-	m3_add_outer(A, sub3(pi, com_curr), sub3(ri, com_rest));
-	e = e0;
+	auto add = [&](float4 q, float4 r) {
+		sq = add3(sq, f3(q));
+		const float3 dq = sub3(f3(q), pi), dr = sub3(f3(r), ri);
+		sdq = add3(sdq, dq);
+		sdr = add3(sdr, dr);
+		m3_add_outer(A, dq, dr);
+		count += 1.0f;
+	};
+	int e = e0;
 	for (; e + 1 < e1; e += 2) {
 		const int j0 = __ldg(nbr + e), j1 = __ldg(nbr + e + 1);
 		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
 		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0, r0 = q0, r1 = q0;
 		if (ok0) { q0 = ld4(pin, j0); r0 = ld4(rest, j0); }
 		if (ok1) { q1 = ld4(pin, j1); r1 = ld4(rest, j1); }
-		if (ok0) m3_add_outer(A, sub3(f3(q0), com_curr), sub3(f3(r0), com_rest));
-		if (ok1) m3_add_outer(A, sub3(f3(q1), com_curr), sub3(f3(r1), com_rest));
+		if (ok0) add(q0, r0);
+		if (ok1) add(q1, r1);
 	}
 	if (e < e1) {
 		const int j = __ldg(nbr + e);
-		if (j >= 0 && j < n) m3_add_outer(A, sub3(f3(ld4(pin, j)), com_curr), sub3(f3(ld4(rest, j)), com_rest));
+		if (j >= 0 && j < n) add(ld4(pin, j), ld4(rest, j));
 	}
+	const float3 com_curr = mul3(sq, sr.w);
+	const float3 cq = sub3(com_curr, pi), cr = sub3(com_rest, ri);
+	m3_add_outer(A, cq, mul3(sdr, -1.0f));
+	m3_add_outer(A, mul3(sdq, -1.0f), cr);
+	m3_add_outer(A, mul3(cq, count), cr);
 	float a_norm_sq = 0.0f;
 #pragma unroll
 	for (int c = 0; c < 3; ++c)
