@@ -1103,7 +1103,7 @@ public:
 					const StepParams* dp = d_params;
 					const float4* cpin = pin;
 					if (la == 4 && S.lanes_a == 0)
-						// automatic: one pass over the members, 4 lanes per cluster
+						// automatic: one pass over the members (any count), 4 lanes per cluster
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_onepass<4>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
@@ -1115,12 +1115,7 @@ public:
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_slots<8, 8, true>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
-					else if (la == 4 && S.lanes_a == 0 && clusters.avg_members > 64.0f)
-						// more than 64 members: 8 lanes x 16 staged slots hold up to 128
-						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8, dev::kSmemBlock), dim3(dev::kSmemBlock),
-							dev::k_volume_solve_smem<8, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p,
-							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
-					else if (la == 4)
+					else if (la == 4)   // 4 lanes, members staged in shared memory (two-pass sums)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4, dev::kSmemBlock), dim3(dev::kSmemBlock),
 							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p,
 							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);

@@ -197,8 +197,9 @@ XPBD_API void xpbd_b200_set_gs(int distance, int volume);
  * 1 one thread per cluster (the reference's thread kernels' summation
  * order), 2 one warp per cluster (its warp kernels' order). */
 XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
-/* Lanes per cluster for the volume solve (2, 4, 8, 32) and per node for the volume
- * gather (4, 8, 32) in automatic mode; 0 restores the automatic choice. */
+/* Lanes per cluster for the volume solve (2, 4, 8, 32: the staged and register forms)
+ * and per node for the volume gather (4, 8, 32) in automatic mode; 0 restores the
+ * automatic choice (solve: the one-pass moment form on 4 lanes; gather: 4 lanes). */
 XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes);
 /* 1 (default): replay each step from a captured CUDA graph; 0: launch kernel by kernel. */
 XPBD_API void xpbd_b200_set_graph(int enabled);

@@ -155,6 +155,25 @@ def test_volume_kernel_shapes_agree_with_oracle(lib, mode):
     assert H.max_err_over_diag(out["b200"], out["oracle"], diag) < H.TOL_100STEP
 
 
+def test_volume_large_clusters_agree_with_oracle(lib):
+    """Clusters of up to 128 members (the dense-contact configuration's cap) in the
+    automatic one-pass volume solve, against the oracle's two-pass sums."""
+    orc = H.oracle()
+    out = {}
+    for name, solver in (("b200", lib), ("oracle", orc)):
+        s = H.scenes.plain_scene_scenario(3000, 4, pins=30, max_members=128)
+        s.setup(solver)
+        s.advance(solver, 10)
+        out[name] = solver.positions()
+    orc.destroy()
+    s = H.scenes.plain_scene_scenario(3000, 4, pins=30, max_members=128)
+    s.setup(lib)
+    lib.step()
+    assert lib.ints("vol_count").max() > 64
+    diag = H.scenes.bbox_diagonal(out["oracle"])
+    assert H.max_err_over_diag(out["b200"], out["oracle"], diag) < H.TOL_100STEP
+
+
 def test_internal_order_does_not_change_results(lib):
     """Morton order inside the engine reproduces the caller-order run bit for bit: every
     list (neighbours, members, clusters per node, hash-cell order) keeps its order."""
