@@ -539,7 +539,7 @@ public:
 		}
 		CK(det_rest.alloc(n)); CK(v_rest.alloc(n)); CK(rest_len.alloc(n)); CK(sigma_rest.alloc(6 * (size_t)n));
 		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * (size_t)n));
-		CK(cudaMemsetAsync(rec.p, 0, rec.bytes(), stream));
+		CK(cudaMemsetAsync(rec.p, 0xff, rec.bytes(), stream));   // every record NaN: no record yet
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		build_components(graph, 50, obj_id, num_objects);
 		single_object = std::all_of(obj_id.begin(), obj_id.end(), [&](int v) { return v == obj_id[0]; });
@@ -2323,11 +2323,11 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 		const std::vector<float> v(E.build_ms, E.build_ms + 8);
 		return copy_host(v, 8, out, cap);
 	}
-	if (s == "cluster_coef") {   // the last iteration's per-cluster coefficient (0: inactive)
-		std::vector<float4> tmp(3 * (size_t)N);
-		if (copy_dev(E.rec.p, 3LL * N, tmp.data(), 3LL * N, E.stream) < 0) return -1;
+	if (s == "cluster_active") {   // 1 where the last iteration's cluster gave a record, else 0
+		std::vector<float4> tmp(2 * (size_t)N);
+		if (copy_dev(E.rec.p, 2LL * N, tmp.data(), 2LL * N, E.stream) < 0) return -1;
 		std::vector<float> v(N);
-		for (int r = 0; r < N; ++r) v[E.perm[r]] = tmp[3 * (size_t)r].w;
+		for (int r = 0; r < N; ++r) v[E.perm[r]] = std::isfinite(tmp[2 * (size_t)r + 1].z) ? 1.0f : 0.0f;
 		return copy_host(v, (long long)v.size(), out, cap);
 	}
 	if (s == "self_col") {

@@ -341,11 +341,22 @@ __device__ __forceinline__ bool cluster_j_sinv(const M3& Scur, float det_rest, f
 	return inverse3x3_safe(Sreg, Sinv, 1e-20f);
 }
 
-__device__ __forceinline__ void store_record(float4* rec, int idx, float3 c, float coef, const M3& S)
+// Cluster blackboard record, 36 bytes in two places so that a record read touches one
+// 32-byte sector plus a 4-byte entry: rec[2 i] = (M00, M11, M22, M01), rec[2 i + 1] =
+// (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float array after the 2N
+// float4.  A record the gather must skip (the reference's coef == 0) has c.x = NaN.
+__device__ __forceinline__ float* rec_cz(float4* rec, int n) { return reinterpret_cast<float*>(rec + 2 * (size_t)n); }
+__device__ __forceinline__ const float* rec_cz(const float4* rec, int n)
 {
-	rec[3 * idx + 0] = make_float4(c.x, c.y, c.z, coef);
-	rec[3 * idx + 1] = make_float4(S.m[0][0], S.m[1][1], S.m[2][2], S.m[1][0]);
-	rec[3 * idx + 2] = make_float4(S.m[2][0], S.m[2][1], 0.0f, 0.0f);
+	return reinterpret_cast<const float*>(rec + 2 * (size_t)n);
+}
+__device__ __forceinline__ void rec_invalidate(float4* rec, int idx) { rec[2 * idx + 1].z = __int_as_float(0x7fc00000); }
+__device__ __forceinline__ void store_record(float4* rec, int n, int idx, float3 c, float coef, const M3& S)
+{
+	if (coef == 0.0f) { rec_invalidate(rec, idx); return; }
+	rec[2 * idx + 0] = make_float4(coef * S.m[0][0], coef * S.m[1][1], coef * S.m[2][2], coef * S.m[1][0]);
+	rec[2 * idx + 1] = make_float4(coef * S.m[2][0], coef * S.m[2][1], c.x, c.y);
+	rec_cz(rec, n)[idx] = c.z;
 }
 
 // Kernel A on groups of S lanes per cluster (32/S clusters per warp).  Lane L of a group
@@ -469,17 +480,17 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_group(int n, const Step
 	}
 	const float denom = group_sum<S>(dsum);
 	if (sl != 0 || !in_range) return;
-	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	if (!valid) { rec_invalidate(rec, idx); return; }
 	const float dt = P->dt;
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const float alpha_t = P->vol_compliance / dt2;
 	const float den = denom + alpha_t;
-	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	if (!(den > 1e-12f)) { rec_invalidate(rec, idx); return; }
 	const float lam = read_lam ? lam_vol[idx] : 0.0f;
 	const float dl = (-C - alpha_t * lam) / den;
-	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, idx, c, dl * gs, Sinv);
+	store_record(rec, n, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A with static register slots: lane sl of an S-lane group owns members
@@ -599,17 +610,17 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_slots(int n, const Step
 	}
 	const float denom = group_sum<S>(dsum);
 	if (sl != 0 || !in_range) return;
-	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	if (!valid) { rec_invalidate(rec, idx); return; }
 	const float dt = P->dt;
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const float alpha_t = P->vol_compliance / dt2;
 	const float den = denom + alpha_t;
-	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	if (!(den > 1e-12f)) { rec_invalidate(rec, idx); return; }
 	const float lam = read_lam ? lam_vol[idx] : 0.0f;
 	const float dl = (-C - alpha_t * lam) / den;
-	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, idx, c, dl * gs, Sinv);
+	store_record(rec, n, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A with the members' positions staged in shared memory: pass 1 gathers each
@@ -736,17 +747,17 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 	}
 	const float denom = group_sum<S>(dsum);
 	if (sl != 0 || !in_range) return;
-	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	if (!valid) { rec_invalidate(rec, idx); return; }
 	const float dt = P->dt;
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const float alpha_t = P->vol_compliance / dt2;
 	const float den = denom + alpha_t;
-	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	if (!(den > 1e-12f)) { rec_invalidate(rec, idx); return; }
 	const float lam = read_lam ? lam_vol[idx] : 0.0f;
 	const float dl = (-C - alpha_t * lam) / den;
-	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, idx, c, dl * gs, Sinv);
+	store_record(rec, n, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A in one pass over the members (S lanes per cluster, members L, L+S, ... of
@@ -759,7 +770,8 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 // follow from them, so the member positions are read once and nothing is staged.
 // Members lie within a few graph spacings of their leader, which keeps the
 // cancellation in the moment form small; the result equals the two-pass form
-// (forward.cu:8531-8664) to FP32 rounding.
+// (forward.cu:8531-8664) to FP32 rounding.  The reference has the same leader-relative
+// moments in its optional one-pass warp kernel (forward.cu:8864-9033, warp mode 3).
 template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
@@ -824,7 +836,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	M3 Sinv;
 	m3_zero(Sinv);
 	if (valid) valid = cluster_j_sinv(Sm, __ldg(det_rest + idx), J, C, Sinv);
-	if (!valid) { rec[3 * idx].w = 0.0f; return; }
+	if (!valid) { rec_invalidate(rec, idx); return; }
 	const float gs = J * inv_n;
 	// W over members and leader (weight w_leader, d = 0)
 	const float wl = p4.w * ims;
@@ -850,12 +862,12 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	const float dt2 = fmaxf(dt * dt, 1e-8f);
 	const float alpha_t = P->vol_compliance / dt2;
 	const float den = denom + alpha_t;
-	if (!(den > 1e-12f)) { rec[3 * idx].w = 0.0f; return; }
+	if (!(den > 1e-12f)) { rec_invalidate(rec, idx); return; }
 	const float lam = read_lam ? lam_vol[idx] : 0.0f;
 	const float dl = (-C - alpha_t * lam) / den;
-	if (!isfinite(dl)) { rec[3 * idx].w = 0.0f; return; }
+	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, idx, c, dl * gs, Sinv);
+	store_record(rec, n, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
@@ -866,7 +878,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const Ste
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
-	rec[3 * idx].w = 0.0f;
+	rec_invalidate(rec, idx);
 	if (mat_type[idx] != 0) return;
 	const float4 p4 = ld4(pin, idx);
 	const float3 pi = f3(p4);
@@ -924,42 +936,29 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const Ste
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) return;
 	lam_vol[idx] = lam + dl;
-	store_record(rec, idx, c, dl * gs, Sinv);
+	store_record(rec, n, idx, c, dl * gs, Sinv);
 }
 
-// one blackboard record (already loaded) applied to a node (forward.cu:9212-9222)
-__device__ __forceinline__ bool gather_rec(float4 r0, float4 r1, float4 r2, float3 pi, float wi, float3& dp)
+// one blackboard record (already loaded) applied to a node (forward.cu:9212-9222):
+// dp = w coef Sinv (p - c), skipped where the cluster gave no record
+__device__ __forceinline__ bool gather_rec(float4 r0, float4 r1, float cz, float3 pi, float wi, float3& dp)
 {
-	const float coef = r0.w;
-	if (coef == 0.0f) return false;
-	M3 S;
-	S.m[0][0] = r1.x; S.m[1][1] = r1.y; S.m[2][2] = r1.z;
-	S.m[0][1] = S.m[1][0] = r1.w;
-	S.m[0][2] = S.m[2][0] = r2.x;
-	S.m[1][2] = S.m[2][1] = r2.y;
-	const float3 d = sub3(pi, make_float3(r0.x, r0.y, r0.z));
-	const float3 g = m3_mulv(S, d);
-	dp = make_float3(g.x * wi * coef, g.y * wi * coef, g.z * wi * coef);
+	if (!isfinite(r1.z)) return false;
+	M3 M;
+	M.m[0][0] = r0.x; M.m[1][1] = r0.y; M.m[2][2] = r0.z;
+	M.m[0][1] = M.m[1][0] = r0.w;
+	M.m[0][2] = M.m[2][0] = r1.x;
+	M.m[1][2] = M.m[2][1] = r1.y;
+	const float3 d = sub3(pi, make_float3(r1.z, r1.w, cz));
+	const float3 g = m3_mulv(M, d);
+	dp = make_float3(g.x * wi, g.y * wi, g.z * wi);
 	return fin3(dp);
 }
 
-// one blackboard record applied to a node (forward.cu:9212-9222)
-__device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, int i, float3 pi, float wi, float3& dp)
+__device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, int n, int i, float3 pi, float wi,
+	float3& dp)
 {
-	const float4 r0 = __ldg(rec + 3 * i);
-	const float coef = r0.w;
-	if (coef == 0.0f) return false;
-	const float4 r1 = __ldg(rec + 3 * i + 1);
-	const float4 r2 = __ldg(rec + 3 * i + 2);
-	M3 S;
-	S.m[0][0] = r1.x; S.m[1][1] = r1.y; S.m[2][2] = r1.z;
-	S.m[0][1] = S.m[1][0] = r1.w;
-	S.m[0][2] = S.m[2][0] = r2.x;
-	S.m[1][2] = S.m[2][1] = r2.y;
-	const float3 d = sub3(pi, make_float3(r0.x, r0.y, r0.z));
-	const float3 g = m3_mulv(S, d);
-	dp = make_float3(g.x * wi * coef, g.y * wi * coef, g.z * wi * coef);
-	return fin3(dp);
+	return gather_rec(__ldg(rec + 2 * i), __ldg(rec + 2 * i + 1), __ldg(rec_cz(rec, n) + i), pi, wi, dp);
 }
 
 __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl, float under_relax)
@@ -974,7 +973,7 @@ __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl,
 
 // Kernel B on groups of S lanes per node (forward.cu:9262-9323 with S = 32): mean over
 // the clusters that contain the node, step clamp 0.25 restLen, under-relaxation.  Reads
-// per node: h reverse indices + h gathered 48-byte records (L2-resident).
+// per node: h reverse indices + h gathered 36-byte records (L2-resident).
 template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
@@ -1004,17 +1003,19 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 	for (; k + S < cnt; k += 2 * S) {
 		const int i0 = __ldg(ridx + off + k), i1 = __ldg(ridx + off + k + S);
 		const bool ok0 = i0 >= 0 && i0 < n, ok1 = i1 >= 0 && i1 < n;
-		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, c0 = a0, a1 = a0, b1 = a0, c1 = a0;
-		if (ok0) { a0 = __ldg(rec + 3 * i0); b0 = __ldg(rec + 3 * i0 + 1); c0 = __ldg(rec + 3 * i0 + 2); }
-		if (ok1) { a1 = __ldg(rec + 3 * i1); b1 = __ldg(rec + 3 * i1 + 1); c1 = __ldg(rec + 3 * i1 + 2); }
+		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
+		float z0 = 0.0f, z1 = 0.0f;
+		const float* cz = rec_cz(rec, n);
+		if (ok0) { a0 = __ldg(rec + 2 * i0); b0 = __ldg(rec + 2 * i0 + 1); z0 = __ldg(cz + i0); }
+		if (ok1) { a1 = __ldg(rec + 2 * i1); b1 = __ldg(rec + 2 * i1 + 1); z1 = __ldg(cz + i1); }
 		float3 dp;
-		if (ok0 && gather_rec(a0, b0, c0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
-		if (ok1 && gather_rec(a1, b1, c1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
+		if (ok0 && gather_rec(a0, b0, z0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
+		if (ok1 && gather_rec(a1, b1, z1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 	}
 	if (k < cnt) {
 		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (i >= 0 && i < n && gather_one(rec, i, pi, wi, dp)) {
+		if (i >= 0 && i < n && gather_one(rec, n, i, pi, wi, dp)) {
 			sum = add3(sum, dp);
 			++received;
 		}
@@ -1047,7 +1048,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_thread(int n, const St
 		const int i = __ldg(ridx + k);
 		if (i < 0 || i >= n) continue;
 		float3 dp;
-		if (!gather_one(rec, i, pi, wi, dp)) continue;
+		if (!gather_one(rec, n, i, pi, wi, dp)) continue;
 		sum = add3(sum, dp);
 		++received;
 	}

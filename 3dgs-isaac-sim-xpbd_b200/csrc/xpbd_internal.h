@@ -11,8 +11,9 @@
 //                                              distance multiplier (updated in place)
 //   vol_off / vol_idx               cluster members (leader excluded), CSR over leaders
 //   rev_off / rev_idx               clusters containing each node (transposed CSR)
-//   rec                             float4[3N] cluster blackboard: (c.xyz, coef),
-//                                              (Sinv xx, yy, zz, xy), (Sinv xz, yz, -, -)
+//   rec                             float4[3N] cluster blackboard, 36 B used per cluster:
+//                                              float4[2N] (M xx, yy, zz, xy), (M xz, yz, c.x, c.y)
+//                                              with M = coef Sinv, then float[N] c.z; c.x = NaN: no record
 #pragma once
 #include <cuda_runtime.h>
 

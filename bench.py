@@ -170,8 +170,8 @@ def algorithmic_bytes(stage, sizes, n):
     rev = sizes[3] / n             # mean reverse-list length
     per = {
         "distance": 28 + 20 * m_dir,
-        "volume_solve": 4 * members + 56,
-        "volume_gather": 4 * rev + 80,
+        "volume_solve": 4 * members + 44,   # 36-byte cluster records
+        "volume_gather": 4 * rev + 68,
         "shape": 48 + 4 * m_dir + 32,   # + the warm-start eigenvector frame, read and written
         "project": 28,
         "predict": 52,
