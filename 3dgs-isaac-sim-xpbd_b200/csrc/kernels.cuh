@@ -3,8 +3,8 @@
 // Every kernel restates one stage of the reference step (runXPBDSimulation,
 // forward.cu:12038-12751) with the same arithmetic order, so results stay within
 // FP32 rounding of the reference; the data layout is this library's own (float4
-// positions with the inverse mass in w, blackboard records as three float4, CSR row
-// starts with an N+1 sentinel, in-place distance multipliers).  None of these stages
+// positions with the inverse mass in w, 36-byte blackboard records, CSR row starts with
+// an N+1 sentinel, in-place distance multipliers).  None of these stages
 // is a dense contraction, so none uses tensor cores; each is bounded by HBM or L2
 // bandwidth (see the per-kernel notes).
 #pragma once
