@@ -91,3 +91,17 @@ def test_batched_partition_gloo():
     assert flat == list(range(len(cost)))
     loads = [sum(cost[k] for k in p) for p in parts]
     assert max(loads) - min(loads) <= max(cost)
+
+
+def test_render_reference_arm_prints_one_line():
+    """`--impl reference --config render`: the CPU restatement times one small frame of
+    the splatting workload and prints the contract's JSON line."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--config", "render",
+           "--gaussians", "3000", "--steps", "1", "--warmup", "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "frames/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["d2h_bytes_per_step"] == 0
