@@ -264,16 +264,18 @@ class XPBD:
         return m.value, s.value
 
     # ---- ChainMail (forward.cu:12808-13006; not in the reference C ABI) ----
-    # The product exports xpbd_b200_chainmail_*, the oracle oracle_chainmail_* and the
-    # reference shim refshim_chainmail_*; the first present is used.
+    # entry points xpbd_b200_chainmail_*; a subclass binding another library with the
+    # same signatures under another prefix sets CHAINMAIL_PREFIX
+    CHAINMAIL_PREFIX = "xpbd_b200_"
+
     def _cm(self, name, argtypes, restype):
-        for prefix in ("xpbd_b200_", "oracle_", "refshim_"):
-            f = getattr(self.raw, prefix + name, None)
-            if f is not None:
-                f.argtypes = argtypes       # on the ctypes function; self.lib may be an engine proxy
-                f.restype = restype
-                return prefix, getattr(self.lib, prefix + name)
-        raise AttributeError(f"{self.path} has no ChainMail entry point {name}")
+        prefix = self.CHAINMAIL_PREFIX
+        f = getattr(self.raw, prefix + name, None)
+        if f is None:
+            raise AttributeError(f"{self.path} has no ChainMail entry point {prefix}{name}")
+        f.argtypes = argtypes       # on the ctypes function; self.lib may be an engine proxy
+        f.restype = restype
+        return prefix, getattr(self.lib, prefix + name)
 
     def chainmail_set_material(self, global_scale=1.0, air=0.1, skin=0.1, bone=0.1, use_edge_stiffness=True,
                                edge_influence=1.0):
@@ -295,13 +297,8 @@ class XPBD:
     def chainmail_times(self):
         """Arrival times (N,), 1e9 where the wave has not arrived."""
         out = np.zeros(max(self.n, 1), np.float32)
-        if hasattr(self.raw, "refshim_float") and not hasattr(self.raw, "xpbd_b200_chainmail_times"):
-            self.raw.refshim_float.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong]
-            self.raw.refshim_float.restype = ctypes.c_int
-            got = self.lib.refshim_float(b"cm_time", out.ctypes.data, out.size)
-        else:
-            _, f = self._cm("chainmail_times", [ctypes.c_void_p, ctypes.c_int], ctypes.c_int)
-            got = f(out.ctypes.data, out.size)
+        _, f = self._cm("chainmail_times", [ctypes.c_void_p, ctypes.c_int], ctypes.c_int)
+        got = f(out.ctypes.data, out.size)
         if got != self.n:
             raise RuntimeError(f"chainmail_times: {self.last_error()}")
         return out[:self.n]
@@ -389,4 +386,84 @@ class XPBD:
         self.destroy()
         if self.handle:
             self.raw.xpbd_b200_engine_free(self.handle)
+            self.handle = None
+
+
+class Arena:
+    """A serving arena (xpbd_b200_arena_*): many sessions resident in one engine's buffers
+    and advanced together, one launch sequence per substep.  Capacities are in rows
+    (Gaussians), directed graph edges, cluster members and reverse-list entries.  A
+    session joins with ``admit(solver)`` — an ``XPBD(instance=True)`` engine that has built
+    its scene and taken its first step — and leaves with ``retire(slot)``; all sessions
+    must share the solver settings."""
+
+    def __init__(self, dll_path, rows, edges, members, rev):
+        L = load(dll_path)
+        L.xpbd_b200_arena_new.argtypes = [ctypes.c_longlong] * 4
+        L.xpbd_b200_arena_new.restype = ctypes.c_void_p
+        L.xpbd_b200_arena_admit.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.xpbd_b200_arena_retire.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.xpbd_b200_arena_step.argtypes = ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 4
+                                           + [ctypes.c_float] * 2 + [ctypes.c_int] + [ctypes.c_void_p] * 3)
+        L.xpbd_b200_arena_positions.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        L.xpbd_b200_arena_sync.argtypes = [ctypes.c_void_p]
+        L.xpbd_b200_arena_usage.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.xpbd_b200_arena_free.argtypes = [ctypes.c_void_p]
+        L.xpbd_b200_arena_free.restype = None
+        self.lib = L
+        self.handle = L.xpbd_b200_arena_new(int(rows), int(edges), int(members), int(rev))
+        if not self.handle:
+            raise RuntimeError(f"xpbd_b200_arena_new: {L.xpbd_last_error().decode(errors='replace')}")
+
+    def _err(self, what):
+        return RuntimeError(f"{what}: {self.lib.xpbd_last_error().decode(errors='replace')}")
+
+    def admit(self, solver):
+        """The session's slot, or None when it does not fit (retire sessions first)."""
+        slot = self.lib.xpbd_b200_arena_admit(self.handle, solver.handle)
+        if slot == -2:
+            return None
+        if slot < 0:
+            raise self._err("xpbd_b200_arena_admit")
+        return slot
+
+    def retire(self, slot):
+        if self.lib.xpbd_b200_arena_retire(self.handle, int(slot)) != 0:
+            raise self._err("xpbd_b200_arena_retire")
+
+    def step(self, k, types, poses, dims, col_slot, pin_slot, pin_idx, targets, margin=0.0, friction=0.0):
+        """Enqueue k substeps of every live session: colliders ``types`` (C,), ``poses``
+        (k, C, 12), ``dims`` (C, 3) acting on the sessions ``col_slot`` (C,); pins of
+        session ``pin_slot`` (P,), Gaussian ``pin_idx`` (P,, the session's own order) at
+        ``targets`` (k, P, 3)."""
+        a = [np.ascontiguousarray(types, np.int32), np.ascontiguousarray(poses, np.float32),
+             np.ascontiguousarray(dims, np.float32), np.ascontiguousarray(col_slot, np.int32),
+             np.ascontiguousarray(pin_slot, np.int32), np.ascontiguousarray(pin_idx, np.int32),
+             np.ascontiguousarray(targets, np.float32)]
+        rc = self.lib.xpbd_b200_arena_step(self.handle, int(k), len(a[0]), a[0].ctypes.data, a[1].ctypes.data,
+                                           a[2].ctypes.data, a[3].ctypes.data, float(margin), float(friction),
+                                           len(a[4]), a[4].ctypes.data, a[5].ctypes.data, a[6].ctypes.data)
+        if rc != 0:
+            raise self._err("xpbd_b200_arena_step")
+
+    def positions(self, slot, n):
+        out = np.empty((n, 3), np.float32)
+        if self.lib.xpbd_b200_arena_positions(self.handle, int(slot), out.ctypes.data, int(n)) != 0:
+            raise self._err("xpbd_b200_arena_positions")
+        return out
+
+    def sync(self):
+        if self.lib.xpbd_b200_arena_sync(self.handle) != 0:
+            raise self._err("xpbd_b200_arena_sync")
+
+    def usage(self):
+        """rows used / capacity, edges, members, reverse entries, live Gaussians, sessions."""
+        out = np.zeros(10, np.int64)
+        self.lib.xpbd_b200_arena_usage(self.handle, out.ctypes.data)
+        keys = ("rows", "rows_cap", "edges", "edges_cap", "members", "members_cap", "rev", "rev_cap", "live", "sessions")
+        return dict(zip(keys, (int(v) for v in out)))
+
+    def close(self):
+        if self.handle:
+            self.lib.xpbd_b200_arena_free(self.handle)
             self.handle = None

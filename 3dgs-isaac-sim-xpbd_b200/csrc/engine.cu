@@ -19,6 +19,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -79,6 +80,10 @@ template <typename T>
 struct DBuf {
 	T* p = nullptr;
 	size_t n = 0;
+	DBuf() = default;
+	DBuf(const DBuf&) = delete;
+	DBuf& operator=(const DBuf&) = delete;
+	~DBuf() { release(); }
 	cudaError_t alloc(size_t count)
 	{
 		release();
@@ -252,8 +257,18 @@ public:
 	DBuf<float> gs_rest, gs_stiff, gs_lam;
 	DBuf<unsigned int> sc_keys;
 	DBuf<int> sc_bucket, sc_start, sc_cursor, sc_idx_sorted, sc_contacts, sc_counts, sc_block_sums, d_obj_id;
+	DBuf<int> sc_fix;                // particles whose candidate lists reached the cap
 	DBuf<float4> sc_dp, sc_sp, sc_sr, sc_sx;
 	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
+	// ellipsoid contact shapes (xpbd_set_contact_shape; forward.cu:150-160, 6733-6757):
+	// bit 1 colliders, bit 2 ground; per Gaussian M = k^2 Sigma (two float4), the longest
+	// semi-axis and the per-step support radius along the ground normal.  Like the
+	// reference's (xpbd_capi.cu:55-56) the setting ends with the scene.
+	int contact_bits = 0;
+	float contact_tau = 0.2f, contact_cap = 0.0f;
+	bool contact_packed = false;
+	DBuf<float> d_opacity, c_rmax, c_rg;
+	DBuf<float4> c_shape;
 	DBuf<int> d_perm;
 	DBuf<KinCollider> d_kin_ext;
 	DBuf<int2> d_kin_range;
@@ -336,8 +351,11 @@ public:
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
 		sc_contacts.release(); sc_counts.release(); sc_block_sums.release(); d_obj_id.release(); sc_dp.release();
+		sc_fix.release();
 		sc_sp.release(); sc_sr.release(); sc_sx.release();
 		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
+		d_opacity.release(); c_rmax.release(); c_rg.release(); c_shape.release();
+		contact_packed = false;
 		att_idx.release(); att_pos.release(); d_perm.release(); d_kin_ext.release(); d_kin_range.release();
 		rs.release();
 		att_active = false;
@@ -533,10 +551,14 @@ public:
 		{
 			const auto sc = to_internal(in_scales.data(), 3);
 			const auto rt = to_internal(in_rots.data(), 4);
+			const auto op = to_internal(in_opacity.data(), 1);
+			CK(d_opacity.alloc(n));
 			CK(cudaMemcpyAsync(d_scales.p, sc.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
 			CK(cudaMemcpyAsync(d_rots.p, rt.data(), sizeof(float) * 4 * n, cudaMemcpyHostToDevice, stream));
+			CK(cudaMemcpyAsync(d_opacity.p, op.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream));
 			CK(cudaStreamSynchronize(stream));
 		}
+		if (contact_bits && pack_contact(false)) return -1;   // set before the scene was on the device
 		CK(det_rest.alloc(n)); CK(v_rest.alloc(n)); CK(rest_len.alloc(n)); CK(sigma_rest.alloc(6 * (size_t)n));
 		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * (size_t)n));
 		CK(cudaMemsetAsync(rec.p, 0xff, rec.bytes(), stream));   // every record NaN: no record yet
@@ -679,6 +701,24 @@ public:
 		obj_shift_valid = false;
 		return sync();
 	}
+
+	// updateContactShapes (forward.cu:6739-6757): pack every Gaussian's contact ellipsoid
+	// from the created shapes (internal order) or from the last deformed shapes that
+	// xpbd_compute_shapes wrote (caller order)
+	int pack_contact(bool deformed)
+	{
+		if (!c_shape.p) { CK(c_shape.alloc(2 * (size_t)n)); CK(c_rmax.alloc(n)); CK(c_rg.alloc(n)); }
+		const float cap = (std::isfinite(contact_cap) && contact_cap > 0.0f) ? contact_cap : 0.0f;
+		dev::k_contact_pack<<<blocks_for(n), kBlock, 0, stream>>>(n, deformed ? d_out_scales.p : d_scales.p,
+			deformed ? d_out_quats.p : d_rots.p, deformed ? d_perm.p : (const int*)nullptr, d_opacity.p, contact_tau,
+			cap, c_shape.p, c_rmax.p);
+		CK(cudaGetLastError());
+		contact_packed = true;
+		return 0;
+	}
+	// runXPBDSimulation's contactOn (forward.cu:12223-12228, 12550)
+	bool contact_col() const { return (contact_bits & 1) && contact_packed; }
+	bool contact_ground() const { return (contact_bits & 2) && contact_packed && S.ground_on; }
 
 	bool object_on() const { return S.object_shape > 0.0f && num_objects > 0; }
 	// the self-collision build keeps only Gaussians near another object (forward.cu:11808-11816)
@@ -853,7 +893,7 @@ public:
 		const int buckets = table + 1;   // + sentinel bucket
 		CK(sc_keys.alloc(n)); CK(sc_bucket.alloc(buckets + 1)); CK(sc_start.alloc(buckets + 1));
 		CK(sc_cursor.alloc(buckets)); CK(sc_idx_sorted.alloc(n)); CK(sc_contacts.alloc((size_t)n * kSelfColMax));
-		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
+		CK(sc_counts.alloc(n)); CK(sc_fix.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
 		CK(cudaMemsetAsync(sc_counts.p, 0, sc_counts.bytes(), stream));
 		return 0;
 	}
@@ -951,6 +991,10 @@ public:
 		P.sc_single_object = single_object ? 1 : 0;
 	}
 
+	// the c.z column of the cluster records (after the 2 x rows float4 of M and c.xy; rows =
+	// the scene's Gaussians, or an arena's capacity)
+	float* recz() const { return reinterpret_cast<float*>(rec.p + 2 * (size_t)(arena ? rows_cap : n)); }
+
 	bool use_warp() const
 	{
 		if (S.warp_mode == 2) return true;
@@ -967,7 +1011,7 @@ public:
 			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
-			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push() };
+			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -1001,14 +1045,20 @@ public:
 		return dim3((unsigned)((items + per_block - 1) / per_block));
 	}
 
-	void enqueue_sc_candidates(dim3 G, dim3 B, const unsigned char* active)
+	// candidate lists: cell-ordered copies, the warp-per-home-cell build, then the
+	// sequential replacement rule for the particles that reached the cap
+	void enqueue_sc_candidates(dim3 G, dim3 B)
 	{
 		launch(ST_SC_BUILD, G, B, dev::k_sc_pack, n, (const int*)sc_idx_sorted.p, (const float4*)pos_curr.p,
 			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)d_obj_id.p, sc_sp.p, sc_sr.p, sc_sx.p);
-		launch(ST_SC_BUILD, G, B, dev::k_sc_build_sorted, n, (const StepParams*)d_params, (const float4*)pos_curr.p,
-			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p, (const int*)sc_start.p,
+		launch(ST_SC_BUILD, G, B, dev::k_sc_build_cells, n, (const StepParams*)d_params, (const unsigned*)sc_keys.p,
+			(const int*)sc_idx_sorted.p, (const int*)sc_start.p, (unsigned)(sc_table - 1), (unsigned)sc_table,
+			(const float4*)sc_sp.p, (const float4*)sc_sr.p, (const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p,
+			sc_fix.p);
+		launch(ST_SC_BUILD, dim3(148), B, dev::k_sc_fixup, (const int*)sc_fix.p, (const StepParams*)d_params,
+			(const float4*)pos_curr.p, (const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_start.p,
 			(unsigned)(sc_table - 1), (const int*)d_obj_id.p, (const float4*)sc_sp.p, (const float4*)sc_sr.p,
-			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p, active);
+			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p);
 	}
 
 	// volume kernel shapes: lanes per cluster (Kernel A) and per node (Kernel B);
@@ -1036,8 +1086,12 @@ public:
 		const dim3 GW = blocks_for((long long)N * 32);   // one warp per Gaussian / cluster
 		const bool sc = selfcol_on();
 		CK(cudaMemsetAsync(d_ctr, 0, offsetof(DevCounters, jstats), stream));
+		const bool cc = contact_col(), cg = contact_ground();
+		const float4* cshape = (cc || cg) ? (const float4*)c_shape.p : (const float4*)nullptr;
+		const float* crmax = cc ? (const float*)c_rmax.p : (const float*)nullptr;
+		const float* crg = cg ? (const float*)c_rg.p : (const float*)nullptr;
 		launch(ST_PREDICT, G, B, dev::k_predict, N, (const StepParams*)d_params, (const float4*)pos_curr.p, pos_next.p,
-			vel.p, S.use_volume ? lam_vol.p : (float*)nullptr);
+			vel.p, S.use_volume ? lam_vol.p : (float*)nullptr, cshape, cg ? c_rg.p : (float*)nullptr);
 		if (object_on()) enqueue_object_step(G, B);
 		const unsigned char* active = sc_limited() ? (const unsigned char*)sc_active.p : nullptr;
 		if (sc) {
@@ -1062,7 +1116,7 @@ public:
 				sc_cursor.p, sc_idx_sorted.p);
 			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
 				sc_idx_sorted.p, (const int*)d_perm.p);
-			enqueue_sc_candidates(G, B, active);
+			enqueue_sc_candidates(G, B);
 			if (obj_push()) CK(cudaMemsetAsync(sc_accum.p, 0, sc_accum.bytes(), stream));
 		}
 		float4* pin = pos_next.p;
@@ -1106,42 +1160,42 @@ public:
 						// automatic: one pass over the members (any count), 4 lanes per cluster
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_onepass<4>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 32)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 32), B, dev::k_volume_solve_group<32, 8>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
-							lam_vol.p, rec.p, rl);
+							lam_vol.p, rec.p, recz(), rl);
 					else if (la == 8)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 8), B, dev::k_volume_solve_slots<8, 8, true>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 4)   // 4 lanes, members staged in shared memory (two-pass sums)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4, dev::kSmemBlock), dim3(dev::kSmemBlock),
 							dev::k_volume_solve_smem<4, 16>, N, dp, cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p,
-							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 3)   // 4 lanes, positions re-read from L1 instead of shared memory
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_slots<4, 16, false>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 2)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 2), B, dev::k_volume_solve_slots<2, 32, false>, N, dp,
 							cpin, (const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
-							(const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else
 						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
-							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, rl);
+							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					if (lb == 32)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 8)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B, dev::k_volume_gather_group<4>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
-							(const int*)rev_idx.p, (const float4*)rec.p, (const float*)rest_len.p);
+							(const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					std::swap(pin, pout);
 				}
 			}
@@ -1165,7 +1219,8 @@ public:
 				launch(ST_PROJECT, G, B, dev::k_project, N, (const StepParams*)d_params, pin, (const float4*)pos_curr.p,
 					sc ? (const int*)sc_counts.p : (const int*)nullptr, (const float4*)sc_dp.p, d_ctr, last ? 1 : 0,
 					(const int*)d_obj_id.p, S.kin_ext.empty() ? (const KinCollider*)nullptr : (const KinCollider*)d_kin_ext.p,
-					(const int2*)d_kin_range.p, (const float4*)sc_cross.p, obj_push() ? sc_accum.p : (float4*)nullptr);
+					(const int2*)d_kin_range.p, (const float4*)sc_cross.p, obj_push() ? sc_accum.p : (float4*)nullptr,
+					cshape, crmax, crg);
 		}
 		if (obj_push()) {   // contact push (forward.cu:12587-12597)
 			const int K = num_objects;
@@ -1175,10 +1230,10 @@ public:
 			launch(ST_PROJECT, dim3((K + 63) / 64), dim3(64), dev::k_obj_push_solve, (int)G.x, K,
 				(const float*)push_partial.p, (const DevCounters*)d_ctr, S.object_shape, push_T.p);
 			launch(ST_PROJECT, G, B, dev::k_obj_push_apply, N, (const StepParams*)d_params, (const int*)d_obj_id.p,
-				(const float4*)sc_accum.p, (const float*)push_T.p, (const DevCounters*)d_ctr, pin);
+				(const float4*)sc_accum.p, (const float*)push_T.p, (const DevCounters*)d_ctr, pin, crg);
 		}
 		launch(ST_VELOCITY, G, B, dev::k_velocity, N, (const StepParams*)d_params, pos_curr.p, (const float4*)pin,
-			vel.p, pos_out3.p, (const int*)d_perm.p);
+			vel.p, pos_out3.p, (const int*)d_perm.p, crg);
 		if (S.jstats) {
 			CK(cudaMemsetAsync(d_ctr->jstats, 0, sizeof(double) * 3, stream));
 			launch(ST_JSTATS, G, B, dev::k_jstats, N, (const float4*)pos_curr.p, (const int*)vol_off.p,
@@ -1264,10 +1319,306 @@ public:
 		event_next = 0;
 	}
 
+	// ------------------------------------------------------------------ serving arena
+	// Many independent sessions resident in one engine's buffers and advanced by one
+	// launch sequence (one graph replay) per substep.  A session is a scene built and
+	// stepped once by an engine of its own; admission copies its state and topology into
+	// the next free rows, edges, members and reverse entries (every array is filled in
+	// admission order, so each CSR stays monotone), shifting its indices by the segment's
+	// bases.  Retirement freezes the rows in place (inverse mass 0, velocity 0: no kernel
+	// moves them and no live row refers to them); trailing retired segments are dropped,
+	// and when the tail is full the live segments are moved down (compaction).  Every
+	// kernel works per row, per cluster or per edge, and each session's colliders act on
+	// its rows only (per-slot ranges of the batched collider list), so a session's
+	// trajectory in the arena is the one it has alone, bit for bit.
+	struct ArenaSeg {
+		int slot = -1, row0 = 0, rows = 0;
+		long long e0 = 0, ne = 0, m0 = 0, nm = 0, r0 = 0, nr = 0;
+		bool live = false;
+		std::vector<int> inv;   // session caller index -> row within the segment
+	};
+	bool arena = false;
+	std::vector<ArenaSeg> segs;
+	int rows_cap = 0, rows_used = 0, next_slot = 0;
+	long long e_cap = 0, m_cap = 0, r_cap = 0, e_used = 0, m_used = 0, r_used = 0;
+
+	int arena_init(long long rows, long long edges, long long members, long long rev)
+	{
+		if (rows <= 0 || rows > INT_MAX - 1 || edges <= 0 || members <= 0 || rev <= 0 || edges > INT_MAX ||
+			members > INT_MAX || rev > INT_MAX)
+			return fail("xpbd_b200_arena_new: invalid capacity (each of rows, edges, members, reverse entries "
+				"1..2^31-1: the CSR offsets are 32-bit)");
+		if (ensure_stream()) return -1;
+		arena = true;
+		rows_cap = (int)rows; e_cap = edges; m_cap = members; r_cap = rev;
+		const size_t R = (size_t)rows;
+		CK(pos_curr.alloc(R)); CK(pos_next.alloc(R)); CK(pos_tmp.alloc(R)); CK(vel.alloc(R)); CK(pos_rest.alloc(R));
+		CK(shape_rest.alloc(R)); CK(shape_q.alloc(R)); CK(pos_out3.alloc(3 * R)); CK(d_perm.alloc(R));
+		CK(d_obj_id.alloc(R)); CK(lam_vol.alloc(R)); CK(det_rest.alloc(R)); CK(rest_len.alloc(R));
+		CK(mat_type.alloc(R)); CK(rec.alloc(3 * R)); CK(inv_mass_saved.alloc(R));
+		CK(off.alloc(R + 1)); CK(vol_off.alloc(R + 1)); CK(rev_off.alloc(R + 1));
+		CK(nbr.alloc((size_t)edges)); CK(ndist.alloc((size_t)edges)); CK(nstiff.alloc((size_t)edges));
+		CK(lam.alloc((size_t)edges)); CK(vol_idx_s.alloc((size_t)members)); CK(rev_idx_s.alloc((size_t)rev));
+		CK(cudaMemsetAsync(off.p, 0, sizeof(int), stream));
+		CK(cudaMemsetAsync(vol_off.p, 0, sizeof(int), stream));
+		CK(cudaMemsetAsync(rev_off.p, 0, sizeof(int), stream));
+		CK(cudaMemsetAsync(rec.p, 0xff, rec.bytes(), stream));
+		n = 0;
+		built = true;
+		stepped = true;
+		return sync();
+	}
+
+	// the settings every session of an arena must share (the launch sequence is common)
+	static bool same_step_settings(const Settings& a, const Settings& b)
+	{
+		return a.iters == b.iters && a.dt == b.dt && a.under_relax == b.under_relax && a.vel_damping == b.vel_damping &&
+			a.stiffness_scale == b.stiffness_scale && a.inv_mass_scale == b.inv_mass_scale &&
+			a.dist_compliance == b.dist_compliance && a.shape_compliance == b.shape_compliance &&
+			a.shape_blend == b.shape_blend && a.use_distance == b.use_distance && a.use_shape == b.use_shape &&
+			a.use_volume == b.use_volume && a.shape_robust == b.shape_robust && a.vol_compliance == b.vol_compliance &&
+			a.dist_gs == b.dist_gs && a.vol_gs == b.vol_gs && a.warp_mode == b.warp_mode && a.lanes_a == b.lanes_a &&
+			a.lanes_b == b.lanes_b && a.ground_on == b.ground_on && a.object_shape == b.object_shape &&
+			a.sc_enabled == b.sc_enabled;
+	}
+
+	// copy `count` elements of src into dst + at, adding `delta` to every non-negative entry
+	int copy_shift(const int* src, int* dst, long long count, int delta)
+	{
+		if (count <= 0) return 0;
+		dev::k_copy_shift<<<(unsigned)((count + kBlock - 1) / kBlock), kBlock, 0, stream>>>(count, src, dst, delta);
+		CK(cudaGetLastError());
+		return 0;
+	}
+
+	template <typename T>
+	int copy_d2d(T* dst, const T* src, size_t count)
+	{
+		if (count) CK(cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyDeviceToDevice, stream));
+		return 0;
+	}
+
+	// admits a built and stepped session engine; returns its slot, -2 when it does not fit
+	int arena_admit(Engine& src)
+	{
+		if (!arena) return fail("xpbd_b200_arena_admit: not an arena");
+		if (&src == this || src.arena || !src.built || !src.stepped || src.n <= 0)
+			return fail("xpbd_b200_arena_admit: the session must be a built and stepped scene");
+		const Settings& t = src.S;
+		if (t.sc_enabled || t.ground_on || t.object_shape > 0.0f || t.dist_gs || t.vol_gs || t.use_angle ||
+			src.contact_bits || (t.use_volume && src.vol_lanes() != 4) || (t.use_volume && src.gather_lanes() != 4))
+			return fail("xpbd_b200_arena_admit: sessions step with Jacobi distance and volume (4-lane kernels), "
+				"shape matching and colliders; self-collision, ground, object shape and contact shapes stay off");
+		bool any_live = false;
+		for (const auto& g : segs) any_live = any_live || g.live;
+		if (any_live && !same_step_settings(S, t))
+			return fail("xpbd_b200_arena_admit: the session's solver settings differ from the arena's");
+		const int rows = src.n;
+		const long long ne = src.graph.off[rows], nm = src.clusters.vol_off[rows], nr = src.clusters.rev_off[rows];
+		auto fits = [&]() {
+			return rows_used + (long long)rows <= rows_cap && e_used + ne <= e_cap && m_used + nm <= m_cap &&
+				r_used + nr <= r_cap;
+		};
+		if (!fits() && arena_compact()) return -1;
+		if (!fits()) return -2;
+		if (!any_live) {
+			const auto kin = S.kin_ext;
+			S = t;
+			S.kin_ext = kin;
+			S.kin_count = 0;
+			S.jstats = false;
+			S.topo_dirty = false;
+			S.use_graph = true;
+		}
+		if (src.sync()) return -1;
+		ArenaSeg g;
+		g.slot = next_slot++;
+		g.row0 = rows_used; g.rows = rows;
+		g.e0 = e_used; g.ne = ne; g.m0 = m_used; g.nm = nm; g.r0 = r_used; g.nr = nr;
+		g.live = true;
+		g.inv = src.inv;
+		const size_t r0 = (size_t)g.row0;
+		if (copy_d2d(pos_curr.p + r0, src.pos_curr.p, rows) || copy_d2d(vel.p + r0, src.vel.p, rows) ||
+			copy_d2d(pos_rest.p + r0, src.pos_rest.p, rows) || copy_d2d(shape_rest.p + r0, src.shape_rest.p, rows) ||
+			copy_d2d(shape_q.p + r0, src.shape_q.p, rows) || copy_d2d(pos_out3.p + 3 * r0, src.pos_out3.p, 3 * (size_t)rows) ||
+			copy_d2d(det_rest.p + r0, src.det_rest.p, rows) || copy_d2d(rest_len.p + r0, src.rest_len.p, rows) ||
+			copy_d2d(mat_type.p + r0, src.mat_type.p, rows) ||
+			copy_d2d(ndist.p + g.e0, src.ndist.p, (size_t)ne) || copy_d2d(nstiff.p + g.e0, src.nstiff.p, (size_t)ne))
+			return -1;
+		if (copy_shift(src.d_perm.p, d_perm.p + r0, rows, g.row0) ||
+			copy_shift(src.off.p, off.p + r0, rows + 1, (int)g.e0) || copy_shift(src.nbr.p, nbr.p + g.e0, ne, g.row0) ||
+			copy_shift(src.vol_off.p, vol_off.p + r0, rows + 1, (int)g.m0) ||
+			copy_shift(src.vol_idx_s.p, vol_idx_s.p + g.m0, nm, g.row0) ||
+			copy_shift(src.rev_off.p, rev_off.p + r0, rows + 1, (int)g.r0) ||
+			copy_shift(src.rev_idx_s.p, rev_idx_s.p + g.r0, nr, g.row0))
+			return -1;
+		dev::k_fill_int<<<blocks_for(rows), kBlock, 0, stream>>>(rows, d_obj_id.p + r0, g.slot);
+		// the inverse masses a pin release restores: the session's own saved ones while it
+		// has pins, else its current ones
+		if (src.att_active && src.inv_mass_saved.p) {
+			if (copy_d2d(inv_mass_saved.p + r0, src.inv_mass_saved.p, rows)) return -1;
+		}
+		else
+			dev::k_get_w<<<blocks_for(rows), kBlock, 0, stream>>>(rows, pos_curr.p + r0, inv_mass_saved.p + r0);
+		CK(cudaGetLastError());
+		// the session's colliders of its last step are the previous poses of its slot's
+		for (int c = 0; c < t.kin_count; ++c) {
+			KinCollider K = t.kin[c];
+			K.obj = g.slot;
+			col_prev[col_key(g.slot, c)] = K;
+		}
+		rows_used += rows; e_used += ne; m_used += nm; r_used += nr;
+		n = rows_used;
+		segs.push_back(std::move(g));
+		++generation;
+		if (sync()) return -1;
+		return segs.back().slot;
+	}
+
+	ArenaSeg* arena_seg(int slot)
+	{
+		for (auto& g : segs)
+			if (g.slot == slot && g.live) return &g;
+		return nullptr;
+	}
+
+	int arena_retire(int slot)
+	{
+		ArenaSeg* g = arena_seg(slot);
+		if (!g) return fail("xpbd_b200_arena_retire: no live session in slot %d", slot);
+		dev::k_freeze_rows<<<blocks_for(g->rows), kBlock, 0, stream>>>(g->rows, pos_curr.p + g->row0, vel.p + g->row0,
+			inv_mass_saved.p + g->row0);
+		CK(cudaGetLastError());
+		g->live = false;
+		while (!segs.empty() && !segs.back().live) {
+			const ArenaSeg& b = segs.back();
+			rows_used = b.row0; e_used = b.e0; m_used = b.m0; r_used = b.r0;
+			segs.pop_back();
+		}
+		n = rows_used;
+		++generation;
+		return 0;
+	}
+
+	// moves the live segments down over the retired ones (through a staging buffer, since
+	// source and destination may overlap) and shifts their indices
+	int arena_compact()
+	{
+		if (sync()) return -1;
+		size_t stage_bytes = 0;
+		for (const auto& g : segs)
+			if (g.live)
+				stage_bytes = std::max(stage_bytes, std::max({ sizeof(float4) * (size_t)g.rows, sizeof(float) * 3 * (size_t)g.rows,
+					sizeof(int) * (size_t)(g.rows + 1), sizeof(int) * (size_t)g.ne, sizeof(int) * (size_t)g.nm,
+					sizeof(int) * (size_t)g.nr }));
+		DBuf<unsigned char> stage;
+		if (stage_bytes) CK(stage.alloc(stage_bytes));
+		auto move = [&](void* base, size_t elem, long long from, long long to, long long count) -> int {
+			if (from == to || count <= 0) return 0;
+			unsigned char* b = static_cast<unsigned char*>(base);
+			CK(cudaMemcpyAsync(stage.p, b + elem * from, elem * count, cudaMemcpyDeviceToDevice, stream));
+			CK(cudaMemcpyAsync(b + elem * to, stage.p, elem * count, cudaMemcpyDeviceToDevice, stream));
+			return 0;
+		};
+		auto move_shift = [&](int* base, long long from, long long to, long long count, int delta) -> int {
+			if (count <= 0 || (from == to && delta == 0)) return 0;
+			CK(cudaMemcpyAsync(stage.p, base + from, sizeof(int) * count, cudaMemcpyDeviceToDevice, stream));
+			return copy_shift(reinterpret_cast<const int*>(stage.p), base + to, count, delta);
+		};
+		std::vector<ArenaSeg> kept;
+		int rows = 0;
+		long long e = 0, m = 0, r = 0;
+		for (auto& g : segs) {
+			if (!g.live) continue;
+			const int dr = rows - g.row0;
+			const long long de = e - g.e0, dm = m - g.m0, drv = r - g.r0;
+			if (dr || de || dm || drv) {
+				const long long a = g.row0, b = rows, k = g.rows;
+				if (move(pos_curr.p, sizeof(float4), a, b, k) || move(vel.p, sizeof(float4), a, b, k) ||
+					move(pos_rest.p, sizeof(float4), a, b, k) || move(shape_rest.p, sizeof(float4), a, b, k) ||
+					move(shape_q.p, sizeof(float4), a, b, k) || move(pos_out3.p, 3 * sizeof(float), a, b, k) ||
+					move(det_rest.p, sizeof(float), a, b, k) || move(rest_len.p, sizeof(float), a, b, k) ||
+					move(inv_mass_saved.p, sizeof(float), a, b, k) || move(mat_type.p, sizeof(int), a, b, k) ||
+					move(d_obj_id.p, sizeof(int), a, b, k) || move(ndist.p, sizeof(float), g.e0, e, g.ne) ||
+					move(nstiff.p, sizeof(float), g.e0, e, g.ne))
+					return -1;
+				if (move_shift(d_perm.p, a, b, k, dr) || move_shift(off.p, a, b, k + 1, (int)de) ||
+					move_shift(nbr.p, g.e0, e, g.ne, dr) || move_shift(vol_off.p, a, b, k + 1, (int)dm) ||
+					move_shift(vol_idx_s.p, g.m0, m, g.nm, dr) || move_shift(rev_off.p, a, b, k + 1, (int)drv) ||
+					move_shift(rev_idx_s.p, g.r0, r, g.nr, dr))
+					return -1;
+				g.row0 = rows; g.e0 = e; g.m0 = m; g.r0 = r;
+			}
+			rows += g.rows; e += g.ne; m += g.nm; r += g.nr;
+			kept.push_back(std::move(g));
+		}
+		segs.swap(kept);
+		rows_used = rows; e_used = e; m_used = m; r_used = r;
+		n = rows_used;
+		++generation;
+		return sync();
+	}
+
+	// k substeps of every live session: per substep the colliders (col_slot[c]: the
+	// session each acts on) and the pins (session pin_slot[p], its Gaussian pin_idx[p])
+	int arena_step(int k, int ncol, const int* types, const float* poses, const float* dims, const int* col_slot,
+		float margin, float friction, int npin, const int* pin_slot, const int* pin_idx, const float* targets)
+	{
+		if (!arena) return fail("xpbd_b200_arena_step: not an arena");
+		if (n <= 0) return 0;
+		std::vector<int> rowsel(std::max(npin, 1));
+		for (int p = 0; p < npin; ++p) {
+			ArenaSeg* g = arena_seg(pin_slot[p]);
+			if (!g || pin_idx[p] < 0 || pin_idx[p] >= g->rows)
+				return fail("xpbd_b200_arena_step: pin %d (slot %d, Gaussian %d) is not in a live session", p, pin_slot[p],
+					pin_idx[p]);
+			rowsel[p] = g->row0 + g->inv[pin_idx[p]];
+		}
+		for (int s = 0; s < k; ++s) {
+			set_colliders_many(ncol, types, poses + (size_t)s * 12 * ncol, dims, col_slot, margin, friction);
+			if (set_attached(npin, rowsel.data(), targets + (size_t)s * 3 * npin, 1.0f, true)) return -1;
+			if (step_async()) return -1;
+		}
+		return 0;
+	}
+
+	// batched colliders, each bound to one object; a collider's previous pose (for the
+	// friction of the moving surface) is the last pose of the same (object, ordinal within
+	// the object), so the list may grow or shrink between calls as objects come and go
+	std::map<long long, KinCollider> col_prev;
+	static long long col_key(int obj, int ordinal) { return ((long long)obj << 24) | (long long)ordinal; }
+
+	void set_colliders_many(int count, const int* types, const float* poses, const float* dims, const int* obj,
+		float margin, float friction)
+	{
+		std::map<long long, KinCollider> seen;
+		std::map<int, int> ordinal;
+		std::vector<KinCollider> next(count);
+		for (int c = 0; c < count; ++c) {
+			KinCollider& K = next[c];
+			const long long key = col_key(obj[c] < 0 ? -1 : obj[c], ordinal[obj[c] < 0 ? -1 : obj[c]]++);
+			const auto it = col_prev.find(key);
+			const KinCollider* prev = it != col_prev.end() ? &it->second : nullptr;
+			const bool keep = prev && prev->type == types[c];
+			for (int a = 0; a < 9; ++a) K.Rp[a] = keep ? prev->R[a] : poses[12 * c + a];
+			for (int a = 0; a < 3; ++a) K.tp[a] = keep ? prev->t[a] : poses[12 * c + 9 + a];
+			K.type = types[c];
+			for (int a = 0; a < 9; ++a) K.R[a] = poses[12 * c + a];
+			for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
+			K.obj = obj[c] < 0 ? -1 : obj[c];
+			seen[key] = K;
+		}
+		col_prev.swap(seen);
+		S.kin_ext.swap(next);
+		S.kin_count = 0;
+		S.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
+		S.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
+	}
+
 	// ------------------------------------------------------------------ attach
 	// setAttachedParticles (forward.cu:6759-6788): restore the saved inverse masses, save
 	// them on first use, then pin idx[] at pos[].
-	int set_attached(int count, const int* idx, const float* pos, float weight = 1.0f)
+	int set_attached(int count, const int* idx, const float* pos, float weight = 1.0f, bool rows = false)
 	{
 		const int N = n;
 		if (att_active)
@@ -1301,7 +1652,8 @@ public:
 			CK(cudaMallocHost(&st.pos, sizeof(float) * 3 * count));
 			st.cap = count;
 		}
-		for (int k = 0; k < count; ++k) st.idx[k] = (idx[k] >= 0 && idx[k] < N) ? inv[idx[k]] : -1;
+		for (int k = 0; k < count; ++k)
+			st.idx[k] = (idx[k] >= 0 && idx[k] < N) ? (rows ? idx[k] : inv[idx[k]]) : -1;
 		memcpy(st.pos, pos, sizeof(float) * 3 * count);
 		CK(cudaMemcpyAsync(att_idx.p, st.idx, sizeof(int) * count, cudaMemcpyHostToDevice, stream));
 		CK(cudaMemcpyAsync(att_pos.p, st.pos, sizeof(float) * 3 * count, cudaMemcpyHostToDevice, stream));
@@ -1569,9 +1921,11 @@ XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const flo
 	const int* edges, const float* rest, const float* stiff)
 {
 	Engine& E = engine();
+	E.sync();
 	E.free_device();
 	E.n = 0;
 	E.stepped = false;
+	E.contact_bits = 0;
 	if (n <= 0 || !pos || !scales || !rots || !opacity || e < 0 || (e > 0 && (!edges || !rest || !stiff)))
 		return fail("xpbd_create: invalid arguments");
 	E.n = n;
@@ -1585,7 +1939,8 @@ XPBD_API int xpbd_create(int n, const float* pos, const float* scales, const flo
 	E.in_edges.assign(edges ? edges : (const int*)nullptr, edges ? edges + 2 * (size_t)e : (const int*)nullptr);
 	E.in_rest.assign(rest ? rest : (const float*)nullptr, rest ? rest + e : (const float*)nullptr);
 	E.in_stiff.assign(stiff ? stiff : (const float*)nullptr, stiff ? stiff + e : (const float*)nullptr);
-	if (E.ensure_stream()) return -1;
+	// the scene goes to the device with the first step (Engine::build); create itself makes
+	// no CUDA call
 	return 0;
 }
 
@@ -1597,6 +1952,7 @@ XPBD_API void xpbd_destroy(void)
 		cur_engine()->free_device();
 		cur_engine()->n = 0;
 		cur_engine()->stepped = false;
+		cur_engine()->contact_bits = 0;
 	}
 }
 
@@ -1722,9 +2078,18 @@ XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const flo
 
 XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 {
-	(void)tau; (void)radiusCap;
-	if (cur_engine()->n <= 0) return fail("xpbd_set_contact_shape: call xpbd_create first");
-	if (enabled) return fail("xpbd_set_contact_shape: ellipsoid contact shapes are not implemented");
+	// xpbd_capi.cu:181-191: packs from the created shapes now, or at the scene's upload
+	// (the first step) when it is not on the device yet
+	Engine& E = *cur_engine();
+	if (E.n <= 0) return fail("xpbd_set_contact_shape: call xpbd_create first");
+	E.contact_bits = enabled;
+	E.contact_tau = tau;
+	E.contact_cap = radiusCap;
+	if (!enabled) return 0;
+	if (E.built) {
+		if (E.pack_contact(false)) return fail("xpbd_set_contact_shape: pack failed: %s", g_err.c_str());
+		return E.sync();
+	}
 	return 0;
 }
 
@@ -1787,6 +2152,8 @@ XPBD_API int xpbd_compute_shapes(float deformEps, float* hostScales, float* host
 	dev::k_deformed_shapes<<<Engine::blocks_for(n), kBlock, 0, E.stream>>>(n, E.pos_rest.p, E.pos_curr.p, E.off.p,
 		E.nbr.p, E.d_scales.p, E.d_rots.p, deformEps, E.d_out_scales.p, E.d_out_quats.p, E.d_ctr, E.d_perm.p);
 	CK(cudaGetLastError());
+	// ellipsoid contacts follow the shapes as drawn, from the next step on (xpbd_capi.cu:255-256)
+	if (E.contact_bits && E.pack_contact(true)) return -1;
 	if (hostScales)
 		CK(cudaMemcpyAsync(hostScales, E.d_out_scales.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, E.stream));
 	if (hostQuats)
@@ -1888,26 +2255,9 @@ XPBD_API int xpbd_b200_set_collider_objects(int count, const int* obj)
 XPBD_API int xpbd_b200_set_colliders_many(int count, const int* types, const float* poses, const float* dims,
 	const int* obj, float margin, float friction)
 {
-	Settings& st = engine().S;
 	if (count < 0 || (count > 0 && (!types || !poses || !dims || !obj)))
 		return fail("xpbd_b200_set_colliders_many: invalid arguments");
-	const bool same = (count == (int)st.kin_ext.size());
-	std::vector<KinCollider> next(count);
-	for (int c = 0; c < count; ++c) {
-		KinCollider& K = next[c];
-		const KinCollider* prev = same ? &st.kin_ext[c] : nullptr;
-		const bool keep = prev && prev->type == types[c];
-		for (int a = 0; a < 9; ++a) K.Rp[a] = keep ? prev->R[a] : poses[12 * c + a];
-		for (int a = 0; a < 3; ++a) K.tp[a] = keep ? prev->t[a] : poses[12 * c + 9 + a];
-		K.type = types[c];
-		for (int a = 0; a < 9; ++a) K.R[a] = poses[12 * c + a];
-		for (int a = 0; a < 3; ++a) { K.t[a] = poses[12 * c + 9 + a]; K.h[a] = fmaxf(dims[3 * c + a], 0.0f); }
-		K.obj = obj[c] < 0 ? -1 : obj[c];
-	}
-	st.kin_ext.swap(next);
-	st.kin_count = 0;
-	st.kin_margin = (std::isfinite(margin) && margin > 0.0f) ? margin : 0.0f;
-	st.kin_friction = (std::isfinite(friction) && friction > 0.0f) ? friction : 0.0f;
+	engine().set_colliders_many(count, types, poses, dims, obj, margin, friction);
 	return 0;
 }
 
@@ -2108,6 +2458,75 @@ XPBD_API int xpbd_b200_step_substeps(int k, int ncol, const int* types, const fl
 }
 
 XPBD_API int xpbd_b200_sync(void) { return cur_engine()->stream ? cur_engine()->sync() : 0; }
+
+// ---- serving arena ----
+XPBD_API void* xpbd_b200_arena_new(long long rows, long long edges, long long members, long long rev)
+{
+	Engine* e = new (std::nothrow) Engine();
+	if (!e) { fail("xpbd_b200_arena_new: out of host memory"); return nullptr; }
+	if (e->arena_init(rows, edges, members, rev)) { delete e; return nullptr; }
+	return e;
+}
+
+XPBD_API int xpbd_b200_arena_admit(void* arena, void* session)
+{
+	if (!arena || !session) return fail("xpbd_b200_arena_admit: null handle");
+	return static_cast<Engine*>(arena)->arena_admit(*static_cast<Engine*>(session));
+}
+
+XPBD_API int xpbd_b200_arena_retire(void* arena, int slot)
+{
+	if (!arena) return fail("xpbd_b200_arena_retire: null handle");
+	return static_cast<Engine*>(arena)->arena_retire(slot);
+}
+
+XPBD_API int xpbd_b200_arena_step(void* arena, int k, int ncol, const int* types, const float* poses, const float* dims,
+	const int* col_slot, float margin, float friction, int npin, const int* pin_slot, const int* pin_idx,
+	const float* targets)
+{
+	if (!arena || k < 0 || ncol < 0 || npin < 0 || (ncol > 0 && (!types || !poses || !dims || !col_slot)) ||
+		(npin > 0 && (!pin_slot || !pin_idx || !targets)))
+		return fail("xpbd_b200_arena_step: invalid arguments");
+	return static_cast<Engine*>(arena)->arena_step(k, ncol, types, poses, dims, col_slot, margin, friction, npin,
+		pin_slot, pin_idx, targets);
+}
+
+XPBD_API int xpbd_b200_arena_positions(void* arena, int slot, float* out, int n)
+{
+	if (!arena || !out) return fail("xpbd_b200_arena_positions: invalid arguments");
+	Engine& A = *static_cast<Engine*>(arena);
+	const auto* g = A.arena_seg(slot);
+	if (!g || n != g->rows) return fail("xpbd_b200_arena_positions: no live session of %d Gaussians in slot %d", n, slot);
+	CK(cudaMemcpyAsync(out, A.pos_out3.p + 3 * (size_t)g->row0, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
+		A.stream));
+	return A.sync();
+}
+
+XPBD_API int xpbd_b200_arena_sync(void* arena)
+{
+	if (!arena) return fail("xpbd_b200_arena_sync: null handle");
+	return static_cast<Engine*>(arena)->sync();
+}
+
+XPBD_API int xpbd_b200_arena_usage(void* arena, long long* out)
+{
+	if (!arena || !out) return fail("xpbd_b200_arena_usage: invalid arguments");
+	const Engine& A = *static_cast<Engine*>(arena);
+	long long live = 0, sessions = 0;
+	for (const auto& g : A.segs)
+		if (g.live) { live += g.rows; ++sessions; }
+	out[0] = A.rows_used; out[1] = A.rows_cap; out[2] = A.e_used; out[3] = A.e_cap; out[4] = A.m_used;
+	out[5] = A.m_cap; out[6] = A.r_used; out[7] = A.r_cap; out[8] = live; out[9] = sessions;
+	return 0;
+}
+
+XPBD_API void xpbd_b200_arena_free(void* arena)
+{
+	Engine* e = static_cast<Engine*>(arena);
+	if (!e) return;
+	e->sync();
+	delete e;
+}
 
 XPBD_API void xpbd_b200_set_gs(int distance, int volume)
 {
@@ -2342,6 +2761,20 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 	return -1;
 }
 
+XPBD_API int xpbd_b200_set_positions(const float* pos, int n)
+{
+	Engine& E = *cur_engine();
+	if (!E.stepped) return fail("xpbd_b200_set_positions: no step yet");
+	if (!pos || n != E.n) return fail("xpbd_b200_set_positions: size mismatch");
+	DBuf<float> tmp;
+	CK(tmp.alloc(3 * (size_t)n));
+	CK(cudaMemcpyAsync(tmp.p, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, E.stream));
+	dev::k_set_positions<<<Engine::blocks_for(n), kBlock, 0, E.stream>>>(n, tmp.p, E.d_perm.p, E.pos_curr.p,
+		E.pos_out3.p);
+	CK(cudaGetLastError());
+	return E.sync();
+}
+
 // The once-per-step self-collision build on caller-given start / predicted positions
 // (x[3N], p[3N]); the candidate total, or -1.  Used to check the hash, order and
 // candidate lists stage by stage.
@@ -2378,7 +2811,7 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	dev::k_scan_add<<<nb, 1024, 0, E.stream>>>(E.sc_start.p, scan_n, E.sc_block_sums.p);
 	dev::k_sc_scatter<<<G, B, 0, E.stream>>>(N, E.sc_keys.p, E.sc_start.p, E.sc_cursor.p, E.sc_idx_sorted.p);
 	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p, E.d_perm.p);
-	E.enqueue_sc_candidates(G, B, nullptr);
+	E.enqueue_sc_candidates(G, B);
 	CK(cudaGetLastError());
 	if (E.read_counters()) return -1;
 	// restore the solver state this stage check borrowed
@@ -2454,6 +2887,31 @@ static int scratch_for_current_device(unsigned char** out)
 	return 0;
 }
 
+// the self-collision constants of one call, passed by value
+struct SelfColConsts {
+	float dc, search, excl2, cross_excl2, fast_rel, search_plus16dc;
+	int within, single_object;
+};
+
+// writes the call's constants into the StepParams block of the scratch array (every other
+// field zero), so that no host memory is copied to the device
+__global__ void __launch_bounds__(256) k_static_params(StepParams* __restrict__ P, SelfColConsts c)
+{
+	unsigned int* w = reinterpret_cast<unsigned int*>(P);
+	for (size_t k = threadIdx.x; k < sizeof(StepParams) / sizeof(unsigned int); k += blockDim.x) w[k] = 0u;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		P->sc_dc = c.dc;
+		P->sc_search = c.search;
+		P->sc_excl2 = c.excl2;
+		P->sc_cross_excl2 = c.cross_excl2;
+		P->sc_fast_rel = c.fast_rel;
+		P->sc_search_plus16dc = c.search_plus16dc;
+		P->sc_within = c.within;
+		P->sc_single_object = c.single_object;
+	}
+}
+
 }  // namespace noalloc
 }  // namespace xpbd
 
@@ -2473,10 +2931,12 @@ static int scratch_for_current_device(unsigned char** out)
 //   stream      cudaStream_t to run on (NULL: legacy default stream)
 //
 // Returns 0 once the work is enqueued, -1 with xpbd_last_error() on bad arguments or a
-// CUDA error.  All scratch sits in one static device array per GPU, reused by every call:
+// CUDA error.  Nothing is copied from host memory: the constants travel as a kernel
+// argument.  All scratch sits in one static device array per GPU, reused by every call:
 // calls that overlap on the GPU (different streams, or several host threads) race on it
 // and must be serialised by the caller.  The first call on a device looks up the array's
-// device address; make that first call outside any CUDA stream capture.
+// device address; make that first call outside any CUDA stream capture.  The count of
+// over-cap replacements (xpbd_self_collision_stats' third figure) is not reported here.
 XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const float* p, const float* rest,
 	const int* obj_id, float spacing, float radius_scale, float exclude_scale, int within_body, int* contacts,
 	int* counts, int* total, void* stream)
@@ -2505,23 +2965,22 @@ XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const fl
 	auto* sr = reinterpret_cast<float4*>(base + kOffSr);
 	auto* sx = reinterpret_cast<float4*>(base + kOffSx);
 	// step constants as the solver derives them (forward.cu:4532-4540, 11798-11831)
-	StepParams hp;
-	memset(&hp, 0, sizeof(hp));
 	const float rs = fminf(fmaxf(std::isfinite(radius_scale) ? radius_scale : 1.5f, 0.1f), 10.0f);
 	const float es = fminf(fmaxf(std::isfinite(exclude_scale) ? exclude_scale : 2.0f, 1.05f), 20.0f);
 	const float dc = rs * spacing;
 	const float search = 1.5f * dc;
 	const float excl = es * dc;
-	hp.sc_dc = dc;
-	hp.sc_search = search;
-	hp.sc_excl2 = excl * excl;
-	hp.sc_cross_excl2 = dc * dc;
-	hp.sc_fast_rel = 0.0f * dc;
-	hp.sc_search_plus16dc = search + 16.0f * dc;
-	hp.sc_within = within_body ? 1 : 0;
-	hp.sc_single_object = obj_id ? 0 : 1;
+	SelfColConsts c;
+	c.dc = dc;
+	c.search = search;
+	c.excl2 = excl * excl;
+	c.cross_excl2 = dc * dc;
+	c.fast_rel = 0.0f * dc;
+	c.search_plus16dc = search + 16.0f * dc;
+	c.within = within_body ? 1 : 0;
+	c.single_object = obj_id ? 0 : 1;
+	k_static_params<<<1, 256, 0, st>>>(d_params, c);
 	// everything the build accumulates into starts from zero on every call
-	CK(cudaMemcpyAsync(d_params, &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st));
 	CK(cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), st));
 	CK(cudaMemsetAsync(bucket, 0, sizeof(int) * kScanN, st));
 	CK(cudaMemsetAsync(cursor, 0, sizeof(int) * kBuckets, st));

@@ -186,12 +186,60 @@ __device__ __forceinline__ float warp_sum(float v)
 }
 
 // ---------------------------------------------------------------------------
+// ellipsoid contact shapes (forward.cu:7355-7399): each Gaussian meets colliders and
+// the ground as its opacity-tau iso-ellipsoid, M = k^2 Sigma with k = sqrt(2 ln(a/tau)),
+// instead of as its centre.  Stored per Gaussian in internal order as two float4,
+// (xx, xy, xz, yy) and (yz, zz, -, -), beside the longest semi-axis rmax[i].
+// ---------------------------------------------------------------------------
+// support distance sqrt(n^T M n) along the unit normal n, summed as forward.cu:7387-7392
+__device__ __forceinline__ float contact_support(float4 a, float4 b, float nx, float ny, float nz)
+{
+	const float q = a.x * nx * nx + a.w * ny * ny + b.y * nz * nz + 2.0f * (a.y * nx * ny + a.z * nx * nz + b.x * ny * nz);
+	return sqrtf(fmaxf(q, 0.0f));
+}
+
+// contactShapePackKernel (forward.cu:7358-7385).  Scales and quaternions are read at
+// slot src[i] (caller order, for the deformed shapes) or i (internal order, rest shapes).
+__global__ void __launch_bounds__(kBlock) k_contact_pack(int n, const float* __restrict__ sc,
+	const float* __restrict__ qt, const int* __restrict__ src, const float* __restrict__ opacity, float tau,
+	float rcap, float4* __restrict__ shape, float* __restrict__ rmax)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const int s = src ? src[i] : i;
+	const float a = opacity[i];
+	const float k = (a > tau && tau > 0.0f) ? sqrtf(2.0f * logf(a / tau)) : 0.0f;
+	float e0 = k * sc[3 * s], e1 = k * sc[3 * s + 1], e2 = k * sc[3 * s + 2];
+	if (rcap > 0.0f) { e0 = fminf(e0, rcap); e1 = fminf(e1, rcap); e2 = fminf(e2, rcap); }
+	if (!(isfinite(e0) && isfinite(e1) && isfinite(e2))) e0 = e1 = e2 = 0.0f;
+	float w = qt[4 * s], x = qt[4 * s + 1], y = qt[4 * s + 2], z = qt[4 * s + 3];
+	const float qn = sqrtf(w * w + x * x + y * y + z * z);
+	if (qn > 1e-20f) { w /= qn; x /= qn; y /= qn; z /= qn; }
+	else { w = 1.0f; x = y = z = 0.0f; }
+	// rotation whose columns are the Gaussian's local axes
+	const float r00 = 1 - 2 * (y * y + z * z), r01 = 2 * (x * y - w * z), r02 = 2 * (x * z + w * y);
+	const float r10 = 2 * (x * y + w * z), r11 = 1 - 2 * (x * x + z * z), r12 = 2 * (y * z - w * x);
+	const float r20 = 2 * (x * z - w * y), r21 = 2 * (y * z + w * x), r22 = 1 - 2 * (x * x + y * y);
+	const float l0 = e0 * e0, l1 = e1 * e1, l2 = e2 * e2;
+	shape[2 * i] = make_float4(r00 * r00 * l0 + r01 * r01 * l1 + r02 * r02 * l2,
+		r00 * r10 * l0 + r01 * r11 * l1 + r02 * r12 * l2,
+		r00 * r20 * l0 + r01 * r21 * l1 + r02 * r22 * l2,
+		r10 * r10 * l0 + r11 * r11 * l1 + r12 * r12 * l2);
+	shape[2 * i + 1] = make_float4(r10 * r20 * l0 + r11 * r21 * l1 + r12 * r22 * l2,
+		r20 * r20 * l0 + r21 * r21 * l1 + r22 * r22 * l2, 0.0f, 0.0f);
+	rmax[i] = fmaxf(e0, fmaxf(e1, e2));
+}
+
+// ---------------------------------------------------------------------------
 // predict (forward.cu:5954-5979); also clears the volume multipliers of the step
-// (forward.cu:12058-12060).  HBM: 16+16 B read, 16+16 B written per Gaussian.
+// (forward.cu:12058-12060) and, with ellipsoid ground contact on, refreshes each
+// Gaussian's support radius along the ground normal (contactGroundRadiusKernel,
+// forward.cu:7394-7399, run once per step at 12223-12227).  HBM: 16+16 B read, 16+16 B
+// written per Gaussian (+32 B read, 4 B written with ground contact shapes).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pos_curr, float4* __restrict__ pos_next, float4* __restrict__ vel,
-	float* __restrict__ lam_vol)
+	float* __restrict__ lam_vol, const float4* __restrict__ cshape, float* __restrict__ crg)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
@@ -200,6 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __r
 	const float dt = P->dt;
 	const float3 g = make_float3(P->gx, P->gy, P->gz);
 	if (lam_vol) lam_vol[i] = 0.0f;
+	if (crg) crg[i] = contact_support(cshape[2 * i], cshape[2 * i + 1], P->gn[0], P->gn[1], P->gn[2]);
 	if (x4.w > 0.0f) {
 		float3 v = add3(f3(v4), mul3(g, dt));
 		const float3 p = add3(f3(x4), mul3(v, dt));
@@ -343,20 +392,15 @@ __device__ __forceinline__ bool cluster_j_sinv(const M3& Scur, float det_rest, f
 
 // Cluster blackboard record, 36 bytes in two places so that a record read touches one
 // 32-byte sector plus a 4-byte entry: rec[2 i] = (M00, M11, M22, M01), rec[2 i + 1] =
-// (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float array after the 2N
-// float4.  A record the gather must skip (the reference's coef == 0) has c.x = NaN.
-__device__ __forceinline__ float* rec_cz(float4* rec, int n) { return reinterpret_cast<float*>(rec + 2 * (size_t)n); }
-__device__ __forceinline__ const float* rec_cz(const float4* rec, int n)
-{
-	return reinterpret_cast<const float*>(rec + 2 * (size_t)n);
-}
+// (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float array recz[i].  A record
+// the gather must skip (the reference's coef == 0) has c.x = NaN.
 __device__ __forceinline__ void rec_invalidate(float4* rec, int idx) { rec[2 * idx + 1].z = __int_as_float(0x7fc00000); }
-__device__ __forceinline__ void store_record(float4* rec, int n, int idx, float3 c, float coef, const M3& S)
+__device__ __forceinline__ void store_record(float4* rec, float* recz, int idx, float3 c, float coef, const M3& S)
 {
 	if (coef == 0.0f) { rec_invalidate(rec, idx); return; }
 	rec[2 * idx + 0] = make_float4(coef * S.m[0][0], coef * S.m[1][1], coef * S.m[2][2], coef * S.m[1][0]);
 	rec[2 * idx + 1] = make_float4(coef * S.m[2][0], coef * S.m[2][1], c.x, c.y);
-	rec_cz(rec, n)[idx] = c.z;
+	recz[idx] = c.z;
 }
 
 // Kernel A on groups of S lanes per cluster (32/S clusters per warp).  Lane L of a group
@@ -379,7 +423,7 @@ template <int S, int VC>
 __global__ void __launch_bounds__(kBlock) k_volume_solve_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, int read_lam)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
 	const int sl = threadIdx.x & (S - 1);
 	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
@@ -490,7 +534,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_group(int n, const Step
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, n, idx, c, dl * gs, Sinv);
+	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A with static register slots: lane sl of an S-lane group owns members
@@ -501,7 +545,7 @@ template <int S, int NS, bool CP>
 __global__ void __launch_bounds__(kBlock) k_volume_solve_slots(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, int read_lam)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
 	const int sl = threadIdx.x & (S - 1);
 	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
@@ -620,7 +664,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_slots(int n, const Step
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, n, idx, c, dl * gs, Sinv);
+	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A with the members' positions staged in shared memory: pass 1 gathers each
@@ -633,7 +677,7 @@ template <int S, int NS>
 __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, int read_lam)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
 	__shared__ float4 stage[NS][kSmemBlock];
 	const int tx = threadIdx.x;
@@ -757,7 +801,7 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, n, idx, c, dl * gs, Sinv);
+	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A in one pass over the members (S lanes per cluster, members L, L+S, ... of
@@ -776,7 +820,7 @@ template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, int read_lam)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
 	const int sl = threadIdx.x & (S - 1);
 	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
@@ -867,14 +911,14 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
-	store_record(rec, n, idx, c, dl * gs, Sinv);
+	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
 __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, int read_lam)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -936,7 +980,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const Ste
 	const float dl = (-C - alpha_t * lam) / den;
 	if (!isfinite(dl)) return;
 	lam_vol[idx] = lam + dl;
-	store_record(rec, n, idx, c, dl * gs, Sinv);
+	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 
 // one blackboard record (already loaded) applied to a node (forward.cu:9212-9222):
@@ -955,10 +999,10 @@ __device__ __forceinline__ bool gather_rec(float4 r0, float4 r1, float cz, float
 	return fin3(dp);
 }
 
-__device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, int n, int i, float3 pi, float wi,
+__device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, const float* __restrict__ recz, int i, float3 pi, float wi,
 	float3& dp)
 {
-	return gather_rec(__ldg(rec + 2 * i), __ldg(rec + 2 * i + 1), __ldg(rec_cz(rec, n) + i), pi, wi, dp);
+	return gather_rec(__ldg(rec + 2 * i), __ldg(rec + 2 * i + 1), __ldg(recz + i), pi, wi, dp);
 }
 
 __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl, float under_relax)
@@ -977,7 +1021,8 @@ __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl,
 template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
-	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ rest_len)
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
+	const float* __restrict__ rest_len)
 {
 	const int sl = threadIdx.x & (S - 1);
 	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
@@ -1005,7 +1050,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 		const bool ok0 = i0 >= 0 && i0 < n, ok1 = i1 >= 0 && i1 < n;
 		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
 		float z0 = 0.0f, z1 = 0.0f;
-		const float* cz = rec_cz(rec, n);
+		const float* cz = recz;
 		if (ok0) { a0 = __ldg(rec + 2 * i0); b0 = __ldg(rec + 2 * i0 + 1); z0 = __ldg(cz + i0); }
 		if (ok1) { a1 = __ldg(rec + 2 * i1); b1 = __ldg(rec + 2 * i1 + 1); z1 = __ldg(cz + i1); }
 		float3 dp;
@@ -1015,7 +1060,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 	if (k < cnt) {
 		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (i >= 0 && i < n && gather_one(rec, n, i, pi, wi, dp)) {
+		if (i >= 0 && i < n && gather_one(rec, recz, i, pi, wi, dp)) {
 			sum = add3(sum, dp);
 			++received;
 		}
@@ -1034,7 +1079,8 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 // Kernel B, one thread per node (forward.cu:9187-9243)
 __global__ void __launch_bounds__(kBlock) k_volume_gather_thread(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
-	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ rest_len)
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
+	const float* __restrict__ rest_len)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1048,7 +1094,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_thread(int n, const St
 		const int i = __ldg(ridx + k);
 		if (i < 0 || i >= n) continue;
 		float3 dp;
-		if (!gather_one(rec, n, i, pi, wi, dp)) continue;
+		if (!gather_one(rec, recz, i, pi, wi, dp)) continue;
 		sum = add3(sum, dp);
 		++received;
 	}
@@ -1637,14 +1683,18 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 
 // ---------------------------------------------------------------------------
 // per-Gaussian projections at the end of an iteration: self-collision apply
-// (forward.cu:7311-7322), kinematic colliders (forward.cu:7425-7518, point contact)
-// and the ground plane (forward.cu:7405-7421), fused in that order.
+// (forward.cu:7311-7322), kinematic colliders (forward.cu:7425-7518) and the ground
+// plane (forward.cu:7405-7421), fused in that order.  With ellipsoid contact shapes
+// (cshape / crmax non-null) a collider's reach grows by the Gaussian's longest
+// semi-axis and its distance shrinks by the support along the contact normal; with
+// ground contact shapes (crg non-null) the plane is offset by the support radius.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
 	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
 	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id,
 	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range, const float4* __restrict__ sc_dp_cross,
-	float4* __restrict__ sc_accum)
+	float4* __restrict__ sc_accum, const float4* __restrict__ cshape, const float* __restrict__ crmax,
+	const float* __restrict__ crg)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1664,7 +1714,8 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 	if (p4.w > 0.0f) {
 		float3 p = f3(p4);
 		const float margin = P->kin_margin, mu = P->kin_friction;
-		const float reach = margin + 0.0f;
+		const float rmax = crmax ? crmax[idx] : 0.0f;
+		const float reach = margin + rmax;   // a centre farther than this keeps its ellipsoid clear too
 		const int my_obj = ((P->kin_filtered || ext_kin) && obj_id) ? obj_id[idx] : -1;
 		// colliders: the reference's list (with optional per-collider object filter), or the
 		// batched list sorted by object, of which only this object's range is visited
@@ -1713,6 +1764,10 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 			const float wx = C.R[0] * n0 + C.R[1] * n1 + C.R[2] * n2;
 			const float wy = C.R[3] * n0 + C.R[4] * n1 + C.R[5] * n2;
 			const float wz = C.R[6] * n0 + C.R[7] * n1 + C.R[8] * n2;
+			if (crmax && rmax > 0.0f) {   // the ellipsoid reaches that much closer along the normal
+				dist -= contact_support(cshape[2 * idx], cshape[2 * idx + 1], wx, wy, wz);
+				if (dist >= margin) continue;
+			}
 			const float corr = margin - dist;
 			const float3 p_in = p;
 			// explicit roundings: the batched-list and reference-list paths of this loop
@@ -1751,7 +1806,7 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 			}
 		}
 		if (P->ground_on) {
-			const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane;
+			const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane - (crg ? crg[idx] : 0.0f);
 			if (c < 0.0f) {
 				p = make_float3(p.x - c * P->gn[0], p.y - c * P->gn[1], p.z - c * P->gn[2]);
 				moved = true;
@@ -1768,7 +1823,7 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __restrict__ P,
 	float4* __restrict__ pos_curr, const float4* __restrict__ pfinal, float4* __restrict__ vel,
-	float* __restrict__ pos_out3, const int* __restrict__ perm)
+	float* __restrict__ pos_out3, const int* __restrict__ perm, const float* __restrict__ crg)
 {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
@@ -1797,7 +1852,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __
 		if (isfinite(dx2)) {
 			v = (dx2 < 1e-18f) ? make_float3(0.0f, 0.0f, 0.0f) : mul3(dx, 1.0f / fmaxf(dt, 1e-8f));
 			const float3 nn = make_float3(P->gn[0], P->gn[1], P->gn[2]);
-			const float gap = nn.x * p.x + nn.y * p.y + nn.z * p.z - P->ground_plane;
+			const float gap = nn.x * p.x + nn.y * p.y + nn.z * p.z - P->ground_plane - (crg ? crg[idx] : 0.0f);
 			if (gap <= P->ground_slop) {
 				const float vn = nn.x * v.x + nn.y * v.y + nn.z * v.z;
 				const float vn_pre = nn.x * v_pre.x + nn.y * v_pre.y + nn.z * v_pre.z;
@@ -2006,10 +2061,129 @@ __global__ void __launch_bounds__(kBlock) k_sc_pack(int n, const int* __restrict
 	sx[t] = x;
 }
 
-// Candidate lists with particles visited in cell order (thread t builds the list of
-// particle idx_sorted[t], so a warp scans overlapping cells) and neighbours read from
-// the cell-ordered copies.  Same cells, same visiting order and same tests as
-// k_sc_build / selfColBuildKernel (forward.cu:7079-7180), hence identical lists.
+// The candidate list of one particle: the 27 cells around its start position in the
+// reference's order (z, y, x nested, kc = 9 (z+1) + 3 (y+1) + (x+1)); a cell whose hash
+// repeats an earlier one of the 27 is skipped (forward.cu:7116-7123); each cell's
+// entries in bucket order through the tests of selfColBuildKernel (forward.cu:7079-7180)
+// and its cap-of-32 replacement rule.  Neighbours are read from the cell-ordered copies.
+// Writes contacts[i * 32 ...]; returns the count, adds the over-cap replacements to over.
+__device__ __forceinline__ int sc_build_one(int i, const StepParams* __restrict__ P, const float4* __restrict__ X,
+	const float4* __restrict__ Pp, const float4* __restrict__ rest, const int* __restrict__ start, unsigned int mask,
+	const int* __restrict__ obj_id, const float4* __restrict__ sp, const float4* __restrict__ sr,
+	const float4* __restrict__ sx, const DevCounters* __restrict__ ctr, int* __restrict__ contacts, int& over)
+{
+	const float4 x = X[i], p = Pp[i];
+	int cnt = 0;
+	if (!(isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) && isfinite(p.z)))
+		return 0;
+	const float inv_cell = ctr->sc_inv_cell;
+	const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
+	const float fast_rel = P->sc_fast_rel;
+	const int within = P->sc_within;
+	// when every particle carries the same object id there are no cross-object pairs,
+	// and a same-object neighbour outside the search radius is rejected right away
+	const bool single_object = P->sc_single_object != 0;
+	const float4 q = rest[i];
+	const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
+	const int oi = obj_id[i];
+	const float search2 = search * search;
+	const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+	int* out = contacts + (size_t)i * kSelfColMax;
+	float prio[kSelfColMax];
+	int tier[kSelfColMax];
+	// a 64-bit filter on the low hash bits settles almost every cell's duplicate test
+	// without comparing; the rest recompute the earlier hashes
+	unsigned int use = 0u;
+	{
+		unsigned long long seen = 0ull;
+		for (int kc = 0; kc < 27; ++kc) {
+			const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
+			const unsigned long long bit = 1ull << (h & 63u);
+			if (seen & bit) {
+				bool dup = false;
+				for (int m = 0; m < kc && !dup; ++m)
+					dup = sc_hash(cx + m % 3 - 1, cy + (m / 3) % 3 - 1, cz + m / 9 - 1, mask) == h;
+				if (dup) continue;
+			}
+			seen |= bit;
+			use |= 1u << kc;
+		}
+	}
+	// the used cells in order, the next cell's bucket range loaded while the current
+	// cell's entries are tested
+	int kc = use ? __ffs(use) - 1 : 27;
+	int cs = 0, ce = 0;
+	if (kc < 27) {
+		const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
+		cs = start[h];
+		ce = start[h + 1];
+	}
+	while (kc < 27) {
+		const unsigned int later = use & ~((2u << kc) - 1u);
+		const int kn = later ? __ffs(later) - 1 : 27;
+		int ns = 0, ne = 0;
+		if (kn < 27) {
+			const unsigned int hn = sc_hash(cx + kn % 3 - 1, cy + (kn / 3) % 3 - 1, cz + kn / 9 - 1, mask);
+			ns = start[hn];
+			ne = start[hn + 1];
+		}
+		for (int t = cs; t < ce; ++t) {
+			// predicted position + index first: most neighbours fail the distance
+			// test, so the rest position / object id is read only for the others
+			const float4 pj = sp[t];
+			const int j = __float_as_int(pj.w);
+			if (j == i) continue;
+			const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+			const float d2 = ex * ex + ey * ey + ez * ez;
+			const bool near_same = d2 < search2;
+			if (!near_same && single_object) continue;
+			const float4 rj = sr[t];
+			const bool cross = __float_as_int(rj.w) != oi;
+			if (!cross && !within) continue;
+			const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
+			const float q2 = qx * qx + qy * qy + qz * qz;
+			float pr;
+			int code = j;
+			if (cross) {
+				const float4 xj = sx[t];
+				const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
+				const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
+				const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
+				const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
+				if (!(dist_x < search + rel)) continue;
+				if (!(q2 >= cross_excl2)) continue;
+				pr = dist_x - rel;
+				if (rel > fast_rel) code = -(j + 1);
+			}
+			else {
+				if (!near_same) continue;
+				if (!(q2 >= excl2)) continue;
+				pr = sqrtf(d2);
+			}
+			const int tr = cross ? 0 : 1;
+			if (cnt < kSelfColMax) {
+				out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
+			}
+			else {
+				int worst = 0;
+				for (int m = 1; m < kSelfColMax; ++m)
+					if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
+				if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
+					out[worst] = code; prio[worst] = pr; tier[worst] = tr;
+				}
+				++over;
+			}
+		}
+		kc = kn;
+		cs = ns;
+		ce = ne;
+	}
+	return cnt;
+}
+
+// Candidate lists, one thread per particle (thread i builds particle i's list; particles
+// are numbered along a Morton curve of their rest positions, so a warp's particles
+// share most of their 27 cells).
 __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
 	const int* __restrict__ idx_sorted, const int* __restrict__ start, unsigned int mask,
@@ -2017,123 +2191,189 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
 	int* __restrict__ counts, const unsigned char* __restrict__ active)
 {
-	// thread i builds the list of particle i: particles are numbered along a Morton curve
-	// of their rest positions, so a warp's particles share most of their 27 cells (same
-	// loop trip counts, same neighbour rows); the list itself does not depend on who builds it
+	(void)idx_sorted;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	const float4 x = X[i], p = Pp[i];
-	int cnt = 0, over = 0;
-	if ((!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) &&
-		isfinite(p.z)) {
-		const float inv_cell = ctr->sc_inv_cell;
-		const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
-		const float fast_rel = P->sc_fast_rel;
-		const int within = P->sc_within;
-		// when every particle carries the same object id there are no cross-object pairs,
-		// and a same-object neighbour outside the search radius is rejected right away
-		const bool single_object = P->sc_single_object != 0;
-		const float4 q = rest[i];
-		const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
-		const int oi = obj_id[i];
-		const float search2 = search * search;
-		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
-		int* out = contacts + (size_t)i * kSelfColMax;
-		float prio[kSelfColMax];
-		int tier[kSelfColMax];
-		// the 27 cells in the reference's order (z, y, x nested, kc = 9 (z+1) + 3 (y+1) +
-		// (x+1)); a cell whose hash repeats an earlier one of the 27 is skipped
-		// (forward.cu:7116-7123).  A 64-bit filter on the low hash bits settles almost
-		// every cell without comparing, the rest recompute the earlier hashes.
-		unsigned int use = 0u;
-		{
-			unsigned long long seen = 0ull;
-			for (int kc = 0; kc < 27; ++kc) {
-				const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
-				const unsigned long long bit = 1ull << (h & 63u);
-				if (seen & bit) {
-					bool dup = false;
-					for (int m = 0; m < kc && !dup; ++m)
-						dup = sc_hash(cx + m % 3 - 1, cy + (m / 3) % 3 - 1, cz + m / 9 - 1, mask) == h;
-					if (dup) continue;
-				}
-				seen |= bit;
-				use |= 1u << kc;
-			}
-		}
-		// the used cells in order, the next cell's bucket range loaded while the current
-		// cell's entries are tested
-		int kc = use ? __ffs(use) - 1 : 27;
-		int cs = 0, ce = 0;
-		if (kc < 27) {
-			const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
-			cs = start[h];
-			ce = start[h + 1];
-		}
-		while (kc < 27) {
-			const unsigned int later = use & ~((2u << kc) - 1u);
-			const int kn = later ? __ffs(later) - 1 : 27;
-			int ns = 0, ne = 0;
-			if (kn < 27) {
-				const unsigned int hn = sc_hash(cx + kn % 3 - 1, cy + (kn / 3) % 3 - 1, cz + kn / 9 - 1, mask);
-				ns = start[hn];
-				ne = start[hn + 1];
-			}
-			for (int t = cs; t < ce; ++t) {
-				// predicted position + index first: most neighbours fail the distance
-				// test, so the rest position / object id is read only for the others
-				const float4 pj = sp[t];
-				const int j = __float_as_int(pj.w);
-				if (j == i) continue;
-				const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-				const float d2 = ex * ex + ey * ey + ez * ez;
-				const bool near_same = d2 < search2;
-				if (!near_same && single_object) continue;
-				const float4 rj = sr[t];
-				const bool cross = __float_as_int(rj.w) != oi;
-				if (!cross && !within) continue;
-				const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
-				const float q2 = qx * qx + qy * qy + qz * qz;
-				float pr;
-				int code = j;
-				if (cross) {
-					const float4 xj = sx[t];
-					const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
-					const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
-					const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
-					const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
-					if (!(dist_x < search + rel)) continue;
-					if (!(q2 >= cross_excl2)) continue;
-					pr = dist_x - rel;
-					if (rel > fast_rel) code = -(j + 1);
-				}
-				else {
-					if (!near_same) continue;
-					if (!(q2 >= excl2)) continue;
-					pr = sqrtf(d2);
-				}
-				const int tr = cross ? 0 : 1;
-				if (cnt < kSelfColMax) {
-					out[cnt] = code; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
-				}
-				else {
-					int worst = 0;
-					for (int m = 1; m < kSelfColMax; ++m)
-						if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
-					if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
-						out[worst] = code; prio[worst] = pr; tier[worst] = tr;
-					}
-					++over;
-				}
-			}
-			kc = kn;
-			cs = ns;
-			ce = ne;
-		}
-	}
+	int over = 0, cnt = 0;
+	if (!active || active[i])
+		cnt = sc_build_one(i, P, X, Pp, rest, start, mask, obj_id, sp, sr, sx, ctr, contacts, over);
 	counts[i] = cnt;
 	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
 	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
+}
+
+// Candidate lists, one warp per run of particles that share a start cell (the home
+// cell).  Such particles have the same 27 neighbour cells in the same order, so the
+// warp concatenates the cells' bucket ranges into one sequence of E entries and tests
+// (home particle, entry) pairs with every lane busy: with k home particles padded to
+// K = 2^ceil(log2 k), lane l tests particle l mod K against entry e0 + l / K.  A
+// particle's accepted entries arrive in entry order across its lanes, so a ballot and
+// a prefix count append them to its list in the reference's order (forward.cu:
+// 7079-7180); the same tests as sc_build_one decide acceptance.  A particle that would
+// pass 32 candidates takes the replacement rule instead: it goes on the fix-up list
+// and k_sc_fixup builds its list with sc_build_one.  Warp w owns the runs that begin
+// at sorted positions [32 w, 32 w + 32) of its buckets.
+__global__ void __launch_bounds__(kBlock) k_sc_build_cells(int n, const StepParams* __restrict__ P,
+	const unsigned int* __restrict__ keys, const int* __restrict__ idx_sorted, const int* __restrict__ start,
+	unsigned int mask, unsigned int sentinel, const float4* __restrict__ sp, const float4* __restrict__ sr,
+	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
+	int* __restrict__ counts, int* __restrict__ fix_list)
+{
+	const int lane = threadIdx.x & 31;
+	const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+	const int base0 = w * 32;
+	if (base0 >= n) return;
+	const unsigned int lt_mask = (1u << lane) - 1u;
+	const float inv_cell = ctr->sc_inv_cell;
+	const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
+	const float fast_rel = P->sc_fast_rel;
+	const int within = P->sc_within;
+	const bool single_object = P->sc_single_object != 0;
+	const float search2 = search * search;
+	// bucket starts in this warp's window
+	const int mypos = base0 + lane;
+	unsigned int mykey = sentinel + 1u;
+	if (mypos < n) mykey = keys[idx_sorted[mypos]];
+	const bool is_start = mypos < n && start[mykey] == mypos;
+	unsigned int starts = __ballot_sync(0xffffffffu, is_start);
+	unsigned int total = 0u;
+	while (starts) {
+		const int l0 = __ffs(starts) - 1;
+		starts &= starts - 1u;
+		const unsigned int b = __shfl_sync(0xffffffffu, mykey, l0);
+		int hb = base0 + l0;
+		const int be = start[b + 1];
+		if (b == sentinel) {   // particles out of the grid (inactive or not finite): no list
+			for (int t = hb + lane; t < be; t += 32) counts[idx_sorted[t]] = 0;
+			continue;
+		}
+		while (hb < be) {
+			// the run of particles from hb sharing hb's start cell (at most 32)
+			const int tp = hb + lane;
+			int ccx = 0, ccy = 0, ccz = 0;
+			if (tp < be) {
+				const float4 xt = sx[tp];
+				ccx = sc_cell(xt.x, inv_cell); ccy = sc_cell(xt.y, inv_cell); ccz = sc_cell(xt.z, inv_cell);
+			}
+			const int cx = __shfl_sync(0xffffffffu, ccx, 0), cy = __shfl_sync(0xffffffffu, ccy, 0),
+				cz = __shfl_sync(0xffffffffu, ccz, 0);
+			const unsigned int same = __ballot_sync(0xffffffffu, tp < be && ccx == cx && ccy == cy && ccz == cz);
+			const int k = (~same) ? __ffs(~same) - 1 : 32;
+			// neighbour cells: lane kc < 27 holds cell kc's bucket range, empty for a
+			// hash that repeats an earlier cell's
+			unsigned int h = 0xffffffffu;
+			if (lane < 27) h = sc_hash(cx + lane % 3 - 1, cy + (lane / 3) % 3 - 1, cz + lane / 9 - 1, mask);
+			bool dup = false;
+#pragma unroll
+			for (int m = 0; m < 26; ++m) {
+				const unsigned int hm = __shfl_sync(0xffffffffu, h, m);
+				dup = dup || (m < lane && hm == h);
+			}
+			int cs = 0, len = 0;
+			if (lane < 27 && !dup) { cs = start[h]; len = start[h + 1] - cs; }
+			int off = len;   // inclusive scan, then exclusive
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const int v = __shfl_up_sync(0xffffffffu, off, o);
+				if (lane >= o) off += v;
+			}
+			const int E = __shfl_sync(0xffffffffu, off, 31);
+			off -= len;
+			// home particle of this lane
+			const int K = k <= 1 ? 1 : (k <= 2 ? 2 : (k <= 4 ? 4 : (k <= 8 ? 8 : (k <= 16 ? 16 : 32))));
+			const int G = 32 / K;
+			const int a = lane & (K - 1), sub = lane / K;
+			const bool home = a < k;
+			int i = -1;
+			float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f), p = x, q = x;
+			if (home) {
+				const int hp = hb + a;
+				p = sp[hp];
+				i = __float_as_int(p.w);
+				q = sr[hp];
+				x = sx[hp];
+			}
+			const bool live = home && isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
+			const int oi = __float_as_int(q.w);
+			const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
+			unsigned int gmask = 0u;   // lanes of this lane's home particle
+			for (int l = a; l < 32; l += K) gmask |= 1u << l;
+			int cnt = 0;
+			bool over = false;
+			for (int e0 = 0; e0 < E; e0 += G) {
+				const int e = e0 + sub;
+				// cell of entry e: the last cell whose offset is <= e
+				int kc = 0;
+#pragma unroll
+				for (int step = 16; step > 0; step >>= 1) {
+					const int mid = kc + step;
+					const int v = __shfl_sync(0xffffffffu, off, mid < 27 ? mid : 26);
+					if (mid < 27 && v <= e) kc = mid;
+				}
+				const int t = __shfl_sync(0xffffffffu, cs, kc) + (e - __shfl_sync(0xffffffffu, off, kc));
+				bool pass = false;
+				int code = 0;
+				if (live && e < E) {
+					const float4 pj = sp[t];
+					const int j = __float_as_int(pj.w);
+					const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+					const float d2 = ex * ex + ey * ey + ez * ez;
+					const bool near_same = d2 < search2;
+					if (j != i && (near_same || !single_object)) {
+						const float4 rj = sr[t];
+						const bool cross = __float_as_int(rj.w) != oi;
+						if (cross || within) {
+							const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
+							const float q2 = qx * qx + qy * qy + qz * qz;
+							code = j;
+							if (cross) {
+								const float4 xj = sx[t];
+								const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
+								const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
+								const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
+								const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
+								pass = (dist_x < search + rel) && (q2 >= cross_excl2);
+								if (rel > fast_rel) code = -(j + 1);
+							}
+							else
+								pass = near_same && (q2 >= excl2);
+						}
+					}
+				}
+				const unsigned int acc = __ballot_sync(0xffffffffu, pass) & gmask;
+				const int rank = __popc(acc & lt_mask);
+				if (pass && cnt + rank < kSelfColMax) contacts[(size_t)i * kSelfColMax + cnt + rank] = code;
+				cnt += __popc(acc);
+				over = over || cnt > kSelfColMax;
+			}
+			if (home && sub == 0) {
+				if (over) fix_list[atomicAdd(&ctr->sc_fix_count, 1u)] = i;
+				else { counts[i] = cnt; total += (unsigned int)cnt; }
+			}
+			hb += k;
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+	if (lane == 0 && total > 0u) atomicAdd(&ctr->sc_contacts, total);
+}
+
+// The particles whose lists reached the cap: sequential build with the replacement
+// rule (sc_build_one), grid-stride over the fix-up list.
+__global__ void __launch_bounds__(kBlock) k_sc_fixup(const int* __restrict__ fix_list, const StepParams* __restrict__ P,
+	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
+	const int* __restrict__ start, unsigned int mask, const int* __restrict__ obj_id, const float4* __restrict__ sp,
+	const float4* __restrict__ sr, const float4* __restrict__ sx, DevCounters* __restrict__ ctr,
+	int* __restrict__ contacts, int* __restrict__ counts)
+{
+	const unsigned int nfix = ctr->sc_fix_count;
+	for (unsigned int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfix; f += gridDim.x * blockDim.x) {
+		const int i = fix_list[f];
+		int over = 0;
+		const int cnt = sc_build_one(i, P, X, Pp, rest, start, mask, obj_id, sp, sr, sx, ctr, contacts, over);
+		counts[i] = cnt;
+		atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
+		if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
+	}
 }
 
 __device__ __forceinline__ bool sc_start_normal(float4 xi, float4 xj, float4 qi, float4 qj, float& nx, float& ny,
@@ -2256,6 +2496,42 @@ __global__ void k_attach(int count, const int* __restrict__ idx, const float* __
 	pos_curr[i] = make_float4(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2], 0.0f);
 	vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	if (obj_w) obj_w[i] = weight;   // rigid-fit weight of object mode (forward.cu:6724)
+}
+
+// caller-order positions into the internal order, inverse masses kept
+__global__ void k_set_positions(int n, const float* __restrict__ pos3, const int* __restrict__ perm,
+	float4* __restrict__ pos, float* __restrict__ pos_out3)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const int o = perm[i];
+	const float x = pos3[3 * o], y = pos3[3 * o + 1], z = pos3[3 * o + 2];
+	pos[i] = make_float4(x, y, z, pos[i].w);
+	pos_out3[3 * o] = x; pos_out3[3 * o + 1] = y; pos_out3[3 * o + 2] = z;
+}
+
+// serving arena: copy of an index array with every non-negative entry shifted by delta
+__global__ void k_copy_shift(long long count, const int* __restrict__ src, int* __restrict__ dst, int delta)
+{
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= count) return;
+	const int v = src[i];
+	dst[i] = v >= 0 ? v + delta : v;
+}
+__global__ void k_fill_int(int n, int* __restrict__ a, int v)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) a[i] = v;
+}
+// a retired session's rows stay in place, frozen: inverse mass 0 (also the value pin
+// releases restore), velocity 0
+__global__ void k_freeze_rows(int n, float4* __restrict__ pos, float4* __restrict__ vel, float* __restrict__ saved_w)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	pos[i].w = 0.0f;
+	vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	saved_w[i] = 0.0f;
 }
 
 __global__ void k_fill(int n, float* __restrict__ a, float v)
@@ -2987,7 +3263,7 @@ __global__ void k_obj_push_solve(int blocks, int K, const float* __restrict__ pa
 // (groundProjectKernel, forward.cu:7405-7421) when it is on
 __global__ void __launch_bounds__(kBlock) k_obj_push_apply(int n, const StepParams* __restrict__ P,
 	const int* __restrict__ obj_id, const float4* __restrict__ accum, const float* __restrict__ T,
-	const DevCounters* __restrict__ ctr, float4* __restrict__ pos)
+	const DevCounters* __restrict__ ctr, float4* __restrict__ pos, const float* __restrict__ crg)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
@@ -3004,7 +3280,7 @@ __global__ void __launch_bounds__(kBlock) k_obj_push_apply(int n, const StepPara
 		}
 	}
 	if (P->ground_on) {
-		const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane;
+		const float c = P->gn[0] * p.x + P->gn[1] * p.y + P->gn[2] * p.z - P->ground_plane - (crg ? crg[i] : 0.0f);
 		if (c < 0.0f) {
 			p.x = p.x - c * P->gn[0]; p.y = p.y - c * P->gn[1]; p.z = p.z - c * P->gn[2];
 			moved = true;

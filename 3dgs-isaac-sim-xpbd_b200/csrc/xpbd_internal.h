@@ -75,6 +75,7 @@ struct DevCounters {
 	unsigned int shapes_deformed;
 	unsigned int shapes_kept;
 	unsigned int sc_active;         // Gaussians in the grid when the object box filter is on ([2])
+	unsigned int sc_fix_count;      // particles whose candidate lists reached the cap (fix-up list)
 	int kin_hits[kMaxColliders];
 	float kin_push[kMaxColliders * kColliderAcc];
 	double jstats[3];               // sum V, sum V J, sum V J^2

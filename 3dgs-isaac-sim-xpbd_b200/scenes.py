@@ -286,6 +286,124 @@ def dense_contact_scenario(n=4_000_000, seed=0, **kw):
     return Scenario(scene, plates, **kw)
 
 
+class RuntimeScenario:
+    """The Isaac runtime's own configuration and call order, on a synthetic object.
+
+    Setup as runtime_loop.py:246-257 (constants at runtime_loop.py:39-71): one solver step
+    per 60 Hz frame with dt 1/60 and 16 iterations, distance and volume constraints
+    (volume compliance 1e-6, 3-ring candidates, 2048-member cap, leader spacing 2), shape
+    matching off with the float polar, object shape keeping 0.9 on the device, ellipsoid
+    contacts (``contact_bits``; the runtime's 1 = colliders) with tau 0.2 and a 0.02 cap,
+    the ground off and gravity 0 for the first (upload) step, then reset, launch at rest
+    and release (runtime_loop.py:402-408).
+
+    Per frame as runtime_loop.py:519-548 and 393-401: the ground plane under the object
+    (restitution 0.9, friction 0.5, contact radius 0.003 H and slop 0.002 H of the object
+    height H, gravity 5.81) set once, two spherical finger pads as colliders (margin
+    0.003 H, friction 0.5), the held Gaussians pinned with the runtime's hold weight, one
+    step, the collider statistics, the positions and the deformed shapes (deform eps
+    1e-2), which re-pack the contact ellipsoids (xpbd_capi.cu:255-256).
+
+    The pads close on the object along y for ``close`` frames (contact only), then each
+    holds the Gaussians within ``hold_radius`` of its centre where they are at that frame
+    (``grasp_pos``, read from the solver unless given) and lifts them +z."""
+
+    ITERS, DT, GRAVITY, FRICTION, RESTITUTION, DAMPING = 16, 1.0 / 60.0, 5.81, 0.5, 0.9, 0.01
+    CONTACT_TAU, CONTACT_CAP, DEFORM_EPS, HOLD_WEIGHT, OBJECT_SHAPE = 0.2, 0.02, 1e-2, 1.0, 0.9
+
+    def __init__(self, scene, contact_bits=1, close=15, close_speed=0.01, lift_speed=0.004, pad_radius=0.1,
+                 pad_gap=0.02, hold_radius=0.13, grasp_pos=None):
+        self.scene = scene
+        self.contact_bits = int(contact_bits)
+        p = scene["pos"].astype(np.float64)
+        self.H = float(p[:, 2].max() - p[:, 2].min())
+        self.floor = float(p[:, 2].min()) - 0.003 * self.H
+        ymax = float(np.abs(p[:, 1]).max())
+        self.pad0 = [np.array([0.0, -(ymax + pad_radius + pad_gap), 0.0]),
+                     np.array([0.0, ymax + pad_radius + pad_gap, 0.0])]
+        self.pad_dir = [np.array([0.0, 1.0, 0.0]), np.array([0.0, -1.0, 0.0])]
+        self.close, self.close_speed, self.lift_speed = int(close), float(close_speed), float(lift_speed)
+        self.pad_radius, self.hold_radius = float(pad_radius), float(hold_radius)
+        self.grasp_pos = grasp_pos
+        self.grasp_idx = None
+        self.k = 0
+
+    @property
+    def n(self):
+        return self.scene["pos"].shape[0]
+
+    def pad_centre(self, side, frame):
+        t = min(frame, self.close)
+        c = self.pad0[side] + self.pad_dir[side] * (self.close_speed * t)
+        return c + np.array([0.0, 0.0, self.lift_speed * max(0, frame - self.close)])
+
+    def colliders(self, frame):
+        poses = [np.concatenate([np.eye(3).reshape(-1), self.pad_centre(s, frame)]) for s in (0, 1)]
+        dims = [[self.pad_radius, 0.0, 0.0]] * 2
+        return [0, 0], np.asarray(poses, np.float32), np.asarray(dims, np.float32)
+
+    def setup(self, solver):
+        solver.create(self.scene)
+        solver.set_solver(iters=self.ITERS, dt=self.DT, under_relax=0.6, vel_damping=self.DAMPING)
+        solver.set_constraints(distance=True, shape=False, angle=False, volume=True)
+        solver.set_volume(compliance=1e-6, ring_k=3, max_members=2048, leader_min_hop=2)
+        solver.set_shape_robust(False)
+        solver.set_object_shape(self.OBJECT_SHAPE)
+        solver.set_object_shape_gpu(True)
+        solver.set_self_collision(False, 1.5, 2.0, False)   # settings outlive create: the runtime's default
+        solver.volume_stats(False)
+        ok = solver.set_contact_shape(self.contact_bits, self.CONTACT_TAU, self.CONTACT_CAP)
+        solver.set_ground(False, (0.0, 0.0, 1.0), 0.0, gravity=0.0)
+        solver.step()
+        solver.reset()
+        solver.launch((0.0, 0.0, 0.0), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+        solver.clear_attached()
+        self.k = 0
+        self.grasp_idx = None
+        return ok
+
+    def _hold(self, solver, frame):
+        if frame <= self.close:
+            return
+        if self.grasp_idx is None:
+            pos = self.grasp_pos if self.grasp_pos is not None else solver.positions()
+            self.grasp_pos = np.asarray(pos, np.float32)
+            idx, ref = [], []
+            for s in (0, 1):
+                c = self.pad_centre(s, self.close)
+                d2 = ((self.grasp_pos.astype(np.float64) - c) ** 2).sum(1)
+                sel = np.nonzero(d2 <= self.hold_radius ** 2)[0]
+                idx.append(sel)
+                ref.append(self.grasp_pos[sel].astype(np.float64) - c)
+            self.grasp_idx, self.grasp_rel = idx, ref
+        idx, pos = [], []
+        for s in (0, 1):
+            idx.append(self.grasp_idx[s])
+            pos.append(self.pad_centre(s, frame) + self.grasp_rel[s])
+        idx = np.concatenate(idx).astype(np.int32)
+        if len(idx) == 0:
+            return
+        w = max(1.0, self.HOLD_WEIGHT * (self.n - len(idx)) / len(idx))
+        solver.set_attached(idx, np.concatenate(pos).astype(np.float32), w)
+
+    def advance(self, solver, count, record=None):
+        """``count`` frames; ``record(solver, frame, shapes)`` after each when given."""
+        for _ in range(count):
+            if self.k == 0:
+                solver.set_ground(True, (0.0, 0.0, 1.0), self.floor, friction=self.FRICTION,
+                                  restitution=self.RESTITUTION, contact_radius=0.003 * self.H,
+                                  contact_slop=0.002 * self.H, gravity=self.GRAVITY)
+            types, poses, dims = self.colliders(self.k + 1)
+            solver.set_colliders(types, poses, dims, margin=0.003 * self.H, friction=self.FRICTION)
+            self._hold(solver, self.k + 1)
+            solver.step()
+            self.k += 1
+            solver.collider_stats(2)
+            shapes = solver.shapes(self.DEFORM_EPS)
+            if record is not None:
+                record(solver, self.k, shapes)
+
+
 def bbox_diagonal(pos):
     p = np.asarray(pos, dtype=np.float64)
     return float(np.linalg.norm(p.max(0) - p.min(0)))

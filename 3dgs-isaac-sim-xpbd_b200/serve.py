@@ -1,16 +1,20 @@
 """Continuous-batching service loop for deformation sessions.
 
 A session is a scene plus a stream of gripper poses (frames).  Sessions arrive over
-time; each is admitted while the resident solver state fits the HBM budget, uploaded
-by a background admission thread (host topology build + upload run beside the GPU
-work of the sessions already resident), and kept resident — one engine instance with
-its own CUDA stream per session — until its last frame.  Every tick, each resident
-session with a pending frame enqueues that frame's substeps on its stream; the GPU
-runs all of them concurrently, and the tick ends when all are done.  A step's latency
-is the time from when it became pending (its session was admitted, or its previous
-step finished) to when its results are ready.
+time and wait in arrival order; each is admitted while it fits the HBM budget (and, if
+one is given, while the arena's predicted step time stays within a latency target).  An
+admission thread builds the session's topology and takes its first substep on an
+engine of its own (beside the GPU work of the resident sessions), then the session
+joins the serving arena (bridge.Arena): its state and topology are copied into the
+arena's packed buffers, where it stays resident until its last frame.  Every tick
+advances every resident session by one frame with ONE library call — one launch
+sequence (one CUDA-graph replay) per substep covers all of them, whatever their sizes —
+carrying every session's collider poses and pin targets.  A step's latency is the time
+from when it became pending (the session joined, or its previous step finished) to
+when its results are ready.
 
-The plain form for comparison steps one session at a time, start to finish.
+The plain form for comparison steps one session at a time, start to finish, each on an
+engine of its own.
 """
 import collections
 import math
@@ -22,7 +26,25 @@ import numpy as np
 
 from . import bridge, scenes
 
-BYTES_PER_GAUSSIAN = 3200   # resident estimate: state, graph, clusters, transposed clusters, blackboard
+BYTES_PER_GAUSSIAN = 3200   # a session engine of its own: state, graph, clusters, transposed clusters, blackboard
+# arena bytes per row (Gaussian): 7 float4 state arrays, caller-order positions, order,
+# object id, multiplier, rest volume terms, material, cluster record, saved inverse
+# mass, three CSR row starts; per directed edge 16 B, per member and reverse entry 4 B
+ARENA_ROW_BYTES = 212
+ARENA_EDGES, ARENA_MEMBERS, ARENA_REV = 12, 66, 68      # capacity per row (8-NN graph, 64-member clusters)
+
+
+def arena_capacity(budget_bytes):
+    """(rows, edges, members, reverse entries) of an arena that fits `budget_bytes`; the
+    arena's CSR offsets are 32-bit, which caps it near 31M rows at these ratios."""
+    per = ARENA_ROW_BYTES + 16 * ARENA_EDGES + 4 * ARENA_MEMBERS + 4 * ARENA_REV
+    rows = max(1, min(int(budget_bytes // per), (2 ** 31 - 1) // ARENA_REV))
+    return rows, rows * ARENA_EDGES, rows * ARENA_MEMBERS, rows * ARENA_REV
+
+
+def arena_bytes(n):
+    """Arena bytes a session of n Gaussians holds (at the capacity ratios)."""
+    return n * (ARENA_ROW_BYTES + 16 * ARENA_EDGES + 4 * ARENA_MEMBERS + 4 * ARENA_REV)
 
 
 def make_sessions(rate, duration, seed=0, n_min=5000, n_max=500000, max_frames=120):
@@ -46,6 +68,8 @@ class Session:
         self.n = n
         self.scen = None
         self.solver = None
+        self.slot = -1
+        self.final = None
         self.pending_since = None
         self.latencies = []
 
@@ -93,18 +117,31 @@ def prepare_sessions(sessions):
     return out
 
 
-def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=None):
+def _frame_arrays(resident, substeps):
+    """Collider poses and pin targets of the next frame of every resident session, as
+    the arena's step call takes them."""
+    types, poses, dims, cslot, pslot, pidx, targets = [], [], [], [], [], [], []
+    for s in resident:
+        ty, po, di, idx, tg = s.scen.frame_inputs(substeps)
+        types.append(ty); poses.append(po); dims.append(di); cslot.append(np.full(len(ty), s.slot, np.int32))
+        pidx.append(idx); targets.append(tg); pslot.append(np.full(len(idx), s.slot, np.int32))
+    cat = np.concatenate
+    return (cat(types), cat(poses, axis=1), cat(dims), cat(cslot), cat(pslot), cat(pidx), cat(targets, axis=1))
+
+
+def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=None, latency_target_ms=None,
+               keep_results=True):
     """Serve `sessions` (tuples from make_sessions, or prepared Session objects) with
-    continuous batching.  Returns stats."""
+    continuous batching in one arena.  Admission in arrival order while the session fits
+    the budget and — with `latency_target_ms` — while the resident Gaussians, at the
+    throughput measured so far, keep a tick within the target.  Returns stats."""
     t0 = time.perf_counter()
+    arena = bridge.Arena(lib_path, *arena_capacity(budget_bytes))
     arrivals = collections.deque(sessions)
     ready = queue.Queue()
-    resident = []
-    resident_bytes = [0.0]
-    lock = threading.Lock()
     stop = threading.Event()
-    queued = [0]                # sessions handed to the admission thread
     backlog = queue.Queue()
+    errors = []
 
     def admitter():
         while not stop.is_set():
@@ -112,68 +149,106 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                 sess = backlog.get(timeout=0.05)
             except queue.Empty:
                 continue
-            sess.admit(lib_path)
+            try:
+                sess.admit(lib_path)
+            except Exception as e:   # surfaced by the serving loop
+                errors.append(e)
             ready.put(sess)
 
     worker = threading.Thread(target=admitter, daemon=True)
     worker.start()
     waiting = collections.deque()
-    done, work, ticks = [], 0, 0
+    resident, joining = [], []
+    done, work, ticks, resident_bytes, resident_gauss, queued = [], 0, 0, 0.0, 0, 0
+    throughput = None            # Gaussian-substeps/s of the ticks so far
+    waits = []
     sid = 0
-    while arrivals or waiting or resident or queued[0] > len(done):
-        now = time.perf_counter() - t0
-        if max_wall and now > max_wall:
-            break
-        while arrivals and _arrival(arrivals[0]) * time_scale <= now:
-            item = arrivals.popleft()
-            if isinstance(item, Session):
-                waiting.append(item)
-            else:
-                a, n, frames, seed = item
-                waiting.append(Session(sid, a * time_scale, n, frames, seed))
-            sid += 1
-        # admission by resident-byte budget, in arrival order
-        while waiting:
-            need = waiting[0].n * BYTES_PER_GAUSSIAN
-            with lock:
-                if resident_bytes[0] + need > budget_bytes:
+    try:
+        while arrivals or waiting or resident or joining or queued > len(done):
+            now = time.perf_counter() - t0
+            if max_wall and now > max_wall:
+                break
+            if errors:
+                raise errors[0]
+            while arrivals and _arrival(arrivals[0]) * time_scale <= now:
+                item = arrivals.popleft()
+                if isinstance(item, Session):
+                    waiting.append(item)
+                else:
+                    a, n, frames, seed = item
+                    waiting.append(Session(sid, a * time_scale, n, frames, seed))
+                sid += 1
+            # admission in arrival order: HBM budget, then the latency target
+            while waiting:
+                s = waiting[0]
+                need = arena_bytes(s.n)
+                if resident_bytes + need > budget_bytes:
                     break
-                resident_bytes[0] += need
-            backlog.put(waiting.popleft())
-            queued[0] += 1
-        while not ready.empty():
-            s = ready.get()
-            s.pending_since = time.perf_counter()
-            resident.append(s)
-        if not resident:
-            time.sleep(0.001)
-            continue
-        for s in resident:
-            s.enqueue_frame()
-        for s in resident:
-            s.solver.lib.xpbd_b200_sync()
-        t_end = time.perf_counter()
-        ticks += 1
-        still = []
-        for s in resident:
-            s.latencies.append(t_end - s.pending_since)
-            s.pending_since = t_end
-            work += s.n * s.scen.substeps
-            if s.frames_left <= 0:
-                with lock:
-                    resident_bytes[0] -= s.n * BYTES_PER_GAUSSIAN
-                s.close()
-                done.append(s)
-            else:
-                still.append(s)
-        resident = still
-    stop.set()
-    worker.join(timeout=5)
+                if latency_target_ms and resident_gauss > 0 and throughput:
+                    tick_ms = (resident_gauss + s.n) * s.substeps / throughput * 1e3
+                    if tick_ms > latency_target_ms:
+                        break
+                resident_bytes += need
+                resident_gauss += s.n
+                backlog.put(waiting.popleft())
+                queued += 1
+            while not ready.empty():
+                joining.append(ready.get())
+            still_joining = []
+            for s in joining:
+                slot = arena.admit(s.solver)
+                if slot is None:          # full until sessions leave (compaction ran already)
+                    still_joining.append(s)
+                    continue
+                s.slot = slot
+                s.solver.close()          # the arena holds the session's state now
+                s.solver = None
+                s.pending_since = time.perf_counter()
+                waits.append(s.pending_since - t0 - s.arrival)
+                resident.append(s)
+            joining = still_joining
+            if not resident:
+                time.sleep(0.001)
+                continue
+            sub = resident[0].scen.substeps
+            ty, po, di, cs, ps, pi, tg = _frame_arrays(resident, sub)
+            t_tick = time.perf_counter()
+            arena.step(sub, ty, po, di, cs, ps, pi, tg)
+            arena.sync()
+            t_end = time.perf_counter()
+            ticks += 1
+            tick_work = sum(s.n for s in resident) * sub
+            rate = tick_work / max(t_end - t_tick, 1e-9)
+            throughput = rate if throughput is None else 0.8 * throughput + 0.2 * rate
+            still = []
+            for s in resident:
+                s.scen.k += sub
+                s.frames_left -= 1
+                s.latencies.append(t_end - s.pending_since)
+                s.pending_since = t_end
+                work += s.n * sub
+                if s.frames_left <= 0:
+                    if keep_results:
+                        s.final = arena.positions(s.slot, s.n)
+                    arena.retire(s.slot)
+                    resident_bytes -= arena_bytes(s.n)
+                    resident_gauss -= s.n
+                    done.append(s)
+                else:
+                    still.append(s)
+            resident = still
+    finally:
+        stop.set()
+        worker.join(timeout=5)
+        usage = arena.usage()
+        arena.close()
     wall = time.perf_counter() - t0
     lat = np.concatenate([np.asarray(s.latencies) for s in done]) if done else np.zeros(1)
     return {"sessions": len(done), "steps": int(lat.size), "wall_s": wall, "ticks": ticks,
             "gauss_substeps_per_s": work / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "sessions_done": done}
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "admission_wait_p50_s": float(np.percentile(waits, 50)) if waits else 0.0,
+            "arena_rows_cap": usage["rows_cap"], "sessions_done": done}
 
 
 def _arrival(item):

@@ -18,7 +18,12 @@ e2e       the same frames through the reference-facing C ABI (xpbd_set_colliders
 roofline  the dominant kernel's algorithmic bytes / its mean CUDA-event duration, from
           the timed frames repeated with an event pair around every kernel, against the
           measured HBM copy bandwidth;
-cpu_baseline  the CPU oracle (OpenMP, all host cores) on a bounded sample.
+cpu_baseline  the CPU oracle (OpenMP, all host cores) on a bounded sample;
+reference_gpu the reference's own CUDA solver compiled from its sources (oracle/_ref) on
+          the same workload and GPU, ms per substep and the ratio;
+batched, served  (default large config, one GPU) the batched 64-object and served
+          halves of the headline metric at reduced step counts, each with its plain
+          one-scene-at-a-time comparison (--config batched / served run them alone).
 
 --impl reference times the reference's CPU path.  The reference has no CPU XPBD
 solver, so this is the C restatement oracle/liboracle.so with all host threads; each
@@ -288,7 +293,45 @@ def bench_b200(args, rank, world):
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, scen_maker=make)
     x.destroy()
+    if world == 1 and args.config == "large" and not args.no_extras:
+        # the other halves of the headline metric, and the reference's own CUDA solver on
+        # this workload and GPU, each at a reduced step count
+        line["reference_gpu"] = reference_gpu(make, ms / (SUBSTEPS * args.steps))
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = 2, 1
+        b = bench_batched(sub, 0, 1)
+        line["batched"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "config", "plain",
+                                             "speedup_vs_plain")}
+        sv = bench_served(sub, 0, 1)
+        line["served"] = {"value": sv["value"], "unit": sv["unit"], "p50_ms": sv["served"]["p50_ms"],
+                          "p99_ms": sv["served"]["p99_ms"], "config": sv["config"], "served": sv["served"],
+                          "plain": sv["plain"], "speedup_vs_plain": sv["speedup_vs_plain"]}
     return line
+
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libxpbd_ref.so")
+
+
+def reference_gpu(make, our_ms_per_substep, substeps=20):
+    """The reference's own CUDA solver, compiled from its sources (oracle/_ref, built by
+    `make -C oracle ref`), on the same workload and GPU through its C ABI: blocking
+    xpbd_step per substep with pins and collider poses re-sent, as a caller does.  A
+    side-by-side figure; nothing of it is on this library's path."""
+    if not os.path.isfile(REF_SO):
+        return {"unavailable": "oracle/_ref/libxpbd_ref.so not built (reference checkout absent at build time)"}
+    scen = make()
+    ref = pkg.bridge.XPBD(REF_SO)
+    scen.setup(ref)
+    ref.volume_stats(False)
+    scen.advance(ref, 11)                        # upload, topology build, warm-up
+    t0 = time.perf_counter()
+    scen.advance(ref, substeps)
+    dt = time.perf_counter() - t0
+    ref.destroy()
+    ms = dt / substeps * 1e3
+    return {"impl": "reference CUDA solver compiled from its sources (sm_100a), blocking xpbd_step",
+            "ms_per_substep": ms, "value": scen.n * substeps / dt, "unit": UNIT, "substeps": substeps,
+            "this_ms_per_substep": our_ms_per_substep, "speedup": ms / our_ms_per_substep}
 
 
 def metric_for(config, n):
@@ -498,6 +541,7 @@ def bench_chainmail(args, rank, world):
     if not args.no_cpu_baseline:
         lib = os.path.join(ROOT, "oracle", "liboracle.so")
         o = pkg.bridge.XPBD(lib)
+        o.CHAINMAIL_PREFIX = "oracle_"           # the oracle's ChainMail entry points
         o.lib.oracle_get_threads.restype = ctypes.c_int
         o.create(sc)
         o.step()
@@ -511,7 +555,34 @@ def bench_chainmail(args, rank, world):
         line["cpu_baseline"] = {"value": n * sweeps * k / dt, "unit": unit, "cores": int(o.lib.oracle_get_threads()),
                                 "kind": "port", "sample": f"{k} steps of the same {n}-Gaussian workload"}
         o.destroy()
+    if not args.no_extras:
+        line["reference_gpu"] = reference_gpu_chainmail(sc, seeds, ms / args.steps)
     return line
+
+
+def reference_gpu_chainmail(sc, seeds, our_ms_per_step):
+    """runChainmailGPU's dense path (forward.cu:12808-13006) of the reference compiled
+    from its sources, on the same scene, seeds and sweeps, through the accessor shim."""
+    if not os.path.isfile(REF_SO):
+        return {"unavailable": "oracle/_ref/libxpbd_ref.so not built (reference checkout absent at build time)"}
+    ref = pkg.bridge.XPBD(REF_SO)
+    ref.CHAINMAIL_PREFIX = "refshim_"
+    ref.create(sc)
+    ref.step()
+    ref.reset()
+    cm = scenes.CHAINMAIL_DEFAULTS
+    for k in range(2):
+        ref.chainmail_seed(*seeds[k])
+        ref.chainmail_run(**cm)
+    steps = min(len(seeds), 5)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        ref.chainmail_seed(*seeds[k])
+        ref.chainmail_run(**cm)
+    dt = time.perf_counter() - t0
+    ref.destroy()
+    return {"impl": "reference runChainmailGPU compiled from its sources (sm_100a)", "ms_per_step": dt / steps * 1e3,
+            "steps": steps, "this_ms_per_step": our_ms_per_step, "speedup": dt / steps * 1e3 / our_ms_per_step}
 
 
 RENDER_W, RENDER_H, RENDER_SH = 1920, 1080, 3
@@ -746,6 +817,8 @@ def main():
     ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail", "dense", "render"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="large config: skip the batched / served / reference-GPU sub-records")
     ap.add_argument("--gaussians", type=int, default=None,
                     help="scene size of the large/plain workload (default 1,000,000 / 20,000)")
     args = ap.parse_args()

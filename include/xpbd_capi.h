@@ -68,8 +68,11 @@ XPBD_API void xpbd_set_colliders(int count, const int* types, const float* poses
 XPBD_API int xpbd_collider_stats(int* hits, float* push, float* centroid, int maxCount);
 /* xpbd_capi.cu:167-172 — adds dv + dw x (x - center) to every free Gaussian's velocity */
 XPBD_API int xpbd_add_rigid_velocity(const float* dv, const float* dw, const float* center);
-/* xpbd_capi.cu:179-191 — ellipsoid contact shapes: 0 accepted; enabling returns -1
- * (not implemented) */
+/* xpbd_capi.cu:179-191 — ellipsoid contact shapes: bit 1 colliders, bit 2 ground, 0 off.
+ * Each Gaussian meets them as its opacity-tau iso-ellipsoid (semi-axes capped at
+ * radiusCap when > 0), packed from the created shapes, then re-packed from the deformed
+ * shapes by every xpbd_compute_shapes.  Before the first step the pack waits for the
+ * scene's upload.  Ends with the scene (create / destroy). */
 XPBD_API int xpbd_set_contact_shape(int enabled, float tau, float radiusCap);
 /* xpbd_capi.cu:195-200 — pins idx[count] at pos[3 count] (inverse mass 0, velocity 0);
  * count 0 releases; the previous pins' inverse masses are restored first */
@@ -220,6 +223,34 @@ XPBD_API int xpbd_b200_sizes(long long* out);
 /* Stage buffers by name, for parity checks (count only when out is NULL). */
 XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap);
 XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap);
+/* Serving arena: many sessions resident in one engine's packed buffers, advanced
+ * together by one launch sequence (one CUDA-graph replay) per substep.  Capacities in
+ * rows (Gaussians), directed edges, cluster members and reverse-list entries, each at
+ * most 2^31-1 (32-bit CSR offsets).  A session joins with arena_admit(arena, engine): an
+ * engine handle (xpbd_b200_engine_new) that has built its scene and taken at least one
+ * step; its state and topology are copied in (the engine may then be freed) and its
+ * slot is returned, or -2 when it does not fit even after compaction, or -1 on error.
+ * Sessions share the solver settings; self-collision, ground, object shape and contact
+ * shapes stay off.  arena_retire frees a slot; arena_step enqueues k substeps of every
+ * live session with per-substep collider poses poses[k][ncol][12] acting on the sessions
+ * col_slot[ncol] and pins (session pin_slot[p], its Gaussian pin_idx[p] in the session's
+ * order) at targets[k][npin][3]; arena_positions copies a session's committed positions
+ * (float3[n], its order); usage fills out[10]: rows used / capacity, edges, members,
+ * reverse entries (used, capacity), live Gaussians, sessions. */
+XPBD_API void* xpbd_b200_arena_new(long long rows, long long edges, long long members, long long rev);
+XPBD_API int xpbd_b200_arena_admit(void* arena, void* session);
+XPBD_API int xpbd_b200_arena_retire(void* arena, int slot);
+XPBD_API int xpbd_b200_arena_step(void* arena, int k, int ncol, const int* types, const float* poses,
+	const float* dims, const int* col_slot, float margin, float friction, int npin, const int* pin_slot,
+	const int* pin_idx, const float* targets);
+XPBD_API int xpbd_b200_arena_positions(void* arena, int slot, float* out, int n);
+XPBD_API int xpbd_b200_arena_sync(void* arena);
+XPBD_API int xpbd_b200_arena_usage(void* arena, long long* out);
+XPBD_API void xpbd_b200_arena_free(void* arena);
+/* Current positions from the caller (float3[n], caller order), velocities kept; after
+ * the first step.  Lets a caller teleport the state, and a test run the deformed-shape
+ * writeback on positions another solver produced. */
+XPBD_API int xpbd_b200_set_positions(const float* pos, int n);
 /* The once-per-step self-collision build on given start / predicted positions
  * (x[3n], p[3n]); returns the candidate total.  Solver state is left unchanged. */
 XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p);

@@ -290,6 +290,11 @@ static struct {
 	int obj_shift_valid;
 	f3* obj_accum;
 	unsigned char* sc_act;
+	/* ellipsoid contact shapes (forward.cu:150-160; xpbd_capi.cu:25-27, 181-191):
+	 * M = k^2 Sigma [6 per Gaussian: xx xy xz yy yz zz], longest semi-axis, ground radius */
+	int contact_on, contact_col, contact_ground, contact_n;
+	float contact_tau, contact_cap;
+	float *contact_M, *contact_rmax, *contact_rg;
 } S;
 
 /* parameters: file statics of forward.cu with their defaults (forward.cu:53-92, 224-265, 300-361) */
@@ -361,6 +366,10 @@ static void free_state(void)
 static void free_all(void)
 {
 	free_state();
+	/* free_all of xpbd_capi.cu:55-56: contact shapes off with the scene */
+	FREE(S.contact_M); FREE(S.contact_rmax); FREE(S.contact_rg);
+	S.contact_on = S.contact_col = S.contact_ground = 0;
+	S.contact_n = 0;
 	FREE(S.pos_in); FREE(S.scales); FREE(S.rots); FREE(S.opacity);
 	FREE(S.edges); FREE(S.edge_rest); FREE(S.edge_stiff);
 	S.n = 0;
@@ -1521,8 +1530,50 @@ static void shape_matching(const f3* pin, f3* pout, float dt)
 	}
 }
 
-/* kinColliderProjectKernel (forward.cu:7425-7518), point contact (no ellipsoid shapes) */
-static void colliders_project(f3* pos, int countHits)
+/* contactSupport (forward.cu:7387-7392): support distance sqrt(n^T M n) */
+static inline float contact_support(const float* m, float nx, float ny, float nz)
+{
+	const float q = m[0] * nx * nx + m[3] * ny * ny + m[5] * nz * nz
+		+ 2.0f * (m[1] * nx * ny + m[2] * nx * nz + m[4] * ny * nz);
+	return sqrtf(fmaxf(q, 0.0f));
+}
+
+/* contactShapePackKernel (forward.cu:7358-7385) over n Gaussians */
+static void contact_pack(const float* sc, const float* qt, const float* op, int n, float tau, float rcap)
+{
+	if (S.contact_n != n) {
+		FREE(S.contact_M); FREE(S.contact_rmax); FREE(S.contact_rg);
+		S.contact_M = malloc(sizeof(float) * 6 * n);
+		S.contact_rmax = malloc(sizeof(float) * n);
+		S.contact_rg = calloc(n, sizeof(float));
+		S.contact_n = n;
+	}
+	for (int i = 0; i < n; ++i) {
+		const float a = op[i];
+		const float k = (a > tau && tau > 0.0f) ? sqrtf(2.0f * logf(a / tau)) : 0.0f;
+		float e0 = k * sc[3 * i], e1 = k * sc[3 * i + 1], e2 = k * sc[3 * i + 2];
+		if (rcap > 0.0f) { e0 = fminf(e0, rcap); e1 = fminf(e1, rcap); e2 = fminf(e2, rcap); }
+		if (!(isfinite(e0) && isfinite(e1) && isfinite(e2))) { e0 = e1 = e2 = 0.0f; }
+		float w = qt[4 * i], x = qt[4 * i + 1], y = qt[4 * i + 2], z = qt[4 * i + 3];
+		const float qn = sqrtf(w * w + x * x + y * y + z * z);
+		if (qn > 1e-20f) { w /= qn; x /= qn; y /= qn; z /= qn; } else { w = 1.0f; x = y = z = 0.0f; }
+		const float r00 = 1 - 2 * (y * y + z * z), r01 = 2 * (x * y - w * z), r02 = 2 * (x * z + w * y);
+		const float r10 = 2 * (x * y + w * z), r11 = 1 - 2 * (x * x + z * z), r12 = 2 * (y * z - w * x);
+		const float r20 = 2 * (x * z - w * y), r21 = 2 * (y * z + w * x), r22 = 1 - 2 * (x * x + y * y);
+		const float l0 = e0 * e0, l1 = e1 * e1, l2 = e2 * e2;
+		float* m = &S.contact_M[6 * i];
+		m[0] = r00 * r00 * l0 + r01 * r01 * l1 + r02 * r02 * l2;
+		m[1] = r00 * r10 * l0 + r01 * r11 * l1 + r02 * r12 * l2;
+		m[2] = r00 * r20 * l0 + r01 * r21 * l1 + r02 * r22 * l2;
+		m[3] = r10 * r10 * l0 + r11 * r11 * l1 + r12 * r12 * l2;
+		m[4] = r10 * r20 * l0 + r11 * r21 * l1 + r12 * r22 * l2;
+		m[5] = r20 * r20 * l0 + r21 * r21 * l1 + r22 * r22 * l2;
+		S.contact_rmax[i] = fmaxf(e0, fmaxf(e1, e2));
+	}
+}
+
+/* kinColliderProjectKernel (forward.cu:7425-7518); cM / cRmax non-NULL: ellipsoid contacts */
+static void colliders_project(f3* pos, int countHits, const float* cM, const float* cRmax)
 {
 	const int N = S.n, nc = P.kin_count;
 	const float margin = P.kin_margin, mu = P.kin_friction;
@@ -1539,7 +1590,8 @@ static void colliders_project(f3* pos, int countHits)
 			if (S.inv_mass[idx] <= 0.0f) continue;
 			f3 p = pos[idx];
 			int moved = 0;
-			const float reach = margin + 0.0f;
+			const float rmax = cRmax ? cRmax[idx] : 0.0f;
+			const float reach = margin + rmax;
 			for (int c = 0; c < nc; ++c) {
 				const kin_t* C = &P.kin[c];
 				const float dx = p.x - C->t[0], dy = p.y - C->t[1], dz = p.z - C->t[2];
@@ -1573,6 +1625,10 @@ static void colliders_project(f3* pos, int countHits)
 				const float wx = C->R[0] * n0 + C->R[1] * n1 + C->R[2] * n2;
 				const float wy = C->R[3] * n0 + C->R[4] * n1 + C->R[5] * n2;
 				const float wz = C->R[6] * n0 + C->R[7] * n1 + C->R[8] * n2;
+				if (cM && rmax > 0.0f) {
+					dist -= contact_support(&cM[6 * idx], wx, wy, wz);
+					if (dist >= margin) continue;
+				}
 				const float corr = margin - dist;
 				const f3 pIn = p;
 				p.x += wx * corr; p.y += wy * corr; p.z += wz * corr;
@@ -1616,8 +1672,8 @@ static void colliders_project(f3* pos, int countHits)
 	}
 }
 
-/* groundProjectKernel (forward.cu:7405-7421), point contact */
-static void ground_project(f3* pos)
+/* groundProjectKernel (forward.cu:7405-7421); rg non-NULL: ellipsoid contacts */
+static void ground_project(f3* pos, const float* rg)
 {
 	const f3 n = mk3(P.ground_n[0], P.ground_n[1], P.ground_n[2]);
 	const float planeD = P.ground_h + P.ground_radius;
@@ -1625,13 +1681,13 @@ static void ground_project(f3* pos)
 	for (int i = 0; i < S.n; ++i) {
 		if (S.inv_mass[i] <= 0.0f) continue;
 		const f3 p = pos[i];
-		const float c = n.x * p.x + n.y * p.y + n.z * p.z - planeD;
+		const float c = n.x * p.x + n.y * p.y + n.z * p.z - planeD - (rg ? rg[i] : 0.0f);
 		if (c < 0.0f) pos[i] = mk3(p.x - c * n.x, p.y - c * n.y, p.z - c * n.z);
 	}
 }
 
 /* xpbdUpdateVelocityKernel (forward.cu:6623-6672) and ...GroundKernel (forward.cu:7528-7599) */
-static void velocity_commit(const f3* pfinal, float dt, int groundOn)
+static void velocity_commit(const f3* pfinal, float dt, int groundOn, const float* rg)
 {
 	const float velDamping = P.vel_damping;
 	const f3 n = mk3(P.ground_n[0], P.ground_n[1], P.ground_n[2]);
@@ -1670,7 +1726,7 @@ static void velocity_commit(const f3* pfinal, float dt, int groundOn)
 		const float dx2 = f3_len2(dx);
 		if (!isfinite(dx2)) { S.vel[idx] = mk3(0, 0, 0); S.pos_curr[idx] = p; continue; }
 		f3 v = (dx2 < 1e-18f) ? mk3(0, 0, 0) : f3_mul(dx, 1.0f / fmaxf(dt, 1e-8f));
-		const float gap = n.x * p.x + n.y * p.y + n.z * p.z - planeD;
+		const float gap = n.x * p.x + n.y * p.y + n.z * p.z - planeD - (rg ? rg[idx] : 0.0f);
 		if (gap <= slop) {
 			const float vn = n.x * v.x + n.y * v.y + n.z * v.z;
 			const float vnPre = n.x * vPre.x + n.y * vPre.y + n.z * vPre.z;
@@ -2279,7 +2335,7 @@ static void sc_active_set(const f3* X, const f3* Pp, float search, float dc)
 
 /* objectContactPush (forward.cu:11858-11890) and the ground re-projection after it
  * (forward.cu:12587-12597) */
-static void object_contact_push(f3* pos)
+static void object_contact_push(f3* pos, const float* rg)
 {
 	const int N = S.n, K = S.obj_k;
 	float* sums = calloc((size_t)K * 4, sizeof(float));
@@ -2311,7 +2367,7 @@ static void object_contact_push(f3* pos)
 	}
 	free(sums);
 	free(T);
-	if (P.ground_on) ground_project(pos);
+	if (P.ground_on) ground_project(pos, rg);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -2334,6 +2390,16 @@ static void run_step(void)
 	const int volGS = P.use_volume && P.vol_gs && S.vol_gs_ncolors > 0;
 	if (distGS) memset(S.gs_lam, 0, sizeof(float) * S.gs_nedges);
 	const int groundOn = P.ground_on;
+	/* ellipsoid contacts (forward.cu:12222-12228): the ground radius once per step */
+	const int contactOn = (S.contact_col || S.contact_ground) && S.contact_M && S.contact_n == N;
+	const float* cRg = NULL;
+	if (contactOn && S.contact_ground && groundOn) {
+		for (int i = 0; i < N; ++i)
+			S.contact_rg[i] = contact_support(&S.contact_M[6 * i], P.ground_n[0], P.ground_n[1], P.ground_n[2]);
+		cRg = S.contact_rg;
+	}
+	const float* cM = (contactOn && S.contact_col) ? S.contact_M : NULL;
+	const float* cRmax = (contactOn && S.contact_col) ? S.contact_rmax : NULL;
 	predict(gravity, dt);
 	const int objOn = object_on_ensure();
 	int limited = 0;
@@ -2383,11 +2449,11 @@ static void run_step(void)
 			f3* t = pin; pin = pout; pout = t;
 		}
 		if (P.sc_enabled && scContacts > 0) sc_solve_apply(pin, objOn ? S.obj_accum : NULL);
-		if (P.kin_count > 0) colliders_project(pin, it == P.iters - 1);
-		if (groundOn) ground_project(pin);
+		if (P.kin_count > 0) colliders_project(pin, it == P.iters - 1, cM, cRmax);
+		if (groundOn) ground_project(pin, cRg);
 	}
-	if (objOn && P.sc_enabled && scContacts > 0) object_contact_push(pin);
-	velocity_commit(pin, dt, groundOn);
+	if (objOn && P.sc_enabled && scContacts > 0) object_contact_push(pin, cRg);
+	velocity_commit(pin, dt, groundOn, cRg);
 	if (P.jstats && P.use_volume >= 0) volume_j_stats();
 }
 
@@ -2553,11 +2619,17 @@ EXPORT int xpbd_add_rigid_velocity(const float* dv, const float* dw, const float
 	return 0;
 }
 
+/* xpbd_set_contact_shape (xpbd_capi.cu:181-191): pack from the created shapes */
 EXPORT int xpbd_set_contact_shape(int enabled, float tau, float radiusCap)
 {
-	(void)tau; (void)radiusCap;
 	if (!S.created) return fail("xpbd_set_contact_shape: call xpbd_create first");
-	if (enabled) return fail("xpbd_set_contact_shape: ellipsoid contact is outside the oracle");
+	S.contact_on = enabled != 0;
+	S.contact_tau = tau;
+	S.contact_cap = radiusCap;
+	if (S.contact_on)
+		contact_pack(S.scales, S.rots, S.opacity, S.n, tau, (isfinite(radiusCap) && radiusCap > 0.0f) ? radiusCap : 0.0f);
+	S.contact_col = (enabled & 1) != 0;
+	S.contact_ground = (enabled & 2) != 0;
 	return 0;
 }
 
@@ -2796,6 +2868,10 @@ EXPORT int xpbd_compute_shapes(float deformEps, float* hostScales, float* hostQu
 	int deformed = 0;
 #pragma omp parallel for schedule(static) reduction(+ : deformed) num_threads(nthreads())
 	for (int i = 0; i < n; ++i) deformed += deformed_shape_node(i, deformEps, sc + 3 * i, qt + 4 * i);
+	/* contact ellipsoids follow the deformed shapes from the next step (xpbd_capi.cu:255-256) */
+	if (S.contact_on)
+		contact_pack(sc, qt, S.opacity, n, S.contact_tau,
+			(isfinite(S.contact_cap) && S.contact_cap > 0.0f) ? S.contact_cap : 0.0f);
 	if (hostScales) memcpy(hostScales, sc, sizeof(float) * 3 * n);
 	if (hostQuats) memcpy(hostQuats, qt, sizeof(float) * 4 * n);
 	free(sc);
@@ -2877,6 +2953,14 @@ EXPORT void xpbd_volume_stats(int enable, float* jvw, float* jvwStd)
 /* oracle-only accessors                                                      */
 /* ------------------------------------------------------------------------- */
 EXPORT void oracle_set_gs(int distance, int volume) { P.dist_gs = distance != 0; P.vol_gs = volume != 0; }
+/* current positions from the caller (float3[n]), velocities kept: lets a test run the
+ * deformed-shape writeback on positions another solver produced */
+EXPORT int oracle_set_positions(const float* pos, int n)
+{
+	if (!S.stepped || !pos || n != S.n) return fail("oracle_set_positions: no step yet or size mismatch");
+	for (int i = 0; i < n; ++i) S.pos_curr[i] = mk3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+	return 0;
+}
 EXPORT void oracle_set_volume_warp_mode(int mode) { P.warp_mode = mode; }
 EXPORT void oracle_set_threads(int n) { P.threads = n > 0 ? n : 0; }
 EXPORT int oracle_get_threads(void) { return nthreads(); }

@@ -30,6 +30,8 @@ extern "C" {
 
 /* Gauss-Seidel toggles (reference forward.cu:3780-3812, not in its C ABI). */
 void oracle_set_gs(int distance, int volume);
+/* current positions (float3[n], caller order); velocities are kept */
+int oracle_set_positions(const float* pos, int n);
 /* Volume Kernel A/B shape: 0 auto (warp when mean members >= 40), 1 thread, 2 warp
  * (forward.cu:4043-4060).  The modes differ only in summation order. */
 void oracle_set_volume_warp_mode(int mode);

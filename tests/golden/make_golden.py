@@ -30,6 +30,8 @@ REF_SO = os.path.join(ROOT, "oracle", "_ref", "libxpbd_ref.so")
 class Ref(pkg.bridge.XPBD):
     """Reference library plus its accessor shim (oracle/ref_shim.cu)."""
 
+    CHAINMAIL_PREFIX = "refshim_"
+
     def __init__(self):
         super().__init__(REF_SO)
         L = self.lib
@@ -65,6 +67,9 @@ class Ref(pkg.bridge.XPBD):
 
     def set_gs(self, dist, vol):
         self.lib.refshim_set_gs(int(dist), int(vol))
+
+    def chainmail_times(self):
+        return self.floats("cm_time")   # the reference keeps them in a file static
 
     def selfcol_build(self, x, p):
         x = np.ascontiguousarray(x, np.float32)
@@ -199,6 +204,38 @@ def chainmail_case(ref):
     return out
 
 
+RUNTIME_CHECKPOINTS = (1, 10, 30, 100)
+
+
+def runtime_case(ref, contact_bits):
+    """The Isaac runtime's configuration and call order (runtime_loop.py:39-71, 246-257,
+    393-401, 519-548) through scenes.RuntimeScenario: 16 iterations at dt 1/60, leader
+    spacing 2 with a 2048-member cap, object shape keeping, ellipsoid contacts, the ground
+    with gravity and restitution, finger pads that close, hold and lift."""
+    sc = scenes.make_scene(4000, 3)
+    scen = scenes.RuntimeScenario(sc, contact_bits=contact_bits)
+    out = scene_arrays(sc)
+    out["contact_bits"] = np.int64(contact_bits)
+    out["checkpoints"] = np.asarray(RUNTIME_CHECKPOINTS, np.int64)
+    hits = []
+
+    def record(solver, frame, shapes):
+        hits.append(solver.collider_stats(2)[0])
+        if frame in RUNTIME_CHECKPOINTS:
+            out[f"pos_{frame}"] = solver.positions()
+            out[f"vel_{frame}"] = ref.floats("vel").reshape(-1, 3)
+            out[f"shape_scales_{frame}"], out[f"shape_quats_{frame}"] = shapes[0], shapes[1]
+            out[f"shape_deformed_{frame}"] = np.int64(shapes[2])
+    t0 = time.time()
+    assert scen.setup(ref)
+    scen.advance(ref, RUNTIME_CHECKPOINTS[-1], record)
+    out["col_hits"] = np.asarray(hits, np.int32)
+    out["grasp_pos"] = scen.grasp_pos
+    out["vol_count"] = ref.ints("vol_count")
+    out["elapsed_s"] = np.float64(time.time() - t0)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -207,7 +244,7 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     names = ["graph_n3000_r1", "graph_n3000_r2", "graph_n3000_k1", "plain_n4000", "plain_n4000_k1",
              "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000", "chainmail_n4000", "object_blobs",
-             "object_plain_n4000"]
+             "object_plain_n4000", "runtime_n4000", "runtime_n4000_ground"]
     if not args.only:
         # One process per case: the reference keeps its solver state in file-static globals.
         import subprocess
@@ -237,6 +274,8 @@ def main():
         "object_blobs": lambda: object_blobs_case(ref),
         "object_plain_n4000": lambda: scenario_case(
             ref, scenes.plain_scene_scenario(4000, 3, pins=40, object_shape=0.9), [1, 10, 100]),
+        "runtime_n4000": lambda: runtime_case(ref, 1),
+        "runtime_n4000_ground": lambda: runtime_case(ref, 3),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only.split(","):

@@ -38,6 +38,7 @@ class Staged(pkg.bridge.XPBD):
     library (xpbd_b200_debug_*) or the reference shim (refshim_*)."""
 
     def __init__(self, path, prefix):
+        self.CHAINMAIL_PREFIX = {"oracle": "oracle_", "b200": "xpbd_b200_", "ref": "refshim_"}[prefix]
         super().__init__(path)
         L = self.lib
         self.prefix = prefix
@@ -85,6 +86,23 @@ class Staged(pkg.bridge.XPBD):
     def set_gs(self, dist, vol):
         fn = {"oracle": "oracle_set_gs", "b200": "xpbd_b200_set_gs", "ref": "refshim_set_gs"}[self.prefix]
         getattr(self.lib, fn)(int(dist), int(vol))
+
+    def chainmail_times(self):
+        if self.prefix != "ref":
+            return super().chainmail_times()
+        out = np.zeros(max(self.n, 1), np.float32)   # the reference keeps them in a file static
+        assert self._float(b"cm_time", out.ctypes.data, out.size) == self.n
+        return out[:self.n]
+
+    def set_positions(self, pos):
+        """Current positions (caller order), velocities kept: oracle_set_positions or
+        xpbd_b200_set_positions."""
+        fn = {"oracle": "oracle_set_positions", "b200": "xpbd_b200_set_positions"}[self.prefix]
+        f = getattr(self.raw, fn)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        f.restype = ctypes.c_int
+        p = np.ascontiguousarray(pos, np.float32)
+        self._check(getattr(self.lib, fn)(p.ctypes.data, len(p)), fn)
 
 
 def oracle():
@@ -150,6 +168,46 @@ def covariances(scales, quats):
 def covariance_rel_err(sa, qa, sb, qb):
     A, B = covariances(sa, qa), covariances(sb, qb)
     return np.linalg.norm((A - B).reshape(-1, 9), axis=1) / np.linalg.norm(B.reshape(-1, 9), axis=1)
+
+
+def quat_angle(qa, qb):
+    """Rotation angle between unit quaternions (sign-free), from the chord |qa - s qb| so that
+    float32 rounding of the norms does not show as an angle (acos near 1 would)."""
+    a = np.asarray(qa, np.float64)
+    b = np.asarray(qb, np.float64)
+    a = a / np.linalg.norm(a, axis=1, keepdims=True)
+    b = b / np.linalg.norm(b, axis=1, keepdims=True)
+    s = np.where((a * b).sum(1) < 0.0, -1.0, 1.0)[:, None]
+    return 4.0 * np.arcsin(np.minimum(1.0, np.linalg.norm(a - s * b, axis=1) / 2.0))
+
+
+# relative eigenvalue gap of Sigma below which a Gaussian's principal axes are
+# ill-conditioned: an FP32 change of 1e-7 in Sigma turns them by more than 5e-6 rad, and
+# two equal scales leave the axes in their plane undetermined
+SHAPE_GAP = 2e-2
+
+
+def shape_parity(sa, qa, sb, qb, diag):
+    """Deformed-shape agreement of (scales, quats) a with reference b: max scale error over
+    the bbox diagonal, max quaternion angle over the well-conditioned Gaussians (relative
+    eigenvalue gap of Sigma >= SHAPE_GAP), the fraction exempt, and the max covariance
+    relative error over the exempt ones."""
+    sa, sb = np.asarray(sa, np.float64), np.asarray(sb, np.float64)
+    lam = np.sort(sb * sb, axis=1)
+    gap = np.minimum(lam[:, 1] - lam[:, 0], lam[:, 2] - lam[:, 1]) / lam[:, 2]
+    good = gap >= SHAPE_GAP
+    ang = quat_angle(qa, qb)
+    cov = covariance_rel_err(sa, qa, sb, qb)
+    return {"scale": float(np.abs(sa - sb).max() / diag),
+            "angle": float(ang[good].max()) if good.any() else 0.0,
+            "exempt": float(1.0 - good.mean()),
+            "cov_exempt": float(cov[~good].max()) if (~good).any() else 0.0,
+            "cov": float(cov.max())}
+
+
+def runtime_scenario(g):
+    """The runtime scenario a golden file holds, with its recorded grasp positions."""
+    return scenes.RuntimeScenario(golden_scene(g), contact_bits=int(g["contact_bits"]), grasp_pos=g["grasp_pos"])
 
 
 def cells_equal(start_a, end_a, start_b, end_b):

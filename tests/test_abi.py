@@ -69,3 +69,46 @@ def test_host_side_errors_without_gpu():
 def test_graft_entry_has_build_and_smoke():
     import __graft_entry__
     assert callable(__graft_entry__.build) and callable(__graft_entry__.smoke)
+
+
+def reference_checkout():
+    """The reference checkout: $XPBD_REFERENCE, else a directory named reference beside
+    this repository; None when neither holds src/xpbd_bridge.py."""
+    for d in (os.environ.get("XPBD_REFERENCE"), os.path.join(os.path.dirname(H.ROOT), "reference")):
+        if d and os.path.isfile(os.path.join(d, "src", "xpbd_bridge.py")):
+            return d
+    return None
+
+
+def test_reference_bridge_sets_up_on_product_library():
+    """The reference's own, unmodified ctypes bridge (src/xpbd_bridge.py) binds this
+    library and runs the runtime's setup calls up to the first step (runtime_loop.py:
+    246-257): create, solver, constraint, volume, shape and object settings, and the
+    ellipsoid contact shapes, which report True (runtime_loop.py:253 falls back to point
+    contact on False and raises on an error)."""
+    import importlib
+    import sys
+    ref = reference_checkout()
+    if ref is None:
+        pytest.skip("no reference checkout (set XPBD_REFERENCE)")
+    sys.path.insert(0, os.path.join(ref, "src"))
+    try:
+        xb = importlib.import_module("xpbd_bridge")
+    finally:
+        sys.path.pop(0)
+    sim = xb.XPBD(H.B200_SO)
+    assert sim.has_attach and sim.has_contact_shape
+    sc = H.scenes.make_scene(400, 3)
+    sim.create(sc)
+    assert sim.lib.xpbd_count() == 400
+    sim.set_solver(iters=16, dt=1 / 60, under_relax=0.6, vel_damping=0.01)
+    sim.set_constraints(distance=True, shape=False, angle=False, volume=True)
+    sim.set_volume(compliance=1e-6, ring_k=3, max_members=2048, leader_min_hop=2)
+    sim.set_shape_robust(False)
+    sim.set_object_shape(0.9)
+    sim.set_object_shape_gpu(True)
+    assert sim.set_contact_shape(1, 0.2, 0.02) is True
+    sim.set_ground(False, (0.0, 0.0, 1.0), 0.0, gravity=0.0)
+    sim.destroy()
+    with pytest.raises(RuntimeError, match="create first"):
+        sim.set_contact_shape(1, 0.2, 0.02)

@@ -60,3 +60,56 @@ def test_served_sessions_match_alone():
         alone.solver.lib.xpbd_b200_sync()
         np.testing.assert_array_equal(alone.solver.positions(), done[k].final)
         alone.close(keep_result=False)
+
+
+def test_arena_retire_and_compaction_match_alone():
+    """Sessions join a small arena, one in the middle retires, a new one only fits after
+    the live sessions are moved down over the hole (compaction); every session's
+    positions equal its solo run's, bit for bit."""
+    specs = {"A": (3000, 101), "B": (5000, 202), "C": (2000, 303), "D": (4000, 404)}
+
+    def session(name):
+        n, seed = specs[name]
+        s = serve.Session(ord(name), 0.0, n, 99, seed)
+        s.admit(H.B200_SO)
+        return s
+
+    rows = 11000
+    arena = H.pkg.bridge.Arena(H.B200_SO, rows, rows * 12, rows * 66, rows * 68)
+    live = {}
+
+    def join(name):
+        s = session(name)
+        s.slot = arena.admit(s.solver)
+        assert s.slot is not None and s.slot >= 0
+        s.solver.close()
+        live[name] = s
+
+    def tick():
+        res = list(live.values())
+        arena.step(10, *serve._frame_arrays(res, 10))
+        arena.sync()
+        for s in res:
+            s.scen.k += 10
+            s.frames_done = getattr(s, "frames_done", 0) + 1
+
+    for name in "ABC":
+        join(name)
+    tick()
+    tick()
+    got = {"B": (arena.positions(live["B"].slot, specs["B"][0]), 2)}
+    arena.retire(live.pop("B").slot)
+    join("D")                                   # 10,000 rows + 4,000 > 11,000: compaction
+    assert arena.usage()["rows"] == 9000
+    for _ in range(3):
+        tick()
+    for name, s in live.items():
+        got[name] = (arena.positions(s.slot, s.n), s.frames_done)
+    arena.close()
+    for name, (pos, frames) in got.items():
+        alone = session(name)
+        for _ in range(frames):
+            alone.enqueue_frame()
+        alone.solver.lib.xpbd_b200_sync()
+        np.testing.assert_array_equal(alone.solver.positions(), pos, err_msg=name)
+        alone.close(keep_result=False)

@@ -202,3 +202,57 @@ def test_object_mode_two_objects(orc):
     assert int(g["sc_stats_30"][1]) < len(g["in_pos"])   # the box filter left some out
     orc.set_object_shape(0.0)
 
+
+
+SHAPE_CASES = ["plain_n4000", "plain_n4000_fpolar", "object_plain_n4000", "plain_n20000"]
+
+
+@pytest.mark.parametrize("case", SHAPE_CASES)
+def test_deformed_shapes_on_reference_positions(orc, case):
+    """The shape writeback (forward.cu:13022-13247) on the positions the reference reached:
+    scales within 1e-5 of the bbox diagonal, quaternions within 1e-4 rad wherever the
+    principal axes are well defined (relative eigenvalue gap >= 2e-2; the rest, at most a
+    tenth, by covariance within 1e-5)."""
+    g = H.load_golden(case)
+    s = H.scenario_for(case)
+    s.setup(orc)
+    s.advance(orc, 1)
+    last = int(g["checkpoints"][-1])
+    orc.set_positions(g[f"pos_{last}"])
+    sc_, q_, k_ = orc.shapes(float(g["deform_eps"]))
+    assert k_ == int(g["shape_deformed"])
+    m = H.shape_parity(sc_, q_, g["shape_scales"], g["shape_quats"], H.scenes.bbox_diagonal(g["in_pos"]))
+    assert m["scale"] < H.TOL_1STEP and m["angle"] < 1e-4, m
+    assert m["exempt"] < 0.1 and m["cov_exempt"] < 1e-5, m
+
+
+@pytest.mark.parametrize("case", ["runtime_n4000", "runtime_n4000_ground"])
+def test_runtime_scenario(orc, case):
+    """The Isaac runtime's configuration and call order (16 iterations at dt 1/60, leader
+    spacing 2, 2048-member cap, object shape keeping, ellipsoid contacts, ground with
+    gravity and restitution, pads that close, hold and lift): positions at 1e-5 of the
+    diagonal after 1 frame and 1e-4 after 10, 30 and 100, collider hits per frame, the
+    deformed shapes after the first frame directly and later by covariance."""
+    g = H.load_golden(case)
+    s = H.runtime_scenario(g)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    got = {}
+
+    def record(solver, frame, shapes):
+        got.setdefault("hits", []).append(solver.collider_stats(2)[0])
+        if frame in g["checkpoints"]:
+            got[frame] = (solver.positions(), shapes)
+    assert s.setup(orc)
+    s.advance(orc, int(g["checkpoints"][-1]), record)
+    np.testing.assert_array_equal(orc.ints("vol_count"), g["vol_count"])
+    hits = np.asarray(got["hits"])
+    assert np.abs(hits - g["col_hits"]).max() <= 1 and (hits != g["col_hits"]).mean() < 0.05
+    for c in g["checkpoints"]:
+        pos, (sc_, q_, k_) = got[int(c)]
+        tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
+        assert H.max_err_over_diag(pos, g[f"pos_{c}"], diag) < tol, c
+        m = H.shape_parity(sc_, q_, g[f"shape_scales_{c}"], g[f"shape_quats_{c}"], diag)
+        if c == 1:
+            assert m["scale"] < H.TOL_1STEP and m["angle"] < 1e-4 and m["exempt"] < 0.1, m
+        else:
+            assert m["scale"] < H.TOL_100STEP and m["cov"] < 1e-2, (c, m)

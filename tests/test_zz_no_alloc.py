@@ -84,6 +84,49 @@ def test_static_scratch_build_matches_allocating_build():
     lib.destroy()
 
 
+def test_static_scratch_build_one_object_without_ids():
+    """obj_id = NULL (one object: the ids are zeroed in the scratch array) against the
+    allocating build of a single-object scene, two calls in a row."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required")
+    lib = H.b200()
+    static_build = _static_fn(lib.lib)
+    s = H.scenes.plain_scene_scenario(6000, 4, pins=30, self_collision=True, within_body=True)
+    s.setup(lib)
+    s.advance(lib, 2)
+    n = s.n
+    spacing = float(lib.floats("self_col")[0])
+    dev = torch.device("cuda:0")
+    rest4 = np.zeros((n, 4), np.float32)
+    rest4[:, :3] = s.scene["pos"]
+    d_rest = torch.from_numpy(rest4).to(dev)
+    d_contacts = torch.full((n * 32,), -7, dtype=torch.int32, device=dev)
+    d_counts = torch.full((n,), -7, dtype=torch.int32, device=dev)
+    d_total = torch.zeros(1, dtype=torch.int32, device=dev)
+    x0 = lib.positions()
+    rng = np.random.default_rng(9)
+    for call in range(2):
+        x = (x0 + rng.normal(0.0, 0.003, x0.shape)).astype(np.float32)
+        p = (x + rng.normal(0.0, 0.004 * (call + 1), x.shape)).astype(np.float32)
+        expected_total = lib.selfcol_build(x, p)
+        exp_counts, exp_contacts = lib.ints("sc_count"), lib.ints("sc_contact")
+        assert expected_total > 0
+        x4 = np.zeros((n, 4), np.float32)
+        p4 = np.zeros((n, 4), np.float32)
+        x4[:, :3], p4[:, :3] = x, p
+        d_x, d_p = torch.from_numpy(x4).to(dev), torch.from_numpy(p4).to(dev)
+        rc = static_build(n, d_x.data_ptr(), d_p.data_ptr(), d_rest.data_ptr(), None, spacing, 1.5, 2.0, 1,
+                          d_contacts.data_ptr(), d_counts.data_ptr(), d_total.data_ptr(),
+                          torch.cuda.current_stream(dev).cuda_stream)
+        assert rc == 0, lib.last_error()
+        torch.cuda.synchronize()
+        assert int(d_total.cpu().item()) == expected_total
+        assert H.contacts_equal(d_counts.cpu().numpy(), d_contacts.cpu().numpy(), exp_counts, exp_contacts), call
+    lib.destroy()
+
+
 def test_static_scratch_limit_is_enforced():
     lib = H.b200()
     static_build = _static_fn(lib.lib)
