@@ -219,27 +219,97 @@ void finish_clusters(int n, const Members& members_of_leader, const std::vector<
 
 }  // namespace
 
-void build_clusters_from_members(const HostGraph& g, const float* rest, int ring_k, int cap, const int* flat,
-	const int* counts, HostClusters& out)
+namespace {
+
+// Leader selection of rebuildVolumeClusters for leader spacing r >= 2 (forward.cu:
+// 10070-10132): in index order, a node whose cover is below the target (min(r, 6)) and
+// that no earlier leader suppressed (within r - 1 hops) becomes a leader, and its list
+// raises the cover of itself and its members; then under-covered nodes are promoted
+// until none is left.  list_of(i) -> (pointer, count) of node i's member list, the same
+// whoever asks (the reference's cover cap is 0, so a list depends on the node alone).
+template <typename ListOf>
+int cover_leaders(const HostGraph& g, int leader_r, const ListOf& list_of, std::vector<char>& leader)
 {
-	// every Gaussian is a leader (leader spacing 1); lists with count -1 are built here
 	const int n = g.n;
-	std::vector<char> leader(n, 1);
-	out.leaders = n;
+	const int target = std::max(1, std::min(6, leader_r));
+	std::vector<int> cover(n, 0), stamp_r(n, -1);
+	int count = 0;
+	std::vector<int> fr, nx;
+	auto take = [&](int i) {
+		leader[i] = 1;
+		++count;
+		const auto m = list_of(i);
+		++cover[i];
+		for (int t = 0; t < m.second; ++t) {
+			const int j = m.first[t];
+			if (j >= 0 && j < n) ++cover[j];
+		}
+	};
+	for (int seed = 0; seed < n; ++seed) {
+		if (cover[seed] >= target) continue;
+		if (stamp_r[seed] == -2) continue;
+		take(seed);
+		fr.clear();
+		stamp_r[seed] = -2;
+		fr.push_back(seed);
+		for (int d = 0; d < leader_r - 1 && !fr.empty(); ++d) {
+			nx.clear();
+			for (int f : fr)
+				for (int e = g.off[f]; e < g.off[f + 1]; ++e) {
+					const int j = g.nbr[e];
+					if (j < 0 || j >= n || stamp_r[j] == -2) continue;
+					stamp_r[j] = -2;
+					nx.push_back(j);
+				}
+			fr.swap(nx);
+		}
+	}
+	bool progressed = true;
+	while (progressed) {
+		progressed = false;
+		for (int i = 0; i < n; ++i) {
+			if (cover[i] >= target || leader[i]) continue;
+			take(i);
+			progressed = true;
+		}
+	}
+	return count;
+}
+
+}  // namespace
+
+void build_clusters_from_lists(const HostGraph& g, const float* rest, int ring_k, int cap, int leader_min_hop,
+	const std::vector<long long>& loff, const std::vector<int>& lidx, const std::vector<int>& counts,
+	HostClusters& out)
+{
+	// every node's list from the GPU (loff / lidx), or -1 in counts where the host builds it
+	const int n = g.n;
+	const int leader_r = std::max(1, leader_min_hop);
 	std::vector<std::vector<int>> host_lists;
 	std::vector<int> host_at(n, -1);
-	{
-		Scratch sc(n);
+	Scratch sc(n);
+	auto list_of = [&](int i) -> std::pair<const int*, int> {
+		if (counts[i] >= 0) return std::make_pair(lidx.data() + loff[i], counts[i]);
+		if (host_at[i] < 0) {
+			host_at[i] = (int)host_lists.size();
+			host_lists.emplace_back();
+			members_of(g, rest, i, ring_k, cap, sc, host_lists.back());
+		}
+		const auto& v = host_lists[host_at[i]];
+		return std::make_pair((const int*)v.data(), (int)v.size());
+	};
+	std::vector<char> leader(n, 0);
+	if (leader_r <= 1) {
+		std::fill(leader.begin(), leader.end(), (char)1);
+		out.leaders = n;
 		for (int i = 0; i < n; ++i)
-			if (counts[i] < 0) {
-				host_at[i] = (int)host_lists.size();
-				host_lists.emplace_back();
-				members_of(g, rest, i, ring_k, cap, sc, host_lists.back());
-			}
+			if (counts[i] < 0) list_of(i);   // build the host lists before the parallel reads
 	}
+	else
+		out.leaders = cover_leaders(g, leader_r, list_of, leader);
 	finish_clusters(n, [&](int i) {
-		if (host_at[i] >= 0) return std::make_pair((const int*)host_lists[host_at[i]].data(), (int)host_lists[host_at[i]].size());
-		return std::make_pair(flat + (size_t)i * cap, counts[i]);
+		if (!leader[i]) return std::make_pair((const int*)nullptr, 0);
+		return list_of(i);
 	}, leader, out);
 }
 
@@ -269,54 +339,17 @@ void build_clusters(const HostGraph& g, const float* rest, int ring_k, int cap, 
 		for (auto& th : pool) th.join();
 	}
 	else {
-		// greedy cover: sparse leaders at >= r hops, then promote under-covered nodes
-		const int target = std::max(1, std::min(6, leader_r));
-		std::vector<int> cover(n, 0), stamp_r(n, -1);
+		// greedy cover, each leader's list built when it is chosen
 		Scratch s(n);
-		int count = 0;
-		std::vector<int> fr, nx;
-		for (int seed = 0; seed < n; ++seed) {
-			if (cover[seed] >= target) continue;
-			if (stamp_r[seed] == -2) continue;
-			leader[seed] = 1;
-			++count;
-			members_of(g, rest, seed, ring_k, cap, s, members[seed]);
-			++cover[seed];
-			for (int j : members[seed])
-				if (j >= 0 && j < n) ++cover[j];
-			fr.clear();
-			stamp_r[seed] = -2;
-			fr.push_back(seed);
-			for (int d = 0; d < leader_r - 1 && !fr.empty(); ++d) {
-				nx.clear();
-				for (int f : fr)
-					for (int e = g.off[f]; e < g.off[f + 1]; ++e) {
-						const int j = g.nbr[e];
-						if (j < 0 || j >= n || stamp_r[j] == -2) continue;
-						stamp_r[j] = -2;
-						nx.push_back(j);
-					}
-				fr.swap(nx);
-			}
-		}
-		bool progressed = true;
-		while (progressed) {
-			progressed = false;
-			for (int i = 0; i < n; ++i) {
-				if (cover[i] >= target || leader[i]) continue;
-				leader[i] = 1;
-				++count;
-				members_of(g, rest, i, ring_k, cap, s, members[i]);
-				++cover[i];
-				for (int j : members[i])
-					if (j >= 0 && j < n) ++cover[j];
-				progressed = true;
-			}
-		}
-		out.leaders = count;
+		out.leaders = cover_leaders(g, leader_r, [&](int i) {
+			if (members[i].empty()) members_of(g, rest, i, ring_k, cap, s, members[i]);
+			return std::make_pair((const int*)members[i].data(), (int)members[i].size());
+		}, leader);
 	}
-	finish_clusters(n, [&](int i) { return std::make_pair((const int*)members[i].data(), (int)members[i].size()); },
-		leader, out);
+	finish_clusters(n, [&](int i) {
+		if (!leader[i]) return std::make_pair((const int*)nullptr, 0);
+		return std::make_pair((const int*)members[i].data(), (int)members[i].size());
+	}, leader, out);
 }
 
 void build_edge_coloring(const HostGraph& g, HostEdgeColoring& out)

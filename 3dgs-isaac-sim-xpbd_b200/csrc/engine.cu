@@ -133,6 +133,8 @@ struct Settings {
 	bool cm_frontier = true;         // ChainMail sweeps on work lists (false: every sweep dense)
 	bool obj_gpu = true;             // object mode's weighted device fit (xpbd_set_object_shape_gpu)
 	bool gpu_builder = true;         // cluster members (BFS + farthest point) built on the GPU
+	bool press_autolog = true;       // press harness: settle at 25/50/75/100 % (forward.cu:565)
+	int fused = 0;                   // substep as one cooperative launch: 0 never, 1 always, 2 the faster (timed)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -290,10 +292,90 @@ public:
 	Staging staging[kStagingSlots];
 	int staging_next = 0;
 
+	// ---- press harness (squashStart / the per-step ramp, forward.cu:4311-4396, 12095-12111):
+	// two plates on the load axis at the rest extent; one closes at ramp_per_sec up to
+	// max_disp, pausing press_dwell_frames at each quarter when autolog is on.  While it
+	// runs the ground, gravity, object shape keeping and self-collision are not applied.
+	bool press_active = false, press_from_lo = false;
+	int press_axis = 1, press_ckpt = 0, press_dwell = 0;
+	float press_lo = 0.0f, press_hi = 0.0f, press_cur = 0.0f, press_max = 0.0f, press_ramp = 0.0f;
+	static constexpr int kPressDwellFrames = 90;
+
+	void press_reset()
+	{
+		press_active = false;
+		press_cur = 0.0f;
+		press_ckpt = 0;
+		press_dwell = 0;
+	}
+
+	// squashStart (forward.cu:4311-4396) in press mode
+	int press_start(int axis, float ramp, float max_disp_pct, bool from_lo)
+	{
+		if (axis < 0 || axis > 2) axis = 1;
+		const float slab = 0.08f;
+		max_disp_pct = fmaxf(0.01f, fminf(1.0f, max_disp_pct));
+		float lo = FLT_MAX, hi = -FLT_MAX;
+		for (int i = 0; i < n; ++i) {
+			const float v = in_pos[3 * (size_t)i + axis];
+			lo = fminf(lo, v);
+			hi = fmaxf(hi, v);
+		}
+		const float extent = hi - lo;
+		const float top = hi - slab * extent, bot = lo + slab * extent;
+		int ntop = 0, nbot = 0;
+		for (int i = 0; i < n; ++i) {
+			const float v = in_pos[3 * (size_t)i + axis];
+			if (v >= top) ++ntop;
+			else if (v <= bot) ++nbot;
+		}
+		if (ntop == 0 || nbot == 0) return fail("xpbd_press_start: squashStart failed (empty %d %% slab on axis %d)", 8, axis);
+		press_axis = axis;
+		press_ramp = ramp;
+		press_lo = lo;
+		press_hi = hi;
+		press_max = max_disp_pct * extent;
+		press_from_lo = from_lo;
+		press_cur = 0.0f;
+		press_ckpt = 0;
+		press_dwell = 0;
+		press_active = true;
+		return 0;
+	}
+
+	// the per-step ramp with its checkpoint dwells (forward.cu:12095-12111)
+	void press_advance()
+	{
+		if (!press_active) return;
+		static const float ckpt[4] = { 0.25f, 0.50f, 0.75f, 1.00f };
+		if (S.press_autolog && press_dwell > 0) {
+			if (--press_dwell == 0) ++press_ckpt;
+			return;
+		}
+		press_cur = fminf(press_cur + press_ramp * S.dt, press_max);
+		if (S.press_autolog && press_ckpt < 4) {
+			const float target = ckpt[press_ckpt] * press_max;
+			if (press_cur >= target) {
+				press_cur = target;
+				press_dwell = kPressDwellFrames;
+			}
+		}
+	}
+
 	// ---- execution ----
 	cudaStream_t stream = nullptr;
 	bool own_stream = false;
 	cudaGraphExec_t graph_exec = nullptr;
+	// the same substep as one cooperative launch, and the autotuner that times both forms
+	// on the first steps after a capture (they give identical results) and keeps the faster
+	cudaGraphExec_t graph_fused = nullptr;
+	long long graph_fused_kernels = 0;
+	static constexpr int kTuneRounds = 3;
+	cudaEvent_t tune_ev[2 * kTuneRounds][2] = {};
+	int tune_n = 0, tune_choice = 0;
+	bool tune_done = true;
+	float tune_ms[2] = { 0.0f, 0.0f };
+	int fused_grid = 0;
 	std::vector<long long> graph_key;
 	long long graph_kernels = 0;
 	long long launches = 0;
@@ -311,6 +393,11 @@ public:
 	{
 		if (graph_exec) cudaGraphExecDestroy(graph_exec);
 		graph_exec = nullptr;
+		if (graph_fused) cudaGraphExecDestroy(graph_fused);
+		graph_fused = nullptr;
+		for (auto& pr : tune_ev)
+			for (auto& e : pr)
+				if (e) { cudaEventDestroy(e); e = nullptr; }
 		graph_key.clear();
 		free_device();
 		if (d_params) cudaFree(d_params);
@@ -507,6 +594,7 @@ public:
 		build_t0 = std::chrono::steady_clock::now();
 		free_device();
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
 		graph_key.clear();
 		if (ensure_stream()) return -1;
 		build_graph(n, n_edges, in_edges.data(), in_rest.data(), in_stiff.data(), graph);
@@ -586,7 +674,7 @@ public:
 	int rebuild_clusters()
 	{
 		build_mark(2);
-		if (S.gpu_builder && S.leader_min_hop <= 1 && n > 0) {
+		if (S.gpu_builder && n > 0) {
 			if (build_members_gpu()) return -1;
 		}
 		else
@@ -643,6 +731,7 @@ public:
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		CK(cudaStreamSynchronize(stream));
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
 		graph_key.clear();
 		++generation;
 		build_mark(6);
@@ -720,7 +809,7 @@ public:
 	bool contact_col() const { return (contact_bits & 1) && contact_packed; }
 	bool contact_ground() const { return (contact_bits & 2) && contact_packed && S.ground_on; }
 
-	bool object_on() const { return S.object_shape > 0.0f && num_objects > 0; }
+	bool object_on() const { return S.object_shape > 0.0f && num_objects > 0 && !press_active; }
 	// the self-collision build keeps only Gaussians near another object (forward.cu:11808-11816)
 	bool sc_limited() const
 	{
@@ -835,30 +924,45 @@ public:
 		return sync();
 	}
 
-	// k-ring BFS + farthest-point members of every leader on the GPU (caller index space),
-	// then the CSRs and colouring on the host (builder.cpp)
+	// k-ring BFS + farthest-point member list of every node on the GPU (caller index
+	// space), in chunks of nodes, gathered into one host CSR; then leader selection (the
+	// greedy cover for leader spacing >= 2), the CSRs and colouring on the host
+	// (builder.cpp).  A list longer than the kernel's candidate buffer is built on the host.
 	int build_members_gpu()
 	{
 		const int cap = std::max(1, S.max_members);
+		const int width = std::min(cap, dev::kBallCap);    // longer balls are the host's
 		const int m = graph.off[n];
 		DBuf<int> d_off, d_nbr, d_members, d_counts;
 		DBuf<float> d_rest3;
+		const int chunk = (int)std::max<long long>(1, std::min<long long>(n, (512ll << 20) / (4ll * width)));
 		CK(d_off.alloc(n + 1)); CK(d_nbr.alloc(std::max(m, 1))); CK(d_rest3.alloc(3 * (size_t)n));
-		CK(d_members.alloc((size_t)n * cap)); CK(d_counts.alloc(n));
+		CK(d_members.alloc((size_t)chunk * width)); CK(d_counts.alloc(chunk));
 		CK(cudaMemcpyAsync(d_off.p, graph.off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream));
 		if (m > 0) CK(cudaMemcpyAsync(d_nbr.p, graph.nbr.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
 		CK(cudaMemcpyAsync(d_rest3.p, in_pos.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, stream));
 		CK(cudaFuncSetAttribute(dev::k_build_members, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dev::kBuildSmem));
-		const int blocks = std::min((n + dev::kBuildWarps - 1) / dev::kBuildWarps, 148 * 16);
-		dev::k_build_members<<<blocks, dev::kBuildWarps * 32, dev::kBuildSmem, stream>>>(n, d_off.p, d_nbr.p, d_rest3.p,
-			S.ring_k, cap, d_members.p, d_counts.p);
-		CK(cudaGetLastError());
-		std::vector<int> flat((size_t)n * cap), counts(n);
-		CK(cudaMemcpyAsync(counts.data(), d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
-		CK(cudaMemcpyAsync(flat.data(), d_members.p, sizeof(int) * (size_t)n * cap, cudaMemcpyDeviceToHost, stream));
-		CK(cudaStreamSynchronize(stream));
+		std::vector<int> flat((size_t)chunk * width), counts(n);
+		std::vector<long long> loff(n + 1, 0);
+		std::vector<int> lidx;
+		for (int c0 = 0; c0 < n; c0 += chunk) {
+			const int c1 = std::min(n, c0 + chunk), cn = c1 - c0;
+			const int blocks = std::min((cn + dev::kBuildWarps - 1) / dev::kBuildWarps, 148 * 16);
+			dev::k_build_members<<<blocks, dev::kBuildWarps * 32, dev::kBuildSmem, stream>>>(n, c0, c1, d_off.p, d_nbr.p,
+				d_rest3.p, S.ring_k, width, d_members.p, d_counts.p);
+			CK(cudaGetLastError());
+			CK(cudaMemcpyAsync(counts.data() + c0, d_counts.p, sizeof(int) * cn, cudaMemcpyDeviceToHost, stream));
+			CK(cudaMemcpyAsync(flat.data(), d_members.p, sizeof(int) * (size_t)cn * width, cudaMemcpyDeviceToHost, stream));
+			CK(cudaStreamSynchronize(stream));
+			for (int i = c0; i < c1; ++i) {
+				const int k = counts[i];   // -1: the ball outgrew the buffer, the host builds the list
+				if (k > 0) lidx.insert(lidx.end(), flat.begin() + (size_t)(i - c0) * width,
+					flat.begin() + (size_t)(i - c0) * width + k);
+				loff[i + 1] = loff[i] + std::max(k, 0);
+			}
+		}
 		build_mark(3);
-		build_clusters_from_members(graph, in_pos.data(), S.ring_k, cap, flat.data(), counts.data(), clusters);
+		build_clusters_from_lists(graph, in_pos.data(), S.ring_k, cap, S.leader_min_hop, loff, lidx, counts, clusters);
 		return 0;
 	}
 
@@ -879,6 +983,7 @@ public:
 		CK(cudaStreamSynchronize(stream));
 		coloring_built = true;
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
 		graph_key.clear();
 		return 0;
 	}
@@ -933,6 +1038,7 @@ public:
 			CK(d_kin_ext.alloc(std::max<size_t>(count, 64)));
 			CK(d_kin_range.alloc(std::max<size_t>(h_kin_range.size(), 64)));
 			if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+			if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
 			graph_key.clear();
 		}
 		CK(cudaMemcpyAsync(d_kin_ext.p, h_kin_sorted.data(), sizeof(KinCollider) * count, cudaMemcpyHostToDevice, stream));
@@ -954,13 +1060,17 @@ public:
 		P.shape_compliance = S.shape_compliance;
 		P.shape_blend = S.shape_blend;
 		P.vel_damping = S.vel_damping;
-		// stepPhysicsOnly gravity: -g * n when g > 0 (forward.cu:13257-13259)
-		if (S.ground_gravity > 0.0f) {
+		// stepPhysicsOnly gravity: -g * n when g > 0 and no press runs (forward.cu:13257-13259)
+		if (S.ground_gravity > 0.0f && !press_active) {
 			P.gx = -S.ground_gravity * S.ground_n[0];
 			P.gy = -S.ground_gravity * S.ground_n[1];
 			P.gz = -S.ground_gravity * S.ground_n[2];
 		}
-		P.ground_on = S.ground_on ? 1 : 0;
+		P.ground_on = (S.ground_on && !press_active) ? 1 : 0;   // groundOn (forward.cu:12140)
+		P.press_on = press_active ? 1 : 0;
+		P.press_axis = press_axis;
+		P.press_lo = press_lo + ((press_active && press_from_lo) ? press_cur : 0.0f);
+		P.press_hi = press_hi - ((press_active && !press_from_lo) ? press_cur : 0.0f);
 		for (int k = 0; k < 3; ++k) P.gn[k] = S.ground_n[k];
 		P.ground_plane = S.ground_h + S.ground_radius;
 		P.ground_slop = S.ground_slop;
@@ -1001,14 +1111,17 @@ public:
 		if (S.warp_mode == 1) return false;
 		return clusters.avg_members >= 40.0f;
 	}
-	bool selfcol_on() const { return S.sc_enabled && spacing > 0.0f && S.sc_radius_scale * spacing > 0.0f; }
+	bool selfcol_on() const
+	{
+		return S.sc_enabled && spacing > 0.0f && S.sc_radius_scale * spacing > 0.0f && !press_active;
+	}
 	bool dist_gs_on() const { return S.use_distance && S.dist_gs && coloring_built && !coloring.edge.empty(); }
 	bool vol_gs_on() const { return S.use_volume && S.vol_gs && clusters.gs_color_off.size() > 1; }
 
 	std::vector<long long> topology_key() const
 	{
 		return { (long long)generation, S.iters, S.use_distance, dist_gs_on(), S.use_volume, vol_gs_on(), vol_lanes(), gather_lanes(),
-			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on(), S.jstats,
+			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on() || press_active, S.jstats,
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
 			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground() };
@@ -1078,6 +1191,62 @@ public:
 		return 4;
 	}
 
+	// the substep forms the fused launch covers (dev::k_substep_fused)
+	bool fused_eligible() const
+	{
+		return !selfcol_on() && !object_on() && !dist_gs_on() && !vol_gs_on() &&
+			(!S.use_volume || (vol_lanes() == 4 && S.lanes_a == 0 && gather_lanes() == 4)) && !S.use_angle && n > 0;
+	}
+
+	// one step as a single cooperative launch (results identical to enqueue_step's sequence)
+	int enqueue_step_fused()
+	{
+		if (!fused_grid) {
+			int dev_id = 0, sms = 0, per_sm = 0;
+			CK(cudaGetDevice(&dev_id));
+			CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id));
+			CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_substep_fused, kBlock, 0));
+			if (per_sm <= 0) return fail("fused substep: no block of the kernel fits an SM");
+			fused_grid = sms * per_sm;
+		}
+		const int grid = (int)std::max<long long>(1, std::min<long long>(fused_grid, ((long long)n * 4 + kBlock - 1) / kBlock));
+		const bool cc = contact_col(), cg = contact_ground();
+		dev::SubstepArgs A;
+		memset(&A, 0, sizeof(A));
+		A.n = n; A.iters = S.iters; A.use_distance = S.use_distance; A.use_volume = S.use_volume;
+		A.use_shape = S.use_shape; A.shape_robust = S.shape_robust;
+		A.project = S.kin_count > 0 || !S.kin_ext.empty() || S.ground_on || press_active;
+		A.P = d_params;
+		A.pos_curr = pos_curr.p; A.pos_next = pos_next.p; A.pos_tmp = pos_tmp.p; A.vel = vel.p; A.lam_vol = lam_vol.p;
+		A.cshape = (cc || cg) ? c_shape.p : nullptr; A.crmax = cc ? c_rmax.p : nullptr; A.crg = cg ? c_rg.p : nullptr;
+		A.off = off.p; A.nbr = nbr.p; A.ndist = ndist.p; A.nstiff = nstiff.p; A.lam = lam.p;
+		A.vol_off = vol_off.p; A.vol_idx = vol_idx_s.p; A.mat_type = mat_type.p; A.rev_off = rev_off.p;
+		A.rev_idx = rev_idx_s.p; A.det_rest = det_rest.p; A.rest_len = rest_len.p; A.rec = rec.p; A.recz = recz();
+		A.pos_rest = pos_rest.p; A.shape_rest = shape_rest.p; A.shape_q = shape_q.p; A.ctr = d_ctr;
+		A.obj_id = d_obj_id.p; A.ext_kin = S.kin_ext.empty() ? nullptr : d_kin_ext.p; A.ext_range = d_kin_range.p;
+		A.pos_out3 = pos_out3.p; A.perm = d_perm.p;
+		CK(cudaMemsetAsync(d_ctr, 0, offsetof(DevCounters, jstats), stream));
+		cudaLaunchConfig_t cfg = {};
+		cfg.gridDim = dim3(grid);
+		cfg.blockDim = dim3(kBlock);
+		cfg.stream = stream;
+		cudaLaunchAttribute attr[1];
+		attr[0].id = cudaLaunchAttributeCooperative;
+		attr[0].val.cooperative = 1;
+		cfg.attrs = attr;
+		cfg.numAttrs = 1;
+		CK(cudaLaunchKernelEx(&cfg, dev::k_substep_fused, A));
+		++launches;
+		if (S.jstats) {
+			CK(cudaMemsetAsync(d_ctr->jstats, 0, sizeof(double) * 3, stream));
+			launch(ST_JSTATS, blocks_for(n), dim3(kBlock), dev::k_jstats, n, (const float4*)pos_curr.p,
+				(const int*)vol_off.p, (const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p,
+				(const float*)v_rest.p, d_ctr);
+		}
+		CK(cudaGetLastError());
+		return 0;
+	}
+
 	// one step's kernel sequence (the body of runXPBDSimulation)
 	int enqueue_step()
 	{
@@ -1122,7 +1291,7 @@ public:
 		float4* pin = pos_next.p;
 		float4* pout = pos_tmp.p;
 		const bool dgs = dist_gs_on(), vgs = vol_gs_on();
-		const bool project = S.kin_count > 0 || !S.kin_ext.empty() || S.ground_on || sc;
+		const bool project = S.kin_count > 0 || !S.kin_ext.empty() || S.ground_on || sc || press_active;
 		for (int it = 0; it < S.iters; ++it) {
 			const int first = (it == 0), last = (it == S.iters - 1);
 			if (dgs) {
@@ -1259,30 +1428,57 @@ public:
 		if (ensure_sc_object_buffers()) return -1;
 		const bool sc_limited_now = sc_limited();
 		if (upload_ext_colliders()) return -1;   // sets the object ranges fill_params reads
+		press_advance();
 		if (upload_params()) return -1;
 		if (profiling || !S.use_graph) {
 			if (enqueue_step()) return -1;
 		}
 		else {
-			const auto key = topology_key();
+			auto key = topology_key();
+			key.push_back(S.fused);
 			if (!graph_exec || key != graph_key) {
 				if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-				cudaGraph_t g = nullptr;
-				CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-				const long long before = launches;
-				const int rc = enqueue_step();
-				const cudaError_t ec = cudaStreamEndCapture(stream, &g);
-				if (rc) { if (g) cudaGraphDestroy(g); return -1; }
-				CK(ec);
-				graph_kernels = launches - before;
-				launches = before;
-				const cudaError_t ei = cudaGraphInstantiate(&graph_exec, g, 0);
-				cudaGraphDestroy(g);
-				CK(ei);
+				if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
+				if (capture(false, &graph_exec, &graph_kernels)) return -1;
+				if (S.fused != 0 && fused_eligible() && capture(true, &graph_fused, &graph_fused_kernels)) {
+					cudaGetLastError();          // the kernel sequence carries on
+					graph_fused = nullptr;
+				}
 				graph_key = key;
+				tune_done = !graph_fused || S.fused != 2;
+				tune_choice = (graph_fused && S.fused == 1) ? 1 : 0;
+				tune_n = 0;
 			}
-			CK(cudaGraphLaunch(graph_exec, stream));
-			launches += graph_kernels;
+			int variant = tune_choice;
+			cudaEvent_t* ev = nullptr;
+			if (!tune_done) {
+				if (tune_n == 2 * kTuneRounds) {
+					// every trial step enqueued: the timings decide (one wait, once per capture)
+					float sum[2] = { 0.0f, 0.0f };
+					for (int t = 0; t < 2 * kTuneRounds; ++t) {
+						float ms = 0.0f;
+						CK(cudaEventSynchronize(tune_ev[t][1]));
+						CK(cudaEventElapsedTime(&ms, tune_ev[t][0], tune_ev[t][1]));
+						sum[t & 1] += ms;
+					}
+					tune_ms[0] = sum[0] / kTuneRounds;
+					tune_ms[1] = sum[1] / kTuneRounds;
+					tune_choice = tune_ms[1] < tune_ms[0] ? 1 : 0;
+					tune_done = true;
+					variant = tune_choice;
+				}
+				else {
+					variant = tune_n & 1;
+					ev = tune_ev[tune_n++];
+					for (int q = 0; q < 2; ++q)
+						if (!ev[q]) CK(cudaEventCreate(&ev[q]));
+					CK(cudaEventRecord(ev[0], stream));
+				}
+			}
+			CK(cudaGraphLaunch(variant ? graph_fused : graph_exec, stream));
+			if (variant) fused_pending = true;
+			if (ev) CK(cudaEventRecord(ev[1], stream));
+			launches += variant ? graph_fused_kernels : graph_kernels;
 		}
 		last_sc_limited = sc_limited_now;
 		if (object_on()) obj_shift_valid = true;
@@ -1290,11 +1486,36 @@ public:
 		return 0;
 	}
 
+	// one captured step: the kernel sequence or the fused launch
+	int capture(bool fused_form, cudaGraphExec_t* exec, long long* kernels)
+	{
+		cudaGraph_t g = nullptr;
+		CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+		const long long before = launches;
+		const int rc = fused_form ? enqueue_step_fused() : enqueue_step();
+		const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+		if (rc) { if (g) cudaGraphDestroy(g); return -1; }
+		CK(ec);
+		*kernels = launches - before;
+		launches = before;
+		const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+		cudaGraphDestroy(g);
+		CK(ei);
+		return 0;
+	}
+
+	bool fused_pending = false;      // a fused launch ran since the last sync
+
 	int sync()
 	{
 		if (!stream) return 0;
 		CK(cudaStreamSynchronize(stream));
 		CK(cudaGetLastError());
+		if (fused_pending && d_ctr) {
+			fused_pending = false;
+			CK(cudaMemcpy(&h_ctr->bar_timeout, &d_ctr->bar_timeout, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+			if (h_ctr->bar_timeout) return fail("fused substep: a grid barrier wait ran out (results invalid)");
+		}
 		return 0;
 	}
 
@@ -2168,6 +2389,7 @@ XPBD_API int xpbd_reset(void)
 	if (!cur_engine()->stepped) return fail("xpbd_reset: no step yet");
 	Engine& E = *cur_engine();
 	if (E.set_attached(0, nullptr, nullptr)) return -1;
+	E.press_reset();
 	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
 	return E.upload_positions(E.in_pos.data(), nullptr);
 }
@@ -2204,23 +2426,38 @@ XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt)
 		v3[3 * i] = vx + (wy * rz - wz * ry); v3[3 * i + 1] = vy + (wz * rx - wx * rz); v3[3 * i + 2] = vz + (wx * ry - wy * rx);
 	}
 	CK(cudaMemsetAsync(E.lam_vol.p, 0, E.lam_vol.bytes(), E.stream));
+	E.press_reset();   // groundLaunch ends a press (forward.cu:4599-4602)
 	return E.upload_positions(p3.data(), v3.data());
 }
 
 XPBD_API int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo)
 {
-	(void)axis; (void)rampPerSec; (void)maxDispPct; (void)fromLo;
-	return fail("xpbd_press_start: the press harness is not implemented");
+	// xpbd_capi.cu:281-288: squashSetPress(true), squashSetPressFromLo, squashStart(axis, 0.08, ...)
+	Engine& E = *cur_engine();
+	if (!E.stepped) return fail("xpbd_press_start: step once first");
+	return E.press_start(axis, rampPerSec, maxDispPct, fromLo != 0);
 }
-XPBD_API void xpbd_press_autolog(int enabled) { (void)enabled; }
-XPBD_API void xpbd_press_stop(void) {}
+XPBD_API void xpbd_press_autolog(int enabled) { engine().S.press_autolog = enabled != 0; }
+XPBD_API void xpbd_press_stop(void)
+{
+	// squashStop (forward.cu:4398-4409): the plates leave, every inverse mass back to 1
+	Engine& E = *cur_engine();
+	if (!E.press_active) return;
+	E.press_active = false;
+	if (E.n > 0 && E.pos_curr.p) {
+		dev::k_set_w<<<Engine::blocks_for(E.n), kBlock, 0, E.stream>>>(E.n, E.pos_curr.p, nullptr, 1.0f);
+		E.sync();
+	}
+}
 XPBD_API int xpbd_press_state(float* lo, float* hi, float* cur, float* mx)
 {
-	if (lo) *lo = 0.0f;
-	if (hi) *hi = 0.0f;
-	if (cur) *cur = 0.0f;
-	if (mx) *mx = 0.0f;
-	return 0;
+	// squashGetProgress + squashGetPlates (forward.cu:4675-4689)
+	const Engine& E = *cur_engine();
+	if (cur) *cur = E.press_cur;
+	if (mx) *mx = E.press_max;
+	if (lo) *lo = E.press_lo + ((E.press_active && E.press_from_lo) ? E.press_cur : 0.0f);
+	if (hi) *hi = E.press_hi - ((E.press_active && !E.press_from_lo) ? E.press_cur : 0.0f);
+	return E.press_active ? 1 : 0;
 }
 
 XPBD_API void xpbd_volume_stats(int enable, float* jvw, float* jvwStd)
@@ -2424,6 +2661,7 @@ XPBD_API int xpbd_b200_set_stream(void* stream)
 	E.own_stream = false;
 	E.stream = static_cast<cudaStream_t>(stream);
 	if (E.graph_exec) { cudaGraphExecDestroy(E.graph_exec); E.graph_exec = nullptr; }
+	if (E.graph_fused) { cudaGraphExecDestroy(E.graph_fused); E.graph_fused = nullptr; }
 	E.graph_key.clear();
 	if (!E.stream) return E.ensure_stream();
 	return 0;
@@ -2537,6 +2775,22 @@ XPBD_API void xpbd_b200_set_gs(int distance, int volume)
 XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { engine().S.warp_mode = std::max(0, std::min(2, mode)); }
 
 XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled != 0; }
+
+XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std::min(2, mode)); }
+
+XPBD_API int xpbd_b200_tuning(float* out)
+{
+	// [0] form in use (0 kernel sequence, 1 fused launch), [1] 1 once decided, [2] [3] mean
+	// trial-step ms of the two forms, [4] launches per step of the form in use
+	const Engine& E = *cur_engine();
+	if (!out) return fail("xpbd_b200_tuning: null output");
+	out[0] = (float)E.tune_choice;
+	out[1] = E.tune_done ? 1.0f : 0.0f;
+	out[2] = E.tune_ms[0];
+	out[3] = E.tune_ms[1];
+	out[4] = (float)(E.tune_choice ? E.graph_fused_kernels : E.graph_kernels);
+	return 0;
+}
 
 XPBD_API void xpbd_b200_set_reorder(int enabled) { engine().S.reorder = enabled != 0; }
 

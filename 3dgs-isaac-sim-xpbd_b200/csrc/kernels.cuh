@@ -30,6 +30,26 @@ __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a
 __device__ __forceinline__ bool fin3(float3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
 __device__ __forceinline__ float comp(float3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
 __device__ __forceinline__ float4 ld4(const float4* p, int i) { return __ldg(p + i); }
+// Loads of data a kernel itself writes must not take the read-only (non-coherent) path:
+// the fused substep kernel writes positions and cluster records in one phase and reads
+// them in the next.  NC = true keeps __ldg where the data is constant for the launch.
+// With NC = false the load is an explicit ld.global (coherent after a grid barrier), so
+// that the compiler cannot turn a load through a const __restrict__ pointer into a
+// read-only one.
+template <bool NC> __device__ __forceinline__ float4 ldv(const float4* p, int i)
+{
+	if (NC) return __ldg(p + i);
+	float4 v;
+	asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p + i));
+	return v;
+}
+template <bool NC> __device__ __forceinline__ float ldv(const float* p, int i)
+{
+	if (NC) return __ldg(p + i);
+	float v;
+	asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p + i));
+	return v;
+}
 
 __device__ __forceinline__ void m3_zero(M3& a)
 {
@@ -237,11 +257,10 @@ __global__ void __launch_bounds__(kBlock) k_contact_pack(int n, const float* __r
 // forward.cu:7394-7399, run once per step at 12223-12227).  HBM: 16+16 B read, 16+16 B
 // written per Gaussian (+32 B read, 4 B written with ground contact shapes).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __restrict__ P,
+__device__ __forceinline__ void predict_row(int i, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pos_curr, float4* __restrict__ pos_next, float4* __restrict__ vel,
 	float* __restrict__ lam_vol, const float4* __restrict__ cshape, float* __restrict__ crg)
 {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const float4 x4 = pos_curr[i];
 	float4 v4 = vel[i];
@@ -260,6 +279,12 @@ __global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __r
 		vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	}
 }
+__global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pos_curr, float4* __restrict__ pos_next, float4* __restrict__ vel,
+	float* __restrict__ lam_vol, const float4* __restrict__ cshape, float* __restrict__ crg)
+{
+	predict_row(blockIdx.x * blockDim.x + threadIdx.x, n, P, pos_curr, pos_next, vel, lam_vol, cshape, crg);
+}
 
 // ---------------------------------------------------------------------------
 // distance constraints, Jacobi (forward.cu:6484-6571).  One thread per Gaussian over
@@ -268,14 +293,14 @@ __global__ void __launch_bounds__(kBlock) k_predict(int n, const StepParams* __r
 // is the same).  The first iteration of a step reads no multiplier (they start at 0)
 // and the last stores none (they are reset next step).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepParams* __restrict__ P,
+template <bool NC>
+__device__ __forceinline__ void distance_row(int idx, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ off,
 	const int* __restrict__ nbr, const float* __restrict__ ndist, const float* __restrict__ nstiff,
 	float* __restrict__ lam, int read_lam, int write_lam)
 {
-	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
-	const float4 p4 = ld4(pin, idx);
+	const float4 p4 = ldv<NC>(pin, idx);
 	const float3 pi = f3(p4);
 	const float ims = P->inv_mass_scale, ss = P->stiffness_scale, gc = P->dist_compliance;
 	const float wi = p4.w * ims;
@@ -314,8 +339,8 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 		const float l0 = read_lam ? lam[edge] : 0.0f, l1 = read_lam ? lam[edge + 1] : 0.0f;
 		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
 		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
-		if (ok0) q0 = ld4(pin, j0);
-		if (ok1) q1 = ld4(pin, j1);
+		if (ok0) q0 = ldv<NC>(pin, j0);
+		if (ok1) q1 = ldv<NC>(pin, j1);
 		const float r0 = __ldg(ndist + edge), r1 = __ldg(ndist + edge + 1);
 		const float s0 = __ldg(nstiff + edge), s1 = __ldg(nstiff + edge + 1);
 		if (ok0) edge_step(edge, q0, l0, r0, s0);
@@ -324,7 +349,7 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 	if (edge < e1) {
 		const int j = __ldg(nbr + edge);
 		const float lambda = read_lam ? lam[edge] : 0.0f;
-		if (j >= 0 && j < n) edge_step(edge, ld4(pin, j), lambda, __ldg(ndist + edge), __ldg(nstiff + edge));
+		if (j >= 0 && j < n) edge_step(edge, ldv<NC>(pin, j), lambda, __ldg(ndist + edge), __ldg(nstiff + edge));
 	}
 	float3 out = pi;
 	if (wi > 0.0f && valid > 0) {
@@ -332,6 +357,14 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 		out = add3(pi, mul3(avg, P->under_relax));
 	}
 	pout[idx] = make_float4(out.x, out.y, out.z, p4.w);
+}
+__global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ off,
+	const int* __restrict__ nbr, const float* __restrict__ ndist, const float* __restrict__ nstiff,
+	float* __restrict__ lam, int read_lam, int write_lam)
+{
+	distance_row<true>(blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, off, nbr, ndist, nstiff, lam, read_lam,
+		write_lam);
 }
 
 // distance Gauss-Seidel, one colour: thread per undirected edge, in place
@@ -816,14 +849,14 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 // cancellation in the moment form small; the result equals the two-pass form
 // (forward.cu:8531-8664) to FP32 rounding.  The reference has the same leader-relative
 // moments in its optional one-pass warp kernel (forward.cu:8864-9033, warp mode 3).
-template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
+template <int S, bool NC>
+__device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	const int sl = threadIdx.x & (S - 1);
-	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const int sl = (int)(gtid & (S - 1));
+	const int idx = (int)(gtid / S);
 	const bool in_range = idx < n;
 	bool valid = in_range && mat_type[idx] == 0;
 	int off = 0, cnt = 0;
@@ -831,7 +864,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	if (valid) {
 		off = voff[idx];
 		cnt = voff[idx + 1] - off;
-		p4 = ld4(pin, idx);
+		p4 = ldv<NC>(pin, idx);
 	}
 	const float3 pi = f3(p4);
 	const float ims = P->inv_mass_scale;
@@ -852,14 +885,14 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 		const int j0 = __ldg(vidx + off + k), j1 = __ldg(vidx + off + k + S);
 		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
 		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
-		if (ok0) q0 = ld4(pin, j0);
-		if (ok1) q1 = ld4(pin, j1);
+		if (ok0) q0 = ldv<NC>(pin, j0);
+		if (ok1) q1 = ldv<NC>(pin, j1);
 		if (ok0) add(q0);
 		if (ok1) add(q1);
 	}
 	if (k < cnt) {
 		const int j = __ldg(vidx + off + k);
-		if (j >= 0 && j < n) add(ld4(pin, j));
+		if (j >= 0 && j < n) add(ldv<NC>(pin, j));
 	}
 #pragma unroll
 	for (int t = 0; t < 20; ++t) m[t] = group_sum<S>(m[t]);
@@ -912,6 +945,15 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	if (!isfinite(dl)) { rec_invalidate(rec, idx); return; }
 	lam_vol[idx] = lam + dl;
 	store_record(rec, recz, idx, c, dl * gs, Sinv);
+}
+template <int S>
+__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
+{
+	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff, vidx, det_rest,
+		mat_type, lam_vol, rec, recz, read_lam);
 }
 
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
@@ -1018,20 +1060,20 @@ __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl,
 // Kernel B on groups of S lanes per node (forward.cu:9262-9323 with S = 32): mean over
 // the clusters that contain the node, step clamp 0.25 restLen, under-relaxation.  Reads
 // per node: h reverse indices + h gathered 36-byte records (L2-resident).
-template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
+template <int S, bool NC>
+__device__ __forceinline__ void gather_group_lane(long long gtid, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)
 {
-	const int sl = threadIdx.x & (S - 1);
-	const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / S);
+	const int sl = (int)(gtid & (S - 1));
+	const int idx = (int)(gtid / S);
 	const bool in_range = idx < n;
 	float4 p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	int off = 0, cnt = 0;
 	float wi = 0.0f;
 	if (in_range) {
-		p4 = ld4(pin, idx);
+		p4 = ldv<NC>(pin, idx);
 		wi = p4.w * P->inv_mass_scale;
 		if (wi > 0.0f) {
 			off = roff[idx];
@@ -1051,8 +1093,8 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
 		float z0 = 0.0f, z1 = 0.0f;
 		const float* cz = recz;
-		if (ok0) { a0 = __ldg(rec + 2 * i0); b0 = __ldg(rec + 2 * i0 + 1); z0 = __ldg(cz + i0); }
-		if (ok1) { a1 = __ldg(rec + 2 * i1); b1 = __ldg(rec + 2 * i1 + 1); z1 = __ldg(cz + i1); }
+		if (ok0) { a0 = ldv<NC>(rec, 2 * i0); b0 = ldv<NC>(rec, 2 * i0 + 1); z0 = ldv<NC>(cz, i0); }
+		if (ok1) { a1 = ldv<NC>(rec, 2 * i1); b1 = ldv<NC>(rec, 2 * i1 + 1); z1 = ldv<NC>(cz, i1); }
 		float3 dp;
 		if (ok0 && gather_rec(a0, b0, z0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 		if (ok1 && gather_rec(a1, b1, z1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
@@ -1060,7 +1102,7 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 	if (k < cnt) {
 		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (i >= 0 && i < n && gather_one(rec, recz, i, pi, wi, dp)) {
+		if (i >= 0 && i < n && gather_rec(ldv<NC>(rec, 2 * i), ldv<NC>(rec, 2 * i + 1), ldv<NC>(recz, i), pi, wi, dp)) {
 			sum = add3(sum, dp);
 			++received;
 		}
@@ -1074,6 +1116,15 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const Ste
 	if (!fin3(avg)) { pout[idx] = p4; return; }
 	const float3 o = gather_finish(pi, avg, __ldg(rest_len + idx), P->under_relax);
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
+}
+template <int S>
+__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
+	const float* __restrict__ rest_len)
+{
+	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff, ridx, rec,
+		recz, rest_len);
 }
 
 // Kernel B, one thread per node (forward.cu:9187-9243)
@@ -1588,15 +1639,14 @@ __global__ void __launch_bounds__(kBlock) k_shape_rest(int n, const float4* __re
 // else float), goal projection.  The rest-only terms come from k_shape_rest.  Three
 // blocks per SM (80 registers, a few spilled) hide more of the FP64 Jacobi chain's
 // latency than two (measured 1.3 -> 1.05 ms per substep at 1M).
-template <bool ROBUST>
-__global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepParams* __restrict__ P,
+template <bool ROBUST, bool NC>
+__device__ __forceinline__ void shape_row(int idx, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
 	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest,
 	float4* __restrict__ shape_q)
 {
-	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
-	const float4 p4 = ld4(pin, idx);
+	const float4 p4 = ldv<NC>(pin, idx);
 	const float3 pi = f3(p4);
 	const float wi = p4.w * P->inv_mass_scale;
 	if (wi <= 0.0f) { pout[idx] = p4; return; }
@@ -1631,14 +1681,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 		const int j0 = __ldg(nbr + e), j1 = __ldg(nbr + e + 1);
 		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
 		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0, r0 = q0, r1 = q0;
-		if (ok0) { q0 = ld4(pin, j0); r0 = ld4(rest, j0); }
-		if (ok1) { q1 = ld4(pin, j1); r1 = ld4(rest, j1); }
+		if (ok0) { q0 = ldv<NC>(pin, j0); r0 = ld4(rest, j0); }
+		if (ok1) { q1 = ldv<NC>(pin, j1); r1 = ld4(rest, j1); }
 		if (ok0) add(q0, r0);
 		if (ok1) add(q1, r1);
 	}
 	if (e < e1) {
 		const int j = __ldg(nbr + e);
-		if (j >= 0 && j < n) add(ld4(pin, j), ld4(rest, j));
+		if (j >= 0 && j < n) add(ldv<NC>(pin, j), ld4(rest, j));
 	}
 	const float3 com_curr = mul3(sq, sr.w);
 	const float3 cq = sub3(com_curr, pi), cr = sub3(com_rest, ri);
@@ -1680,6 +1730,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 	const float3 o = add3(pi, mul3(sub3(goal, pi), scale));
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
+template <bool ROBUST>
+__global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
+	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest,
+	float4* __restrict__ shape_q)
+{
+	shape_row<ROBUST, true>(blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, rest, off, nbr, shape_rest, shape_q);
+}
 
 // ---------------------------------------------------------------------------
 // per-Gaussian projections at the end of an iteration: self-collision apply
@@ -1689,17 +1747,29 @@ __global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepPara
 // semi-axis and its distance shrinks by the support along the contact normal; with
 // ground contact shapes (crg non-null) the plane is offset by the support radius.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
+__device__ __forceinline__ void project_row(int idx, int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
 	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
 	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id,
 	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range, const float4* __restrict__ sc_dp_cross,
 	float4* __restrict__ sc_accum, const float4* __restrict__ cshape, const float* __restrict__ crmax,
 	const float* __restrict__ crg)
 {
-	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
 	float4 p4 = pos[idx];
 	bool moved = false;
+	// press plates (squashPressProjectKernel, forward.cu:9411-9424): a centre outside
+	// [lo, hi] on the load axis goes onto the plate; the other axes are free (no friction)
+	if (P->press_on && p4.w > 0.0f) {
+		const int ax = P->press_axis;
+		const float v = ax == 0 ? p4.x : (ax == 1 ? p4.y : p4.z);
+		if (v < P->press_lo || v > P->press_hi) {
+			const float t = v < P->press_lo ? P->press_lo : P->press_hi;
+			if (ax == 0) p4.x = t;
+			else if (ax == 1) p4.y = t;
+			else p4.z = t;
+			moved = true;
+		}
+	}
 	if (sc_count && sc_count[idx] > 0) {
 		const float4 d = sc_dp[idx];
 		p4.x = p4.x + d.x; p4.y = p4.y + d.y; p4.z = p4.z + d.z;
@@ -1816,16 +1886,25 @@ __global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __r
 	}
 	if (moved) pos[idx] = p4;
 }
+__global__ void __launch_bounds__(kBlock) k_project(int n, const StepParams* __restrict__ P, float4* __restrict__ pos,
+	const float4* __restrict__ pos_start, const int* __restrict__ sc_count, const float4* __restrict__ sc_dp,
+	DevCounters* __restrict__ ctr, int count_hits, const int* __restrict__ obj_id,
+	const KinCollider* __restrict__ ext_kin, const int2* __restrict__ ext_range, const float4* __restrict__ sc_dp_cross,
+	float4* __restrict__ sc_accum, const float4* __restrict__ cshape, const float* __restrict__ crmax,
+	const float* __restrict__ crg)
+{
+	project_row(blockIdx.x * blockDim.x + threadIdx.x, n, P, pos, pos_start, sc_count, sc_dp, ctr, count_hits, obj_id,
+		ext_kin, ext_range, sc_dp_cross, sc_accum, cshape, crmax, crg);
+}
 
 // ---------------------------------------------------------------------------
 // velocity commit (forward.cu:6623-6672) and its ground variant (forward.cu:7528-7599);
 // also refreshes the caller-layout float3 position mirror.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __restrict__ P,
+__device__ __forceinline__ void velocity_row(int idx, int n, const StepParams* __restrict__ P,
 	float4* __restrict__ pos_curr, const float4* __restrict__ pfinal, float4* __restrict__ vel,
 	float* __restrict__ pos_out3, const int* __restrict__ perm, const float* __restrict__ crg)
 {
-	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= n) return;
 	const float4 x4 = pos_curr[idx];
 	const float4 p4 = pfinal[idx];
@@ -1882,6 +1961,12 @@ __global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __
 		pos_out3[o + 1] = p.y;
 		pos_out3[o + 2] = p.z;
 	}
+}
+__global__ void __launch_bounds__(kBlock) k_velocity(int n, const StepParams* __restrict__ P,
+	float4* __restrict__ pos_curr, const float4* __restrict__ pfinal, float4* __restrict__ vel,
+	float* __restrict__ pos_out3, const int* __restrict__ perm, const float* __restrict__ crg)
+{
+	velocity_row(blockIdx.x * blockDim.x + threadIdx.x, n, P, pos_curr, pfinal, vel, pos_out3, perm, crg);
 }
 
 // ---------------------------------------------------------------------------
@@ -2812,6 +2897,124 @@ __global__ void __launch_bounds__(kBlock) k_deformed_shapes(int n, const float4*
 }
 
 // ===========================================================================
+// The whole substep in one cooperative launch: predict, then per iteration distance,
+// volume solve and gather, shape matching and the projections, then the velocity
+// commit, with a grid-wide barrier between phases.  Every phase runs the same
+// per-item code as its own kernel (the *_row / *_lane functions above, with plain
+// loads for the data the launch itself writes), so the result is that of the kernel
+// sequence bit for bit; what changes is one launch per substep instead of one per
+// phase.  Covers the default forms (Jacobi distance, 4-lane one-pass volume solve and
+// gather, shape matching, colliders, ground, press, contact shapes); self-collision,
+// object mode and the Gauss-Seidel forms keep the kernel sequence.
+// ===========================================================================
+struct SubstepArgs {
+	int n, iters, use_distance, use_volume, use_shape, shape_robust, project;
+	const StepParams* P;
+	float4 *pos_curr, *pos_next, *pos_tmp, *vel;
+	float* lam_vol;
+	const float4* cshape;
+	const float* crmax;
+	float* crg;
+	const int *off, *nbr;
+	const float *ndist, *nstiff;
+	float* lam;
+	const int *vol_off, *vol_idx, *mat_type, *rev_off, *rev_idx;
+	const float *det_rest, *rest_len;
+	float4* rec;
+	float* recz;
+	const float4 *pos_rest, *shape_rest;
+	float4* shape_q;
+	DevCounters* ctr;
+	const int* obj_id;
+	const KinCollider* ext_kin;
+	const int2* ext_range;
+	float* pos_out3;
+	const int* perm;
+};
+
+// Grid-wide barrier of the fused launch (all blocks are co-resident: the launch is
+// cooperative).  Thread 0 of each block publishes its block's writes, arrives, and the
+// last to arrive opens the next generation; the wait is bounded (about 2^24 polls of at
+// least 64 ns): if it runs out, bar_timeout is set and the launch runs to its end with
+// the host reporting the error, instead of hanging the GPU.
+__device__ __forceinline__ void grid_barrier(DevCounters* __restrict__ ctr)
+{
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		volatile unsigned int* gen = &ctr->bar_gen;
+		const unsigned int g = *gen;
+		__threadfence();
+		if (atomicAdd(&ctr->bar_count, 1u) + 1u == gridDim.x) {
+			ctr->bar_count = 0u;
+			__threadfence();
+			atomicAdd(&ctr->bar_gen, 1u);
+		}
+		else {
+			unsigned int polls = 0;
+			while (*gen == g) {
+				if (++polls > (1u << 24)) { atomicExch(&ctr->bar_timeout, 1u); break; }
+				__nanosleep(64);
+			}
+		}
+		__threadfence();
+	}
+	__syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlock, 2) k_substep_fused(SubstepArgs A)
+{
+	DevCounters* ctr = A.ctr;
+	const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	const long long nth = (long long)gridDim.x * blockDim.x;
+	const int lane = threadIdx.x & 31;
+	const long long wbase = tid - lane;   // lane-group phases: whole warps iterate together
+	const int n = A.n;
+	const StepParams* P = A.P;
+	for (long long i = tid; i < n; i += nth)
+		predict_row((int)i, n, P, A.pos_curr, A.pos_next, A.vel, A.use_volume ? A.lam_vol : nullptr, A.cshape, A.crg);
+	grid_barrier(ctr);
+	float4* pin = A.pos_next;
+	float4* pout = A.pos_tmp;
+	for (int it = 0; it < A.iters; ++it) {
+		const int first = (it == 0), last = (it == A.iters - 1);
+		if (A.use_distance) {
+			for (long long i = tid; i < n; i += nth)
+				distance_row<false>((int)i, n, P, pin, pout, A.off, A.nbr, A.ndist, A.nstiff, A.lam, first ? 0 : 1,
+					last ? 0 : 1);
+			grid_barrier(ctr);
+			float4* t = pin; pin = pout; pout = t;
+		}
+		if (A.use_volume) {
+			for (long long b = wbase; b < 4LL * n; b += nth)
+				solve_onepass_lane<4, false>(b + lane, n, P, pin, A.vol_off, A.vol_idx, A.det_rest, A.mat_type, A.lam_vol,
+					A.rec, A.recz, first ? 0 : 1);
+			grid_barrier(ctr);
+			for (long long b = wbase; b < 4LL * n; b += nth)
+				gather_group_lane<4, false>(b + lane, n, P, pin, pout, A.rev_off, A.rev_idx, A.rec, A.recz, A.rest_len);
+			grid_barrier(ctr);
+			float4* t = pin; pin = pout; pout = t;
+		}
+		if (A.use_shape) {
+			for (long long i = tid; i < n; i += nth) {
+				if (A.shape_robust)
+					shape_row<true, false>((int)i, n, P, pin, pout, A.pos_rest, A.off, A.nbr, A.shape_rest, A.shape_q);
+				else
+					shape_row<false, false>((int)i, n, P, pin, pout, A.pos_rest, A.off, A.nbr, A.shape_rest, A.shape_q);
+			}
+			grid_barrier(ctr);
+			float4* t = pin; pin = pout; pout = t;
+		}
+		if (A.project) {
+			for (long long i = tid; i < n; i += nth)
+				project_row((int)i, n, P, pin, A.pos_curr, nullptr, nullptr, A.ctr, last ? 1 : 0, A.obj_id, A.ext_kin,
+					A.ext_range, nullptr, nullptr, A.cshape, A.crmax, A.crg);
+			grid_barrier(ctr);
+		}
+	}
+	for (long long i = tid; i < n; i += nth) velocity_row((int)i, n, P, A.pos_curr, pin, A.vel, A.pos_out3, A.perm, A.crg);
+}
+
+// ===========================================================================
 // Upload-time cluster builder on the GPU (every Gaussian a leader): k-ring BFS and the
 // farthest-point subsample of rebuildVolumeClusters (forward.cu:9814-10033), one warp
 // per leader, in the caller's index space.  Same visiting order, same candidate order,
@@ -2860,17 +3063,18 @@ __device__ __forceinline__ void build_argmax(float& v, int& m)
 	}
 }
 
-__global__ void __launch_bounds__(kBuildWarps * 32) k_build_members(int n, const int* __restrict__ off,
-	const int* __restrict__ nbr, const float* __restrict__ rest3, int ring_k, int cap, int* __restrict__ members,
-	int* __restrict__ counts)
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_members(int n, int first, int last,
+	const int* __restrict__ off, const int* __restrict__ nbr, const float* __restrict__ rest3, int ring_k, int cap,
+	int* __restrict__ members, int* __restrict__ counts)
 {
+	// lists of nodes [first, last); node i's at members[(i - first) * cap ...], counts[i - first]
 	extern __shared__ int build_sm[];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	int* col = build_sm + w * (kBallCap * 2 + kBallSet);
 	float* md = reinterpret_cast<float*>(col + kBallCap);
 	int* set = col + 2 * kBallCap;
 	const unsigned int lt = (1u << lane) - 1u;
-	for (int i = blockIdx.x * kBuildWarps + w; i < n; i += gridDim.x * kBuildWarps) {
+	for (int i = first + blockIdx.x * kBuildWarps + w; i < last; i += gridDim.x * kBuildWarps) {
 		int count = 0;
 		bool overflow = false;
 		if (ring_k <= 1) {
@@ -2921,13 +3125,13 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_members(int n, const
 			}
 		}
 		__syncwarp();
-		int* out = members + (size_t)i * cap;
+		int* out = members + (size_t)(i - first) * cap;
 		if (overflow) {
-			if (lane == 0) counts[i] = -1;   // built on the host
+			if (lane == 0) counts[i - first] = -1;   // built on the host
 		}
 		else if (count <= cap) {
 			for (int t = lane; t < count; t += 32) out[t] = col[t];
-			if (lane == 0) counts[i] = count;
+			if (lane == 0) counts[i - first] = count;
 		}
 		else {
 			// farthest point: start at the candidate farthest from the leader; each pick
@@ -2961,7 +3165,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_members(int n, const
 				if (nm < 0) break;
 				cur = nm;
 			}
-			if (lane == 0) counts[i] = picks;
+			if (lane == 0) counts[i - first] = picks;
 		}
 		__syncwarp();
 	}

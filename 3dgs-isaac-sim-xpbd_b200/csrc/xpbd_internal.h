@@ -62,6 +62,8 @@ struct StepParams {
 	int sc_single_object;           // every particle has the same object id
 	int kin_filtered;               // some collider acts on one object only
 	int kin_ext_ranges;             // objects with a range in the batched collider list
+	int press_on, press_axis;       // press harness plates on the rest axis (forward.cu:9411-9424)
+	float press_lo, press_hi;
 	KinCollider kin[kMaxColliders];
 };
 
@@ -76,6 +78,8 @@ struct DevCounters {
 	unsigned int shapes_kept;
 	unsigned int sc_active;         // Gaussians in the grid when the object box filter is on ([2])
 	unsigned int sc_fix_count;      // particles whose candidate lists reached the cap (fix-up list)
+	unsigned int bar_count, bar_gen; // grid barrier of the fused substep launch
+	unsigned int bar_timeout;       // a barrier wait of the fused launch ran out (error)
 	int kin_hits[kMaxColliders];
 	float kin_push[kMaxColliders * kColliderAcc];
 	double jstats[3];               // sum V, sum V J, sum V J^2
@@ -111,10 +115,11 @@ struct HostEdgeColoring {
 void build_graph(int n, int e, const int* edges, const float* rest, const float* stiff, HostGraph& g);
 void build_clusters(const HostGraph& g, const float* rest_pos3, int ring_k, int cap, int leader_min_hop,
 	HostClusters& out);
-// the same for leader spacing 1 from member lists built on the GPU: flat[i * cap ...],
-// counts[i] entries each, or -1 where the host builds leader i's list
-void build_clusters_from_members(const HostGraph& g, const float* rest_pos3, int ring_k, int cap, const int* flat,
-	const int* counts, HostClusters& out);
+// the same from every node's member list built on the GPU: node i's list at
+// lidx[loff[i] ...], counts[i] entries, or counts[i] = -1 where the host builds it
+void build_clusters_from_lists(const HostGraph& g, const float* rest_pos3, int ring_k, int cap, int leader_min_hop,
+	const std::vector<long long>& loff, const std::vector<int>& lidx, const std::vector<int>& counts,
+	HostClusters& out);
 void build_edge_coloring(const HostGraph& g, HostEdgeColoring& out);
 void build_components(const HostGraph& g, int min_component, std::vector<int>& obj_id, int& num_objects);
 float graph_spacing(const HostGraph& g);

@@ -99,13 +99,18 @@ XPBD_API int xpbd_reset(void);
 /* xpbd_capi.cu:272-276 — rest pose rotated by tilt (axis * angle) about the centre of
  * mass, velocity lin + ang x (x - com) */
 XPBD_API int xpbd_launch(const float* lin, const float* ang, const float* tilt);
-/* xpbd_capi.cu:281-288 — press harness: not implemented, returns -1 */
+/* xpbd_capi.cu:281-288 — press harness: plates at the rest extent of axis 0/1/2, the max
+ * (or, fromLo, the min) one closing at rampPerSec up to maxDispPct (0.01..1) of the
+ * extent; centres past a plate are projected onto it (no friction).  While it runs the
+ * ground, gravity, object shape keeping and self-collision are not applied.  -1 before
+ * the first step or when an 8 % end slab is empty. */
 XPBD_API int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo);
-/* xpbd_capi.cu:291 */
+/* xpbd_capi.cu:291 — settle 90 steps at 25/50/75/100 % of the displacement (default on) */
 XPBD_API void xpbd_press_autolog(int enabled);
-/* xpbd_capi.cu:294 */
+/* xpbd_capi.cu:294 — plates off, every inverse mass back to 1 (positions kept) */
 XPBD_API void xpbd_press_stop(void);
-/* xpbd_capi.cu:297-303 — returns 0 (no press active) */
+/* xpbd_capi.cu:297-303 — plate coordinates lo/hi, displacement, maximum; 1 while a press
+ * runs.  xpbd_reset and xpbd_launch end a press. */
 XPBD_API int xpbd_press_state(float* lo, float* hi, float* curDisp, float* maxDisp);
 /* xpbd_capi.cu:306-310 — enables per-step volume-weighted J statistics and returns
  * the last ones computed (mean, std) */
@@ -206,6 +211,14 @@ XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
 XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes);
 /* 1 (default): replay each step from a captured CUDA graph; 0: launch kernel by kernel. */
 XPBD_API void xpbd_b200_set_graph(int enabled);
+/* The substep as ONE cooperative launch (grid-wide barriers between its phases; same
+ * results as the kernel sequence, bit for bit) where the configuration allows it
+ * (no self-collision, object mode or Gauss-Seidel forms): 0 never, 1 always, 2 (default)
+ * the autotuner times both forms on the first steps after each capture and keeps the
+ * faster.  xpbd_b200_tuning fills out[5]: form in use (1 fused), decided, mean trial ms
+ * of the sequence and of the fused launch, launches per step. */
+XPBD_API void xpbd_b200_set_fused(int mode);
+XPBD_API int xpbd_b200_tuning(float* out);
 /* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
  * ABI; results identical); 0: caller order.  Takes effect at the next upload. */
 XPBD_API void xpbd_b200_set_reorder(int enabled);

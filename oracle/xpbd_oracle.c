@@ -297,6 +297,13 @@ static struct {
 	float *contact_M, *contact_rmax, *contact_rg;
 } S;
 
+/* press harness: the squash statics of forward.cu:530-568 in press mode; they outlive
+ * create / destroy like the reference's */
+static struct {
+	int active, axis, from_lo, ckpt, dwell, autolog;
+	float lo, hi, cur, max, ramp;
+} Q = { 0, 1, 0, 0, 0, 1, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f };
+
 /* parameters: file statics of forward.cu with their defaults (forward.cu:53-92, 224-265, 300-361) */
 static struct {
 	int iters;
@@ -2218,7 +2225,7 @@ static void obj_ensure_cache(void)
 static int object_on(void) { return P.obj_shape > 0.0f && S.obj_k > 0; }
 static int object_on_ensure(void)
 {
-	if (!(P.obj_shape > 0.0f)) return 0;
+	if (!(P.obj_shape > 0.0f) || Q.active) return 0;   /* objShape (forward.cu:12141) */
 	obj_ensure_cache();
 	return object_on();
 }
@@ -2374,11 +2381,45 @@ static void object_contact_push(f3* pos, const float* rg)
 /* one step: runXPBDSimulation (forward.cu:12038-12751) via stepPhysicsOnly  */
 /* (forward.cu:13253-13264)                                                   */
 /* ------------------------------------------------------------------------- */
+/* the press ramp with its checkpoint dwells, once per step (forward.cu:12095-12111) */
+static void press_advance(void)
+{
+	static const float ckpt[4] = { 0.25f, 0.50f, 0.75f, 1.00f };
+	if (!Q.active) return;
+	if (Q.autolog && Q.dwell > 0) {
+		if (--Q.dwell == 0) ++Q.ckpt;
+		return;
+	}
+	Q.cur = fminf(Q.cur + Q.ramp * P.dt, Q.max);
+	if (Q.autolog && Q.ckpt < 4) {
+		const float target = ckpt[Q.ckpt] * Q.max;
+		if (Q.cur >= target) { Q.cur = target; Q.dwell = 90; }
+	}
+}
+
+/* squashPressProjectKernel (forward.cu:9411-9424) */
+static void press_project(f3* pos)
+{
+	const float lo = Q.lo + (Q.from_lo ? Q.cur : 0.0f), hi = Q.hi - (Q.from_lo ? 0.0f : Q.cur);
+	const int ax = Q.axis;
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+	for (int i = 0; i < S.n; ++i) {
+		if (S.inv_mass[i] <= 0.0f) continue;
+		f3 p = pos[i];
+		const float v = ax == 0 ? p.x : (ax == 1 ? p.y : p.z);
+		if (!(v < lo) && !(v > hi)) continue;
+		const float t = (v < lo) ? lo : hi;
+		if (ax == 0) p.x = t; else if (ax == 1) p.y = t; else p.z = t;
+		pos[i] = p;
+	}
+}
+
 static void run_step(void)
 {
 	const int N = S.n;
 	const float dt = P.dt;
-	const f3 gravity = (P.ground_gravity > 0.0f)
+	press_advance();
+	const f3 gravity = (P.ground_gravity > 0.0f && !Q.active)
 		? mk3(-P.ground_gravity * P.ground_n[0], -P.ground_gravity * P.ground_n[1], -P.ground_gravity * P.ground_n[2])
 		: mk3(0, 0, 0);
 	if (P.use_distance && S.m > 0) {
@@ -2389,7 +2430,8 @@ static void run_step(void)
 	const int distGS = P.use_distance && P.dist_gs && S.gs_nedges > 0;
 	const int volGS = P.use_volume && P.vol_gs && S.vol_gs_ncolors > 0;
 	if (distGS) memset(S.gs_lam, 0, sizeof(float) * S.gs_nedges);
-	const int groundOn = P.ground_on;
+	const int groundOn = P.ground_on && !Q.active;   /* forward.cu:12140 */
+	const int scOn = P.sc_enabled && !Q.active;       /* forward.cu:12179 */
 	/* ellipsoid contacts (forward.cu:12222-12228): the ground radius once per step */
 	const int contactOn = (S.contact_col || S.contact_ground) && S.contact_M && S.contact_n == N;
 	const float* cRg = NULL;
@@ -2409,7 +2451,7 @@ static void run_step(void)
 		S.obj_shift_valid = 1;
 	}
 	int scContacts = 0;
-	if (P.sc_enabled) {
+	if (scOn) {
 		sc_build_active(S.pos_curr, S.pos_next, limited);
 		scContacts = S.sc_contacts;
 		if (objOn && scContacts > 0) memset(S.obj_accum, 0, sizeof(f3) * N);
@@ -2448,11 +2490,12 @@ static void run_step(void)
 			shape_matching(pin, pout, dt);
 			f3* t = pin; pin = pout; pout = t;
 		}
-		if (P.sc_enabled && scContacts > 0) sc_solve_apply(pin, objOn ? S.obj_accum : NULL);
+		if (Q.active) press_project(pin);
+		if (scOn && scContacts > 0) sc_solve_apply(pin, objOn ? S.obj_accum : NULL);
 		if (P.kin_count > 0) colliders_project(pin, it == P.iters - 1, cM, cRmax);
 		if (groundOn) ground_project(pin, cRg);
 	}
-	if (objOn && P.sc_enabled && scContacts > 0) object_contact_push(pin, cRg);
+	if (objOn && scOn && scContacts > 0) object_contact_push(pin, cRg);
 	velocity_commit(pin, dt, groundOn, cRg);
 	if (P.jstats && P.use_volume >= 0) volume_j_stats();
 }
@@ -2883,6 +2926,7 @@ EXPORT int xpbd_compute_shapes(float deformEps, float* hostScales, float* hostQu
 EXPORT int xpbd_reset(void)
 {
 	if (!S.stepped) return fail("xpbd_reset: no step yet");
+	Q.active = 0; Q.cur = 0.0f; Q.ckpt = 0; Q.dwell = 0;   /* squashReset (forward.cu:4411-4427) */
 	if (S.att_active) memcpy(S.inv_mass, S.inv_mass_saved, sizeof(float) * S.n);
 	S.att_active = 0;
 	memcpy(S.pos_curr, S.pos_rest, sizeof(f3) * S.n);
@@ -2896,6 +2940,7 @@ EXPORT int xpbd_reset(void)
 EXPORT int xpbd_launch(const float* lin, const float* ang, const float* tilt)
 {
 	if (!S.stepped) return fail("xpbd_launch: no step yet");
+	Q.active = 0; Q.cur = 0.0f; Q.ckpt = 0; Q.dwell = 0;   /* groundLaunch ends a press (forward.cu:4599-4602) */
 	const int N = S.n;
 	double cx = 0.0, cy = 0.0, cz = 0.0;
 	for (int i = 0; i < N; ++i) { cx += S.pos_rest[i].x; cy += S.pos_rest[i].y; cz += S.pos_rest[i].z; }
@@ -2925,20 +2970,47 @@ EXPORT int xpbd_launch(const float* lin, const float* ang, const float* tilt)
 	return 0;
 }
 
+/* xpbd_press_start (capi:281-288) -> squashStart in press mode (forward.cu:4311-4396) */
 EXPORT int xpbd_press_start(int axis, float rampPerSec, float maxDispPct, int fromLo)
 {
-	(void)axis; (void)rampPerSec; (void)maxDispPct; (void)fromLo;
-	return fail("xpbd_press_start: the press harness is outside the oracle");
+	if (!S.stepped) return fail("xpbd_press_start: step once first");
+	if (axis < 0 || axis > 2) axis = 1;
+	const float slab = 0.08f;
+	maxDispPct = fmaxf(0.01f, fminf(1.0f, maxDispPct));
+	float lo = FLT_MAX, hi = -FLT_MAX;
+	for (int i = 0; i < S.n; ++i) {
+		const float v = S.pos_in[3 * i + axis];
+		lo = fminf(lo, v);
+		hi = fmaxf(hi, v);
+	}
+	const float extent = hi - lo;
+	const float top = hi - slab * extent, bot = lo + slab * extent;
+	int ntop = 0, nbot = 0;
+	for (int i = 0; i < S.n; ++i) {
+		const float v = S.pos_in[3 * i + axis];
+		if (v >= top) ++ntop; else if (v <= bot) ++nbot;
+	}
+	if (ntop == 0 || nbot == 0) return fail("xpbd_press_start: squashStart failed");
+	Q.axis = axis; Q.ramp = rampPerSec; Q.lo = lo; Q.hi = hi; Q.max = maxDispPct * extent;
+	Q.from_lo = fromLo != 0; Q.cur = 0.0f; Q.ckpt = 0; Q.dwell = 0; Q.active = 1;
+	return 0;
 }
-EXPORT void xpbd_press_autolog(int enabled) { (void)enabled; }
-EXPORT void xpbd_press_stop(void) {}
+EXPORT void xpbd_press_autolog(int enabled) { Q.autolog = enabled != 0; }
+/* squashStop (forward.cu:4398-4409) */
+EXPORT void xpbd_press_stop(void)
+{
+	if (!Q.active) return;
+	Q.active = 0;
+	for (int i = 0; i < S.n && S.inv_mass; ++i) S.inv_mass[i] = 1.0f;
+}
+/* squashGetProgress + squashGetPlates (forward.cu:4675-4689) */
 EXPORT int xpbd_press_state(float* lo, float* hi, float* cur, float* mx)
 {
-	if (lo) *lo = 0.0f;
-	if (hi) *hi = 0.0f;
-	if (cur) *cur = 0.0f;
-	if (mx) *mx = 0.0f;
-	return 0;
+	if (cur) *cur = Q.cur;
+	if (mx) *mx = Q.max;
+	if (lo) *lo = Q.lo + ((Q.active && Q.from_lo) ? Q.cur : 0.0f);
+	if (hi) *hi = Q.hi - ((Q.active && !Q.from_lo) ? Q.cur : 0.0f);
+	return Q.active ? 1 : 0;
 }
 
 /* setVolumeJStatsEnabled + getVolumeJVolumeWeighted (forward.cu:4081-4099) */

@@ -236,6 +236,50 @@ def runtime_case(ref, contact_bits):
     return out
 
 
+PRESS_CHECKPOINTS = (1, 10, 40)
+
+
+def press_script(solver, record):
+    """Press harness through the C ABI (xpbd_capi.cu:281-303; forward.cu:4311-4409,
+    9411-9424, 12095-12111): a plate closing down the z axis at 1.2/s without settling
+    pauses, stopped; then one closing up from below at 3/s with the 25/50/75/100 %
+    pauses (the first one ends within the run); then reset.  record(tag, solver) after
+    the marked steps."""
+    solver.step()
+    solver.press_autolog(False)
+    solver.press_start(2, 1.2, 0.4, 0)
+    record("start", solver)
+    for k in range(1, PRESS_CHECKPOINTS[-1] + 1):
+        solver.step()
+        if k in PRESS_CHECKPOINTS:
+            record(f"a{k}", solver)
+    solver.press_stop()
+    solver.step()
+    record("stopped", solver)
+    solver.press_autolog(True)
+    solver.press_start(2, 3.0, 0.5, 1)
+    for k in range(1, 101):          # the 25 % pause (90 steps) ends at step 93
+        solver.step()
+        record(f"b{k}", solver)
+    solver.reset()
+    record("reset", solver)
+    solver.press_autolog(True)
+
+
+def press_case(ref):
+    sc = scenes.make_scene(3000, 7)
+    scen = scenes.Scenario(sc, [], substeps=1, iters=8)
+    scen.setup(ref)
+    out = scene_arrays(sc)
+
+    def record(tag, solver):
+        out[f"state_{tag}"] = np.asarray(solver.press_state(), np.float32)
+        if tag in ("a1", "a10", "a40", "stopped", "b100"):
+            out[f"pos_{tag}"] = solver.positions()
+    press_script(ref, record)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -244,7 +288,7 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     names = ["graph_n3000_r1", "graph_n3000_r2", "graph_n3000_k1", "plain_n4000", "plain_n4000_k1",
              "plain_n4000_fpolar", "plain_n4000_gs", "plain_n20000", "selfcol_blobs", "misc_n2000", "chainmail_n4000", "object_blobs",
-             "object_plain_n4000", "runtime_n4000", "runtime_n4000_ground"]
+             "object_plain_n4000", "runtime_n4000", "runtime_n4000_ground", "press_n3000"]
     if not args.only:
         # One process per case: the reference keeps its solver state in file-static globals.
         import subprocess
@@ -276,6 +320,7 @@ def main():
             ref, scenes.plain_scene_scenario(4000, 3, pins=40, object_shape=0.9), [1, 10, 100]),
         "runtime_n4000": lambda: runtime_case(ref, 1),
         "runtime_n4000_ground": lambda: runtime_case(ref, 3),
+        "press_n3000": lambda: press_case(ref),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only.split(","):

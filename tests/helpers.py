@@ -205,6 +205,25 @@ def shape_parity(sa, qa, sb, qb, diag):
             "cov": float(cov.max())}
 
 
+def press_run(solver, g):
+    """tests/golden/make_golden.py's press script on the golden file's scene: the
+    recorded press states and positions by tag."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    s = scenes.Scenario(golden_scene(g), [], substeps=1, iters=8)
+    s.setup(solver)
+    got = {}
+
+    def record(tag, sv):
+        got[f"state_{tag}"] = np.asarray(sv.press_state(), np.float32)
+        if f"pos_{tag}" in g.files:
+            got[f"pos_{tag}"] = sv.positions()
+    mg.press_script(solver, record)
+    return got
+
+
 def runtime_scenario(g):
     """The runtime scenario a golden file holds, with its recorded grasp positions."""
     return scenes.RuntimeScenario(golden_scene(g), contact_bits=int(g["contact_bits"]), grasp_pos=g["grasp_pos"])

@@ -63,7 +63,7 @@ def test_host_side_errors_without_gpu():
     rc = L.xpbd_create(0, sc["pos"].ravel(), sc["scales"].ravel(), sc["rots"].ravel(), sc["opacity"], 0,
                        np.zeros(2, np.int32), np.zeros(1, np.float32), np.zeros(1, np.float32))
     assert rc == -1 and "invalid arguments" in x.last_error()
-    assert L.xpbd_press_start(0, 0.1, 10.0, 1) == -1
+    assert L.xpbd_press_start(0, 0.1, 10.0, 1) == -1 and "step once first" in x.last_error()
 
 
 def test_graft_entry_has_build_and_smoke():

@@ -196,18 +196,21 @@ def test_internal_order_does_not_change_results(lib):
     assert H.contacts_equal(out[0][4], out[0][5], out[1][4], out[1][5])
 
 
-@pytest.mark.parametrize("knn,ring,cap", [(8, 3, 64), (8, 1, 64), (12, 3, 128), (8, 6, 64)])
-def test_gpu_cluster_builder_matches_host(lib, knn, ring, cap):
-    """Member lists built on the GPU (BFS + farthest point, one warp per leader) equal the
-    host builder's, and so the reference's (the golden topology tests use the GPU path);
-    ring 6 sends the leaders whose ball exceeds the GPU's 1024 candidates to the host."""
+@pytest.mark.parametrize("knn,ring,cap,hop", [(8, 3, 64, 1), (8, 1, 64, 1), (12, 3, 128, 1), (8, 6, 64, 1),
+                                              (8, 3, 2048, 2), (8, 3, 64, 2), (8, 2, 64, 3), (8, 6, 2048, 2)])
+def test_gpu_cluster_builder_matches_host(lib, knn, ring, cap, hop):
+    """Member lists built on the GPU (BFS + farthest point, one warp per node) equal the
+    host builder's, and so the reference's (the golden topology tests use the GPU path),
+    for every leader spacing: with spacing >= 2 the greedy cover picks leaders from the
+    precomputed lists.  Ring 6 sends the balls that exceed the GPU's 1024 candidates to
+    the host; the 2048 cap is the runtime's."""
     import ctypes
     lib.lib.xpbd_b200_set_gpu_builder.argtypes = [ctypes.c_int]
     sc = H.scenes.make_scene(6000, 9, knn=knn)
     out = []
     for gpu in (1, 0):
         lib.lib.xpbd_b200_set_gpu_builder(gpu)
-        s = H.scenes.Scenario(sc, [], ring_k=ring, max_members=cap)
+        s = H.scenes.Scenario(sc, [], ring_k=ring, max_members=cap, leader_min_hop=hop)
         s.setup(lib)
         s.advance(lib, 1)
         out.append({k: lib.ints(k) for k in ("vol_offset", "vol_count", "vol_idx", "rev_offset", "rev_count", "rev_idx")})
@@ -498,3 +501,60 @@ def test_large_scene_1m_against_oracle(lib):
     assert H.contacts_equal(lib.ints("sc_count"), lib.ints("sc_contact"), orc.ints("sc_count"), orc.ints("sc_contact"))
     orc.destroy()
     lib.destroy()
+
+
+def test_press_harness(lib):
+    """Press plates through the C ABI (xpbd_press_start / autolog / stop / state, reset
+    ending a press) against the reference's own run."""
+    g = H.load_golden("press_n3000")
+    got = H.press_run(lib, g)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    for k in g.files:
+        if k.startswith("state_"):
+            np.testing.assert_allclose(got[k], g[k], rtol=1e-6, atol=1e-6, err_msg=k)
+        elif k.startswith("pos_"):
+            tol = H.TOL_1STEP if k == "pos_a1" else H.TOL_100STEP
+            assert H.max_err_over_diag(got[k], g[k], diag) < tol, k
+
+
+@pytest.mark.parametrize("case", ["plain", "ground_contact", "press"])
+def test_fused_substep_matches_kernel_sequence(lib, case):
+    """The substep as one cooperative launch (xpbd_b200_set_fused 1) and under the
+    autotuner (2) gives the kernel sequence's results (0) bit for bit: pinned grippers
+    with capsule colliders; ground, gravity and ellipsoid contacts on both colliders and
+    ground; the press plates."""
+    import ctypes
+    L = lib.raw
+    L.xpbd_b200_set_fused.argtypes = [ctypes.c_int]
+    L.xpbd_b200_tuning.argtypes = [ctypes.c_void_p]
+    out = {}
+    for mode in (0, 1, 2):
+        L.xpbd_b200_set_fused(mode)
+        if case == "plain":
+            s = H.scenes.plain_scene_scenario(3000, 5, pins=30)
+            s.setup(lib)
+            s.advance(lib, 12)
+        elif case == "ground_contact":
+            s = H.scenes.RuntimeScenario(H.scenes.make_scene(2500, 6), contact_bits=3)
+            s.setup(lib)
+            lib.set_object_shape(0.0)           # object mode keeps the kernel sequence
+            s.advance(lib, 25)
+        else:
+            s = H.scenes.Scenario(H.scenes.make_scene(2500, 7), [], substeps=1, iters=8)
+            s.setup(lib)
+            lib.step()
+            lib.press_autolog(False)
+            lib.press_start(2, 1.2, 0.4, 0)
+            for _ in range(10):
+                lib.step()
+            lib.press_stop()
+        out[mode] = lib.positions()
+        t = np.zeros(5, np.float32)
+        L.xpbd_b200_tuning(t.ctypes.data)
+        if mode == 1:
+            assert t[0] == 1.0 and t[4] <= 2, t      # one launch per step (+ the J statistics)
+        if mode == 2:
+            assert t[1] == 1.0, t                    # the autotuner decided
+    L.xpbd_b200_set_fused(0)
+    np.testing.assert_array_equal(out[1], out[0])
+    np.testing.assert_array_equal(out[2], out[0])

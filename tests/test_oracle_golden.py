@@ -256,3 +256,17 @@ def test_runtime_scenario(orc, case):
             assert m["scale"] < H.TOL_1STEP and m["angle"] < 1e-4 and m["exempt"] < 0.1, m
         else:
             assert m["scale"] < H.TOL_100STEP and m["cov"] < 1e-2, (c, m)
+
+
+def test_press_harness(orc):
+    """Press plates (xpbd_press_*): plate positions, displacement and the 25/50/75/100 %
+    settling pauses step for step, positions within the tolerances."""
+    g = H.load_golden("press_n3000")
+    got = H.press_run(orc, g)
+    diag = H.scenes.bbox_diagonal(g["in_pos"])
+    for k in g.files:
+        if k.startswith("state_"):
+            np.testing.assert_allclose(got[k], g[k], rtol=1e-6, atol=1e-6, err_msg=k)
+        elif k.startswith("pos_"):
+            tol = H.TOL_1STEP if k == "pos_a1" else H.TOL_100STEP
+            assert H.max_err_over_diag(got[k], g[k], diag) < tol, k
