@@ -73,11 +73,19 @@ class Session:
         self.pending_since = None
         self.latencies = []
 
-    def prepare(self):
-        """The session's scene and gripper stream (host work, done by the admission thread)."""
+    def prepare(self, pool=None):
+        """The session's scene and gripper stream (host work, done by the admission thread).
+        With a scene `pool` (list of scenes), the pool scene closest in size stands in for
+        the session's own, so that scene generation stays out of the serving loop."""
         rng = np.random.default_rng(self.seed)
         radii = tuple(float(r) for r in rng.uniform(0.3, 1.5, 3))
-        sc = scenes.make_scene(self.n, self.seed, radii=radii)
+        if pool:
+            sizes = np.array([p["pos"].shape[0] for p in pool], np.float64)
+            sc = pool[int(np.argmin(np.abs(np.log(sizes) - math.log(self.n))))]
+            self.n = sc["pos"].shape[0]
+            radii = tuple(float(v) for v in np.abs(sc["pos"]).max(0))
+        else:
+            sc = scenes.make_scene(self.n, self.seed, radii=radii)
         vel = (float(rng.uniform(0.002, 0.01)), 0.0, 0.0)
         g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, math.radians(float(rng.uniform(-1, 1))))
         self.scen = scenes.Scenario(sc, [g], substeps=self.substeps, iters=self.iters)
@@ -107,14 +115,21 @@ class Session:
             self.solver = None
 
 
-def prepare_sessions(sessions):
-    """Session objects with their scenes generated (the request payloads a server receives)."""
+def prepare_sessions(sessions, pool=None):
+    """Session objects with their scenes generated, or taken from a scene pool (the
+    request payloads a server receives)."""
     out = []
     for k, (a, n, frames, seed) in enumerate(sessions):
         s = Session(k, a, n, frames, seed)
-        s.prepare()
+        s.prepare(pool)
         out.append(s)
     return out
+
+
+def scene_pool(n_min, n_max, count=12, seed=0):
+    """`count` scenes with log-spaced sizes in [n_min, n_max] (the config-0 distribution)."""
+    sizes = np.exp(np.linspace(math.log(n_min), math.log(n_max), count))
+    return [scenes.make_scene(int(round(n)), seed + k) for k, n in enumerate(sizes)]
 
 
 def _frame_arrays(resident, substeps):
@@ -160,7 +175,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
     waiting = collections.deque()
     resident, joining = [], []
     done, work, ticks, resident_bytes, resident_gauss, queued = [], 0, 0, 0.0, 0, 0
-    throughput = None            # Gaussian-substeps/s of the ticks so far
+    throughput = 2.0e8           # Gaussian-substeps/s: a prior, then the ticks' running mean
     waits = []
     sid = 0
     try:
@@ -184,7 +199,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                 need = arena_bytes(s.n)
                 if resident_bytes + need > budget_bytes:
                     break
-                if latency_target_ms and resident_gauss > 0 and throughput:
+                if latency_target_ms and resident_gauss > 0:
                     tick_ms = (resident_gauss + s.n) * s.substeps / throughput * 1e3
                     if tick_ms > latency_target_ms:
                         break
@@ -219,7 +234,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             ticks += 1
             tick_work = sum(s.n for s in resident) * sub
             rate = tick_work / max(t_end - t_tick, 1e-9)
-            throughput = rate if throughput is None else 0.8 * throughput + 0.2 * rate
+            throughput = 0.8 * throughput + 0.2 * rate
             still = []
             for s in resident:
                 s.scen.k += sub
