@@ -27,11 +27,12 @@ def library_path():
     return os.path.join(PKG_DIR, LIB_NAME)
 
 
-def XPBD(dll_path=None):
-    """The reference bridge's ``XPBD`` bound to the B200 library (or ``dll_path``)."""
+def XPBD(dll_path=None, instance=False):
+    """The reference bridge's ``XPBD`` bound to the B200 library (or ``dll_path``); with
+    ``instance=True`` an engine of its own instead of the library's singleton."""
     path = dll_path or os.environ.get("XPBD_B200_DLL") or library_path()
     if not os.path.isfile(path):
         raise FileNotFoundError(
             f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
             "or `make -C 3dgs-isaac-sim-xpbd_b200/csrc`")
-    return bridge.XPBD(path)
+    return bridge.XPBD(path, instance=instance)
