@@ -368,14 +368,28 @@ public:
 	cudaGraphExec_t graph_exec = nullptr;
 	// the same substep as one cooperative launch, and the autotuner that times both forms
 	// on the first steps after a capture (they give identical results) and keeps the faster
-	cudaGraphExec_t graph_fused = nullptr;
-	long long graph_fused_kernels = 0;
+	// the step forms the autotuner chooses from, all with the same results: 0 the kernel
+	// sequence, 1 the fused launch, 2 and 3 the sequence with its distance and volume
+	// kernels compiled for 6 and 8 resident blocks per SM
+	static constexpr int kForms = 4;
+	static constexpr int kFormOcc[kForms] = { 0, 0, 6, 8 };
+	cudaGraphExec_t graph_form[kForms] = {};
+	long long form_kernels[kForms] = {};
+	cudaGraphExec_t& graph_fused = graph_form[1];
+	long long& graph_fused_kernels = form_kernels[1];
 	static constexpr int kTuneRounds = 3;
-	cudaEvent_t tune_ev[2 * kTuneRounds][2] = {};
+	cudaEvent_t tune_ev[kForms * kTuneRounds][2] = {};
+	int tune_forms[kForms] = {}, tune_nforms = 0;
 	int tune_n = 0, tune_choice = 0;
 	bool tune_done = true;
-	float tune_ms[2] = { 0.0f, 0.0f };
+	float tune_ms[kForms] = {};
 	int fused_grid = 0;
+	void destroy_forms()
+	{
+		graph_form[0] = nullptr;   // the sequence's graph is graph_exec, destroyed with it
+		for (int f = 1; f < kForms; ++f)
+			if (graph_form[f]) { cudaGraphExecDestroy(graph_form[f]); graph_form[f] = nullptr; }
+	}
 	std::vector<long long> graph_key;
 	long long graph_kernels = 0;
 	long long launches = 0;
@@ -393,8 +407,7 @@ public:
 	{
 		if (graph_exec) cudaGraphExecDestroy(graph_exec);
 		graph_exec = nullptr;
-		if (graph_fused) cudaGraphExecDestroy(graph_fused);
-		graph_fused = nullptr;
+		destroy_forms();
 		for (auto& pr : tune_ev)
 			for (auto& e : pr)
 				if (e) { cudaEventDestroy(e); e = nullptr; }
@@ -594,7 +607,7 @@ public:
 		build_t0 = std::chrono::steady_clock::now();
 		free_device();
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
+		destroy_forms();
 		graph_key.clear();
 		if (ensure_stream()) return -1;
 		build_graph(n, n_edges, in_edges.data(), in_rest.data(), in_stiff.data(), graph);
@@ -648,7 +661,7 @@ public:
 		}
 		if (contact_bits && pack_contact(false)) return -1;   // set before the scene was on the device
 		CK(det_rest.alloc(n)); CK(v_rest.alloc(n)); CK(rest_len.alloc(n)); CK(sigma_rest.alloc(6 * (size_t)n));
-		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * (size_t)n));
+		CK(mat_type.alloc(n)); CK(lam_vol.alloc(n)); CK(rec.alloc(3 * rec_rows()));
 		CK(cudaMemsetAsync(rec.p, 0xff, rec.bytes(), stream));   // every record NaN: no record yet
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		build_components(graph, 50, obj_id, num_objects);
@@ -731,7 +744,7 @@ public:
 		CK(cudaMemsetAsync(lam_vol.p, 0, lam_vol.bytes(), stream));
 		CK(cudaStreamSynchronize(stream));
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
+		destroy_forms();
 		graph_key.clear();
 		++generation;
 		build_mark(6);
@@ -983,7 +996,7 @@ public:
 		CK(cudaStreamSynchronize(stream));
 		coloring_built = true;
 		if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-		if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
+		destroy_forms();
 		graph_key.clear();
 		return 0;
 	}
@@ -1038,7 +1051,7 @@ public:
 			CK(d_kin_ext.alloc(std::max<size_t>(count, 64)));
 			CK(d_kin_range.alloc(std::max<size_t>(h_kin_range.size(), 64)));
 			if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-			if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
+			destroy_forms();
 			graph_key.clear();
 		}
 		CK(cudaMemcpyAsync(d_kin_ext.p, h_kin_sorted.data(), sizeof(KinCollider) * count, cudaMemcpyHostToDevice, stream));
@@ -1103,7 +1116,9 @@ public:
 
 	// the c.z column of the cluster records (after the 2 x rows float4 of M and c.xy; rows =
 	// the scene's Gaussians, or an arena's capacity)
-	float* recz() const { return reinterpret_cast<float*>(rec.p + 2 * (size_t)(arena ? rows_cap : n)); }
+	float* recz() const { return reinterpret_cast<float*>(rec.p + 2 * rec_rows()); }
+	// record slots: the rows rounded up to the 8-record blocks of the interleaved halves
+	size_t rec_rows() const { return ((size_t)(arena ? rows_cap : n) + 7) & ~(size_t)7; }
 
 	bool use_warp() const
 	{
@@ -1247,8 +1262,9 @@ public:
 		return 0;
 	}
 
-	// one step's kernel sequence (the body of runXPBDSimulation)
-	int enqueue_step()
+	// one step's kernel sequence (the body of runXPBDSimulation); occ = 6 or 8 launches the
+	// distance and default volume kernels compiled for that many blocks per SM
+	int enqueue_step(int occ = 0)
 	{
 		const int N = n;
 		const dim3 B(kBlock), G = blocks_for(N);
@@ -1304,7 +1320,8 @@ public:
 				}
 			}
 			else if (S.use_distance) {
-				launch(ST_DISTANCE, G, B, dev::k_distance_jacobi, N, (const StepParams*)d_params, (const float4*)pin,
+				auto k = occ == 8 ? dev::k_distance_occ<8> : occ == 6 ? dev::k_distance_occ<6> : dev::k_distance_jacobi;
+				launch(ST_DISTANCE, G, B, k, N, (const StepParams*)d_params, (const float4*)pin,
 					pout, (const int*)off.p, (const int*)nbr.p, (const float*)ndist.p, (const float*)nstiff.p, lam.p,
 					first ? 0 : 1, last ? 0 : 1);
 				std::swap(pin, pout);
@@ -1327,7 +1344,9 @@ public:
 					const float4* cpin = pin;
 					if (la == 4 && S.lanes_a == 0)
 						// automatic: one pass over the members (any count), 4 lanes per cluster
-						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, dev::k_volume_solve_onepass<4>, N, dp, cpin,
+						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B,
+							occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
+							: dev::k_volume_solve_onepass<4>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 32)
@@ -1360,7 +1379,9 @@ public:
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 4)
-						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B, dev::k_volume_gather_group<4>, N, dp, cpin,
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B,
+							occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
+							: dev::k_volume_gather_group<4>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
@@ -1431,54 +1452,70 @@ public:
 		press_advance();
 		if (upload_params()) return -1;
 		if (profiling || !S.use_graph) {
-			if (enqueue_step()) return -1;
+			// eager launches (per-kernel events in profiling mode): the chosen sequence form
+			if (enqueue_step(kFormOcc[tune_choice == 1 ? 0 : tune_choice])) return -1;
 		}
 		else {
 			auto key = topology_key();
 			key.push_back(S.fused);
 			if (!graph_exec || key != graph_key) {
 				if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
-				if (graph_fused) { cudaGraphExecDestroy(graph_fused); graph_fused = nullptr; }
-				if (capture(false, &graph_exec, &graph_kernels)) return -1;
-				if (S.fused != 0 && fused_eligible() && capture(true, &graph_fused, &graph_fused_kernels)) {
-					cudaGetLastError();          // the kernel sequence carries on
-					graph_fused = nullptr;
+				destroy_forms();
+				if (capture(0, &graph_exec, &graph_kernels)) return -1;
+				graph_form[0] = graph_exec;
+				form_kernels[0] = graph_kernels;
+				// the other forms; one that fails to capture is left out (the sequence carries on)
+				for (int f = 1; f < kForms; ++f) {
+					const bool want = (f == 1) ? (S.fused != 0 && fused_eligible()) : (S.fused == 2);
+					if (want && capture(f, &graph_form[f], &form_kernels[f])) {
+						cudaGetLastError();
+						graph_form[f] = nullptr;
+					}
 				}
 				graph_key = key;
-				tune_done = !graph_fused || S.fused != 2;
-				tune_choice = (graph_fused && S.fused == 1) ? 1 : 0;
+				tune_nforms = 0;
+				for (int f = 0; f < kForms; ++f)
+					if (graph_form[f] && (S.fused == 2 || f == (S.fused == 1 ? 1 : 0))) tune_forms[tune_nforms++] = f;
+				if (tune_nforms == 0) tune_forms[tune_nforms++] = 0;
+				tune_done = tune_nforms == 1;
+				tune_choice = tune_forms[0];
 				tune_n = 0;
+				for (float& v : tune_ms) v = 0.0f;
 			}
 			int variant = tune_choice;
 			cudaEvent_t* ev = nullptr;
 			if (!tune_done) {
-				if (tune_n == 2 * kTuneRounds) {
+				if (tune_n == tune_nforms * kTuneRounds) {
 					// every trial step enqueued: the timings decide (one wait, once per capture)
-					float sum[2] = { 0.0f, 0.0f };
-					for (int t = 0; t < 2 * kTuneRounds; ++t) {
+					float sum[kForms] = {};
+					for (int t = 0; t < tune_n; ++t) {
 						float ms = 0.0f;
 						CK(cudaEventSynchronize(tune_ev[t][1]));
 						CK(cudaEventElapsedTime(&ms, tune_ev[t][0], tune_ev[t][1]));
-						sum[t & 1] += ms;
+						sum[tune_forms[t % tune_nforms]] += ms;
 					}
-					tune_ms[0] = sum[0] / kTuneRounds;
-					tune_ms[1] = sum[1] / kTuneRounds;
-					tune_choice = tune_ms[1] < tune_ms[0] ? 1 : 0;
+					int best = tune_forms[0];
+					for (int q = 0; q < tune_nforms; ++q) {
+						const int f = tune_forms[q];
+						tune_ms[f] = sum[f] / kTuneRounds;
+						if (tune_ms[f] < tune_ms[best]) best = f;
+					}
+					tune_choice = best;
 					tune_done = true;
 					variant = tune_choice;
 				}
 				else {
-					variant = tune_n & 1;
+					variant = tune_forms[tune_n % tune_nforms];
 					ev = tune_ev[tune_n++];
 					for (int q = 0; q < 2; ++q)
 						if (!ev[q]) CK(cudaEventCreate(&ev[q]));
 					CK(cudaEventRecord(ev[0], stream));
 				}
 			}
-			CK(cudaGraphLaunch(variant ? graph_fused : graph_exec, stream));
-			if (variant) fused_pending = true;
+			CK(cudaGraphLaunch(graph_form[variant], stream));
+			if (variant == 1) fused_pending = true;
 			if (ev) CK(cudaEventRecord(ev[1], stream));
-			launches += variant ? graph_fused_kernels : graph_kernels;
+			launches += form_kernels[variant];
 		}
 		last_sc_limited = sc_limited_now;
 		if (object_on()) obj_shift_valid = true;
@@ -1487,12 +1524,12 @@ public:
 	}
 
 	// one captured step: the kernel sequence or the fused launch
-	int capture(bool fused_form, cudaGraphExec_t* exec, long long* kernels)
+	int capture(int form, cudaGraphExec_t* exec, long long* kernels)
 	{
 		cudaGraph_t g = nullptr;
 		CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
 		const long long before = launches;
-		const int rc = fused_form ? enqueue_step_fused() : enqueue_step();
+		const int rc = form == 1 ? enqueue_step_fused() : enqueue_step(kFormOcc[form]);
 		const cudaError_t ec = cudaStreamEndCapture(stream, &g);
 		if (rc) { if (g) cudaGraphDestroy(g); return -1; }
 		CK(ec);
@@ -1576,7 +1613,7 @@ public:
 		CK(pos_curr.alloc(R)); CK(pos_next.alloc(R)); CK(pos_tmp.alloc(R)); CK(vel.alloc(R)); CK(pos_rest.alloc(R));
 		CK(shape_rest.alloc(R)); CK(shape_q.alloc(R)); CK(pos_out3.alloc(3 * R)); CK(d_perm.alloc(R));
 		CK(d_obj_id.alloc(R)); CK(lam_vol.alloc(R)); CK(det_rest.alloc(R)); CK(rest_len.alloc(R));
-		CK(mat_type.alloc(R)); CK(rec.alloc(3 * R)); CK(inv_mass_saved.alloc(R));
+		CK(mat_type.alloc(R)); CK(rec.alloc(3 * rec_rows())); CK(inv_mass_saved.alloc(R));
 		CK(off.alloc(R + 1)); CK(vol_off.alloc(R + 1)); CK(rev_off.alloc(R + 1));
 		CK(nbr.alloc((size_t)edges)); CK(ndist.alloc((size_t)edges)); CK(nstiff.alloc((size_t)edges));
 		CK(lam.alloc((size_t)edges)); CK(vol_idx_s.alloc((size_t)members)); CK(rev_idx_s.alloc((size_t)rev));
@@ -2661,7 +2698,7 @@ XPBD_API int xpbd_b200_set_stream(void* stream)
 	E.own_stream = false;
 	E.stream = static_cast<cudaStream_t>(stream);
 	if (E.graph_exec) { cudaGraphExecDestroy(E.graph_exec); E.graph_exec = nullptr; }
-	if (E.graph_fused) { cudaGraphExecDestroy(E.graph_fused); E.graph_fused = nullptr; }
+	E.destroy_forms();
 	E.graph_key.clear();
 	if (!E.stream) return E.ensure_stream();
 	return 0;
@@ -2780,15 +2817,18 @@ XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std
 
 XPBD_API int xpbd_b200_tuning(float* out)
 {
-	// [0] form in use (0 kernel sequence, 1 fused launch), [1] 1 once decided, [2] [3] mean
-	// trial-step ms of the two forms, [4] launches per step of the form in use
+	// [0] form in use (0 kernel sequence, 1 fused launch, 2 / 3 the sequence with 6 / 8
+	// blocks per SM for distance and volume), [1] 1 once decided, [2] [3] mean trial-step
+	// ms of forms 0 and 1, [4] launches per step of the form in use, [5] [6] of forms 2, 3
 	const Engine& E = *cur_engine();
 	if (!out) return fail("xpbd_b200_tuning: null output");
 	out[0] = (float)E.tune_choice;
 	out[1] = E.tune_done ? 1.0f : 0.0f;
 	out[2] = E.tune_ms[0];
 	out[3] = E.tune_ms[1];
-	out[4] = (float)(E.tune_choice ? E.graph_fused_kernels : E.graph_kernels);
+	out[4] = (float)E.form_kernels[E.tune_choice];
+	out[5] = E.tune_ms[2];
+	out[6] = E.tune_ms[3];
 	return 0;
 }
 
@@ -2997,10 +3037,14 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 		return copy_host(v, 8, out, cap);
 	}
 	if (s == "cluster_active") {   // 1 where the last iteration's cluster gave a record, else 0
-		std::vector<float4> tmp(2 * (size_t)N);
-		if (copy_dev(E.rec.p, 2LL * N, tmp.data(), 2LL * N, E.stream) < 0) return -1;
+		const long long slots = 2LL * (long long)E.rec_rows();
+		std::vector<float4> tmp((size_t)slots);
+		if (copy_dev(E.rec.p, slots, tmp.data(), slots, E.stream) < 0) return -1;
 		std::vector<float> v(N);
-		for (int r = 0; r < N; ++r) v[E.perm[r]] = std::isfinite(tmp[2 * (size_t)r + 1].z) ? 1.0f : 0.0f;
+		for (int r = 0; r < N; ++r) {
+			const size_t b = ((size_t)(r >> 3) << 4) | (size_t)(r & 7) | 8;   // the record's second half
+			v[E.perm[r]] = std::isfinite(tmp[b].z) ? 1.0f : 0.0f;
+		}
 		return copy_host(v, (long long)v.size(), out, cap);
 	}
 	if (s == "self_col") {

@@ -366,6 +366,15 @@ __global__ void __launch_bounds__(kBlock) k_distance_jacobi(int n, const StepPar
 	distance_row<true>(blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, off, nbr, ndist, nstiff, lam, read_lam,
 		write_lam);
 }
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_distance_occ(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ off,
+	const int* __restrict__ nbr, const float* __restrict__ ndist, const float* __restrict__ nstiff,
+	float* __restrict__ lam, int read_lam, int write_lam)
+{
+	distance_row<true>(blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, off, nbr, ndist, nstiff, lam, read_lam,
+		write_lam);
+}
 
 // distance Gauss-Seidel, one colour: thread per undirected edge, in place
 // (forward.cu:6576-6621)
@@ -424,15 +433,21 @@ __device__ __forceinline__ bool cluster_j_sinv(const M3& Scur, float det_rest, f
 }
 
 // Cluster blackboard record, 36 bytes in two places so that a record read touches one
-// 32-byte sector plus a 4-byte entry: rec[2 i] = (M00, M11, M22, M01), rec[2 i + 1] =
+// 16-byte halves plus a 4-byte entry: rec[rec_a(i)] = (M00, M11, M22, M01), rec[rec_b(i)] =
 // (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float array recz[i].  A record
 // the gather must skip (the reference's coef == 0) has c.x = NaN.
-__device__ __forceinline__ void rec_invalidate(float4* rec, int idx) { rec[2 * idx + 1].z = __int_as_float(0x7fc00000); }
+// The two halves of records are interleaved in blocks of 8 records (the 8 first halves,
+// then the 8 second halves): a 128-byte line holds the same half of 8 neighbouring
+// clusters, which the lanes of a gather warp, walking Morton-sorted lists, often load
+// together.
+__device__ __forceinline__ int rec_a(int i) { return ((i >> 3) << 4) | (i & 7); }
+__device__ __forceinline__ int rec_b(int i) { return rec_a(i) | 8; }
+__device__ __forceinline__ void rec_invalidate(float4* rec, int idx) { rec[rec_b(idx)].z = __int_as_float(0x7fc00000); }
 __device__ __forceinline__ void store_record(float4* rec, float* recz, int idx, float3 c, float coef, const M3& S)
 {
 	if (coef == 0.0f) { rec_invalidate(rec, idx); return; }
-	rec[2 * idx + 0] = make_float4(coef * S.m[0][0], coef * S.m[1][1], coef * S.m[2][2], coef * S.m[1][0]);
-	rec[2 * idx + 1] = make_float4(coef * S.m[2][0], coef * S.m[2][1], c.x, c.y);
+	rec[rec_a(idx)] = make_float4(coef * S.m[0][0], coef * S.m[1][1], coef * S.m[2][2], coef * S.m[1][0]);
+	rec[rec_b(idx)] = make_float4(coef * S.m[2][0], coef * S.m[2][1], c.x, c.y);
 	recz[idx] = c.z;
 }
 
@@ -955,6 +970,15 @@ __global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const St
 	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff, vidx, det_rest,
 		mat_type, lam_vol, rec, recz, read_lam);
 }
+template <int S, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_solve_occ(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
+	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
+{
+	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff, vidx, det_rest,
+		mat_type, lam_vol, rec, recz, read_lam);
+}
 
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
 __global__ void __launch_bounds__(kBlock) k_volume_solve_thread(int n, const StepParams* __restrict__ P,
@@ -1044,7 +1068,7 @@ __device__ __forceinline__ bool gather_rec(float4 r0, float4 r1, float cz, float
 __device__ __forceinline__ bool gather_one(const float4* __restrict__ rec, const float* __restrict__ recz, int i, float3 pi, float wi,
 	float3& dp)
 {
-	return gather_rec(__ldg(rec + 2 * i), __ldg(rec + 2 * i + 1), __ldg(recz + i), pi, wi, dp);
+	return gather_rec(__ldg(rec + rec_a(i)), __ldg(rec + rec_b(i)), __ldg(recz + i), pi, wi, dp);
 }
 
 __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl, float under_relax)
@@ -1093,8 +1117,8 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
 		float z0 = 0.0f, z1 = 0.0f;
 		const float* cz = recz;
-		if (ok0) { a0 = ldv<NC>(rec, 2 * i0); b0 = ldv<NC>(rec, 2 * i0 + 1); z0 = ldv<NC>(cz, i0); }
-		if (ok1) { a1 = ldv<NC>(rec, 2 * i1); b1 = ldv<NC>(rec, 2 * i1 + 1); z1 = ldv<NC>(cz, i1); }
+		if (ok0) { a0 = ldv<NC>(rec, rec_a(i0)); b0 = ldv<NC>(rec, rec_b(i0)); z0 = ldv<NC>(cz, i0); }
+		if (ok1) { a1 = ldv<NC>(rec, rec_a(i1)); b1 = ldv<NC>(rec, rec_b(i1)); z1 = ldv<NC>(cz, i1); }
 		float3 dp;
 		if (ok0 && gather_rec(a0, b0, z0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 		if (ok1 && gather_rec(a1, b1, z1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
@@ -1102,7 +1126,7 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	if (k < cnt) {
 		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (i >= 0 && i < n && gather_rec(ldv<NC>(rec, 2 * i), ldv<NC>(rec, 2 * i + 1), ldv<NC>(recz, i), pi, wi, dp)) {
+		if (i >= 0 && i < n && gather_rec(ldv<NC>(rec, rec_a(i)), ldv<NC>(rec, rec_b(i)), ldv<NC>(recz, i), pi, wi, dp)) {
 			sum = add3(sum, dp);
 			++received;
 		}
@@ -1119,6 +1143,19 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 }
 template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
+	const float* __restrict__ rest_len)
+{
+	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff, ridx, rec,
+		recz, rest_len);
+}
+
+// The distance, volume solve and gather kernels compiled for MINB resident blocks per SM
+// (fewer registers, more warps in flight for these latency-bound gathers): the same
+// per-item code, so the same results; the autotuner picks among the forms by timing.
+template <int S, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)

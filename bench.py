@@ -144,6 +144,21 @@ def bind_ext(L):
     L.xpbd_b200_stage_name.argtypes = [ctypes.c_int]
     L.xpbd_b200_launch_count.restype = ctypes.c_longlong
     L.xpbd_b200_sizes.argtypes = [ctypes.c_void_p]
+    L.xpbd_b200_set_fused.argtypes = [ctypes.c_int]
+    L.xpbd_b200_tuning.argtypes = [ctypes.c_void_p]
+
+
+FORMS = ("kernel sequence", "fused cooperative launch", "sequence, volume kernels at 6 blocks/SM",
+         "sequence, volume kernels at 8 blocks/SM")
+
+
+def tuning(L):
+    """The step form the autotuner chose and the mean trial-step times of every form."""
+    t = np.zeros(7, np.float32)
+    L.xpbd_b200_tuning(t.ctypes.data)
+    ms = {FORMS[0]: float(t[2]), FORMS[1]: float(t[3]), FORMS[2]: float(t[5]), FORMS[3]: float(t[6])}
+    return {"form": FORMS[int(t[0])], "decided": bool(t[1]), "trial_ms_per_substep": {k: v for k, v in ms.items() if v > 0},
+            "launches_per_substep": int(t[4])}
 
 
 def run_frames(solver, scen, frames, blocking):
@@ -206,6 +221,7 @@ def bench_b200(args, rank, world):
     bind_ext(x.lib)
     stream = torch.cuda.Stream()
     x.lib.xpbd_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    x.lib.xpbd_b200_set_fused(2)                     # the autotuner picks the step form (same results)
     scen.setup(x)
     run_frames(x, scen, 1, blocking=True)            # upload + build (not timed)
     with torch.cuda.stream(stream):
@@ -231,6 +247,7 @@ def bench_b200(args, rank, world):
         clk = clocks.stop()
         ms = ev0.elapsed_time(ev1)
         launches = x.lib.xpbd_b200_launch_count() - launches0
+        tuned = tuning(x.lib)
 
         # ---- the same frames again with a CUDA event pair around every kernel (eager
         # launches): per-stage times and the dominant kernel's mean launch duration ----
@@ -288,6 +305,7 @@ def bench_b200(args, rank, world):
                      "measured_over": "the timed frames repeated with an event pair around each kernel"},
         "stages_ms_per_step": {k2: v[0] / args.steps for k2, v in sorted(stages.items(), key=lambda kv: -kv[1][0])},
         "clocks": clk,
+        "autotuner": tuned,
     }
     line["residuals_fp64"] = residuals_fp64(x, scen)
     if not args.no_cpu_baseline:

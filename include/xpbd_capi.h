@@ -211,12 +211,14 @@ XPBD_API void xpbd_b200_set_volume_warp_mode(int mode);
 XPBD_API void xpbd_b200_set_volume_lanes(int solve_lanes, int gather_lanes);
 /* 1 (default): replay each step from a captured CUDA graph; 0: launch kernel by kernel. */
 XPBD_API void xpbd_b200_set_graph(int enabled);
-/* The substep as ONE cooperative launch (grid-wide barriers between its phases; same
- * results as the kernel sequence, bit for bit) where the configuration allows it
- * (no self-collision, object mode or Gauss-Seidel forms): 0 never, 1 always, 2 (default)
- * the autotuner times both forms on the first steps after each capture and keeps the
- * faster.  xpbd_b200_tuning fills out[5]: form in use (1 fused), decided, mean trial ms
- * of the sequence and of the fused launch, launches per step. */
+/* Step forms, all with the same results bit for bit: the kernel sequence (form 0); the
+ * substep as ONE cooperative launch with grid-wide barriers between its phases (form 1,
+ * where the configuration allows it: no self-collision, object mode or Gauss-Seidel
+ * forms); the sequence with its distance and volume kernels compiled for 6 or 8
+ * resident blocks per SM (forms 2, 3).  Mode 0 (default) runs form 0, 1 runs form 1,
+ * 2 lets the autotuner time every form on the first steps after each capture and keep
+ * the fastest.  xpbd_b200_tuning fills out[7]: form in use, decided, mean trial ms of
+ * forms 0 and 1, launches per step of the form in use, mean trial ms of forms 2 and 3. */
 XPBD_API void xpbd_b200_set_fused(int mode);
 XPBD_API int xpbd_b200_tuning(float* out);
 /* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
