@@ -126,6 +126,22 @@ def prepare_sessions(sessions, pool=None):
     return out
 
 
+def partition_sessions(sessions, ranks):
+    """Sessions split over `ranks` GPUs, each with an arena of its own: longest work first
+    (Gaussians x frames) onto the least loaded rank, each rank's share in arrival order.
+    Sessions are independent, so the ranks exchange nothing while they serve."""
+    def work(item):
+        return item.n * item.frames_total if isinstance(item, Session) else item[1] * item[2]
+    order = sorted(range(len(sessions)), key=lambda k: (-work(sessions[k]), k))
+    load = [0.0] * ranks
+    bins = [[] for _ in range(ranks)]
+    for k in order:
+        r = min(range(ranks), key=lambda q: (load[q], q))
+        bins[r].append(k)
+        load[r] += work(sessions[k])
+    return [sorted(b) for b in bins]
+
+
 def scene_pool(n_min, n_max, count=12, seed=0):
     """`count` scenes with log-spaced sizes in [n_min, n_max] (the config-0 distribution)."""
     sizes = np.exp(np.linspace(math.log(n_min), math.log(n_max), count))

@@ -105,3 +105,40 @@ def test_render_reference_arm_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "frames/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def _served_partition_worker(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        sessions = H.pkg.serve.make_sessions(200.0, 2.0, seed=0, n_min=5000, n_max=500000, max_frames=120)
+        mine = H.pkg.serve.partition_sessions(sessions, world)[rank]
+        parts = [None] * world
+        dist.all_gather_object(parts, mine)
+        out[rank] = (len(sessions), parts)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_served_sessions_partition_over_ranks_gloo():
+    """Served sessions split over two ranks (one arena each, nothing exchanged while
+    serving): every session on exactly one rank, each rank's share in arrival order, the
+    ranks' work within the largest session's of each other."""
+    world = 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_served_partition_worker, args=(world, port, out), nprocs=world, join=True)
+        got = dict(out)
+    total, parts = got[0]
+    assert got[1][1] == parts
+    flat = sorted(k for p in parts for k in p)
+    assert flat == list(range(total))
+    assert all(p == sorted(p) for p in parts)
+    sessions = H.pkg.serve.make_sessions(200.0, 2.0, seed=0, n_min=5000, n_max=500000, max_frames=120)
+    work = [sum(sessions[k][1] * sessions[k][2] for k in p) for p in parts]
+    assert abs(work[0] - work[1]) <= max(s[1] * s[2] for s in sessions)
