@@ -1512,7 +1512,24 @@ public:
 					CK(cudaEventRecord(ev[0], stream));
 				}
 			}
-			CK(cudaGraphLaunch(graph_form[variant], stream));
+			cudaError_t el = cudaGraphLaunch(graph_form[variant], stream);
+			if (el != cudaSuccess && variant != 0) {
+				// a form that will not launch leaves the candidates; the sequence takes the step
+				cudaGetLastError();
+				cudaGraphExecDestroy(graph_form[variant]);
+				graph_form[variant] = nullptr;
+				int k = 0;
+				for (int q = 0; q < tune_nforms; ++q)
+					if (tune_forms[q] != variant) tune_forms[k++] = tune_forms[q];
+				tune_nforms = std::max(k, 1);
+				tune_forms[0] = tune_nforms == 1 && k == 0 ? 0 : tune_forms[0];
+				tune_done = true;
+				tune_choice = 0;
+				if (ev) { CK(cudaEventRecord(ev[1], stream)); ev = nullptr; }
+				variant = 0;
+				el = cudaGraphLaunch(graph_form[0], stream);
+			}
+			CK(el);
 			if (variant == 1) fused_pending = true;
 			if (ev) CK(cudaEventRecord(ev[1], stream));
 			launches += form_kernels[variant];
