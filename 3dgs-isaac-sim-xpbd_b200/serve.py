@@ -95,9 +95,9 @@ class Session:
         sc = self.scen
         return scenes.Scenario(sc.scene, sc.grippers, substeps=self.substeps, iters=self.iters)
 
-    def admit(self, lib_path):
+    def admit(self, lib_path, pool=None):
         if self.scen is None:
-            self.prepare()
+            self.prepare(pool)
         self.solver = bridge.XPBD(lib_path, instance=True)
         self.scen.setup(self.solver)
         self.scen.advance(self.solver, 1)          # upload + topology build (first substep)
@@ -161,11 +161,12 @@ def _frame_arrays(resident, substeps):
 
 
 def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=None, latency_target_ms=None,
-               keep_results=True):
+               keep_results=True, pool=None):
     """Serve `sessions` (tuples from make_sessions, or prepared Session objects) with
     continuous batching in one arena.  Admission in arrival order while the session fits
     the budget and — with `latency_target_ms` — while the resident Gaussians, at the
-    throughput measured so far, keep a tick within the target.  Returns stats."""
+    throughput measured so far, keep a tick within the target.  Sessions given as tuples
+    are prepared when admitted (from `pool` when given).  Returns stats."""
     t0 = time.perf_counter()
     arena = bridge.Arena(lib_path, *arena_capacity(budget_bytes))
     arrivals = collections.deque(sessions)
@@ -181,7 +182,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             except queue.Empty:
                 continue
             try:
-                sess.admit(lib_path)
+                sess.admit(lib_path, pool)
             except Exception as e:   # surfaced by the serving loop
                 errors.append(e)
             ready.put(sess)
@@ -207,6 +208,8 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                     waiting.append(item)
                 else:
                     a, n, frames, seed = item
+                    if pool:                 # the pool scene that will stand in for it
+                        n = min((p["pos"].shape[0] for p in pool), key=lambda v: abs(math.log(v) - math.log(n)))
                     waiting.append(Session(sid, a * time_scale, n, frames, seed))
                 sid += 1
             # admission in arrival order: HBM budget, then the latency target
@@ -286,7 +289,7 @@ def _arrival(item):
     return item.arrival if isinstance(item, Session) else item[0]
 
 
-def run_plain(lib_path, sessions, max_wall=None):
+def run_plain(lib_path, sessions, max_wall=None, pool=None):
     """One session at a time, start to finish, on one engine (no overlap)."""
     t0 = time.perf_counter()
     work, lats, count = 0, [], 0
@@ -299,7 +302,7 @@ def run_plain(lib_path, sessions, max_wall=None):
         else:
             a, n, frames, seed = item
             s = Session(k, a, n, frames, seed)
-        s.admit(lib_path)
+        s.admit(lib_path, pool)
         while s.frames_left > 0:
             t1 = time.perf_counter()
             s.enqueue_frame()

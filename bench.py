@@ -771,16 +771,14 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
     lib = pkg.library_path()
     t0 = time.perf_counter()
     pool = serve.scene_pool(5000, 500000, 12)
-    prepared = serve.prepare_sessions(sessions, pool)
     prep_s = time.perf_counter() - t0
     runs = {}
     for name, target in (("latency_bound", 1000.0 / 60.0), ("hbm_bound", None)):
-        r = serve.run_served(lib, prepared, budget_bytes=150e9, max_wall=max_wall, latency_target_ms=target,
-                             keep_results=False)
+        r = serve.run_served(lib, sessions, budget_bytes=150e9, max_wall=max_wall, latency_target_ms=target,
+                             keep_results=False, pool=pool)
         r.pop("sessions_done", None)
         runs[name] = r
-        prepared = serve.prepare_sessions(sessions, pool)     # fresh scenario state for the next run
-    plain = serve.run_plain(lib, prepared, max_wall=max_wall) if world == 1 else None
+    plain = serve.run_plain(lib, sessions, max_wall=max_wall, pool=pool) if world == 1 else None
     if world > 1:
         # whole-job figures: work summed, wall time the slowest rank's; latencies of rank 0
         import torch.distributed as dist
