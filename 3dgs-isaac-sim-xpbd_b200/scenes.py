@@ -161,6 +161,8 @@ class Scenario:
         solver.set_shape_robust(self.shape_robust)
         solver.set_self_collision(self.self_collision, 1.5, 2.0, self.within_body)
         solver.set_object_shape(self.object_shape)   # settings outlive create / destroy: always set
+        solver.set_ground(False, (0.0, 0.0, 1.0), 0.0, gravity=0.0)
+        solver.set_colliders([], [], [])   # drops the last scene's collider poses (friction velocity)
         solver.volume_stats(False)
         self.k = 0
 
@@ -351,6 +353,7 @@ class RuntimeScenario:
         solver.set_object_shape(self.OBJECT_SHAPE)
         solver.set_object_shape_gpu(True)
         solver.set_self_collision(False, 1.5, 2.0, False)   # settings outlive create: the runtime's default
+        solver.set_colliders([], [], [])   # and so do the colliders' last poses
         solver.volume_stats(False)
         ok = solver.set_contact_shape(self.contact_bits, self.CONTACT_TAU, self.CONTACT_CAP)
         solver.set_ground(False, (0.0, 0.0, 1.0), 0.0, gravity=0.0)

@@ -251,11 +251,17 @@ def test_runtime_scenario(orc, case):
         pos, (sc_, q_, k_) = got[int(c)]
         tol = H.TOL_1STEP if c == 1 else H.TOL_100STEP
         assert H.max_err_over_diag(pos, g[f"pos_{c}"], diag) < tol, c
+        # along the trajectory the 1-ring fit amplifies the positions' differences (a
+        # squashed neighbourhood is ill-conditioned): covariances at p99 only
+        rel = H.covariance_rel_err(sc_, q_, g[f"shape_scales_{c}"], g[f"shape_quats_{c}"])
+        assert np.percentile(rel, 99) < 1e-3, (c, np.percentile(rel, 99))
+    # the writeback itself on the positions the reference reached, at every checkpoint
+    for c in g["checkpoints"]:
+        orc.set_positions(g[f"pos_{c}"])
+        sc_, q_, _ = orc.shapes(H.scenes.RuntimeScenario.DEFORM_EPS)
         m = H.shape_parity(sc_, q_, g[f"shape_scales_{c}"], g[f"shape_quats_{c}"], diag)
-        if c == 1:
-            assert m["scale"] < H.TOL_1STEP and m["angle"] < 1e-4 and m["exempt"] < 0.1, m
-        else:
-            assert m["scale"] < H.TOL_100STEP and m["cov"] < 1e-2, (c, m)
+        assert m["scale"] < H.TOL_1STEP and m["angle"] < 1e-4, (c, m)
+        assert m["exempt"] < 0.1 and m["cov_exempt"] < 1e-5, (c, m)
 
 
 def test_press_harness(orc):
