@@ -135,6 +135,7 @@ struct Settings {
 	bool gpu_builder = true;         // cluster members (BFS + farthest point) built on the GPU
 	bool press_autolog = true;       // press harness: settle at 25/50/75/100 % (forward.cu:565)
 	int fused = 0;                   // substep as one cooperative launch: 0 never, 1 always, 2 the faster (timed)
+	int sc_near = 1;                 // one-object scenes: candidate lists from the near-pair grid
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -259,7 +260,10 @@ public:
 	DBuf<float> gs_rest, gs_stiff, gs_lam;
 	DBuf<unsigned int> sc_keys;
 	DBuf<int> sc_bucket, sc_start, sc_cursor, sc_idx_sorted, sc_contacts, sc_counts, sc_block_sums, d_obj_id;
-	DBuf<int> sc_fix;                // particles whose candidate lists reached the cap
+	// near-pair grid of one-object scenes: keys, bucket counts / starts, (p, index) by bucket
+	DBuf<unsigned int> nf_keys;
+	DBuf<int> nf_bucket, nf_start;
+	DBuf<float4> nf_p;
 	DBuf<float4> sc_dp, sc_sp, sc_sr, sc_sx;
 	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
 	// ellipsoid contact shapes (xpbd_set_contact_shape; forward.cu:150-160, 6733-6757):
@@ -451,7 +455,7 @@ public:
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
 		sc_contacts.release(); sc_counts.release(); sc_block_sums.release(); d_obj_id.release(); sc_dp.release();
-		sc_fix.release();
+		nf_keys.release(); nf_bucket.release(); nf_start.release(); nf_p.release();
 		sc_sp.release(); sc_sr.release(); sc_sx.release();
 		d_scales.release(); d_rots.release(); d_out_scales.release(); d_out_quats.release(); inv_mass_saved.release();
 		d_opacity.release(); c_rmax.release(); c_rg.release(); c_shape.release();
@@ -1011,7 +1015,9 @@ public:
 		const int buckets = table + 1;   // + sentinel bucket
 		CK(sc_keys.alloc(n)); CK(sc_bucket.alloc(buckets + 1)); CK(sc_start.alloc(buckets + 1));
 		CK(sc_cursor.alloc(buckets)); CK(sc_idx_sorted.alloc(n)); CK(sc_contacts.alloc((size_t)n * kSelfColMax));
-		CK(sc_counts.alloc(n)); CK(sc_fix.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
+		CK(nf_keys.alloc(n)); CK(nf_bucket.alloc(buckets)); CK(nf_start.alloc(buckets + 1)); CK(nf_p.alloc(n));
+		CK(cudaMemsetAsync(nf_bucket.p, 0, nf_bucket.bytes(), stream));
+		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
 		CK(cudaMemsetAsync(sc_counts.p, 0, sc_counts.bytes(), stream));
 		return 0;
 	}
@@ -1139,7 +1145,8 @@ public:
 			S.use_shape, S.shape_robust, selfcol_on(), S.kin_count > 0 || S.ground_on || selfcol_on() || press_active, S.jstats,
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
-			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground() };
+			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground(),
+			selfcol_on() && sc_near_on() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -1173,20 +1180,60 @@ public:
 		return dim3((unsigned)((items + per_block - 1) / per_block));
 	}
 
-	// candidate lists: cell-ordered copies, the warp-per-home-cell build, then the
-	// sequential replacement rule for the particles that reached the cap
-	void enqueue_sc_candidates(dim3 G, dim3 B)
+	bool sc_near_on() const { return S.sc_near && single_object; }
+
+	// The once-per-step self-collision build (selfColBuild, forward.cu:11796-11849): cell
+	// size from the largest predicted displacement, then the candidate lists.  One-object
+	// scenes take the near-pair grid (k_sc_build_near); otherwise the reference's hash of
+	// the start positions, its stable counting sort and the 27-cell scan.  ref_structure
+	// also builds the hash / sorted order / cell ranges when the near-pair grid is used
+	// (the stage check reads them).
+	int enqueue_sc_build(const unsigned char* active, bool ref_structure = false)
 	{
-		launch(ST_SC_BUILD, G, B, dev::k_sc_pack, n, (const int*)sc_idx_sorted.p, (const float4*)pos_curr.p,
+		const int N = n;
+		const dim3 B(kBlock), G = blocks_for(N);
+		const int buckets = sc_table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
+		const unsigned mask = (unsigned)(sc_table - 1);
+		launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr, active);
+		launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
+		const bool near = sc_near_on();
+		if (!near || ref_structure) {
+			CK(cudaMemsetAsync(sc_bucket.p, 0, sc_bucket.bytes(), stream));
+			CK(cudaMemsetAsync(sc_cursor.p, 0, sc_cursor.bytes(), stream));
+			launch(ST_SC_BUILD, G, B, dev::k_sc_keys, N, (const float4*)pos_curr.p, (const DevCounters*)d_ctr, mask,
+				(unsigned)sc_table, sc_keys.p, sc_bucket.p, active);
+			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_blocks, (const int*)sc_bucket.p, sc_start.p, scan_n,
+				sc_block_sums.p);
+			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, nb);
+			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_add, sc_start.p, scan_n, (const int*)sc_block_sums.p);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_scatter, N, (const unsigned*)sc_keys.p, (const int*)sc_start.p,
+				sc_cursor.p, sc_idx_sorted.p);
+			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
+				sc_idx_sorted.p, (const int*)d_perm.p);
+		}
+		if (near) {
+			// fine grid: counts, starts, scatter (the scatter returns the counts to zero)
+			const int fscan = sc_table + 1, fnb = (fscan + 1023) / 1024;
+			launch(ST_SC_BUILD, G, B, dev::k_sc_near_keys, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
+				(const float4*)pos_next.p, active, mask, nf_keys.p, nf_bucket.p);
+			launch(ST_SC_BUILD, dim3(fnb), dim3(1024), dev::k_scan_blocks, (const int*)nf_bucket.p, nf_start.p, fscan,
+				sc_block_sums.p);
+			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, fnb);
+			launch(ST_SC_BUILD, dim3(fnb), dim3(1024), dev::k_scan_add, nf_start.p, fscan, (const int*)sc_block_sums.p);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_near_scatter, N, (const unsigned*)nf_keys.p, (const int*)nf_start.p,
+				nf_bucket.p, (const float4*)pos_next.p, nf_p.p);
+			launch(ST_SC_BUILD, G, B, dev::k_sc_build_near, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
+				(const float4*)pos_next.p, (const float4*)pos_rest.p, active, (const int*)nf_start.p, mask,
+				(const float4*)nf_p.p, (const int*)d_perm.p, d_ctr, sc_contacts.p, sc_counts.p);
+			return 0;
+		}
+		launch(ST_SC_BUILD, G, B, dev::k_sc_pack, N, (const int*)sc_idx_sorted.p, (const float4*)pos_curr.p,
 			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)d_obj_id.p, sc_sp.p, sc_sr.p, sc_sx.p);
-		launch(ST_SC_BUILD, G, B, dev::k_sc_build_cells, n, (const StepParams*)d_params, (const unsigned*)sc_keys.p,
-			(const int*)sc_idx_sorted.p, (const int*)sc_start.p, (unsigned)(sc_table - 1), (unsigned)sc_table,
-			(const float4*)sc_sp.p, (const float4*)sc_sr.p, (const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p,
-			sc_fix.p);
-		launch(ST_SC_BUILD, dim3(148), B, dev::k_sc_fixup, (const int*)sc_fix.p, (const StepParams*)d_params,
-			(const float4*)pos_curr.p, (const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_start.p,
-			(unsigned)(sc_table - 1), (const int*)d_obj_id.p, (const float4*)sc_sp.p, (const float4*)sc_sr.p,
-			(const float4*)sc_sx.p, d_ctr, sc_contacts.p, sc_counts.p);
+		launch(ST_SC_BUILD, G, B, dev::k_sc_build_sorted, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
+			(const float4*)pos_next.p, (const float4*)pos_rest.p, (const int*)sc_idx_sorted.p, (const int*)sc_start.p,
+			mask, (const int*)d_obj_id.p, (const float4*)sc_sp.p, (const float4*)sc_sr.p, (const float4*)sc_sx.p,
+			d_ctr, sc_contacts.p, sc_counts.p, active);
+		return 0;
 	}
 
 	// volume kernel shapes: lanes per cluster (Kernel A) and per node (Kernel B);
@@ -1284,24 +1331,7 @@ public:
 				launch(ST_SC_BUILD, G, B, dev::k_sc_active, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
 					(const float4*)pos_next.p, (const int*)d_obj_id.p, (const float*)obj_boxes.p,
 					(const float*)obj_disp.p, num_objects, sc_active.p, d_ctr);
-			const int buckets = sc_table + 1;
-			CK(cudaMemsetAsync(sc_bucket.p, 0, sc_bucket.bytes(), stream));
-			CK(cudaMemsetAsync(sc_cursor.p, 0, sc_cursor.bytes(), stream));
-			launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr, active);
-			launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
-			launch(ST_SC_BUILD, G, B, dev::k_sc_keys, N, (const float4*)pos_curr.p, (const DevCounters*)d_ctr,
-				(unsigned)(sc_table - 1), (unsigned)sc_table, sc_keys.p, sc_bucket.p, active);
-			const int scan_n = buckets + 1;
-			const int nb = (scan_n + 1023) / 1024;
-			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_blocks, (const int*)sc_bucket.p, sc_start.p, scan_n,
-				sc_block_sums.p);
-			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, nb);
-			launch(ST_SC_BUILD, dim3(nb), dim3(1024), dev::k_scan_add, sc_start.p, scan_n, (const int*)sc_block_sums.p);
-			launch(ST_SC_BUILD, G, B, dev::k_sc_scatter, N, (const unsigned*)sc_keys.p, (const int*)sc_start.p,
-				sc_cursor.p, sc_idx_sorted.p);
-			launch(ST_SC_BUILD, blocks_for(buckets), B, dev::k_sc_order, buckets, (const int*)sc_start.p,
-				sc_idx_sorted.p, (const int*)d_perm.p);
-			enqueue_sc_candidates(G, B);
+			if (enqueue_sc_build(active)) return -1;
 			if (obj_push()) CK(cudaMemsetAsync(sc_accum.p, 0, sc_accum.bytes(), stream));
 		}
 		float4* pin = pos_next.p;
@@ -2831,6 +2861,7 @@ XPBD_API void xpbd_b200_set_volume_warp_mode(int mode) { engine().S.warp_mode = 
 XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled != 0; }
 
 XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std::min(2, mode)); }
+XPBD_API void xpbd_b200_set_selfcol_near(int enabled) { engine().S.sc_near = enabled ? 1 : 0; }
 
 XPBD_API int xpbd_b200_tuning(float* out)
 {
@@ -3113,20 +3144,7 @@ XPBD_API int xpbd_b200_selfcol_build(const float* x, const float* p)
 	CK(cudaMemcpyAsync(E.pos_curr.p, a.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemcpyAsync(E.pos_next.p, b.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, E.stream));
 	CK(cudaMemsetAsync(E.d_ctr, 0, sizeof(DevCounters), E.stream));
-	const dim3 B(kBlock), G = Engine::blocks_for(N);
-	const int buckets = E.sc_table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
-	CK(cudaMemsetAsync(E.sc_bucket.p, 0, E.sc_bucket.bytes(), E.stream));
-	CK(cudaMemsetAsync(E.sc_cursor.p, 0, E.sc_cursor.bytes(), E.stream));
-	dev::k_sc_disp<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.pos_next.p, E.d_ctr, nullptr);
-	dev::k_sc_setup<<<1, 1, 0, E.stream>>>(E.d_params, E.d_ctr);
-	dev::k_sc_keys<<<G, B, 0, E.stream>>>(N, E.pos_curr.p, E.d_ctr, (unsigned)(E.sc_table - 1), (unsigned)E.sc_table,
-		E.sc_keys.p, E.sc_bucket.p, nullptr);
-	dev::k_scan_blocks<<<nb, 1024, 0, E.stream>>>(E.sc_bucket.p, E.sc_start.p, scan_n, E.sc_block_sums.p);
-	dev::k_scan_sums<<<1, 1024, 0, E.stream>>>(E.sc_block_sums.p, nb);
-	dev::k_scan_add<<<nb, 1024, 0, E.stream>>>(E.sc_start.p, scan_n, E.sc_block_sums.p);
-	dev::k_sc_scatter<<<G, B, 0, E.stream>>>(N, E.sc_keys.p, E.sc_start.p, E.sc_cursor.p, E.sc_idx_sorted.p);
-	dev::k_sc_order<<<Engine::blocks_for(buckets), B, 0, E.stream>>>(buckets, E.sc_start.p, E.sc_idx_sorted.p, E.d_perm.p);
-	E.enqueue_sc_candidates(G, B);
+	if (E.enqueue_sc_build(nullptr, true)) return -1;
 	CK(cudaGetLastError());
 	if (E.read_counters()) return -1;
 	// restore the solver state this stage check borrowed

@@ -2324,178 +2324,190 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
 }
 
-// Candidate lists, one warp per run of particles that share a start cell (the home
-// cell).  Such particles have the same 27 neighbour cells in the same order, so the
-// warp concatenates the cells' bucket ranges into one sequence of E entries and tests
-// (home particle, entry) pairs with every lane busy: with k home particles padded to
-// K = 2^ceil(log2 k), lane l tests particle l mod K against entry e0 + l / K.  A
-// particle's accepted entries arrive in entry order across its lanes, so a ballot and
-// a prefix count append them to its list in the reference's order (forward.cu:
-// 7079-7180); the same tests as sc_build_one decide acceptance.  A particle that would
-// pass 32 candidates takes the replacement rule instead: it goes on the fix-up list
-// and k_sc_fixup builds its list with sc_build_one.  Warp w owns the runs that begin
-// at sorted positions [32 w, 32 w + 32) of its buckets.
-__global__ void __launch_bounds__(kBlock) k_sc_build_cells(int n, const StepParams* __restrict__ P,
-	const unsigned int* __restrict__ keys, const int* __restrict__ idx_sorted, const int* __restrict__ start,
-	unsigned int mask, unsigned int sentinel, const float4* __restrict__ sp, const float4* __restrict__ sr,
-	const float4* __restrict__ sx, DevCounters* __restrict__ ctr, int* __restrict__ contacts,
-	int* __restrict__ counts, int* __restrict__ fix_list)
+// ---------------------------------------------------------------------------
+// Near-pair candidate lists for a scene of one object.
+//
+// There every accepted pair is a same-object pair, accepted when its predicted
+// positions are closer than the search radius and its rest positions at least the
+// exclusion distance apart (sc_build_one's same-object branch).  The reference finds
+// those pairs by scanning the 27 cells around each start position with cells of
+// search + 2 max|p - x| (about 100 entries per particle in a moving scene, nearly all
+// rejected).  Here a second grid hashes the PREDICTED positions with cells of
+// kNearCellScale x search, so a pair within the search radius is always in adjacent
+// cells (the margin absorbs the rounding of p / cell for coordinates up to ~2000 cells
+// from the origin) and the 27 cells hold about 1/6 of the entries.  Whatever the grid,
+// the list must be the reference's: its order is the order in which the reference
+// visits the pairs — the first of the particle's 27 start-position cells whose hash is
+// the neighbour's bucket, then the caller index within the bucket (the stable sort) —
+// and the cap-of-32 replacement rule depends on that order.  So each accepted pair
+// gets the key (kc, caller index); a neighbour whose bucket is none of the 27 (possible
+// only when the reference's cell size is capped) is dropped as the reference never
+// sees it; the keys are taken in ascending order in batches of kNearBatch (the batch's
+// smallest keys above the last one taken, one rescan per batch) and fed through the
+// same append / replacement code.  Lists, counts and the over-cap count equal the
+// cell-hash scan's bit for bit.
+// ---------------------------------------------------------------------------
+constexpr float kNearCellScale = 1.001f;
+constexpr int kNearBatch = 48;
+
+__device__ __forceinline__ float sc_near_inv(const StepParams* __restrict__ P)
 {
-	const int lane = threadIdx.x & 31;
-	const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-	const int base0 = w * 32;
-	if (base0 >= n) return;
-	const unsigned int lt_mask = (1u << lane) - 1u;
-	const float inv_cell = ctr->sc_inv_cell;
-	const float search = P->sc_search, excl2 = P->sc_excl2, cross_excl2 = P->sc_cross_excl2;
-	const float fast_rel = P->sc_fast_rel;
-	const int within = P->sc_within;
-	const bool single_object = P->sc_single_object != 0;
-	const float search2 = search * search;
-	// bucket starts in this warp's window
-	const int mypos = base0 + lane;
-	unsigned int mykey = sentinel + 1u;
-	if (mypos < n) mykey = keys[idx_sorted[mypos]];
-	const bool is_start = mypos < n && start[mykey] == mypos;
-	unsigned int starts = __ballot_sync(0xffffffffu, is_start);
-	unsigned int total = 0u;
-	while (starts) {
-		const int l0 = __ffs(starts) - 1;
-		starts &= starts - 1u;
-		const unsigned int b = __shfl_sync(0xffffffffu, mykey, l0);
-		int hb = base0 + l0;
-		const int be = start[b + 1];
-		if (b == sentinel) {   // particles out of the grid (inactive or not finite): no list
-			for (int t = hb + lane; t < be; t += 32) counts[idx_sorted[t]] = 0;
-			continue;
-		}
-		while (hb < be) {
-			// the run of particles from hb sharing hb's start cell (at most 32)
-			const int tp = hb + lane;
-			int ccx = 0, ccy = 0, ccz = 0;
-			if (tp < be) {
-				const float4 xt = sx[tp];
-				ccx = sc_cell(xt.x, inv_cell); ccy = sc_cell(xt.y, inv_cell); ccz = sc_cell(xt.z, inv_cell);
-			}
-			const int cx = __shfl_sync(0xffffffffu, ccx, 0), cy = __shfl_sync(0xffffffffu, ccy, 0),
-				cz = __shfl_sync(0xffffffffu, ccz, 0);
-			const unsigned int same = __ballot_sync(0xffffffffu, tp < be && ccx == cx && ccy == cy && ccz == cz);
-			const int k = (~same) ? __ffs(~same) - 1 : 32;
-			// neighbour cells: lane kc < 27 holds cell kc's bucket range, empty for a
-			// hash that repeats an earlier cell's
-			unsigned int h = 0xffffffffu;
-			if (lane < 27) h = sc_hash(cx + lane % 3 - 1, cy + (lane / 3) % 3 - 1, cz + lane / 9 - 1, mask);
-			bool dup = false;
-#pragma unroll
-			for (int m = 0; m < 26; ++m) {
-				const unsigned int hm = __shfl_sync(0xffffffffu, h, m);
-				dup = dup || (m < lane && hm == h);
-			}
-			int cs = 0, len = 0;
-			if (lane < 27 && !dup) { cs = start[h]; len = start[h + 1] - cs; }
-			int off = len;   // inclusive scan, then exclusive
-#pragma unroll
-			for (int o = 1; o < 32; o <<= 1) {
-				const int v = __shfl_up_sync(0xffffffffu, off, o);
-				if (lane >= o) off += v;
-			}
-			const int E = __shfl_sync(0xffffffffu, off, 31);
-			off -= len;
-			// home particle of this lane
-			const int K = k <= 1 ? 1 : (k <= 2 ? 2 : (k <= 4 ? 4 : (k <= 8 ? 8 : (k <= 16 ? 16 : 32))));
-			const int G = 32 / K;
-			const int a = lane & (K - 1), sub = lane / K;
-			const bool home = a < k;
-			int i = -1;
-			float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f), p = x, q = x;
-			if (home) {
-				const int hp = hb + a;
-				p = sp[hp];
-				i = __float_as_int(p.w);
-				q = sr[hp];
-				x = sx[hp];
-			}
-			const bool live = home && isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
-			const int oi = __float_as_int(q.w);
-			const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
-			unsigned int gmask = 0u;   // lanes of this lane's home particle
-			for (int l = a; l < 32; l += K) gmask |= 1u << l;
-			int cnt = 0;
-			bool over = false;
-			for (int e0 = 0; e0 < E; e0 += G) {
-				const int e = e0 + sub;
-				// cell of entry e: the last cell whose offset is <= e
-				int kc = 0;
-#pragma unroll
-				for (int step = 16; step > 0; step >>= 1) {
-					const int mid = kc + step;
-					const int v = __shfl_sync(0xffffffffu, off, mid < 27 ? mid : 26);
-					if (mid < 27 && v <= e) kc = mid;
-				}
-				const int t = __shfl_sync(0xffffffffu, cs, kc) + (e - __shfl_sync(0xffffffffu, off, kc));
-				bool pass = false;
-				int code = 0;
-				if (live && e < E) {
-					const float4 pj = sp[t];
-					const int j = __float_as_int(pj.w);
-					const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
-					const float d2 = ex * ex + ey * ey + ez * ez;
-					const bool near_same = d2 < search2;
-					if (j != i && (near_same || !single_object)) {
-						const float4 rj = sr[t];
-						const bool cross = __float_as_int(rj.w) != oi;
-						if (cross || within) {
-							const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
-							const float q2 = qx * qx + qy * qy + qz * qz;
-							code = j;
-							if (cross) {
-								const float4 xj = sx[t];
-								const float fx = x.x - xj.x, fy = x.y - xj.y, fz = x.z - xj.z;
-								const float dist_x = sqrtf(fx * fx + fy * fy + fz * fz);
-								const float rx = dix - (pj.x - xj.x), ry = diy - (pj.y - xj.y), rz = diz - (pj.z - xj.z);
-								const float rel = sqrtf(rx * rx + ry * ry + rz * rz);
-								pass = (dist_x < search + rel) && (q2 >= cross_excl2);
-								if (rel > fast_rel) code = -(j + 1);
-							}
-							else
-								pass = near_same && (q2 >= excl2);
-						}
-					}
-				}
-				const unsigned int acc = __ballot_sync(0xffffffffu, pass) & gmask;
-				const int rank = __popc(acc & lt_mask);
-				if (pass && cnt + rank < kSelfColMax) contacts[(size_t)i * kSelfColMax + cnt + rank] = code;
-				cnt += __popc(acc);
-				over = over || cnt > kSelfColMax;
-			}
-			if (home && sub == 0) {
-				if (over) fix_list[atomicAdd(&ctr->sc_fix_count, 1u)] = i;
-				else { counts[i] = cnt; total += (unsigned int)cnt; }
-			}
-			hb += k;
-		}
-	}
-	for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
-	if (lane == 0 && total > 0u) atomicAdd(&ctr->sc_contacts, total);
+	return 1.0f / (P->sc_search * kNearCellScale);
 }
 
-// The particles whose lists reached the cap: sequential build with the replacement
-// rule (sc_build_one), grid-stride over the fix-up list.
-__global__ void __launch_bounds__(kBlock) k_sc_fixup(const int* __restrict__ fix_list, const StepParams* __restrict__ P,
+// fine-grid keys: predicted position's cell; particles outside the reference grid
+// (inactive, or a start / predicted position not finite) are left out
+__global__ void __launch_bounds__(kBlock) k_sc_near_keys(int n, const StepParams* __restrict__ P,
+	const float4* __restrict__ X, const float4* __restrict__ Pp, const unsigned char* __restrict__ active,
+	unsigned int mask, unsigned int* __restrict__ keys, int* __restrict__ bucket)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float4 x = X[i], p = Pp[i];
+	unsigned int k = 0xffffffffu;
+	if ((!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) &&
+		isfinite(p.z)) {
+		const float inv = sc_near_inv(P);
+		k = sc_hash(sc_cell(p.x, inv), sc_cell(p.y, inv), sc_cell(p.z, inv), mask);
+		atomicAdd(&bucket[k], 1);
+	}
+	keys[i] = k;
+}
+
+// scatter predicted position + index into the fine buckets (order within a bucket is
+// free: the lists are ordered by key afterwards); leaves the bucket counts at zero
+__global__ void __launch_bounds__(kBlock) k_sc_near_scatter(int n, const unsigned int* __restrict__ keys,
+	const int* __restrict__ start, int* __restrict__ bucket, const float4* __restrict__ Pp, float4* __restrict__ fp)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const unsigned int k = keys[i];
+	if (k == 0xffffffffu) return;
+	const int pos = start[k] + atomicSub(&bucket[k], 1) - 1;
+	const float4 p = Pp[i];
+	fp[pos] = make_float4(p.x, p.y, p.z, __int_as_float(i));
+}
+
+// the key of accepted neighbour j of particle i: the first of i's 27 start cells
+// (reference order) whose hash is j's bucket, then j's caller index; ~0 = never visited
+__device__ __forceinline__ unsigned long long sc_near_key(int cx, int cy, int cz, float4 xj, float inv_cell,
+	unsigned int mask, unsigned int caller_j)
+{
+	const unsigned int hj = sc_hash(sc_cell(xj.x, inv_cell), sc_cell(xj.y, inv_cell), sc_cell(xj.z, inv_cell), mask);
+	for (int kc = 0; kc < 27; ++kc)
+		if (sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask) == hj)
+			return ((unsigned long long)kc << 32) | caller_j;
+	return ~0ull;
+}
+
+__global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
-	const int* __restrict__ start, unsigned int mask, const int* __restrict__ obj_id, const float4* __restrict__ sp,
-	const float4* __restrict__ sr, const float4* __restrict__ sx, DevCounters* __restrict__ ctr,
+	const unsigned char* __restrict__ active, const int* __restrict__ start_f, unsigned int mask,
+	const float4* __restrict__ fp, const int* __restrict__ perm, DevCounters* __restrict__ ctr,
 	int* __restrict__ contacts, int* __restrict__ counts)
 {
-	const unsigned int nfix = ctr->sc_fix_count;
-	for (unsigned int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfix; f += gridDim.x * blockDim.x) {
-		const int i = fix_list[f];
-		int over = 0;
-		const int cnt = sc_build_one(i, P, X, Pp, rest, start, mask, obj_id, sp, sr, sx, ctr, contacts, over);
-		counts[i] = cnt;
-		atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
-		if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	int cnt = 0, over = 0;
+	const float4 x = X[i], p = Pp[i];
+	if ((!active || active[i]) && P->sc_within && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) &&
+		isfinite(p.y) && isfinite(p.z)) {
+		const float search = P->sc_search, excl2 = P->sc_excl2;
+		const float search2 = search * search;
+		const float inv = sc_near_inv(P);
+		const float4 q = rest[i];
+		const int fx = sc_cell(p.x, inv), fy = sc_cell(p.y, inv), fz = sc_cell(p.z, inv);
+		// the fine cells whose hash does not repeat an earlier one's
+		unsigned int use = 0u;
+		{
+			unsigned long long seen = 0ull;
+			for (int kc = 0; kc < 27; ++kc) {
+				const unsigned int h = sc_hash(fx + kc % 3 - 1, fy + (kc / 3) % 3 - 1, fz + kc / 9 - 1, mask);
+				const unsigned long long bit = 1ull << (h & 63u);
+				if (seen & bit) {
+					bool dup = false;
+					for (int m = 0; m < kc && !dup; ++m)
+						dup = sc_hash(fx + m % 3 - 1, fy + (m / 3) % 3 - 1, fz + m / 9 - 1, mask) == h;
+					if (dup) continue;
+				}
+				seen |= bit;
+				use |= 1u << kc;
+			}
+		}
+		// the particle's own reference cell, for the keys
+		const float inv_cell = ctr->sc_inv_cell;
+		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+		int* out = contacts + (size_t)i * kSelfColMax;
+		float prio[kSelfColMax];
+		int tier[kSelfColMax];
+		unsigned long long last = 0ull;
+		bool first_batch = true;
+		for (;;) {
+			// the kNearBatch smallest keys above `last`, ascending
+			unsigned long long bk[kNearBatch];
+			float bd2[kNearBatch];
+			int bj[kNearBatch];
+			int nb = 0;
+			bool more = false;
+			unsigned int u = use;
+			while (u) {
+				const int kc = __ffs(u) - 1;
+				u &= u - 1u;
+				const unsigned int h = sc_hash(fx + kc % 3 - 1, fy + (kc / 3) % 3 - 1, fz + kc / 9 - 1, mask);
+				const int cs = start_f[h], ce = start_f[h + 1];
+				for (int t = cs; t < ce; ++t) {
+					const float4 pj = fp[t];
+					const int j = __float_as_int(pj.w);
+					if (j == i) continue;
+					const float ex = p.x - pj.x, ey = p.y - pj.y, ez = p.z - pj.z;
+					const float d2 = ex * ex + ey * ey + ez * ez;
+					if (!(d2 < search2)) continue;
+					const float4 rj = rest[j];
+					const float qx = q.x - rj.x, qy = q.y - rj.y, qz = q.z - rj.z;
+					const float q2 = qx * qx + qy * qy + qz * qz;
+					if (!(q2 >= excl2)) continue;
+					const unsigned long long key =
+						sc_near_key(cx, cy, cz, X[j], inv_cell, mask, (unsigned int)(perm ? perm[j] : j));
+					if (key == ~0ull || (!first_batch && key <= last)) continue;
+					if (nb == kNearBatch) {
+						more = true;
+						if (key >= bk[kNearBatch - 1]) continue;
+						--nb;   // the largest leaves the batch
+					}
+					int m = nb;
+					while (m > 0 && bk[m - 1] > key) {
+						bk[m] = bk[m - 1]; bd2[m] = bd2[m - 1]; bj[m] = bj[m - 1];
+						--m;
+					}
+					bk[m] = key; bd2[m] = d2; bj[m] = j;
+					++nb;
+				}
+			}
+			// the reference's append / replacement, in key order
+			for (int a = 0; a < nb; ++a) {
+				const float pr = sqrtf(bd2[a]);
+				const int tr = 1;
+				if (cnt < kSelfColMax) {
+					out[cnt] = bj[a]; prio[cnt] = pr; tier[cnt] = tr; ++cnt;
+				}
+				else {
+					int worst = 0;
+					for (int m = 1; m < kSelfColMax; ++m)
+						if (tier[m] > tier[worst] || (tier[m] == tier[worst] && prio[m] > prio[worst])) worst = m;
+					if (tr < tier[worst] || (tr == tier[worst] && pr < prio[worst])) {
+						out[worst] = bj[a]; prio[worst] = pr; tier[worst] = tr;
+					}
+					++over;
+				}
+			}
+			if (!more) break;
+			last = bk[nb - 1];
+			first_batch = false;
+		}
 	}
+	counts[i] = cnt;
+	if (cnt > 0) atomicAdd(&ctr->sc_contacts, (unsigned int)cnt);
+	if (over > 0) atomicAdd(&ctr->sc_overflow, (unsigned int)over);
 }
 
 __device__ __forceinline__ bool sc_start_normal(float4 xi, float4 xj, float4 qi, float4 qj, float& nx, float& ny,

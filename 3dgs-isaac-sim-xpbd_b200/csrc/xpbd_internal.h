@@ -77,7 +77,6 @@ struct DevCounters {
 	unsigned int shapes_deformed;
 	unsigned int shapes_kept;
 	unsigned int sc_active;         // Gaussians in the grid when the object box filter is on ([2])
-	unsigned int sc_fix_count;      // particles whose candidate lists reached the cap (fix-up list)
 	unsigned int bar_count, bar_gen; // grid barrier of the fused substep launch
 	unsigned int bar_timeout;       // a barrier wait of the fused launch ran out (error)
 	int kin_hits[kMaxColliders];

@@ -221,6 +221,11 @@ XPBD_API void xpbd_b200_set_graph(int enabled);
  * forms 0 and 1, launches per step of the form in use, mean trial ms of forms 2 and 3. */
 XPBD_API void xpbd_b200_set_fused(int mode);
 XPBD_API int xpbd_b200_tuning(float* out);
+/* Self-collision candidate lists of a one-object scene: 1 (default) from a grid of the
+ * predicted positions with cells of the search radius, re-ordered into the reference's
+ * visiting order; 0 from the reference's own 27-cell scan of the start-position hash
+ * (selfColBuildKernel).  The lists are identical either way. */
+XPBD_API void xpbd_b200_set_selfcol_near(int enabled);
 /* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
  * ABI; results identical); 0: caller order.  Takes effect at the next upload. */
 XPBD_API void xpbd_b200_set_reorder(int enabled);

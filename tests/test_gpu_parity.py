@@ -473,6 +473,51 @@ def test_contact_shapes_agree_with_oracle(lib):
     assert H.max_err_over_diag(out["oracle", 1, 10], out["oracle", 3, 10], diag) > 1e-4   # ground shapes matter
 
 
+def test_selfcol_near_grid_matches_cell_scan(lib):
+    """One-object scenes build their candidate lists from a grid of the predicted
+    positions (cells of the search radius) and re-order them into the reference's
+    visiting order; the lists, counts, totals and over-cap counts equal the reference's
+    27-cell scan of the start-position hash (and the oracle's) bit for bit.  Inputs: the
+    two halves of a body predicted 0.05 toward each other, and 300 Gaussians collapsed to
+    within 2e-5 of one point (about 300 accepted pairs each: several key batches and the
+    cap-of-32 replacement rule).  Then a few frames of the large scene under both builds
+    give identical positions."""
+    sc = H.scenes.make_scene(60000, 5)
+    x = sc["pos"].copy()
+    p = x.copy()
+    p[:, 0] += np.where(x[:, 0] > 0.0, np.float32(-0.05), np.float32(0.05))
+    d = np.linalg.norm(x - np.float32([0.2, 0.1, 0.0]), axis=1)
+    blob = np.argsort(d, kind="stable")[:300]
+    jitter = np.random.default_rng(3).uniform(-1e-5, 1e-5, (300, 3)).astype(np.float32)
+    p[blob] = np.float32([0.2, 0.1, 0.0]) + jitter
+    orc = H.oracle()
+    got = {}
+    for name, solver, near in (("near", lib, 1), ("scan", lib, 0), ("oracle", orc, None)):
+        s = H.scenes.large_scene_scenario(scene=sc)
+        s.setup(solver)
+        solver.step()
+        if near is not None:
+            solver.lib.xpbd_b200_set_selfcol_near(near)
+        total = solver.selfcol_build(x, p)
+        got[name] = (total, solver.self_collision_stats(), solver.ints("sc_count"), solver.ints("sc_contact"))
+    lib.lib.xpbd_b200_set_selfcol_near(1)
+    orc.destroy()
+    assert got["near"][0] > 10000 and got["near"][1][2] > 0   # candidates and replacements
+    for other in ("scan", "oracle"):
+        assert got["near"][0] == got[other][0], other
+        assert got["near"][1][0] == got[other][1][0] and got["near"][1][2] == got[other][1][2], other
+        assert H.contacts_equal(got["near"][2], got["near"][3], got[other][2], got[other][3]), other
+    pos = {}
+    for near in (1, 0):
+        lib.lib.xpbd_b200_set_selfcol_near(near)
+        s = H.scenes.large_scene_scenario(30000)
+        s.setup(lib)
+        s.advance(lib, 3)
+        pos[near] = lib.positions()
+    lib.lib.xpbd_b200_set_selfcol_near(1)
+    np.testing.assert_array_equal(pos[1], pos[0])
+
+
 def test_large_scene_1m_against_oracle(lib):
     """The 1,000,000-Gaussian large scene at the bench's settings (8-NN graph, 64-member
     clusters of 3-ring candidates, shape matching, self-collision within the body, two
