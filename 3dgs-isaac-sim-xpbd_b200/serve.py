@@ -2,19 +2,22 @@
 
 A session is a scene plus a stream of gripper poses (frames).  Sessions arrive over
 time and wait in arrival order; each is admitted while it fits the HBM budget (and, if
-one is given, while the arena's predicted step time stays within a latency target).  An
-admission thread builds the session's topology and takes its first substep on an
-engine of its own (beside the GPU work of the resident sessions), then the session
-joins the serving arena (bridge.Arena): its state and topology are copied into the
-arena's packed buffers, where it stays resident until its last frame.  Every tick
+one is given, while the arena's predicted step time stays within a latency target).  A
+session joins the serving arena (bridge.Arena) from an engine that holds its scene
+prepared at rest — topology built by one upload step, then reset to the rest state
+(xpbd_reset) — by a device copy of that engine's state and topology into the arena's
+packed buffers, where it stays resident until its last frame.  Sessions whose scene
+comes from a ScenePool share the pool scene's prepared engine (its topology is built
+once); others are prepared by an admission thread on an engine of their own, beside
+the GPU work of the resident sessions.  Every tick
 advances every resident session by one frame with ONE library call — one launch
 sequence (one CUDA-graph replay) per substep covers all of them, whatever their sizes —
 carrying every session's collider poses and pin targets.  A step's latency is the time
 from when it became pending (the session joined, or its previous step finished) to
 when its results are ready.
 
-The plain form for comparison steps one session at a time, start to finish, each on an
-engine of its own.
+The plain form for comparison steps one session at a time, start to finish, on the
+same prepared engines (reset to rest before each session).
 """
 import collections
 import math
@@ -68,6 +71,8 @@ class Session:
         self.n = n
         self.scen = None
         self.solver = None
+        self.pool_index = None
+        self.src, self.own = None, False   # the engine it joins the arena from; closed after if own
         self.slot = -1
         self.final = None
         self.pending_since = None
@@ -81,7 +86,8 @@ class Session:
         radii = tuple(float(r) for r in rng.uniform(0.3, 1.5, 3))
         if pool:
             sizes = np.array([p["pos"].shape[0] for p in pool], np.float64)
-            sc = pool[int(np.argmin(np.abs(np.log(sizes) - math.log(self.n))))]
+            self.pool_index = int(np.argmin(np.abs(np.log(sizes) - math.log(self.n))))
+            sc = pool[self.pool_index]
             self.n = sc["pos"].shape[0]
             radii = tuple(float(v) for v in np.abs(sc["pos"]).max(0))
         else:
@@ -95,12 +101,22 @@ class Session:
         sc = self.scen
         return scenes.Scenario(sc.scene, sc.grippers, substeps=self.substeps, iters=self.iters)
 
+    def source(self, lib_path, pool=None):
+        """The engine the session joins the arena from: the pool scene's shared prepared
+        engine, or (no ScenePool) one of its own, prepared here."""
+        if self.scen is None:
+            self.prepare(pool)
+        if isinstance(pool, ScenePool) and self.pool_index is not None:
+            return pool.prepared(self.pool_index, lib_path)
+        self.admit(lib_path)
+        return self.solver
+
     def admit(self, lib_path, pool=None):
+        """An engine of the session's own with its scene prepared at rest."""
         if self.scen is None:
             self.prepare(pool)
         self.solver = bridge.XPBD(lib_path, instance=True)
-        self.scen.setup(self.solver)
-        self.scen.advance(self.solver, 1)          # upload + topology build (first substep)
+        prepare_at_rest(self.solver, self.scen)
 
     def enqueue_frame(self):
         """The next frame's substeps, with their collider poses and pin targets, in one call."""
@@ -142,10 +158,51 @@ def partition_sessions(sessions, ranks):
     return [sorted(b) for b in bins]
 
 
+class ScenePool(list):
+    """Scenes standing in for request payloads (a list of scene dicts), each with an engine
+    that holds it prepared at rest, built on first use (`prepared`) or all at once
+    (`prepare_all`): create, the session settings, one upload step, reset."""
+
+    def __init__(self, items, substeps=10, iters=4):
+        super().__init__(items)
+        self.substeps, self.iters = substeps, iters
+        self.engines = {}
+
+    def index_for(self, n):
+        sizes = np.array([p["pos"].shape[0] for p in self], np.float64)
+        return int(np.argmin(np.abs(np.log(sizes) - math.log(n))))
+
+    def prepared(self, k, lib_path):
+        eng = self.engines.get(k)
+        if eng is None:
+            eng = bridge.XPBD(lib_path, instance=True)
+            prepare_at_rest(eng, scenes.Scenario(self[k], [], substeps=self.substeps, iters=self.iters))
+            self.engines[k] = eng
+        return eng
+
+    def prepare_all(self, lib_path):
+        for k in range(len(self)):
+            self.prepared(k, lib_path)
+
+    def close(self):
+        for eng in self.engines.values():
+            eng.close()
+        self.engines = {}
+
+
+def prepare_at_rest(solver, scen):
+    """Settings of `scen` on `solver`, its scene uploaded and the topology built by one
+    step, then the state reset to rest (positions, velocities, multipliers)."""
+    scen.setup(solver)
+    solver.step()
+    solver.reset()
+    scen.k = 0
+
+
 def scene_pool(n_min, n_max, count=12, seed=0):
     """`count` scenes with log-spaced sizes in [n_min, n_max] (the config-0 distribution)."""
     sizes = np.exp(np.linspace(math.log(n_min), math.log(n_max), count))
-    return [scenes.make_scene(int(round(n)), seed + k) for k, n in enumerate(sizes)]
+    return ScenePool([scenes.make_scene(int(round(n)), seed + k) for k, n in enumerate(sizes)])
 
 
 def _frame_arrays(resident, substeps):
@@ -166,9 +223,12 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
     continuous batching in one arena.  Admission in arrival order while the session fits
     the budget and — with `latency_target_ms` — while the resident Gaussians, at the
     throughput measured so far, keep a tick within the target.  Sessions given as tuples
-    are prepared when admitted (from `pool` when given).  Returns stats."""
+    are prepared when admitted (from `pool` when given).  With a ScenePool a session
+    joins straight from its pool scene's prepared engine; otherwise the admission thread
+    prepares an engine of its own first.  Returns stats."""
     t0 = time.perf_counter()
     arena = bridge.Arena(lib_path, *arena_capacity(budget_bytes))
+    shared = isinstance(pool, ScenePool)
     arrivals = collections.deque(sessions)
     ready = queue.Queue()
     stop = threading.Event()
@@ -182,7 +242,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             except queue.Empty:
                 continue
             try:
-                sess.admit(lib_path, pool)
+                sess.src, sess.own = sess.source(lib_path, pool), True
             except Exception as e:   # surfaced by the serving loop
                 errors.append(e)
             ready.put(sess)
@@ -224,19 +284,28 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                         break
                 resident_bytes += need
                 resident_gauss += s.n
-                backlog.put(waiting.popleft())
+                s = waiting.popleft()
                 queued += 1
+                if shared:
+                    if s.scen is None:
+                        s.prepare(pool)
+                    s.src, s.own = s.source(lib_path, pool), False
+                    ready.put(s)
+                else:
+                    backlog.put(s)
             while not ready.empty():
                 joining.append(ready.get())
             still_joining = []
             for s in joining:
-                slot = arena.admit(s.solver)
+                slot = arena.admit(s.src)
                 if slot is None:          # full until sessions leave (compaction ran already)
                     still_joining.append(s)
                     continue
                 s.slot = slot
-                s.solver.close()          # the arena holds the session's state now
-                s.solver = None
+                if s.own:                 # the arena holds the session's state now
+                    s.src.close()
+                    s.solver = None
+                s.src = None
                 s.pending_since = time.perf_counter()
                 waits.append(s.pending_since - t0 - s.arrival)
                 resident.append(s)
@@ -290,26 +359,40 @@ def _arrival(item):
 
 
 def run_plain(lib_path, sessions, max_wall=None, pool=None):
-    """One session at a time, start to finish, on one engine (no overlap)."""
+    """One session at a time, start to finish (no overlap): on its pool scene's prepared
+    engine, reset to rest before and after, with a ScenePool; else on an engine of its
+    own."""
     t0 = time.perf_counter()
     work, lats, count = 0, [], 0
+    shared = isinstance(pool, ScenePool)
     for k, item in enumerate(sessions):
         if max_wall and time.perf_counter() - t0 > max_wall:
             break
         if isinstance(item, Session):
             s = Session(item.sid, item.arrival, item.n, item.frames_total, item.seed)
             s.scen = item.fresh_scenario()
+            s.pool_index = item.pool_index
         else:
             a, n, frames, seed = item
             s = Session(k, a, n, frames, seed)
-        s.admit(lib_path, pool)
+        if shared:
+            if s.scen is None:
+                s.prepare(pool)
+            s.solver = pool.prepared(s.pool_index, lib_path)
+            s.solver.reset()
+        else:
+            s.admit(lib_path, pool)
         while s.frames_left > 0:
             t1 = time.perf_counter()
             s.enqueue_frame()
             s.solver.lib.xpbd_b200_sync()
             lats.append(time.perf_counter() - t1)
             work += s.n * s.scen.substeps
-        s.close()
+        if shared:
+            s.solver.reset()
+            s.solver = None
+        else:
+            s.close()
         count += 1
     wall = time.perf_counter() - t0
     lat = np.asarray(lats) if lats else np.zeros(1)

@@ -62,6 +62,30 @@ def test_served_sessions_match_alone():
         alone.close(keep_result=False)
 
 
+def test_served_from_scene_pool_matches_alone():
+    """Sessions whose scenes come from a ScenePool join the arena from the pool scene's
+    shared prepared engine (two of them from the same one); each session's positions
+    equal those of its scene prepared on an engine of its own and stepped alone; the
+    plain loop runs the same sessions on the shared engines."""
+    pool = serve.scene_pool(2000, 6000, count=2)
+    sessions = [(0.0, 2000, 3, 11), (0.0, 6000, 2, 12), (0.005, 2100, 2, 13)]
+    stats = serve.run_served(H.B200_SO, sessions, budget_bytes=1e12, pool=pool)
+    assert stats["sessions"] == 3 and stats["steps"] == 7
+    done = {s.sid: s for s in stats["sessions_done"]}
+    for k, (a, n, frames, seed) in enumerate(sessions):
+        alone = serve.Session(k, a, n, frames, seed)
+        alone.prepare(pool)
+        alone.admit(H.B200_SO)
+        while alone.frames_left > 0:
+            alone.enqueue_frame()
+        alone.solver.lib.xpbd_b200_sync()
+        np.testing.assert_array_equal(alone.solver.positions(), done[k].final)
+        alone.close(keep_result=False)
+    plain = serve.run_plain(H.B200_SO, sessions, pool=pool)
+    assert plain["sessions"] == 3 and plain["steps"] == 7
+    pool.close()
+
+
 def test_arena_retire_and_compaction_match_alone():
     """Sessions join a small arena, one in the middle retires, a new one only fits after
     the live sessions are moved down over the hole (compaction); every session's
