@@ -100,47 +100,6 @@ struct DBuf {
 	size_t bytes() const { return sizeof(T) * n; }
 };
 
-// Per-tile unions for the staged volume kernels: rows [t * tile, (t + 1) * tile) of a
-// CSR list form tile t; its entries' sorted unique valid values go to t_ids (tile t at
-// [t_off[t], t_off[t + 1])) and every entry becomes its 16-bit slot in that union
-// (0xffff for an invalid entry).  Returns the largest union, or -1 when one exceeds cap.
-static int build_tile_slots(int n, int tile, const std::vector<int>& off, const std::vector<int>& idx, int cap,
-	std::vector<int>& t_off, std::vector<int>& t_ids, std::vector<unsigned short>& slot)
-{
-	const int tiles = (n + tile - 1) / tile;
-	std::vector<std::vector<int>> uni(tiles);
-	std::atomic<int> too_big{ 0 };
-	slot.assign(idx.size(), 0xffffu);
-	parallel_for(tiles, [&](int t0, int t1) {
-		std::vector<int> u;
-		for (int t = t0; t < t1; ++t) {
-			const int r0 = t * tile, r1 = std::min(n, r0 + tile);
-			u.clear();
-			for (int k = off[r0]; k < off[r1]; ++k)
-				if (idx[k] >= 0 && idx[k] < n) u.push_back(idx[k]);
-			std::sort(u.begin(), u.end());
-			u.erase(std::unique(u.begin(), u.end()), u.end());
-			if ((int)u.size() > cap) { too_big = 1; continue; }
-			for (int k = off[r0]; k < off[r1]; ++k)
-				if (idx[k] >= 0 && idx[k] < n)
-					slot[k] = (unsigned short)(std::lower_bound(u.begin(), u.end(), idx[k]) - u.begin());
-			uni[t] = u;
-		}
-	});
-	if (too_big) return -1;
-	t_off.assign(tiles + 1, 0);
-	int max_u = 0;
-	for (int t = 0; t < tiles; ++t) {
-		t_off[t + 1] = t_off[t] + (int)uni[t].size();
-		max_u = std::max(max_u, (int)uni[t].size());
-	}
-	t_ids.resize(t_off[tiles]);
-	parallel_for(tiles, [&](int t0, int t1) {
-		for (int t = t0; t < t1; ++t) std::copy(uni[t].begin(), uni[t].end(), t_ids.begin() + t_off[t]);
-	});
-	return max_u;
-}
-
 // Solver settings.  Like the reference's file-static settings (forward.cu:53-92,
 // 224-265, 300-361) they outlive create/destroy; defaults are the reference's.
 struct Settings {
@@ -177,7 +136,6 @@ struct Settings {
 	bool press_autolog = true;       // press harness: settle at 25/50/75/100 % (forward.cu:565)
 	int fused = 0;                   // substep as one cooperative launch: 0 never, 1 always, 2 the faster (timed)
 	int sc_near = 1;                 // one-object scenes: candidate lists from the near-pair grid
-	int vol_tiled = 1;               // 4-lane volume kernels on staged per-tile unions (when built)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -296,10 +254,6 @@ public:
 	DBuf<float> ndist, nstiff, lam;
 	DBuf<int> vol_off, vol_idx, rev_off, rev_idx, mat_type, vol_gs_order;
 	DBuf<int> vol_idx_s, rev_idx_s;  // the same lists, rows sorted along the Morton curve
-	// staged volume kernels: per-tile unions and 16-bit slots of the sorted lists
-	DBuf<unsigned short> vol_slot, rev_slot;
-	DBuf<int> vt_off, vt_ids, rt_off, rt_ids;
-	int vt_max = 0, rt_max = 0;      // largest union (0: not built)
 	DBuf<float> det_rest, v_rest, rest_len, sigma_rest, lam_vol;
 	DBuf<float4> rec;
 	DBuf<int2> gs_edge;
@@ -497,8 +451,6 @@ public:
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
 		vol_idx_s.release(); rev_idx_s.release();
-		vol_slot.release(); rev_slot.release(); vt_off.release(); vt_ids.release(); rt_off.release(); rt_ids.release();
-		vt_max = rt_max = 0;
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
@@ -780,7 +732,6 @@ public:
 			CK(cudaMemcpyAsync(rev_idx_s.p, rs.data(), sizeof(int) * rs.size(), cudaMemcpyHostToDevice, stream));
 			CK(cudaStreamSynchronize(stream));
 			build_mark(5);
-			if (build_tiles(voff_i, vs, roff_i, rs)) return -1;
 		}
 		vol_gs_order.release();
 		std::vector<int> order_i(clusters.gs_order.size());
@@ -1195,7 +1146,7 @@ public:
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
 			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground(),
-			selfcol_on() && sc_near_on(), solve_tiled(), gather_tiled() };
+			selfcol_on() && sc_near_on() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -1209,22 +1160,6 @@ public:
 			cudaEventRecord(a, stream);
 		}
 		kernel<<<grid, block, 0, stream>>>(args...);
-		++launches;
-		if (profiling) {
-			cudaEventRecord(b, stream);
-			prof_records.push_back({ stage, a, b });
-		}
-	}
-	template <typename K, typename... A>
-	void launch_smem(int stage, dim3 grid, dim3 block, size_t smem, K kernel, A... args)
-	{
-		cudaEvent_t a = nullptr, b = nullptr;
-		if (profiling) {
-			a = next_event();
-			b = next_event();
-			cudaEventRecord(a, stream);
-		}
-		kernel<<<grid, block, smem, stream>>>(args...);
 		++launches;
 		if (profiling) {
 			cudaEventRecord(b, stream);
@@ -1246,41 +1181,6 @@ public:
 	}
 
 	bool sc_near_on() const { return S.sc_near && single_object; }
-
-	// the staged volume kernels' tile unions (at most kTileSolveCap positions / kTileGatherCap
-	// records per tile: 64 KB / 72 KB of shared memory); not built where a tile exceeds them
-	static constexpr int kTileSolveCap = 4096, kTileGatherCap = 2048;
-	int build_tiles(const std::vector<int>& voff_i, const std::vector<int>& vs, const std::vector<int>& roff_i,
-		const std::vector<int>& rs)
-	{
-		vt_max = rt_max = 0;
-		std::vector<int> t_off, t_ids;
-		std::vector<unsigned short> slot;
-		const int vm = build_tile_slots(n, dev::kTileItems, voff_i, vs, kTileSolveCap, t_off, t_ids, slot);
-		if (vm > 0) {
-			CK(vol_slot.alloc(slot.size())); CK(vt_off.alloc(t_off.size())); CK(vt_ids.alloc(t_ids.size()));
-			CK(cudaMemcpy(vol_slot.p, slot.data(), sizeof(unsigned short) * slot.size(), cudaMemcpyHostToDevice));
-			CK(cudaMemcpy(vt_off.p, t_off.data(), sizeof(int) * t_off.size(), cudaMemcpyHostToDevice));
-			CK(cudaMemcpy(vt_ids.p, t_ids.data(), sizeof(int) * t_ids.size(), cudaMemcpyHostToDevice));
-			CK(cudaFuncSetAttribute(dev::k_volume_solve_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				(int)(sizeof(float4) * vm)));
-			vt_max = vm;
-		}
-		const int rm = build_tile_slots(n, dev::kTileItems, roff_i, rs, kTileGatherCap, t_off, t_ids, slot);
-		if (rm > 0) {
-			CK(rev_slot.alloc(slot.size())); CK(rt_off.alloc(t_off.size())); CK(rt_ids.alloc(t_ids.size()));
-			CK(cudaMemcpy(rev_slot.p, slot.data(), sizeof(unsigned short) * slot.size(), cudaMemcpyHostToDevice));
-			CK(cudaMemcpy(rt_off.p, t_off.data(), sizeof(int) * t_off.size(), cudaMemcpyHostToDevice));
-			CK(cudaMemcpy(rt_ids.p, t_ids.data(), sizeof(int) * t_ids.size(), cudaMemcpyHostToDevice));
-			CK(cudaFuncSetAttribute(dev::k_volume_gather_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				(int)gather_tile_smem(rm)));
-			rt_max = rm;
-		}
-		return 0;
-	}
-	static size_t gather_tile_smem(int max_u) { return sizeof(float4) * 2 * (size_t)max_u + sizeof(float) * (size_t)max_u; }
-	bool solve_tiled() const { return S.vol_tiled && vt_max > 0 && !arena; }
-	bool gather_tiled() const { return S.vol_tiled && rt_max > 0 && !arena; }
 
 	// The once-per-step self-collision build (selfColBuild, forward.cu:11796-11849): cell
 	// size from the largest predicted displacement, then the candidate lists.  One-object
@@ -1472,12 +1372,7 @@ public:
 					const int rl = first ? 0 : 1;
 					const StepParams* dp = d_params;
 					const float4* cpin = pin;
-					if (la == 4 && S.lanes_a == 0 && occ == 0 && solve_tiled())
-						launch_smem(ST_VOL_SOLVE, blocks_for((long long)N * 4), B, sizeof(float4) * vt_max,
-							dev::k_volume_solve_tiled, N, dp, cpin, (const int*)vol_off.p, (const unsigned short*)vol_slot.p,
-							(const int*)vt_off.p, (const int*)vt_ids.p, (const float*)det_rest.p, (const int*)mat_type.p,
-							lam_vol.p, rec.p, recz(), rl);
-					else if (la == 4 && S.lanes_a == 0)
+					if (la == 4 && S.lanes_a == 0)
 						// automatic: one pass over the members (any count), 4 lanes per cluster
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
@@ -1513,11 +1408,6 @@ public:
 					else if (lb == 8)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
-					else if (lb == 4 && occ == 0 && gather_tiled())
-						launch_smem(ST_VOL_GATHER, blocks_for((long long)N * 4), B, gather_tile_smem(rt_max),
-							dev::k_volume_gather_tiled, N, dp, cpin, pout, (const int*)rev_off.p,
-							(const unsigned short*)rev_slot.p, (const int*)rt_off.p, (const int*)rt_ids.p, rt_max,
-							(const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
@@ -2972,7 +2862,6 @@ XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled 
 
 XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std::min(2, mode)); }
 XPBD_API void xpbd_b200_set_selfcol_near(int enabled) { engine().S.sc_near = enabled ? 1 : 0; }
-XPBD_API void xpbd_b200_set_volume_tiled(int enabled) { engine().S.vol_tiled = enabled ? 1 : 0; }
 
 XPBD_API int xpbd_b200_tuning(float* out)
 {
@@ -3037,9 +2926,8 @@ XPBD_API long long xpbd_b200_launch_count(void) { return cur_engine()->launches;
 XPBD_API int xpbd_b200_sizes(long long* out)
 {
 	// [0] N, [1] directed edges, [2] cluster members, [3] reverse entries, [4] GS edges,
-	// [5] GS edge colours, [6] GS clusters, [7] GS cluster colours, [8] hash table, [9] candidates,
-	// [10] / [11] the staged volume solve's / gather's largest tile union (0: not built)
-	for (int k = 0; k < 12; ++k) out[k] = 0;
+	// [5] GS edge colours, [6] GS clusters, [7] GS cluster colours, [8] hash table, [9] candidates
+	for (int k = 0; k < 10; ++k) out[k] = 0;
 	if (!cur_engine()->built) return -1;
 	Engine& E = *cur_engine();
 	out[0] = E.n;
@@ -3052,8 +2940,6 @@ XPBD_API int xpbd_b200_sizes(long long* out)
 	out[7] = E.clusters.gs_color_off.empty() ? 0 : (long long)E.clusters.gs_color_off.size() - 1;
 	out[8] = E.sc_table;
 	if (E.sc_table && !E.read_counters()) out[9] = E.h_ctr->sc_contacts;
-	out[10] = E.vt_max;
-	out[11] = E.rt_max;
 	return 0;
 }
 

@@ -864,20 +864,12 @@ __global__ void __launch_bounds__(kSmemBlock) k_volume_solve_smem(int n, const S
 // cancellation in the moment form small; the result equals the two-pass form
 // (forward.cu:8531-8664) to FP32 rounding.  The reference has the same leader-relative
 // moments in its optional one-pass warp kernel (forward.cu:8864-9033, warp mode 3).
-// Staged forms (IdxT = unsigned short): the member list holds slots into the block's
-// staged copy `stage` of the positions its clusters read (kTileNone = no member), in the
-// same order as the global list; everything else is the same code.
-constexpr unsigned short kTileNone = 0xffffu;
-
-template <int S, bool NC, typename IdxT = int>
+template <int S, bool NC>
 __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const StepParams* __restrict__ P,
-	const float4* __restrict__ pin, const int* __restrict__ voff, const IdxT* __restrict__ vidx,
+	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
-	float4* __restrict__ rec, float* __restrict__ recz, int read_lam, const float4* stage = nullptr)
+	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	constexpr bool kStaged = sizeof(IdxT) == 2;
-	auto member_ok = [&](int j) { return kStaged ? j != (int)kTileNone : (j >= 0 && j < n); };
-	auto member = [&](int j) { return kStaged ? stage[j] : ldv<NC>(pin, j); };
 	const int sl = (int)(gtid & (S - 1));
 	const int idx = (int)(gtid / S);
 	const bool in_range = idx < n;
@@ -905,17 +897,17 @@ __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const 
 	};
 	int k = sl;
 	for (; k + S < cnt; k += 2 * S) {
-		const int j0 = (int)__ldg(vidx + off + k), j1 = (int)__ldg(vidx + off + k + S);
-		const bool ok0 = member_ok(j0), ok1 = member_ok(j1);
+		const int j0 = __ldg(vidx + off + k), j1 = __ldg(vidx + off + k + S);
+		const bool ok0 = j0 >= 0 && j0 < n, ok1 = j1 >= 0 && j1 < n;
 		float4 q0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), q1 = q0;
-		if (ok0) q0 = member(j0);
-		if (ok1) q1 = member(j1);
+		if (ok0) q0 = ldv<NC>(pin, j0);
+		if (ok1) q1 = ldv<NC>(pin, j1);
 		if (ok0) add(q0);
 		if (ok1) add(q1);
 	}
 	if (k < cnt) {
-		const int j = (int)__ldg(vidx + off + k);
-		if (member_ok(j)) add(member(j));
+		const int j = __ldg(vidx + off + k);
+		if (j >= 0 && j < n) add(ldv<NC>(pin, j));
 	}
 #pragma unroll
 	for (int t = 0; t < 20; ++t) m[t] = group_sum<S>(m[t]);
@@ -1092,17 +1084,12 @@ __device__ __forceinline__ float3 gather_finish(float3 pi, float3 avg, float rl,
 // Kernel B on groups of S lanes per node (forward.cu:9262-9323 with S = 32): mean over
 // the clusters that contain the node, step clamp 0.25 restLen, under-relaxation.  Reads
 // per node: h reverse indices + h gathered 36-byte records (L2-resident).
-// Staged forms (IdxT = unsigned short): the reverse list holds slots into the block's
-// staged copies of the records (sa, sb: the two float4 halves, sz: c.z).
-template <int S, bool NC, typename IdxT = int>
+template <int S, bool NC>
 __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
-	const IdxT* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
-	const float* __restrict__ rest_len, const float4* st_a = nullptr, const float4* st_b = nullptr,
-	const float* st_z = nullptr)
+	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
+	const float* __restrict__ rest_len)
 {
-	constexpr bool kStaged = sizeof(IdxT) == 2;
-	auto rec_ok = [&](int i) { return kStaged ? i != (int)kTileNone : (i >= 0 && i < n); };
 	const int sl = (int)(gtid & (S - 1));
 	const int idx = (int)(gtid / S);
 	const bool in_range = idx < n;
@@ -1125,35 +1112,23 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	// the one-at-a-time loop, so the sum is the same bit for bit
 	int k = sl;
 	for (; k + S < cnt; k += 2 * S) {
-		const int i0 = (int)__ldg(ridx + off + k), i1 = (int)__ldg(ridx + off + k + S);
-		const bool ok0 = rec_ok(i0), ok1 = rec_ok(i1);
+		const int i0 = __ldg(ridx + off + k), i1 = __ldg(ridx + off + k + S);
+		const bool ok0 = i0 >= 0 && i0 < n, ok1 = i1 >= 0 && i1 < n;
 		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
 		float z0 = 0.0f, z1 = 0.0f;
 		const float* cz = recz;
-		if constexpr (kStaged) {
-			if (ok0) { a0 = st_a[i0]; b0 = st_b[i0]; z0 = st_z[i0]; }
-			if (ok1) { a1 = st_a[i1]; b1 = st_b[i1]; z1 = st_z[i1]; }
-		}
-		else {
-			if (ok0) { a0 = ldv<NC>(rec, rec_a(i0)); b0 = ldv<NC>(rec, rec_b(i0)); z0 = ldv<NC>(cz, i0); }
-			if (ok1) { a1 = ldv<NC>(rec, rec_a(i1)); b1 = ldv<NC>(rec, rec_b(i1)); z1 = ldv<NC>(cz, i1); }
-		}
+		if (ok0) { a0 = ldv<NC>(rec, rec_a(i0)); b0 = ldv<NC>(rec, rec_b(i0)); z0 = ldv<NC>(cz, i0); }
+		if (ok1) { a1 = ldv<NC>(rec, rec_a(i1)); b1 = ldv<NC>(rec, rec_b(i1)); z1 = ldv<NC>(cz, i1); }
 		float3 dp;
 		if (ok0 && gather_rec(a0, b0, z0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 		if (ok1 && gather_rec(a1, b1, z1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 	}
 	if (k < cnt) {
-		const int i = (int)__ldg(ridx + off + k);
+		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (rec_ok(i)) {
-			float4 a, b;
-			float z;
-			if constexpr (kStaged) { a = st_a[i]; b = st_b[i]; z = st_z[i]; }
-			else { a = ldv<NC>(rec, rec_a(i)); b = ldv<NC>(rec, rec_b(i)); z = ldv<NC>(recz, i); }
-			if (gather_rec(a, b, z, pi, wi, dp)) {
-				sum = add3(sum, dp);
-				++received;
-			}
+		if (i >= 0 && i < n && gather_rec(ldv<NC>(rec, rec_a(i)), ldv<NC>(rec, rec_b(i)), ldv<NC>(recz, i), pi, wi, dp)) {
+			sum = add3(sum, dp);
+			++received;
 		}
 	}
 	const float sx = group_sum<S>(sum.x), sy = group_sum<S>(sum.y), sz = group_sum<S>(sum.z);
@@ -1187,50 +1162,6 @@ __global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int n, const
 {
 	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff, ridx, rec,
 		recz, rest_len);
-}
-
-// Staged (tiled) volume kernels.  Block b owns the kTileItems clusters / nodes
-// [64 b, 64 b + 64) (4 lanes each, as the group kernels); at upload, the sorted union of
-// the Gaussians its clusters read (solve) or of the clusters its nodes read (gather) is
-// listed per tile (tile_off / tile_ids) and every list entry replaced by its 16-bit slot
-// in that union.  The block first copies the union's positions / records into shared
-// memory (about 6x fewer global loads: Morton-neighbouring rows share most entries),
-// then runs the group kernels' code on the copies, in the same order: identical results.
-constexpr int kTileItems = kBlock / 4;
-
-__global__ void __launch_bounds__(kBlock) k_volume_solve_tiled(int n, const StepParams* __restrict__ P,
-	const float4* __restrict__ pin, const int* __restrict__ voff, const unsigned short* __restrict__ vslot,
-	const int* __restrict__ tile_off, const int* __restrict__ tile_ids, const float* __restrict__ det_rest,
-	const int* __restrict__ mat_type, float* __restrict__ lam_vol, float4* __restrict__ rec, float* __restrict__ recz,
-	int read_lam)
-{
-	extern __shared__ float4 tile_pos[];
-	const int u0 = tile_off[blockIdx.x], nu = tile_off[blockIdx.x + 1] - u0;
-	for (int u = threadIdx.x; u < nu; u += blockDim.x) tile_pos[u] = ldv<true>(pin, tile_ids[u0 + u]);
-	__syncthreads();
-	solve_onepass_lane<4, true, unsigned short>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff,
-		vslot, det_rest, mat_type, lam_vol, rec, recz, read_lam, tile_pos);
-}
-
-__global__ void __launch_bounds__(kBlock) k_volume_gather_tiled(int n, const StepParams* __restrict__ P,
-	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
-	const unsigned short* __restrict__ rslot, const int* __restrict__ tile_off, const int* __restrict__ tile_ids,
-	int max_union, const float4* __restrict__ rec, const float* __restrict__ recz, const float* __restrict__ rest_len)
-{
-	extern __shared__ float4 tile_rec[];
-	float4* sa = tile_rec;
-	float4* sb = tile_rec + max_union;
-	float* sz = reinterpret_cast<float*>(tile_rec + 2 * max_union);
-	const int u0 = tile_off[blockIdx.x], nu = tile_off[blockIdx.x + 1] - u0;
-	for (int u = threadIdx.x; u < nu; u += blockDim.x) {
-		const int c = tile_ids[u0 + u];
-		sa[u] = ldv<true>(rec, rec_a(c));
-		sb[u] = ldv<true>(rec, rec_b(c));
-		sz[u] = ldv<true>(recz, c);
-	}
-	__syncthreads();
-	gather_group_lane<4, true, unsigned short>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff,
-		rslot, rec, recz, rest_len, sa, sb, sz);
 }
 
 // Kernel B, one thread per node (forward.cu:9187-9243)

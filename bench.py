@@ -227,7 +227,7 @@ def bench_b200(args, rank, world):
     with torch.cuda.stream(stream):
         run_frames(x, scen, args.warmup, blocking=False)
         torch.cuda.synchronize()
-        sizes = np.zeros(12, np.int64)
+        sizes = np.zeros(10, np.int64)
         x.lib.xpbd_b200_sizes(sizes.ctypes.data)
 
         # ---- timed region: device-resident throughput, one CUDA-graph replay per substep ----
@@ -296,8 +296,6 @@ def bench_b200(args, rank, world):
         "config": {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": scen.iters,
                    "graph_edges_directed": int(sizes[1]), "cluster_members": int(sizes[2]),
                    "hash_table": int(sizes[8]), "parallelism": f"replicas x{world}",
-                   "volume_tiles": {"solve_max_union": int(sizes[10]), "gather_max_union": int(sizes[11]),
-                                    "nodes_per_tile": 64},
                    "l2": "inputs larger than L2 (working set > 2 GB per replica)"},
         "e2e": {"value": n * SUBSTEPS * e2e_frames * world / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": pos_bytes, "frames": e2e_frames},
@@ -529,7 +527,7 @@ def bench_chainmail(args, rank, world):
     ev3.record(stream)
     torch.cuda.synchronize()
     relax_ms = ev2.elapsed_time(ev3) / r
-    sizes = np.zeros(12, np.int64)
+    sizes = np.zeros(10, np.int64)
     L.xpbd_b200_sizes(sizes.ctypes.data)
     d = sizes[1] / n
     relax_bytes = (44 + 12 * d) * n          # pos in/out, (time, density), row offsets; nbr, rest, stiffness per edge

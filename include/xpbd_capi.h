@@ -226,10 +226,6 @@ XPBD_API int xpbd_b200_tuning(float* out);
  * visiting order; 0 from the reference's own 27-cell scan of the start-position hash
  * (selfColBuildKernel).  The lists are identical either way. */
 XPBD_API void xpbd_b200_set_selfcol_near(int enabled);
-/* 4-lane volume solve and gather: 1 (default) on per-tile unions staged in shared memory
- * with 16-bit local indices (built at upload where every tile's union fits), 0 on the
- * global lists.  Same results either way. */
-XPBD_API void xpbd_b200_set_volume_tiled(int enabled);
 /* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
  * ABI; results identical); 0: caller order.  Takes effect at the next upload. */
 XPBD_API void xpbd_b200_set_reorder(int enabled);
@@ -241,9 +237,8 @@ XPBD_API void xpbd_b200_reset_stage_times(void);
 XPBD_API const char* xpbd_b200_stage_name(int stage);
 /* Kernels launched by the engine since load (graph replays count every kernel node). */
 XPBD_API long long xpbd_b200_launch_count(void);
-/* Topology sizes after the first step (out[12]): N, edges, cluster members, reverse
- * entries, GS edges, GS edge colours, GS clusters, GS cluster colours, hash table,
- * candidates, the staged volume solve's and gather's largest tile union (0: not built). */
+/* Topology sizes after the first step: N, edges, cluster members, reverse entries, GS
+ * edges, GS edge colours, GS clusters, GS cluster colours, hash table, candidates. */
 XPBD_API int xpbd_b200_sizes(long long* out);
 /* Stage buffers by name, for parity checks (count only when out is NULL). */
 XPBD_API int xpbd_b200_debug_int(const char* name, int* out, long long cap);

@@ -518,25 +518,6 @@ def test_selfcol_near_grid_matches_cell_scan(lib):
     np.testing.assert_array_equal(pos[1], pos[0])
 
 
-def test_volume_tiled_matches_global_lists(lib):
-    """The staged volume kernels (per-tile unions in shared memory, 16-bit local indices)
-    give the global-list kernels' positions bit for bit: the large scene's settings
-    (64-member clusters, self-collision, grippers) and the runtime's (2048-member cap,
-    leader spacing 2, object shape keeping, contacts, ground)."""
-    sc = H.scenes.make_scene(40000, 2)
-    g = H.load_golden("runtime_n4000")
-    for make in (lambda: H.scenes.large_scene_scenario(scene=sc), lambda: H.runtime_scenario(g)):
-        pos = {}
-        for tiled in (1, 0):
-            lib.lib.xpbd_b200_set_volume_tiled(tiled)
-            s = make()
-            s.setup(lib)
-            s.advance(lib, 3)
-            pos[tiled] = lib.positions()
-        lib.lib.xpbd_b200_set_volume_tiled(1)
-        np.testing.assert_array_equal(pos[1], pos[0])
-
-
 def test_large_scene_1m_against_oracle(lib):
     """The 1,000,000-Gaussian large scene at the bench's settings (8-NN graph, 64-member
     clusters of 3-ring candidates, shape matching, self-collision within the body, two
