@@ -2020,6 +2020,49 @@ __device__ __forceinline__ int sc_cell(float v, float inv_cell)
 	return (int)floorf(fminf(fmaxf(v * inv_cell, -1.0e9f), 1.0e9f));
 }
 
+// The hashes of the 27 cells around (cx, cy, cz) in the reference's order kc = 9 (dz + 1)
+// + 3 (dy + 1) + (dx + 1): sc_hash(cx + dx, cy + dy, cz + dz) = ((cx P1 + dx P1) ^ ...)
+// in 32-bit wrap-around arithmetic, so the per-axis products are formed once and a cell
+// costs three multiply-adds, two XORs and the mask (kc decoded without division).
+struct Hash27 {
+	unsigned int bx, by, bz, mask;
+	__device__ __forceinline__ Hash27(int cx, int cy, int cz, unsigned int m)
+		: bx((unsigned int)cx * 73856093u), by((unsigned int)cy * 19349663u), bz((unsigned int)cz * 83492791u),
+		  mask(m)
+	{
+	}
+	__device__ __forceinline__ unsigned int operator()(int kc) const
+	{
+		const int q = (kc * 11) >> 5;   // kc / 3 for kc < 27
+		const int iz = (kc * 57) >> 9;  // kc / 9
+		const int ix = kc - 3 * q, iy = q - 3 * iz;
+		return ((bx + (unsigned int)(ix - 1) * 73856093u) ^ (by + (unsigned int)(iy - 1) * 19349663u) ^
+			(bz + (unsigned int)(iz - 1) * 83492791u)) & mask;
+	}
+};
+
+// bit kc set for the cells whose hash repeats no earlier cell's (the reference visits a
+// bucket once, forward.cu:7116-7123); a 64-bit filter on the low hash bits settles
+// almost every test without comparing, the rest compare with the earlier hashes
+__device__ __forceinline__ unsigned int hash27_unique(const Hash27& H)
+{
+	unsigned int use = 0u;
+	unsigned long long seen = 0ull;
+#pragma unroll
+	for (int kc = 0; kc < 27; ++kc) {
+		const unsigned int h = H(kc);
+		const unsigned long long bit = 1ull << (h & 63u);
+		if (seen & bit) {
+			bool dup = false;
+			for (int m = 0; m < kc && !dup; ++m) dup = H(m) == h;
+			if (dup) continue;
+		}
+		seen |= bit;
+		use |= 1u << kc;
+	}
+	return use;
+}
+
 // max predict displacement^2 (selfColDispKernel + DeviceReduce::Max)
 __global__ void __launch_bounds__(kBlock) k_sc_disp(int n, const float4* __restrict__ x, const float4* __restrict__ p,
 	DevCounters* __restrict__ ctr, const unsigned char* __restrict__ active)
@@ -2209,34 +2252,17 @@ __device__ __forceinline__ int sc_build_one(int i, const StepParams* __restrict_
 	const float dix = p.x - x.x, diy = p.y - x.y, diz = p.z - x.z;
 	const int oi = obj_id[i];
 	const float search2 = search * search;
-	const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+	const Hash27 H(sc_cell(x.x, inv_cell), sc_cell(x.y, inv_cell), sc_cell(x.z, inv_cell), mask);
 	int* out = contacts + (size_t)i * kSelfColMax;
 	float prio[kSelfColMax];
 	int tier[kSelfColMax];
-	// a 64-bit filter on the low hash bits settles almost every cell's duplicate test
-	// without comparing; the rest recompute the earlier hashes
-	unsigned int use = 0u;
-	{
-		unsigned long long seen = 0ull;
-		for (int kc = 0; kc < 27; ++kc) {
-			const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
-			const unsigned long long bit = 1ull << (h & 63u);
-			if (seen & bit) {
-				bool dup = false;
-				for (int m = 0; m < kc && !dup; ++m)
-					dup = sc_hash(cx + m % 3 - 1, cy + (m / 3) % 3 - 1, cz + m / 9 - 1, mask) == h;
-				if (dup) continue;
-			}
-			seen |= bit;
-			use |= 1u << kc;
-		}
-	}
+	const unsigned int use = hash27_unique(H);
 	// the used cells in order, the next cell's bucket range loaded while the current
 	// cell's entries are tested
 	int kc = use ? __ffs(use) - 1 : 27;
 	int cs = 0, ce = 0;
 	if (kc < 27) {
-		const unsigned int h = sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask);
+		const unsigned int h = H(kc);
 		cs = start[h];
 		ce = start[h + 1];
 	}
@@ -2245,7 +2271,7 @@ __device__ __forceinline__ int sc_build_one(int i, const StepParams* __restrict_
 		const int kn = later ? __ffs(later) - 1 : 27;
 		int ns = 0, ne = 0;
 		if (kn < 27) {
-			const unsigned int hn = sc_hash(cx + kn % 3 - 1, cy + (kn / 3) % 3 - 1, cz + kn / 9 - 1, mask);
+			const unsigned int hn = H(kn);
 			ns = start[hn];
 			ne = start[hn + 1];
 		}
@@ -2390,13 +2416,13 @@ __global__ void __launch_bounds__(kBlock) k_sc_near_scatter(int n, const unsigne
 
 // the key of accepted neighbour j of particle i: the first of i's 27 start cells
 // (reference order) whose hash is j's bucket, then j's caller index; ~0 = never visited
-__device__ __forceinline__ unsigned long long sc_near_key(int cx, int cy, int cz, float4 xj, float inv_cell,
-	unsigned int mask, unsigned int caller_j)
+__device__ __forceinline__ unsigned long long sc_near_key(const Hash27& Href, float4 xj, float inv_cell,
+	unsigned int caller_j)
 {
-	const unsigned int hj = sc_hash(sc_cell(xj.x, inv_cell), sc_cell(xj.y, inv_cell), sc_cell(xj.z, inv_cell), mask);
+	const unsigned int hj =
+		sc_hash(sc_cell(xj.x, inv_cell), sc_cell(xj.y, inv_cell), sc_cell(xj.z, inv_cell), Href.mask);
 	for (int kc = 0; kc < 27; ++kc)
-		if (sc_hash(cx + kc % 3 - 1, cy + (kc / 3) % 3 - 1, cz + kc / 9 - 1, mask) == hj)
-			return ((unsigned long long)kc << 32) | caller_j;
+		if (Href(kc) == hj) return ((unsigned long long)kc << 32) | caller_j;
 	return ~0ull;
 }
 
@@ -2416,27 +2442,11 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 		const float search2 = search * search;
 		const float inv = sc_near_inv(P);
 		const float4 q = rest[i];
-		const int fx = sc_cell(p.x, inv), fy = sc_cell(p.y, inv), fz = sc_cell(p.z, inv);
-		// the fine cells whose hash does not repeat an earlier one's
-		unsigned int use = 0u;
-		{
-			unsigned long long seen = 0ull;
-			for (int kc = 0; kc < 27; ++kc) {
-				const unsigned int h = sc_hash(fx + kc % 3 - 1, fy + (kc / 3) % 3 - 1, fz + kc / 9 - 1, mask);
-				const unsigned long long bit = 1ull << (h & 63u);
-				if (seen & bit) {
-					bool dup = false;
-					for (int m = 0; m < kc && !dup; ++m)
-						dup = sc_hash(fx + m % 3 - 1, fy + (m / 3) % 3 - 1, fz + m / 9 - 1, mask) == h;
-					if (dup) continue;
-				}
-				seen |= bit;
-				use |= 1u << kc;
-			}
-		}
+		const Hash27 Hf(sc_cell(p.x, inv), sc_cell(p.y, inv), sc_cell(p.z, inv), mask);
+		const unsigned int use = hash27_unique(Hf);   // the fine cells, each bucket once
 		// the particle's own reference cell, for the keys
 		const float inv_cell = ctr->sc_inv_cell;
-		const int cx = sc_cell(x.x, inv_cell), cy = sc_cell(x.y, inv_cell), cz = sc_cell(x.z, inv_cell);
+		const Hash27 Href(sc_cell(x.x, inv_cell), sc_cell(x.y, inv_cell), sc_cell(x.z, inv_cell), mask);
 		int* out = contacts + (size_t)i * kSelfColMax;
 		float prio[kSelfColMax];
 		int tier[kSelfColMax];
@@ -2449,12 +2459,24 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 			int bj[kNearBatch];
 			int nb = 0;
 			bool more = false;
-			unsigned int u = use;
-			while (u) {
-				const int kc = __ffs(u) - 1;
-				u &= u - 1u;
-				const unsigned int h = sc_hash(fx + kc % 3 - 1, fy + (kc / 3) % 3 - 1, fz + kc / 9 - 1, mask);
-				const int cs = start_f[h], ce = start_f[h + 1];
+			// the used fine cells in order, the next one's bucket range loaded while the
+			// current one's entries are tested
+			int kc = use ? __ffs(use) - 1 : 27;
+			int cs = 0, ce = 0;
+			if (kc < 27) {
+				const unsigned int h = Hf(kc);
+				cs = start_f[h];
+				ce = start_f[h + 1];
+			}
+			while (kc < 27) {
+				const unsigned int later = use & ~((2u << kc) - 1u);
+				const int kn = later ? __ffs(later) - 1 : 27;
+				int ns = 0, ne = 0;
+				if (kn < 27) {
+					const unsigned int hn = Hf(kn);
+					ns = start_f[hn];
+					ne = start_f[hn + 1];
+				}
 				for (int t = cs; t < ce; ++t) {
 					const float4 pj = fp[t];
 					const int j = __float_as_int(pj.w);
@@ -2467,7 +2489,7 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 					const float q2 = qx * qx + qy * qy + qz * qz;
 					if (!(q2 >= excl2)) continue;
 					const unsigned long long key =
-						sc_near_key(cx, cy, cz, X[j], inv_cell, mask, (unsigned int)(perm ? perm[j] : j));
+						sc_near_key(Href, X[j], inv_cell, (unsigned int)(perm ? perm[j] : j));
 					if (key == ~0ull || (!first_batch && key <= last)) continue;
 					if (nb == kNearBatch) {
 						more = true;
@@ -2482,6 +2504,9 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 					bk[m] = key; bd2[m] = d2; bj[m] = j;
 					++nb;
 				}
+				kc = kn;
+				cs = ns;
+				ce = ne;
 			}
 			// the reference's append / replacement, in key order
 			for (int a = 0; a < nb; ++a) {
