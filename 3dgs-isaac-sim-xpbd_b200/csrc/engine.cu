@@ -264,6 +264,7 @@ public:
 	DBuf<unsigned int> nf_keys;
 	DBuf<int> nf_bucket, nf_start;
 	DBuf<float4> nf_p;
+	int nf_cap = 0;                  // cells of the near-pair grid at most
 	DBuf<float4> sc_dp, sc_sp, sc_sr, sc_sx;
 	DBuf<float> d_scales, d_rots, d_out_scales, d_out_quats, inv_mass_saved;
 	// ellipsoid contact shapes (xpbd_set_contact_shape; forward.cu:150-160, 6733-6757):
@@ -1015,9 +1016,11 @@ public:
 		const int buckets = table + 1;   // + sentinel bucket
 		CK(sc_keys.alloc(n)); CK(sc_bucket.alloc(buckets + 1)); CK(sc_start.alloc(buckets + 1));
 		CK(sc_cursor.alloc(buckets)); CK(sc_idx_sorted.alloc(n)); CK(sc_contacts.alloc((size_t)n * kSelfColMax));
-		CK(nf_keys.alloc(n)); CK(nf_bucket.alloc(buckets)); CK(nf_start.alloc(buckets + 1)); CK(nf_p.alloc(n));
+		nf_cap = std::max(4096, 2 * n);
+		CK(nf_keys.alloc(n)); CK(nf_bucket.alloc(nf_cap + 1)); CK(nf_start.alloc(nf_cap + 2)); CK(nf_p.alloc(n));
+		CK(sc_block_sums.alloc((std::max(buckets, nf_cap) + 2 + 1023) / 1024 + 1));
 		CK(cudaMemsetAsync(nf_bucket.p, 0, nf_bucket.bytes(), stream));
-		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n)); CK(sc_block_sums.alloc((buckets + 1 + 1023) / 1024 + 1));
+		CK(sc_counts.alloc(n)); CK(sc_dp.alloc(n)); CK(sc_sp.alloc(n)); CK(sc_sr.alloc(n)); CK(sc_sx.alloc(n));
 		CK(cudaMemsetAsync(sc_counts.p, 0, sc_counts.bytes(), stream));
 		return 0;
 	}
@@ -1212,10 +1215,14 @@ public:
 				sc_idx_sorted.p, (const int*)d_perm.p);
 		}
 		if (near) {
-			// fine grid: counts, starts, scatter (the scatter returns the counts to zero)
-			const int fscan = sc_table + 1, fnb = (fscan + 1023) / 1024;
-			launch(ST_SC_BUILD, G, B, dev::k_sc_near_keys, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
-				(const float4*)pos_next.p, active, mask, nf_keys.p, nf_bucket.p);
+			// dense grid of the predicted positions: box, cell size, counts, starts, scatter
+			const int fscan = nf_cap + 1, fnb = (fscan + 1023) / 1024;
+			launch(ST_SC_BUILD, G, B, dev::k_sc_near_bounds, N, (const float4*)pos_curr.p, (const float4*)pos_next.p,
+				active, d_ctr);
+			launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_near_setup, (const StepParams*)d_params, d_ctr, nf_cap);
+			CK(cudaMemsetAsync(nf_bucket.p, 0, nf_bucket.bytes(), stream));
+			launch(ST_SC_BUILD, G, B, dev::k_sc_near_keys, N, (const float4*)pos_curr.p, (const float4*)pos_next.p,
+				active, (const DevCounters*)d_ctr, nf_keys.p, nf_bucket.p);
 			launch(ST_SC_BUILD, dim3(fnb), dim3(1024), dev::k_scan_blocks, (const int*)nf_bucket.p, nf_start.p, fscan,
 				sc_block_sums.p);
 			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, fnb);

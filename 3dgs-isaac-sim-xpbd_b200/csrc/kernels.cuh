@@ -2356,52 +2356,133 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 // There every accepted pair is a same-object pair, accepted when its predicted
 // positions are closer than the search radius and its rest positions at least the
 // exclusion distance apart (sc_build_one's same-object branch).  The reference finds
-// those pairs by scanning the 27 cells around each start position with cells of
-// search + 2 max|p - x| (about 100 entries per particle in a moving scene, nearly all
-// rejected).  Here a second grid hashes the PREDICTED positions with cells of
-// kNearCellScale x search, so a pair within the search radius is always in adjacent
-// cells (the margin absorbs the rounding of p / cell for coordinates up to ~2000 cells
-// from the origin) and the 27 cells hold about 1/6 of the entries.  Whatever the grid,
-// the list must be the reference's: its order is the order in which the reference
-// visits the pairs — the first of the particle's 27 start-position cells whose hash is
-// the neighbour's bucket, then the caller index within the bucket (the stable sort) —
-// and the cap-of-32 replacement rule depends on that order.  So each accepted pair
-// gets the key (kc, caller index); a neighbour whose bucket is none of the 27 (possible
-// only when the reference's cell size is capped) is dropped as the reference never
-// sees it; the keys are taken in ascending order in batches of kNearBatch (the batch's
-// smallest keys above the last one taken, one rescan per batch) and fed through the
-// same append / replacement code.  Lists, counts and the over-cap count equal the
-// cell-hash scan's bit for bit.
+// those pairs by scanning the 27 hashed cells around each start position (cells of
+// search + 2 max|p - x|), bucket by bucket.  Here a dense grid covers the box of the
+// PREDICTED positions with cells of at least kNearCellScale x search (x fastest), so a
+// pair within the search radius always lies in adjacent cells, and the three cells of
+// one (y, z) row around a particle are one contiguous range of the cell-sorted array:
+// nine row ranges per particle instead of 27 bucket ranges (no hash, no duplicate
+// buckets; longer, more even trip counts for the lanes of a warp).  The margin of the
+// cell size absorbs the rounding of (p - origin) / cell.  Whatever the grid, the list
+// must be the reference's: its order is the order in which the reference visits the
+// pairs — the first of the particle's 27 start-position cells whose hash is the
+// neighbour's bucket, then the caller index within the bucket (the stable sort) — and
+// the cap-of-32 replacement rule depends on that order.  So each accepted pair gets the
+// key (kc, caller index); a neighbour whose bucket is none of the 27 (possible only when
+// the reference's cell size is capped) is dropped, as the reference never sees it; the
+// keys are taken in ascending order in batches of kNearBatch (the batch's smallest keys
+// above the last one taken, one rescan per batch) and fed through the same append /
+// replacement code.  Lists, counts and the over-cap count equal the 27-cell scan's bit
+// for bit.
 // ---------------------------------------------------------------------------
-constexpr float kNearCellScale = 1.001f;
+constexpr float kNearCellScale = 1.01f;
 constexpr int kNearBatch = 48;
 
-__device__ __forceinline__ float sc_near_inv(const StepParams* __restrict__ P)
+// order-preserving unsigned image of a (non-NaN) float, for atomicMax
+__device__ __forceinline__ unsigned int f_order(float v)
 {
-	return 1.0f / (P->sc_search * kNearCellScale);
+	const unsigned int b = __float_as_uint(v);
+	return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float f_unorder(unsigned int u)
+{
+	return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
-// fine-grid keys: predicted position's cell; particles outside the reference grid
-// (inactive, or a start / predicted position not finite) are left out
-__global__ void __launch_bounds__(kBlock) k_sc_near_keys(int n, const StepParams* __restrict__ P,
-	const float4* __restrict__ X, const float4* __restrict__ Pp, const unsigned char* __restrict__ active,
-	unsigned int mask, unsigned int* __restrict__ keys, int* __restrict__ bucket)
+__device__ __forceinline__ bool sc_near_member(const float4& x, const float4& p, const unsigned char* active, int i)
+{
+	return (!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) &&
+		isfinite(p.y) && isfinite(p.z);
+}
+
+// box of the predicted positions of the grid's particles (min kept complemented, so
+// both ends are atomicMax on zero-initialised counters)
+__global__ void __launch_bounds__(kBlock) k_sc_near_bounds(int n, const float4* __restrict__ X,
+	const float4* __restrict__ Pp, const unsigned char* __restrict__ active, DevCounters* __restrict__ ctr)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned int lo[3] = { 0u, 0u, 0u }, hi[3] = { 0u, 0u, 0u };
+	if (i < n) {
+		const float4 x = X[i], p = Pp[i];
+		if (sc_near_member(x, p, active, i)) {
+			const float v[3] = { p.x, p.y, p.z };
+#pragma unroll
+			for (int a = 0; a < 3; ++a) { lo[a] = ~f_order(v[a]); hi[a] = f_order(v[a]); }
+		}
+	}
+#pragma unroll
+	for (int a = 0; a < 3; ++a) {
+		for (int o = 16; o > 0; o >>= 1) {
+			lo[a] = max(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+			hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+		}
+	}
+	if ((threadIdx.x & 31) == 0 && (hi[0] | hi[1] | hi[2])) {
+#pragma unroll
+		for (int a = 0; a < 3; ++a) { atomicMax(&ctr->nb_lo[a], lo[a]); atomicMax(&ctr->nb_hi[a], hi[a]); }
+	}
+}
+
+// grid origin, cell size (>= kNearCellScale x search, grown until the cells fit `cap`)
+// and cells per axis
+__global__ void k_sc_near_setup(const StepParams* __restrict__ P, DevCounters* __restrict__ ctr, int cap)
+{
+	float cell = P->sc_search * kNearCellScale;
+	float lo[3] = { 0.0f, 0.0f, 0.0f }, ext[3] = { 0.0f, 0.0f, 0.0f };
+	if (ctr->nb_hi[0] | ctr->nb_hi[1] | ctr->nb_hi[2]) {
+		for (int a = 0; a < 3; ++a) {
+			lo[a] = f_unorder(~ctr->nb_lo[a]);
+			ext[a] = fmaxf(f_unorder(ctr->nb_hi[a]) - lo[a], 0.0f);
+		}
+	}
+	if (!(cell > 0.0f) || !isfinite(cell)) cell = 1.0f;
+	double dims[3];
+	for (int round = 0; round < 64; ++round) {
+		double total = 1.0;
+		for (int a = 0; a < 3; ++a) {
+			dims[a] = floor((double)ext[a] / (double)cell) + 1.0;
+			total *= dims[a];
+		}
+		if (total <= (double)cap) break;
+		cell = (float)((double)cell * cbrt(total / (double)cap) * 1.001);
+	}
+	for (int a = 0; a < 3; ++a) {
+		ctr->nb_origin[a] = lo[a];
+		ctr->nb_dim[a] = (int)dims[a];
+	}
+	ctr->nb_inv = 1.0f / cell;
+}
+
+__device__ __forceinline__ int sc_near_axis(float v, float o, float inv, int dim)
+{
+	return min(max((int)floorf((v - o) * inv), 0), dim - 1);
+}
+
+// dense-grid keys (cell index, x fastest) of the grid's particles and cell counts;
+// particles outside the reference's grid (inactive, or a start / predicted position not
+// finite) are left out
+__global__ void __launch_bounds__(kBlock) k_sc_near_keys(int n, const float4* __restrict__ X,
+	const float4* __restrict__ Pp, const unsigned char* __restrict__ active, const DevCounters* __restrict__ ctr,
+	unsigned int* __restrict__ keys, int* __restrict__ bucket)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const float4 x = X[i], p = Pp[i];
 	unsigned int k = 0xffffffffu;
-	if ((!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) && isfinite(p.y) &&
-		isfinite(p.z)) {
-		const float inv = sc_near_inv(P);
-		k = sc_hash(sc_cell(p.x, inv), sc_cell(p.y, inv), sc_cell(p.z, inv), mask);
+	if (sc_near_member(x, p, active, i)) {
+		const float inv = ctr->nb_inv;
+		const int dx = ctr->nb_dim[0], dy = ctr->nb_dim[1], dz = ctr->nb_dim[2];
+		const int ix = sc_near_axis(p.x, ctr->nb_origin[0], inv, dx);
+		const int iy = sc_near_axis(p.y, ctr->nb_origin[1], inv, dy);
+		const int iz = sc_near_axis(p.z, ctr->nb_origin[2], inv, dz);
+		k = (unsigned int)((iz * dy + iy) * dx + ix);
 		atomicAdd(&bucket[k], 1);
 	}
 	keys[i] = k;
 }
 
-// scatter predicted position + index into the fine buckets (order within a bucket is
-// free: the lists are ordered by key afterwards); leaves the bucket counts at zero
+// scatter predicted position + index into the cells (order within a cell is free: the
+// lists are ordered by key afterwards); leaves the cell counts at zero
 __global__ void __launch_bounds__(kBlock) k_sc_near_scatter(int n, const unsigned int* __restrict__ keys,
 	const int* __restrict__ start, int* __restrict__ bucket, const float4* __restrict__ Pp, float4* __restrict__ fp)
 {
@@ -2426,6 +2507,8 @@ __device__ __forceinline__ unsigned long long sc_near_key(const Hash27& Href, fl
 	return ~0ull;
 }
 
+// mask: the reference's hash table mask (for the keys); start_f / fp: the dense grid's
+// cell starts and (p, index) by cell
 __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
 	const unsigned char* __restrict__ active, const int* __restrict__ start_f, unsigned int mask,
@@ -2436,14 +2519,27 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 	if (i >= n) return;
 	int cnt = 0, over = 0;
 	const float4 x = X[i], p = Pp[i];
-	if ((!active || active[i]) && P->sc_within && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) &&
-		isfinite(p.y) && isfinite(p.z)) {
+	if (P->sc_within && sc_near_member(x, p, active, i)) {
 		const float search = P->sc_search, excl2 = P->sc_excl2;
 		const float search2 = search * search;
-		const float inv = sc_near_inv(P);
 		const float4 q = rest[i];
-		const Hash27 Hf(sc_cell(p.x, inv), sc_cell(p.y, inv), sc_cell(p.z, inv), mask);
-		const unsigned int use = hash27_unique(Hf);   // the fine cells, each bucket once
+		const float inv = ctr->nb_inv;
+		const int dx = ctr->nb_dim[0], dy = ctr->nb_dim[1], dz = ctr->nb_dim[2];
+		const int ix = sc_near_axis(p.x, ctr->nb_origin[0], inv, dx);
+		const int iy = sc_near_axis(p.y, ctr->nb_origin[1], inv, dy);
+		const int iz = sc_near_axis(p.z, ctr->nb_origin[2], inv, dz);
+		const int x0 = max(ix - 1, 0), x1 = min(ix + 1, dx - 1);
+		// row r = 3 (dz + 1) + (dy + 1): its cells x0..x1 are one range of the sorted array
+		auto row_range = [&](int r, int& cs, int& ce) {
+			const int qr = (r * 11) >> 5;   // r / 3
+			const int z = iz + qr - 1, y = iy + (r - 3 * qr) - 1;
+			cs = ce = 0;
+			if (z >= 0 && z < dz && y >= 0 && y < dy) {
+				const int row = (z * dy + y) * dx;
+				cs = start_f[row + x0];
+				ce = start_f[row + x1 + 1];
+			}
+		};
 		// the particle's own reference cell, for the keys
 		const float inv_cell = ctr->sc_inv_cell;
 		const Hash27 Href(sc_cell(x.x, inv_cell), sc_cell(x.y, inv_cell), sc_cell(x.z, inv_cell), mask);
@@ -2459,24 +2555,13 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 			int bj[kNearBatch];
 			int nb = 0;
 			bool more = false;
-			// the used fine cells in order, the next one's bucket range loaded while the
-			// current one's entries are tested
-			int kc = use ? __ffs(use) - 1 : 27;
-			int cs = 0, ce = 0;
-			if (kc < 27) {
-				const unsigned int h = Hf(kc);
-				cs = start_f[h];
-				ce = start_f[h + 1];
-			}
-			while (kc < 27) {
-				const unsigned int later = use & ~((2u << kc) - 1u);
-				const int kn = later ? __ffs(later) - 1 : 27;
+			// the nine rows in turn, the next row's range loaded while the current one's
+			// entries are tested
+			int cs, ce;
+			row_range(0, cs, ce);
+			for (int r = 0; r < 9; ++r) {
 				int ns = 0, ne = 0;
-				if (kn < 27) {
-					const unsigned int hn = Hf(kn);
-					ns = start_f[hn];
-					ne = start_f[hn + 1];
-				}
+				if (r < 8) row_range(r + 1, ns, ne);
 				for (int t = cs; t < ce; ++t) {
 					const float4 pj = fp[t];
 					const int j = __float_as_int(pj.w);
@@ -2504,7 +2589,6 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParam
 					bk[m] = key; bd2[m] = d2; bj[m] = j;
 					++nb;
 				}
-				kc = kn;
 				cs = ns;
 				ce = ne;
 			}

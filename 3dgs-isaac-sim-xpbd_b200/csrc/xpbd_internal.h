@@ -79,6 +79,11 @@ struct DevCounters {
 	unsigned int sc_active;         // Gaussians in the grid when the object box filter is on ([2])
 	unsigned int bar_count, bar_gen; // grid barrier of the fused substep launch
 	unsigned int bar_timeout;       // a barrier wait of the fused launch ran out (error)
+	// near-pair grid of one-object scenes: box of the predicted positions (order-preserving
+	// images; the minimum complemented), origin, 1 / cell and cells per axis
+	unsigned int nb_lo[3], nb_hi[3];
+	float nb_origin[3], nb_inv;
+	int nb_dim[3];
 	int kin_hits[kMaxColliders];
 	float kin_push[kMaxColliders * kColliderAcc];
 	double jstats[3];               // sum V, sum V J, sum V J^2
