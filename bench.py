@@ -322,11 +322,14 @@ def bench_b200(args, rank, world):
         b = bench_batched(sub, 0, 1)
         line["batched"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps", "config", "plain",
                                              "speedup_vs_plain")}
-        sv = bench_served(sub, 0, 1, duration=10.0, max_wall=30.0)
+        sv = bench_served(sub, 0, 1, duration=10.0, max_wall=20.0)
         line["served"] = {"value": sv["value"], "unit": sv["unit"], "p50_ms": sv["served"]["p50_ms"],
                           "p99_ms": sv["served"]["p99_ms"], "config": sv["config"], "served": sv["served"],
                           "served_hbm_bound": sv["served_hbm_bound"], "plain": sv["plain"],
-                          "speedup_vs_plain": sv["speedup_vs_plain"]}
+                          "plain_engine_per_session": sv["plain_engine_per_session"],
+                          "admission_target_ms": sv["admission_target_ms"],
+                          "speedup_vs_plain": sv["speedup_vs_plain"],
+                          "speedup_vs_plain_engine_per_session": sv["speedup_vs_plain_engine_per_session"]}
     return line
 
 
@@ -755,8 +758,9 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
     """Poisson session arrivals at 200/s (5e3-5e5 Gaussians, 1-120 frames of 10 substeps x
     4 iterations) served with continuous batching in one arena, against one session at a
     time.  Sessions are admitted by the 150 GB HBM budget and, in the latency-bound run,
-    also while the arena's predicted tick stays within one 60 Hz frame (16.7 ms); the
-    others wait in arrival order.  Scenes come from a pool of 12 pre-generated sizes
+    also while the arena's predicted tick stays within three quarters of a 60 Hz frame
+    (12.5 ms: the rest of the frame absorbs admission copies and host work, so that
+    step latencies stay within the frame); the others wait in arrival order.  Scenes come from a pool of 12 pre-generated sizes
     (generation is host Python and would otherwise bound the arrival rate)."""
     serve = pkg.serve
     rate = 200.0
@@ -776,12 +780,15 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
     pool.prepare_all(lib)            # each pool scene's topology, built once before the runs
     prep_s = time.perf_counter() - t0
     runs = {}
-    for name, target in (("latency_bound", 1000.0 / 60.0), ("hbm_bound", None)):
+    for name, target in (("latency_bound", 0.75 * 1000.0 / 60.0), ("hbm_bound", None)):
         r = serve.run_served(lib, sessions, budget_bytes=150e9, max_wall=max_wall, latency_target_ms=target,
                              keep_results=False, pool=pool)
         r.pop("sessions_done", None)
         runs[name] = r
     plain = serve.run_plain(lib, sessions, max_wall=max_wall, pool=pool) if world == 1 else None
+    # the reference runtime's pattern: an engine of its own per session (upload and
+    # topology build included), one session at a time
+    plain_own = serve.run_plain(lib, sessions, max_wall=max_wall, pool=list(pool)) if world == 1 else None
     pool.close()
     if world > 1:
         # whole-job figures: work summed, wall time the slowest rank's; latencies of rank 0
@@ -808,9 +815,14 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
                                    f"built once per pool scene) before the runs ({prep_s:.1f} s); admission = a device "
                                    "copy of the pool scene's prepared engine into the arena; the plain loop steps the "
                                    "same prepared engines, reset to rest per session"},
+            "admission_target_ms": 0.75 * 1000.0 / 60.0,
             "served": lb, "served_hbm_bound": runs["hbm_bound"], "plain": plain,
+            "plain_engine_per_session": plain_own,
             "speedup_vs_plain": (lb["gauss_substeps_per_s"] / max(plain["gauss_substeps_per_s"], 1e-9)
-                                 if world == 1 else None)}
+                                 if world == 1 else None),
+            "speedup_vs_plain_engine_per_session": (lb["gauss_substeps_per_s"] /
+                                                    max(plain_own["gauss_substeps_per_s"], 1e-9)
+                                                    if world == 1 else None)}
 
 
 def bench_reference(args, rank, world):
