@@ -136,6 +136,7 @@ struct Settings {
 	bool press_autolog = true;       // press harness: settle at 25/50/75/100 % (forward.cu:565)
 	int fused = 0;                   // substep as one cooperative launch: 0 never, 1 always, 2 the faster (timed)
 	int sc_near = 1;                 // one-object scenes: candidate lists from the near-pair grid
+	int vol_chunk = 1 << 20;         // rows per solve + gather chunk of a packed scene (0: one pass)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -164,6 +165,7 @@ public:
 	// ---- host topology (caller index space) and the internal order ----
 	std::vector<int> perm, inv;
 	std::vector<unsigned long long> lcode;   // Morton code in its component's box, per caller index
+	std::vector<int> comp_row0;      // first row of each component in internal order (+ n), when contiguous
 	HostGraph graph;
 	HostClusters clusters;
 	HostEdgeColoring coloring;
@@ -517,26 +519,14 @@ public:
 		return c;
 	}
 
+	// Internal order: objects (graph components) one after another, in the order of their
+	// lowest caller index, each along the Morton curve of its own box; a single object
+	// gets the Morton order of the scene's box.  Objects that share space (a packed batch)
+	// then keep their rows, and the cache lines they gather, to themselves.
 	void compute_order()
 	{
 		perm.resize(n);
 		inv.resize(n);
-		for (int i = 0; i < n; ++i) perm[i] = i;
-		if (S.reorder && n > 1) {
-			float lo[3] = { FLT_MAX, FLT_MAX, FLT_MAX }, hi[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
-			for (int i = 0; i < n; ++i)
-				for (int a = 0; a < 3; ++a) {
-					const float v = in_pos[3 * i + a];
-					if (std::isfinite(v)) { lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
-				}
-			std::vector<unsigned long long> code(n);
-			for (int i = 0; i < n; ++i) code[i] = morton_code(&in_pos[3 * i], lo, hi);
-			std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return code[a] < code[b]; });
-		}
-		for (int r = 0; r < n; ++r) inv[perm[r]] = r;
-		// Morton code within each connected component's own box: orders the rows of the
-		// 4- and 8-lane volume lists the same way whatever the renumbering and whatever
-		// other objects share the scene
 		std::vector<int> parent(n);
 		for (int i = 0; i < n; ++i) parent[i] = i;
 		auto root = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
@@ -548,18 +538,60 @@ public:
 				if (ri != rj) parent[ri] = rj;
 			}
 		std::vector<float> clo(3 * (size_t)n, FLT_MAX), chi(3 * (size_t)n, -FLT_MAX);
+		std::vector<int> rank(n, -1), comp(n);
+		int comps = 0;
 		for (int i = 0; i < n; ++i) {
 			const int r = root(i);
+			comp[i] = r;
+			if (rank[r] < 0) rank[r] = comps++;
 			for (int a = 0; a < 3; ++a) {
 				const float v = in_pos[3 * i + a];
 				if (std::isfinite(v)) { clo[3 * r + a] = std::min(clo[3 * r + a], v); chi[3 * r + a] = std::max(chi[3 * r + a], v); }
 			}
 		}
+		// Morton code within each component's own box: also orders the rows of the 4- and
+		// 8-lane volume lists the same way whatever the renumbering and whatever other
+		// objects share the scene
 		lcode.resize(n);
 		for (int i = 0; i < n; ++i) {
-			const int r = root(i);
+			const int r = comp[i];
 			lcode[i] = morton_code(&in_pos[3 * i], &clo[3 * r], &chi[3 * r]);
 		}
+		for (int i = 0; i < n; ++i) perm[i] = i;
+		if (S.reorder && n > 1)
+			std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+				const int ra = rank[comp[a]], rb = rank[comp[b]];
+				if (ra != rb) return ra < rb;
+				return lcode[a] < lcode[b];
+			});
+		for (int r = 0; r < n; ++r) inv[perm[r]] = r;
+		comp_row0.clear();
+		if (S.reorder || comps == 1) {
+			for (int r = 0; r < n; ++r)
+				if (r == 0 || rank[comp[perm[r]]] != rank[comp[perm[r - 1]]]) comp_row0.push_back(r);
+			comp_row0.push_back(n);
+		}
+	}
+
+	// [row0, row1) ranges of whole components of about S.vol_chunk rows (one range when
+	// chunking is off, the components are not contiguous, or in an arena)
+	std::vector<int2> volume_chunks() const
+	{
+		std::vector<int2> out;
+		if (S.vol_chunk <= 0 || arena || comp_row0.size() < 3 || comp_row0.back() != n) {
+			out.push_back(make_int2(0, n));
+			return out;
+		}
+		int start = 0;
+		for (size_t c = 1; c < comp_row0.size(); ++c) {
+			const int end = comp_row0[c];
+			const bool last = c + 1 == comp_row0.size();
+			if (end - start >= S.vol_chunk || last) {
+				out.push_back(make_int2(start, end));
+				start = end;
+			}
+		}
+		return out;
 	}
 
 	// caller-order CSR (off[N+1], idx) -> internal order, neighbour order kept
@@ -1149,7 +1181,7 @@ public:
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
 			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground(),
-			selfcol_on() && sc_near_on() };
+			selfcol_on() && sc_near_on(), (long long)volume_chunks().size() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -1379,11 +1411,29 @@ public:
 					const int rl = first ? 0 : 1;
 					const StepParams* dp = d_params;
 					const float4* cpin = pin;
-					if (la == 4 && S.lanes_a == 0)
-						// automatic: one pass over the members (any count), 4 lanes per cluster
+					if (la == 4 && S.lanes_a == 0 && lb == 4) {
+						// automatic: one pass over the members (any count), 4 lanes per cluster and
+						// per node; objects packed in one scene run solve + gather chunk by chunk
+						// (whole objects of about vol_chunk rows), so that a chunk's cluster records
+						// are still in L2 when its gather reads them (same per-item work: identical)
+						auto ks = occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
+							: dev::k_volume_solve_onepass<4>;
+						auto kg = occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
+							: dev::k_volume_gather_group<4>;
+						for (const int2 c : volume_chunks()) {
+							const long long rows = (long long)c.y - c.x;
+							launch(ST_VOL_SOLVE, blocks_for(rows * 4), B, ks, c.x, c.y, dp, cpin, (const int*)vol_off.p,
+								(const int*)vol_idx_s.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p,
+								rec.p, recz(), rl);
+							launch(ST_VOL_GATHER, blocks_for(rows * 4), B, kg, c.x, c.y, dp, cpin, pout,
+								(const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(),
+								(const float*)rest_len.p);
+						}
+					}
+					else if (la == 4 && S.lanes_a == 0)
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
-							: dev::k_volume_solve_onepass<4>, N, dp, cpin,
+							: dev::k_volume_solve_onepass<4>, 0, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 32)
@@ -1409,16 +1459,19 @@ public:
 					else
 						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
 							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
-					if (lb == 32)
-						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, N, dp, cpin,
+					if (la == 4 && S.lanes_a == 0 && lb == 4) {
+						// (solve and gather launched together above)
+					}
+					else if (lb == 32)
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, 0, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 8)
-						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, 0, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
-							: dev::k_volume_gather_group<4>, N, dp, cpin,
+							: dev::k_volume_gather_group<4>, 0, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
@@ -2869,6 +2922,7 @@ XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled 
 
 XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std::min(2, mode)); }
 XPBD_API void xpbd_b200_set_selfcol_near(int enabled) { engine().S.sc_near = enabled ? 1 : 0; }
+XPBD_API void xpbd_b200_set_volume_chunk(int rows) { engine().S.vol_chunk = std::max(0, rows); }
 
 XPBD_API int xpbd_b200_tuning(float* out)
 {

@@ -962,22 +962,22 @@ __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const 
 	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int row0, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff, vidx, det_rest,
-		mat_type, lam_vol, rec, recz, read_lam);
+	solve_onepass_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
+		voff, vidx, det_rest, mat_type, lam_vol, rec, recz, read_lam);
 }
 template <int S, int MINB>
-__global__ void __launch_bounds__(kBlock, MINB) k_volume_solve_occ(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_solve_occ(int row0, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, voff, vidx, det_rest,
-		mat_type, lam_vol, rec, recz, read_lam);
+	solve_onepass_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
+		voff, vidx, det_rest, mat_type, lam_vol, rec, recz, read_lam);
 }
 
 // Kernel A, one thread per cluster (forward.cu:8531-8664): sequential sums, leader first.
@@ -1142,26 +1142,26 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
 template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int row0, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)
 {
-	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff, ridx, rec,
-		recz, rest_len);
+	gather_group_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+		roff, ridx, rec, recz, rest_len);
 }
 
 // The distance, volume solve and gather kernels compiled for MINB resident blocks per SM
 // (fewer registers, more warps in flight for these latency-bound gathers): the same
 // per-item code, so the same results; the autotuner picks among the forms by timing.
 template <int S, int MINB>
-__global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int row0, int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)
 {
-	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout, roff, ridx, rec,
-		recz, rest_len);
+	gather_group_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+		roff, ridx, rec, recz, rest_len);
 }
 
 // Kernel B, one thread per node (forward.cu:9187-9243)
