@@ -136,7 +136,6 @@ struct Settings {
 	bool press_autolog = true;       // press harness: settle at 25/50/75/100 % (forward.cu:565)
 	int fused = 0;                   // substep as one cooperative launch: 0 never, 1 always, 2 the faster (timed)
 	int sc_near = 1;                 // one-object scenes: candidate lists from the near-pair grid
-	int vol_chunk = 1 << 20;         // rows per solve + gather chunk of a packed scene (0: one pass)
 	Settings()
 	{
 		for (auto& v : kin_obj) v = -1;
@@ -165,7 +164,6 @@ public:
 	// ---- host topology (caller index space) and the internal order ----
 	std::vector<int> perm, inv;
 	std::vector<unsigned long long> lcode;   // Morton code in its component's box, per caller index
-	std::vector<int> comp_row0;      // first row of each component in internal order (+ n), when contiguous
 	HostGraph graph;
 	HostClusters clusters;
 	HostEdgeColoring coloring;
@@ -565,33 +563,6 @@ public:
 				return lcode[a] < lcode[b];
 			});
 		for (int r = 0; r < n; ++r) inv[perm[r]] = r;
-		comp_row0.clear();
-		if (S.reorder || comps == 1) {
-			for (int r = 0; r < n; ++r)
-				if (r == 0 || rank[comp[perm[r]]] != rank[comp[perm[r - 1]]]) comp_row0.push_back(r);
-			comp_row0.push_back(n);
-		}
-	}
-
-	// [row0, row1) ranges of whole components of about S.vol_chunk rows (one range when
-	// chunking is off, the components are not contiguous, or in an arena)
-	std::vector<int2> volume_chunks() const
-	{
-		std::vector<int2> out;
-		if (S.vol_chunk <= 0 || arena || comp_row0.size() < 3 || comp_row0.back() != n) {
-			out.push_back(make_int2(0, n));
-			return out;
-		}
-		int start = 0;
-		for (size_t c = 1; c < comp_row0.size(); ++c) {
-			const int end = comp_row0[c];
-			const bool last = c + 1 == comp_row0.size();
-			if (end - start >= S.vol_chunk || last) {
-				out.push_back(make_int2(start, end));
-				start = end;
-			}
-		}
-		return out;
 	}
 
 	// caller-order CSR (off[N+1], idx) -> internal order, neighbour order kept
@@ -1181,7 +1152,7 @@ public:
 			(long long)S.kin_ext.empty(), (long long)(size_t)d_kin_ext.p,
 			(long long)coloring.color_off.size(), (long long)clusters.gs_color_off.size(), (long long)sc_table,
 			object_on(), att_active && S.obj_gpu, sc_limited(), obj_push(), contact_col(), contact_ground(),
-			selfcol_on() && sc_near_on(), (long long)volume_chunks().size() };
+			selfcol_on() && sc_near_on() };
 	}
 
 	// ------------------------------------------------------------------ launching
@@ -1229,9 +1200,11 @@ public:
 		const dim3 B(kBlock), G = blocks_for(N);
 		const int buckets = sc_table + 1, scan_n = buckets + 1, nb = (scan_n + 1023) / 1024;
 		const unsigned mask = (unsigned)(sc_table - 1);
-		launch(ST_SC_BUILD, G, B, dev::k_sc_disp, N, (const float4*)pos_curr.p, (const float4*)pos_next.p, d_ctr, active);
-		launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
 		const bool near = sc_near_on();
+		// displacement max (and, for the near-pair grid, the box of the predicted positions)
+		launch(ST_SC_BUILD, dim3(std::min<unsigned>(G.x, 148u * 8u)), B, dev::k_sc_disp, N, (const float4*)pos_curr.p,
+			(const float4*)pos_next.p, d_ctr, active, near ? 1 : 0);
+		launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_setup, (const StepParams*)d_params, d_ctr);
 		if (!near || ref_structure) {
 			CK(cudaMemsetAsync(sc_bucket.p, 0, sc_bucket.bytes(), stream));
 			CK(cudaMemsetAsync(sc_cursor.p, 0, sc_cursor.bytes(), stream));
@@ -1247,10 +1220,8 @@ public:
 				sc_idx_sorted.p, (const int*)d_perm.p);
 		}
 		if (near) {
-			// dense grid of the predicted positions: box, cell size, counts, starts, scatter
+			// dense grid of the predicted positions: cell size, counts, starts, scatter
 			const int fscan = nf_cap + 1, fnb = (fscan + 1023) / 1024;
-			launch(ST_SC_BUILD, G, B, dev::k_sc_near_bounds, N, (const float4*)pos_curr.p, (const float4*)pos_next.p,
-				active, d_ctr);
 			launch(ST_SC_BUILD, dim3(1), dim3(1), dev::k_sc_near_setup, (const StepParams*)d_params, d_ctr, nf_cap);
 			CK(cudaMemsetAsync(nf_bucket.p, 0, nf_bucket.bytes(), stream));
 			launch(ST_SC_BUILD, G, B, dev::k_sc_near_keys, N, (const float4*)pos_curr.p, (const float4*)pos_next.p,
@@ -1411,29 +1382,11 @@ public:
 					const int rl = first ? 0 : 1;
 					const StepParams* dp = d_params;
 					const float4* cpin = pin;
-					if (la == 4 && S.lanes_a == 0 && lb == 4) {
-						// automatic: one pass over the members (any count), 4 lanes per cluster and
-						// per node; objects packed in one scene run solve + gather chunk by chunk
-						// (whole objects of about vol_chunk rows), so that a chunk's cluster records
-						// are still in L2 when its gather reads them (same per-item work: identical)
-						auto ks = occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
-							: dev::k_volume_solve_onepass<4>;
-						auto kg = occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
-							: dev::k_volume_gather_group<4>;
-						for (const int2 c : volume_chunks()) {
-							const long long rows = (long long)c.y - c.x;
-							launch(ST_VOL_SOLVE, blocks_for(rows * 4), B, ks, c.x, c.y, dp, cpin, (const int*)vol_off.p,
-								(const int*)vol_idx_s.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p,
-								rec.p, recz(), rl);
-							launch(ST_VOL_GATHER, blocks_for(rows * 4), B, kg, c.x, c.y, dp, cpin, pout,
-								(const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(),
-								(const float*)rest_len.p);
-						}
-					}
-					else if (la == 4 && S.lanes_a == 0)
+					if (la == 4 && S.lanes_a == 0)
+						// automatic: one pass over the members (any count), 4 lanes per cluster
 						launch(ST_VOL_SOLVE, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_solve_occ<4, 8> : occ == 6 ? dev::k_volume_solve_occ<4, 6>
-							: dev::k_volume_solve_onepass<4>, 0, N, dp, cpin,
+							: dev::k_volume_solve_onepass<4>, N, dp, cpin,
 							(const int*)vol_off.p, (const int*)vol_idx_s.p, (const float*)det_rest.p,
 							(const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					else if (la == 32)
@@ -1459,19 +1412,16 @@ public:
 					else
 						launch(ST_VOL_SOLVE, G, B, dev::k_volume_solve_thread, N, dp, cpin, (const int*)vol_off.p,
 							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
-					if (la == 4 && S.lanes_a == 0 && lb == 4) {
-						// (solve and gather launched together above)
-					}
-					else if (lb == 32)
-						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, 0, N, dp, cpin,
+					if (lb == 32)
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 8)
-						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, 0, N, dp, cpin,
+						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
-							: dev::k_volume_gather_group<4>, 0, N, dp, cpin,
+							: dev::k_volume_gather_group<4>, N, dp, cpin,
 							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
@@ -1784,7 +1734,10 @@ public:
 			return rows_used + (long long)rows <= rows_cap && e_used + ne <= e_cap && m_used + nm <= m_cap &&
 				r_used + nr <= r_cap;
 		};
-		if (!fits() && arena_compact()) return -1;
+		// compaction only helps when retired segments left holes below the tail
+		bool holes = false;
+		for (const auto& g : segs) holes = holes || !g.live;
+		if (!fits() && holes && arena_compact()) return -1;
 		if (!fits()) return -2;
 		if (!any_live) {
 			const auto kin = S.kin_ext;
@@ -2922,7 +2875,6 @@ XPBD_API void xpbd_b200_set_graph(int enabled) { engine().S.use_graph = enabled 
 
 XPBD_API void xpbd_b200_set_fused(int mode) { engine().S.fused = std::max(0, std::min(2, mode)); }
 XPBD_API void xpbd_b200_set_selfcol_near(int enabled) { engine().S.sc_near = enabled ? 1 : 0; }
-XPBD_API void xpbd_b200_set_volume_chunk(int rows) { engine().S.vol_chunk = std::max(0, rows); }
 
 XPBD_API int xpbd_b200_tuning(float* out)
 {
@@ -3387,7 +3339,7 @@ XPBD_API int xpbd_b200_selfcol_candidates_static(int n, const float* x, const fl
 	const auto* Pp = reinterpret_cast<const float4*>(p);
 	const auto* R = reinterpret_cast<const float4*>(rest);
 	const dim3 B(kBlock), G((n + kBlock - 1) / kBlock);
-	dev::k_sc_disp<<<G, B, 0, st>>>(n, X, Pp, d_ctr, nullptr);
+	dev::k_sc_disp<<<G, B, 0, st>>>(n, X, Pp, d_ctr, nullptr, 0);
 	dev::k_sc_setup<<<1, 1, 0, st>>>(d_params, d_ctr);
 	dev::k_sc_keys<<<G, B, 0, st>>>(n, X, d_ctr, (unsigned)(table - 1), (unsigned)table, keys, bucket, nullptr);
 	dev::k_scan_blocks<<<nb, 1024, 0, st>>>(bucket, start, scan_n, sums);

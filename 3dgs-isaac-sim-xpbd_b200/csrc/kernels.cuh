@@ -962,21 +962,21 @@ __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const 
 	store_record(rec, recz, idx, c, dl * gs, Sinv);
 }
 template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int row0, int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock) k_volume_solve_onepass(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	solve_onepass_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
+	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
 		voff, vidx, det_rest, mat_type, lam_vol, rec, recz, read_lam);
 }
 template <int S, int MINB>
-__global__ void __launch_bounds__(kBlock, MINB) k_volume_solve_occ(int row0, int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_solve_occ(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, const int* __restrict__ voff, const int* __restrict__ vidx,
 	const float* __restrict__ det_rest, const int* __restrict__ mat_type, float* __restrict__ lam_vol,
 	float4* __restrict__ rec, float* __restrict__ recz, int read_lam)
 {
-	solve_onepass_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
+	solve_onepass_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin,
 		voff, vidx, det_rest, mat_type, lam_vol, rec, recz, read_lam);
 }
 
@@ -1142,12 +1142,12 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
 template <int S>
-__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int row0, int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)
 {
-	gather_group_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
 		roff, ridx, rec, recz, rest_len);
 }
 
@@ -1155,12 +1155,12 @@ __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int row0, int n,
 // (fewer registers, more warps in flight for these latency-bound gathers): the same
 // per-item code, so the same results; the autotuner picks among the forms by timing.
 template <int S, int MINB>
-__global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int row0, int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
 	const float* __restrict__ rest_len)
 {
-	gather_group_lane<S, true>((long long)row0 * S + (long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
 		roff, ridx, rec, recz, rest_len);
 }
 
@@ -2063,26 +2063,56 @@ __device__ __forceinline__ unsigned int hash27_unique(const Hash27& H)
 	return use;
 }
 
-// max predict displacement^2 (selfColDispKernel + DeviceReduce::Max)
-__global__ void __launch_bounds__(kBlock) k_sc_disp(int n, const float4* __restrict__ x, const float4* __restrict__ p,
-	DevCounters* __restrict__ ctr, const unsigned char* __restrict__ active)
+// order-preserving unsigned image of a (non-NaN) float, for atomicMax
+__device__ __forceinline__ unsigned int f_order(float v)
 {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	float d2 = 0.0f;
-	if (i < n && (!active || active[i])) {
+	const unsigned int b = __float_as_uint(v);
+	return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float f_unorder(unsigned int u)
+{
+	return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// max predict displacement^2 (selfColDispKernel + DeviceReduce::Max); with `bounds`,
+// also the box of the predicted positions of the particles in the grid (active, start
+// and predicted position finite) for the near-pair grid: order-preserving images, the
+// minimum complemented, so that both ends are atomicMax on zero-initialised counters.
+// Grid-stride over the particles, one set of atomics per block.
+__global__ void __launch_bounds__(kBlock) k_sc_disp(int n, const float4* __restrict__ x, const float4* __restrict__ p,
+	DevCounters* __restrict__ ctr, const unsigned char* __restrict__ active, int bounds)
+{
+	unsigned int m[7] = { 0u, 0u, 0u, 0u, 0u, 0u, 0u };   // disp^2 bits, lo x y z, hi x y z
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		if (active && !active[i]) continue;
 		const float4 a = x[i], b = p[i];
 		const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
 		const float v = dx * dx + dy * dy + dz * dz;
-		d2 = isfinite(v) ? v : 0.0f;
+		m[0] = max(m[0], __float_as_uint(isfinite(v) ? v : 0.0f));
+		if (bounds && isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(b.x) && isfinite(b.y) &&
+			isfinite(b.z)) {
+			const float c[3] = { b.x, b.y, b.z };
+#pragma unroll
+			for (int k = 0; k < 3; ++k) { m[1 + k] = max(m[1 + k], ~f_order(c[k])); m[4 + k] = max(m[4 + k], f_order(c[k])); }
+		}
 	}
-	for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
-	__shared__ float smax[kBlock / 32];
-	if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = d2;
+	__shared__ unsigned int sm[7][kBlock / 32];
+#pragma unroll
+	for (int k = 0; k < 7; ++k) {
+		for (int o = 16; o > 0; o >>= 1) m[k] = max(m[k], __shfl_xor_sync(0xffffffffu, m[k], o));
+		if ((threadIdx.x & 31) == 0) sm[k][threadIdx.x >> 5] = m[k];
+	}
 	__syncthreads();
 	if (threadIdx.x < 32) {
-		float v = (threadIdx.x < blockDim.x / 32) ? smax[threadIdx.x] : 0.0f;
-		for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-		if (threadIdx.x == 0) atomicMax(&ctr->sc_max_disp2_bits, __float_as_uint(v));
+#pragma unroll
+		for (int k = 0; k < 7; ++k) {
+			unsigned int v = (threadIdx.x < blockDim.x / 32) ? sm[k][threadIdx.x] : 0u;
+			for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+			if (threadIdx.x == 0) {
+				if (k == 0) atomicMax(&ctr->sc_max_disp2_bits, v);
+				else if (bounds && v) atomicMax(k < 4 ? &ctr->nb_lo[k - 1] : &ctr->nb_hi[k - 4], v);
+			}
+		}
 	}
 }
 
@@ -2378,49 +2408,10 @@ __global__ void __launch_bounds__(kBlock) k_sc_build_sorted(int n, const StepPar
 constexpr float kNearCellScale = 1.01f;
 constexpr int kNearBatch = 48;
 
-// order-preserving unsigned image of a (non-NaN) float, for atomicMax
-__device__ __forceinline__ unsigned int f_order(float v)
-{
-	const unsigned int b = __float_as_uint(v);
-	return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-__device__ __forceinline__ float f_unorder(unsigned int u)
-{
-	return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 __device__ __forceinline__ bool sc_near_member(const float4& x, const float4& p, const unsigned char* active, int i)
 {
 	return (!active || active[i]) && isfinite(x.x) && isfinite(x.y) && isfinite(x.z) && isfinite(p.x) &&
 		isfinite(p.y) && isfinite(p.z);
-}
-
-// box of the predicted positions of the grid's particles (min kept complemented, so
-// both ends are atomicMax on zero-initialised counters)
-__global__ void __launch_bounds__(kBlock) k_sc_near_bounds(int n, const float4* __restrict__ X,
-	const float4* __restrict__ Pp, const unsigned char* __restrict__ active, DevCounters* __restrict__ ctr)
-{
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	unsigned int lo[3] = { 0u, 0u, 0u }, hi[3] = { 0u, 0u, 0u };
-	if (i < n) {
-		const float4 x = X[i], p = Pp[i];
-		if (sc_near_member(x, p, active, i)) {
-			const float v[3] = { p.x, p.y, p.z };
-#pragma unroll
-			for (int a = 0; a < 3; ++a) { lo[a] = ~f_order(v[a]); hi[a] = f_order(v[a]); }
-		}
-	}
-#pragma unroll
-	for (int a = 0; a < 3; ++a) {
-		for (int o = 16; o > 0; o >>= 1) {
-			lo[a] = max(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
-			hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
-		}
-	}
-	if ((threadIdx.x & 31) == 0 && (hi[0] | hi[1] | hi[2])) {
-#pragma unroll
-		for (int a = 0; a < 3; ++a) { atomicMax(&ctr->nb_lo[a], lo[a]); atomicMax(&ctr->nb_hi[a], hi[a]); }
-	}
 }
 
 // grid origin, cell size (>= kNearCellScale x search, grown until the cells fit `cap`)

@@ -297,9 +297,9 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                 joining.append(ready.get())
             still_joining = []
             for s in joining:
-                slot = arena.admit(s.src)
-                if slot is None:          # full until sessions leave (compaction ran already)
-                    still_joining.append(s)
+                slot = arena.admit(s.src) if not still_joining else None
+                if slot is None:          # full until sessions leave (compaction ran already); the
+                    still_joining.append(s)   # later ones keep their arrival order behind it
                     continue
                 s.slot = slot
                 if s.own:                 # the arena holds the session's state now

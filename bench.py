@@ -221,7 +221,9 @@ def bench_b200(args, rank, world):
     bind_ext(x.lib)
     stream = torch.cuda.Stream()
     x.lib.xpbd_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
-    x.lib.xpbd_b200_set_fused(2)                     # the autotuner picks the step form (same results)
+    # the autotuner picks the step form (same results); a profiler's serialised launches
+    # distort its trial timings, so captures fix the form with --form sequence
+    x.lib.xpbd_b200_set_fused(2 if args.form == "auto" else 0)
     scen.setup(x)
     run_frames(x, scen, 1, blocking=True)            # upload + build (not timed)
     with torch.cuda.stream(stream):
@@ -758,9 +760,9 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
     """Poisson session arrivals at 200/s (5e3-5e5 Gaussians, 1-120 frames of 10 substeps x
     4 iterations) served with continuous batching in one arena, against one session at a
     time.  Sessions are admitted by the 150 GB HBM budget and, in the latency-bound run,
-    also while the arena's predicted tick stays within three quarters of a 60 Hz frame
-    (12.5 ms: the rest of the frame absorbs admission copies and host work, so that
-    step latencies stay within the frame); the others wait in arrival order.  Scenes come from a pool of 12 pre-generated sizes
+    also while the arena's predicted tick stays within 60 % of a 60 Hz frame (10 ms: the
+    rest of the frame absorbs admission copies and host work, so that step latencies
+    stay within the frame); the others wait in arrival order.  Scenes come from a pool of 12 pre-generated sizes
     (generation is host Python and would otherwise bound the arrival rate)."""
     serve = pkg.serve
     rate = 200.0
@@ -780,7 +782,7 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
     pool.prepare_all(lib)            # each pool scene's topology, built once before the runs
     prep_s = time.perf_counter() - t0
     runs = {}
-    for name, target in (("latency_bound", 0.75 * 1000.0 / 60.0), ("hbm_bound", None)):
+    for name, target in (("latency_bound", 0.6 * 1000.0 / 60.0), ("hbm_bound", None)):
         r = serve.run_served(lib, sessions, budget_bytes=150e9, max_wall=max_wall, latency_target_ms=target,
                              keep_results=False, pool=pool)
         r.pop("sessions_done", None)
@@ -815,7 +817,7 @@ def bench_served(args, rank, world, duration=None, max_wall=None):
                                    f"built once per pool scene) before the runs ({prep_s:.1f} s); admission = a device "
                                    "copy of the pool scene's prepared engine into the arena; the plain loop steps the "
                                    "same prepared engines, reset to rest per session"},
-            "admission_target_ms": 0.75 * 1000.0 / 60.0,
+            "admission_target_ms": 0.6 * 1000.0 / 60.0,
             "served": lb, "served_hbm_bound": runs["hbm_bound"], "plain": plain,
             "plain_engine_per_session": plain_own,
             "speedup_vs_plain": (lb["gauss_substeps_per_s"] / max(plain["gauss_substeps_per_s"], 1e-9)
@@ -885,6 +887,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="large", choices=["large", "plain", "batched", "served", "chainmail", "dense", "render"])
     ap.add_argument("--cpu-substeps", type=int, default=2)
+    ap.add_argument("--form", default="auto", choices=["auto", "sequence"],
+                    help="step form: the autotuner's choice, or the kernel sequence (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="large config: skip the batched / served / reference-GPU sub-records")

@@ -226,11 +226,6 @@ XPBD_API int xpbd_b200_tuning(float* out);
  * visiting order; 0 from the reference's own 27-cell scan of the start-position hash
  * (selfColBuildKernel).  The lists are identical either way. */
 XPBD_API void xpbd_b200_set_selfcol_near(int enabled);
-/* Scenes of several objects (graph components, kept contiguous by the internal order):
- * the 4-lane volume solve and gather run chunk by chunk over whole objects of about
- * `rows` rows (default 1,048,576; 0 = one pass over the scene), so that a chunk's cluster
- * records are still in L2 when its gather reads them.  Same results either way. */
-XPBD_API void xpbd_b200_set_volume_chunk(int rows);
 /* 1 (default): keep Gaussians in Morton order inside the engine (caller order at the
  * ABI; results identical); 0: caller order.  Takes effect at the next upload. */
 XPBD_API void xpbd_b200_set_reorder(int enabled);

@@ -47,23 +47,6 @@ def test_engine_instances_are_independent():
     c.close()
 
 
-def test_volume_chunks_match_one_pass():
-    """A packed scene of several objects runs the volume solve + gather chunk by chunk
-    (whole objects per chunk); the positions equal one pass over the scene, bit for bit."""
-    objs = H.pkg.batch.make_objects(6, seed=4, n_min=1500, n_max=6000)
-    pos = {}
-    for chunk in (0, 4000):
-        c = H.pkg.bridge.XPBD(H.B200_SO, instance=True)
-        c.lib.xpbd_b200_set_volume_chunk(chunk)
-        b = H.pkg.batch.Batch(objs)
-        b.setup(c)
-        b.advance(c, 30)
-        pos[chunk] = c.positions()
-        c.lib.xpbd_b200_set_volume_chunk(1 << 20)
-        c.close()
-    np.testing.assert_array_equal(pos[4000], pos[0])
-
-
 def test_served_sessions_match_alone():
     sessions = [(0.0, 3000, 3, 101), (0.0, 5000, 2, 202), (0.01, 2000, 4, 303)]
     stats = serve.run_served(H.B200_SO, sessions, budget_bytes=1e12)
