@@ -182,10 +182,12 @@ class Scenario:
             return [], np.zeros((0, 12), np.float32), np.zeros((0, 3), np.float32)
         return [c[0] for c in cols], np.stack([c[1] for c in cols]), np.stack([c[2] for c in cols])
 
-    def frame_inputs(self, count):
+    def frame_inputs(self, count, k0=None):
         """The next ``count`` substeps' collider poses (count, K, 12) and pin targets
-        (count, P, 3), with the collider types and dims and the pinned indices."""
-        ts = [(self.k + 1 + s) / self.substeps for s in range(count)]
+        (count, P, 3), with the collider types and dims and the pinned indices; from
+        substep ``k0`` instead of the current one when given."""
+        k0 = self.k if k0 is None else k0
+        ts = [(k0 + 1 + s) / self.substeps for s in range(count)]
         types, _, dims = self.colliders(ts[0])
         poses = np.stack([self.colliders(t)[1] for t in ts]).astype(np.float32) if self.grippers \
             else np.zeros((count, 0, 12), np.float32)

@@ -207,10 +207,12 @@ def scene_pool(n_min, n_max, count=12, seed=0):
 
 def _frame_arrays(resident, substeps):
     """Collider poses and pin targets of the next frame of every resident session, as
-    the arena's step call takes them."""
+    the arena's step call takes them (a session's inputs prepared ahead, `next_inputs`,
+    are used when they are for its current substep)."""
     types, poses, dims, cslot, pslot, pidx, targets = [], [], [], [], [], [], []
     for s in resident:
-        ty, po, di, idx, tg = s.scen.frame_inputs(substeps)
+        pre = getattr(s, "next_inputs", None)
+        ty, po, di, idx, tg = pre[1] if pre is not None and pre[0] == s.scen.k else s.scen.frame_inputs(substeps)
         types.append(ty); poses.append(po); dims.append(di); cslot.append(np.full(len(ty), s.slot, np.int32))
         pidx.append(idx); targets.append(tg); pslot.append(np.full(len(idx), s.slot, np.int32))
     cat = np.concatenate
@@ -253,6 +255,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
     resident, joining = [], []
     done, work, ticks, resident_bytes, resident_gauss, queued = [], 0, 0, 0.0, 0, 0
     throughput = 2.0e8           # Gaussian-substeps/s: a prior, then the ticks' running mean
+    phase = {"admit": 0.0, "inputs": 0.0, "step_call": 0.0, "prefetch": 0.0, "sync": 0.0}   # host seconds
     waits = []
     sid = 0
     try:
@@ -296,6 +299,7 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             while not ready.empty():
                 joining.append(ready.get())
             still_joining = []
+            t_adm = time.perf_counter()
             for s in joining:
                 slot = arena.admit(s.src) if not still_joining else None
                 if slot is None:          # full until sessions leave (compaction ran already); the
@@ -310,15 +314,27 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
                 waits.append(s.pending_since - t0 - s.arrival)
                 resident.append(s)
             joining = still_joining
+            phase["admit"] += time.perf_counter() - t_adm
             if not resident:
                 time.sleep(0.001)
                 continue
             sub = resident[0].scen.substeps
+            t_in = time.perf_counter()
             ty, po, di, cs, ps, pi, tg = _frame_arrays(resident, sub)
             t_tick = time.perf_counter()
             arena.step(sub, ty, po, di, cs, ps, pi, tg)
+            t_call = time.perf_counter()
+            # while the GPU runs this tick: the next frame's inputs of the sessions that stay
+            for s in resident:
+                if s.frames_left > 1:
+                    s.next_inputs = (s.scen.k + sub, s.scen.frame_inputs(sub, s.scen.k + sub))
+            t_pre = time.perf_counter()
             arena.sync()
             t_end = time.perf_counter()
+            phase["inputs"] += t_tick - t_in
+            phase["step_call"] += t_call - t_tick
+            phase["prefetch"] += t_pre - t_call
+            phase["sync"] += t_end - t_pre
             ticks += 1
             tick_work = sum(s.n for s in resident) * sub
             rate = tick_work / max(t_end - t_tick, 1e-9)
@@ -351,7 +367,8 @@ def run_served(lib_path, sessions, budget_bytes=150e9, time_scale=1.0, max_wall=
             "gauss_substeps_per_s": work / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "admission_wait_p50_s": float(np.percentile(waits, 50)) if waits else 0.0,
-            "arena_rows_cap": usage["rows_cap"], "sessions_done": done}
+            "arena_rows_cap": usage["rows_cap"], "host_phase_s": {k: round(v, 3) for k, v in phase.items()},
+            "sessions_done": done}
 
 
 def _arrival(item):

@@ -225,7 +225,16 @@ def bench_b200(args, rank, world):
     # distort its trial timings, so captures fix the form with --form sequence
     x.lib.xpbd_b200_set_fused(2 if args.form == "auto" else 0)
     scen.setup(x)
+    t_up = time.perf_counter()
     run_frames(x, scen, 1, blocking=True)            # upload + build (not timed)
+    first_frame_s = time.perf_counter() - t_up
+    bms = np.zeros(8, np.float32)
+    x.lib.xpbd_b200_debug_float.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong]
+    x.lib.xpbd_b200_debug_float(b"build_ms", bms.ctypes.data, 8)
+    upload = {k: round(float(v), 1) for k, v in zip(("graph", "order", "state", "cluster_members", "cluster_lists",
+                                                      "sorted_lists", "rest_state", "other"), bms)}
+    upload["total"] = round(float(bms.sum()), 1)
+    upload["first_frame_s"] = round(first_frame_s, 2)
     with torch.cuda.stream(stream):
         run_frames(x, scen, args.warmup, blocking=False)
         torch.cuda.synchronize()
@@ -302,6 +311,7 @@ def bench_b200(args, rank, world):
         "e2e": {"value": n * SUBSTEPS * e2e_frames * world / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": pos_bytes, "frames": e2e_frames},
         "gpu_launches": int(launches),
+        "upload_ms": upload,
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
