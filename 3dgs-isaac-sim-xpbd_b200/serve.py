@@ -20,6 +20,7 @@ The plain form for comparison steps one session at a time, start to finish, on t
 same prepared engines (reset to rest before each session).
 """
 import collections
+import copy
 import math
 import queue
 import threading
@@ -93,7 +94,15 @@ class Session:
         else:
             sc = scenes.make_scene(self.n, self.seed, radii=radii)
         vel = (float(rng.uniform(0.002, 0.01)), 0.0, 0.0)
-        g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, math.radians(float(rng.uniform(-1, 1))))
+        twist = math.radians(float(rng.uniform(-1, 1)))
+        cached = pool.grippers.get(self.pool_index) if isinstance(pool, ScenePool) else None
+        if cached is None:
+            g = scenes.Gripper(sc["pos"], (0.8 * radii[0], 0.0, 0.0), 20, vel, twist)
+            if isinstance(pool, ScenePool):
+                pool.grippers[self.pool_index] = g
+        # the pinned set depends on the scene only: sessions of one pool scene share it
+        g = copy.copy(pool.grippers[self.pool_index]) if isinstance(pool, ScenePool) else g
+        g.velocity, g.twist = np.asarray(vel, dtype=np.float64), float(twist)
         self.scen = scenes.Scenario(sc, [g], substeps=self.substeps, iters=self.iters)
 
     def fresh_scenario(self):
@@ -167,6 +176,7 @@ class ScenePool(list):
         super().__init__(items)
         self.substeps, self.iters = substeps, iters
         self.engines = {}
+        self.grippers = {}   # pool index -> gripper with the pinned set (the same for every session)
 
     def index_for(self, n):
         sizes = np.array([p["pos"].shape[0] for p in self], np.float64)
