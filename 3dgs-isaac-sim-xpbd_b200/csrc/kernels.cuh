@@ -1527,24 +1527,30 @@ __device__ __forceinline__ bool shape_rotation_double_warm(const M3& A, M3& Rout
 	}
 	{
 		// the converged frame (a proper rotation: products of rotations), as a unit
-		// quaternion for the next call (largest-component extraction)
-		const double tr = v[0][0] + v[1][1] + v[2][2];
-		double qw, qx, qy, qz;
-		if (tr > 0.0) {
-			const double s2 = 2.0 * sqrt(1.0 + tr);
-			qw = 0.25 * s2; qx = (v[2][1] - v[1][2]) / s2; qy = (v[0][2] - v[2][0]) / s2; qz = (v[1][0] - v[0][1]) / s2;
-		} else if (v[0][0] > v[1][1] && v[0][0] > v[2][2]) {
-			const double s2 = 2.0 * sqrt(fmax(1.0 + v[0][0] - v[1][1] - v[2][2], 1e-30));
-			qw = (v[2][1] - v[1][2]) / s2; qx = 0.25 * s2; qy = (v[0][1] + v[1][0]) / s2; qz = (v[0][2] + v[2][0]) / s2;
-		} else if (v[1][1] > v[2][2]) {
-			const double s2 = 2.0 * sqrt(fmax(1.0 + v[1][1] - v[0][0] - v[2][2], 1e-30));
-			qw = (v[0][2] - v[2][0]) / s2; qx = (v[0][1] + v[1][0]) / s2; qy = 0.25 * s2; qz = (v[1][2] + v[2][1]) / s2;
+		// quaternion for the next call (largest-component extraction).  Kept in FP32: it
+		// only seeds the next call's Jacobi (re-normalised in FP64 there), whose stop test
+		// decides the result
+		float f[3][3];
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+#pragma unroll
+			for (int c = 0; c < 3; ++c) f[r][c] = (float)v[r][c];
+		const float tr = f[0][0] + f[1][1] + f[2][2];
+		float qw, qx, qy, qz;
+		if (tr > 0.0f) {
+			const float s2 = 2.0f * sqrtf(1.0f + tr), r2 = 1.0f / s2;
+			qw = 0.25f * s2; qx = (f[2][1] - f[1][2]) * r2; qy = (f[0][2] - f[2][0]) * r2; qz = (f[1][0] - f[0][1]) * r2;
+		} else if (f[0][0] > f[1][1] && f[0][0] > f[2][2]) {
+			const float s2 = 2.0f * sqrtf(fmaxf(1.0f + f[0][0] - f[1][1] - f[2][2], 1e-30f)), r2 = 1.0f / s2;
+			qw = (f[2][1] - f[1][2]) * r2; qx = 0.25f * s2; qy = (f[0][1] + f[1][0]) * r2; qz = (f[0][2] + f[2][0]) * r2;
+		} else if (f[1][1] > f[2][2]) {
+			const float s2 = 2.0f * sqrtf(fmaxf(1.0f + f[1][1] - f[0][0] - f[2][2], 1e-30f)), r2 = 1.0f / s2;
+			qw = (f[0][2] - f[2][0]) * r2; qx = (f[0][1] + f[1][0]) * r2; qy = 0.25f * s2; qz = (f[1][2] + f[2][1]) * r2;
 		} else {
-			const double s2 = 2.0 * sqrt(fmax(1.0 + v[2][2] - v[0][0] - v[1][1], 1e-30));
-			qw = (v[1][0] - v[0][1]) / s2; qx = (v[0][2] + v[2][0]) / s2; qy = (v[1][2] + v[2][1]) / s2; qz = 0.25 * s2;
+			const float s2 = 2.0f * sqrtf(fmaxf(1.0f + f[2][2] - f[0][0] - f[1][1], 1e-30f)), r2 = 1.0f / s2;
+			qw = (f[1][0] - f[0][1]) * r2; qx = (f[0][2] + f[2][0]) * r2; qy = (f[1][2] + f[2][1]) * r2; qz = 0.25f * s2;
 		}
-		warm = isfinite(qw + qx + qy + qz) ? make_float4((float)qw, (float)qx, (float)qy, (float)qz)
-			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		warm = isfinite(qw + qx + qy + qz) ? make_float4(qw, qx, qy, qz) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	}
 	double ev[3] = { m[0][0], m[1][1], m[2][2] };
 #pragma unroll
@@ -1556,12 +1562,17 @@ __device__ __forceinline__ bool shape_rotation_double_warm(const M3& A, M3& Rout
 #pragma unroll
 				for (int rr = 0; rr < 3; ++rr) { const double tv = v[rr][i]; v[rr][i] = v[rr][j]; v[rr][j] = tv; }
 			}
+	// singular values and their inverses from one reciprocal square root each (in place
+	// of a square root and a division: equal to FP64 rounding)
 	double S[3], Si[3];
 #pragma unroll
-	for (int i = 0; i < 3; ++i) S[i] = sqrt(ev[i] > 0.0 ? ev[i] : 0.0);
+	for (int i = 0; i < 3; ++i) {
+		Si[i] = ev[i] > 0.0 ? rsqrt(ev[i]) : 0.0;
+		S[i] = ev[i] > 0.0 ? ev[i] * Si[i] : 0.0;
+	}
 	const double smax = (S[2] > 1e-300) ? S[2] : 1e-300;
 #pragma unroll
-	for (int i = 0; i < 3; ++i) Si[i] = (S[i] > 1e-12 * smax) ? 1.0 / S[i] : 0.0;
+	for (int i = 0; i < 3; ++i) Si[i] = (S[i] > 1e-12 * smax) ? Si[i] : 0.0;
 	double u[3][3];
 #pragma unroll
 	for (int r = 0; r < 3; ++r)
