@@ -200,6 +200,13 @@ def algorithmic_bytes(stage, sizes, n):
     return None if per is None else per * n
 
 
+def workload_config(name, n, scen, edges_directed, members, hash_table, world):
+    """The line's `config`, the same for both arms of the single-scene workloads."""
+    return {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": scen.iters,
+            "graph_edges_directed": edges_directed, "cluster_members": members, "hash_table": hash_table,
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (working set > 2 GB per replica)"}
+
+
 def max_over_ranks(values, world, device):
     """Element-wise maximum of `values` over all ranks (the job's time is its slowest rank's)."""
     if world <= 1:
@@ -304,10 +311,7 @@ def bench_b200(args, rank, world):
         "metric": metric_for(args.config, n), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid scene; no public dataset)",
-        "config": {"workload": name, "n_gaussians": n, "substeps_per_step": SUBSTEPS, "iterations": scen.iters,
-                   "graph_edges_directed": int(sizes[1]), "cluster_members": int(sizes[2]),
-                   "hash_table": int(sizes[8]), "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (working set > 2 GB per replica)"},
+        "config": workload_config(name, n, scen, int(sizes[1]), int(sizes[2]), int(sizes[8]), world),
         "e2e": {"value": n * SUBSTEPS * e2e_frames * world / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": pos_bytes, "frames": e2e_frames},
         "gpu_launches": int(launches),
@@ -858,13 +862,24 @@ def bench_reference(args, rank, world):
     dt = time.perf_counter() - t0
     cores = int(o.lib.oracle_get_threads())
     value = scen.n * steps / dt
+    n = scen.n
+    f = o.lib.oracle_int
+    f.argtypes, f.restype = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong], ctypes.c_int
+    cnt = np.zeros(max(f(b"vol_count", None, 0), 1), np.int32)
+    f(b"vol_count", cnt.ctypes.data, cnt.size)
+    members = int(cnt.astype(np.int64).sum())
+    table = 1024
+    while table < 2 * n:
+        table <<= 1
+    cfg = workload_config(name, n, scen, 2 * len(scen.scene["edges"]), members, table if scen.self_collision else 0,
+                          world)
     o.destroy()
-    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
-            "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid scene)",
-            "config": {"workload": name, "step": "one substep (CPU sample of the workload)"},
+    return {"impl": "reference", "metric": metric_for(args.config, n), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid scene; no public dataset)", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{steps} substeps of the {scen.n}-Gaussian workload"},
+                             "sample": f"{steps} substeps (one per step) of the {n}-Gaussian workload"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
