@@ -1364,9 +1364,22 @@ __device__ __forceinline__ void jacobi_rotate_d(double (&m)[3][3], double (&v)[3
 {
 	constexpr int r = 3 - p - q;
 	const double app = m[p][p], aqq = m[q][q], apq = m[p][q];
-	const double phi = 0.5 * (aqq - app) / (apq + 1e-300);
-	const double t = (phi >= 0.0) ? 1.0 / (phi + sqrt(1.0 + phi * phi)) : 1.0 / (phi - sqrt(1.0 + phi * phi));
-	const double c = 1.0 / sqrt(1.0 + t * t);
+	// t = sgn(phi) / (|phi| + sqrt(1 + phi^2)) with phi = (aqq - app) / (2 apq'), apq' =
+	// apq + 1e-300, written as 2 |apq'| sgn / (|d| + sqrt(d^2 + 4 apq'^2)), d = aqq - app:
+	// one division and one square root instead of two each (c from a reciprocal square
+	// root).  Where d and apq' are both so small that their squares would underflow, the
+	// phi form.
+	const double d = aqq - app, h = apq + 1e-300;
+	double t;
+	if (fabs(d) > 1e-140 || fabs(h) > 1e-140) {
+		const double sgn = (d == 0.0 || (d > 0.0) == (h > 0.0)) ? 1.0 : -1.0;
+		t = sgn * (2.0 * fabs(h)) / (fabs(d) + sqrt(d * d + 4.0 * h * h));
+	}
+	else {
+		const double phi = 0.5 * d / h;
+		t = (phi >= 0.0) ? 1.0 / (phi + sqrt(1.0 + phi * phi)) : 1.0 / (phi - sqrt(1.0 + phi * phi));
+	}
+	const double c = rsqrt(1.0 + t * t);
 	const double s = t * c;
 	m[p][p] = app - t * apq;
 	m[q][q] = aqq + t * apq;
