@@ -1129,7 +1129,7 @@ public:
 	// the c.z column of the cluster records (after the 2 x rows float4 of M and c.xy; rows =
 	// the scene's Gaussians, or an arena's capacity)
 	float* recz() const { return reinterpret_cast<float*>(rec.p + 2 * rec_rows()); }
-	// record slots: the rows rounded up to the 8-record blocks of the interleaved halves
+	// record slots: the rows rounded up to a multiple of 8
 	size_t rec_rows() const { return ((size_t)(arena ? rows_cap : n) + 7) & ~(size_t)7; }
 
 	bool use_warp() const
@@ -3103,7 +3103,7 @@ XPBD_API int xpbd_b200_debug_float(const char* name, float* out, long long cap)
 		if (copy_dev(E.rec.p, slots, tmp.data(), slots, E.stream) < 0) return -1;
 		std::vector<float> v(N);
 		for (int r = 0; r < N; ++r) {
-			const size_t b = ((size_t)(r >> 3) << 4) | (size_t)(r & 7) | 8;   // the record's second half
+			const size_t b = 2 * (size_t)r + 1;   // the record's second half
 			v[E.perm[r]] = std::isfinite(tmp[b].z) ? 1.0f : 0.0f;
 		}
 		return copy_host(v, (long long)v.size(), out, cap);

@@ -432,16 +432,25 @@ __device__ __forceinline__ bool cluster_j_sinv(const M3& Scur, float det_rest, f
 	return inverse3x3_safe(Sreg, Sinv, 1e-20f);
 }
 
-// Cluster blackboard record, 36 bytes in two places so that a record read touches one
-// 16-byte halves plus a 4-byte entry: rec[rec_a(i)] = (M00, M11, M22, M01), rec[rec_b(i)] =
-// (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float array recz[i].  A record
-// the gather must skip (the reference's coef == 0) has c.x = NaN.
-// The two halves of records are interleaved in blocks of 8 records (the 8 first halves,
-// then the 8 second halves): a 128-byte line holds the same half of 8 neighbouring
-// clusters, which the lanes of a gather warp, walking Morton-sorted lists, often load
-// together.
-__device__ __forceinline__ int rec_a(int i) { return ((i >> 3) << 4) | (i & 7); }
-__device__ __forceinline__ int rec_b(int i) { return rec_a(i) | 8; }
+// Cluster blackboard record, 36 bytes: one aligned 32-byte sector rec[2i], rec[2i + 1] =
+// (M00, M11, M22, M01), (M02, M12, c.x, c.y) with M = coef Sinv, and c.z in the float
+// array recz[i].  A record the gather must skip (the reference's coef == 0) has c.x =
+// NaN.  The gather fetches the sector with one 256-bit load (ld.global.v8.f32, sm_100).
+__device__ __forceinline__ int rec_a(int i) { return 2 * i; }
+__device__ __forceinline__ int rec_b(int i) { return 2 * i + 1; }
+// both halves of record i in one 256-bit load; NC: read-only path (records written by an
+// earlier launch), else a coherent load (records written earlier in the same launch)
+template <bool NC>
+__device__ __forceinline__ void ld_rec(const float4* rec, int i, float4& a, float4& b)
+{
+	const float4* p = rec + 2 * (size_t)i;
+	if (NC)
+		asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+			: "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w) : "l"(p));
+	else
+		asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+			: "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w) : "l"(p) : "memory");
+}
 __device__ __forceinline__ void rec_invalidate(float4* rec, int idx) { rec[rec_b(idx)].z = __int_as_float(0x7fc00000); }
 __device__ __forceinline__ void store_record(float4* rec, float* recz, int idx, float3 c, float coef, const M3& S)
 {
@@ -1117,8 +1126,8 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 		float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b0 = a0, a1 = a0, b1 = a0;
 		float z0 = 0.0f, z1 = 0.0f;
 		const float* cz = recz;
-		if (ok0) { a0 = ldv<NC>(rec, rec_a(i0)); b0 = ldv<NC>(rec, rec_b(i0)); z0 = ldv<NC>(cz, i0); }
-		if (ok1) { a1 = ldv<NC>(rec, rec_a(i1)); b1 = ldv<NC>(rec, rec_b(i1)); z1 = ldv<NC>(cz, i1); }
+		if (ok0) { ld_rec<NC>(rec, i0, a0, b0); z0 = ldv<NC>(cz, i0); }
+		if (ok1) { ld_rec<NC>(rec, i1, a1, b1); z1 = ldv<NC>(cz, i1); }
 		float3 dp;
 		if (ok0 && gather_rec(a0, b0, z0, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
 		if (ok1 && gather_rec(a1, b1, z1, pi, wi, dp)) { sum = add3(sum, dp); ++received; }
@@ -1126,7 +1135,9 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	if (k < cnt) {
 		const int i = __ldg(ridx + off + k);
 		float3 dp;
-		if (i >= 0 && i < n && gather_rec(ldv<NC>(rec, rec_a(i)), ldv<NC>(rec, rec_b(i)), ldv<NC>(recz, i), pi, wi, dp)) {
+		float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a;
+		if (i >= 0 && i < n) ld_rec<NC>(rec, i, a, b);
+		if (i >= 0 && i < n && gather_rec(a, b, ldv<NC>(recz, i), pi, wi, dp)) {
 			sum = add3(sum, dp);
 			++received;
 		}
