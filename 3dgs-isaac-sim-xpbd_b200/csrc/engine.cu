@@ -1231,7 +1231,7 @@ public:
 			launch(ST_SC_BUILD, dim3(1), dim3(1024), dev::k_scan_sums, sc_block_sums.p, fnb);
 			launch(ST_SC_BUILD, dim3(fnb), dim3(1024), dev::k_scan_add, nf_start.p, fscan, (const int*)sc_block_sums.p);
 			launch(ST_SC_BUILD, G, B, dev::k_sc_near_scatter, N, (const unsigned*)nf_keys.p, (const int*)nf_start.p,
-				nf_bucket.p, (const float4*)pos_next.p, nf_p.p);
+				nf_bucket.p, (const float4*)pos_next.p, nf_p.p, sc_counts.p);
 			launch(ST_SC_BUILD, G, B, dev::k_sc_build_near, N, (const StepParams*)d_params, (const float4*)pos_curr.p,
 				(const float4*)pos_next.p, (const float4*)pos_rest.p, active, (const int*)nf_start.p, mask,
 				(const float4*)nf_p.p, (const int*)d_perm.p, d_ctr, sc_contacts.p, sc_counts.p);

@@ -2508,14 +2508,16 @@ __global__ void __launch_bounds__(kBlock) k_sc_near_keys(int n, const float4* __
 }
 
 // scatter predicted position + index into the cells (order within a cell is free: the
-// lists are ordered by key afterwards); leaves the cell counts at zero
+// lists are ordered by key afterwards); leaves the cell counts at zero; a particle outside
+// the grid gets its empty candidate list here
 __global__ void __launch_bounds__(kBlock) k_sc_near_scatter(int n, const unsigned int* __restrict__ keys,
-	const int* __restrict__ start, int* __restrict__ bucket, const float4* __restrict__ Pp, float4* __restrict__ fp)
+	const int* __restrict__ start, int* __restrict__ bucket, const float4* __restrict__ Pp, float4* __restrict__ fp,
+	int* __restrict__ counts)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	const unsigned int k = keys[i];
-	if (k == 0xffffffffu) return;
+	if (k == 0xffffffffu) { counts[i] = 0; return; }
 	const int pos = start[k] + atomicSub(&bucket[k], 1) - 1;
 	const float4 p = Pp[i];
 	fp[pos] = make_float4(p.x, p.y, p.z, __int_as_float(i));
@@ -2534,18 +2536,21 @@ __device__ __forceinline__ unsigned long long sc_near_key(const Hash27& Href, fl
 }
 
 // mask: the reference's hash table mask (for the keys); start_f / fp: the dense grid's
-// cell starts and (p, index) by cell
+// cell starts and (p, index) by cell.  Thread t takes the t-th particle in cell order, so
+// the lanes of a warp share cells and row ranges and run even trip counts (particles
+// outside the grid got their zero count from k_sc_near_scatter).
 __global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
 	const unsigned char* __restrict__ active, const int* __restrict__ start_f, unsigned int mask,
 	const float4* __restrict__ fp, const int* __restrict__ perm, DevCounters* __restrict__ ctr,
 	int* __restrict__ contacts, int* __restrict__ counts)
 {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= start_f[ctr->nb_dim[0] * ctr->nb_dim[1] * ctr->nb_dim[2]]) return;
+	const int i = __float_as_int(fp[t].w);
 	int cnt = 0, over = 0;
 	const float4 x = X[i], p = Pp[i];
-	if (P->sc_within && sc_near_member(x, p, active, i)) {
+	if (P->sc_within) {
 		const float search = P->sc_search, excl2 = P->sc_excl2;
 		const float search2 = search * search;
 		const float4 q = rest[i];
