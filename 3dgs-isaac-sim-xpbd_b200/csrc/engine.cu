@@ -100,6 +100,20 @@ struct DBuf {
 	size_t bytes() const { return sizeof(T) * n; }
 };
 
+// Rows [0, n) in chunks of 256, each chunk sorted by row length (longest first): the
+// groups of a warp then run rows of similar length, and the chunk keeps them local
+static std::vector<int> length_order(int n, const std::vector<int>& off)
+{
+	std::vector<int> ord(n);
+	for (int r = 0; r < n; ++r) ord[r] = r;
+	for (int c0 = 0; c0 < n; c0 += 256) {
+		const int c1 = std::min(n, c0 + 256);
+		std::stable_sort(ord.begin() + c0, ord.begin() + c1,
+			[&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
+	}
+	return ord;
+}
+
 // Solver settings.  Like the reference's file-static settings (forward.cu:53-92,
 // 224-265, 300-361) they outlive create/destroy; defaults are the reference's.
 struct Settings {
@@ -254,6 +268,7 @@ public:
 	DBuf<float> ndist, nstiff, lam;
 	DBuf<int> vol_off, vol_idx, rev_off, rev_idx, mat_type, vol_gs_order;
 	DBuf<int> vol_idx_s, rev_idx_s;  // the same lists, rows sorted along the Morton curve
+	DBuf<int> gather_order;          // gather group -> node: nodes of similar reverse-list length side by side
 	DBuf<float> det_rest, v_rest, rest_len, sigma_rest, lam_vol;
 	DBuf<float4> rec;
 	DBuf<int2> gs_edge;
@@ -451,7 +466,7 @@ public:
 		obj_shift_valid = false;
 		pos_out3.release(); off.release(); nbr.release(); ndist.release(); nstiff.release(); lam.release();
 		vol_off.release(); vol_idx.release(); rev_off.release(); rev_idx.release(); mat_type.release();
-		vol_idx_s.release(); rev_idx_s.release();
+		vol_idx_s.release(); rev_idx_s.release(); gather_order.release();
 		vol_gs_order.release(); det_rest.release(); v_rest.release(); rest_len.release(); sigma_rest.release();
 		lam_vol.release(); rec.release(); gs_edge.release(); gs_rest.release(); gs_stiff.release(); gs_lam.release();
 		sc_keys.release(); sc_bucket.release(); sc_start.release(); sc_cursor.release(); sc_idx_sorted.release();
@@ -734,6 +749,12 @@ public:
 			CK(vol_idx_s.alloc(vs.size())); CK(rev_idx_s.alloc(rs.size()));
 			CK(cudaMemcpyAsync(vol_idx_s.p, vs.data(), sizeof(int) * vs.size(), cudaMemcpyHostToDevice, stream));
 			CK(cudaMemcpyAsync(rev_idx_s.p, rs.data(), sizeof(int) * rs.size(), cudaMemcpyHostToDevice, stream));
+			{
+				const std::vector<int> ord = length_order(n, roff_i);
+				CK(gather_order.alloc(n));
+				CK(cudaMemcpyAsync(gather_order.p, ord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+				CK(cudaStreamSynchronize(stream));
+			}
 			CK(cudaStreamSynchronize(stream));
 			build_mark(5);
 		}
@@ -1414,15 +1435,15 @@ public:
 							(const int*)vol_idx.p, (const float*)det_rest.p, (const int*)mat_type.p, lam_vol.p, rec.p, recz(), rl);
 					if (lb == 32)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 32), B, dev::k_volume_gather_group<32>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p, (const int*)gather_order.p);
 					else if (lb == 8)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 8), B, dev::k_volume_gather_group<8>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p, (const int*)gather_order.p);
 					else if (lb == 4)
 						launch(ST_VOL_GATHER, blocks_for((long long)N * 4), B,
 							occ == 8 ? dev::k_volume_gather_occ<4, 8> : occ == 6 ? dev::k_volume_gather_occ<4, 6>
 							: dev::k_volume_gather_group<4>, N, dp, cpin,
-							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);
+							pout, (const int*)rev_off.p, (const int*)rev_idx_s.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p, (const int*)gather_order.p);
 					else
 						launch(ST_VOL_GATHER, G, B, dev::k_volume_gather_thread, N, dp, cpin, pout, (const int*)rev_off.p,
 							(const int*)rev_idx.p, (const float4*)rec.p, (const float*)recz(), (const float*)rest_len.p);

@@ -1152,13 +1152,20 @@ __device__ __forceinline__ void gather_group_lane(long long gtid, int n, const S
 	const float3 o = gather_finish(pi, avg, __ldg(rest_len + idx), P->under_relax);
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
+// node of gather group g: order[g] when an order is given (nodes of similar reverse-list
+// length side by side, so the groups of a warp run even trip counts)
+__device__ __forceinline__ int ordered_node(const int* __restrict__ order, int g, int n)
+{
+	return (order && g < n) ? __ldg(order + g) : g;
+}
 template <int S>
 __global__ void __launch_bounds__(kBlock) k_volume_gather_group(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
-	const float* __restrict__ rest_len)
+	const float* __restrict__ rest_len, const int* __restrict__ order)
 {
-	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+	const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	gather_group_lane<S, true>((long long)ordered_node(order, (int)(g / S), n) * S + (g & (S - 1)), n, P, pin, pout,
 		roff, ridx, rec, recz, rest_len);
 }
 
@@ -1169,9 +1176,10 @@ template <int S, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) k_volume_gather_occ(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const int* __restrict__ roff,
 	const int* __restrict__ ridx, const float4* __restrict__ rec, const float* __restrict__ recz,
-	const float* __restrict__ rest_len)
+	const float* __restrict__ rest_len, const int* __restrict__ order)
 {
-	gather_group_lane<S, true>((long long)blockIdx.x * blockDim.x + threadIdx.x, n, P, pin, pout,
+	const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	gather_group_lane<S, true>((long long)ordered_node(order, (int)(g / S), n) * S + (g & (S - 1)), n, P, pin, pout,
 		roff, ridx, rec, recz, rest_len);
 }
 
