@@ -892,14 +892,21 @@ __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const 
 	}
 	const float3 pi = f3(p4);
 	const float ims = P->inv_mass_scale;
-	// m[0..9]: count, d, d d^T (xx yy zz xy xz yz); m[10..19]: the same weighted by w
+	// m[0..9]: count, d, d d^T (xx yy zz xy xz yz); m[10..19]: the same weighted by w.
+	// The weighted sums are formed in a second pass over the members only when their
+	// inverse masses differ; otherwise they are w times the plain ones
 	float m[20];
 #pragma unroll
 	for (int t = 0; t < 20; ++t) m[t] = 0.0f;
+	float wmin = INFINITY, wmax = -INFINITY;
 	auto add = [&](float4 q) {
 		const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z, w = q.w * ims;
 		m[0] += 1.0f; m[1] += dx; m[2] += dy; m[3] += dz;
 		m[4] += dx * dx; m[5] += dy * dy; m[6] += dz * dz; m[7] += dx * dy; m[8] += dx * dz; m[9] += dy * dz;
+		wmin = fminf(wmin, w); wmax = fmaxf(wmax, w);
+	};
+	auto add_w = [&](float4 q) {
+		const float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z, w = q.w * ims;
 		m[10] += w; m[11] += w * dx; m[12] += w * dy; m[13] += w * dz;
 		m[14] += w * dx * dx; m[15] += w * dy * dy; m[16] += w * dz * dz;
 		m[17] += w * dx * dy; m[18] += w * dx * dz; m[19] += w * dy * dz;
@@ -919,7 +926,27 @@ __device__ __forceinline__ void solve_onepass_lane(long long gtid, int n, const 
 		if (j >= 0 && j < n) add(ldv<NC>(pin, j));
 	}
 #pragma unroll
-	for (int t = 0; t < 20; ++t) m[t] = group_sum<S>(m[t]);
+	for (int t = 0; t < 10; ++t) m[t] = group_sum<S>(m[t]);
+#pragma unroll
+	for (int o = 1; o < S; o <<= 1) {
+		wmin = fminf(wmin, __shfl_xor_sync(0xffffffffu, wmin, o, S));
+		wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o, S));
+	}
+	const bool mixed = wmin < wmax;   // warp-uniform second pass (full-warp shuffles)
+	if (__any_sync(0xffffffffu, mixed)) {
+		if (mixed)
+			for (int k2 = sl; k2 < cnt; k2 += S) {
+				const int j = __ldg(vidx + off + k2);
+				if (j >= 0 && j < n) add_w(ldv<NC>(pin, j));
+			}
+#pragma unroll
+		for (int t = 10; t < 20; ++t) m[t] = group_sum<S>(m[t]);
+	}
+	if (!mixed) {   // one inverse mass over the members (or no member)
+		const float w0 = wmin <= wmax ? wmin : 0.0f;
+#pragma unroll
+		for (int t = 0; t < 10; ++t) m[10 + t] = w0 * m[t];
+	}
 	const int used = (int)(m[0] + 0.5f);
 	valid = valid && used >= 3;
 	const float inv_n = 1.0f / (float)(used + 1);
