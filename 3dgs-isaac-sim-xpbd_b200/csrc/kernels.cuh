@@ -1911,36 +1911,38 @@ __device__ __forceinline__ void project_row(int idx, int n, const StepParams* __
 			const KinCollider& C = cols[c];
 			if (C.obj >= 0 && C.obj != my_obj) continue;
 			const float dx = p.x - C.t[0], dy = p.y - C.t[1], dz = p.z - C.t[2];
-			const float q0 = C.R[0] * dx + C.R[3] * dy + C.R[6] * dz;
-			const float q1 = C.R[1] * dx + C.R[4] * dy + C.R[7] * dz;
-			const float q2 = C.R[2] * dx + C.R[5] * dy + C.R[8] * dz;
-			float n0 = 0.0f, n1 = 0.0f, n2 = 1.0f, dist;
-			if (C.type == 1) {
-				const float a0 = fabsf(q0) - C.h[0], a1 = fabsf(q1) - C.h[1], a2 = fabsf(q2) - C.h[2];
-				if (a0 > 0.0f || a1 > 0.0f || a2 > 0.0f) {
-					const float o0 = fmaxf(a0, 0.0f), o1 = fmaxf(a1, 0.0f), o2 = fmaxf(a2, 0.0f);
-					dist = sqrtf(o0 * o0 + o1 * o1 + o2 * o2);
+			const float lx = C.R[0] * dx + C.R[3] * dy + C.R[6] * dz;
+			const float ly = C.R[1] * dx + C.R[4] * dy + C.R[7] * dz;
+			const float lz = C.R[2] * dx + C.R[5] * dy + C.R[8] * dz;
+			// (lx, ly, lz): the point in the collider frame; (nx, ny, nz): the outward normal
+			// there; dist: the signed distance to the surface
+			float nx = 0.0f, ny = 0.0f, nz = 1.0f, dist;
+			if (C.type == 1) {   // box: excess over the half extents, its positive part outside
+				const float ex = fabsf(lx) - C.h[0], ey = fabsf(ly) - C.h[1], ez = fabsf(lz) - C.h[2];
+				if (ex > 0.0f || ey > 0.0f || ez > 0.0f) {
+					const float bx = fmaxf(ex, 0.0f), by = fmaxf(ey, 0.0f), bz = fmaxf(ez, 0.0f);
+					dist = sqrtf(bx * bx + by * by + bz * bz);
 					if (dist >= reach) continue;
 					const float inv = 1.0f / fmaxf(dist, 1e-20f);
-					n0 = copysignf(o0 * inv, q0); n1 = copysignf(o1 * inv, q1); n2 = copysignf(o2 * inv, q2);
+					nx = copysignf(bx * inv, lx); ny = copysignf(by * inv, ly); nz = copysignf(bz * inv, lz);
 				}
 				else {
-					if (a0 >= a1 && a0 >= a2) { dist = a0; n0 = (q0 >= 0.0f) ? 1.0f : -1.0f; n2 = 0.0f; }
-					else if (a1 >= a2) { dist = a1; n1 = (q1 >= 0.0f) ? 1.0f : -1.0f; n2 = 0.0f; }
-					else { dist = a2; n2 = (q2 >= 0.0f) ? 1.0f : -1.0f; }
+					if (ex >= ey && ex >= ez) { dist = ex; nx = (lx >= 0.0f) ? 1.0f : -1.0f; nz = 0.0f; }
+					else if (ey >= ez) { dist = ey; ny = (ly >= 0.0f) ? 1.0f : -1.0f; nz = 0.0f; }
+					else { dist = ez; nz = (lz >= 0.0f) ? 1.0f : -1.0f; }
 				}
 			}
-			else {
-				float e2 = q2;
-				if (C.type == 2) e2 = q2 - fminf(fmaxf(q2, -C.h[1]), C.h[1]);
-				const float r = sqrtf(q0 * q0 + q1 * q1 + e2 * e2);
-				dist = r - C.h[0];
+			else {   // sphere (type 0) or capsule (type 2: segment along local z, half length h[1])
+				float az = lz;
+				if (C.type == 2) az = lz - fminf(fmaxf(lz, -C.h[1]), C.h[1]);
+				const float rad = sqrtf(lx * lx + ly * ly + az * az);
+				dist = rad - C.h[0];
 				if (dist >= reach) continue;
-				if (r > 1e-20f) { n0 = q0 / r; n1 = q1 / r; n2 = e2 / r; }
+				if (rad > 1e-20f) { nx = lx / rad; ny = ly / rad; nz = az / rad; }
 			}
-			const float wx = C.R[0] * n0 + C.R[1] * n1 + C.R[2] * n2;
-			const float wy = C.R[3] * n0 + C.R[4] * n1 + C.R[5] * n2;
-			const float wz = C.R[6] * n0 + C.R[7] * n1 + C.R[8] * n2;
+			const float wx = C.R[0] * nx + C.R[1] * ny + C.R[2] * nz;
+			const float wy = C.R[3] * nx + C.R[4] * ny + C.R[5] * nz;
+			const float wz = C.R[6] * nx + C.R[7] * ny + C.R[8] * nz;
 			if (crmax && rmax > 0.0f) {   // the ellipsoid reaches that much closer along the normal
 				dist -= contact_support(cshape[2 * idx], cshape[2 * idx + 1], wx, wy, wz);
 				if (dist >= margin) continue;
@@ -1952,9 +1954,9 @@ __device__ __forceinline__ void project_row(int idx, int n, const StepParams* __
 			float3 dp = make_float3(__fmul_rn(wx, corr), __fmul_rn(wy, corr), __fmul_rn(wz, corr));
 			p.x = __fadd_rn(p.x, dp.x); p.y = __fadd_rn(p.y, dp.y); p.z = __fadd_rn(p.z, dp.z);
 			if (mu > 0.0f) {
-				const float ox = C.Rp[0] * q0 + C.Rp[1] * q1 + C.Rp[2] * q2 + C.tp[0];
-				const float oy = C.Rp[3] * q0 + C.Rp[4] * q1 + C.Rp[5] * q2 + C.tp[1];
-				const float oz = C.Rp[6] * q0 + C.Rp[7] * q1 + C.Rp[8] * q2 + C.tp[2];
+				const float ox = C.Rp[0] * lx + C.Rp[1] * ly + C.Rp[2] * lz + C.tp[0];
+				const float oy = C.Rp[3] * lx + C.Rp[4] * ly + C.Rp[5] * lz + C.tp[1];
+				const float oz = C.Rp[6] * lx + C.Rp[7] * ly + C.Rp[8] * lz + C.tp[2];
 				const float4 x0 = pos_start[idx];
 				const float rx = (p.x - x0.x) - (p_in.x - ox), ry = (p.y - x0.y) - (p_in.y - oy),
 					rz = (p.z - x0.z) - (p_in.z - oz);
