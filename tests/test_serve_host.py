@@ -53,3 +53,33 @@ def test_frame_arrays_cover_every_session():
         np.testing.assert_array_equal(pi[p0:p0 + m], idx1)
         assert (ps[p0:p0 + m] == s.slot).all()
         c0, p0 = c0 + k, p0 + m
+
+
+def test_pool_sessions_share_the_pinned_set_not_the_motion():
+    """Sessions of one pool scene share the gripper's pinned set (computed once per pool
+    scene) but keep their own velocity and twist; the inputs equal those of a session
+    whose gripper was built from scratch."""
+    pool = serve.scene_pool(500, 2000, count=2)
+    a = serve.Session(0, 0.0, 2000, 3, 21)
+    b = serve.Session(1, 0.0, 2000, 3, 22)
+    a.prepare(pool)
+    b.prepare(pool)
+    ga, gb = a.scen.grippers[0], b.scen.grippers[0]
+    assert ga.idx is gb.idx and ga is not gb
+    assert not np.array_equal(ga.velocity, gb.velocity) or ga.twist != gb.twist
+    own = serve.Session(2, 0.0, 2000, 3, 22)
+    own.prepare(list(pool))                            # a plain list: gripper built from scratch
+    for x, y in zip(b.scen.frame_inputs(10), own.scen.frame_inputs(10)):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_prefetched_inputs_equal_the_next_frame():
+    """The next tick's inputs prepared while the GPU runs the current one are those the
+    session's frame call makes when its substep counter arrives there."""
+    pool = serve.scene_pool(500, 2000, count=2)
+    s = serve.Session(0, 0.0, 1500, 4, 5)
+    s.prepare(pool)
+    ahead = s.scen.frame_inputs(10, s.scen.k + 10)
+    s.scen.k += 10
+    for x, y in zip(ahead, s.scen.frame_inputs(10)):
+        np.testing.assert_array_equal(x, y)
