@@ -1840,7 +1840,7 @@ __device__ __forceinline__ void shape_row(int idx, int n, const StepParams* __re
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
 template <bool ROBUST>
-__global__ void __launch_bounds__(kBlock, 3) k_shape_match(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, 4) k_shape_match(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
 	const int* __restrict__ off, const int* __restrict__ nbr, const float4* __restrict__ shape_rest,
 	float4* __restrict__ shape_q)
@@ -2578,7 +2578,7 @@ __device__ __forceinline__ unsigned long long sc_near_key(const Hash27& Href, fl
 // cell starts and (p, index) by cell.  Thread t takes the t-th particle in cell order, so
 // the lanes of a warp share cells and row ranges and run even trip counts (particles
 // outside the grid got their zero count from k_sc_near_scatter).
-__global__ void __launch_bounds__(kBlock) k_sc_build_near(int n, const StepParams* __restrict__ P,
+__global__ void __launch_bounds__(kBlock, 6) k_sc_build_near(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
 	const unsigned char* __restrict__ active, const int* __restrict__ start_f, unsigned int mask,
 	const float4* __restrict__ fp, const int* __restrict__ perm, DevCounters* __restrict__ ctr,
