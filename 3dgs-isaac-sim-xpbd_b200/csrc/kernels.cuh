@@ -1839,6 +1839,8 @@ __device__ __forceinline__ void shape_row(int idx, int n, const StepParams* __re
 	const float3 o = add3(pi, mul3(sub3(goal, pi), scale));
 	pout[idx] = make_float4(o.x, o.y, o.z, p4.w);
 }
+// four resident blocks per SM (64 registers, some spills): more warps hide the FP64
+// chain's latency better than fewer spills (measured against three and five)
 template <bool ROBUST>
 __global__ void __launch_bounds__(kBlock, 4) k_shape_match(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ pin, float4* __restrict__ pout, const float4* __restrict__ rest,
@@ -2578,6 +2580,8 @@ __device__ __forceinline__ unsigned long long sc_near_key(const Hash27& Href, fl
 // cell starts and (p, index) by cell.  Thread t takes the t-th particle in cell order, so
 // the lanes of a warp share cells and row ranges and run even trip counts (particles
 // outside the grid got their zero count from k_sc_near_scatter).
+// six resident blocks per SM: the row scans are latency bound; the spills fall in the
+// rarely used key batches
 __global__ void __launch_bounds__(kBlock, 6) k_sc_build_near(int n, const StepParams* __restrict__ P,
 	const float4* __restrict__ X, const float4* __restrict__ Pp, const float4* __restrict__ rest,
 	const unsigned char* __restrict__ active, const int* __restrict__ start_f, unsigned int mask,
