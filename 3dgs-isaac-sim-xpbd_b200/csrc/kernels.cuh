@@ -2951,7 +2951,11 @@ __global__ void __launch_bounds__(kBlock) k_jstats(int n, const float4* __restri
 // deformed Gaussian shapes (deformedShapeKernel, forward.cu:13063-13225; robust
 // F estimate forward.cu:450) with the FP64 Jacobi of symEig3Double (13022-13060)
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void sym_eig3_double(double a[3][3], double ev[3], double V[3][3])
+// Eigen-decomposition of a symmetric 3x3 matrix in FP64 by cyclic Jacobi sweeps over the
+// pivots (0,1), (0,2), (1,2) (symEig3Double's order and stop: off-diagonal mass below
+// 1e-15 of the diagonal's, at most 32 sweeps), each rotation the one shape matching uses
+// (jacobi_rotate_d).  Columns of V: eigenvectors; ev: eigenvalues in diagonal order.
+__device__ __noinline__ void sym_eig3_double(double (&a)[3][3], double (&ev)[3], double (&V)[3][3])
 {
 #pragma unroll
 	for (int r = 0; r < 3; ++r)
@@ -2961,34 +2965,9 @@ __device__ __noinline__ void sym_eig3_double(double a[3][3], double ev[3], doubl
 		const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
 		const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
 		if (off <= 1e-15 * diag + 1e-300) break;
-#pragma unroll
-		for (int k = 0; k < 3; ++k) {
-			const int p = (k == 2) ? 1 : 0, q = (k == 0) ? 1 : 2;
-			const double apq = a[p][q];
-			if (fabs(apq) <= 1e-300) continue;
-			const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
-			const double t = ((theta >= 0.0) ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-			const double c = 1.0 / sqrt(t * t + 1.0);
-			const double s = t * c;
-#pragma unroll
-			for (int m = 0; m < 3; ++m) {
-				const double amp = a[m][p], amq = a[m][q];
-				a[m][p] = c * amp - s * amq;
-				a[m][q] = s * amp + c * amq;
-			}
-#pragma unroll
-			for (int m = 0; m < 3; ++m) {
-				const double apm = a[p][m], aqm = a[q][m];
-				a[p][m] = c * apm - s * aqm;
-				a[q][m] = s * apm + c * aqm;
-			}
-#pragma unroll
-			for (int m = 0; m < 3; ++m) {
-				const double vmp = V[m][p], vmq = V[m][q];
-				V[m][p] = c * vmp - s * vmq;
-				V[m][q] = s * vmp + c * vmq;
-			}
-		}
+		if (fabs(a[0][1]) > 1e-300) jacobi_rotate_d<0, 1>(a, V);
+		if (fabs(a[0][2]) > 1e-300) jacobi_rotate_d<0, 2>(a, V);
+		if (fabs(a[1][2]) > 1e-300) jacobi_rotate_d<1, 2>(a, V);
 	}
 	ev[0] = a[0][0]; ev[1] = a[1][1]; ev[2] = a[2][2];
 }
